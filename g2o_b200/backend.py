@@ -1,0 +1,309 @@
+"""Python host side of the B200 solver backend, over the C-ABI of
+include/g2o_cuda.h (libg2o_b200.so, built in-tree by g2o_b200/build.py).
+
+It mirrors the reference's plugin interface for this path:
+
+* ``OptimizationAlgorithmFactory.instance().construct(name)`` returns the
+  parameters of a registered algorithm ("lm_cuda", "gn_cuda_pcg6_3", ...) or
+  ``None`` for an unknown name, as g2o's factory returns nullptr
+  (g2o/core/optimization_algorithm_factory.cpp:74-84);
+* ``SparseOptimizer`` holds a graph, ``initialize_optimization()`` uploads it
+  (initializeOptimization + buildStructure), ``optimize(n)`` runs n outer
+  iterations and returns the iteration count (0 on Fail, -1 when not
+  initialized), ``active_chi2()`` / ``active_robust_chi2()`` give the chi2.
+
+There is no CPU fallback: if the library or a CUDA device is missing, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import List, Optional
+
+import numpy as np
+
+from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocHessianInfo, G2ocIterationStats, G2ocParams,
+                  Graph, POSE_DIM, POSE_EST_DIM)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libg2o_b200.so")
+HEADER_PATH = os.path.join(_HERE, "..", "include", "g2o_cuda.h")
+_LIB = None
+
+
+class G2ocError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{ERROR_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def library() -> C.CDLL:
+    """Load libg2o_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: build it with `python -m g2o_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    sig = {
+        "g2oc_abi_version": ([], C.c_int),
+        "g2oc_last_error": ([], C.c_char_p),
+        "g2oc_default_params": ([vp], None),
+        "g2oc_list_solvers": ([C.c_char_p, C.c_size_t], C.c_int),
+        "g2oc_construct": ([C.c_char_p, vp], C.c_int),
+        "g2oc_create": ([C.c_int, C.POINTER(vp)], C.c_int),
+        "g2oc_destroy": ([vp], None),
+        "g2oc_set_params": ([vp, vp], C.c_int),
+        "g2oc_upload": ([vp, vp], C.c_int),
+        "g2oc_get_hessian_info": ([vp, vp], C.c_int),
+        "g2oc_set_estimates": ([vp, dp, dp], C.c_int),
+        "g2oc_download": ([vp, dp, dp], C.c_int),
+        "g2oc_optimize": ([vp, C.c_int, vp, C.POINTER(C.c_int)], C.c_int),
+        "g2oc_chi2": ([vp, dp, dp], C.c_int),
+        "g2oc_errors": ([vp, dp], C.c_int),
+        "g2oc_jacobians": ([vp, dp, dp], C.c_int),
+        "g2oc_build_system": ([vp], C.c_int),
+        "g2oc_get_pattern": ([vp, ip, ip, ip], C.c_int),
+        "g2oc_get_hessian": ([vp, dp, dp, dp, dp], C.c_int),
+        "g2oc_schur": ([vp, C.c_double, dp, dp], C.c_int),
+        "g2oc_solve": ([vp, C.c_double, dp, ip], C.c_int),
+        "g2oc_solve_block_system": ([vp, C.c_int32, C.c_int32, ip, C.c_int32, ip, dp, dp, dp, ip], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = L
+    return L
+
+
+def header_symbols(path: str = HEADER_PATH) -> List[str]:
+    """Function names declared in include/g2o_cuda.h."""
+    text = open(path).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(g2oc_\w+)\s*\(", text, re.M)))
+
+
+def _check(status):
+    if status != 0:
+        msg = library().g2oc_last_error()
+        raise G2ocError(status, msg.decode() if msg else "")
+
+
+def _p(a, t=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def default_params(**kw) -> G2ocParams:
+    p = G2ocParams()
+    library().g2oc_default_params(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class OptimizationAlgorithmFactory:
+    """Name registry of the backend's algorithms (g2o's OptimizationAlgorithmFactory)."""
+
+    _instance = None
+
+    @classmethod
+    def instance(cls):
+        if cls._instance is None:
+            cls._instance = cls()
+        return cls._instance
+
+    def list_solvers(self) -> List[str]:
+        buf = C.create_string_buffer(4096)
+        _check(library().g2oc_list_solvers(buf, len(buf)))
+        return buf.value.decode().split(";")
+
+    def construct(self, name: str) -> Optional[G2ocParams]:
+        p = G2ocParams()
+        st = library().g2oc_construct(name.encode(), C.byref(p))
+        if st != 0:
+            return None
+        return p
+
+
+class CudaProblem:
+    """One device context holding one graph: the C-ABI handle."""
+
+    def __init__(self, graph: Graph, params: Optional[G2ocParams] = None, device: int = 0):
+        self.graph = graph
+        self._h = C.c_void_p()
+        _check(library().g2oc_create(device, C.byref(self._h)))
+        self.params = params or default_params()
+        _check(library().g2oc_set_params(self._h, C.byref(self.params)))
+        self._cg = graph.to_c()
+        _check(library().g2oc_upload(self._h, C.byref(self._cg)))
+        self.info = G2ocHessianInfo()
+        _check(library().g2oc_get_hessian_info(self._h, C.byref(self.info)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            library().g2oc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def is_ba(self):
+        return self.graph.edge_type == EDGE_PROJECT_XYZ2UV
+
+    def set_params(self, params: G2ocParams):
+        self.params = params
+        _check(library().g2oc_set_params(self._h, C.byref(params)))
+
+    def estimates(self):
+        g = self.graph
+        pose = np.empty((g.num_poses, POSE_EST_DIM[g.pose_type]))
+        point = np.empty((max(g.num_points, 1), 3))
+        _check(library().g2oc_download(self._h, _p(pose), _p(point)))
+        return pose, point[: g.num_points]
+
+    def set_estimates(self, pose, point=None):
+        pose = np.ascontiguousarray(pose, np.float64)
+        pt = None if point is None else np.ascontiguousarray(point, np.float64)
+        _check(library().g2oc_set_estimates(self._h, _p(pose), _p(pt)))
+
+    def optimize(self, iterations):
+        stats = (G2ocIterationStats * max(iterations, 1))()
+        done = C.c_int()
+        _check(library().g2oc_optimize(self._h, iterations, stats, C.byref(done)))
+        n = done.value if done.value > 0 else iterations
+        out = []
+        for i in range(iterations):
+            if stats[i].levenberg_iterations == 0 and stats[i].time_iteration == 0 and i >= n:
+                break
+            out.append(stats[i].as_dict())
+        return done.value, out
+
+    def chi2(self):
+        a, b = C.c_double(), C.c_double()
+        _check(library().g2oc_chi2(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def errors(self):
+        e = np.empty((self.info.num_active_edges, self.graph.edge_dim))
+        _check(library().g2oc_errors(self._h, _p(e)))
+        return e
+
+    def jacobians(self):
+        D = self.graph.edge_dim
+        pd = POSE_DIM[self.graph.pose_type]
+        d0 = 3 if self.is_ba else pd
+        n = self.info.num_active_edges
+        j0, j1 = np.empty((n, D, d0)), np.empty((n, D, pd))
+        _check(library().g2oc_jacobians(self._h, _p(j0), _p(j1)))
+        return j0, j1
+
+    def build_system(self):
+        _check(library().g2oc_build_system(self._h))
+
+    def pattern(self):
+        i = self.info
+        hpp = np.empty((i.hpp_nnzb, 2), np.int32)
+        hpl = np.empty((max(i.hpl_nnzb, 1), 2), np.int32)
+        sch = np.empty((max(i.schur_nnzb, 1), 2), np.int32)
+        _check(library().g2oc_get_pattern(self._h, _p(hpp, C.c_int32), _p(hpl, C.c_int32), _p(sch, C.c_int32)))
+        return hpp, hpl[: i.hpl_nnzb], sch[: i.schur_nnzb]
+
+    def hessian(self):
+        i = self.info
+        pd = i.pose_dim
+        hpp = np.empty((i.hpp_nnzb, pd, pd))
+        hll = np.empty((max(i.num_free_points, 1), 3, 3))
+        hpl = np.empty((max(i.hpl_nnzb, 1), pd, 3))
+        b = np.empty(i.vector_size)
+        _check(library().g2oc_get_hessian(self._h, _p(hpp), _p(hll), _p(hpl), _p(b)))
+        return hpp, hll[: i.num_free_points], hpl[: i.hpl_nnzb], b
+
+    def schur(self, lam):
+        i = self.info
+        pd = i.pose_dim
+        S = np.empty((i.schur_nnzb, pd, pd))
+        bs = np.empty(i.num_free_poses * pd)
+        _check(library().g2oc_schur(self._h, lam, _p(S), _p(bs)))
+        return S, bs
+
+    def solve(self, lam):
+        x = np.empty(self.info.vector_size)
+        it = C.c_int32()
+        st = library().g2oc_solve(self._h, lam, _p(x), C.byref(it))
+        return st, x, it.value
+
+
+def solve_block_system(linear_solver, block_offsets, block_rc, values, b, params=None, device=0):
+    """LinearSolver::solve on a caller block matrix through a fresh context."""
+    L = library()
+    h = C.c_void_p()
+    _check(L.g2oc_create(device, C.byref(h)))
+    try:
+        if params is not None:
+            _check(L.g2oc_set_params(h, C.byref(params)))
+        offs = np.ascontiguousarray(block_offsets, np.int32)
+        rc = np.ascontiguousarray(block_rc, np.int32)
+        vals = np.ascontiguousarray(values, np.float64)
+        bb = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(bb)
+        it = C.c_int32()
+        st = L.g2oc_solve_block_system(h, linear_solver, len(offs) - 1, _p(offs, C.c_int32), len(rc),
+                                       _p(rc, C.c_int32), _p(vals), _p(bb), _p(x), C.byref(it))
+        return st, x, it.value
+    finally:
+        L.g2oc_destroy(h)
+
+
+class SparseOptimizer:
+    """The reference's SparseOptimizer driving the device algorithm
+    (g2o/core/sparse_optimizer.cpp:209-287, 393-455)."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.graph: Optional[Graph] = None
+        self.params: Optional[G2ocParams] = None
+        self._problem: Optional[CudaProblem] = None
+        self.batch_statistics = []
+
+    def set_algorithm(self, params: G2ocParams):
+        self.params = params
+        if self._problem is not None:
+            self._problem.set_params(params)
+
+    def set_graph(self, graph: Graph):
+        self.graph = graph
+        self._problem = None
+
+    def initialize_optimization(self) -> bool:
+        if self.graph is None or self.graph.num_edges == 0:
+            return False
+        self._problem = CudaProblem(self.graph, self.params, self.device)
+        return True
+
+    def optimize(self, iterations: int) -> int:
+        if self._problem is None:
+            return -1
+        done, stats = self._problem.optimize(iterations)
+        self.batch_statistics = stats
+        pose, point = self._problem.estimates()
+        self.graph.pose_estimate[...] = pose
+        if self.graph.point_estimate is not None:
+            self.graph.point_estimate[...] = point
+        return done
+
+    def active_chi2(self) -> float:
+        return self._problem.chi2()[0]
+
+    def active_robust_chi2(self) -> float:
+        return self._problem.chi2()[1]

@@ -1,0 +1,479 @@
+// ba_kernels.cuh -- device kernels of the bundle-adjustment path
+// (EdgeProjectXYZ2UV between VertexPointXYZ landmarks, marginalized, and
+// VertexSE3Expmap cameras). Real is the storage/accumulation type of the
+// Jacobians, Hessian blocks and Schur products (double: FP64 path; float:
+// mixed path). Errors, chi2, the gradient b and the solution x are FP64 in
+// both paths.
+//
+// Every sum is a fixed-order reduction (per-thread loop, fixed shuffle tree,
+// fixed shared-memory tree, partials summed in index order), so results are
+// bit-identical run to run; no floating-point atomics.
+#pragma once
+
+#include "g2o_math.cuh"
+#include "reduce.cuh"
+
+namespace g2oc {
+
+struct BAEdges {
+  int n;                  // active edges
+  const int2* v;          // (point index, pose index), point-major device order
+  const double2* z;       // measurement
+  const double4* om;      // (Omega00, Omega01, Omega11, Huber delta; <= 0: none)
+  const int* hpl;         // Hpl block per edge or -1
+};
+
+struct BACamEdges {       // camera-major copy of the edges of free cameras
+  const int* ptr;         // Cf + 1
+  const int2* v;
+  const double2* z;
+  const double4* om;
+};
+
+struct BAVertices {
+  double* cam;            // C x 8: qx qy qz qw tx ty tz pad (SE3Quat)
+  double* pt;             // P x 4: x y z pad
+  const int* free_pose;   // Cf: pose index of Hessian row h
+  const int* free_point;  // Pf: point index of landmark l
+  double f, cx, cy;
+};
+
+// Per-edge residual, robust weight and weighted error in FP64.
+// robust weight = rho'(e^T Omega e) (BaseEdge::robustInformation keeps rho'
+// only, g2o/core/base_edge.h:156-162); we = -rho' Omega e
+// (BaseFixedSizedEdge::constructQuadraticForm, base_fixed_sized_edge.hpp:48-63).
+__device__ __forceinline__ void ba_edge_error(const BAVertices& V, int2 v, double2 z, double4 om,
+                                              double e[2], double Xc[3], double& chi2, double& w) {
+  const double* cam = V.cam + (size_t)v.y * 8;
+  const double* X = V.pt + (size_t)v.x * 4;
+  ba_transform(cam, X, Xc);
+  e[0] = z.x - (Xc[0] / Xc[2] * V.f + V.cx);
+  e[1] = z.y - (Xc[1] / Xc[2] * V.f + V.cy);
+  const double t0 = om.x * e[0] + om.y * e[1];
+  const double t1 = om.y * e[0] + om.z * e[1];
+  chi2 = e[0] * t0 + e[1] * t1;
+  w = 1.0;
+  if (om.w > 0.0) {
+    double rho[3];
+    huber(chi2, om.w, rho);
+    w = rho[1];
+  }
+}
+
+// computeActiveErrors + activeChi2 / activeRobustChi2
+// (g2o/core/sparse_optimizer.cpp:78-130): partials[2*block] = (chi2, robust)
+__global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials) {
+  double c = 0.0, r = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n; k += gridDim.x * blockDim.x) {
+    double e[2], Xc[3], chi2, w;
+    const double4 om = E.om[k];
+    ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, w);
+    c += chi2;
+    if (om.w > 0.0) {
+      double rho[3];
+      huber(chi2, om.w, rho);
+      r += rho[0];
+    } else {
+      r += chi2;
+    }
+  }
+  block_sum2(c, r, partials + 2 * blockIdx.x);
+}
+
+// per-edge errors (parity hook)
+__global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= E.n) return;
+  double e[2], Xc[3], chi2, w;
+  ba_edge_error(V, E.v[k], E.z[k], E.om[k], e, Xc, chi2, w);
+  err[2 * k] = e[0];
+  err[2 * k + 1] = e[1];
+}
+
+// per-edge Jacobians in FP64 (parity hook): Jp 2x3, Jc 2x6
+__global__ void ba_jacobians_kernel(BAEdges E, BAVertices V, double* jp, double* jc) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= E.n) return;
+  const int2 v = E.v[k];
+  const double* cam = V.cam + (size_t)v.y * 8;
+  double Xc[3];
+  ba_transform(cam, V.pt + (size_t)v.x * 4, Xc);
+  double Jp[6], Jc[12];
+  ba_jacobians_from_xc(cam, Xc, V.f, Jp, Jc);
+  for (int i = 0; i < 6; ++i) jp[6 * k + i] = Jp[i];
+  for (int i = 0; i < 12; ++i) jc[12 * k + i] = Jc[i];
+}
+
+// Landmark pass of BlockSolver::buildSystem (block_solver.hpp:492-565) for the
+// landmark side: one thread per free landmark walks its edges (contiguous in
+// the point-major order), accumulates H_ll = sum Jp^T Om' Jp and
+// b_l = sum Jp^T we, and writes each Hpl block Jc^T Om' Jp (the transposed
+// mapping of block_solver.hpp:210-216). Edges sharing a (camera, landmark)
+// block are adjacent and summed in order.
+template <typename Real>
+__global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int Pf, Real* hll, Real* hpl,
+                                 double* b_l) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  Real H[6] = {0, 0, 0, 0, 0, 0};
+  double bl[3] = {0, 0, 0};
+  Real B[18];
+  int cur = -1;
+  const int k1 = l_ptr[l + 1];
+  for (int k = l_ptr[l]; k < k1; ++k) {
+    const int2 v = E.v[k];
+    const double4 om = E.om[k];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
+    const double* cam = V.cam + (size_t)v.y * 8;
+    Real camr[8], Xr[3];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) camr[i] = (Real)cam[i];
+    Xr[0] = (Real)Xc[0]; Xr[1] = (Real)Xc[1]; Xr[2] = (Real)Xc[2];
+    Real Jp[6], Jc[12];
+    ba_jacobians_from_xc(camr, Xr, (Real)V.f, Jp, Jc);
+    const double we0 = -w * (om.x * e[0] + om.y * e[1]);
+    const double we1 = -w * (om.y * e[0] + om.z * e[1]);
+    const Real o00 = (Real)(w * om.x), o01 = (Real)(w * om.y), o11 = (Real)(w * om.z);
+    // AtO = Jp^T Om' (3x2)
+    Real A0[3], A1[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      A0[i] = Jp[i] * o00 + Jp[3 + i] * o01;
+      A1[i] = Jp[i] * o01 + Jp[3 + i] * o11;
+    }
+    H[0] += A0[0] * Jp[0] + A1[0] * Jp[3];
+    H[1] += A0[0] * Jp[1] + A1[0] * Jp[4];
+    H[2] += A0[0] * Jp[2] + A1[0] * Jp[5];
+    H[3] += A0[1] * Jp[1] + A1[1] * Jp[4];
+    H[4] += A0[1] * Jp[2] + A1[1] * Jp[5];
+    H[5] += A0[2] * Jp[2] + A1[2] * Jp[5];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bl[i] += (double)Jp[i] * we0 + (double)Jp[3 + i] * we1;
+    const int blk = E.hpl[k];
+    if (blk >= 0) {
+      if (blk != cur) {
+        if (cur >= 0) {
+#pragma unroll
+          for (int i = 0; i < 18; ++i) hpl[(size_t)cur * 18 + i] = B[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 18; ++i) B[i] = Real(0);
+        cur = blk;
+      }
+      // B(6x3) += Jc^T (Om' Jp) = Jc^T (AtO)^T
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) B[r * 3 + c] += Jc[r] * A0[c] + Jc[6 + r] * A1[c];
+    }
+  }
+  if (cur >= 0) {
+#pragma unroll
+    for (int i = 0; i < 18; ++i) hpl[(size_t)cur * 18 + i] = B[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) hll[(size_t)l * 6 + i] = H[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) b_l[(size_t)l * 3 + i] = bl[i];
+}
+
+// Camera pass: one CTA per free camera sums H_pp = sum Jc^T Om' Jc (21 unique)
+// and b_p = sum Jc^T we over the camera's edges with a fixed-order block
+// reduction, and writes the full 6x6 block.
+template <typename Real, int THREADS>
+__global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVertices V, Real* hpp, double* b_p) {
+  const int h = blockIdx.x;
+  Real H[21];
+  double bp[6];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) H[i] = Real(0);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) bp[i] = 0.0;
+  const int j1 = CE.ptr[h + 1];
+  for (int j = CE.ptr[h] + threadIdx.x; j < j1; j += THREADS) {
+    const int2 v = CE.v[j];
+    const double4 om = CE.om[j];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
+    const double* cam = V.cam + (size_t)v.y * 8;
+    Real camr[8], Xr[3];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) camr[i] = (Real)cam[i];
+    Xr[0] = (Real)Xc[0]; Xr[1] = (Real)Xc[1]; Xr[2] = (Real)Xc[2];
+    Real Jp[6], Jc[12];
+    ba_jacobians_from_xc(camr, Xr, (Real)V.f, Jp, Jc);
+    const double we0 = -w * (om.x * e[0] + om.y * e[1]);
+    const double we1 = -w * (om.y * e[0] + om.z * e[1]);
+    const Real o00 = (Real)(w * om.x), o01 = (Real)(w * om.y), o11 = (Real)(w * om.z);
+    Real A0[6], A1[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      A0[i] = Jc[i] * o00 + Jc[6 + i] * o01;
+      A1[i] = Jc[i] * o01 + Jc[6 + i] * o11;
+    }
+    int t = 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = r; c < 6; ++c) H[t++] += A0[r] * Jc[c] + A1[r] * Jc[6 + c];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) bp[i] += (double)Jc[i] * we0 + (double)Jc[6 + i] * we1;
+  }
+  __shared__ double red[THREADS / 32][27];
+  block_sum_array<Real, 21, THREADS>(H, &red[0][0]);
+  block_sum_array<double, 6, THREADS>(bp, &red[0][0]);
+  if (threadIdx.x == 0) {
+    Real* out = hpp + (size_t)h * 36;
+    int t = 0;
+    for (int r = 0; r < 6; ++r)
+      for (int c = r; c < 6; ++c) {
+        out[r * 6 + c] = H[t];
+        out[c * 6 + r] = H[t];
+        ++t;
+      }
+    for (int i = 0; i < 6; ++i) b_p[(size_t)h * 6 + i] = bp[i];
+  }
+}
+
+// ---------------------------------------------------------------- Schur
+// Landmark step of the Schur loop (block_solver.hpp:359-378): Dinv =
+// (H_ll + lambda I)^-1 and, per Hpl block of the landmark, BD = B Dinv.
+template <typename Real>
+__global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_ptr, int Pf, double lambda,
+                               Real* dinv, Real* bd, int* nonfinite) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  const Real* h = hll + (size_t)l * 6;
+  double A[9] = {(double)h[0] + lambda, (double)h[1], (double)h[2],
+                 (double)h[1], (double)h[3] + lambda, (double)h[4],
+                 (double)h[2], (double)h[4], (double)h[5] + lambda};
+  double Di[9];
+  if (!inverse3(A, Di)) *nonfinite = 1;
+  Real D[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    D[i] = (Real)Di[i];
+    dinv[(size_t)l * 9 + i] = D[i];
+  }
+  const int b1 = hb_ptr[l + 1];
+  for (int a = hb_ptr[l]; a < b1; ++a) {
+    const Real* B = hpl + (size_t)a * 18;
+    Real Bl[18];
+#pragma unroll
+    for (int i = 0; i < 18; ++i) Bl[i] = B[i];
+    Real* o = bd + (size_t)a * 18;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        o[r * 3 + c] = Bl[r * 3] * D[c] + Bl[r * 3 + 1] * D[3 + c] + Bl[r * 3 + 2] * D[6 + c];
+  }
+}
+
+// Schur blocks (block_solver.hpp:379-427, with Hschur <- Hpp at :343-345):
+// S(i1,i2) = Hpp(i1,i2) + lambda I [diagonal] - sum over co-observing pairs
+// BD_a B_b^T, pairs in landmark order. Six threads per block, one per row.
+template <typename Real>
+__global__ void schur_blocks(const int* sp_ptr, const int2* sp_ab, const int* s_hpp, int nnzS, const Real* hpp,
+                             const Real* bd, const Real* hpl, double lambda, Real* S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t / 6, r = t % 6;
+  if (s >= nnzS) return;
+  double acc[6];
+  const int hb = s_hpp[s];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) acc[c] = 0.0;
+  const int p1 = sp_ptr[s + 1];
+  for (int p = sp_ptr[s]; p < p1; ++p) {
+    const int2 ab = sp_ab[p];
+    const Real* D = bd + (size_t)ab.x * 18 + r * 3;
+    const Real d0 = D[0], d1 = D[1], d2 = D[2];
+    const Real* B = hpl + (size_t)ab.y * 18;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) acc[c] += (double)(d0 * B[c * 3] + d1 * B[c * 3 + 1] + d2 * B[c * 3 + 2]);
+  }
+  Real* out = S + (size_t)s * 36 + r * 6;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double v = -acc[c];
+    if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + r * 6 + c] + (r == c ? lambda : 0.0);
+    out[c] = (Real)v;
+  }
+}
+
+// Reduced right-hand side (block_solver.hpp:366-392, 429-433): one warp per
+// free camera, bs = r_p - sum_a B_a Dinv_l r_l over the camera's Hpl blocks.
+template <typename Real>
+__global__ void schur_rhs(const int* hc_ptr, const int* hc_blk, const int* hpl_col, int Cf, const Real* hpl,
+                          const Real* dinv, const double* r_p, const double* r_l, double* bs) {
+  const int h = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (h >= Cf) return;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int e1 = hc_ptr[h + 1];
+  for (int p = hc_ptr[h] + lane; p < e1; p += 32) {
+    const int a = hc_blk[p];
+    const int l = hpl_col[a];
+    const Real* D = dinv + (size_t)l * 9;
+    const double* rl = r_l + (size_t)l * 3;
+    double db[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) db[i] = (double)D[i * 3] * rl[0] + (double)D[i * 3 + 1] * rl[1] + (double)D[i * 3 + 2] * rl[2];
+    const Real* B = hpl + (size_t)a * 18;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[r] += (double)B[r * 3] * db[0] + (double)B[r * 3 + 1] * db[1] + (double)B[r * 3 + 2] * db[2];
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
+  if (lane < 6) {
+    double v = acc[0];
+#pragma unroll
+    for (int r = 1; r < 6; ++r)
+      if (lane == r) v = acc[r];
+    bs[(size_t)h * 6 + lane] = r_p[(size_t)h * 6 + lane] - v;
+  }
+}
+
+// Landmark back-substitution (block_solver.hpp:449-474):
+// x_l = Dinv (r_l - sum_a B_a^T x_p(row a))
+template <typename Real>
+__global__ void ba_backsub(const int* hb_ptr, const int* hpl_row, int Pf, const Real* hpl, const Real* dinv,
+                           const double* r_l, const double* x_p, double* x_l) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  double cl[3] = {r_l[(size_t)l * 3], r_l[(size_t)l * 3 + 1], r_l[(size_t)l * 3 + 2]};
+  const int b1 = hb_ptr[l + 1];
+  for (int a = hb_ptr[l]; a < b1; ++a) {
+    const Real* B = hpl + (size_t)a * 18;
+    const double* xp = x_p + (size_t)hpl_row[a] * 6;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) s += (double)B[r * 3 + c] * xp[r];
+      cl[c] -= s;
+    }
+  }
+  const Real* D = dinv + (size_t)l * 9;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    x_l[(size_t)l * 3 + i] = (double)D[i * 3] * cl[0] + (double)D[i * 3 + 1] * cl[1] + (double)D[i * 3 + 2] * cl[2];
+}
+
+// Residual of the damped full system in FP64 for the mixed-precision
+// refinement: r_p = b_p - (Hpp + lambda I) x_p - sum_a B_a x_l
+template <typename Real>
+__global__ void ba_resid_cam(const int* hc_ptr, const int* hc_blk, const int* hpl_col, int Cf, const Real* hpl,
+                             const Real* hpp, double lambda, const double* b_p, const double* x_p,
+                             const double* x_l, double* r_p) {
+  const int h = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (h >= Cf) return;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int e1 = hc_ptr[h + 1];
+  for (int p = hc_ptr[h] + lane; p < e1; p += 32) {
+    const int a = hc_blk[p];
+    const double* xl = x_l + (size_t)hpl_col[a] * 3;
+    const Real* B = hpl + (size_t)a * 18;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[r] += (double)B[r * 3] * xl[0] + (double)B[r * 3 + 1] * xl[1] + (double)B[r * 3 + 2] * xl[2];
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
+  if (lane < 6) {
+    double v = acc[0];
+#pragma unroll
+    for (int r = 1; r < 6; ++r)
+      if (lane == r) v = acc[r];
+    const Real* H = hpp + (size_t)h * 36 + lane * 6;
+    const double* xp = x_p + (size_t)h * 6;
+    double hx = lambda * xp[lane];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) hx += (double)H[c] * xp[c];
+    r_p[(size_t)h * 6 + lane] = b_p[(size_t)h * 6 + lane] - hx - v;
+  }
+}
+
+// r_l = b_l - sum_a B_a^T x_p - (H_ll + lambda I) x_l
+template <typename Real>
+__global__ void ba_resid_lm(const int* hb_ptr, const int* hpl_row, int Pf, const Real* hpl, const Real* hll,
+                            double lambda, const double* b_l, const double* x_p, const double* x_l, double* r_l) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  const double* xl = x_l + (size_t)l * 3;
+  const Real* h = hll + (size_t)l * 6;
+  double r[3];
+  r[0] = b_l[(size_t)l * 3] - ((double)h[0] * xl[0] + (double)h[1] * xl[1] + (double)h[2] * xl[2] + lambda * xl[0]);
+  r[1] = b_l[(size_t)l * 3 + 1] - ((double)h[1] * xl[0] + (double)h[3] * xl[1] + (double)h[4] * xl[2] + lambda * xl[1]);
+  r[2] = b_l[(size_t)l * 3 + 2] - ((double)h[2] * xl[0] + (double)h[4] * xl[1] + (double)h[5] * xl[2] + lambda * xl[2]);
+  const int b1 = hb_ptr[l + 1];
+  for (int a = hb_ptr[l]; a < b1; ++a) {
+    const Real* B = hpl + (size_t)a * 18;
+    const double* xp = x_p + (size_t)hpl_row[a] * 6;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s += (double)B[q * 3 + c] * xp[q];
+      r[c] -= s;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) r_l[(size_t)l * 3 + i] = r[i];
+}
+
+// SparseOptimizer::update (sparse_optimizer.cpp:457-468) with
+// VertexSE3Expmap::oplusImpl (g2o/types/sba/vertex_se3_expmap.cpp:48-51):
+// T <- exp(dx) * T; VertexPointXYZ: p <- p + dx (vertex_pointxyz.h:47-50)
+__global__ void ba_oplus(BAVertices V, int Cf, int Pf, const double* x, int* nonfinite) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < Cf) {
+    double u[6];
+    bool bad = false;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      u[i] = x[(size_t)t * 6 + i];
+      bad |= !isfinite(u[i]);
+    }
+    if (bad) *nonfinite = 1;
+    double* cam = V.cam + (size_t)V.free_pose[t] * 8;
+    SE3Q<double> T;
+    T.q = Q4<double>{cam[0], cam[1], cam[2], cam[3]};
+    T.t[0] = cam[4]; T.t[1] = cam[5]; T.t[2] = cam[6];
+    SE3Q<double> R = se3q_mul(se3q_exp(u), T);
+    cam[0] = R.q.x; cam[1] = R.q.y; cam[2] = R.q.z; cam[3] = R.q.w;
+    cam[4] = R.t[0]; cam[5] = R.t[1]; cam[6] = R.t[2];
+  } else if (t < Cf + Pf) {
+    const int l = t - Cf;
+    double* p = V.pt + (size_t)V.free_point[l] * 4;
+    const double* u = x + (size_t)Cf * 6 + (size_t)l * 3;
+    if (!isfinite(u[0]) || !isfinite(u[1]) || !isfinite(u[2])) *nonfinite = 1;
+    p[0] += u[0];
+    p[1] += u[1];
+    p[2] += u[2];
+  }
+}
+
+// max |diag| over Hpp and H_ll (computeLambdaInit,
+// optimization_algorithm_levenberg.cpp:155-167): partial maxima per block
+template <typename Real>
+__global__ void ba_max_diag(const Real* hpp, int Cf, const Real* hll, int Pf, double* partials) {
+  double m = 0.0;
+  const int n = Cf * 6 + Pf * 3;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double v;
+    if (t < Cf * 6) {
+      const int h = t / 6, d = t % 6;
+      v = fabs((double)hpp[(size_t)h * 36 + d * 7]);
+    } else {
+      const int l = (t - Cf * 6) / 3, d = (t - Cf * 6) % 3;
+      const int idx = d == 0 ? 0 : d == 1 ? 3 : 5;
+      v = fabs((double)hll[(size_t)l * 6 + idx]);
+    }
+    m = fmax(m, v);
+  }
+  block_max(m, partials + blockIdx.x);
+}
+
+}  // namespace g2oc

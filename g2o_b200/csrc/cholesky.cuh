@@ -1,0 +1,400 @@
+// cholesky.cuh -- LinearSolverCudaCholesky: FP64 tiled Cholesky of the
+// (reduced) block system, the role of LinearSolverEigen's SimplicialLLT and
+// LinearSolverDense's LDLT (g2o/solvers/eigen/linear_solver_eigen.h:94-191,
+// g2o/solvers/dense/linear_solver_dense.h:57-105).
+//
+// Plan (once per pattern, on the host): reverse Cuthill-McKee block ordering
+// for sparse systems, then a symbolic factorization at the level of 64x64
+// tiles, giving per step k the list of nonzero panel tiles and the list of
+// trailing tile pairs to update. Numeric (every solve, on the device): the
+// permuted matrix is expanded into a dense column-major buffer, and only the
+// structurally nonzero tiles are factored (potrf of the diagonal tile, trsm
+// of the panel, gemm/syrk of the trailing tiles), followed by blocked
+// forward / backward substitution. A non-positive pivot sets the info flag
+// (G2OC_ERR_NOT_PD at the boundary); nothing traps.
+#pragma once
+
+#include <algorithm>
+#include <queue>
+#include <vector>
+
+#include "g2oc_internal.h"
+#include "pcg_kernels.cuh"
+
+namespace g2oc {
+
+constexpr int kTile = 64;
+
+struct CholPlan {
+  int nb = 0, bs = 0, n = 0, np = 0, nt = 0;
+  const void* key = nullptr;  // pattern identity
+  std::vector<int> perm;      // block i -> position
+  std::vector<int> pnl_ptr, pnl;     // per k: tiles i > k with L(i,k) != 0
+  std::vector<int> upd_ptr;          // per k: range into upd
+  std::vector<int2> upd;             // trailing pairs (i, j), i >= j > k
+  std::vector<int> bwd_ptr, bwd;     // per k: tiles i < k with L(k,i) != 0
+  DBuf<int> d_perm, d_pnl, d_bwd, d_blkcol;
+  DBuf<int2> d_upd;
+  DBuf<double> A, y;
+  DBuf<int> info;
+};
+
+// reverse Cuthill-McKee on the block graph
+static void rcm_order(int nb, const std::vector<int32_t>& rc, std::vector<int>& perm) {
+  std::vector<std::vector<int>> adj(nb);
+  for (size_t k = 0; k < rc.size() / 2; ++k) {
+    const int r = rc[2 * k], c = rc[2 * k + 1];
+    if (r != c) {
+      adj[r].push_back(c);
+      adj[c].push_back(r);
+    }
+  }
+  std::vector<int> order;
+  order.reserve(nb);
+  std::vector<char> seen(nb, 0);
+  while ((int)order.size() < nb) {
+    int start = -1;
+    size_t best = SIZE_MAX;
+    for (int i = 0; i < nb; ++i)
+      if (!seen[i] && adj[i].size() < best) {
+        best = adj[i].size();
+        start = i;
+      }
+    std::queue<int> q;
+    q.push(start);
+    seen[start] = 1;
+    while (!q.empty()) {
+      const int u = q.front();
+      q.pop();
+      order.push_back(u);
+      std::vector<int> nbr;
+      for (int v : adj[u])
+        if (!seen[v]) {
+          seen[v] = 1;
+          nbr.push_back(v);
+        }
+      std::sort(nbr.begin(), nbr.end(), [&](int a, int b) {
+        return adj[a].size() < adj[b].size() || (adj[a].size() == adj[b].size() && a < b);
+      });
+      for (int v : nbr) q.push(v);
+    }
+  }
+  perm.assign(nb, 0);
+  for (int i = 0; i < nb; ++i) perm[order[nb - 1 - i]] = i;
+}
+
+static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_t>& rc, bool reorder,
+                           const std::vector<int>& col_of_block, cudaStream_t st) {
+  P.nb = nb;
+  P.bs = bs;
+  P.n = nb * bs;
+  P.nt = (P.n + kTile - 1) / kTile;
+  P.np = P.nt * kTile;
+  if (reorder) rcm_order(nb, rc, P.perm);
+  else {
+    P.perm.resize(nb);
+    for (int i = 0; i < nb; ++i) P.perm[i] = i;
+  }
+  const int nt = P.nt;
+  std::vector<char> nz((size_t)nt * nt, 0);
+  auto mark = [&](int r, int c) {
+    const int a0 = P.perm[r] * bs, b0 = P.perm[c] * bs;
+    for (int ti = a0 / kTile; ti <= (a0 + bs - 1) / kTile; ++ti)
+      for (int tj = b0 / kTile; tj <= (b0 + bs - 1) / kTile; ++tj) {
+        const int i = std::max(ti, tj), j = std::min(ti, tj);
+        nz[(size_t)i * nt + j] = 1;
+      }
+  };
+  for (size_t k = 0; k < rc.size() / 2; ++k) mark(rc[2 * k], rc[2 * k + 1]);
+  for (int t = 0; t < nt; ++t) nz[(size_t)t * nt + t] = 1;
+  P.pnl_ptr.assign(nt + 1, 0);
+  P.upd_ptr.assign(nt + 1, 0);
+  P.pnl.clear();
+  P.upd.clear();
+  std::vector<int> cols;
+  for (int k = 0; k < nt; ++k) {
+    cols.clear();
+    for (int i = k + 1; i < nt; ++i)
+      if (nz[(size_t)i * nt + k]) cols.push_back(i);
+    for (size_t a = 0; a < cols.size(); ++a)
+      for (size_t b = 0; b <= a; ++b) {
+        nz[(size_t)cols[a] * nt + cols[b]] = 1;
+        P.upd.push_back(make_int2(cols[a], cols[b]));
+      }
+    P.pnl.insert(P.pnl.end(), cols.begin(), cols.end());
+    P.pnl_ptr[k + 1] = (int)P.pnl.size();
+    P.upd_ptr[k + 1] = (int)P.upd.size();
+  }
+  // backward lists: for k, tiles i < k with L(k, i) != 0
+  P.bwd_ptr.assign(nt + 1, 0);
+  P.bwd.clear();
+  for (int k = 0; k < nt; ++k) {
+    for (int i = 0; i < k; ++i)
+      if (nz[(size_t)k * nt + i]) P.bwd.push_back(i);
+    P.bwd_ptr[k + 1] = (int)P.bwd.size();
+  }
+  G2OC_TRY(P.d_perm.upload(P.perm, st));
+  G2OC_TRY(P.d_pnl.upload(P.pnl.empty() ? std::vector<int>{0} : P.pnl, st));
+  G2OC_TRY(P.d_upd.upload(P.upd.empty() ? std::vector<int2>{make_int2(0, 0)} : P.upd, st));
+  G2OC_TRY(P.d_bwd.upload(P.bwd.empty() ? std::vector<int>{0} : P.bwd, st));
+  G2OC_TRY(P.d_blkcol.upload(col_of_block, st));
+  G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
+  G2OC_TRY(P.y.alloc(P.np));
+  G2OC_TRY(P.info.alloc(1));
+  return G2OC_OK;
+}
+
+// dense column-major A(np x np): permuted blocks and their transposes,
+// identity on the padding
+template <typename Real>
+__global__ void chol_densify(SysDev<Real> S, const int* blk_col, int nnzb, int bs, const int* perm, int n, int np,
+                             double* A) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)bs * bs;
+  if (t < (long long)nnzb * per) {
+    const int p = (int)(t / per), e = (int)(t % per);
+    const int r = S.row[p], c = blk_col[p];
+    const int i = e / bs, j = e % bs;
+    const int gi = perm[r] * bs + i, gj = perm[c] * bs + j;
+    const double v = (double)S.val[(size_t)p * per + e];
+    A[(size_t)gj * np + gi] = v;
+    A[(size_t)gi * np + gj] = v;
+  } else {
+    const long long pad = t - (long long)nnzb * per;
+    if (pad < np - n) {
+      const int g = n + (int)pad;
+      A[(size_t)g * np + g] = 1.0;
+    }
+  }
+}
+
+// factor the diagonal tile k in shared memory (lower)
+__global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
+  __shared__ double T[kTile][kTile + 1];
+  const size_t base = (size_t)k * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int i = e % kTile, j = e / kTile;
+    T[i][j] = A[(base + j) * np + base + i];
+  }
+  __syncthreads();
+  for (int j = 0; j < kTile; ++j) {
+    if (threadIdx.x == 0) {
+      const double d = T[j][j];
+      if (!(d > 0.0)) *info = 1;
+      T[j][j] = sqrt(d > 0.0 ? d : 1.0);
+    }
+    __syncthreads();
+    const double piv = T[j][j];
+    for (int i = j + 1 + threadIdx.x; i < kTile; i += blockDim.x) T[i][j] /= piv;
+    __syncthreads();
+    const int m = kTile - j - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = j + 1 + e % m, c = j + 1 + e / m;
+      if (i >= c) T[i][c] -= T[i][j] * T[c][j];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int i = e % kTile, j = e / kTile;
+    if (i >= j) A[(base + j) * np + base + i] = T[i][j];
+  }
+}
+
+// panel: L(i,k) = A(i,k) L(k,k)^-T for the listed tiles i
+constexpr int kTileSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
+
+__global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
+  extern __shared__ double sm_trsm[];
+  double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
+  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
+  const int ti = tiles[blockIdx.x];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    L[r][c] = A[(kb + c) * np + kb + r];
+    X[r][c] = A[(kb + c) * np + ib + r];
+  }
+  __syncthreads();
+  // each of 4 thread groups handles 16 rows; within a row the columns are sequential
+  const int row = threadIdx.x % kTile;
+  const int grp = threadIdx.x / kTile;  // 0..3
+  if (grp == 0) {
+    for (int c = 0; c < kTile; ++c) {
+      double v = X[row][c];
+      for (int t = 0; t < c; ++t) v -= X[row][t] * L[c][t];
+      X[row][c] = v / L[c][c];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    A[(kb + c) * np + ib + r] = X[r][c];
+  }
+}
+
+// trailing update: A(i,j) -= L(i,k) L(j,k)^T for the listed pairs; 4x4 per thread
+__global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
+  extern __shared__ double sm_gemm[];
+  double (*Li)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm);
+  double (*Lj)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm + kTile * (kTile + 1));
+  const int2 ij = pairs[blockIdx.x];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)ij.x * kTile, jb = (size_t)ij.y * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    Li[r][c] = A[(kb + c) * np + ib + r];
+    Lj[r][c] = A[(kb + c) * np + jb + r];
+  }
+  __syncthreads();
+  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int t = 0; t < kTile; ++t) {
+    double x[4], y[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      x[a] = Li[tr + 16 * a][t];
+      y[a] = Lj[tc + 16 * a][t];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+  }
+  const bool diag = ij.x == ij.y;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = tr + 16 * a, c = tc + 16 * b;
+      if (diag && r < c) continue;
+      A[(jb + c) * np + ib + r] -= acc[a][b];
+    }
+}
+
+// permuted right-hand side y(perm) = b
+__global__ void chol_load_rhs(const double* b, const int* perm, int nb, int bs, int n, int np, double* y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) y[perm[t / bs] * bs + t % bs] = b[t];
+  else if (t < np) y[t] = 0.0;
+}
+
+__global__ void chol_store_x(const double* y, const int* perm, int bs, int n, double* x) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) x[t] = y[perm[t / bs] * bs + t % bs];
+}
+
+// L(k,k) y_k = y_k
+__global__ void chol_fwd_diag(const double* A, int np, int k, double* y) {
+  __shared__ double v[kTile];
+  const size_t kb = (size_t)k * kTile;
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int r = 0; r < kTile; ++r) {
+      double s = v[r];
+      for (int t = 0; t < r; ++t) s -= A[(kb + t) * np + kb + r] * v[t];
+      v[r] = s / A[(kb + r) * np + kb + r];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+}
+
+// y_i -= L(i,k) y_k for the listed tiles i > k
+__global__ void chol_fwd_update(const double* A, int np, int k, const int* tiles, double* y) {
+  const int ti = tiles[blockIdx.x];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
+  __shared__ double yk[kTile];
+  if (threadIdx.x < kTile) yk[threadIdx.x] = y[kb + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < kTile) {
+    const int r = threadIdx.x;
+    double s = 0.0;
+    for (int t = 0; t < kTile; ++t) s += A[(kb + t) * np + ib + r] * yk[t];
+    y[ib + r] -= s;
+  }
+}
+
+// L(k,k)^T x_k = y_k
+__global__ void chol_bwd_diag(const double* A, int np, int k, double* y) {
+  __shared__ double v[kTile];
+  const size_t kb = (size_t)k * kTile;
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int r = kTile - 1; r >= 0; --r) {
+      double s = v[r];
+      for (int t = r + 1; t < kTile; ++t) s -= A[(kb + r) * np + kb + t] * v[t];
+      v[r] = s / A[(kb + r) * np + kb + r];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+}
+
+// y_i -= L(k,i)^T y_k for the listed tiles i < k
+__global__ void chol_bwd_update(const double* A, int np, int k, const int* tiles, double* y) {
+  const int ti = tiles[blockIdx.x];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
+  __shared__ double yk[kTile];
+  if (threadIdx.x < kTile) yk[threadIdx.x] = y[kb + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x < kTile) {
+    const int c = threadIdx.x;
+    double s = 0.0;
+    for (int t = 0; t < kTile; ++t) s += A[(ib + c) * np + kb + t] * yk[t];
+    y[ib + c] -= s;
+  }
+}
+
+template <typename Real>
+static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, int nnzb, const double* rhs, double* xout,
+                      int* ok) {
+  const int np = P.np, nt = P.nt;
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  G2OC_CUDA_TRY(cudaMemsetAsync(P.A.p, 0, P.A.bytes(), st));
+  G2OC_CUDA_TRY(cudaMemsetAsync(P.info.p, 0, sizeof(int), st));
+  const long long work = (long long)nnzb * P.bs * P.bs + (np - P.n);
+  chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.d_blkcol.p, nnzb, P.bs, P.d_perm.p, P.n, np,
+                                                                 P.A.p);
+  for (int k = 0; k < nt; ++k) {
+    chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.info.p);
+    const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
+    if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k]);
+    const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];
+    if (nu > 0) chol_gemm<<<nu, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_upd.p + P.upd_ptr[k]);
+  }
+  const cudaError_t e1 = cudaGetLastError();
+  if (e1 != cudaSuccess) {
+    set_error("cholesky launch: %s", cudaGetErrorString(e1));
+    return G2OC_ERR_CUDA;
+  }
+  chol_load_rhs<<<(np + 255) / 256, 256, 0, st>>>(rhs, P.d_perm.p, P.nb, P.bs, P.n, np, P.y.p);
+  for (int k = 0; k < nt; ++k) {
+    chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
+    const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
+    if (np_k > 0) chol_fwd_update<<<np_k, kTile, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
+  }
+  for (int k = nt - 1; k >= 0; --k) {
+    chol_bwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
+    const int nbk = P.bwd_ptr[k + 1] - P.bwd_ptr[k];
+    if (nbk > 0) chol_bwd_update<<<nbk, kTile, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
+  }
+  chol_store_x<<<(P.n + 255) / 256, 256, 0, st>>>(P.y.p, P.d_perm.p, P.bs, P.n, xout);
+  const cudaError_t e2 = cudaGetLastError();
+  if (e2 != cudaSuccess) {
+    set_error("cholesky solve launch: %s", cudaGetErrorString(e2));
+    return G2OC_ERR_CUDA;
+  }
+  int info = 0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&info, P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  *ok = info == 0;
+  return G2OC_OK;
+}
+
+}  // namespace g2oc

@@ -1,0 +1,1206 @@
+// g2oc_api.cu -- the C-ABI of include/g2o_cuda.h: context, upload, the
+// Gauss-Newton / Levenberg-Marquardt drivers over the device block solver,
+// and the parity hooks. Host code only orchestrates: every per-edge,
+// per-vertex, per-block and per-vector loop of the iteration runs in the
+// kernels of ba_kernels.cuh, pg_kernels.cuh, pcg_kernels.cuh,
+// lm_kernels.cuh and cholesky.cuh.
+#include <cstdarg>
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ba_kernels.cuh"
+#include "cholesky.cuh"
+#include "g2oc_internal.h"
+#include "lm_kernels.cuh"
+#include "pcg_kernels.cuh"
+#include "pg_kernels.cuh"
+
+namespace g2oc {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+#define G2OC_LAUNCH_CHECK()                                                             \
+  do {                                                                                  \
+    cudaError_t _e = cudaGetLastError();                                                \
+    if (_e != cudaSuccess) {                                                            \
+      ::g2oc::set_error("%s:%d kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(_e)); \
+      return G2OC_ERR_CUDA;                                                             \
+    }                                                                                   \
+  } while (0)
+
+static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs: fixed grid of the reductions
+constexpr int kPcgChunkMax = 64;
+
+// --------------------------------------------------------------- engine
+struct EngineBase {
+  virtual ~EngineBase() = default;
+  virtual int alloc() = 0;
+  virtual int build_system() = 0;
+  virtual int max_diag() = 0;  // -> sc.max_diag
+  virtual int solve(double lambda, int* pcg_iters) = 0;  // -> x, sc.solve_ok
+  virtual int get_hessian(double* hpp, double* hll, double* hpl) = 0;
+  virtual int schur_export(double lambda, double* S, double* bs) = 0;
+};
+
+}  // namespace g2oc
+
+struct g2oc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  g2oc_params prm{};
+  g2oc::Structure S;
+  bool uploaded = false;
+  bool system_built = false;
+  double f = 1, cx = 0, cy = 0;
+  // vertex state
+  g2oc::DBuf<double> pose, point, pose_bak, point_bak;
+  g2oc::DBuf<int> oplus_count, free_pose, free_point;
+  // BA edges
+  g2oc::DBuf<int2> e_v, c_v;
+  g2oc::DBuf<double2> e_z, c_z;
+  g2oc::DBuf<double4> e_om, c_om;
+  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, sp_ptr, s_hpp;
+  g2oc::DBuf<int2> sp_ab;
+  // pose-graph edges
+  g2oc::DBuf<int2> pe_v;
+  g2oc::DBuf<double> pe_zinv, pe_info, pe_delta;
+  g2oc::DBuf<uint8_t> pe_trans;
+  g2oc::DBuf<int> hb_src_ptr, hb_src, bv_src_ptr, bv_src;
+  // linear system lists
+  g2oc::DBuf<int> sys_col_ptr, sys_row, sys_diag, sys_rowu_ptr, sys_rowu_blk, sys_rowu_col;
+  // FP64 vectors
+  g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf;
+  g2oc::DBuf<g2oc::DevScalars> sc;
+  g2oc::DBuf<g2oc::PcgState> pcg;
+  g2oc::DBuf<int> flag;  // nonfinite flag
+  std::unique_ptr<g2oc::EngineBase> eng;
+  std::unique_ptr<g2oc::CholPlan> chol;
+  int last_pcg_iterations = 0;
+  ~g2oc_ctx() {
+    eng.reset();
+    chol.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+  int vec_size() const { return S.Cf * S.pd + S.Pf * 3; }
+  g2oc::BAVertices ba_vertices() {
+    g2oc::BAVertices V;
+    V.cam = pose.p;
+    V.pt = point.p;
+    V.free_pose = free_pose.p;
+    V.free_point = free_point.p;
+    V.f = f;
+    V.cx = cx;
+    V.cy = cy;
+    return V;
+  }
+  g2oc::BAEdges ba_edges() {
+    g2oc::BAEdges E;
+    E.n = (int)S.act.size();
+    E.v = e_v.p;
+    E.z = e_z.p;
+    E.om = e_om.p;
+    E.hpl = e_hpl.p;
+    return E;
+  }
+  g2oc::PGEdges pg_edges() {
+    g2oc::PGEdges E;
+    E.n = (int)S.act.size();
+    E.v = pe_v.p;
+    E.zinv = pe_zinv.p;
+    E.info = pe_info.p;
+    E.delta = pe_delta.p;
+    return E;
+  }
+};
+
+namespace g2oc {
+
+// ------------------------------------------------------------ PCG driver
+template <typename Real, int BS>
+static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const Real* minv, const double* rhs, double* xout, Real* r,
+                   Real* s, Real* d0, Real* d1, Real* q, bool relative_only, int* iters) {
+  cudaStream_t st = c->stream;
+  PcgState cfg{};
+  // configure the state (keeps residual_carry)
+  PcgState host;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  cfg = host;
+  cfg.tolerance = c->prm.pcg_tolerance;
+  cfg.max_iter = c->prm.pcg_max_iterations < 0 ? A.nb * BS : c->prm.pcg_max_iterations;
+  cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
+  cfg.relative_only = relative_only ? 1 : 0;
+  cfg.counter = 0;
+  cfg.done = 0;
+  cfg.k = 0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+  const int nbv = cdiv(A.nb, 128);
+  pcg_init<Real, BS><<<nbv, 128, 0, st>>>(A.nb, rhs, minv, r, s, xout, c->partials.p, c->pcg.p);
+  G2OC_LAUNCH_CHECK();
+  constexpr int SPMV_T = 256;
+  const int nbs = cdiv(A.nb, SPMV_T / 32);
+  int chunk = 4;
+  int launched = 0;
+  for (;;) {
+    for (int k = 0; k < chunk; ++k) {
+      pcg_spmv<Real, BS, SPMV_T><<<nbs, SPMV_T, 0, st>>>(A, s, d0, d1, q, c->partials.p, c->pcg.p);
+      pcg_update<Real, BS><<<nbv, 128, 0, st>>>(A.nb, minv, d0, d1, q, r, s, xout, c->partials.p, c->pcg.p);
+    }
+    G2OC_LAUNCH_CHECK();
+    launched += chunk;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    if (host.done) break;
+    if (launched > cfg.max_iter + 2) {
+      set_error("PCG did not report completion after %d iterations", launched);
+      return G2OC_ERR_TIMEOUT;
+    }
+    chunk = chunk * 2 > kPcgChunkMax ? kPcgChunkMax : chunk * 2;
+  }
+  if (iters) *iters = host.iterations;
+  return G2OC_OK;
+}
+
+static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, double* out1, double add0 = 0.0) {
+  finalize_sum_kernel<<<1, 256, 0, c->stream>>>(c->partials.p, nparts, stride, out0, out1, add0);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
+// ---------------------------------------------------------- the engine
+template <typename Real>
+struct Engine final : EngineBase {
+  g2oc_ctx* c;
+  // Hessian
+  DBuf<Real> hpp, hll, hpl, bd, dinv, Sval, sysval, minv;
+  DBuf<Real> r, s, d0, d1, q;
+  DBuf<Real> hcontrib;
+  DBuf<double> bcontrib;
+  explicit Engine(g2oc_ctx* ctx) : c(ctx) {}
+
+  int alloc() override {
+    const Structure& S = c->S;
+    const int pd = S.pd;
+    G2OC_TRY(hpp.alloc((size_t)S.hpp_rc.size() / 2 * pd * pd));
+    if (S.ba) {
+      G2OC_TRY(hll.alloc((size_t)S.Pf * 6 + 1));
+      G2OC_TRY(hpl.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
+      G2OC_TRY(bd.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
+      G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
+      G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
+    } else {
+      G2OC_TRY(hcontrib.alloc((size_t)S.act.size() * 3 * pd * pd));
+      G2OC_TRY(bcontrib.alloc((size_t)S.act.size() * 2 * pd));
+    }
+    if (!(S.ba && S.schur)) G2OC_TRY(sysval.alloc((size_t)S.sys_nnzb * pd * pd + 1));
+    const size_t n = (size_t)S.Cf * pd;
+    G2OC_TRY(minv.alloc((size_t)S.Cf * pd * pd));
+    G2OC_TRY(r.alloc(n));
+    G2OC_TRY(s.alloc(n));
+    G2OC_TRY(d0.alloc(n));
+    G2OC_TRY(d1.alloc(n));
+    G2OC_TRY(q.alloc(n));
+    return G2OC_OK;
+  }
+
+  SysDev<Real> sys(const Real* val) {
+    SysDev<Real> A;
+    A.nb = c->S.sys_nb;
+    A.col_ptr = c->sys_col_ptr.p;
+    A.row = c->sys_row.p;
+    A.diag = c->sys_diag.p;
+    A.rowu_ptr = c->sys_rowu_ptr.p;
+    A.rowu_blk = c->sys_rowu_blk.p;
+    A.rowu_col = c->sys_rowu_col.p;
+    A.val = val;
+    return A;
+  }
+
+  int build_system() override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.ba) {
+      if (S.Pf > 0) {
+        ba_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf,
+                                                                 hll.p, hpl.p, c->b.p + (size_t)S.Cf * 6);
+        G2OC_LAUNCH_CHECK();
+      }
+      if (S.Cf > 0) {
+        BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
+        ba_camera_pass<Real, 128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), hpp.p, c->b.p);
+        G2OC_LAUNCH_CHECK();
+      }
+    } else {
+      const int n = (int)S.act.size();
+      if (S.pose_type == G2OC_POSE_SE2) {
+        pg_linearize<Real, G2OC_POSE_SE2><<<cdiv(n, 128), 128, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
+                                                                        hcontrib.p, bcontrib.p);
+        G2OC_LAUNCH_CHECK();
+        const int nnzb = (int)S.hpp_rc.size() / 2;
+        pg_assemble_h<Real, 3><<<cdiv((long long)nnzb * 3, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
+                                                                               hcontrib.p, hpp.p);
+        pg_assemble_b<3><<<cdiv((long long)S.Cf * 3, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
+                                                                       bcontrib.p, c->b.p);
+      } else {
+        pg_linearize<Real, G2OC_POSE_SE3><<<cdiv(n, 64), 64, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
+                                                                      hcontrib.p, bcontrib.p);
+        G2OC_LAUNCH_CHECK();
+        const int nnzb = (int)S.hpp_rc.size() / 2;
+        pg_assemble_h<Real, 6><<<cdiv((long long)nnzb * 6, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
+                                                                               hcontrib.p, hpp.p);
+        pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
+                                                                       bcontrib.p, c->b.p);
+      }
+      G2OC_LAUNCH_CHECK();
+    }
+    return G2OC_OK;
+  }
+
+  int max_diag() override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.ba) ba_max_diag<Real><<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
+    else if (S.pd == 3) pg_max_diag<Real, 3><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
+    else pg_max_diag<Real, 6><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
+    G2OC_LAUNCH_CHECK();
+    finalize_max_kernel<<<1, 256, 0, st>>>(c->partials.p, kRedBlocks, &c->sc.p->max_diag);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  // S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T, with Dinv and BD
+  int schur(double lambda) {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.Pf > 0) {
+      schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
+                                                             c->flag.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    const int nnzS = (int)S.schur_rc.size() / 2;
+    if (nnzS == 0) return G2OC_OK;
+    schur_blocks<Real><<<cdiv((long long)nnzS * 6, 192), 192, 0, st>>>(c->sp_ptr.p, c->sp_ab.p, c->s_hpp.p, nnzS,
+                                                                      hpp.p, bd.p, hpl.p, lambda, Sval.p);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int schur_rhs_from(const double* rp, const double* rl, double* bs) {
+    const Structure& S = c->S;
+    schur_rhs<Real><<<cdiv(S.Cf, 4), 128, 0, c->stream>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p,
+                                                          dinv.p, rp, rl, bs);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int pcg_solve(const Real* val, const double* rhs, double* xout, bool relative_only, int* iters) {
+    const Structure& S = c->S;
+    SysDev<Real> A = sys(val);
+    if (S.pd == 6) {
+      pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+      G2OC_LAUNCH_CHECK();
+      return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, relative_only, iters);
+    }
+    pcg_diag_inv<Real, 3><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+    G2OC_LAUNCH_CHECK();
+    return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, relative_only, iters);
+  }
+
+  int chol_solve(const Real* val, const double* rhs, double* xout, int* ok) {
+    const Structure& S = c->S;
+    if (!c->chol) {
+      const std::vector<int32_t>& rc = S.ba ? S.schur_rc : S.hpp_rc;
+      std::vector<int> col(rc.size() / 2);
+      for (size_t k = 0; k < col.size(); ++k) col[k] = rc[2 * k + 1];
+      std::unique_ptr<CholPlan> P(new CholPlan());
+      G2OC_TRY(chol_plan_build(*P, S.sys_nb, S.pd, rc, !S.ba, col, c->stream));
+      c->chol = std::move(P);
+    }
+    return g2oc::chol_solve<Real>(*c->chol, c->stream, sys(val), S.sys_nnzb, rhs, xout, ok);
+  }
+
+  int solve(double lambda, int* pcg_iters) override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    int it_total = 0, it = 0;
+    int ok = 1;
+    const bool use_chol = c->prm.linear_solver == G2OC_LINEAR_CHOLESKY ||
+                          (c->prm.linear_solver == 2 && !S.ba);
+    if (S.Cf == 0) {
+      // every pose fixed: only the landmarks move, x_l = (H_ll + lambda)^-1 b_l
+      G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, c->x.bytes(), st));
+      if (S.ba && S.Pf > 0) {
+        if (S.schur) {
+          schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
+                                                                 c->flag.p);
+          ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, c->b.p,
+                                                             c->xs.p, c->x.p);
+          G2OC_LAUNCH_CHECK();
+        }
+      }
+    } else if (S.ba && S.schur) {
+      G2OC_TRY(schur(lambda));
+      const double* bp = c->b.p;
+      const double* bl = c->b.p + (size_t)S.Cf * 6;
+      G2OC_TRY(schur_rhs_from(bp, bl, c->rhs.p));
+      if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
+      else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false, &it));
+      it_total += it;
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      if (S.Pf > 0) {
+        ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, bl, c->xs.p,
+                                                           c->x.p + (size_t)S.Cf * 6);
+        G2OC_LAUNCH_CHECK();
+      }
+      // mixed precision: iterative refinement on the FP64 residual of the full damped system
+      if (sizeof(Real) == 4 && ok) {
+        const int n = c->vec_size();
+        for (int k = 0; k < c->prm.refine_max_iterations; ++k) {
+          double* rp = c->resid.p;
+          double* rl = c->resid.p + (size_t)S.Cf * 6;
+          ba_resid_cam<Real><<<cdiv(S.Cf, 4), 128, 0, st>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p, hpp.p,
+                                                            lambda, bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
+          if (S.Pf > 0)
+            ba_resid_lm<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, hll.p, lambda, bl,
+                                                               c->x.p, c->x.p + (size_t)S.Cf * 6, rl);
+          G2OC_LAUNCH_CHECK();
+          G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
+          if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
+          else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true, &it));
+          it_total += it;
+          G2OC_CUDA_TRY(cudaMemcpyAsync(c->dx.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          if (S.Pf > 0) {
+            ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, rl,
+                                                               c->xs.p, c->dx.p + (size_t)S.Cf * 6);
+            G2OC_LAUNCH_CHECK();
+          }
+          axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, n);
+          G2OC_LAUNCH_CHECK();
+        }
+      }
+    } else {
+      const int nnzb = S.sys_nnzb;
+      G2OC_CUDA_TRY(cudaMemcpyAsync(sysval.p, hpp.p, (size_t)nnzb * S.pd * S.pd * sizeof(Real),
+                                    cudaMemcpyDeviceToDevice, st));
+      if (S.pd == 3) damp_diag<Real, 3><<<cdiv(S.Cf * 3, 128), 128, 0, st>>>(c->sys_diag.p, S.Cf, lambda, sysval.p);
+      else damp_diag<Real, 6><<<cdiv(S.Cf * 6, 128), 128, 0, st>>>(c->sys_diag.p, S.Cf, lambda, sysval.p);
+      G2OC_LAUNCH_CHECK();
+      if (use_chol) G2OC_TRY(chol_solve(sysval.p, c->b.p, c->x.p, &ok));
+      else G2OC_TRY(pcg_solve(sysval.p, c->b.p, c->x.p, false, &it));
+      it_total += it;
+    }
+    c->last_pcg_iterations = it_total;
+    if (pcg_iters) *pcg_iters = it_total;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&c->sc.p->solve_ok, &ok, sizeof(int), cudaMemcpyHostToDevice, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    return G2OC_OK;
+  }
+
+  const int* hpl_row() { return c->hpl_row.p; }
+
+  template <typename T>
+  static void to_double(const std::vector<T>& in, double* out) {
+    for (size_t i = 0; i < in.size(); ++i) out[i] = (double)in[i];
+  }
+
+  int get_hessian(double* hpp_out, double* hll_out, double* hpl_out) override {
+    const Structure& S = c->S;
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (hpp_out) {
+      std::vector<Real> h(hpp.n);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), hpp.p, hpp.bytes(), cudaMemcpyDeviceToHost));
+      to_double(h, hpp_out);
+    }
+    if (S.ba && hll_out && S.Pf > 0) {
+      std::vector<Real> h((size_t)S.Pf * 6);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), hll.p, h.size() * sizeof(Real), cudaMemcpyDeviceToHost));
+      for (int l = 0; l < S.Pf; ++l) {
+        const Real* a = h.data() + (size_t)l * 6;
+        double* o = hll_out + (size_t)l * 9;
+        o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
+        o[3] = a[1]; o[4] = a[3]; o[5] = a[4];
+        o[6] = a[2]; o[7] = a[4]; o[8] = a[5];
+      }
+    }
+    if (S.ba && hpl_out && !S.hpl_rc.empty()) {
+      std::vector<Real> h(S.hpl_rc.size() / 2 * 18);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), hpl.p, h.size() * sizeof(Real), cudaMemcpyDeviceToHost));
+      to_double(h, hpl_out);
+    }
+    return G2OC_OK;
+  }
+
+  int schur_export(double lambda, double* S_out, double* bs_out) override {
+    const Structure& S = c->S;
+    if (!S.ba || !S.schur) {
+      set_error("the graph has no Schur complement (no marginalized vertices)");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    G2OC_TRY(schur(lambda));
+    G2OC_TRY(schur_rhs_from(c->b.p, c->b.p + (size_t)S.Cf * 6, c->rhs.p));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (S_out) {
+      std::vector<Real> h(S.schur_rc.size() / 2 * 36);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), Sval.p, h.size() * sizeof(Real), cudaMemcpyDeviceToHost));
+      to_double(h, S_out);
+    }
+    if (bs_out) G2OC_CUDA_TRY(cudaMemcpy(bs_out, c->rhs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    return G2OC_OK;
+  }
+};
+
+// ------------------------------------------------------------ driver ops
+static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  if (S.ba) ba_chi2_kernel<<<kRedBlocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  else if (S.pose_type == G2OC_POSE_SE2)
+    pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
+  else pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
+  G2OC_LAUNCH_CHECK();
+  return finalize_sum(c, kRedBlocks, 2, out_plain, out_robust);
+}
+
+static int oplus(g2oc_ctx* c) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  if (S.ba) ba_oplus<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
+  else if (S.pose_type == G2OC_POSE_SE2)
+    pg_oplus<G2OC_POSE_SE2><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
+                                                             c->oplus_count.p, c->flag.p);
+  else pg_oplus<G2OC_POSE_SE3><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
+                                                                c->oplus_count.p, c->flag.p);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
+static int push(g2oc_ctx* c) {
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose_bak.p, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  if (c->point.n)
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point_bak.p, c->point.p, c->point.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  return G2OC_OK;
+}
+
+static int pop(g2oc_ctx* c) {
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, c->pose_bak.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  if (c->point.n)
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point.p, c->point_bak.p, c->point.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  return G2OC_OK;
+}
+
+struct PhaseTimer {
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit PhaseTimer(cudaStream_t s) : st(s) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  ~PhaseTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { cudaEventRecord(a, st); }
+  double stop() {
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+  }
+};
+
+// OptimizationAlgorithmLevenberg::solve (optimization_algorithm_levenberg.cpp:60-153)
+static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
+  cudaStream_t st = c->stream;
+  DevScalars* sc = c->sc.p;
+  PhaseTimer tm(st);
+  tm.start();
+  G2OC_TRY(chi2_to(c, &sc->chi2_plain, &sc->chi2_current));
+  stv->time_residuals = tm.stop();
+  tm.start();
+  G2OC_TRY(c->eng->build_system());
+  c->system_built = true;
+  stv->time_quadratic_form = tm.stop();
+  if (iteration == 0) {
+    G2OC_TRY(c->eng->max_diag());
+    lm_init_lambda<<<1, 32, 0, st>>>(sc, c->prm.initial_lambda, c->prm.tau);
+    G2OC_LAUNCH_CHECK();
+  }
+  const int n = c->vec_size();
+  double rho = 0;
+  int qmax = 0;
+  DevScalars h{};
+  do {
+    G2OC_TRY(push(c));
+    DevScalars cur;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&cur, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    tm.start();
+    int pcg_it = 0;
+    G2OC_TRY(c->eng->solve(cur.lambda, &pcg_it));
+    stv->time_linear_solver += tm.stop();
+    stv->iterations_linear_solver += pcg_it;
+    tm.start();
+    G2OC_TRY(oplus(c));
+    stv->time_update += tm.stop();
+    G2OC_TRY(chi2_to(c, nullptr, &sc->chi2_temp));
+    lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p);
+    G2OC_LAUNCH_CHECK();
+    G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &sc->scale, nullptr, 1e-3));
+    lm_decide<<<1, 32, 0, st>>>(sc);
+    G2OC_LAUNCH_CHECK();
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&h, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    rho = h.rho;
+    if (!h.accept) {
+      G2OC_TRY(pop(c));
+      if (!std::isfinite(h.lambda)) {
+        qmax++;
+        stv->levenberg_iterations = qmax;
+        break;
+      }
+    }
+    qmax++;
+    stv->levenberg_iterations = qmax;
+  } while (rho < 0 && qmax < c->prm.max_trials_after_failure);
+  stv->lambda = h.lambda;
+  if (qmax == c->prm.max_trials_after_failure || rho == 0 || !std::isfinite(h.lambda)) *result = G2OC_RESULT_TERMINATE;
+  else *result = G2OC_RESULT_OK;
+  return G2OC_OK;
+}
+
+// OptimizationAlgorithmGaussNewton::solve (optimization_algorithm_gauss_newton.cpp:48-93)
+static int gn_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
+  (void)iteration;
+  PhaseTimer tm(c->stream);
+  tm.start();
+  G2OC_TRY(chi2_to(c, &c->sc.p->chi2_plain, &c->sc.p->chi2_current));
+  stv->time_residuals = tm.stop();
+  tm.start();
+  G2OC_TRY(c->eng->build_system());
+  c->system_built = true;
+  stv->time_quadratic_form = tm.stop();
+  tm.start();
+  int it = 0;
+  G2OC_TRY(c->eng->solve(0.0, &it));
+  stv->time_linear_solver = tm.stop();
+  stv->iterations_linear_solver = it;
+  tm.start();
+  G2OC_TRY(oplus(c));
+  stv->time_update = tm.stop();
+  DevScalars h;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *result = h.solve_ok ? G2OC_RESULT_OK : G2OC_RESULT_FAIL;
+  return G2OC_OK;
+}
+
+static int reset_pcg(g2oc_ctx* c) {
+  PcgState p{};
+  p.residual_carry = -1.0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &p, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
+  return G2OC_OK;
+}
+
+static int check_ctx(g2oc_ctx* c, bool need_upload) {
+  if (!c) {
+    set_error("context is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (need_upload && !c->uploaded) {
+    set_error("no graph uploaded");
+    return G2OC_ERR_STATE;
+  }
+  G2OC_CUDA_TRY(cudaSetDevice(c->device));
+  return G2OC_OK;
+}
+
+// inverse measurement on the host, once per upload
+static void inverse_measurement(int et, const double* m, double* out) {
+  if (et == G2OC_EDGE_SE2) {
+    se2_inv(m, out);
+  } else {
+    iso_inv(m, out);
+  }
+}
+
+}  // namespace g2oc
+
+using namespace g2oc;
+
+extern "C" {
+
+int g2oc_abi_version(void) { return G2OC_ABI_VERSION; }
+
+const char* g2oc_last_error(void) { return g_err; }
+
+void g2oc_default_params(g2oc_params* p) {
+  if (!p) return;
+  p->algorithm = G2OC_ALGO_LEVENBERG;
+  p->linear_solver = G2OC_LINEAR_PCG;
+  p->precision = G2OC_PREC_FP64;
+  p->pcg_max_iterations = -1;
+  p->pcg_tolerance = 1e-6;
+  p->pcg_absolute_tolerance = 1;
+  p->max_trials_after_failure = 10;
+  p->initial_lambda = 0.0;
+  p->tau = 1e-5;
+  p->refine_max_iterations = 1;
+  p->refine_tolerance = 1e-10;
+}
+
+// names registered by this library, "<gn|lm>_cuda[_<variant>]"
+static const char* kSolvers[][2] = {
+    {"gn_cuda", "Gauss-Newton: B200 block solver, FP64, PCG with Schur / Cholesky without"},
+    {"lm_cuda", "Levenberg: B200 block solver, FP64, PCG with Schur / Cholesky without"},
+    {"gn_cuda_pcg", "Gauss-Newton: B200 block solver, FP64, block-Jacobi PCG"},
+    {"lm_cuda_pcg", "Levenberg: B200 block solver, FP64, block-Jacobi PCG"},
+    {"gn_cuda_pcg6_3", "Gauss-Newton: B200 BlockSolver<6,3>, FP64, block-Jacobi PCG"},
+    {"lm_cuda_pcg6_3", "Levenberg: B200 BlockSolver<6,3>, FP64, block-Jacobi PCG"},
+    {"gn_cuda_pcg3_3", "Gauss-Newton: B200 BlockSolver<3,3>, FP64, block-Jacobi PCG"},
+    {"lm_cuda_pcg3_3", "Levenberg: B200 BlockSolver<3,3>, FP64, block-Jacobi PCG"},
+    {"gn_cuda_chol", "Gauss-Newton: B200 block solver, FP64, dense Cholesky"},
+    {"lm_cuda_chol", "Levenberg: B200 block solver, FP64, dense Cholesky"},
+    {"gn_cuda_mixed", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
+    {"lm_cuda_mixed", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
+};
+
+int g2oc_list_solvers(char* buf, size_t size) {
+  std::string s;
+  for (auto& e : kSolvers) {
+    if (!s.empty()) s += ";";
+    s += e[0];
+  }
+  if (!buf || size < s.size() + 1) {
+    set_error("buffer too small: %zu bytes needed", s.size() + 1);
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  memcpy(buf, s.c_str(), s.size() + 1);
+  return G2OC_OK;
+}
+
+int g2oc_construct(const char* name, g2oc_params* p) {
+  if (!name || !p) {
+    set_error("name or params is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  bool found = false;
+  for (auto& e : kSolvers)
+    if (strcmp(e[0], name) == 0) found = true;
+  if (!found) {
+    set_error("SOLVER FACTORY: Unable to create solver %s", name);
+    return G2OC_ERR_UNKNOWN_SOLVER;
+  }
+  const std::string n(name);
+  g2oc_default_params(p);
+  p->algorithm = n.substr(0, 2) == "gn" ? G2OC_ALGO_GAUSS_NEWTON : G2OC_ALGO_LEVENBERG;
+  const std::string v = n.size() > 7 ? n.substr(8) : "";
+  if (v.empty()) p->linear_solver = 2;  // PCG with Schur, Cholesky without
+  else if (v.rfind("chol", 0) == 0) p->linear_solver = G2OC_LINEAR_CHOLESKY;
+  else if (v == "mixed") {
+    p->linear_solver = G2OC_LINEAR_PCG;
+    p->precision = G2OC_PREC_MIXED;
+  } else p->linear_solver = G2OC_LINEAR_PCG;
+  return G2OC_OK;
+}
+
+int g2oc_create(int device, g2oc_ctx** out) {
+  if (!out) {
+    set_error("out is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return G2OC_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) {
+    set_error("device %d out of range (%d devices)", device, n);
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  cudaDeviceProp prop;
+  G2OC_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) {
+    set_error("device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+    return G2OC_ERR_NO_DEVICE;
+  }
+  G2OC_CUDA_TRY(cudaSetDevice(device));
+  std::unique_ptr<g2oc_ctx> c(new g2oc_ctx());
+  c->device = device;
+  G2OC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  g2oc_default_params(&c->prm);
+  G2OC_TRY(c->sc.alloc(1));
+  G2OC_TRY(c->pcg.alloc(1));
+  G2OC_TRY(c->flag.alloc(1));
+  G2OC_TRY(c->partials.alloc(2 * 8192));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->sc.p, 0, sizeof(DevScalars), c->stream));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->flag.p, 0, sizeof(int), c->stream));
+  G2OC_TRY(reset_pcg(c.get()));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *out = c.release();
+  return G2OC_OK;
+}
+
+void g2oc_destroy(g2oc_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+static int make_engine(g2oc_ctx* c) {
+  if (c->prm.precision == G2OC_PREC_MIXED) c->eng.reset(new Engine<float>(c));
+  else c->eng.reset(new Engine<double>(c));
+  G2OC_TRY(c->eng->alloc());
+  c->system_built = false;
+  return G2OC_OK;
+}
+
+int g2oc_set_params(g2oc_ctx* c, const g2oc_params* p) {
+  G2OC_TRY(check_ctx(c, false));
+  if (!p) {
+    set_error("params is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (p->algorithm < 0 || p->algorithm > 1 || p->linear_solver < 0 || p->linear_solver > 2 || p->precision < 0 ||
+      p->precision > 1 || p->max_trials_after_failure < 1 || p->pcg_tolerance < 0) {
+    set_error("invalid parameter value");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const bool prec_changed = p->precision != c->prm.precision;
+  c->prm = *p;
+  if (c->uploaded && prec_changed) G2OC_TRY(make_engine(c));
+  return G2OC_OK;
+}
+
+int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
+  G2OC_TRY(check_ctx(c, false));
+  c->uploaded = false;
+  c->eng.reset();
+  c->chol.reset();
+  Structure& S = c->S;
+  S = Structure();
+  G2OC_TRY(build_structure(g, S));
+  cudaStream_t st = c->stream;
+  const int na = (int)S.act.size();
+  c->f = g->focal_length;
+  c->cx = g->principal_point[0];
+  c->cy = g->principal_point[1];
+  // vertices
+  if (S.ba) {
+    std::vector<double> cam((size_t)S.C * 8, 0.0), pt((size_t)S.P * 4, 0.0);
+    for (int i = 0; i < S.C; ++i) {
+      const double* v = g->pose_estimate + (size_t)i * 7;
+      double* o = cam.data() + (size_t)i * 8;
+      o[0] = v[3]; o[1] = v[4]; o[2] = v[5]; o[3] = v[6];
+      o[4] = v[0]; o[5] = v[1]; o[6] = v[2];
+    }
+    for (int i = 0; i < S.P; ++i)
+      for (int k = 0; k < 3; ++k) pt[(size_t)i * 4 + k] = g->point_estimate[(size_t)i * 3 + k];
+    G2OC_TRY(c->pose.upload(cam, st));
+    G2OC_TRY(c->point.upload(pt, st));
+    G2OC_TRY(c->point_bak.alloc(pt.size()));
+  } else {
+    std::vector<double> est(g->pose_estimate, g->pose_estimate + (size_t)S.C * S.ped);
+    G2OC_TRY(c->pose.upload(est, st));
+    c->point.release();
+    c->point_bak.release();
+  }
+  G2OC_TRY(c->pose_bak.alloc(c->pose.n));
+  G2OC_TRY(c->oplus_count.alloc(S.C));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, S.C * sizeof(int), st));
+  G2OC_TRY(c->free_pose.upload(S.free_pose_of_h, st));
+  G2OC_TRY(c->free_point.upload(S.free_point_of_l, st));
+  if (S.ba) {
+    std::vector<int2> ev(na), cv(S.c_edge.size());
+    std::vector<double2> ez(na), cz(S.c_edge.size());
+    std::vector<double4> eo(na), co(S.c_edge.size());
+    for (int k = 0; k < na; ++k) {
+      const int e = S.dev_edge[k];
+      ev[k] = make_int2(g->edge_vertex[2 * e], g->edge_vertex[2 * e + 1]);
+      ez[k] = make_double2(g->measurement[2 * e], g->measurement[2 * e + 1]);
+      const double* I = g->information + (size_t)e * 4;
+      eo[k] = make_double4(I[0], I[1], I[3], g->robust_delta ? g->robust_delta[e] : 0.0);
+    }
+    for (size_t j = 0; j < S.c_edge.size(); ++j) {
+      cv[j] = ev[S.c_edge[j]];
+      cz[j] = ez[S.c_edge[j]];
+      co[j] = eo[S.c_edge[j]];
+    }
+    G2OC_TRY(c->e_v.upload(ev, st));
+    G2OC_TRY(c->e_z.upload(ez, st));
+    G2OC_TRY(c->e_om.upload(eo, st));
+    G2OC_TRY(c->e_hpl.upload(S.e_hpl, st));
+    G2OC_TRY(c->l_ptr.upload(S.l_ptr, st));
+    G2OC_TRY(c->c_ptr.upload(S.c_ptr, st));
+    G2OC_TRY(c->c_v.upload(cv, st));
+    G2OC_TRY(c->c_z.upload(cz, st));
+    G2OC_TRY(c->c_om.upload(co, st));
+    G2OC_TRY(c->hb_ptr.upload(S.hb_ptr, st));
+    const size_t nh = S.hpl_rc.size() / 2;
+    std::vector<int> hr(nh), hcl(nh);
+    for (size_t b = 0; b < nh; ++b) {
+      hr[b] = S.hpl_rc[2 * b];
+      hcl[b] = S.hpl_rc[2 * b + 1];
+    }
+    G2OC_TRY(c->hpl_row.upload(hr, st));
+    G2OC_TRY(c->hpl_col.upload(hcl, st));
+    G2OC_TRY(c->hc_ptr.upload(S.hc_ptr, st));
+    G2OC_TRY(c->hc_blk.upload(S.hc_blk, st));
+    G2OC_TRY(c->sp_ptr.upload(S.sp_ptr, st));
+    std::vector<int2> ab(S.sp_ab.size() / 2);
+    for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.sp_ab[2 * i], S.sp_ab[2 * i + 1]);
+    G2OC_TRY(c->sp_ab.upload(ab, st));
+    G2OC_TRY(c->s_hpp.upload(S.s_hpp, st));
+  } else {
+    const int D = S.D, ZD = S.md;
+    std::vector<int2> ev(na);
+    std::vector<double> zi((size_t)na * ZD), info((size_t)na * D * D), dl(na);
+    for (int k = 0; k < na; ++k) {
+      const int e = S.act[k];
+      ev[k] = make_int2(g->edge_vertex[2 * e], g->edge_vertex[2 * e + 1]);
+      inverse_measurement(S.edge_type, g->measurement + (size_t)e * ZD, zi.data() + (size_t)k * ZD);
+      memcpy(info.data() + (size_t)k * D * D, g->information + (size_t)e * D * D, D * D * sizeof(double));
+      dl[k] = g->robust_delta ? g->robust_delta[e] : 0.0;
+    }
+    G2OC_TRY(c->pe_v.upload(ev, st));
+    G2OC_TRY(c->pe_zinv.upload(zi, st));
+    G2OC_TRY(c->pe_info.upload(info, st));
+    G2OC_TRY(c->pe_delta.upload(dl, st));
+    G2OC_TRY(c->pe_trans.upload(S.pe_trans, st));
+    G2OC_TRY(c->hb_src_ptr.upload(S.hb_src_ptr, st));
+    G2OC_TRY(c->hb_src.upload(S.hb_src, st));
+    G2OC_TRY(c->bv_src_ptr.upload(S.bv_src_ptr, st));
+    G2OC_TRY(c->bv_src.upload(S.bv_src, st));
+  }
+  G2OC_TRY(c->sys_col_ptr.upload(S.sys_col_ptr, st));
+  G2OC_TRY(c->sys_row.upload(S.sys_row, st));
+  G2OC_TRY(c->sys_diag.upload(S.sys_diag, st));
+  G2OC_TRY(c->sys_rowu_ptr.upload(S.sys_rowu_ptr, st));
+  G2OC_TRY(c->sys_rowu_blk.upload(S.sys_rowu_blk, st));
+  G2OC_TRY(c->sys_rowu_col.upload(S.sys_rowu_col, st));
+  const int n = c->vec_size();
+  G2OC_TRY(c->b.alloc(n));
+  G2OC_TRY(c->x.alloc(n));
+  G2OC_TRY(c->dx.alloc(n));
+  G2OC_TRY(c->resid.alloc(n));
+  G2OC_TRY(c->xs.alloc((size_t)S.Cf * S.pd));
+  G2OC_TRY(c->rhs.alloc((size_t)S.Cf * S.pd));
+  G2OC_TRY(c->errbuf.alloc((size_t)na * 36));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, n * sizeof(double), st));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->b.p, 0, n * sizeof(double), st));
+  G2OC_TRY(reset_pcg(c));
+  G2OC_TRY(make_engine(c));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  c->uploaded = true;
+  return G2OC_OK;
+}
+
+int g2oc_get_hessian_info(g2oc_ctx* c, g2oc_hessian_info* info) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!info) return G2OC_ERR_INVALID_ARGUMENT;
+  const Structure& S = c->S;
+  info->num_free_poses = S.Cf;
+  info->num_free_points = S.Pf;
+  info->pose_dim = S.pd;
+  info->point_dim = S.ba ? 3 : 0;
+  info->hpp_nnzb = (int)(S.hpp_rc.size() / 2);
+  info->hpl_nnzb = (int)(S.hpl_rc.size() / 2);
+  info->schur_nnzb = (int)(S.schur_rc.size() / 2);
+  info->num_active_edges = (int)S.act.size();
+  info->vector_size = c->vec_size();
+  return G2OC_OK;
+}
+
+int g2oc_set_estimates(g2oc_ctx* c, const double* pose, const double* point) {
+  G2OC_TRY(check_ctx(c, true));
+  const Structure& S = c->S;
+  if (pose) {
+    if (S.ba) {
+      std::vector<double> cam((size_t)S.C * 8, 0.0);
+      for (int i = 0; i < S.C; ++i) {
+        const double* v = pose + (size_t)i * 7;
+        double* o = cam.data() + (size_t)i * 8;
+        o[0] = v[3]; o[1] = v[4]; o[2] = v[5]; o[3] = v[6];
+        o[4] = v[0]; o[5] = v[1]; o[6] = v[2];
+      }
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, cam.data(), c->pose.bytes(), cudaMemcpyHostToDevice, c->stream));
+      G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    } else {
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, pose, c->pose.bytes(), cudaMemcpyHostToDevice, c->stream));
+    }
+  }
+  if (point && S.ba && S.P > 0) {
+    std::vector<double> pt((size_t)S.P * 4, 0.0);
+    for (int i = 0; i < S.P; ++i)
+      for (int k = 0; k < 3; ++k) pt[(size_t)i * 4 + k] = point[(size_t)i * 3 + k];
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point.p, pt.data(), c->point.bytes(), cudaMemcpyHostToDevice, c->stream));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->system_built = false;
+  return G2OC_OK;
+}
+
+int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
+  G2OC_TRY(check_ctx(c, true));
+  const Structure& S = c->S;
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (pose) {
+    if (S.ba) {
+      std::vector<double> cam((size_t)S.C * 8);
+      G2OC_CUDA_TRY(cudaMemcpy(cam.data(), c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < S.C; ++i) {
+        const double* o = cam.data() + (size_t)i * 8;
+        double* v = pose + (size_t)i * 7;
+        v[0] = o[4]; v[1] = o[5]; v[2] = o[6];
+        v[3] = o[0]; v[4] = o[1]; v[5] = o[2]; v[6] = o[3];
+      }
+    } else {
+      G2OC_CUDA_TRY(cudaMemcpy(pose, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost));
+    }
+  }
+  if (point && S.ba && S.P > 0) {
+    std::vector<double> pt((size_t)S.P * 4);
+    G2OC_CUDA_TRY(cudaMemcpy(pt.data(), c->point.p, c->point.bytes(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < S.P; ++i)
+      for (int k = 0; k < 3; ++k) point[(size_t)i * 3 + k] = pt[(size_t)i * 4 + k];
+  }
+  return G2OC_OK;
+}
+
+int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int* done) {
+  G2OC_TRY(check_ctx(c, true));
+  if (iterations < 0) {
+    set_error("iterations < 0");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  G2OC_TRY(reset_pcg(c));  // LinearSolverPCG::init via BlockSolver::init
+  int result = G2OC_RESULT_OK;
+  int it = 0;
+  for (int i = 0; i < iterations && result == G2OC_RESULT_OK; ++i) {
+    g2oc_iteration_stats stv;
+    memset(&stv, 0, sizeof(stv));
+    PhaseTimer tm(c->stream);
+    tm.start();
+    if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, i, &stv, &result));
+    else G2OC_TRY(gn_iteration(c, i, &stv, &result));
+    stv.iteration = i;
+    stv.result = result;
+    if (stats) {
+      G2OC_TRY(chi2_to(c, nullptr, &c->sc.p->chi2_plain));
+      DevScalars h;
+      G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+      G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+      stv.chi2 = h.chi2_plain;
+      if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) stv.lambda = h.lambda;
+    }
+    stv.time_iteration = tm.stop();
+    if (stats) stats[i] = stv;
+    ++it;
+  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (done) *done = (result == G2OC_RESULT_FAIL) ? 0 : it;
+  return G2OC_OK;
+}
+
+int g2oc_chi2(g2oc_ctx* c, double* chi2, double* robust) {
+  G2OC_TRY(check_ctx(c, true));
+  G2OC_TRY(chi2_to(c, &c->sc.p->chi2_plain, &c->sc.p->chi2_temp));
+  DevScalars h;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (chi2) *chi2 = h.chi2_plain;
+  if (robust) *robust = h.chi2_temp;
+  return G2OC_OK;
+}
+
+int g2oc_errors(g2oc_ctx* c, double* out) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!out) return G2OC_ERR_INVALID_ARGUMENT;
+  const Structure& S = c->S;
+  const int na = (int)S.act.size();
+  if (S.ba) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
+  else if (S.pose_type == G2OC_POSE_SE2)
+    pg_errors_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
+  else pg_errors_kernel<G2OC_POSE_SE3><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
+  G2OC_LAUNCH_CHECK();
+  std::vector<double> h((size_t)na * S.D);
+  G2OC_CUDA_TRY(cudaMemcpyAsync(h.data(), c->errbuf.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int a = 0; a < na; ++a)
+    memcpy(out + (size_t)a * S.D, h.data() + (size_t)S.dev_of_act[a] * S.D, S.D * sizeof(double));
+  return G2OC_OK;
+}
+
+int g2oc_jacobians(g2oc_ctx* c, double* j0, double* j1) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!j0 || !j1) return G2OC_ERR_INVALID_ARGUMENT;
+  const Structure& S = c->S;
+  const int na = (int)S.act.size();
+  const int d0 = S.ba ? 3 : S.pd, d1 = S.pd, D = S.D;
+  DBuf<double> a, b;
+  G2OC_TRY(a.alloc((size_t)na * D * d0));
+  G2OC_TRY(b.alloc((size_t)na * D * d1));
+  if (S.ba) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
+  else if (S.pose_type == G2OC_POSE_SE2)
+    pg_jacobians_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
+  else pg_jacobians_kernel<G2OC_POSE_SE3><<<cdiv(na, 64), 64, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
+  G2OC_LAUNCH_CHECK();
+  std::vector<double> ha(a.n), hb(b.n);
+  G2OC_CUDA_TRY(cudaMemcpyAsync(ha.data(), a.p, a.bytes(), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(hb.data(), b.p, b.bytes(), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < na; ++k) {
+    const size_t dev = S.dev_of_act[k];
+    memcpy(j0 + (size_t)k * D * d0, ha.data() + dev * D * d0, D * d0 * sizeof(double));
+    memcpy(j1 + (size_t)k * D * d1, hb.data() + dev * D * d1, D * d1 * sizeof(double));
+  }
+  return G2OC_OK;
+}
+
+int g2oc_build_system(g2oc_ctx* c) {
+  G2OC_TRY(check_ctx(c, true));
+  G2OC_TRY(c->eng->build_system());
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->system_built = true;
+  return G2OC_OK;
+}
+
+int g2oc_get_pattern(g2oc_ctx* c, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* schur_rc) {
+  G2OC_TRY(check_ctx(c, true));
+  const Structure& S = c->S;
+  if (hpp_rc) memcpy(hpp_rc, S.hpp_rc.data(), S.hpp_rc.size() * sizeof(int32_t));
+  if (hpl_rc) memcpy(hpl_rc, S.hpl_rc.data(), S.hpl_rc.size() * sizeof(int32_t));
+  if (schur_rc) memcpy(schur_rc, S.schur_rc.data(), S.schur_rc.size() * sizeof(int32_t));
+  return G2OC_OK;
+}
+
+int g2oc_get_hessian(g2oc_ctx* c, double* hpp, double* hll, double* hpl, double* b) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->system_built) {
+    set_error("call g2oc_build_system first");
+    return G2OC_ERR_STATE;
+  }
+  G2OC_TRY(c->eng->get_hessian(hpp, hll, hpl));
+  if (b) G2OC_CUDA_TRY(cudaMemcpy(b, c->b.p, c->b.bytes(), cudaMemcpyDeviceToHost));
+  return G2OC_OK;
+}
+
+int g2oc_schur(g2oc_ctx* c, double lambda, double* S_out, double* bs) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->system_built) {
+    set_error("call g2oc_build_system first");
+    return G2OC_ERR_STATE;
+  }
+  return c->eng->schur_export(lambda, S_out, bs);
+}
+
+int g2oc_solve(g2oc_ctx* c, double lambda, double* x, int32_t* iters) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->system_built) {
+    set_error("call g2oc_build_system first");
+    return G2OC_ERR_STATE;
+  }
+  int it = 0;
+  G2OC_TRY(c->eng->solve(lambda, &it));
+  DevScalars h;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (iters) *iters = it;
+  if (x) G2OC_CUDA_TRY(cudaMemcpy(x, c->x.p, c->x.bytes(), cudaMemcpyDeviceToHost));
+  return h.solve_ok ? G2OC_OK : G2OC_ERR_NOT_PD;
+}
+
+int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, const int32_t* offs, int32_t nnzb,
+                            const int32_t* rc, const double* values, const double* b, double* x, int32_t* iters) {
+  G2OC_TRY(check_ctx(c, false));
+  if (nb <= 0 || !offs || nnzb <= 0 || !rc || !values || !b || !x) {
+    set_error("invalid block system arguments");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const int bs = offs[1] - offs[0];
+  for (int i = 0; i < nb; ++i)
+    if (offs[i + 1] - offs[i] != bs) {
+      set_error("only uniform block sizes are supported");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+  if (bs != 3 && bs != 6) {
+    set_error("block size %d not supported (3 or 6)", bs);
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  std::vector<int32_t> rcv(rc, rc + 2 * (size_t)nnzb);
+  for (int k = 0; k < nnzb; ++k) {
+    const int r = rc[2 * k], cc = rc[2 * k + 1];
+    if (r < 0 || cc < 0 || r >= nb || cc >= nb || r > cc ||
+        (k > 0 && (rc[2 * k - 1] > cc || (rc[2 * k - 1] == cc && rc[2 * k - 2] >= r)))) {
+      set_error("blocks must be upper-triangular and listed column-major");
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+  }
+  // a temporary context-local system: reuse the structure lists of a scratch Structure
+  Structure tmp;
+  build_sym_lists(nb, rcv, tmp);
+  for (int i = 0; i < nb; ++i)
+    if (tmp.sys_diag[i] < 0) {
+      set_error("diagonal block %d missing", i);
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+  cudaStream_t st = c->stream;
+  DBuf<int> cp, rw, dg, rup, rub, ruc;
+  DBuf<double> val, rhs, xo, mi, r, s, d0, d1, q;
+  G2OC_TRY(cp.upload(tmp.sys_col_ptr, st));
+  G2OC_TRY(rw.upload(tmp.sys_row, st));
+  G2OC_TRY(dg.upload(tmp.sys_diag, st));
+  G2OC_TRY(rup.upload(tmp.sys_rowu_ptr, st));
+  G2OC_TRY(rub.upload(tmp.sys_rowu_blk, st));
+  G2OC_TRY(ruc.upload(tmp.sys_rowu_col, st));
+  G2OC_TRY(val.upload(std::vector<double>(values, values + (size_t)nnzb * bs * bs), st));
+  const int n = nb * bs;
+  G2OC_TRY(rhs.upload(std::vector<double>(b, b + n), st));
+  G2OC_TRY(xo.alloc(n));
+  SysDev<double> A{nb, cp.p, rw.p, dg.p, rup.p, rub.p, ruc.p, val.p};
+  int it = 0, ok = 1;
+  if (linear_solver == G2OC_LINEAR_CHOLESKY) {
+    CholPlan P;
+    std::vector<int> col(nnzb);
+    for (int k = 0; k < nnzb; ++k) col[k] = rc[2 * k + 1];
+    G2OC_TRY(chol_plan_build(P, nb, bs, rcv, true, col, st));
+    G2OC_TRY(chol_solve<double>(P, st, A, nnzb, rhs.p, xo.p, &ok));
+  } else {
+    G2OC_TRY(mi.alloc((size_t)nb * bs * bs));
+    G2OC_TRY(r.alloc(n));
+    G2OC_TRY(s.alloc(n));
+    G2OC_TRY(d0.alloc(n));
+    G2OC_TRY(d1.alloc(n));
+    G2OC_TRY(q.alloc(n));
+    G2OC_TRY(reset_pcg(c));
+    if (bs == 3) {
+      pcg_diag_inv<double, 3><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
+      G2OC_TRY((run_pcg<double, 3>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, false, &it)));
+    } else {
+      pcg_diag_inv<double, 6><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
+      G2OC_TRY((run_pcg<double, 6>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, false, &it)));
+    }
+  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  G2OC_CUDA_TRY(cudaMemcpy(x, xo.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (iters) *iters = it;
+  return ok ? G2OC_OK : G2OC_ERR_NOT_PD;
+}
+
+}  // extern "C"

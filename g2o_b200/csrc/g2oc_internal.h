@@ -1,0 +1,147 @@
+// g2oc_internal.h -- shared declarations of the backend: host-side structure
+// (index mapping and block patterns, computed once per upload), device
+// buffers, and the context behind the C-ABI handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/g2o_cuda.h"
+
+namespace g2oc {
+
+void set_error(const char* fmt, ...);
+
+#define G2OC_CUDA_TRY(expr)                                                         \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess) {                                                        \
+      ::g2oc::set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(_e)); \
+      return G2OC_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+#define G2OC_TRY(expr)            \
+  do {                            \
+    int _s = (expr);              \
+    if (_s != G2OC_OK) return _s; \
+  } while (0)
+
+// Device allocation owned by the context (cudaMalloc at upload, cudaFree at
+// re-upload or destroy).
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    if (count == n && p) return G2OC_OK;
+    release();
+    if (count == 0) return G2OC_OK;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+      p = nullptr;
+      return G2OC_ERR_CUDA;
+    }
+    n = count;
+    return G2OC_OK;
+  }
+  int upload(const std::vector<T>& v, cudaStream_t s) {
+    G2OC_TRY(alloc(v.size()));
+    if (!v.empty()) G2OC_CUDA_TRY(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return G2OC_OK;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------ structure
+// Everything BlockSolver::buildStructure and SparseOptimizer::buildIndexMapping
+// decide, laid out for the device (g2o/core/block_solver.hpp:110-269,
+// g2o/core/sparse_optimizer.cpp:175-287).
+struct Structure {
+  int pose_type = 0, edge_type = 0;
+  int C = 0, P = 0, E = 0;
+  int pd = 0, ped = 0, D = 0, md = 0;
+  bool ba = false, schur = false;
+  std::vector<int> act;                 // active edge ids, insertion order
+  std::vector<int> pose_h, point_l;     // Hessian index of each pose / landmark index of each point, -1 = none
+  std::vector<int> free_pose_of_h;      // pose index of Hessian row h
+  std::vector<int> free_point_of_l;     // point index of landmark l
+  int Cf = 0, Pf = 0;
+  // patterns, (row, col) in column-major order
+  std::vector<int32_t> hpp_rc, hpl_rc, schur_rc;
+  std::vector<int> hpp_diag;            // Hpp block index of the diagonal of row h
+
+  // ---- BA (EdgeProjectXYZ2UV): device edge order = point-major
+  // (free landmarks by landmark index, then edges of fixed points), cameras
+  // ascending within a point.
+  std::vector<int> dev_edge;            // device position -> edge id
+  std::vector<int> dev_of_act;          // active position -> device position
+  std::vector<int> l_ptr;               // Pf + 1, device edge range of landmark l
+  std::vector<int> e_hpl;               // per device edge, Hpl block or -1
+  std::vector<int> hb_ptr;              // Pf + 1, Hpl block range of landmark l
+  std::vector<int> c_ptr;               // Cf + 1, camera-major range of free camera h
+  std::vector<int> c_edge;              // camera-major -> device edge
+  std::vector<int> hc_ptr, hc_blk;      // Cf + 1 / hpl_nnzb: Hpl blocks by camera row
+  std::vector<int> s_hpp;               // per Schur block: Hpp block or -1
+  std::vector<int> sp_ptr;              // nnzS + 1: pair range per Schur block
+  std::vector<int32_t> sp_ab;           // 2 per pair: (Hpl block a, Hpl block b), row(a) <= row(b)
+  int64_t num_pairs = 0;
+
+  // ---- pose graphs (EdgeSE2 / EdgeSE3): device edge order = active order
+  std::vector<int> pe_blk;              // 3 per active edge: Hpp block of (v0,v0), (v1,v1), (v0,v1) or -1
+  std::vector<uint8_t> pe_trans;        // (v0,v1) stored transposed (hessian index of v0 > v1)
+  std::vector<int> hb_src_ptr, hb_src;  // per Hpp block: contributions, encoded edge*3 + slot
+  std::vector<int> bv_src_ptr, bv_src;  // per free pose: contributions, encoded edge*2 + which
+
+  // ---- the linear system matrix (S for BA, Hpp for pose graphs) as a block
+  // symmetric matrix in column-major upper storage
+  int sys_nb = 0, sys_nnzb = 0;
+  std::vector<int> sys_col_ptr;         // nb + 1, column-major ranges (diagonal last)
+  std::vector<int> sys_row;             // per block
+  std::vector<int> sys_diag;            // per row: block index of the diagonal
+  std::vector<int> sys_rowu_ptr, sys_rowu_blk, sys_rowu_col;  // strictly-upper blocks listed by row
+};
+
+int build_structure(const g2oc_graph* g, Structure& s);
+// block-symmetric matrix lists (column/row listings) from a column-major pattern
+void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s);
+
+// ------------------------------------------------------------ device scalars
+// LM / PCG control state kept on the device so the trial loop needs one small
+// read-back per trial.
+struct DevScalars {
+  double chi2_current;   // currentChi of the LM iteration
+  double chi2_temp;      // tempChi after the trial update
+  double chi2_plain;     // activeChi2
+  double lambda;
+  double ni;
+  double scale;          // computeScale() + 1e-3
+  double rho;
+  double max_diag;
+  double pcg_residual;   // LinearSolverPCG::_residual carried between solves
+  double pcg_d0;
+  double pcg_dn;
+  double refine_rnorm;   // mixed precision: |r| / |b| of the last refinement
+  int pcg_iterations;
+  int pcg_done;
+  int solve_ok;
+  int accept;            // last trial accepted
+  int nonfinite;         // a non-finite value was met
+  int pad[3];
+};
+
+}  // namespace g2oc

@@ -1,0 +1,79 @@
+// lm_kernels.cuh -- Levenberg-Marquardt control on the device
+// (OptimizationAlgorithmLevenberg::solve / computeLambdaInit / computeScale,
+// g2o/core/optimization_algorithm_levenberg.cpp:60-176) and small vector
+// kernels shared by the paths.
+#pragma once
+
+#include "g2oc_internal.h"
+#include "reduce.cuh"
+
+namespace g2oc {
+
+// lambda_0 = initialLambda if set, else tau * max diag(H); ni = 2
+__global__ void lm_init_lambda(DevScalars* sc, double user_lambda, double tau) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    sc->lambda = user_lambda > 0.0 ? user_lambda : tau * sc->max_diag;
+    sc->ni = 2.0;
+  }
+}
+
+// One trial's decision. rho = (chi_current - chi_temp) / (scale + 1e-3);
+// accept: lambda *= max(1/3, min(2/3, 1 - (2 rho - 1)^3)), ni = 2;
+// reject: lambda *= ni, ni *= 2 (estimates restored by the host).
+__global__ void lm_decide(DevScalars* sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const bool ok2 = sc->solve_ok != 0;
+  double tempChi = sc->chi2_temp;
+  if (!ok2) tempChi = 1.79769313486231570815e+308;
+  double rho = sc->chi2_current - tempChi;
+  const double scale = ok2 ? sc->scale : 1.0;  // sc->scale already holds computeScale() + 1e-3
+  rho /= scale;
+  if (rho > 0 && isfinite(tempChi) && ok2) {
+    double alpha = 1. - pow((2 * rho - 1), 3);
+    alpha = fmin(alpha, 2. / 3.);
+    const double scaleFactor = fmax(1. / 3., alpha);
+    sc->lambda *= scaleFactor;
+    sc->ni = 2;
+    sc->chi2_current = tempChi;
+    sc->accept = 1;
+  } else {
+    sc->lambda *= sc->ni;
+    sc->ni *= 2;
+    sc->accept = 0;
+  }
+  sc->rho = rho;
+}
+
+// partial sums of x (lambda x + b) (computeScale)
+__global__ void lm_scale_partials(const double* x, const double* b, int n, const DevScalars* sc, double* partials) {
+  const double lambda = sc->lambda;
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += x[i] * (lambda * x[i] + b[i]);
+  s = block_sum1(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// sum of squares partials (refinement residual norms)
+__global__ void sumsq_partials(const double* a, int n, double* partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * a[i];
+  s = block_sum1(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void axpy_kernel(double* y, const double* x, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+template <typename Real, int BS>
+__global__ void damp_diag(const int* diag, int nb, double lambda, Real* dst) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb * BS) return;
+  const int i = t / BS, d = t % BS;
+  Real* v = dst + (size_t)diag[i] * BS * BS + d * (BS + 1);
+  *v = (Real)((double)*v + lambda);
+}
+
+}  // namespace g2oc

@@ -1,0 +1,294 @@
+"""Seeded synthetic graphs for the benchmark configurations.
+
+No dataset is shipped with g2o for this path; these generators follow the
+form of the reference's own example generators (g2o/examples/ba/ba_demo.cpp:
+cameras on a trajectory looking at a point cloud, Gaussian pixel noise,
+outliers handled by a Huber kernel; g2o/examples/sphere/create_sphere.cpp:
+rings of SE3 poses with odometry and ring-to-ring edges, noise on the
+translation and on the quaternion vector part) with the sizes of the
+benchmark configurations:
+
+* ``pose_graph_2d``  3,500 VertexSE2, Manhattan random walk, EdgeSE2 odometry
+  and ~2,000 loop closures, GN + Cholesky.
+* ``pose_graph_3d``  2,500 VertexSE3 on 10 rings x 250 on a 50 m sphere, EdgeSE3.
+* ``bundle_adjustment``  1,000 VertexSE3Expmap on a 30 m ring, 200,000
+  VertexPointXYZ in a 20x20x5 m box, ~1.0M EdgeProjectXYZ2UV, Huber.
+
+Every generator takes a seed; the benchmark configurations use
+20261203 + configuration index.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3, POSE_SE2, POSE_SE3,
+                  POSE_SE3EXPMAP, Graph)
+
+SEED_BASE = 20261203
+
+
+# ------------------------------------------------------------------ helpers
+def _wrap(a):
+    return (a + np.pi) % (2 * np.pi) - np.pi
+
+
+def _rot_to_quat(R):
+    """Rotation matrices (..., 3, 3) -> quaternions (..., 4) xyzw with w >= 0."""
+    R = np.asarray(R, dtype=np.float64)
+    q = np.empty(R.shape[:-2] + (4,))
+    tr = R[..., 0, 0] + R[..., 1, 1] + R[..., 2, 2]
+    w = 0.5 * np.sqrt(np.maximum(1.0 + tr, 0.0))
+    x = 0.5 * np.sqrt(np.maximum(1.0 + R[..., 0, 0] - R[..., 1, 1] - R[..., 2, 2], 0.0))
+    y = 0.5 * np.sqrt(np.maximum(1.0 - R[..., 0, 0] + R[..., 1, 1] - R[..., 2, 2], 0.0))
+    z = 0.5 * np.sqrt(np.maximum(1.0 - R[..., 0, 0] - R[..., 1, 1] + R[..., 2, 2], 0.0))
+    x = np.copysign(x, R[..., 2, 1] - R[..., 1, 2])
+    y = np.copysign(y, R[..., 0, 2] - R[..., 2, 0])
+    z = np.copysign(z, R[..., 1, 0] - R[..., 0, 1])
+    q[..., 0], q[..., 1], q[..., 2], q[..., 3] = x, y, z, w
+    q /= np.linalg.norm(q, axis=-1, keepdims=True)
+    return q
+
+
+def _quat_to_rot(q):
+    x, y, z, w = q[..., 0], q[..., 1], q[..., 2], q[..., 3]
+    R = np.empty(q.shape[:-1] + (3, 3))
+    R[..., 0, 0] = 1 - 2 * (y * y + z * z)
+    R[..., 0, 1] = 2 * (x * y - z * w)
+    R[..., 0, 2] = 2 * (x * z + y * w)
+    R[..., 1, 0] = 2 * (x * y + z * w)
+    R[..., 1, 1] = 1 - 2 * (x * x + z * z)
+    R[..., 1, 2] = 2 * (y * z - x * w)
+    R[..., 2, 0] = 2 * (x * z - y * w)
+    R[..., 2, 1] = 2 * (y * z + x * w)
+    R[..., 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def _axis_angle(v):
+    """Rodrigues: rotation vectors (..., 3) -> matrices."""
+    v = np.asarray(v, dtype=np.float64)
+    th = np.linalg.norm(v, axis=-1)[..., None, None]
+    K = np.zeros(v.shape[:-1] + (3, 3))
+    K[..., 0, 1], K[..., 0, 2] = -v[..., 2], v[..., 1]
+    K[..., 1, 0], K[..., 1, 2] = v[..., 2], -v[..., 0]
+    K[..., 2, 0], K[..., 2, 1] = -v[..., 1], v[..., 0]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        a = np.where(th > 1e-12, np.sin(th) / th, 1.0)
+        b = np.where(th > 1e-12, (1 - np.cos(th)) / (th * th), 0.5)
+    return np.eye(3) + a * K + b * (K @ K)
+
+
+def _compact_quat_noise(rng, n, sigma):
+    """Rotation matrices from a quaternion whose vector part is N(0, sigma)."""
+    qv = rng.normal(0.0, sigma, size=(n, 3))
+    w = np.sqrt(np.maximum(1.0 - np.sum(qv * qv, axis=1), 0.0))
+    return _quat_to_rot(np.concatenate([qv, w[:, None]], axis=1))
+
+
+def _iso12(R, t):
+    return np.concatenate([R.reshape(-1, 9), t.reshape(-1, 3)], axis=1)
+
+
+# ---------------------------------------------------------- 2D pose graph
+def pose_graph_2d(num_poses=3500, num_closures=2000, seed=SEED_BASE + 0):
+    rng = np.random.default_rng(seed)
+    # Manhattan random walk: 1 m steps, turn +-90 deg with p = 0.3
+    pos = np.zeros((num_poses, 2))
+    th = np.zeros(num_poses)
+    for i in range(1, num_poses):
+        t = th[i - 1]
+        if rng.random() < 0.3:
+            t = _wrap(t + (np.pi / 2 if rng.random() < 0.5 else -np.pi / 2))
+        th[i] = t
+        pos[i] = pos[i - 1] + np.round([math.cos(t), math.sin(t)])
+    # candidate loop closures: non-consecutive pairs closer than 1.5 m
+    cells = {}
+    for i, p in enumerate(np.round(pos).astype(np.int64)):
+        cells.setdefault((int(p[0]), int(p[1])), []).append(i)
+    cand = []
+    for (cx, cy), idx in cells.items():
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                other = cells.get((cx + dx, cy + dy))
+                if not other:
+                    continue
+                for i in idx:
+                    for j in other:
+                        if j > i + 1 and np.hypot(*(pos[j] - pos[i])) < 1.5:
+                            cand.append((i, j))
+    cand = np.array(sorted(cand), dtype=np.int64).reshape(-1, 2)
+    if len(cand) > num_closures:
+        cand = cand[np.sort(rng.choice(len(cand), num_closures, replace=False))]
+    pairs = np.concatenate([np.stack([np.arange(num_poses - 1), np.arange(1, num_poses)], 1), cand])
+    # true relative poses Xi^-1 Xj
+    i, j = pairs[:, 0], pairs[:, 1]
+    d = pos[j] - pos[i]
+    c, s = np.cos(th[i]), np.sin(th[i])
+    rel = np.stack([c * d[:, 0] + s * d[:, 1], -s * d[:, 0] + c * d[:, 1], _wrap(th[j] - th[i])], 1)
+    sig = np.array([0.05, 0.05, 0.01])
+    meas = rel + rng.normal(0.0, 1.0, size=rel.shape) * sig
+    meas[:, 2] = _wrap(meas[:, 2])
+    info = np.tile(np.diag(1.0 / sig ** 2).reshape(1, 9), (len(pairs), 1))
+    # initial guess: compose noisy odometry
+    est = np.zeros((num_poses, 3))
+    est[0] = [pos[0, 0], pos[0, 1], th[0]]
+    for k in range(num_poses - 1):
+        x, y, t = est[k]
+        m = meas[k]
+        est[k + 1] = [x + math.cos(t) * m[0] - math.sin(t) * m[1],
+                      y + math.sin(t) * m[0] + math.cos(t) * m[1], _wrap(t + m[2])]
+    fixed = np.zeros(num_poses, np.uint8)
+    fixed[0] = 1
+    g = Graph(POSE_SE2, EDGE_SE2, est, pairs.astype(np.int32), meas, info, pose_fixed=fixed,
+              name=f"pose_graph_2d_{num_poses}")
+    g.extra["truth"] = np.stack([pos[:, 0], pos[:, 1], th], 1)
+    return g
+
+
+# ---------------------------------------------------------- 3D pose graph
+def pose_graph_3d(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
+    rng = np.random.default_rng(seed)
+    n = num_rings * per_ring
+    R = np.zeros((n, 3, 3))
+    t = np.zeros((n, 3))
+    for k in range(num_rings):
+        pol = np.pi * (k + 1) / (num_rings + 1)
+        for j in range(per_ring):
+            az = 2 * np.pi * j / per_ring
+            idx = k * per_ring + j
+            t[idx] = radius * np.array([np.sin(pol) * np.cos(az), np.sin(pol) * np.sin(az), np.cos(pol)])
+            R[idx] = _axis_angle(np.array([0.0, 0.0, az + np.pi / 2])) @ _axis_angle(np.array([pol - np.pi / 2, 0, 0]))
+    edges = []
+    for k in range(num_rings):
+        base = k * per_ring
+        for j in range(per_ring - 1):
+            edges.append((base + j, base + j + 1))
+        if k + 1 < num_rings:
+            edges.append((base + per_ring - 1, base + per_ring))  # chain to the next ring
+    odo = len(edges)
+    for k in range(num_rings):
+        base = k * per_ring
+        edges.append((base, base + per_ring - 1))  # ring closure
+    for k in range(num_rings - 1):
+        a, b = k * per_ring, (k + 1) * per_ring
+        nxt = t[b:b + per_ring]
+        for j in range(per_ring):
+            jj = int(np.argmin(np.linalg.norm(nxt - t[a + j], axis=1)))
+            edges.append((a + j, b + jj))
+    edges = np.array(edges, dtype=np.int64)
+    i, j = edges[:, 0], edges[:, 1]
+    Rt = np.transpose(R[i], (0, 2, 1))
+    relR = Rt @ R[j]
+    relt = np.einsum("nab,nb->na", Rt, t[j] - t[i])
+    sig_t, sig_r = 0.01, 0.005
+    nR = _compact_quat_noise(rng, len(edges), sig_r)
+    nt = rng.normal(0.0, sig_t, size=(len(edges), 3))
+    mR = relR @ nR
+    mt = relt + np.einsum("nab,nb->na", relR, nt)
+    meas = _iso12(mR, mt)
+    info = np.tile(np.diag([1 / sig_t ** 2] * 3 + [1 / (sig_r ** 2)] * 3).reshape(1, 36), (len(edges), 1))
+    # initial guess: compose the noisy chain
+    eR = np.zeros((n, 3, 3))
+    et = np.zeros((n, 3))
+    eR[0], et[0] = R[0], t[0]
+    for k in range(odo):
+        a, b = edges[k]
+        eR[b] = eR[a] @ mR[k]
+        et[b] = et[a] + eR[a] @ mt[k]
+    fixed = np.zeros(n, np.uint8)
+    fixed[0] = 1
+    g = Graph(POSE_SE3, EDGE_SE3, _iso12(eR, et), edges.astype(np.int32), meas, info, pose_fixed=fixed,
+              name=f"pose_graph_3d_{n}")
+    g.extra["truth"] = _iso12(R, t)
+    return g
+
+
+# ------------------------------------------------------ bundle adjustment
+def _look_at(centers, target):
+    fwd = target[None, :] - centers
+    fwd /= np.linalg.norm(fwd, axis=1, keepdims=True)
+    up = np.array([0.0, 0.0, 1.0])
+    x = np.cross(fwd, up)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    y = np.cross(fwd, x)
+    Rcw = np.stack([x, y, fwd], axis=1)  # rows: camera axes in world
+    tcw = -np.einsum("nab,nb->na", Rcw, centers)
+    return Rcw, tcw
+
+
+def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, height=1.5,
+                      box=(10.0, 10.0, 5.0), mean_obs=5.0, min_obs=2, max_obs=20,
+                      focal=500.0, width=640, height_px=480, pixel_noise=1.0, outlier_ratio=0.01,
+                      pose_noise=(0.05, 0.01), point_noise=0.1, num_fixed=2,
+                      seed=SEED_BASE + 2, chunk=2048):
+    """Ring of inward-looking cameras observing a box of points (ba_demo form)."""
+    rng = np.random.default_rng(seed)
+    az = 2 * np.pi * np.arange(num_cameras) / num_cameras
+    centers = np.stack([ring_radius * np.cos(az), ring_radius * np.sin(az), np.full(num_cameras, height)], 1)
+    Rcw, tcw = _look_at(centers, np.array([0.0, 0.0, box[2] / 2]))
+    X = np.stack([rng.uniform(-box[0], box[0], num_points), rng.uniform(-box[1], box[1], num_points),
+                  rng.uniform(0.0, box[2], num_points)], 1)
+    cx, cy = width / 2.0, height_px / 2.0
+    kdraw = np.clip(rng.geometric(1.0 / mean_obs, size=num_points), min_obs, max_obs)
+    pts, cams, uvs = [], [], []
+    for s in range(0, num_points, chunk):
+        Xs = X[s:s + chunk]
+        Xc = np.einsum("cab,pb->pca", Rcw, Xs) + tcw[None, :, :]
+        z = Xc[..., 2]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            u = focal * Xc[..., 0] / z + cx
+            v = focal * Xc[..., 1] / z + cy
+        vis = (z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height_px)
+        keys = rng.random(vis.shape)
+        keys[~vis] = 2.0
+        order = np.argsort(keys, axis=1)
+        nvis = vis.sum(axis=1)
+        k = np.minimum(kdraw[s:s + chunk], nvis)
+        for r in range(Xs.shape[0]):
+            if k[r] < 2:
+                continue
+            sel = np.sort(order[r, :k[r]])
+            pts.append(np.full(len(sel), s + r))
+            cams.append(sel)
+            uvs.append(np.stack([u[r, sel], v[r, sel]], 1))
+    pts = np.concatenate(pts)
+    cams = np.concatenate(cams)
+    uv = np.concatenate(uvs) + rng.normal(0.0, pixel_noise, size=(len(pts), 2))
+    out = rng.random(len(pts)) < outlier_ratio
+    uv[out] = np.stack([rng.uniform(0, width, out.sum()), rng.uniform(0, height_px, out.sum())], 1)
+    # keep only observed points, renumbered in order
+    used = np.unique(pts)
+    remap = -np.ones(num_points, np.int64)
+    remap[used] = np.arange(len(used))
+    pts = remap[pts]
+    Xt = X[used]
+    # initial guess
+    dR = _axis_angle(rng.normal(0.0, pose_noise[1], size=(num_cameras, 3)))
+    dt = rng.normal(0.0, pose_noise[0], size=(num_cameras, 3))
+    R0 = dR @ Rcw
+    t0 = np.einsum("nab,nb->na", dR, tcw) + dt
+    fixed = np.zeros(num_cameras, np.uint8)
+    fixed[:num_fixed] = 1
+    R0[:num_fixed], t0[:num_fixed] = Rcw[:num_fixed], tcw[:num_fixed]
+    pose_est = np.concatenate([t0, _rot_to_quat(R0)], axis=1)
+    X0 = Xt + rng.normal(0.0, point_noise, size=Xt.shape)
+    E = len(pts)
+    info = np.tile(np.eye(2).reshape(1, 4), (E, 1))
+    g = Graph(POSE_SE3EXPMAP, EDGE_PROJECT_XYZ2UV, pose_est,
+              np.stack([pts, cams], 1).astype(np.int32), uv, info, pose_fixed=fixed,
+              point_estimate=X0, point_fixed=np.zeros(len(Xt), np.uint8),
+              robust_delta=np.full(E, math.sqrt(5.991)), focal_length=focal,
+              principal_point=(cx, cy), name=f"bundle_adjustment_{num_cameras}x{len(Xt)}")
+    g.extra["truth_pose"] = np.concatenate([tcw, _rot_to_quat(Rcw)], axis=1)
+    g.extra["truth_point"] = Xt
+    g.extra["outliers"] = out
+    return g
+
+
+CONFIGS = {
+    "pg2d": lambda: pose_graph_2d(),
+    "pg3d": lambda: pose_graph_3d(),
+    "ba": lambda: bundle_adjustment(),
+}

@@ -1,0 +1,215 @@
+/*
+ * g2o_cuda.h -- C-ABI of the B200 (sm_100a) solver backend.
+ *
+ * This is the drop-in boundary between g2o's host C++ (SparseOptimizer,
+ * OptimizationAlgorithmFactory) and the device solver. Only plain pointers,
+ * sizes and status codes cross it; no C++, Eigen or torch types.
+ *
+ * Each entry point names the g2o interface it replaces (paths are relative to
+ * the g2o source tree):
+ *
+ *   g2oc_create / g2oc_destroy      OptimizationAlgorithmFactory::construct
+ *                                   (g2o/core/optimization_algorithm_factory.cpp:74-84)
+ *                                   and ~OptimizationAlgorithm
+ *   g2oc_construct                  the creator's name parsing
+ *                                   (g2o/solvers/pcg/solver_pcg.cpp:49-72)
+ *   g2oc_upload                     SparseOptimizer::initializeOptimization +
+ *                                   buildIndexMapping + BlockSolver::buildStructure
+ *                                   (g2o/core/sparse_optimizer.cpp:175-287,
+ *                                    g2o/core/block_solver.hpp:110-269)
+ *   g2oc_optimize                   SparseOptimizer::optimize with
+ *                                   OptimizationAlgorithm{Levenberg,GaussNewton}::solve
+ *                                   (g2o/core/sparse_optimizer.cpp:393-455,
+ *                                    g2o/core/optimization_algorithm_levenberg.cpp:60-153,
+ *                                    g2o/core/optimization_algorithm_gauss_newton.cpp:48-93)
+ *   g2oc_chi2 / g2oc_errors         computeActiveErrors + activeChi2 / activeRobustChi2
+ *                                   (g2o/core/sparse_optimizer.cpp:78-130)
+ *   g2oc_jacobians                  Edge::linearizeOplus (per-edge Jacobians)
+ *   g2oc_build_system               BlockSolver::buildSystem (g2o/core/block_solver.hpp:492-565)
+ *   g2oc_get_pattern / g2oc_get_hessian   the Hpp/Hpl/Hll/Hschur block patterns and
+ *                                   values (SparseBlockMatrix::blockCols order)
+ *   g2oc_schur                      BlockSolver::setLambda + the Schur part of
+ *                                   BlockSolver::solve (g2o/core/block_solver.hpp:331-448, 567-606)
+ *   g2oc_solve                      setLambda + BlockSolver::solve + restoreDiagonal
+ *   g2oc_solve_block_system         LinearSolver<MatrixType>::solve(A, x, b)
+ *                                   (g2o/core/linear_solver.h:64-65) on a caller block matrix
+ *   g2oc_download / g2oc_set_estimates   vertex estimate read-back / write
+ *
+ * Conventions
+ *   - Every function returns G2OC_OK (0) or a positive G2OC_ERR_* code and
+ *     never aborts the process. g2oc_last_error() gives a message.
+ *   - All host buffers are owned by the caller. A context owns its device
+ *     memory and one CUDA stream. A context is not thread-safe; use one per
+ *     host thread.
+ *   - Vertices are given in g2o id order: poses first (index 0..num_poses-1),
+ *     then points. The Hessian order follows SparseOptimizer::buildIndexMapping:
+ *     free non-marginalized vertices in that order, then marginalized ones;
+ *     fixed vertices get no Hessian index.
+ *   - Edges are given in insertion (internalId) order.
+ *   - Block patterns are listed column-major over the upper triangle
+ *     (column, then row), the order of SparseBlockMatrix::blockCols(); block
+ *     values are dense row-major.
+ */
+#ifndef G2O_CUDA_H
+#define G2O_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define G2OC_ABI_VERSION 1
+
+/* status codes */
+#define G2OC_OK 0
+#define G2OC_ERR_INVALID_ARGUMENT 1 /* null pointer, bad size, bad enum */
+#define G2OC_ERR_BAD_GRAPH 2        /* unsupported types, index out of range, empty graph */
+#define G2OC_ERR_CUDA 3             /* a CUDA runtime call failed */
+#define G2OC_ERR_NOT_PD 4           /* Cholesky met a non-positive pivot */
+#define G2OC_ERR_NAN 5              /* non-finite value in error, Hessian or update */
+#define G2OC_ERR_STATE 6            /* call order violated (e.g. optimize before upload) */
+#define G2OC_ERR_NO_DEVICE 7        /* no CUDA device or wrong architecture */
+#define G2OC_ERR_UNKNOWN_SOLVER 8   /* g2oc_construct: name not registered */
+#define G2OC_ERR_TIMEOUT 9          /* a bounded device-side wait gave up */
+#define G2OC_ERR_NOT_SUPPORTED 10   /* combination not implemented */
+
+/* vertex / edge types (g2o class names) */
+#define G2OC_POSE_SE2 1        /* VertexSE2: estimate (x, y, theta) */
+#define G2OC_POSE_SE3 2        /* VertexSE3: Isometry3, 12 doubles: R row-major (9) then t (3) */
+#define G2OC_POSE_SE3EXPMAP 3  /* VertexSE3Expmap: SE3Quat::toVector (tx,ty,tz,qx,qy,qz,qw) */
+
+#define G2OC_EDGE_SE2 1            /* EdgeSE2(VertexSE2, VertexSE2), D=3, measurement (x,y,theta) */
+#define G2OC_EDGE_SE3 2            /* EdgeSE3(VertexSE3, VertexSE3), D=6, measurement Isometry3 (12) */
+#define G2OC_EDGE_PROJECT_XYZ2UV 3 /* EdgeProjectXYZ2UV(VertexPointXYZ, VertexSE3Expmap), D=2 */
+
+/* algorithm / linear solver / precision */
+#define G2OC_ALGO_GAUSS_NEWTON 0
+#define G2OC_ALGO_LEVENBERG 1
+
+#define G2OC_LINEAR_PCG 0      /* block-Jacobi PCG (LinearSolverPCG semantics) */
+#define G2OC_LINEAR_CHOLESKY 1 /* dense Cholesky of the (reduced) system */
+
+#define G2OC_PREC_FP64 0  /* every kernel in FP64 */
+#define G2OC_PREC_MIXED 1 /* FP32 J/H/Schur/SpMV + FP64 refinement, FP64 chi2 and LM control */
+
+/* SolverResult of OptimizationAlgorithm::solve (g2o/core/optimization_algorithm.h:48) */
+#define G2OC_RESULT_OK 1
+#define G2OC_RESULT_FAIL -1
+#define G2OC_RESULT_TERMINATE 2
+
+typedef struct g2oc_graph {
+  int32_t pose_type;           /* G2OC_POSE_* */
+  int32_t num_poses;
+  const double* pose_estimate; /* num_poses * {3, 12, 7} */
+  const uint8_t* pose_fixed;   /* num_poses, may be NULL (none fixed) */
+  int32_t num_points;          /* VertexPointXYZ count (0 for pose graphs) */
+  const double* point_estimate;/* num_points * 3 */
+  const uint8_t* point_fixed;  /* num_points, may be NULL */
+  int32_t edge_type;           /* G2OC_EDGE_* */
+  int32_t num_edges;
+  const int32_t* edge_vertex;  /* num_edges * 2: (vertex0, vertex1). For
+                                  PROJECT_XYZ2UV vertex0 is a point index and
+                                  vertex1 a pose index; otherwise both are pose
+                                  indices. */
+  const double* measurement;   /* num_edges * {3, 12, 2} */
+  const double* information;   /* num_edges * D*D, row-major, symmetric */
+  const double* robust_delta;  /* num_edges Huber deltas; <= 0 or NULL: no kernel */
+  double focal_length;         /* CameraParameters (PROJECT_XYZ2UV only) */
+  double principal_point[2];
+} g2oc_graph;
+
+typedef struct g2oc_params {
+  int32_t algorithm;                 /* G2OC_ALGO_* */
+  int32_t linear_solver;             /* G2OC_LINEAR_* */
+  int32_t precision;                 /* G2OC_PREC_* */
+  int32_t pcg_max_iterations;        /* -1: system dimension (LinearSolverPCG::_maxIter) */
+  double pcg_tolerance;              /* 1e-6 (LinearSolverPCG::_tolerance) */
+  int32_t pcg_absolute_tolerance;    /* 1 (LinearSolverPCG::_absoluteTolerance) */
+  int32_t max_trials_after_failure;  /* 10 ("maxTrialsAfterFailure" property) */
+  double initial_lambda;             /* 0: tau * max diag(H) ("initialLambda" property) */
+  double tau;                        /* 1e-5 */
+  int32_t refine_max_iterations;     /* mixed precision: outer FP64 refinement steps (default 4) */
+  double refine_tolerance;           /* mixed precision: stop when |r|/|b| below (default 1e-10) */
+} g2oc_params;
+
+/* one per outer iteration, the fields of G2OBatchStatistics (g2o/core/batch_stats.h:40-82) */
+typedef struct g2oc_iteration_stats {
+  int32_t iteration;
+  int32_t result;                 /* G2OC_RESULT_* */
+  int32_t levenberg_iterations;   /* trials in this iteration */
+  int32_t iterations_linear_solver; /* PCG iterations, summed over trials */
+  double chi2;                    /* activeRobustChi2 after the iteration */
+  double lambda;                  /* current LM lambda after the iteration */
+  double time_residuals;          /* seconds, device-timed */
+  double time_quadratic_form;
+  double time_schur_complement;
+  double time_linear_solver;
+  double time_update;
+  double time_iteration;
+} g2oc_iteration_stats;
+
+typedef struct g2oc_hessian_info {
+  int32_t num_free_poses;   /* Hpp block rows */
+  int32_t num_free_points;  /* Hll block rows (marginalized) */
+  int32_t pose_dim;         /* 3 or 6 */
+  int32_t point_dim;        /* 3 or 0 */
+  int32_t hpp_nnzb;         /* upper blocks incl. diagonal */
+  int32_t hpl_nnzb;
+  int32_t schur_nnzb;       /* upper blocks incl. diagonal, 0 without Schur */
+  int32_t num_active_edges;
+  int64_t vector_size;      /* Solver::vectorSize() */
+} g2oc_hessian_info;
+
+typedef struct g2oc_ctx g2oc_ctx;
+
+/* library */
+int g2oc_abi_version(void);
+const char* g2oc_last_error(void);
+void g2oc_default_params(g2oc_params* params);
+/* Registered names, ';'-separated, into buf (OptimizationAlgorithmFactory::listSolvers). */
+int g2oc_list_solvers(char* buf, size_t buf_size);
+/* Fill params from a registered name such as "lm_cuda" or "gn_cuda_pcg6_3".
+   Unknown names return G2OC_ERR_UNKNOWN_SOLVER and leave params untouched
+   (the factory returns nullptr for them). */
+int g2oc_construct(const char* name, g2oc_params* params);
+
+/* context */
+int g2oc_create(int device, g2oc_ctx** out);
+void g2oc_destroy(g2oc_ctx* ctx);
+int g2oc_set_params(g2oc_ctx* ctx, const g2oc_params* params);
+
+/* graph */
+int g2oc_upload(g2oc_ctx* ctx, const g2oc_graph* graph);
+int g2oc_get_hessian_info(g2oc_ctx* ctx, g2oc_hessian_info* info);
+int g2oc_set_estimates(g2oc_ctx* ctx, const double* pose_estimate, const double* point_estimate);
+int g2oc_download(g2oc_ctx* ctx, double* pose_estimate, double* point_estimate);
+
+/* optimization: stats may be NULL, else iterations entries */
+int g2oc_optimize(g2oc_ctx* ctx, int iterations, g2oc_iteration_stats* stats, int* iterations_done);
+
+/* parity hooks at the current estimate */
+int g2oc_chi2(g2oc_ctx* ctx, double* chi2, double* robust_chi2);
+int g2oc_errors(g2oc_ctx* ctx, double* errors);                 /* num_active_edges * D */
+int g2oc_jacobians(g2oc_ctx* ctx, double* jac0, double* jac1);  /* row-major D x dim(v0), D x dim(v1) */
+int g2oc_build_system(g2oc_ctx* ctx);
+int g2oc_get_pattern(g2oc_ctx* ctx, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* schur_rc); /* pairs (row, col) */
+int g2oc_get_hessian(g2oc_ctx* ctx, double* hpp, double* hll, double* hpl, double* b);
+int g2oc_schur(g2oc_ctx* ctx, double lambda, double* schur_blocks, double* bschur);
+int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations);
+
+/* LinearSolver::solve on a caller block matrix: symmetric, upper blocks given
+   column-major as (row, col) block pairs with row-major dense values; block
+   sizes from block_offsets (num_blocks + 1 entries, scalar offsets). x gets
+   the solution; PCG uses the LinearSolverPCG defaults from params. */
+int g2oc_solve_block_system(g2oc_ctx* ctx, int32_t linear_solver, int32_t num_block_rows,
+                            const int32_t* block_offsets, int32_t nnzb, const int32_t* block_rc,
+                            const double* values, const double* b, double* x,
+                            int32_t* iterations);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G2O_CUDA_H */

@@ -1,0 +1,99 @@
+"""The C-ABI boundary: header/ctypes layouts agree, the library loads and
+exports every declared entry point, and the factory behaves like g2o's
+OptimizationAlgorithmFactory (unit_test/solver/allocate_algorithm_test.cpp:48-127).
+No GPU compute here."""
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import pytest
+
+from g2o_b200 import abi, backend
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _c_layout():
+    src = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "g2o_cuda.h"
+#define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m));
+int main(void) {
+  printf("g2oc_graph %zu\n", sizeof(g2oc_graph));
+  F(g2oc_graph, pose_estimate) F(g2oc_graph, num_points) F(g2oc_graph, edge_vertex)
+  F(g2oc_graph, robust_delta) F(g2oc_graph, focal_length) F(g2oc_graph, principal_point)
+  printf("g2oc_params %zu\n", sizeof(g2oc_params));
+  F(g2oc_params, pcg_tolerance) F(g2oc_params, initial_lambda) F(g2oc_params, refine_tolerance)
+  printf("g2oc_iteration_stats %zu\n", sizeof(g2oc_iteration_stats));
+  F(g2oc_iteration_stats, chi2) F(g2oc_iteration_stats, time_iteration)
+  printf("g2oc_hessian_info %zu\n", sizeof(g2oc_hessian_info));
+  F(g2oc_hessian_info, vector_size)
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(src)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    return dict(line.split() for line in out.strip().splitlines())
+
+
+def test_struct_layouts_match_header():
+    lay = _c_layout()
+    structs = {"g2oc_graph": abi.G2ocGraph, "g2oc_params": abi.G2ocParams,
+               "g2oc_iteration_stats": abi.G2ocIterationStats, "g2oc_hessian_info": abi.G2ocHessianInfo}
+    for name, cls in structs.items():
+        assert int(lay[name]) == C.sizeof(cls), name
+    for key, val in lay.items():
+        if "." in key:
+            s, m = key.split(".")
+            cls = structs[s]
+            field = "lambda_" if m == "lambda" else m
+            assert getattr(cls, field).offset == int(val), key
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    names = backend.header_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(cuda_lib, n), n
+    assert cuda_lib.g2oc_abi_version() == 1
+
+
+def test_factory_lists_and_constructs():
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    names = fac.list_solvers()
+    for n in ["gn_cuda", "lm_cuda", "lm_cuda_pcg6_3", "gn_cuda_pcg3_3", "lm_cuda_chol", "lm_cuda_mixed"]:
+        assert n in names
+    for n in names:
+        p = fac.construct(n)
+        assert p is not None, n
+        assert p.algorithm == (abi.ALGO_GAUSS_NEWTON if n.startswith("gn") else abi.ALGO_LEVENBERG)
+    assert fac.construct("lm_cuda_mixed").precision == abi.PREC_MIXED
+    assert fac.construct("gn_cuda_chol").linear_solver == abi.LINEAR_CHOLESKY
+    assert fac.construct("gn_cuda_pcg6_3").linear_solver == abi.LINEAR_PCG
+    assert fac.construct("non_existing_solver") is None
+    assert fac.construct("") is None
+
+
+def test_default_params_are_the_reference_defaults():
+    p = backend.default_params()
+    assert p.pcg_tolerance == 1e-6 and p.pcg_max_iterations == -1 and p.pcg_absolute_tolerance == 1
+    assert p.max_trials_after_failure == 10 and p.tau == 1e-5 and p.initial_lambda == 0.0
+
+
+def test_create_without_device_reports_no_device(cuda_lib):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    h = C.c_void_p()
+    st = cuda_lib.g2oc_create(0, C.byref(h))
+    assert st == abi.G2OC_ERR_NO_DEVICE
+    assert not h.value

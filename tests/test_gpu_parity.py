@@ -1,0 +1,241 @@
+"""Parity of the CUDA path (through the C-ABI) with the FP64 oracle on the same
+seeded graphs.
+
+Tolerances (FP64 path): errors and Jacobians 1e-12 relative; Hessian blocks,
+gradient and Schur blocks 1e-10 relative per block (the bar for the plain
+FP64 form); block patterns bit-exact; linear solves and LM trajectories
+within the stated tolerances of each test.
+"""
+import numpy as np
+import pytest
+
+from g2o_b200 import synth
+from g2o_b200.abi import (ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, LINEAR_CHOLESKY, LINEAR_PCG, PREC_MIXED)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def backend():
+    from g2o_b200 import backend as B
+    B.library()
+    return B
+
+
+def small_ba(seed=7, cams=40, points=3000, **kw):
+    return synth.bundle_adjustment(num_cameras=cams, num_points=points, seed=seed, **kw)
+
+
+def rel_block_err(a, b):
+    """max over blocks of |a-b|_max / max(|b|_max, tiny)"""
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return float((np.abs(a - b).max(axis=1) / scale).max())
+
+
+def relnorm(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def both(backend, oracle_lib, g, **prm):
+    o = oracle_lib.OracleProblem(g, oracle_lib.default_params(**prm))
+    c = backend.CudaProblem(g, backend.default_params(**prm))
+    return o, c
+
+
+# ----------------------------------------------------------------- BA
+def test_ba_structure_is_bit_exact(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    for f in ("num_free_poses", "num_free_points", "hpp_nnzb", "hpl_nnzb", "schur_nnzb", "num_active_edges",
+              "vector_size"):
+        assert getattr(o.info, f) == getattr(c.info, f), f
+    for a, b in zip(o.pattern(), c.pattern()):
+        assert np.array_equal(a, b)
+
+
+def test_ba_errors_jacobians_chi2(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    assert relnorm(c.errors(), o.errors()) < 1e-12
+    j0c, j1c = c.jacobians()
+    j0o, j1o = o.jacobians()
+    assert rel_block_err(j0c, j0o) < 1e-12
+    assert rel_block_err(j1c, j1o) < 1e-12
+    (a, b), (x, y) = c.chi2(), o.chi2()
+    assert abs(a - x) <= 1e-12 * x and abs(b - y) <= 1e-12 * y
+
+
+def test_ba_hessian_and_gradient(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    o.build_system()
+    c.build_system()
+    hpp_o, hll_o, hpl_o, b_o = o.hessian()
+    hpp_c, hll_c, hpl_c, b_c = c.hessian()
+    assert rel_block_err(hpp_c, hpp_o) < 1e-10
+    assert rel_block_err(hll_c, hll_o) < 1e-10
+    assert rel_block_err(hpl_c, hpl_o) < 1e-10
+    n = o.info.num_free_poses * 6
+    assert rel_block_err(b_c[:n].reshape(-1, 6), b_o[:n].reshape(-1, 6)) < 1e-10
+    assert relnorm(b_c[n:], b_o[n:]) < 1e-10
+
+
+@pytest.mark.parametrize("lam", [0.0, 1e-3, 10.0])
+def test_ba_schur_complement(backend, oracle_lib, lam):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    o.build_system()
+    c.build_system()
+    So, bso = o.schur(lam)
+    Sc, bsc = c.schur(lam)
+    assert rel_block_err(Sc, So) < 1e-10
+    assert relnorm(bsc, bso) < 1e-10
+
+
+def test_ba_pcg_solve_matches_oracle(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    o.build_system()
+    c.build_system()
+    so, xo, ito = o.solve(1e-2)
+    sc, xc, itc = c.solve(1e-2)
+    assert so == 0 and sc == 0
+    assert abs(itc - ito) <= 1
+    assert relnorm(xc, xo) < 1e-6
+
+
+def test_ba_cholesky_solve_is_exact(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g, linear_solver=LINEAR_CHOLESKY)
+    o.build_system()
+    c.build_system()
+    so, xo, _ = o.solve(1e-2)
+    sc, xc, _ = c.solve(1e-2)
+    assert so == 0 and sc == 0
+    assert relnorm(xc, xo) < 1e-9
+
+
+def test_ba_lm_trajectory(backend, oracle_lib):
+    g = small_ba()
+    o, c = both(backend, oracle_lib, g)
+    do, so = o.optimize(20)
+    dc, sc = c.optimize(20)
+    assert do == dc == 20
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"]
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["chi2"], b["chi2"])
+    po, qo = o.estimates()
+    pc, qc = c.estimates()
+    assert np.abs(pc - po).max() < 1e-5
+    assert np.abs(qc - qo).max() < 1e-4
+
+
+def test_ba_mixed_precision_reaches_fp64_chi2(backend, oracle_lib):
+    g = small_ba()
+    o = oracle_lib.OracleProblem(g)
+    _, so = o.optimize(20)
+    target = so[-1]["chi2"]
+    c = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED))
+    _, sc = c.optimize(30)
+    best = min(s["chi2"] for s in sc)
+    assert best <= target * (1 + 1e-6), (best, target)
+
+
+def test_ba_fixed_points_and_duplicate_observations(backend, oracle_lib):
+    g = small_ba(seed=11, cams=12, points=400)
+    g.point_fixed[::7] = 1
+    # duplicate a few observations (same camera observes the same point twice)
+    dup = np.arange(0, g.num_edges, 97)
+    for name in ("edge_vertex", "measurement", "information", "robust_delta"):
+        a = getattr(g, name)
+        setattr(g, name, np.ascontiguousarray(np.concatenate([a, a[dup]])))
+    g.measurement[-len(dup):] += 0.5
+    o, c = both(backend, oracle_lib, g)
+    for a, b in zip(o.pattern(), c.pattern()):
+        assert np.array_equal(a, b)
+    o.build_system()
+    c.build_system()
+    for a, b in zip(c.hessian()[:3], o.hessian()[:3]):
+        assert rel_block_err(a, b) < 1e-10
+    do, so = o.optimize(5)
+    dc, sc = c.optimize(5)
+    assert abs(sc[-1]["chi2"] - so[-1]["chi2"]) <= 1e-6 * so[-1]["chi2"]
+
+
+def test_ba_without_robust_kernel(backend, oracle_lib):
+    g = small_ba(seed=5, cams=10, points=300)
+    g.robust_delta = None
+    o, c = both(backend, oracle_lib, g)
+    (a, b), (x, y) = c.chi2(), o.chi2()
+    assert a == pytest.approx(x, rel=1e-12) and b == pytest.approx(a, rel=0)
+    o.build_system()
+    c.build_system()
+    assert rel_block_err(c.hessian()[0], o.hessian()[0]) < 1e-10
+
+
+# ------------------------------------------------------------ pose graphs
+def test_pose_graph_2d_gn_cholesky(backend, oracle_lib):
+    g = synth.pose_graph_2d(num_poses=600, num_closures=200, seed=3)
+    o, c = both(backend, oracle_lib, g, algorithm=ALGO_GAUSS_NEWTON, linear_solver=LINEAR_CHOLESKY)
+    for a, b in zip(o.pattern(), c.pattern()):
+        assert np.array_equal(a, b)
+    assert relnorm(c.errors(), o.errors()) < 1e-12
+    j = c.jacobians(), o.jacobians()
+    assert rel_block_err(j[0][0], j[1][0]) < 1e-12 and rel_block_err(j[0][1], j[1][1]) < 1e-12
+    o.build_system()
+    c.build_system()
+    assert rel_block_err(c.hessian()[0], o.hessian()[0]) < 1e-10
+    assert relnorm(c.hessian()[3], o.hessian()[3]) < 1e-10
+    do, so = o.optimize(10)
+    dc, sc = c.optimize(10)
+    assert do == dc == 10
+    for a, b in zip(sc, so):
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-8 * b["chi2"], (a["chi2"], b["chi2"])
+
+
+def test_pose_graph_3d_lm(backend, oracle_lib):
+    g = synth.pose_graph_3d(num_rings=4, per_ring=40, radius=10.0, seed=4)
+    o, c = both(backend, oracle_lib, g, algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_CHOLESKY)
+    assert relnorm(c.errors(), o.errors()) < 1e-12
+    j = c.jacobians(), o.jacobians()
+    assert rel_block_err(j[0][0], j[1][0]) < 1e-10 and rel_block_err(j[0][1], j[1][1]) < 1e-10
+    o.build_system()
+    c.build_system()
+    assert rel_block_err(c.hessian()[0], o.hessian()[0]) < 1e-10
+    do, so = o.optimize(10)
+    dc, sc = c.optimize(10)
+    assert do == dc
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"]
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-7 * b["chi2"], (a["chi2"], b["chi2"])
+
+
+def test_pose_graph_pcg(backend, oracle_lib):
+    g = synth.pose_graph_3d(num_rings=4, per_ring=40, radius=10.0, seed=4)
+    o, c = both(backend, oracle_lib, g, algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_PCG)
+    do, so = o.optimize(5)
+    dc, sc = c.optimize(5)
+    for a, b in zip(sc, so):
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["chi2"], b["chi2"])
+
+
+# -------------------------------------------------------- linear solvers
+def test_reference_block_system_on_gpu(backend):
+    from tests.test_oracle_pinning import is_approx, load_sparse_system
+    offs, rc, vals, b, x, _ = load_sparse_system()
+    for _ in range(2):
+        st, sol, _ = backend.solve_block_system(LINEAR_CHOLESKY, offs, rc, vals, b)
+        assert st == 0 and is_approx(sol, x, 1e-6)
+    prm = backend.default_params(pcg_tolerance=1e-20, pcg_max_iterations=200)
+    st, sol, it = backend.solve_block_system(LINEAR_PCG, offs, rc, vals, b, prm)
+    assert st == 0 and it > 0 and is_approx(sol, x, 1e-6)
+
+
+def test_not_positive_definite_is_reported(backend):
+    offs = np.array([0, 3, 6], np.int32)
+    rc = np.array([[0, 0], [0, 1], [1, 1]], np.int32)
+    vals = np.concatenate([np.eye(3).ravel(), 2 * np.eye(3).ravel(), np.eye(3).ravel()])
+    st, _, _ = backend.solve_block_system(LINEAR_CHOLESKY, offs, rc, vals, np.ones(6))
+    assert st == 4  # G2OC_ERR_NOT_PD
