@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark: bundle adjustment, Levenberg-Marquardt with Schur complement and
+block-Jacobi PCG (g2o's lm_pcg6_3 path) on the 1,000-camera / 200,000-point /
+~1.03M-edge synthetic configuration, 20 LM iterations per run.
+
+Our arm (default): the B200 backend through its C-ABI, mixed precision (FP32
+Jacobians / Hessian / Schur / SpMV storage, FP64 Krylov vectors, chi2, LM
+control and true-residual refinement). One step = one complete 20-iteration
+optimization from the initial estimates; `value` = LM iterations per second
+over K steps with the graph resident in HBM, timed with CUDA events on the
+solver's stream. The plain FP64 GPU form is timed the same way and reported
+beside it, with the mixed run's time to the FP64 run's final chi2 (+1e-6
+relative) and the linearization throughput in edges/s.
+
+`e2e`: the same metric through the C-ABI with host buffers: every step uploads
+the graph from pinned host memory (g2oc_upload: structure + H2D), optimizes 20
+iterations and downloads the estimates.
+
+Reference arm (--impl reference): the FP64 CPU restatement of the reference's
+path (oracle/, g2o cannot be built here: Eigen3 is absent) on all host cores,
+one LM iteration from the initial estimates per step.
+
+Multi-GPU (torchrun): the path is run as independent replicas, one per GPU
+(weak scaling); rank 0 prints the max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ITERATIONS = 20
+METRIC = "BA LM iter/s, time to FP64 chi2+-1e-6 (mixed vs FP64 GPU); edges/s linearize"
+FALLBACK_HBM_GBS = 6650.0
+WORKLOAD = "bundle_adjustment_1000cam_200000pt_1.03Medges_huber_lm20"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-iterations", type=int, default=1)
+    return ap.parse_args()
+
+
+def dist_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(kernel, info, E, real):
+    """Bytes each array element read or written once, per launch (the model
+    DESIGN.md states)."""
+    C, P = info.num_free_poses, info.num_free_points
+    nH, nS = info.hpl_nnzb, info.schur_nnzb
+    n = C * 6
+    if kernel == "ba_landmark_pass":
+        return 60 * E + 32 * P + 64 * C + 18 * real * nH + (6 * real + 24) * P
+    if kernel == "ba_camera_pass":
+        return 88 * E + (36 * real + 48) * C
+    if kernel == "schur_landmark":
+        return (6 + 9) * real * P + 36 * real * nH
+    if kernel == "schur_blocks":
+        return 8 * (nH * 5) + 36 * real * nH + 36 * real * C + 36 * real * nS + 4 * nS
+    if kernel == "pcg_spmv":
+        return 36 * real * nS + 12 * nS + 4 * 8 * n
+    if kernel == "chi2":
+        return 56 * E + 32 * P + 64 * C
+    if kernel == "ba_backsub":
+        return (18 * real + 4) * nH + (9 * real + 48) * P + 8 * n
+    return None
+
+
+def traffic_table():
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch from the
+    committed ncu summary (profiles/dram_traffic.txt: kernel precision bytes)."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                out[(parts[0], parts[1])] = float(parts[2])
+    return out
+
+
+def build_graph():
+    from g2o_b200 import synth
+    return synth.bundle_adjustment()
+
+
+def pinned_copy(g):
+    """The graph's arrays copied into page-locked host memory."""
+    import torch
+
+    def pin(a):
+        if a is None:
+            return None
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    h = g.copy()
+    for name in ("pose_estimate", "edge_vertex", "measurement", "information", "pose_fixed", "point_estimate",
+                 "point_fixed", "robust_delta"):
+        setattr(h, name, pin(getattr(h, name)))
+    return h
+
+
+def cpu_baseline(g, iters, threads):
+    from oracle import oracle
+    prob = oracle.OracleProblem(g, oracle.default_params(), threads=threads)
+    t0 = time.perf_counter()
+    done, st = prob.optimize(iters)
+    dt = time.perf_counter() - t0
+    return iters / dt, dt, st
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    from oracle import oracle
+    g = build_graph()
+    threads = os.cpu_count() or 1
+    prob = oracle.OracleProblem(g, oracle.default_params(), threads=threads)
+    pose0, point0 = prob.estimates()
+    times = []
+    for s in range(args.warmup + args.steps):
+        prob.set_estimates(pose0, point0)
+        t0 = time.perf_counter()
+        prob.optimize(1)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    T = sum(times)
+    value = args.steps / T
+    sample = f"one LM iteration (Schur + block-Jacobi PCG, FP64) of the full configuration per step, {threads} threads"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, BA generator)",
+        "config": {"workload": WORKLOAD, "iterations": 1, "cameras": g.num_poses, "points": g.num_points,
+                   "edges": g.num_edges, "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    rank, world, local = dist_info()
+    import numpy as np
+    import torch
+    from g2o_b200 import backend
+    from g2o_b200.abi import PREC_MIXED
+
+    device = local
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    g = build_graph()
+    E = g.num_edges
+    fac = backend.OptimizationAlgorithmFactory.instance()
+
+    def timed_runs(prob, steps, warmup, timing=False):
+        stream = torch.cuda.ExternalStream(prob.stream(), device=device)
+        for _ in range(warmup):
+            prob.restore_initial_estimates()
+            prob.optimize(ITERATIONS)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        prob.set_kernel_timing(timing)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        iters = 0
+        stats = None
+        ev0.record(stream)
+        for _ in range(steps):
+            prob.restore_initial_estimates()
+            done, stats = prob.optimize(ITERATIONS)
+            iters += len(stats)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=f"cuda:{device}")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+            torch.distributed.barrier()
+        return ms, iters, stats
+
+    # plain FP64 GPU form: the reference semantics in FP64, and the target chi2
+    p64 = backend.CudaProblem(g, fac.construct("lm_cuda_pcg6_3"), device=device)
+    ms64, it64, st64 = timed_runs(p64, max(1, min(args.steps, 3)), 1)
+    target = st64[-1]["chi2"]
+    fp64_ips = it64 / (ms64 * 1e-3)
+    fp64_time_20 = ms64 * 1e-3 / max(1, min(args.steps, 3))
+    p64.close()
+
+    # mixed precision: the headline
+    pm = backend.CudaProblem(g, fac.construct("lm_cuda_mixed"), device=device)
+    clocks = ClockSampler(device)
+    ms, iters, stm = timed_runs(pm, args.steps, args.warmup, timing=True)
+    clk = clocks.stop()
+    total_launches, kstats = pm.kernel_stats()
+    value = world * iters / (ms * 1e-3)
+    cum = 0.0
+    t_to = None
+    for s in stm:
+        cum += s["time_iteration"]
+        if s["chi2"] <= target * (1 + 1e-6):
+            t_to = cum
+            break
+    lin_ms = sum(kstats.get(k, (0, 0.0))[1] for k in ("ba_landmark_pass", "ba_camera_pass"))
+    lin_launches = kstats.get("ba_camera_pass", (0, 0))[0]
+    edges_per_s = (E * lin_launches) / (lin_ms * 1e-3) if lin_ms > 0 else None
+    # dominant kernel and its roofline
+    dom = max(kstats.items(), key=lambda kv: kv[1][1])
+    dname, (dlaunch, dms) = dom
+    real = 4
+    algo = algorithmic_bytes(dname, pm.info, pm.info.num_active_edges, real)
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if algo is not None and dlaunch > 0:
+        per_launch_s = dms * 1e-3 / dlaunch
+        achieved = algo / per_launch_s / 1e9
+        tr = traffic_table().get((dname, "mixed"))
+        roof = {"kernel": dname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": tr,
+                "algorithmic_bytes_per_launch": algo, "avg_launch_ms": dms / dlaunch, "launches": dlaunch}
+    kernel_table = {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in sorted(kstats.items(),
+                                                                                  key=lambda kv: -kv[1][1])}
+
+    # end to end through the C-ABI with host buffers (pinned): upload + optimize + download
+    hg = pinned_copy(g)
+    h2d = sum(a.nbytes for a in (hg.pose_estimate, hg.edge_vertex, hg.measurement, hg.information, hg.pose_fixed,
+                                 hg.point_estimate, hg.point_fixed, hg.robust_delta) if a is not None)
+    pose_out = np.empty((g.num_poses, 7))
+    point_out = np.empty((g.num_points, 3))
+    d2h = pose_out.nbytes + point_out.nbytes
+    import ctypes as C
+    L = backend.library()
+    stream = torch.cuda.ExternalStream(pm.stream(), device=device)
+    cg = hg.to_c()
+    for _ in range(1):
+        backend._check(L.g2oc_upload(pm.handle, C.byref(cg)))
+        pm.optimize(ITERATIONS)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e_steps = max(1, min(args.steps, 3))
+    e_iters = 0
+    e0.record(stream)
+    for _ in range(e_steps):
+        backend._check(L.g2oc_upload(pm.handle, C.byref(cg)))
+        d, st = pm.optimize(ITERATIONS)
+        e_iters += len(st)
+        backend._check(L.g2oc_download(pm.handle, backend._p(pose_out), backend._p(point_out)))
+    e1.record(stream)
+    e1.synchronize()
+    ems = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ems], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e_value = world * e_iters / (ems * 1e-3)
+    pm.close()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        ips, dt, _ = cpu_baseline(g, args.cpu_sample_iterations, threads)
+        cpu = {"value": ips, "unit": "iter/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_sample_iterations} LM iteration(s) of the full configuration from the initial "
+                         f"estimates, FP64 restatement of the reference path, {threads} threads, {dt:.2f} s"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32/f64 (FP32 Hessian/Schur/SpMV storage; FP64 vectors, chi2, LM)",
+        "data": "synthetic (seeded BA generator: ring cameras, box points, 1 px noise, 1% outliers, Huber)",
+        "config": {"workload": WORKLOAD, "iterations_per_step": ITERATIONS, "cameras": g.num_poses,
+                   "points": g.num_points, "edges": E, "schur_blocks": int(pm.info.schur_nnzb),
+                   "parallelism": "replicas" if world > 1 else "single-gpu",
+                   "l2": "working set ~0.6 GB > 126 MB L2; every step streams it"},
+        "fp64_gpu": {"iter_per_s": fp64_ips, "time_20_iterations_s": fp64_time_20, "final_chi2": target},
+        "mixed": {"final_chi2": stm[-1]["chi2"], "time_to_fp64_chi2_s": t_to,
+                  "speedup_vs_fp64": value / world / fp64_ips},
+        "linearize_edges_per_s": edges_per_s,
+        "roofline": roof,
+        "kernels": kernel_table,
+        "gpu_launches": int(total_launches),
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "iter/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

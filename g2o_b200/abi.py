@@ -102,6 +102,10 @@ class G2ocIterationStats(C.Structure):
         return {f[0].rstrip("_"): getattr(self, f[0]) for f in self._fields_}
 
 
+class G2ocKernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("total_ms", C.c_double)]
+
+
 class G2ocHessianInfo(C.Structure):
     _fields_ = [
         ("num_free_poses", C.c_int32),

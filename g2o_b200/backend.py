@@ -24,8 +24,8 @@ from typing import List, Optional
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocHessianInfo, G2ocIterationStats, G2ocParams,
-                  Graph, POSE_DIM, POSE_EST_DIM)
+from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocHessianInfo, G2ocIterationStats, G2ocKernelStat,
+                  G2ocParams, Graph, POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libg2o_b200.so")
@@ -71,6 +71,10 @@ def library() -> C.CDLL:
         "g2oc_schur": ([vp, C.c_double, dp, dp], C.c_int),
         "g2oc_solve": ([vp, C.c_double, dp, ip], C.c_int),
         "g2oc_solve_block_system": ([vp, C.c_int32, C.c_int32, ip, C.c_int32, ip, dp, dp, dp, ip], C.c_int),
+        "g2oc_get_stream": ([vp, C.POINTER(vp)], C.c_int),
+        "g2oc_restore_initial_estimates": ([vp], C.c_int),
+        "g2oc_set_kernel_timing": ([vp, C.c_int], C.c_int),
+        "g2oc_get_kernel_stats": ([vp, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -164,6 +168,24 @@ class CudaProblem:
     def set_params(self, params: G2ocParams):
         self.params = params
         _check(library().g2oc_set_params(self._h, C.byref(params)))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(library().g2oc_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def restore_initial_estimates(self):
+        _check(library().g2oc_restore_initial_estimates(self._h))
+
+    def set_kernel_timing(self, enable: bool):
+        _check(library().g2oc_set_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        arr = (G2ocKernelStat * 64)()
+        n = C.c_int()
+        tot = C.c_int64()
+        _check(library().g2oc_get_kernel_stats(self._h, arr, 64, C.byref(n), C.byref(tot)))
+        return tot.value, {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 64))}
 
     def estimates(self):
         g = self.graph

@@ -237,8 +237,9 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
 }
 
 // ---------------------------------------------------------------- Schur
-// Landmark step of the Schur loop (block_solver.hpp:359-378): Dinv =
-// (H_ll + lambda I)^-1 and, per Hpl block of the landmark, BD = B Dinv.
+// Landmark step of the Schur loop (block_solver.hpp:359-378):
+// Dinv = (H_ll + lambda I)^-1; with bd != nullptr also BD = B Dinv per Hpl
+// block (only for cameras too large to stage in shared memory).
 template <typename Real>
 __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_ptr, int Pf, double lambda,
                                Real* dinv, Real* bd, int* nonfinite) {
@@ -256,57 +257,142 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
     D[i] = (Real)Di[i];
     dinv[(size_t)l * 9 + i] = D[i];
   }
+  if (!bd) return;
   const int b1 = hb_ptr[l + 1];
   for (int a = hb_ptr[l]; a < b1; ++a) {
     const Real* B = hpl + (size_t)a * 18;
-    Real Bl[18];
-#pragma unroll
-    for (int i = 0; i < 18; ++i) Bl[i] = B[i];
     Real* o = bd + (size_t)a * 18;
 #pragma unroll
     for (int r = 0; r < 6; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        o[r * 3 + c] = Bl[r * 3] * D[c] + Bl[r * 3 + 1] * D[3 + c] + Bl[r * 3 + 2] * D[6 + c];
+      for (int c = 0; c < 3; ++c) o[r * 3 + c] = B[r * 3] * D[c] + B[r * 3 + 1] * D[3 + c] + B[r * 3 + 2] * D[6 + c];
   }
 }
 
-// Schur blocks (block_solver.hpp:379-427, with Hschur <- Hpp at :343-345):
-// S(i1,i2) = Hpp(i1,i2) + lambda I [diagonal] - sum over co-observing pairs
-// BD_a B_b^T, pairs in landmark order. Six threads per block, one per row.
 template <typename Real>
-__global__ void schur_blocks(const int* sp_ptr, const int2* sp_ab, const int* s_hpp, int nnzS, const Real* hpp,
-                             const Real* bd, const Real* hpl, double lambda, Real* S) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = t / 6, r = t % 6;
-  if (s >= nnzS) return;
-  double acc[6];
-  const int hb = s_hpp[s];
-#pragma unroll
-  for (int c = 0; c < 6; ++c) acc[c] = 0.0;
-  const int p1 = sp_ptr[s + 1];
-  for (int p = sp_ptr[s]; p < p1; ++p) {
-    const int2 ab = sp_ab[p];
-    const Real* D = bd + (size_t)ab.x * 18 + r * 3;
-    const Real d0 = D[0], d1 = D[1], d2 = D[2];
-    const Real* B = hpl + (size_t)ab.y * 18;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) acc[c] += (double)(d0 * B[c * 3] + d1 * B[c * 3 + 1] + d2 * B[c * 3 + 2]);
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using T = double2;
+};
+template <>
+struct Vec2<float> {
+  using T = float2;
+};
+
+// Schur complement by camera rows (block_solver.hpp:343-433): one CTA per
+// free camera r stages BD_a = B_a Dinv_l for the camera's Hpl blocks in
+// shared memory; then two lanes per Schur block (r, c) of the row (lane
+// parity = rows 0-2 or 3-5, 18 FP64 accumulators each) sum -BD_a B_b^T over
+// the block's co-observing pairs in landmark order (B_b read from L1/L2) and
+// add Hpp(r, c) (+ lambda on the diagonal). With bs != nullptr the reduced
+// right-hand side bs_r = b_r - sum_a BD_a b_l(a) is formed from the same
+// staged blocks. S is written in the row-SoA layout of sys_offset.
+template <typename Real, bool A_SMEM, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
+    schur_rows(const int* hc_ptr, const int* hc_blk, const int* hpl_col, const Real* hpl, const Real* dinv,
+               const Real* bd, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs,
+               const int* s_hpp, const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l,
+               double* bs) {
+  using R2 = typename Vec2<Real>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Real* BDa = reinterpret_cast<Real*>(smem_raw);
+  const int r = blockIdx.x;
+  const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (A_SMEM) {
+    for (int t = threadIdx.x; t < na * 18; t += THREADS) {
+      const int blk = t / 18, e = t % 18;
+      const int a = hc_blk[a0 + blk];
+      const Real* B = hpl + (size_t)a * 18 + (e / 3) * 3;
+      const Real* D = dinv + (size_t)hpl_col[a] * 9 + (e % 3);
+      BDa[t] = B[0] * D[0] + B[1] * D[3] + B[2] * D[6];
+    }
+    __syncthreads();
   }
-  Real* out = S + (size_t)s * 36 + r * 6;
+  auto bd_of = [&](int al) -> const Real* {
+    return A_SMEM ? BDa + (size_t)al * 18 : bd + (size_t)hc_blk[a0 + al] * 18;
+  };
+  if (bs && warp == 0) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = lane; t < na; t += 32) {
+      const double* bl = b_l + (size_t)hpl_col[hc_blk[a0 + t]] * 3;
+      const Real* D = bd_of(t);
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    double v = -acc[c];
-    if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + r * 6 + c] + (r == c ? lambda : 0.0);
-    out[c] = (Real)v;
+      for (int q = 0; q < 6; ++q) acc[q] += (double)D[q * 3] * bl[0] + (double)D[q * 3 + 1] * bl[1] + (double)D[q * 3 + 2] * bl[2];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
+    if (lane < 6) {
+      double v = acc[0];
+#pragma unroll
+      for (int q = 1; q < 6; ++q)
+        if (lane == q) v = acc[q];
+      bs[(size_t)r * 6 + lane] = b_p[(size_t)r * 6 + lane] - v;
+    }
+  }
+  const int half = threadIdx.x & 1;
+  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
+  Real* Sr = S + (size_t)rb * 36;
+  for (int j = threadIdx.x >> 1; j < nblk; j += THREADS / 2) {
+    const int k = rb + j;
+    double acc[18];
+#pragma unroll
+    for (int t = 0; t < 18; ++t) acc[t] = 0.0;
+    const int p1 = pair_ptr[k + 1];
+    for (int p = pair_ptr[k]; p < p1; ++p) {
+      const int2 pr = pairs[p];
+      const Real* D = bd_of(pr.x) + half * 9;
+      Real d[9];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) d[t] = D[t];
+      const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)pr.y * 18);
+      Real b[18];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const R2 v = B2[t];
+        b[2 * t] = v.x;
+        b[2 * t + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+          acc[i * 6 + c] += (double)(d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2]);
+    }
+    const int hb = s_hpp[k];
+    const bool dg = rcol[k] == r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const int row = half * 3 + i;
+        const int e = row * 6 + c;
+        double v = -acc[i * 6 + c];
+        if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
+        if (dg && row == c) v += lambda;
+        Sr[(size_t)e * nblk + j] = (Real)v;
+      }
   }
 }
 
-// Reduced right-hand side (block_solver.hpp:366-392, 429-433): one warp per
-// free camera, bs = r_p - sum_a B_a Dinv_l r_l over the camera's Hpl blocks.
+// db_l = Dinv_l r_l
+template <typename Real>
+__global__ void schur_db(const Real* dinv, const double* r_l, int Pf, double* db) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  const Real* D = dinv + (size_t)l * 9;
+  const double* rl = r_l + (size_t)l * 3;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    db[(size_t)l * 3 + i] = (double)D[i * 3] * rl[0] + (double)D[i * 3 + 1] * rl[1] + (double)D[i * 3 + 2] * rl[2];
+}
+
+// Reduced right-hand side for a given (r_p, r_l) (block_solver.hpp:366-392,
+// 429-433): one warp per free camera, bs = r_p - sum_a B_a db_l(a).
 template <typename Real>
 __global__ void schur_rhs(const int* hc_ptr, const int* hc_blk, const int* hpl_col, int Cf, const Real* hpl,
-                          const Real* dinv, const double* r_p, const double* r_l, double* bs) {
+                          const double* db, const double* r_p, double* bs) {
   const int h = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x & 31;
   if (h >= Cf) return;
@@ -314,23 +400,18 @@ __global__ void schur_rhs(const int* hc_ptr, const int* hc_blk, const int* hpl_c
   const int e1 = hc_ptr[h + 1];
   for (int p = hc_ptr[h] + lane; p < e1; p += 32) {
     const int a = hc_blk[p];
-    const int l = hpl_col[a];
-    const Real* D = dinv + (size_t)l * 9;
-    const double* rl = r_l + (size_t)l * 3;
-    double db[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) db[i] = (double)D[i * 3] * rl[0] + (double)D[i * 3 + 1] * rl[1] + (double)D[i * 3 + 2] * rl[2];
+    const double* d = db + (size_t)hpl_col[a] * 3;
     const Real* B = hpl + (size_t)a * 18;
 #pragma unroll
-    for (int r = 0; r < 6; ++r) acc[r] += (double)B[r * 3] * db[0] + (double)B[r * 3 + 1] * db[1] + (double)B[r * 3 + 2] * db[2];
+    for (int q = 0; q < 6; ++q) acc[q] += (double)B[q * 3] * d[0] + (double)B[q * 3 + 1] * d[1] + (double)B[q * 3 + 2] * d[2];
   }
 #pragma unroll
-  for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
+  for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
   if (lane < 6) {
     double v = acc[0];
 #pragma unroll
-    for (int r = 1; r < 6; ++r)
-      if (lane == r) v = acc[r];
+    for (int q = 1; q < 6; ++q)
+      if (lane == q) v = acc[q];
     bs[(size_t)h * 6 + lane] = r_p[(size_t)h * 6 + lane] - v;
   }
 }

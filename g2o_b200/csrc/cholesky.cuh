@@ -33,7 +33,7 @@ struct CholPlan {
   std::vector<int> upd_ptr;          // per k: range into upd
   std::vector<int2> upd;             // trailing pairs (i, j), i >= j > k
   std::vector<int> bwd_ptr, bwd;     // per k: tiles i < k with L(k,i) != 0
-  DBuf<int> d_perm, d_pnl, d_bwd, d_blkcol;
+  DBuf<int> d_perm, d_pnl, d_bwd;
   DBuf<int2> d_upd;
   DBuf<double> A, y;
   DBuf<int> info;
@@ -84,7 +84,7 @@ static void rcm_order(int nb, const std::vector<int32_t>& rc, std::vector<int>& 
 }
 
 static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_t>& rc, bool reorder,
-                           const std::vector<int>& col_of_block, cudaStream_t st) {
+                           cudaStream_t st) {
   P.nb = nb;
   P.bs = bs;
   P.n = nb * bs;
@@ -137,7 +137,6 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
   G2OC_TRY(P.d_pnl.upload(P.pnl.empty() ? std::vector<int>{0} : P.pnl, st));
   G2OC_TRY(P.d_upd.upload(P.upd.empty() ? std::vector<int2>{make_int2(0, 0)} : P.upd, st));
   G2OC_TRY(P.d_bwd.upload(P.bwd.empty() ? std::vector<int>{0} : P.bwd, st));
-  G2OC_TRY(P.d_blkcol.upload(col_of_block, st));
   G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
   G2OC_TRY(P.y.alloc(P.np));
   G2OC_TRY(P.info.alloc(1));
@@ -147,16 +146,17 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
 // dense column-major A(np x np): permuted blocks and their transposes,
 // identity on the padding
 template <typename Real>
-__global__ void chol_densify(SysDev<Real> S, const int* blk_col, int nnzb, int bs, const int* perm, int n, int np,
-                             double* A) {
+__global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int np, double* A) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long per = (long long)bs * bs;
+  const int nnzb = S.nnzb;
   if (t < (long long)nnzb * per) {
     const int p = (int)(t / per), e = (int)(t % per);
-    const int r = S.row[p], c = blk_col[p];
+    const int r = S.brow[p], c = S.rcol[p];
     const int i = e / bs, j = e % bs;
     const int gi = perm[r] * bs + i, gj = perm[c] * bs + j;
-    const double v = (double)S.val[(size_t)p * per + e];
+    const int rb = S.rptr[r], nblk = S.rptr[r + 1] - rb;
+    const double v = (double)S.val[(size_t)rb * per + (size_t)e * nblk + (p - rb)];
     A[(size_t)gj * np + gi] = v;
     A[(size_t)gi * np + gj] = v;
   } else {
@@ -351,22 +351,24 @@ __global__ void chol_bwd_update(const double* A, int np, int k, const int* tiles
 }
 
 template <typename Real>
-static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, int nnzb, const double* rhs, double* xout,
-                      int* ok) {
+static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const double* rhs, double* xout, int* ok,
+                      long long* nlaunch) {
+  const int nnzb = S.nnzb;
+  long long nl = 4;  // densify, load_rhs, store_x, + memsets
   const int np = P.np, nt = P.nt;
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
   G2OC_CUDA_TRY(cudaMemsetAsync(P.A.p, 0, P.A.bytes(), st));
   G2OC_CUDA_TRY(cudaMemsetAsync(P.info.p, 0, sizeof(int), st));
   const long long work = (long long)nnzb * P.bs * P.bs + (np - P.n);
-  chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.d_blkcol.p, nnzb, P.bs, P.d_perm.p, P.n, np,
-                                                                 P.A.p);
+  chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.bs, P.d_perm.p, P.n, np, P.A.p);
   for (int k = 0; k < nt; ++k) {
     chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.info.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k]);
     const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];
     if (nu > 0) chol_gemm<<<nu, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_upd.p + P.upd_ptr[k]);
+    nl += 1 + (np_k > 0) + (nu > 0);
   }
   const cudaError_t e1 = cudaGetLastError();
   if (e1 != cudaSuccess) {
@@ -378,11 +380,13 @@ static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, int n
     chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_fwd_update<<<np_k, kTile, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
+    nl += 1 + (np_k > 0);
   }
   for (int k = nt - 1; k >= 0; --k) {
     chol_bwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
     const int nbk = P.bwd_ptr[k + 1] - P.bwd_ptr[k];
     if (nbk > 0) chol_bwd_update<<<nbk, kTile, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
+    nl += 1 + (nbk > 0);
   }
   chol_store_x<<<(P.n + 255) / 256, 256, 0, st>>>(P.y.p, P.d_perm.p, P.bs, P.n, xout);
   const cudaError_t e2 = cudaGetLastError();
@@ -390,6 +394,7 @@ static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, int n
     set_error("cholesky solve launch: %s", cudaGetErrorString(e2));
     return G2OC_ERR_CUDA;
   }
+  if (nlaunch) *nlaunch += nl - 1;
   int info = 0;
   G2OC_CUDA_TRY(cudaMemcpyAsync(&info, P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));

@@ -54,6 +54,25 @@ struct EngineBase {
   virtual int schur_export(double lambda, double* S, double* bs) = 0;
 };
 
+// kernel identifiers for the launch counters and the optional per-launch
+// CUDA-event timing (g2oc_set_kernel_timing / g2oc_get_kernel_stats)
+enum KernelId {
+  K_CHI2, K_ERRORS, K_JACOBIANS, K_LANDMARK_PASS, K_CAMERA_PASS, K_SCHUR_LANDMARK, K_SCHUR_BLOCKS, K_SCHUR_RHS,
+  K_BACKSUB, K_RESID_CAM, K_RESID_LM, K_OPLUS, K_MAX_DIAG, K_PCG_DIAG_INV, K_PCG_INIT, K_PCG_SPMV, K_PCG_UPDATE,
+  K_PCG_CHECK, K_PG_LINEARIZE, K_PG_ASSEMBLE_H, K_PG_ASSEMBLE_B, K_DAMP, K_LM_CONTROL, K_REDUCE, K_AXPY,
+  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_COUNT
+};
+static const char* kKernelNames[K_COUNT] = {
+  "chi2", "errors", "jacobians", "ba_landmark_pass", "ba_camera_pass", "schur_landmark", "schur_blocks",
+  "schur_rhs", "ba_backsub", "ba_resid_cam", "ba_resid_lm", "oplus", "max_diag", "pcg_diag_inv", "pcg_init",
+  "pcg_spmv", "pcg_update", "pcg_check_dn", "pg_linearize", "pg_assemble_h", "pg_assemble_b", "damp_diag",
+  "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db"};
+
+struct PendingTiming {
+  int kid;
+  cudaEvent_t a, b;
+};
+
 }  // namespace g2oc
 
 struct g2oc_ctx {
@@ -65,32 +84,66 @@ struct g2oc_ctx {
   bool system_built = false;
   double f = 1, cx = 0, cy = 0;
   // vertex state
-  g2oc::DBuf<double> pose, point, pose_bak, point_bak;
+  g2oc::DBuf<double> pose, point, pose_bak, point_bak, pose_init, point_init;
   g2oc::DBuf<int> oplus_count, free_pose, free_point;
   // BA edges
   g2oc::DBuf<int2> e_v, c_v;
   g2oc::DBuf<double2> e_z, c_z;
   g2oc::DBuf<double4> e_om, c_om;
-  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, sp_ptr, s_hpp;
-  g2oc::DBuf<int2> sp_ab;
+  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, s_pair_ptr, s_hpp;
+  g2oc::DBuf<int2> s_pairs;
   // pose-graph edges
   g2oc::DBuf<int2> pe_v;
   g2oc::DBuf<double> pe_zinv, pe_info, pe_delta;
   g2oc::DBuf<uint8_t> pe_trans;
   g2oc::DBuf<int> hb_src_ptr, hb_src, bv_src_ptr, bv_src;
   // linear system lists
-  g2oc::DBuf<int> sys_col_ptr, sys_row, sys_diag, sys_rowu_ptr, sys_rowu_blk, sys_rowu_col;
+  g2oc::DBuf<int> sys_perm, sys_rptr, sys_rcol, sys_brow, sys_diag, sys_cptr, sys_cblk;
   // FP64 vectors
-  g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf;
+  g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
   g2oc::DBuf<g2oc::DevScalars> sc;
   g2oc::DBuf<g2oc::PcgState> pcg;
   g2oc::DBuf<int> flag;  // nonfinite flag
   std::unique_ptr<g2oc::EngineBase> eng;
   std::unique_ptr<g2oc::CholPlan> chol;
   int last_pcg_iterations = 0;
+  double last_schur_s = 0.0;
+  double last_refine_dn = 0.0;
+  long long refine_steps = 0;
+  // launch accounting
+  bool timing = false;
+  long long kcount[g2oc::K_COUNT] = {};
+  double ktime_ms[g2oc::K_COUNT] = {};
+  long long chol_launches = 0;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<g2oc::PendingTiming> pending;
+  cudaEvent_t event() {
+    if (!event_pool.empty()) {
+      cudaEvent_t e = event_pool.back();
+      event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void flush_timing() {
+    if (pending.empty()) return;
+    cudaEventSynchronize(pending.back().b);
+    for (auto& p : pending) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.a, p.b);
+      ktime_ms[p.kid] += ms;
+      event_pool.push_back(p.a);
+      event_pool.push_back(p.b);
+    }
+    pending.clear();
+  }
   ~g2oc_ctx() {
     eng.reset();
     chol.reset();
+    flush_timing();
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
   int vec_size() const { return S.Cf * S.pd + S.Pf * 3; }
@@ -127,36 +180,64 @@ struct g2oc_ctx {
 
 namespace g2oc {
 
+// Counts one kernel launch and, when timing is on, brackets it with CUDA
+// events on the context's stream. Used as `G2OC_K(id) kernel<<<...>>>(...);`
+struct LaunchScope {
+  g2oc_ctx* c;
+  int kid;
+  bool done = false;
+  cudaEvent_t e0 = nullptr;
+  LaunchScope(g2oc_ctx* ctx, int id) : c(ctx), kid(id) {
+    if (c->timing) {
+      e0 = c->event();
+      cudaEventRecord(e0, c->stream);
+    }
+  }
+  ~LaunchScope() {
+    c->kcount[kid]++;
+    if (c->timing) {
+      cudaEvent_t e1 = c->event();
+      cudaEventRecord(e1, c->stream);
+      c->pending.push_back(PendingTiming{kid, e0, e1});
+      if (c->pending.size() > 8192) c->flush_timing();
+    }
+  }
+};
+#define G2OC_K(kid) for (::g2oc::LaunchScope _ls(c, ::g2oc::kid); !_ls.done; _ls.done = true)
+
 // ------------------------------------------------------------ PCG driver
 template <typename Real, int BS>
-static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const Real* minv, const double* rhs, double* xout, Real* r,
-                   Real* s, Real* d0, Real* d1, Real* q, bool relative_only, int* iters) {
+static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs, double* xout,
+                   double* r, double* s, double* d0, double* d1, double* q, double* qrow, double* tbuf,
+                   bool fixed_d0, int* iters) {
   cudaStream_t st = c->stream;
-  PcgState cfg{};
-  // configure the state (keeps residual_carry)
   PcgState host;
   G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-  cfg = host;
+  PcgState cfg = host;  // keeps residual_carry and, for correction solves, d0
   cfg.tolerance = c->prm.pcg_tolerance;
   cfg.max_iter = c->prm.pcg_max_iterations < 0 ? A.nb * BS : c->prm.pcg_max_iterations;
   cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
-  cfg.relative_only = relative_only ? 1 : 0;
+  cfg.fixed_d0 = fixed_d0 ? 1 : 0;
   cfg.counter = 0;
   cfg.done = 0;
   cfg.k = 0;
+  cfg.breakdown = 0;
   G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
   const int nbv = cdiv(A.nb, 128);
-  pcg_init<Real, BS><<<nbv, 128, 0, st>>>(A.nb, rhs, minv, r, s, xout, c->partials.p, c->pcg.p);
+  G2OC_K(K_PCG_INIT) pcg_init<BS><<<nbv, 128, 0, st>>>(A.nb, rhs, minv, r, s, xout, c->partials.p, c->pcg.p);
   G2OC_LAUNCH_CHECK();
-  constexpr int SPMV_T = 256;
-  const int nbs = cdiv(A.nb, SPMV_T / 32);
+  constexpr int WT = 256;
+  const int nbw = cdiv(A.nb, WT / 32);
   int chunk = 4;
   int launched = 0;
   for (;;) {
     for (int k = 0; k < chunk; ++k) {
-      pcg_spmv<Real, BS, SPMV_T><<<nbs, SPMV_T, 0, st>>>(A, s, d0, d1, q, c->partials.p, c->pcg.p);
-      pcg_update<Real, BS><<<nbv, 128, 0, st>>>(A.nb, minv, d0, d1, q, r, s, xout, c->partials.p, c->pcg.p);
+      G2OC_K(K_PCG_SPMV) pcg_rowpass<Real, BS, WT><<<nbw, WT, 0, st>>>(A, s, d0, d1, qrow, tbuf, c->pcg.p);
+      G2OC_K(K_PCG_COLPASS) pcg_colpass<Real, BS, WT><<<nbw, WT, 0, st>>>(A, d0, d1, qrow, tbuf, q, c->partials.p,
+                                                                          c->pcg.p);
+      G2OC_K(K_PCG_UPDATE) pcg_update<BS><<<nbv, 128, 0, st>>>(A.nb, minv, d0, d1, q, r, s, xout, c->partials.p,
+                                                               c->pcg.p);
     }
     G2OC_LAUNCH_CHECK();
     launched += chunk;
@@ -174,18 +255,41 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const Real* minv, const d
 }
 
 static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, double* out1, double add0 = 0.0) {
-  finalize_sum_kernel<<<1, 256, 0, c->stream>>>(c->partials.p, nparts, stride, out0, out1, add0);
+  G2OC_K(K_REDUCE) finalize_sum_kernel<<<1, 256, 0, c->stream>>>(c->partials.p, nparts, stride, out0, out1, add0);
   G2OC_LAUNCH_CHECK();
   return G2OC_OK;
 }
+
+struct PhaseTimer {
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  explicit PhaseTimer(cudaStream_t s) : st(s) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  ~PhaseTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start() { cudaEventRecord(a, st); }
+  double stop() {
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3;
+  }
+};
 
 // ---------------------------------------------------------- the engine
 template <typename Real>
 struct Engine final : EngineBase {
   g2oc_ctx* c;
   // Hessian
-  DBuf<Real> hpp, hll, hpl, bd, dinv, Sval, sysval, minv;
-  DBuf<Real> r, s, d0, d1, q;
+  DBuf<Real> hpp, hll, hpl, bd, dinv, Sval, sysval;
+  DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf;
+  bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
+  size_t schur_smem = 0;
   DBuf<Real> hcontrib;
   DBuf<double> bcontrib;
   explicit Engine(g2oc_ctx* ctx) : c(ctx) {}
@@ -197,33 +301,39 @@ struct Engine final : EngineBase {
     if (S.ba) {
       G2OC_TRY(hll.alloc((size_t)S.Pf * 6 + 1));
       G2OC_TRY(hpl.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
-      G2OC_TRY(bd.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
       G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
       G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
+      schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
+      stage_in_smem = schur_smem <= 200 * 1024;
+      if (!stage_in_smem) G2OC_TRY(bd.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
+      G2OC_TRY(c->db.alloc((size_t)S.Pf * 3 + 1));
     } else {
       G2OC_TRY(hcontrib.alloc((size_t)S.act.size() * 3 * pd * pd));
       G2OC_TRY(bcontrib.alloc((size_t)S.act.size() * 2 * pd));
     }
     if (!(S.ba && S.schur)) G2OC_TRY(sysval.alloc((size_t)S.sys_nnzb * pd * pd + 1));
     const size_t n = (size_t)S.Cf * pd;
-    G2OC_TRY(minv.alloc((size_t)S.Cf * pd * pd));
-    G2OC_TRY(r.alloc(n));
-    G2OC_TRY(s.alloc(n));
-    G2OC_TRY(d0.alloc(n));
-    G2OC_TRY(d1.alloc(n));
-    G2OC_TRY(q.alloc(n));
+    G2OC_TRY(minv.alloc((size_t)S.Cf * pd * pd + 1));
+    G2OC_TRY(r.alloc(n + 1));
+    G2OC_TRY(s.alloc(n + 1));
+    G2OC_TRY(d0.alloc(n + 1));
+    G2OC_TRY(d1.alloc(n + 1));
+    G2OC_TRY(q.alloc(n + 1));
+    G2OC_TRY(qrow.alloc(n + 1));
+    G2OC_TRY(tbuf.alloc((size_t)S.sys_nnzb * pd + 1));
     return G2OC_OK;
   }
 
   SysDev<Real> sys(const Real* val) {
     SysDev<Real> A;
     A.nb = c->S.sys_nb;
-    A.col_ptr = c->sys_col_ptr.p;
-    A.row = c->sys_row.p;
+    A.nnzb = c->S.sys_nnzb;
+    A.rptr = c->sys_rptr.p;
+    A.rcol = c->sys_rcol.p;
+    A.brow = c->sys_brow.p;
     A.diag = c->sys_diag.p;
-    A.rowu_ptr = c->sys_rowu_ptr.p;
-    A.rowu_blk = c->sys_rowu_blk.p;
-    A.rowu_col = c->sys_rowu_col.p;
+    A.cptr = c->sys_cptr.p;
+    A.cblk = c->sys_cblk.p;
     A.val = val;
     return A;
   }
@@ -233,34 +343,34 @@ struct Engine final : EngineBase {
     cudaStream_t st = c->stream;
     if (S.ba) {
       if (S.Pf > 0) {
-        ba_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf,
+        G2OC_K(K_LANDMARK_PASS) ba_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf,
                                                                  hll.p, hpl.p, c->b.p + (size_t)S.Cf * 6);
         G2OC_LAUNCH_CHECK();
       }
       if (S.Cf > 0) {
         BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
-        ba_camera_pass<Real, 128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), hpp.p, c->b.p);
+        G2OC_K(K_CAMERA_PASS) ba_camera_pass<Real, 128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), hpp.p, c->b.p);
         G2OC_LAUNCH_CHECK();
       }
     } else {
       const int n = (int)S.act.size();
       if (S.pose_type == G2OC_POSE_SE2) {
-        pg_linearize<Real, G2OC_POSE_SE2><<<cdiv(n, 128), 128, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
+        G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE2><<<cdiv(n, 128), 128, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
                                                                         hcontrib.p, bcontrib.p);
         G2OC_LAUNCH_CHECK();
         const int nnzb = (int)S.hpp_rc.size() / 2;
-        pg_assemble_h<Real, 3><<<cdiv((long long)nnzb * 3, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
+        G2OC_K(K_PG_ASSEMBLE_H) pg_assemble_h<Real, 3><<<cdiv((long long)nnzb * 3, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
                                                                                hcontrib.p, hpp.p);
-        pg_assemble_b<3><<<cdiv((long long)S.Cf * 3, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
+        G2OC_K(K_PG_ASSEMBLE_B) pg_assemble_b<3><<<cdiv((long long)S.Cf * 3, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
                                                                        bcontrib.p, c->b.p);
       } else {
-        pg_linearize<Real, G2OC_POSE_SE3><<<cdiv(n, 64), 64, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
+        G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE3><<<cdiv(n, 64), 64, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
                                                                       hcontrib.p, bcontrib.p);
         G2OC_LAUNCH_CHECK();
         const int nnzb = (int)S.hpp_rc.size() / 2;
-        pg_assemble_h<Real, 6><<<cdiv((long long)nnzb * 6, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
+        G2OC_K(K_PG_ASSEMBLE_H) pg_assemble_h<Real, 6><<<cdiv((long long)nnzb * 6, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
                                                                                hcontrib.p, hpp.p);
-        pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
+        G2OC_K(K_PG_ASSEMBLE_B) pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
                                                                        bcontrib.p, c->b.p);
       }
       G2OC_LAUNCH_CHECK();
@@ -271,64 +381,84 @@ struct Engine final : EngineBase {
   int max_diag() override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    if (S.ba) ba_max_diag<Real><<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
-    else if (S.pd == 3) pg_max_diag<Real, 3><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
-    else pg_max_diag<Real, 6><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
+    if (S.ba) G2OC_K(K_MAX_DIAG) ba_max_diag<Real><<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
+    else if (S.pd == 3) G2OC_K(K_MAX_DIAG) pg_max_diag<Real, 3><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
+    else G2OC_K(K_MAX_DIAG) pg_max_diag<Real, 6><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
     G2OC_LAUNCH_CHECK();
-    finalize_max_kernel<<<1, 256, 0, st>>>(c->partials.p, kRedBlocks, &c->sc.p->max_diag);
+    G2OC_K(K_REDUCE) finalize_max_kernel<<<1, 256, 0, st>>>(c->partials.p, kRedBlocks, &c->sc.p->max_diag);
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
-  // S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T, with Dinv and BD
-  int schur(double lambda) {
+  // S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T (internal row order) and,
+  // when bs != nullptr, the reduced right-hand side of b
+  int schur(double lambda, double* bs) {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (S.Pf > 0) {
-      schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
-                                                             c->flag.p);
+      G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
+          hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, stage_in_smem ? nullptr : bd.p, c->flag.p);
       G2OC_LAUNCH_CHECK();
     }
-    const int nnzS = (int)S.schur_rc.size() / 2;
-    if (nnzS == 0) return G2OC_OK;
-    schur_blocks<Real><<<cdiv((long long)nnzS * 6, 192), 192, 0, st>>>(c->sp_ptr.p, c->sp_ab.p, c->s_hpp.p, nnzS,
-                                                                      hpp.p, bd.p, hpl.p, lambda, Sval.p);
+    if (S.Cf == 0) return G2OC_OK;
+    constexpr int T = 512;
+    const double* bp = c->b.p;
+    const double* bl = c->b.p + (size_t)S.Cf * 6;
+    if (stage_in_smem) {
+      auto kern = schur_rows<Real, true, T>;
+      G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+      G2OC_K(K_SCHUR_BLOCKS) kern<<<S.Cf, T, schur_smem, st>>>(
+          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, nullptr, c->sys_rptr.p, c->sys_rcol.p,
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
+    } else {
+      G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, false, T><<<S.Cf, T, 0, st>>>(
+          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bd.p, c->sys_rptr.p, c->sys_rcol.p,
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
+    }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
   int schur_rhs_from(const double* rp, const double* rl, double* bs) {
     const Structure& S = c->S;
-    schur_rhs<Real><<<cdiv(S.Cf, 4), 128, 0, c->stream>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p,
-                                                          dinv.p, rp, rl, bs);
+    if (S.Pf > 0) {
+      G2OC_K(K_SCHUR_DB) schur_db<Real><<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(dinv.p, rl, S.Pf, c->db.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    G2OC_K(K_SCHUR_RHS) schur_rhs<Real><<<cdiv(S.Cf, 4), 128, 0, c->stream>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p,
+                                                                             S.Cf, hpl.p, c->db.p, rp, bs);
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
-  int pcg_solve(const Real* val, const double* rhs, double* xout, bool relative_only, int* iters) {
+  // fixed_d0: a correction solve of the refinement, stopping at the d0 of
+  // the first solve (which set the preconditioner)
+  int pcg_solve(const Real* val, const double* rhs, double* xout, bool fixed_d0, int* iters) {
     const Structure& S = c->S;
     SysDev<Real> A = sys(val);
     if (S.pd == 6) {
-      pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
-      G2OC_LAUNCH_CHECK();
-      return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, relative_only, iters);
+      if (!fixed_d0) {
+        G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+        G2OC_LAUNCH_CHECK();
+      }
+      return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
     }
-    pcg_diag_inv<Real, 3><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
-    G2OC_LAUNCH_CHECK();
-    return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, relative_only, iters);
+    if (!fixed_d0) {
+      G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 3><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
   }
 
   int chol_solve(const Real* val, const double* rhs, double* xout, int* ok) {
     const Structure& S = c->S;
     if (!c->chol) {
-      const std::vector<int32_t>& rc = S.ba ? S.schur_rc : S.hpp_rc;
-      std::vector<int> col(rc.size() / 2);
-      for (size_t k = 0; k < col.size(); ++k) col[k] = rc[2 * k + 1];
+      const std::vector<int32_t>& rc = S.ba && S.schur ? S.schur_rc : S.hpp_rc;
       std::unique_ptr<CholPlan> P(new CholPlan());
-      G2OC_TRY(chol_plan_build(*P, S.sys_nb, S.pd, rc, !S.ba, col, c->stream));
+      G2OC_TRY(chol_plan_build(*P, S.sys_nb, S.pd, rc, !S.ba, c->stream));
       c->chol = std::move(P);
     }
-    return g2oc::chol_solve<Real>(*c->chol, c->stream, sys(val), S.sys_nnzb, rhs, xout, ok);
+    return g2oc::chol_solve<Real>(*c->chol, c->stream, sys(val), rhs, xout, ok, &c->kcount[K_CHOLESKY]);
   }
 
   int solve(double lambda, int* pcg_iters) override {
@@ -343,59 +473,75 @@ struct Engine final : EngineBase {
       G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, c->x.bytes(), st));
       if (S.ba && S.Pf > 0) {
         if (S.schur) {
-          schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
+          G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
                                                                  c->flag.p);
-          ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, c->b.p,
+          G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, c->b.p,
                                                              c->xs.p, c->x.p);
           G2OC_LAUNCH_CHECK();
         }
       }
     } else if (S.ba && S.schur) {
-      G2OC_TRY(schur(lambda));
+      PhaseTimer tm(st);
+      tm.start();
+      G2OC_TRY(schur(lambda, c->rhs.p));
       const double* bp = c->b.p;
       const double* bl = c->b.p + (size_t)S.Cf * 6;
-      G2OC_TRY(schur_rhs_from(bp, bl, c->rhs.p));
+      c->last_schur_s = tm.stop();
       if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
       else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false, &it));
       it_total += it;
       G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
       if (S.Pf > 0) {
-        ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, bl, c->xs.p,
+        G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, bl, c->xs.p,
                                                            c->x.p + (size_t)S.Cf * 6);
         G2OC_LAUNCH_CHECK();
       }
-      // mixed precision: iterative refinement on the FP64 residual of the full damped system
-      if (sizeof(Real) == 4 && ok) {
+      // mixed precision: FP64 iterative refinement on the true residual of
+      // the damped full system, r = b - (H + lambda I) x. A correction is
+      // solved only while the reduced residual's M-norm is above the d0 the
+      // first solve stopped at, i.e. while the FP32 storage of H / S / Dinv,
+      // not the PCG tolerance, limits the step.
+      if (sizeof(Real) == 4 && ok && !use_chol) {
         const int n = c->vec_size();
         for (int k = 0; k < c->prm.refine_max_iterations; ++k) {
           double* rp = c->resid.p;
           double* rl = c->resid.p + (size_t)S.Cf * 6;
-          ba_resid_cam<Real><<<cdiv(S.Cf, 4), 128, 0, st>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p, hpp.p,
+          G2OC_K(K_RESID_CAM) ba_resid_cam<Real><<<cdiv(S.Cf, 4), 128, 0, st>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p, hpp.p,
                                                             lambda, bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
           if (S.Pf > 0)
-            ba_resid_lm<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, hll.p, lambda, bl,
+            G2OC_K(K_RESID_LM) ba_resid_lm<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, hll.p, lambda, bl,
                                                                c->x.p, c->x.p + (size_t)S.Cf * 6, rl);
           G2OC_LAUNCH_CHECK();
           G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
-          if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
-          else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true, &it));
+          G2OC_K(K_PCG_CHECK) pcg_check_dn<6><<<cdiv(S.Cf, 128), 128, 0, st>>>(S.Cf, minv.p, c->rhs.p, c->partials.p, c->pcg.p);
+          G2OC_LAUNCH_CHECK();
+          PcgState ps;
+          G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+          G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+          c->last_refine_dn = ps.check_dn;
+          if (!(ps.check_dn > ps.d0)) break;
+          G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true, &it));
           it_total += it;
+          c->refine_steps++;
           G2OC_CUDA_TRY(cudaMemcpyAsync(c->dx.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
           if (S.Pf > 0) {
-            ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, rl,
+            G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, rl,
                                                                c->xs.p, c->dx.p + (size_t)S.Cf * 6);
             G2OC_LAUNCH_CHECK();
           }
-          axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, n);
+          G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, n);
           G2OC_LAUNCH_CHECK();
         }
       }
     } else {
       const int nnzb = S.sys_nnzb;
-      G2OC_CUDA_TRY(cudaMemcpyAsync(sysval.p, hpp.p, (size_t)nnzb * S.pd * S.pd * sizeof(Real),
-                                    cudaMemcpyDeviceToDevice, st));
-      if (S.pd == 3) damp_diag<Real, 3><<<cdiv(S.Cf * 3, 128), 128, 0, st>>>(c->sys_diag.p, S.Cf, lambda, sysval.p);
-      else damp_diag<Real, 6><<<cdiv(S.Cf * 6, 128), 128, 0, st>>>(c->sys_diag.p, S.Cf, lambda, sysval.p);
+      const long long nel = (long long)nnzb * S.pd * S.pd;
+      if (S.pd == 3)
+        G2OC_K(K_DAMP) sys_gather_damped<Real, 3><<<cdiv(nel, 256), 256, 0, st>>>(
+            hpp.p, c->sys_perm.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, nnzb, lambda, sysval.p);
+      else
+        G2OC_K(K_DAMP) sys_gather_damped<Real, 6><<<cdiv(nel, 256), 256, 0, st>>>(
+            hpp.p, c->sys_perm.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, nnzb, lambda, sysval.p);
       G2OC_LAUNCH_CHECK();
       if (use_chol) G2OC_TRY(chol_solve(sysval.p, c->b.p, c->x.p, &ok));
       else G2OC_TRY(pcg_solve(sysval.p, c->b.p, c->x.p, false, &it));
@@ -448,13 +594,16 @@ struct Engine final : EngineBase {
       set_error("the graph has no Schur complement (no marginalized vertices)");
       return G2OC_ERR_NOT_SUPPORTED;
     }
-    G2OC_TRY(schur(lambda));
-    G2OC_TRY(schur_rhs_from(c->b.p, c->b.p + (size_t)S.Cf * 6, c->rhs.p));
+    G2OC_TRY(schur(lambda, c->rhs.p));
     G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (S_out) {
-      std::vector<Real> h(S.schur_rc.size() / 2 * 36);
+      std::vector<Real> h((size_t)S.sys_nnzb * 36);
       G2OC_CUDA_TRY(cudaMemcpy(h.data(), Sval.p, h.size() * sizeof(Real), cudaMemcpyDeviceToHost));
-      to_double(h, S_out);
+      for (int k = 0; k < S.sys_nnzb; ++k) {
+        const int r = S.sys_brow[k], rb = S.sys_rptr[r], nblk = S.sys_rptr[r + 1] - rb;
+        for (int e = 0; e < 36; ++e)
+          S_out[(size_t)S.sys_perm[k] * 36 + e] = (double)h[sys_offset<6>(rb, nblk, k - rb, e)];
+      }
     }
     if (bs_out) G2OC_CUDA_TRY(cudaMemcpy(bs_out, c->rhs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToHost));
     return G2OC_OK;
@@ -465,10 +614,10 @@ struct Engine final : EngineBase {
 static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba) ba_chi2_kernel<<<kRedBlocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kRedBlocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE2)
-    pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
-  else pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
+    G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
+  else G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   G2OC_LAUNCH_CHECK();
   return finalize_sum(c, kRedBlocks, 2, out_plain, out_robust);
 }
@@ -476,11 +625,11 @@ static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
 static int oplus(g2oc_ctx* c) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba) ba_oplus<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
+  if (S.ba) G2OC_K(K_OPLUS) ba_oplus<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
   else if (S.pose_type == G2OC_POSE_SE2)
-    pg_oplus<G2OC_POSE_SE2><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
+    G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE2><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
                                                              c->oplus_count.p, c->flag.p);
-  else pg_oplus<G2OC_POSE_SE3><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
+  else G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE3><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
                                                                 c->oplus_count.p, c->flag.p);
   G2OC_LAUNCH_CHECK();
   return G2OC_OK;
@@ -500,27 +649,6 @@ static int pop(g2oc_ctx* c) {
   return G2OC_OK;
 }
 
-struct PhaseTimer {
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  explicit PhaseTimer(cudaStream_t s) : st(s) {
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-  }
-  ~PhaseTimer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-  void start() { cudaEventRecord(a, st); }
-  double stop() {
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    return ms * 1e-3;
-  }
-};
-
 // OptimizationAlgorithmLevenberg::solve (optimization_algorithm_levenberg.cpp:60-153)
 static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
   cudaStream_t st = c->stream;
@@ -535,7 +663,7 @@ static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
   stv->time_quadratic_form = tm.stop();
   if (iteration == 0) {
     G2OC_TRY(c->eng->max_diag());
-    lm_init_lambda<<<1, 32, 0, st>>>(sc, c->prm.initial_lambda, c->prm.tau);
+    G2OC_K(K_LM_CONTROL) lm_init_lambda<<<1, 32, 0, st>>>(sc, c->prm.initial_lambda, c->prm.tau);
     G2OC_LAUNCH_CHECK();
   }
   const int n = c->vec_size();
@@ -549,17 +677,20 @@ static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
     G2OC_CUDA_TRY(cudaStreamSynchronize(st));
     tm.start();
     int pcg_it = 0;
+    c->last_schur_s = 0.0;
     G2OC_TRY(c->eng->solve(cur.lambda, &pcg_it));
-    stv->time_linear_solver += tm.stop();
+    const double tsolve = tm.stop();
+    stv->time_schur_complement += c->last_schur_s;
+    stv->time_linear_solver += tsolve - c->last_schur_s;
     stv->iterations_linear_solver += pcg_it;
     tm.start();
     G2OC_TRY(oplus(c));
     stv->time_update += tm.stop();
     G2OC_TRY(chi2_to(c, nullptr, &sc->chi2_temp));
-    lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p);
+    G2OC_K(K_LM_CONTROL) lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p);
     G2OC_LAUNCH_CHECK();
     G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &sc->scale, nullptr, 1e-3));
-    lm_decide<<<1, 32, 0, st>>>(sc);
+    G2OC_K(K_LM_CONTROL) lm_decide<<<1, 32, 0, st>>>(sc);
     G2OC_LAUNCH_CHECK();
     G2OC_CUDA_TRY(cudaMemcpyAsync(&h, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
     G2OC_CUDA_TRY(cudaStreamSynchronize(st));
@@ -594,8 +725,11 @@ static int gn_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
   stv->time_quadratic_form = tm.stop();
   tm.start();
   int it = 0;
+  c->last_schur_s = 0.0;
   G2OC_TRY(c->eng->solve(0.0, &it));
-  stv->time_linear_solver = tm.stop();
+  const double tsolve = tm.stop();
+  stv->time_schur_complement = c->last_schur_s;
+  stv->time_linear_solver = tsolve - c->last_schur_s;
   stv->iterations_linear_solver = it;
   tm.start();
   G2OC_TRY(oplus(c));
@@ -657,7 +791,7 @@ void g2oc_default_params(g2oc_params* p) {
   p->max_trials_after_failure = 10;
   p->initial_lambda = 0.0;
   p->tau = 1e-5;
-  p->refine_max_iterations = 1;
+  p->refine_max_iterations = 2;
   p->refine_tolerance = 1e-10;
 }
 
@@ -821,6 +955,12 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     c->point_bak.release();
   }
   G2OC_TRY(c->pose_bak.alloc(c->pose.n));
+  G2OC_TRY(c->pose_init.alloc(c->pose.n));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose_init.p, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, st));
+  if (c->point.n) {
+    G2OC_TRY(c->point_init.alloc(c->point.n));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point_init.p, c->point.p, c->point.bytes(), cudaMemcpyDeviceToDevice, st));
+  }
   G2OC_TRY(c->oplus_count.alloc(S.C));
   G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, S.C * sizeof(int), st));
   G2OC_TRY(c->free_pose.upload(S.free_pose_of_h, st));
@@ -861,10 +1001,10 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->hpl_col.upload(hcl, st));
     G2OC_TRY(c->hc_ptr.upload(S.hc_ptr, st));
     G2OC_TRY(c->hc_blk.upload(S.hc_blk, st));
-    G2OC_TRY(c->sp_ptr.upload(S.sp_ptr, st));
-    std::vector<int2> ab(S.sp_ab.size() / 2);
-    for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.sp_ab[2 * i], S.sp_ab[2 * i + 1]);
-    G2OC_TRY(c->sp_ab.upload(ab, st));
+    G2OC_TRY(c->s_pair_ptr.upload(S.s_pair_ptr, st));
+    std::vector<int2> ab(S.s_pairs.size() / 2);
+    for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.s_pairs[2 * i], S.s_pairs[2 * i + 1]);
+    G2OC_TRY(c->s_pairs.upload(ab, st));
     G2OC_TRY(c->s_hpp.upload(S.s_hpp, st));
   } else {
     const int D = S.D, ZD = S.md;
@@ -887,12 +1027,13 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->bv_src_ptr.upload(S.bv_src_ptr, st));
     G2OC_TRY(c->bv_src.upload(S.bv_src, st));
   }
-  G2OC_TRY(c->sys_col_ptr.upload(S.sys_col_ptr, st));
-  G2OC_TRY(c->sys_row.upload(S.sys_row, st));
+  G2OC_TRY(c->sys_perm.upload(S.sys_perm, st));
+  G2OC_TRY(c->sys_rptr.upload(S.sys_rptr, st));
+  G2OC_TRY(c->sys_rcol.upload(S.sys_rcol, st));
+  G2OC_TRY(c->sys_brow.upload(S.sys_brow, st));
   G2OC_TRY(c->sys_diag.upload(S.sys_diag, st));
-  G2OC_TRY(c->sys_rowu_ptr.upload(S.sys_rowu_ptr, st));
-  G2OC_TRY(c->sys_rowu_blk.upload(S.sys_rowu_blk, st));
-  G2OC_TRY(c->sys_rowu_col.upload(S.sys_rowu_col, st));
+  G2OC_TRY(c->sys_cptr.upload(S.sys_cptr, st));
+  G2OC_TRY(c->sys_cblk.upload(S.sys_cblk, st));
   const int n = c->vec_size();
   G2OC_TRY(c->b.alloc(n));
   G2OC_TRY(c->x.alloc(n));
@@ -1034,10 +1175,10 @@ int g2oc_errors(g2oc_ctx* c, double* out) {
   if (!out) return G2OC_ERR_INVALID_ARGUMENT;
   const Structure& S = c->S;
   const int na = (int)S.act.size();
-  if (S.ba) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
+  if (S.ba) G2OC_K(K_ERRORS) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
   else if (S.pose_type == G2OC_POSE_SE2)
-    pg_errors_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
-  else pg_errors_kernel<G2OC_POSE_SE3><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
+    G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
+  else G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE3><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
   G2OC_LAUNCH_CHECK();
   std::vector<double> h((size_t)na * S.D);
   G2OC_CUDA_TRY(cudaMemcpyAsync(h.data(), c->errbuf.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1056,10 +1197,10 @@ int g2oc_jacobians(g2oc_ctx* c, double* j0, double* j1) {
   DBuf<double> a, b;
   G2OC_TRY(a.alloc((size_t)na * D * d0));
   G2OC_TRY(b.alloc((size_t)na * D * d1));
-  if (S.ba) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
+  if (S.ba) G2OC_K(K_JACOBIANS) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
   else if (S.pose_type == G2OC_POSE_SE2)
-    pg_jacobians_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
-  else pg_jacobians_kernel<G2OC_POSE_SE3><<<cdiv(na, 64), 64, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
+    G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
+  else G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE3><<<cdiv(na, 64), 64, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
   G2OC_LAUNCH_CHECK();
   std::vector<double> ha(a.n), hb(b.n);
   G2OC_CUDA_TRY(cudaMemcpyAsync(ha.data(), a.p, a.bytes(), cudaMemcpyDeviceToHost, c->stream));
@@ -1152,7 +1293,7 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
       return G2OC_ERR_INVALID_ARGUMENT;
     }
   }
-  // a temporary context-local system: reuse the structure lists of a scratch Structure
+  // the system in the internal (row-major upper) order
   Structure tmp;
   build_sym_lists(nb, rcv, tmp);
   for (int i = 0; i < nb; ++i)
@@ -1160,27 +1301,32 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
       set_error("diagonal block %d missing", i);
       return G2OC_ERR_INVALID_ARGUMENT;
     }
+  const size_t per = (size_t)bs * bs;
+  std::vector<double> vint((size_t)nnzb * per);
+  for (int k = 0; k < nnzb; ++k) {
+    const int r = tmp.sys_brow[k], rb = tmp.sys_rptr[r], nblk = tmp.sys_rptr[r + 1] - rb;
+    for (size_t e = 0; e < per; ++e)
+      vint[(size_t)rb * per + e * nblk + (k - rb)] = values[(size_t)tmp.sys_perm[k] * per + e];
+  }
   cudaStream_t st = c->stream;
-  DBuf<int> cp, rw, dg, rup, rub, ruc;
-  DBuf<double> val, rhs, xo, mi, r, s, d0, d1, q;
-  G2OC_TRY(cp.upload(tmp.sys_col_ptr, st));
-  G2OC_TRY(rw.upload(tmp.sys_row, st));
+  DBuf<int> rp, rcl, brw, dg, cp, cb;
+  DBuf<double> val, rhs, xo, mi, r, s, d0, d1, q, qrow, tb;
+  G2OC_TRY(rp.upload(tmp.sys_rptr, st));
+  G2OC_TRY(rcl.upload(tmp.sys_rcol, st));
+  G2OC_TRY(brw.upload(tmp.sys_brow, st));
   G2OC_TRY(dg.upload(tmp.sys_diag, st));
-  G2OC_TRY(rup.upload(tmp.sys_rowu_ptr, st));
-  G2OC_TRY(rub.upload(tmp.sys_rowu_blk, st));
-  G2OC_TRY(ruc.upload(tmp.sys_rowu_col, st));
-  G2OC_TRY(val.upload(std::vector<double>(values, values + (size_t)nnzb * bs * bs), st));
+  G2OC_TRY(cp.upload(tmp.sys_cptr, st));
+  G2OC_TRY(cb.upload(tmp.sys_cblk.empty() ? std::vector<int>{0} : tmp.sys_cblk, st));
+  G2OC_TRY(val.upload(vint, st));
   const int n = nb * bs;
   G2OC_TRY(rhs.upload(std::vector<double>(b, b + n), st));
   G2OC_TRY(xo.alloc(n));
-  SysDev<double> A{nb, cp.p, rw.p, dg.p, rup.p, rub.p, ruc.p, val.p};
+  SysDev<double> A{nb, nnzb, rp.p, rcl.p, brw.p, dg.p, cp.p, cb.p, val.p};
   int it = 0, ok = 1;
   if (linear_solver == G2OC_LINEAR_CHOLESKY) {
     CholPlan P;
-    std::vector<int> col(nnzb);
-    for (int k = 0; k < nnzb; ++k) col[k] = rc[2 * k + 1];
-    G2OC_TRY(chol_plan_build(P, nb, bs, rcv, true, col, st));
-    G2OC_TRY(chol_solve<double>(P, st, A, nnzb, rhs.p, xo.p, &ok));
+    G2OC_TRY(chol_plan_build(P, nb, bs, rcv, true, st));
+    G2OC_TRY(chol_solve<double>(P, st, A, rhs.p, xo.p, &ok, &c->kcount[K_CHOLESKY]));
   } else {
     G2OC_TRY(mi.alloc((size_t)nb * bs * bs));
     G2OC_TRY(r.alloc(n));
@@ -1188,13 +1334,15 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
     G2OC_TRY(d0.alloc(n));
     G2OC_TRY(d1.alloc(n));
     G2OC_TRY(q.alloc(n));
+    G2OC_TRY(qrow.alloc(n));
+    G2OC_TRY(tb.alloc((size_t)nnzb * bs));
     G2OC_TRY(reset_pcg(c));
     if (bs == 3) {
-      pcg_diag_inv<double, 3><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
-      G2OC_TRY((run_pcg<double, 3>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, false, &it)));
+      G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<double, 3><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
+      G2OC_TRY((run_pcg<double, 3>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tb.p, false, &it)));
     } else {
-      pcg_diag_inv<double, 6><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
-      G2OC_TRY((run_pcg<double, 6>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, false, &it)));
+      G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<double, 6><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);
+      G2OC_TRY((run_pcg<double, 6>(c, A, mi.p, rhs.p, xo.p, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tb.p, false, &it)));
     }
   }
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1203,4 +1351,60 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
   return ok ? G2OC_OK : G2OC_ERR_NOT_PD;
 }
 
+int g2oc_get_stream(g2oc_ctx* c, void** stream) {
+  G2OC_TRY(check_ctx(c, false));
+  if (!stream) {
+    set_error("stream is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  *stream = (void*)c->stream;
+  return G2OC_OK;
+}
+
+int g2oc_restore_initial_estimates(g2oc_ctx* c) {
+  G2OC_TRY(check_ctx(c, true));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, c->pose_init.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  if (c->point.n)
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point.p, c->point_init.p, c->point.bytes(), cudaMemcpyDeviceToDevice, c->stream));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, c->oplus_count.bytes(), c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->system_built = false;
+  return G2OC_OK;
+}
+
+int g2oc_set_kernel_timing(g2oc_ctx* c, int enable) {
+  G2OC_TRY(check_ctx(c, false));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->flush_timing();
+  for (int k = 0; k < K_COUNT; ++k) {
+    c->kcount[k] = 0;
+    c->ktime_ms[k] = 0.0;
+  }
+  c->timing = enable != 0;
+  return G2OC_OK;
+}
+
+int g2oc_get_kernel_stats(g2oc_ctx* c, g2oc_kernel_stat* out, int capacity, int* count, int64_t* total) {
+  G2OC_TRY(check_ctx(c, false));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->flush_timing();
+  int n = 0;
+  long long t = 0;
+  for (int k = 0; k < K_COUNT; ++k) {
+    t += c->kcount[k];
+    if (c->kcount[k] == 0) continue;
+    if (out && n < capacity) {
+      memset(out[n].name, 0, sizeof(out[n].name));
+      strncpy(out[n].name, kKernelNames[k], sizeof(out[n].name) - 1);
+      out[n].launches = c->kcount[k];
+      out[n].total_ms = c->ktime_ms[k];
+    }
+    ++n;
+  }
+  if (count) *count = n;
+  if (total) *total = t;
+  return G2OC_OK;
+}
+
 }  // extern "C"
+

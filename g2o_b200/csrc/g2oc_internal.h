@@ -96,9 +96,14 @@ struct Structure {
   std::vector<int> c_ptr;               // Cf + 1, camera-major range of free camera h
   std::vector<int> c_edge;              // camera-major -> device edge
   std::vector<int> hc_ptr, hc_blk;      // Cf + 1 / hpl_nnzb: Hpl blocks by camera row
-  std::vector<int> s_hpp;               // per Schur block: Hpp block or -1
-  std::vector<int> sp_ptr;              // nnzS + 1: pair range per Schur block
-  std::vector<int32_t> sp_ab;           // 2 per pair: (Hpl block a, Hpl block b), row(a) <= row(b)
+  std::vector<int> hc_pos;              // per Hpl block: position in its camera's list
+  int max_blocks_per_cam = 0;
+  // Schur pairs per Schur block in the internal (row-major) order: the
+  // co-observing (a, b) pairs of BD_a B_b^T, a as a position in row r's
+  // camera list, b as an Hpl block, in landmark order
+  std::vector<int> s_pair_ptr;          // nnzS + 1
+  std::vector<int32_t> s_pairs;         // 2 per pair
+  std::vector<int> s_hpp;               // per internal Schur block: Hpp block or -1
   int64_t num_pairs = 0;
 
   // ---- pose graphs (EdgeSE2 / EdgeSE3): device edge order = active order
@@ -107,17 +112,21 @@ struct Structure {
   std::vector<int> hb_src_ptr, hb_src;  // per Hpp block: contributions, encoded edge*3 + slot
   std::vector<int> bv_src_ptr, bv_src;  // per free pose: contributions, encoded edge*2 + which
 
-  // ---- the linear system matrix (S for BA, Hpp for pose graphs) as a block
-  // symmetric matrix in column-major upper storage
+  // ---- the linear system matrix (S for BA, Hpp for pose graphs): upper
+  // blocks stored row by row (internal order, diagonal first in each row);
+  // sys_perm maps an internal block to its index in the column-major pattern
   int sys_nb = 0, sys_nnzb = 0;
-  std::vector<int> sys_col_ptr;         // nb + 1, column-major ranges (diagonal last)
-  std::vector<int> sys_row;             // per block
-  std::vector<int> sys_diag;            // per row: block index of the diagonal
-  std::vector<int> sys_rowu_ptr, sys_rowu_blk, sys_rowu_col;  // strictly-upper blocks listed by row
+  std::vector<int> sys_perm;            // internal -> column-major pattern index
+  std::vector<int> sys_rptr;            // nb + 1
+  std::vector<int> sys_rcol;            // per internal block: column
+  std::vector<int> sys_brow;            // per internal block: row
+  std::vector<int> sys_diag;            // per row: internal index of the diagonal
+  std::vector<int> sys_cptr, sys_cblk;  // strictly-upper blocks by column, rows ascending
 };
 
 int build_structure(const g2oc_graph* g, Structure& s);
-// block-symmetric matrix lists (column/row listings) from a column-major pattern
+// internal row-major order and column lists of a block-symmetric matrix from
+// its column-major upper pattern
 void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s);
 
 // ------------------------------------------------------------ device scalars

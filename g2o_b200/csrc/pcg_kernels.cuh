@@ -1,15 +1,21 @@
 // pcg_kernels.cuh -- block-Jacobi preconditioned conjugate gradients on a
-// symmetric block matrix stored as upper-triangular blocks in column-major
-// order, the device form of LinearSolverPCG::solve / mult / multDiag
-// (g2o/solvers/pcg/linear_solver_pcg.hpp:87-205). Real is the matrix and
-// Krylov-vector type, BS the block size (3 or 6). The solution x and all
-// dot products are FP64.
+// symmetric block matrix, the device form of LinearSolverPCG::solve / mult /
+// multDiag (g2o/solvers/pcg/linear_solver_pcg.hpp:87-205). Real is the
+// storage type of the matrix blocks (double, or float on the mixed path,
+// where the matrix is the dominant traffic), BS the block size (3 or 6). The
+// Krylov vectors, the preconditioner, the solution and all dot products are
+// FP64.
 //
-// One iteration is two kernels: pcg_spmv (direction update d = s + beta d
-// fused into q = A d, partial d.q) and pcg_update (x, r, s = M^-1 r, partial
-// r.s). Scalars live in PcgState on the device; the last block of each kernel
-// (atomic ticket, no waiting) sums the partials in index order and advances
-// the state, so the host only polls `done`.
+// Storage: only the upper blocks, row by row (each row's blocks contiguous,
+// diagonal first), so the product reads the matrix once: the row pass forms
+// sum_c A(r,c) d_c for its row and writes the transposed contributions
+// A(r,c)^T d_r per block; the column pass sums those per column in row order.
+// One PCG iteration is three kernels: row pass (with the direction update
+// d = s + beta d fused in), column pass (q, partial d.q, alpha), update (x, r,
+// s = M^-1 r, partial r.s, beta, stop test). Scalars live in PcgState on the
+// device; the last block of a kernel (atomic ticket, no waiting) sums the
+// partials in index order and advances the state, so the host only polls
+// `done`. All sums are in a fixed order: results are bit-reproducible.
 #pragma once
 
 #include "g2o_math.cuh"
@@ -20,14 +26,25 @@ namespace g2oc {
 template <typename Real>
 struct SysDev {
   int nb;
-  const int* col_ptr;   // nb + 1, column-major ranges, diagonal last
-  const int* row;       // per block
-  const int* diag;      // per row: block of the diagonal
-  const int* rowu_ptr;  // nb + 1, strictly-upper blocks listed by row
-  const int* rowu_blk;
-  const int* rowu_col;
-  const Real* val;      // BS*BS row-major per block
+  int nnzb;
+  const int* rptr;   // nb + 1: blocks of row r (upper, diagonal first)
+  const int* rcol;   // per block: column
+  const int* brow;   // per block: row
+  const int* diag;   // per row: block of the diagonal
+  const int* cptr;   // nb + 1: strictly-upper blocks of column c
+  const int* cblk;   //         (block indices, rows ascending)
+  const Real* val;   // block values, row-SoA layout (sys_offset)
 };
+
+// Storage of the block values: the blocks of row r occupy the contiguous
+// range [rptr[r] * BS*BS, rptr[r+1] * BS*BS); inside it entry e (row-major
+// within the block) of the row's j-th block sits at e * nblk_r + j, so the
+// same entry of consecutive blocks is contiguous (coalesced when one lane
+// handles one block).
+template <int BS>
+__host__ __device__ __forceinline__ size_t sys_offset(int rbase, int nblk, int j, int e) {
+  return (size_t)rbase * BS * BS + (size_t)e * nblk + j;
+}
 
 struct PcgState {
   double dn;              // r^T M^-1 r of the current iterate
@@ -36,31 +53,32 @@ struct PcgState {
   double beta;
   double residual_carry;  // LinearSolverPCG::_residual (0.5 * final dn of the previous solve)
   double tolerance;
+  double check_dn;        // M-norm of a given residual (refinement check)
   unsigned int counter;   // last-block ticket
   int k;                  // completed iterations
   int done;
   int iterations;
   int max_iter;
   int absolute_tolerance;
-  int relative_only;      // refinement solves: ignore the carried residual
-  int pad;
+  int fixed_d0;           // correction solves: keep d0 of the first solve, leave the carry
+  int breakdown;          // d.q <= 0 met (the matrix is not positive definite along d)
 };
 
 // M^-1: inverse of each diagonal block (computed in FP64)
 template <typename Real, int BS>
-__global__ void pcg_diag_inv(SysDev<Real> A, Real* minv, int* nonfinite) {
+__global__ void pcg_diag_inv(SysDev<Real> A, double* minv, int* nonfinite) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.nb) return;
-  const Real* D = A.val + (size_t)A.diag[i] * BS * BS;
+  const int rb = A.rptr[i], nblk = A.rptr[i + 1] - rb, j = A.diag[i] - rb;
   double M[BS * BS], I[BS * BS];
 #pragma unroll
-  for (int k = 0; k < BS * BS; ++k) M[k] = (double)D[k];
+  for (int k = 0; k < BS * BS; ++k) M[k] = (double)A.val[sys_offset<BS>(rb, nblk, j, k)];
   bool ok;
   if (BS == 3) ok = inverse3(M, I);
   else ok = inverse_gj<double, BS>(M, I);
   if (!ok) *nonfinite = 1;
 #pragma unroll
-  for (int k = 0; k < BS * BS; ++k) minv[(size_t)i * BS * BS + k] = (Real)I[k];
+  for (int k = 0; k < BS * BS; ++k) minv[(size_t)i * BS * BS + k] = I[k];
 }
 
 __device__ __forceinline__ bool last_block_ticket(unsigned int* counter) {
@@ -83,27 +101,27 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
 
 // r = b, x = 0, s = M^-1 r, dn = r.s, d0 = tol * dn (raised to the carried
 // residual when absolute tolerance is on), linear_solver_pcg.hpp:117-137
-template <typename Real, int BS>
-__global__ void pcg_init(int nb, const double* b, const Real* minv, Real* r, Real* s, double* x, double* partials,
-                         PcgState* st) {
+template <int BS>
+__global__ void pcg_init(int nb, const double* b, const double* minv, double* r, double* s, double* x,
+                         double* partials, PcgState* st) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double dot = 0.0;
   if (i < nb) {
-    Real rb[BS];
+    double rb[BS];
 #pragma unroll
     for (int k = 0; k < BS; ++k) {
-      rb[k] = (Real)b[(size_t)i * BS + k];
+      rb[k] = b[(size_t)i * BS + k];
       r[(size_t)i * BS + k] = rb[k];
       x[(size_t)i * BS + k] = 0.0;
     }
-    const Real* M = minv + (size_t)i * BS * BS;
+    const double* M = minv + (size_t)i * BS * BS;
 #pragma unroll
     for (int a = 0; a < BS; ++a) {
-      Real v = Real(0);
+      double v = 0.0;
 #pragma unroll
       for (int c = 0; c < BS; ++c) v += M[a * BS + c] * rb[c];
       s[(size_t)i * BS + a] = v;
-      dot += (double)rb[a] * (double)v;
+      dot += rb[a] * v;
     }
   }
   dot = block_sum1(dot);
@@ -112,90 +130,127 @@ __global__ void pcg_init(int nb, const double* b, const Real* minv, Real* r, Rea
     const double dn = sum_partials(partials, gridDim.x);
     if (threadIdx.x == 0) {
       st->counter = 0;
-      double d0 = st->tolerance * dn;
-      if (st->absolute_tolerance && !st->relative_only) {
-        if (st->residual_carry > 0.0 && st->residual_carry > d0) d0 = st->residual_carry;
+      double d0 = st->d0;
+      if (!st->fixed_d0) {
+        d0 = st->tolerance * dn;
+        if (st->absolute_tolerance) {
+          if (st->residual_carry > 0.0 && st->residual_carry > d0) d0 = st->residual_carry;
+        }
       }
       st->d0 = d0;
       st->dn = dn;
       st->beta = 0.0;
       st->k = 0;
+      st->breakdown = 0;
       st->done = (dn <= d0 || st->max_iter <= 0) ? 1 : 0;
       if (st->done) {
         st->iterations = 0;
-        if (!st->relative_only) st->residual_carry = 0.5 * dn;
+        if (!st->fixed_d0) st->residual_carry = 0.5 * dn;
       }
     }
   }
 }
 
-// d_k = s + beta d_{k-1} (ping-pong by parity of k), q = A d_k (both the
-// upper blocks and their transposes, as LinearSolverPCG::mult), partial d.q.
-// One warp per block row.
+// Row pass: d_k = s + beta d_{k-1} (ping-pong by parity of k), for row r
+// qrow_r = sum_c A(r,c) d_c, and per strictly-upper block T_b = A(r,c)^T d_r.
+// One warp per block row; lane j takes blocks j, j+32, ... of the row, and
+// with the row-SoA layout each entry load is coalesced across the warp.
 template <typename Real, int BS, int THREADS>
-__global__ void __launch_bounds__(THREADS) pcg_spmv(SysDev<Real> A, const Real* s, Real* d0buf, Real* d1buf, Real* q,
-                                                    double* partials, PcgState* st) {
+__global__ void __launch_bounds__(THREADS) pcg_rowpass(SysDev<Real> A, const double* s, double* d0buf,
+                                                       double* d1buf, double* qrow, double* tbuf,
+                                                       const PcgState* st) {
   if (st->done) return;
   const int k = st->k;
   const double beta = st->beta;
-  Real* dcur = (k & 1) ? d1buf : d0buf;
-  const Real* dprev = (k & 1) ? d0buf : d1buf;
-  const Real rb = (Real)beta;
+  double* dcur = (k & 1) ? d1buf : d0buf;
+  const double* dprev = (k & 1) ? d0buf : d1buf;
   const bool use_prev = beta != 0.0;
   const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
-  double dot = 0.0;
-  if (i < A.nb) {
-    Real acc[BS];
+  const int r = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
+  if (r >= A.nb) return;
+  auto dval = [&](int j, double* out) {
 #pragma unroll
-    for (int a = 0; a < BS; ++a) acc[a] = Real(0);
-    auto dval = [&](int j, Real* out) {
-#pragma unroll
-      for (int c = 0; c < BS; ++c) {
-        Real v = s[(size_t)j * BS + c];
-        if (use_prev) v += rb * dprev[(size_t)j * BS + c];
-        out[c] = v;
-      }
-    };
-    // column i: blocks (rj, i) with rj <= i contribute A(rj,i)^T d_rj
-    const int c1 = A.col_ptr[i + 1];
-    for (int p = A.col_ptr[i] + lane; p < c1; p += 32) {
-      const int rj = A.row[p];
-      Real dj[BS];
-      dval(rj, dj);
-      const Real* M = A.val + (size_t)p * BS * BS;
-#pragma unroll
-      for (int r = 0; r < BS; ++r)
-#pragma unroll
-        for (int c = 0; c < BS; ++c) acc[c] += M[r * BS + c] * dj[r];
+    for (int c = 0; c < BS; ++c) {
+      double v = s[(size_t)j * BS + c];
+      if (use_prev) v += beta * dprev[(size_t)j * BS + c];
+      out[c] = v;
     }
-    // row i: strictly-upper blocks (i, cj) contribute A(i,cj) d_cj
-    const int r1 = A.rowu_ptr[i + 1];
-    for (int p = A.rowu_ptr[i] + lane; p < r1; p += 32) {
-      const int cj = A.rowu_col[p];
-      Real dj[BS];
-      dval(cj, dj);
-      const Real* M = A.val + (size_t)A.rowu_blk[p] * BS * BS;
+  };
+  double dr[BS];
+  dval(r, dr);
+  double acc[BS];
 #pragma unroll
-      for (int r = 0; r < BS; ++r)
+  for (int a = 0; a < BS; ++a) acc[a] = 0.0;
+  const int rb = A.rptr[r], nblk = A.rptr[r + 1] - rb;
+  const Real* base = A.val + (size_t)rb * BS * BS;
+  for (int j = lane; j < nblk; j += 32) {
+    const int c = A.rcol[rb + j];
+    double dc[BS];
+    dval(c, dc);
+    double tj[BS];
 #pragma unroll
-        for (int c = 0; c < BS; ++c) acc[r] += M[r * BS + c] * dj[c];
+    for (int b = 0; b < BS; ++b) tj[b] = 0.0;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int b = 0; b < BS; ++b) {
+        const double m = (double)base[(size_t)(i * BS + b) * nblk + j];
+        acc[i] += m * dc[b];
+        tj[b] += m * dr[i];
+      }
+    if (c != r) {
+      double* t = tbuf + (size_t)(rb + j) * BS;
+#pragma unroll
+      for (int b = 0; b < BS; ++b) t[b] = tj[b];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < BS; ++a) acc[a] = warp_sum(acc[a]);
+  if (lane < BS) {
+    double qa = acc[0], da = dr[0];
+#pragma unroll
+    for (int a = 1; a < BS; ++a)
+      if (lane == a) {
+        qa = acc[a];
+        da = dr[a];
+      }
+    qrow[(size_t)r * BS + lane] = qa;
+    dcur[(size_t)r * BS + lane] = da;
+  }
+}
+
+// Column pass: q_c = qrow_c + sum over strictly-upper blocks (r, c) of T_b,
+// rows ascending; partial d.q; the last block sets alpha = dn / d.q.
+template <typename Real, int BS, int THREADS>
+__global__ void __launch_bounds__(THREADS) pcg_colpass(SysDev<Real> A, const double* d0buf, const double* d1buf,
+                                                       const double* qrow, const double* tbuf, double* q,
+                                                       double* partials, PcgState* st) {
+  if (st->done) return;
+  const int k = st->k;
+  const double* dcur = (k & 1) ? d1buf : d0buf;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
+  double dot = 0.0;
+  if (c < A.nb) {
+    double acc[BS];
+#pragma unroll
+    for (int a = 0; a < BS; ++a) acc[a] = 0.0;
+    const int p1 = A.cptr[c + 1];
+    for (int p = A.cptr[c] + lane; p < p1; p += 32) {
+      const double* t = tbuf + (size_t)A.cblk[p] * BS;
+#pragma unroll
+      for (int a = 0; a < BS; ++a) acc[a] += t[a];
     }
 #pragma unroll
     for (int a = 0; a < BS; ++a) acc[a] = warp_sum(acc[a]);
-    Real di[BS];
-    dval(i, di);
     if (lane < BS) {
-      Real qa = acc[0], da = di[0];
+      double qa = acc[0];
 #pragma unroll
       for (int a = 1; a < BS; ++a)
-        if (lane == a) {
-          qa = acc[a];
-          da = di[a];
-        }
-      q[(size_t)i * BS + lane] = qa;
-      dcur[(size_t)i * BS + lane] = da;
-      dot = (double)da * (double)qa;
+        if (lane == a) qa = acc[a];
+      qa += qrow[(size_t)c * BS + lane];
+      q[(size_t)c * BS + lane] = qa;
+      dot = dcur[(size_t)c * BS + lane] * qa;
     }
   }
   dot = block_sum1(dot);
@@ -205,39 +260,51 @@ __global__ void __launch_bounds__(THREADS) pcg_spmv(SysDev<Real> A, const Real* 
     if (threadIdx.x == 0) {
       st->counter = 0;
       st->alpha = st->dn / dq;
+      if (!(dq > 0.0)) st->breakdown = 1;
     }
   }
 }
 
 // x += alpha d, r -= alpha q, s = M^-1 r, dn = r.s, beta = dn / dn_old;
 // stop when dn <= d0 or after max_iter iterations (linear_solver_pcg.hpp:139-158)
-template <typename Real, int BS>
-__global__ void pcg_update(int nb, const Real* minv, const Real* d0buf, const Real* d1buf, const Real* q, Real* r,
-                           Real* s, double* x, double* partials, PcgState* st) {
+template <int BS>
+__global__ void pcg_update(int nb, const double* minv, const double* d0buf, const double* d1buf, const double* q,
+                           double* r, double* s, double* x, double* partials, PcgState* st) {
   if (st->done) return;
   const int k = st->k;
+  if (st->breakdown) {
+    // d.q <= 0: the (rounded) matrix is not positive definite along d; stop
+    // with the current iterate instead of stepping along a non-descent
+    // direction (cannot occur for an SPD FP64 system, where d.q > 0 whenever
+    // dn > d0)
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->done = 1;
+      st->iterations = k;
+      if (!st->fixed_d0) st->residual_carry = 0.5 * st->dn;
+    }
+    return;
+  }
   const double alpha = st->alpha;
-  const Real* d = (k & 1) ? d1buf : d0buf;
+  const double* d = (k & 1) ? d1buf : d0buf;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double dot = 0.0;
   if (i < nb) {
-    Real rb[BS];
-    const Real ra = (Real)alpha;
+    double rb[BS];
 #pragma unroll
     for (int c = 0; c < BS; ++c) {
       const size_t o = (size_t)i * BS + c;
-      x[o] += alpha * (double)d[o];
-      rb[c] = r[o] - ra * q[o];
+      x[o] += alpha * d[o];
+      rb[c] = r[o] - alpha * q[o];
       r[o] = rb[c];
     }
-    const Real* M = minv + (size_t)i * BS * BS;
+    const double* M = minv + (size_t)i * BS * BS;
 #pragma unroll
     for (int a = 0; a < BS; ++a) {
-      Real v = Real(0);
+      double v = 0.0;
 #pragma unroll
       for (int c = 0; c < BS; ++c) v += M[a * BS + c] * rb[c];
       s[(size_t)i * BS + a] = v;
-      dot += (double)rb[a] * (double)v;
+      dot += rb[a] * v;
     }
   }
   dot = block_sum1(dot);
@@ -252,10 +319,52 @@ __global__ void pcg_update(int nb, const Real* minv, const Real* d0buf, const Re
       if (dn <= st->d0 || k + 1 >= st->max_iter) {
         st->done = 1;
         st->iterations = k + 1;
-        if (!st->relative_only) st->residual_carry = 0.5 * dn;
+        if (!st->fixed_d0) st->residual_carry = 0.5 * dn;
       }
     }
   }
+}
+
+// M-norm r^T M^-1 r of a residual in FP64 -> st->check_dn (refinement check)
+template <int BS>
+__global__ void pcg_check_dn(int nb, const double* minv, const double* r, double* partials, PcgState* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double dot = 0.0;
+  if (i < nb) {
+    const double* M = minv + (size_t)i * BS * BS;
+    const double* rb = r + (size_t)i * BS;
+#pragma unroll
+    for (int a = 0; a < BS; ++a) {
+      double v = 0.0;
+#pragma unroll
+      for (int c = 0; c < BS; ++c) v += M[a * BS + c] * rb[c];
+      dot += rb[a] * v;
+    }
+  }
+  dot = block_sum1(dot);
+  if (threadIdx.x == 0) partials[blockIdx.x] = dot;
+  if (last_block_ticket(&st->counter)) {
+    const double dn = sum_partials(partials, gridDim.x);
+    if (threadIdx.x == 0) {
+      st->counter = 0;
+      st->check_dn = dn;
+    }
+  }
+}
+
+// internal (row-SoA) system from a column-major pattern matrix (blocks
+// row-major inside), with lambda added to the diagonal
+template <typename Real, int BS>
+__global__ void sys_gather_damped(const Real* src, const int* perm, const int* brow, const int* rptr, const int* rcol,
+                                  int nnzb, double lambda, Real* dst) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nnzb * BS * BS) return;
+  const int k = (int)(t / (BS * BS)), e = (int)(t % (BS * BS));
+  double v = (double)src[(size_t)perm[k] * BS * BS + e];
+  const int r = brow[k];
+  if (r == rcol[k] && e / BS == e % BS) v += lambda;
+  const int rb = rptr[r];
+  dst[sys_offset<BS>(rb, rptr[r + 1] - rb, k - rb, e)] = (Real)v;
 }
 
 }  // namespace g2oc

@@ -66,32 +66,35 @@ void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s) {
   const int nnzb = (int)(rc.size() / 2);
   s.sys_nb = nb;
   s.sys_nnzb = nnzb;
-  s.sys_col_ptr.assign(nb + 1, 0);
-  s.sys_row.resize(nnzb);
+  // internal order: by (row, col); the column-major pattern lists (col, row)
+  std::vector<uint64_t> keys(nnzb);
+  for (int k = 0; k < nnzb; ++k) keys[k] = (uint64_t)rc[2 * k] * (uint64_t)nb + (uint64_t)rc[2 * k + 1];
+  std::vector<uint32_t> perm;
+  radix_sort(keys, perm);
+  s.sys_perm.assign(perm.begin(), perm.end());
+  s.sys_rptr.assign(nb + 1, 0);
+  s.sys_rcol.resize(nnzb);
+  s.sys_brow.resize(nnzb);
   s.sys_diag.assign(nb, -1);
-  std::vector<int> rows_key;
-  rows_key.reserve(nnzb);
-  std::vector<int> upper_idx;
+  std::vector<int> ckey;
+  std::vector<int> cidx;
   for (int k = 0; k < nnzb; ++k) {
-    const int r = rc[2 * k], c = rc[2 * k + 1];
-    s.sys_col_ptr[c + 1]++;
-    s.sys_row[k] = r;
+    const int p = (int)perm[k];
+    const int r = rc[2 * p], c = rc[2 * p + 1];
+    s.sys_rptr[r + 1]++;
+    s.sys_rcol[k] = c;
+    s.sys_brow[k] = r;
     if (r == c) s.sys_diag[r] = k;
     else {
-      rows_key.push_back(r);
-      upper_idx.push_back(k);
+      ckey.push_back(c);
+      cidx.push_back(k);
     }
   }
-  for (int i = 0; i < nb; ++i) s.sys_col_ptr[i + 1] += s.sys_col_ptr[i];
+  for (int i = 0; i < nb; ++i) s.sys_rptr[i + 1] += s.sys_rptr[i];
   std::vector<int> order;
-  counting_sort(rows_key, nb, order, s.sys_rowu_ptr);
-  s.sys_rowu_blk.resize(order.size());
-  s.sys_rowu_col.resize(order.size());
-  for (size_t i = 0; i < order.size(); ++i) {
-    const int k = upper_idx[order[i]];
-    s.sys_rowu_blk[i] = k;
-    s.sys_rowu_col[i] = rc[2 * k + 1];
-  }
+  counting_sort(ckey, nb, order, s.sys_cptr);
+  s.sys_cblk.resize(order.size());
+  for (size_t i = 0; i < order.size(); ++i) s.sys_cblk[i] = cidx[order[i]];
 }
 
 static int build_ba(const g2oc_graph* g, Structure& s) {
@@ -200,11 +203,18 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     s.hpp_rc[2 * h + 1] = h;
     s.hpp_diag[h] = h;
   }
+  // position of each Hpl block in its camera's list
+  s.hc_pos.assign(nhpl, 0);
+  s.max_blocks_per_cam = 0;
+  for (int h = 0; h < s.Cf; ++h) {
+    s.max_blocks_per_cam = std::max(s.max_blocks_per_cam, s.hc_ptr[h + 1] - s.hc_ptr[h]);
+    for (int p = s.hc_ptr[h]; p < s.hc_ptr[h + 1]; ++p) s.hc_pos[s.hc_blk[p]] = p - s.hc_ptr[h];
+  }
   // Schur pattern: Hpp pattern + co-observing pose pairs (block_solver.hpp:229-266),
   // with the pair list of each block in landmark order
   s.schur_rc.clear();
-  s.sp_ptr.clear();
-  s.sp_ab.clear();
+  s.s_pair_ptr.clear();
+  s.s_pairs.clear();
   s.s_hpp.clear();
   if (s.schur) {
     int64_t np = 0;
@@ -214,7 +224,7 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     }
     s.num_pairs = np;
     const uint64_t Cf = (uint64_t)s.Cf;
-    std::vector<uint64_t> keys;
+    std::vector<uint64_t> keys;  // row-major: r * Cf + c
     keys.reserve(np + s.Cf);
     std::vector<int32_t> pa2;
     pa2.reserve(2 * np);
@@ -222,33 +232,45 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
       for (int a = s.hb_ptr[l]; a < s.hb_ptr[l + 1]; ++a)
         for (int b = a; b < s.hb_ptr[l + 1]; ++b) {
           const uint64_t r = (uint64_t)s.hpl_rc[2 * a], c = (uint64_t)s.hpl_rc[2 * b];
-          keys.push_back(c * Cf + r);
-          pa2.push_back(a);
+          keys.push_back(r * Cf + c);
+          pa2.push_back(s.hc_pos[a]);
           pa2.push_back(b);
         }
     for (int h = 0; h < s.Cf; ++h) keys.push_back((uint64_t)h * Cf + h);  // diagonal markers (no pair)
     std::vector<uint32_t> perm;
     radix_sort(keys, perm);
-    s.sp_ab.reserve(2 * np);
-    s.sp_ptr.push_back(0);
+    s.s_pairs.reserve(2 * np);
+    std::vector<int32_t> rm_rc;  // internal (row-major) blocks
+    s.s_pair_ptr.push_back(0);
     uint64_t prev = ~0ull;
     for (size_t i = 0; i < keys.size(); ++i) {
       if (keys[i] != prev) {
-        if (prev != ~0ull) s.sp_ptr.push_back((int)(s.sp_ab.size() / 2));
+        if (prev != ~0ull) s.s_pair_ptr.push_back((int)(s.s_pairs.size() / 2));
         prev = keys[i];
-        const int c = (int)(keys[i] / Cf), r = (int)(keys[i] % Cf);
-        s.schur_rc.push_back(r);
-        s.schur_rc.push_back(c);
+        const int r = (int)(keys[i] / Cf), c = (int)(keys[i] % Cf);
+        rm_rc.push_back(r);
+        rm_rc.push_back(c);
         s.s_hpp.push_back(r == c ? s.hpp_diag[r] : -1);
       }
       const uint32_t p = perm[i];
       if (p < (uint32_t)np) {
-        s.sp_ab.push_back(pa2[2 * (size_t)p]);
-        s.sp_ab.push_back(pa2[2 * (size_t)p + 1]);
+        s.s_pairs.push_back(pa2[2 * (size_t)p]);
+        s.s_pairs.push_back(pa2[2 * (size_t)p + 1]);
       }
     }
-    s.sp_ptr.push_back((int)(s.sp_ab.size() / 2));
-    build_sym_lists(s.Cf, s.schur_rc, s);
+    s.s_pair_ptr.push_back((int)(s.s_pairs.size() / 2));
+    // column-major pattern (the order of SparseBlockMatrix::blockCols)
+    const size_t nS = rm_rc.size() / 2;
+    std::vector<uint64_t> ck(nS);
+    for (size_t k = 0; k < nS; ++k) ck[k] = (uint64_t)rm_rc[2 * k + 1] * Cf + (uint64_t)rm_rc[2 * k];
+    std::vector<uint32_t> cperm;
+    radix_sort(ck, cperm);
+    s.schur_rc.resize(2 * nS);
+    for (size_t i = 0; i < nS; ++i) {
+      s.schur_rc[2 * i] = rm_rc[2 * (size_t)cperm[i]];
+      s.schur_rc[2 * i + 1] = rm_rc[2 * (size_t)cperm[i] + 1];
+    }
+    build_sym_lists(s.Cf, s.schur_rc, s);  // internal order = row-major = the order above
   } else {
     build_sym_lists(s.Cf, s.hpp_rc, s);
   }

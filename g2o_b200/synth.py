@@ -233,9 +233,10 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     cx, cy = width / 2.0, height_px / 2.0
     kdraw = np.clip(rng.geometric(1.0 / mean_obs, size=num_points), min_obs, max_obs)
     pts, cams, uvs = [], [], []
+    Rm = np.ascontiguousarray(Rcw.reshape(num_cameras * 3, 3).T)
     for s in range(0, num_points, chunk):
         Xs = X[s:s + chunk]
-        Xc = np.einsum("cab,pb->pca", Rcw, Xs) + tcw[None, :, :]
+        Xc = (Xs @ Rm).reshape(Xs.shape[0], num_cameras, 3) + tcw[None, :, :]
         z = Xc[..., 2]
         with np.errstate(divide="ignore", invalid="ignore"):
             u = focal * Xc[..., 0] / z + cx
@@ -243,16 +244,20 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
         vis = (z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height_px)
         keys = rng.random(vis.shape)
         keys[~vis] = 2.0
-        order = np.argsort(keys, axis=1)
-        nvis = vis.sum(axis=1)
-        k = np.minimum(kdraw[s:s + chunk], nvis)
-        for r in range(Xs.shape[0]):
-            if k[r] < 2:
-                continue
-            sel = np.sort(order[r, :k[r]])
-            pts.append(np.full(len(sel), s + r))
-            cams.append(sel)
-            uvs.append(np.stack([u[r, sel], v[r, sel]], 1))
+        m = min(max_obs, num_cameras)
+        cand = np.argpartition(keys, m - 1, axis=1)[:, :m]
+        ck = np.take_along_axis(keys, cand, axis=1)
+        cand = np.take_along_axis(cand, np.argsort(ck, axis=1), axis=1)
+        k = np.minimum(kdraw[s:s + chunk], vis.sum(axis=1))
+        k[k < 2] = 0
+        take = np.arange(m)[None, :] < k[:, None]
+        cand = np.where(take, cand, num_cameras)
+        cand.sort(axis=1)  # cameras ascending within a point
+        rows, cols = np.nonzero(cand < num_cameras)
+        sel = cand[rows, cols]
+        pts.append(s + rows)
+        cams.append(sel)
+        uvs.append(np.stack([u[rows, sel], v[rows, sel]], 1))
     pts = np.concatenate(pts)
     cams = np.concatenate(cams)
     uv = np.concatenate(uvs) + rng.normal(0.0, pixel_noise, size=(len(pts), 2))

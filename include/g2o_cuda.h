@@ -130,8 +130,8 @@ typedef struct g2oc_params {
   int32_t max_trials_after_failure;  /* 10 ("maxTrialsAfterFailure" property) */
   double initial_lambda;             /* 0: tau * max diag(H) ("initialLambda" property) */
   double tau;                        /* 1e-5 */
-  int32_t refine_max_iterations;     /* mixed precision: outer FP64 refinement steps (default 4) */
-  double refine_tolerance;           /* mixed precision: stop when |r|/|b| below (default 1e-10) */
+  int32_t refine_max_iterations;     /* mixed precision: max FP64 refinement corrections per solve (default 2) */
+  double refine_tolerance;           /* reserved (default 1e-10) */
 } g2oc_params;
 
 /* one per outer iteration, the fields of G2OBatchStatistics (g2o/core/batch_stats.h:40-82) */
@@ -162,6 +162,13 @@ typedef struct g2oc_hessian_info {
   int64_t vector_size;      /* Solver::vectorSize() */
 } g2oc_hessian_info;
 
+/* per-kernel launch count and (when timing is on) summed CUDA-event time */
+typedef struct g2oc_kernel_stat {
+  char name[32];
+  int64_t launches;
+  double total_ms;
+} g2oc_kernel_stat;
+
 typedef struct g2oc_ctx g2oc_ctx;
 
 /* library */
@@ -179,12 +186,18 @@ int g2oc_construct(const char* name, g2oc_params* params);
 int g2oc_create(int device, g2oc_ctx** out);
 void g2oc_destroy(g2oc_ctx* ctx);
 int g2oc_set_params(g2oc_ctx* ctx, const g2oc_params* params);
+/* the context's CUDA stream (cudaStream_t), for callers that order their own
+   work or CUDA events after the solver's */
+int g2oc_get_stream(g2oc_ctx* ctx, void** stream);
 
 /* graph */
 int g2oc_upload(g2oc_ctx* ctx, const g2oc_graph* graph);
 int g2oc_get_hessian_info(g2oc_ctx* ctx, g2oc_hessian_info* info);
 int g2oc_set_estimates(g2oc_ctx* ctx, const double* pose_estimate, const double* point_estimate);
 int g2oc_download(g2oc_ctx* ctx, double* pose_estimate, double* point_estimate);
+/* restore the estimates given to g2oc_upload (device copy); the whole-graph
+   counterpart of OptimizableGraph::push/pop (g2o/core/optimizable_graph.cpp) */
+int g2oc_restore_initial_estimates(g2oc_ctx* ctx);
 
 /* optimization: stats may be NULL, else iterations entries */
 int g2oc_optimize(g2oc_ctx* ctx, int iterations, g2oc_iteration_stats* stats, int* iterations_done);
@@ -198,6 +211,13 @@ int g2oc_get_pattern(g2oc_ctx* ctx, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* s
 int g2oc_get_hessian(g2oc_ctx* ctx, double* hpp, double* hll, double* hpl, double* b);
 int g2oc_schur(g2oc_ctx* ctx, double lambda, double* schur_blocks, double* bschur);
 int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations);
+
+/* instrumentation, the device-side counterpart of G2OBatchStatistics /
+   ScopedTictoc (g2o/core/batch_stats.h:40-82, g2o/stuff/tictoc.h:59):
+   enable (and reset) per-kernel launch counting with CUDA-event timing on the
+   context's stream; read the per-kernel counts and times and the total count */
+int g2oc_set_kernel_timing(g2oc_ctx* ctx, int enable);
+int g2oc_get_kernel_stats(g2oc_ctx* ctx, g2oc_kernel_stat* out, int capacity, int* count, int64_t* total_launches);
 
 /* LinearSolver::solve on a caller block matrix: symmetric, upper blocks given
    column-major as (row, col) block pairs with row-major dense values; block

@@ -1692,7 +1692,7 @@ void orc_default_params(g2oc_params* p) {
   p->max_trials_after_failure = 10;
   p->initial_lambda = 0.0;
   p->tau = 1e-5;
-  p->refine_max_iterations = 4;
+  p->refine_max_iterations = 2;
   p->refine_tolerance = 1e-10;
 }
 
