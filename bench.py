@@ -103,22 +103,22 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def algorithmic_bytes(kernel, info, E, real):
+def algorithmic_bytes(kernel, info, E, real, num_pairs):
     """Bytes each array element read or written once, per launch (the model
-    DESIGN.md states)."""
+    DESIGN.md states). real = bytes of the Hessian/Schur storage type."""
     C, P = info.num_free_poses, info.num_free_points
     nH, nS = info.hpl_nnzb, info.schur_nnzb
     n = C * 6
-    if kernel == "ba_landmark_pass":
+    if kernel == "ba_landmark_pass":   # edges (v 8, z 16, Om/delta 32, hpl 4), points, cameras -> Hpl, Hll, b_l
         return 60 * E + 32 * P + 64 * C + 18 * real * nH + (6 * real + 24) * P
-    if kernel == "ba_camera_pass":
+    if kernel == "ba_camera_pass":     # camera-major edge copy + point gather -> Hpp, b_p
         return 88 * E + (36 * real + 48) * C
-    if kernel == "schur_landmark":
-        return (6 + 9) * real * P + 36 * real * nH
-    if kernel == "schur_blocks":
-        return 8 * (nH * 5) + 36 * real * nH + 36 * real * C + 36 * real * nS + 4 * nS
-    if kernel == "pcg_spmv":
-        return 36 * real * nS + 12 * nS + 4 * 8 * n
+    if kernel == "schur_rows":         # Hpl, Dinv, Hpp, b_l, pair lists -> S (upper), b_schur
+        return 18 * real * nH + 9 * real * P + 36 * real * C + 24 * P + 8 * num_pairs + 8 * nS + 36 * real * nS + 48 * C
+    if kernel == "pcg_spmv":           # row pass: S (upper) + column index -> transposed contributions T
+        return (36 * real + 4) * nS + 48 * (nS - C) + 4 * 8 * n
+    if kernel == "pcg_colpass":
+        return (48 + 4) * (nS - C) + 3 * 8 * n
     if kernel == "chi2":
         return 56 * E + 32 * P + 64 * C
     if kernel == "ba_backsub":
@@ -277,7 +277,7 @@ def run_ours(args):
     dom = max(kstats.items(), key=lambda kv: kv[1][1])
     dname, (dlaunch, dms) = dom
     real = 4
-    algo = algorithmic_bytes(dname, pm.info, pm.info.num_active_edges, real)
+    algo = algorithmic_bytes(dname, pm.info, pm.info.num_active_edges, real, pm.info.schur_pairs)
     peak, peak_kind = measured_peaks()
     roof = None
     if algo is not None and dlaunch > 0:

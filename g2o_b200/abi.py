@@ -117,6 +117,7 @@ class G2ocHessianInfo(C.Structure):
         ("schur_nnzb", C.c_int32),
         ("num_active_edges", C.c_int32),
         ("vector_size", C.c_int64),
+        ("schur_pairs", C.c_int64),
     ]
 
 

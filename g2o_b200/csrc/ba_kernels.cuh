@@ -126,12 +126,13 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
-    Real camr[8], Xr[3];
-#pragma unroll
-    for (int i = 0; i < 7; ++i) camr[i] = (Real)cam[i];
-    Xr[0] = (Real)Xc[0]; Xr[1] = (Real)Xc[1]; Xr[2] = (Real)Xc[2];
+    double Jpd[6], Jcd[12];
+    ba_jacobians_from_xc(cam, Xc, V.f, Jpd, Jcd);
     Real Jp[6], Jc[12];
-    ba_jacobians_from_xc(camr, Xr, (Real)V.f, Jp, Jc);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) Jp[i] = (Real)Jpd[i];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) Jc[i] = (Real)Jcd[i];
     const double we0 = -w * (om.x * e[0] + om.y * e[1]);
     const double we1 = -w * (om.y * e[0] + om.z * e[1]);
     const Real o00 = (Real)(w * om.x), o01 = (Real)(w * om.y), o11 = (Real)(w * om.z);
@@ -149,7 +150,7 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
     H[4] += A0[1] * Jp[2] + A1[1] * Jp[5];
     H[5] += A0[2] * Jp[2] + A1[2] * Jp[5];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) bl[i] += (double)Jp[i] * we0 + (double)Jp[3 + i] * we1;
+    for (int i = 0; i < 3; ++i) bl[i] += Jpd[i] * we0 + Jpd[3 + i] * we1;
     const int blk = E.hpl[k];
     if (blk >= 0) {
       if (blk != cur) {
@@ -197,12 +198,11 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
-    Real camr[8], Xr[3];
+    double Jpd[6], Jcd[12];
+    ba_jacobians_from_xc(cam, Xc, V.f, Jpd, Jcd);
+    Real Jc[12];
 #pragma unroll
-    for (int i = 0; i < 7; ++i) camr[i] = (Real)cam[i];
-    Xr[0] = (Real)Xc[0]; Xr[1] = (Real)Xc[1]; Xr[2] = (Real)Xc[2];
-    Real Jp[6], Jc[12];
-    ba_jacobians_from_xc(camr, Xr, (Real)V.f, Jp, Jc);
+    for (int i = 0; i < 12; ++i) Jc[i] = (Real)Jcd[i];
     const double we0 = -w * (om.x * e[0] + om.y * e[1]);
     const double we1 = -w * (om.y * e[0] + om.z * e[1]);
     const Real o00 = (Real)(w * om.x), o01 = (Real)(w * om.y), o11 = (Real)(w * om.z);
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
 #pragma unroll
       for (int c = r; c < 6; ++c) H[t++] += A0[r] * Jc[c] + A1[r] * Jc[6 + c];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) bp[i] += (double)Jc[i] * we0 + (double)Jc[6 + i] * we1;
+    for (int i = 0; i < 6; ++i) bp[i] += Jcd[i] * we0 + Jcd[6 + i] * we1;
   }
   __shared__ double red[THREADS / 32][27];
   block_sum_array<Real, 21, THREADS>(H, &red[0][0]);
@@ -238,11 +238,12 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
 
 // ---------------------------------------------------------------- Schur
 // Landmark step of the Schur loop (block_solver.hpp:359-378):
-// Dinv = (H_ll + lambda I)^-1; with bd != nullptr also BD = B Dinv per Hpl
-// block (only for cameras too large to stage in shared memory).
+// Dinv = (H_ll + lambda I)^-1 and BD_a = B_a Dinv for every Hpl block a of
+// the landmark, written in camera-major order (bdc[hc_index[a]]) so a camera
+// row's blocks are contiguous for the Schur row kernel.
 template <typename Real>
-__global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_ptr, int Pf, double lambda,
-                               Real* dinv, Real* bd, int* nonfinite) {
+__global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_ptr, const int* hc_index, int Pf,
+                               double lambda, Real* dinv, Real* bdc, int* nonfinite) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= Pf) return;
   const Real* h = hll + (size_t)l * 6;
@@ -257,11 +258,11 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
     D[i] = (Real)Di[i];
     dinv[(size_t)l * 9 + i] = D[i];
   }
-  if (!bd) return;
+  if (!bdc) return;
   const int b1 = hb_ptr[l + 1];
   for (int a = hb_ptr[l]; a < b1; ++a) {
     const Real* B = hpl + (size_t)a * 18;
-    Real* o = bd + (size_t)a * 18;
+    Real* o = bdc + (size_t)hc_index[a] * 18;
 #pragma unroll
     for (int r = 0; r < 6; ++r)
 #pragma unroll
@@ -281,43 +282,96 @@ struct Vec2<float> {
 };
 
 // Schur complement by camera rows (block_solver.hpp:343-433): one CTA per
-// free camera r stages BD_a = B_a Dinv_l for the camera's Hpl blocks in
-// shared memory; then two lanes per Schur block (r, c) of the row (lane
-// parity = rows 0-2 or 3-5, 18 FP64 accumulators each) sum -BD_a B_b^T over
-// the block's co-observing pairs in landmark order (B_b read from L1/L2) and
-// add Hpp(r, c) (+ lambda on the diagonal). With bs != nullptr the reduced
-// right-hand side bs_r = b_r - sum_a BD_a b_l(a) is formed from the same
-// staged blocks. S is written in the row-SoA layout of sys_offset.
-template <typename Real, bool A_SMEM, int THREADS>
+// free camera r stages the camera's BD_a blocks (contiguous in bdc) in shared
+// memory with coalesced loads. The diagonal block S(r, r) = Hpp(r) + lambda I
+// - sum_a BD_a B_a^T over all of the camera's landmarks is reduced by the
+// whole CTA (fixed assignment and tree); each off-diagonal block (r, c) is
+// summed by two lanes (lane parity = rows 0-2 or 3-5, 18 FP64 accumulators
+// each) over its co-observing pairs in landmark order, with B_b from L1/L2.
+// With bs != nullptr the reduced right-hand side bs_r = b_r - sum_a BD_a
+// b_l(a) is formed from the same staged blocks. S is written in the row-SoA
+// layout of sys_offset.
+template <typename Real, int THREADS, bool STAGE>
 __global__ void __launch_bounds__(THREADS, 1)
     schur_rows(const int* hc_ptr, const int* hc_blk, const int* hpl_col, const Real* hpl, const Real* dinv,
-               const Real* bd, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs,
-               const int* s_hpp, const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l,
-               double* bs) {
+               const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs, const int* s_hpp,
+               const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l, double* bs) {
   using R2 = typename Vec2<Real>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Real* BDa = reinterpret_cast<Real*>(smem_raw);
+  __shared__ double red[THREADS / 32][21];
   const int r = blockIdx.x;
   const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (A_SMEM) {
-    for (int t = threadIdx.x; t < na * 18; t += THREADS) {
-      const int blk = t / 18, e = t % 18;
-      const int a = hc_blk[a0 + blk];
-      const Real* B = hpl + (size_t)a * 18 + (e / 3) * 3;
-      const Real* D = dinv + (size_t)hpl_col[a] * 9 + (e % 3);
-      BDa[t] = B[0] * D[0] + B[1] * D[3] + B[2] * D[6];
+  // the camera's BD_a = B_a Dinv_l blocks, one thread per block: staged in
+  // shared memory, or (cameras with more blocks than shared memory holds)
+  // written to the camera-major scratch bdc and read back in place
+  Real* BDw = STAGE ? reinterpret_cast<Real*>(smem_raw) : const_cast<Real*>(bdc) + (size_t)a0 * 18;
+  for (int t = threadIdx.x; t < na; t += THREADS) {
+    const int a = hc_blk[a0 + t];
+    const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)a * 18);
+    const Real* Dl = dinv + (size_t)hpl_col[a] * 9;
+    Real b[18], D[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const R2 v = B2[q];
+      b[2 * q] = v.x;
+      b[2 * q + 1] = v.y;
+      D[q] = Dl[q];
     }
-    __syncthreads();
+    Real* o = BDw + (size_t)t * 18;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o[i * 3 + c] = b[i * 3] * D[c] + b[i * 3 + 1] * D[3 + c] + b[i * 3 + 2] * D[6 + c];
   }
-  auto bd_of = [&](int al) -> const Real* {
-    return A_SMEM ? BDa + (size_t)al * 18 : bd + (size_t)hc_blk[a0 + al] * 18;
-  };
+  if (!STAGE) __threadfence_block();
+  __syncthreads();
+  const Real* BDa = BDw;
+  // diagonal block
+  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
+  Real* Sr = S + (size_t)rb * 36;
+  {
+    double acc[21];
+#pragma unroll
+    for (int t = 0; t < 21; ++t) acc[t] = 0.0;
+    for (int t = threadIdx.x; t < na; t += THREADS) {
+      const Real* D = BDa + (size_t)t * 18;
+      const Real* B = hpl + (size_t)hc_blk[a0 + t] * 18;
+      Real d[18], b[18];
+#pragma unroll
+      for (int q = 0; q < 18; ++q) {
+        d[q] = D[q];
+        b[q] = B[q];
+      }
+      int u = 0;
+#pragma unroll
+      for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int c = i; c < 6; ++c, ++u)
+          acc[u] += (double)(d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2]);
+    }
+    block_sum_array<double, 21, THREADS>(acc, &red[0][0]);
+    if (threadIdx.x == 0) {
+      const int hb = s_hpp[rb];
+      int u = 0;
+      for (int i = 0; i < 6; ++i)
+        for (int c = i; c < 6; ++c, ++u) {
+          double v = -acc[u] + (i == c ? lambda : 0.0);
+          if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
+          Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
+          if (c != i) {
+            double w = -acc[u];
+            if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
+            Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
+          }
+        }
+    }
+  }
   if (bs && warp == 0) {
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int t = lane; t < na; t += 32) {
       const double* bl = b_l + (size_t)hpl_col[hc_blk[a0 + t]] * 3;
-      const Real* D = bd_of(t);
+      const Real* D = BDa + (size_t)t * 18;
 #pragma unroll
       for (int q = 0; q < 6; ++q) acc[q] += (double)D[q * 3] * bl[0] + (double)D[q * 3 + 1] * bl[1] + (double)D[q * 3 + 2] * bl[2];
     }
@@ -331,10 +385,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       bs[(size_t)r * 6 + lane] = b_p[(size_t)r * 6 + lane] - v;
     }
   }
+  // off-diagonal blocks (the row's diagonal is its first block)
   const int half = threadIdx.x & 1;
-  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
-  Real* Sr = S + (size_t)rb * 36;
-  for (int j = threadIdx.x >> 1; j < nblk; j += THREADS / 2) {
+  for (int j = 1 + (threadIdx.x >> 1); j < nblk; j += THREADS / 2) {
     const int k = rb + j;
     double acc[18];
 #pragma unroll
@@ -342,7 +395,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int p1 = pair_ptr[k + 1];
     for (int p = pair_ptr[k]; p < p1; ++p) {
       const int2 pr = pairs[p];
-      const Real* D = bd_of(pr.x) + half * 9;
+      const Real* D = BDa + (size_t)pr.x * 18 + half * 9;
       Real d[9];
 #pragma unroll
       for (int t = 0; t < 9; ++t) d[t] = D[t];
@@ -361,16 +414,13 @@ __global__ void __launch_bounds__(THREADS, 1)
           acc[i * 6 + c] += (double)(d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2]);
     }
     const int hb = s_hpp[k];
-    const bool dg = rcol[k] == r;
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
-        const int row = half * 3 + i;
-        const int e = row * 6 + c;
+        const int e = (half * 3 + i) * 6 + c;
         double v = -acc[i * 6 + c];
         if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
-        if (dg && row == c) v += lambda;
         Sr[(size_t)e * nblk + j] = (Real)v;
       }
   }
@@ -442,66 +492,82 @@ __global__ void ba_backsub(const int* hb_ptr, const int* hpl_row, int Pf, const 
     x_l[(size_t)l * 3 + i] = (double)D[i * 3] * cl[0] + (double)D[i * 3 + 1] * cl[1] + (double)D[i * 3 + 2] * cl[2];
 }
 
-// Residual of the damped full system in FP64 for the mixed-precision
-// refinement: r_p = b_p - (Hpp + lambda I) x_p - sum_a B_a x_l
-template <typename Real>
-__global__ void ba_resid_cam(const int* hc_ptr, const int* hc_blk, const int* hpl_col, int Cf, const Real* hpl,
-                             const Real* hpp, double lambda, const double* b_p, const double* x_p,
-                             const double* x_l, double* r_p) {
-  const int h = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  const int lane = threadIdx.x & 31;
-  if (h >= Cf) return;
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  const int e1 = hc_ptr[h + 1];
-  for (int p = hc_ptr[h] + lane; p < e1; p += 32) {
-    const int a = hc_blk[p];
-    const double* xl = x_l + (size_t)hpl_col[a] * 3;
-    const Real* B = hpl + (size_t)a * 18;
-#pragma unroll
-    for (int r = 0; r < 6; ++r) acc[r] += (double)B[r * 3] * xl[0] + (double)B[r * 3 + 1] * xl[1] + (double)B[r * 3 + 2] * xl[2];
-  }
-#pragma unroll
-  for (int r = 0; r < 6; ++r) acc[r] = warp_sum(acc[r]);
-  if (lane < 6) {
-    double v = acc[0];
-#pragma unroll
-    for (int r = 1; r < 6; ++r)
-      if (lane == r) v = acc[r];
-    const Real* H = hpp + (size_t)h * 36 + lane * 6;
-    const double* xp = x_p + (size_t)h * 6;
-    double hx = lambda * xp[lane];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) hx += (double)H[c] * xp[c];
-    r_p[(size_t)h * 6 + lane] = b_p[(size_t)h * 6 + lane] - hx - v;
-  }
-}
-
-// r_l = b_l - sum_a B_a^T x_p - (H_ll + lambda I) x_l
-template <typename Real>
-__global__ void ba_resid_lm(const int* hb_ptr, const int* hpl_row, int Pf, const Real* hpl, const Real* hll,
-                            double lambda, const double* b_l, const double* x_p, const double* x_l, double* r_l) {
+// Matrix-free FP64 residual of the damped normal equations for the
+// mixed-precision refinement, r = b - (J^T Om' J + lambda I) x, with the
+// Jacobians recomputed in FP64 from the edges (no FP32 Hessian involved).
+// Landmark side: one thread per free landmark over its edges.
+__global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l_ptr, int Pf, const int* pose_h,
+                                    double lambda, const double* b_l, const double* x_p, const double* x_l,
+                                    double* r_l) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= Pf) return;
   const double* xl = x_l + (size_t)l * 3;
-  const Real* h = hll + (size_t)l * 6;
-  double r[3];
-  r[0] = b_l[(size_t)l * 3] - ((double)h[0] * xl[0] + (double)h[1] * xl[1] + (double)h[2] * xl[2] + lambda * xl[0]);
-  r[1] = b_l[(size_t)l * 3 + 1] - ((double)h[1] * xl[0] + (double)h[3] * xl[1] + (double)h[4] * xl[2] + lambda * xl[1]);
-  r[2] = b_l[(size_t)l * 3 + 2] - ((double)h[2] * xl[0] + (double)h[4] * xl[1] + (double)h[5] * xl[2] + lambda * xl[2]);
-  const int b1 = hb_ptr[l + 1];
-  for (int a = hb_ptr[l]; a < b1; ++a) {
-    const Real* B = hpl + (size_t)a * 18;
-    const double* xp = x_p + (size_t)hpl_row[a] * 6;
+  double acc[3] = {lambda * xl[0], lambda * xl[1], lambda * xl[2]};
+  const int k1 = l_ptr[l + 1];
+  for (int k = l_ptr[l]; k < k1; ++k) {
+    const int2 v = E.v[k];
+    const double4 om = E.om[k];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
+    double Jp[6], Jc[12];
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    double u0 = Jp[0] * xl[0] + Jp[1] * xl[1] + Jp[2] * xl[2];
+    double u1 = Jp[3] * xl[0] + Jp[4] * xl[1] + Jp[5] * xl[2];
+    const int h = pose_h[v.y];
+    if (h >= 0) {
+      const double* xp = x_p + (size_t)h * 6;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      double s = 0.0;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) s += (double)B[q * 3 + c] * xp[q];
-      r[c] -= s;
+      for (int q = 0; q < 6; ++q) {
+        u0 += Jc[q] * xp[q];
+        u1 += Jc[6 + q] * xp[q];
+      }
     }
+    const double o0 = w * (om.x * u0 + om.y * u1), o1 = w * (om.y * u0 + om.z * u1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] += Jp[i] * o0 + Jp[3 + i] * o1;
   }
 #pragma unroll
-  for (int i = 0; i < 3; ++i) r_l[(size_t)l * 3 + i] = r[i];
+  for (int i = 0; i < 3; ++i) r_l[(size_t)l * 3 + i] = b_l[(size_t)l * 3 + i] - acc[i];
+}
+
+// Camera side: one CTA per free camera over its edges, fixed-order reduction.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) ba_resid64_camera(BACamEdges CE, BAVertices V, const int* point_l,
+                                                             double lambda, const double* b_p, const double* x_p,
+                                                             const double* x_l, double* r_p) {
+  const int h = blockIdx.x;
+  const double* xp = x_p + (size_t)h * 6;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int j1 = CE.ptr[h + 1];
+  for (int j = CE.ptr[h] + threadIdx.x; j < j1; j += THREADS) {
+    const int2 v = CE.v[j];
+    const double4 om = CE.om[j];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
+    double Jp[6], Jc[12];
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    double u0 = 0.0, u1 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      u0 += Jc[q] * xp[q];
+      u1 += Jc[6 + q] * xp[q];
+    }
+    const int l = point_l[v.x];
+    if (l >= 0) {
+      const double* xl = x_l + (size_t)l * 3;
+      u0 += Jp[0] * xl[0] + Jp[1] * xl[1] + Jp[2] * xl[2];
+      u1 += Jp[3] * xl[0] + Jp[4] * xl[1] + Jp[5] * xl[2];
+    }
+    const double o0 = w * (om.x * u0 + om.y * u1), o1 = w * (om.y * u0 + om.z * u1);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[q] += Jc[q] * o0 + Jc[6 + q] * o1;
+  }
+  __shared__ double red[THREADS / 32][6];
+  block_sum_array<double, 6, THREADS>(acc, &red[0][0]);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r_p[(size_t)h * 6 + q] = b_p[(size_t)h * 6 + q] - lambda * xp[q] - acc[q];
+  }
 }
 
 // SparseOptimizer::update (sparse_optimizer.cpp:457-468) with

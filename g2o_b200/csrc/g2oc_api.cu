@@ -42,6 +42,7 @@ static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b)
 
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs: fixed grid of the reductions
 constexpr int kPcgChunkMax = 64;
+constexpr int kMixedInnerMaxIter = 256;
 
 // --------------------------------------------------------------- engine
 struct EngineBase {
@@ -85,12 +86,12 @@ struct g2oc_ctx {
   double f = 1, cx = 0, cy = 0;
   // vertex state
   g2oc::DBuf<double> pose, point, pose_bak, point_bak, pose_init, point_init;
-  g2oc::DBuf<int> oplus_count, free_pose, free_point;
+  g2oc::DBuf<int> oplus_count, free_pose, free_point, pose_h, point_l;
   // BA edges
   g2oc::DBuf<int2> e_v, c_v;
   g2oc::DBuf<double2> e_z, c_z;
   g2oc::DBuf<double4> e_om, c_om;
-  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, s_pair_ptr, s_hpp;
+  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, hc_index, s_pair_ptr, s_hpp;
   g2oc::DBuf<int2> s_pairs;
   // pose-graph edges
   g2oc::DBuf<int2> pe_v;
@@ -217,6 +218,10 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const
   PcgState cfg = host;  // keeps residual_carry and, for correction solves, d0
   cfg.tolerance = c->prm.pcg_tolerance;
   cfg.max_iter = c->prm.pcg_max_iterations < 0 ? A.nb * BS : c->prm.pcg_max_iterations;
+  // FP32-stored system (mixed path): the inner solve is a correction step of
+  // the FP64 refinement, so its iterations are capped; the FP64 residual
+  // check decides whether another correction is needed
+  if (sizeof(Real) == 4 && cfg.max_iter > kMixedInnerMaxIter) cfg.max_iter = kMixedInnerMaxIter;
   cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
   cfg.fixed_d0 = fixed_d0 ? 1 : 0;
   cfg.counter = 0;
@@ -227,15 +232,20 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const
   const int nbv = cdiv(A.nb, 128);
   G2OC_K(K_PCG_INIT) pcg_init<BS><<<nbv, 128, 0, st>>>(A.nb, rhs, minv, r, s, xout, c->partials.p, c->pcg.p);
   G2OC_LAUNCH_CHECK();
-  constexpr int WT = 256;
-  const int nbw = cdiv(A.nb, WT / 32);
+  const bool wide = A.nnzb >= 64 * A.nb;  // dense-ish rows: 256 threads per row, else 32
   int chunk = 4;
   int launched = 0;
   for (;;) {
     for (int k = 0; k < chunk; ++k) {
-      G2OC_K(K_PCG_SPMV) pcg_rowpass<Real, BS, WT><<<nbw, WT, 0, st>>>(A, s, d0, d1, qrow, tbuf, c->pcg.p);
-      G2OC_K(K_PCG_COLPASS) pcg_colpass<Real, BS, WT><<<nbw, WT, 0, st>>>(A, d0, d1, qrow, tbuf, q, c->partials.p,
-                                                                          c->pcg.p);
+      if (wide) {
+        G2OC_K(K_PCG_SPMV) pcg_rowpass<Real, BS, 256><<<A.nb, 256, 0, st>>>(A, s, d0, d1, qrow, tbuf, c->pcg.p);
+        G2OC_K(K_PCG_COLPASS) pcg_colpass<Real, BS, 256><<<A.nb, 256, 0, st>>>(A, d0, d1, qrow, tbuf, q,
+                                                                                c->partials.p, c->pcg.p);
+      } else {
+        G2OC_K(K_PCG_SPMV) pcg_rowpass<Real, BS, 32><<<A.nb, 32, 0, st>>>(A, s, d0, d1, qrow, tbuf, c->pcg.p);
+        G2OC_K(K_PCG_COLPASS) pcg_colpass<Real, BS, 32><<<A.nb, 32, 0, st>>>(A, d0, d1, qrow, tbuf, q,
+                                                                              c->partials.p, c->pcg.p);
+      }
       G2OC_K(K_PCG_UPDATE) pcg_update<BS><<<nbv, 128, 0, st>>>(A.nb, minv, d0, d1, q, r, s, xout, c->partials.p,
                                                                c->pcg.p);
     }
@@ -286,7 +296,7 @@ template <typename Real>
 struct Engine final : EngineBase {
   g2oc_ctx* c;
   // Hessian
-  DBuf<Real> hpp, hll, hpl, bd, dinv, Sval, sysval;
+  DBuf<Real> hpp, hll, hpl, bdc, dinv, Sval, sysval;
   DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf;
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
   size_t schur_smem = 0;
@@ -304,8 +314,9 @@ struct Engine final : EngineBase {
       G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
       G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
       schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
-      stage_in_smem = schur_smem <= 200 * 1024;
-      if (!stage_in_smem) G2OC_TRY(bd.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
+      stage_in_smem = schur_smem <= 190 * 1024;
+      if (!stage_in_smem) schur_smem = 0;
+      if (!stage_in_smem) G2OC_TRY(bdc.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
       G2OC_TRY(c->db.alloc((size_t)S.Pf * 3 + 1));
     } else {
       G2OC_TRY(hcontrib.alloc((size_t)S.act.size() * 3 * pd * pd));
@@ -397,7 +408,7 @@ struct Engine final : EngineBase {
     cudaStream_t st = c->stream;
     if (S.Pf > 0) {
       G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
-          hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, stage_in_smem ? nullptr : bd.p, c->flag.p);
+          hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, dinv.p, nullptr, c->flag.p);
       G2OC_LAUNCH_CHECK();
     }
     if (S.Cf == 0) return G2OC_OK;
@@ -405,14 +416,14 @@ struct Engine final : EngineBase {
     const double* bp = c->b.p;
     const double* bl = c->b.p + (size_t)S.Cf * 6;
     if (stage_in_smem) {
-      auto kern = schur_rows<Real, true, T>;
+      auto kern = schur_rows<Real, T, true>;
       G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<S.Cf, T, schur_smem, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, nullptr, c->sys_rptr.p, c->sys_rcol.p,
+          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
     } else {
-      G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, false, T><<<S.Cf, T, 0, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bd.p, c->sys_rptr.p, c->sys_rcol.p,
+      G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false><<<S.Cf, T, 0, st>>>(
+          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
     }
     G2OC_LAUNCH_CHECK();
@@ -473,8 +484,8 @@ struct Engine final : EngineBase {
       G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, c->x.bytes(), st));
       if (S.ba && S.Pf > 0) {
         if (S.schur) {
-          G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, bd.p,
-                                                                 c->flag.p);
+          G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
+              hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, dinv.p, nullptr, c->flag.p);
           G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, c->b.p,
                                                              c->xs.p, c->x.p);
           G2OC_LAUNCH_CHECK();
@@ -497,39 +508,53 @@ struct Engine final : EngineBase {
         G2OC_LAUNCH_CHECK();
       }
       // mixed precision: FP64 iterative refinement on the true residual of
-      // the damped full system, r = b - (H + lambda I) x. A correction is
-      // solved only while the reduced residual's M-norm is above the d0 the
-      // first solve stopped at, i.e. while the FP32 storage of H / S / Dinv,
-      // not the PCG tolerance, limits the step.
+      // the damped normal equations, r = b - (J^T Om' J + lambda I) x, formed
+      // matrix-free from the edges in FP64. A correction is solved (FP32
+      // Schur + PCG, stopping at the d0 of the first solve) only while the
+      // reduced residual's M-norm is above that d0, i.e. while the FP32
+      // storage of H / S / Dinv, not the PCG tolerance, limits the step; a
+      // correction that raises the residual is undone and ends the loop.
       if (sizeof(Real) == 4 && ok && !use_chol) {
         const int n = c->vec_size();
-        for (int k = 0; k < c->prm.refine_max_iterations; ++k) {
+        double prev = -1.0;
+        for (int k = 0; k <= c->prm.refine_max_iterations; ++k) {
           double* rp = c->resid.p;
           double* rl = c->resid.p + (size_t)S.Cf * 6;
-          G2OC_K(K_RESID_CAM) ba_resid_cam<Real><<<cdiv(S.Cf, 4), 128, 0, st>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, S.Cf, hpl.p, hpp.p,
-                                                            lambda, bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
           if (S.Pf > 0)
-            G2OC_K(K_RESID_LM) ba_resid_lm<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, hll.p, lambda, bl,
-                                                               c->x.p, c->x.p + (size_t)S.Cf * 6, rl);
+            G2OC_K(K_RESID_LM) ba_resid64_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(
+                c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, c->pose_h.p, lambda, bl, c->x.p,
+                c->x.p + (size_t)S.Cf * 6, rl);
+          BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
+          G2OC_K(K_RESID_CAM) ba_resid64_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p, lambda,
+                                                                           bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
           G2OC_LAUNCH_CHECK();
           G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
-          G2OC_K(K_PCG_CHECK) pcg_check_dn<6><<<cdiv(S.Cf, 128), 128, 0, st>>>(S.Cf, minv.p, c->rhs.p, c->partials.p, c->pcg.p);
+          G2OC_K(K_PCG_CHECK) pcg_check_dn<6><<<cdiv(S.Cf, 128), 128, 0, st>>>(S.Cf, minv.p, c->rhs.p, c->partials.p,
+                                                                               c->pcg.p);
           G2OC_LAUNCH_CHECK();
           PcgState ps;
           G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
           G2OC_CUDA_TRY(cudaStreamSynchronize(st));
           c->last_refine_dn = ps.check_dn;
-          if (!(ps.check_dn > ps.d0)) break;
+          if (prev >= 0.0 && !(ps.check_dn < prev)) {
+            // the last correction did not reduce the true residual: undo it
+            G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, -1.0, n);
+            G2OC_LAUNCH_CHECK();
+            break;
+          }
+          if (!(ps.check_dn > ps.d0) || k == c->prm.refine_max_iterations) break;
+          prev = ps.check_dn;
           G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true, &it));
           it_total += it;
           c->refine_steps++;
           G2OC_CUDA_TRY(cudaMemcpyAsync(c->dx.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
           if (S.Pf > 0) {
-            G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, rl,
-                                                               c->xs.p, c->dx.p + (size_t)S.Cf * 6);
+            G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p,
+                                                                               dinv.p, rl, c->xs.p,
+                                                                               c->dx.p + (size_t)S.Cf * 6);
             G2OC_LAUNCH_CHECK();
           }
-          G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, n);
+          G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, 1.0, n);
           G2OC_LAUNCH_CHECK();
         }
       }
@@ -965,6 +990,8 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, S.C * sizeof(int), st));
   G2OC_TRY(c->free_pose.upload(S.free_pose_of_h, st));
   G2OC_TRY(c->free_point.upload(S.free_point_of_l, st));
+  G2OC_TRY(c->pose_h.upload(S.pose_h, st));
+  if (S.ba) G2OC_TRY(c->point_l.upload(S.point_l, st));
   if (S.ba) {
     std::vector<int2> ev(na), cv(S.c_edge.size());
     std::vector<double2> ez(na), cz(S.c_edge.size());
@@ -1001,6 +1028,9 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->hpl_col.upload(hcl, st));
     G2OC_TRY(c->hc_ptr.upload(S.hc_ptr, st));
     G2OC_TRY(c->hc_blk.upload(S.hc_blk, st));
+    std::vector<int> hcidx(S.hc_blk.size());
+    for (size_t p = 0; p < S.hc_blk.size(); ++p) hcidx[S.hc_blk[p]] = (int)p;
+    G2OC_TRY(c->hc_index.upload(hcidx, st));
     G2OC_TRY(c->s_pair_ptr.upload(S.s_pair_ptr, st));
     std::vector<int2> ab(S.s_pairs.size() / 2);
     for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.s_pairs[2 * i], S.s_pairs[2 * i + 1]);
@@ -1064,6 +1094,7 @@ int g2oc_get_hessian_info(g2oc_ctx* c, g2oc_hessian_info* info) {
   info->schur_nnzb = (int)(S.schur_rc.size() / 2);
   info->num_active_edges = (int)S.act.size();
   info->vector_size = c->vec_size();
+  info->schur_pairs = S.num_pairs;
   return G2OC_OK;
 }
 

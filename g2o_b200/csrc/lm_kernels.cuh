@@ -62,9 +62,9 @@ __global__ void sumsq_partials(const double* a, int n, double* partials) {
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-__global__ void axpy_kernel(double* y, const double* x, int n) {
+__global__ void axpy_kernel(double* y, const double* x, double a, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) y[i] += x[i];
+  if (i < n) y[i] += a * x[i];
 }
 
 template <typename Real, int BS>

@@ -153,21 +153,21 @@ __global__ void pcg_init(int nb, const double* b, const double* minv, double* r,
 
 // Row pass: d_k = s + beta d_{k-1} (ping-pong by parity of k), for row r
 // qrow_r = sum_c A(r,c) d_c, and per strictly-upper block T_b = A(r,c)^T d_r.
-// One warp per block row; lane j takes blocks j, j+32, ... of the row, and
-// with the row-SoA layout each entry load is coalesced across the warp.
+// One CTA per block row; thread t takes blocks t, t + THREADS, ... of the row
+// (with the row-SoA layout each entry load is coalesced across the warp),
+// then a fixed-order CTA reduction.
 template <typename Real, int BS, int THREADS>
 __global__ void __launch_bounds__(THREADS) pcg_rowpass(SysDev<Real> A, const double* s, double* d0buf,
                                                        double* d1buf, double* qrow, double* tbuf,
                                                        const PcgState* st) {
   if (st->done) return;
+  __shared__ double red[THREADS / 32][BS];
   const int k = st->k;
   const double beta = st->beta;
   double* dcur = (k & 1) ? d1buf : d0buf;
   const double* dprev = (k & 1) ? d0buf : d1buf;
   const bool use_prev = beta != 0.0;
-  const int lane = threadIdx.x & 31;
-  const int r = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
-  if (r >= A.nb) return;
+  const int r = blockIdx.x;
   auto dval = [&](int j, double* out) {
 #pragma unroll
     for (int c = 0; c < BS; ++c) {
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(THREADS) pcg_rowpass(SysDev<Real> A, const dou
   for (int a = 0; a < BS; ++a) acc[a] = 0.0;
   const int rb = A.rptr[r], nblk = A.rptr[r + 1] - rb;
   const Real* base = A.val + (size_t)rb * BS * BS;
-  for (int j = lane; j < nblk; j += 32) {
+  for (int j = threadIdx.x; j < nblk; j += THREADS) {
     const int c = A.rcol[rb + j];
     double dc[BS];
     dval(c, dc);
@@ -204,57 +204,48 @@ __global__ void __launch_bounds__(THREADS) pcg_rowpass(SysDev<Real> A, const dou
       for (int b = 0; b < BS; ++b) t[b] = tj[b];
     }
   }
+  block_sum_array<double, BS, THREADS>(acc, &red[0][0]);
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int a = 0; a < BS; ++a) acc[a] = warp_sum(acc[a]);
-  if (lane < BS) {
-    double qa = acc[0], da = dr[0];
-#pragma unroll
-    for (int a = 1; a < BS; ++a)
-      if (lane == a) {
-        qa = acc[a];
-        da = dr[a];
-      }
-    qrow[(size_t)r * BS + lane] = qa;
-    dcur[(size_t)r * BS + lane] = da;
+    for (int a = 0; a < BS; ++a) {
+      qrow[(size_t)r * BS + a] = acc[a];
+      dcur[(size_t)r * BS + a] = dr[a];
+    }
   }
 }
 
 // Column pass: q_c = qrow_c + sum over strictly-upper blocks (r, c) of T_b,
-// rows ascending; partial d.q; the last block sets alpha = dn / d.q.
+// rows in a fixed thread assignment; partial d.q; the last block sets
+// alpha = dn / d.q. One CTA per column.
 template <typename Real, int BS, int THREADS>
 __global__ void __launch_bounds__(THREADS) pcg_colpass(SysDev<Real> A, const double* d0buf, const double* d1buf,
                                                        const double* qrow, const double* tbuf, double* q,
                                                        double* partials, PcgState* st) {
   if (st->done) return;
+  __shared__ double red[THREADS / 32][BS];
   const int k = st->k;
   const double* dcur = (k & 1) ? d1buf : d0buf;
-  const int lane = threadIdx.x & 31;
-  const int c = blockIdx.x * (THREADS / 32) + (threadIdx.x >> 5);
-  double dot = 0.0;
-  if (c < A.nb) {
-    double acc[BS];
+  const int c = blockIdx.x;
+  double acc[BS];
 #pragma unroll
-    for (int a = 0; a < BS; ++a) acc[a] = 0.0;
-    const int p1 = A.cptr[c + 1];
-    for (int p = A.cptr[c] + lane; p < p1; p += 32) {
-      const double* t = tbuf + (size_t)A.cblk[p] * BS;
+  for (int a = 0; a < BS; ++a) acc[a] = 0.0;
+  const int p1 = A.cptr[c + 1];
+  for (int p = A.cptr[c] + threadIdx.x; p < p1; p += THREADS) {
+    const double* t = tbuf + (size_t)A.cblk[p] * BS;
 #pragma unroll
-      for (int a = 0; a < BS; ++a) acc[a] += t[a];
-    }
-#pragma unroll
-    for (int a = 0; a < BS; ++a) acc[a] = warp_sum(acc[a]);
-    if (lane < BS) {
-      double qa = acc[0];
-#pragma unroll
-      for (int a = 1; a < BS; ++a)
-        if (lane == a) qa = acc[a];
-      qa += qrow[(size_t)c * BS + lane];
-      q[(size_t)c * BS + lane] = qa;
-      dot = dcur[(size_t)c * BS + lane] * qa;
-    }
+    for (int a = 0; a < BS; ++a) acc[a] += t[a];
   }
-  dot = block_sum1(dot);
-  if (threadIdx.x == 0) partials[blockIdx.x] = dot;
+  block_sum_array<double, BS, THREADS>(acc, &red[0][0]);
+  double dot = 0.0;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int a = 0; a < BS; ++a) {
+      const double qa = acc[a] + qrow[(size_t)c * BS + a];
+      q[(size_t)c * BS + a] = qa;
+      dot += dcur[(size_t)c * BS + a] * qa;
+    }
+    partials[blockIdx.x] = dot;
+  }
   if (last_block_ticket(&st->counter)) {
     const double dq = sum_partials(partials, gridDim.x);
     if (threadIdx.x == 0) {

@@ -29,7 +29,7 @@ int main(void) {
   printf("g2oc_iteration_stats %zu\n", sizeof(g2oc_iteration_stats));
   F(g2oc_iteration_stats, chi2) F(g2oc_iteration_stats, time_iteration)
   printf("g2oc_hessian_info %zu\n", sizeof(g2oc_hessian_info));
-  F(g2oc_hessian_info, vector_size)
+  F(g2oc_hessian_info, vector_size) F(g2oc_hessian_info, schur_pairs)
   return 0;
 }
 """

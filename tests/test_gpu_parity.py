@@ -49,7 +49,7 @@ def test_ba_structure_is_bit_exact(backend, oracle_lib):
     g = small_ba()
     o, c = both(backend, oracle_lib, g)
     for f in ("num_free_poses", "num_free_points", "hpp_nnzb", "hpl_nnzb", "schur_nnzb", "num_active_edges",
-              "vector_size"):
+              "vector_size", "schur_pairs"):
         assert getattr(o.info, f) == getattr(c.info, f), f
     for a, b in zip(o.pattern(), c.pattern()):
         assert np.array_equal(a, b)
