@@ -62,6 +62,7 @@ def library() -> C.CDLL:
         "g2oc_set_estimates": ([vp, dp, dp], C.c_int),
         "g2oc_download": ([vp, dp, dp], C.c_int),
         "g2oc_optimize": ([vp, C.c_int, vp, C.POINTER(C.c_int)], C.c_int),
+        "g2oc_iterate": ([vp, C.c_int, vp, C.POINTER(C.c_int)], C.c_int),
         "g2oc_chi2": ([vp, dp, dp], C.c_int),
         "g2oc_errors": ([vp, dp], C.c_int),
         "g2oc_jacobians": ([vp, dp, dp], C.c_int),
@@ -210,6 +211,12 @@ class CudaProblem:
                 break
             out.append(stats[i].as_dict())
         return done.value, out
+
+    def iterate(self, iteration):
+        st = G2ocIterationStats()
+        res = C.c_int()
+        _check(library().g2oc_iterate(self._h, iteration, C.byref(st), C.byref(res)))
+        return res.value, st.as_dict()
 
     def chi2(self):
         a, b = C.c_double(), C.c_double()

@@ -1,0 +1,59 @@
+"""Command-line runner, the counterpart of g2o_cli's `-solver <name> -i <n>`
+(g2o/apps/g2o_cli/g2o.cpp:133-187) for the synthetic configurations:
+
+    python -m g2o_b200.cli --config ba --solver lm_cuda_pcg6_3 -i 20 [-stats]
+
+Prints one line per iteration with chi2, lambda, trial and PCG counts and the
+phase times (the fields of G2OBatchStatistics).
+"""
+import argparse
+import sys
+
+from . import backend, synth
+
+CONFIGS = {
+    "ba": lambda: synth.bundle_adjustment(),
+    "ba_small": lambda: synth.bundle_adjustment(num_cameras=100, num_points=20000, seed=99),
+    "pg2d": lambda: synth.pose_graph_2d(),
+    "pg3d": lambda: synth.pose_graph_3d(),
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--config", default="ba", choices=sorted(CONFIGS))
+    ap.add_argument("--solver", default="lm_cuda_pcg6_3")
+    ap.add_argument("-i", "--iterations", type=int, default=20)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("-stats", "--stats", action="store_true", help="print per-kernel launch counts and times")
+    ap.add_argument("--listSolvers", action="store_true")
+    a = ap.parse_args(argv)
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    if a.listSolvers:
+        print("\n".join(fac.list_solvers()))
+        return 0
+    params = fac.construct(a.solver)
+    if params is None:
+        print(f"unknown solver {a.solver}", file=sys.stderr)
+        return 1
+    g = CONFIGS[a.config]()
+    prob = backend.CudaProblem(g, params, device=a.device)
+    prob.set_kernel_timing(a.stats)
+    chi0, rchi0 = prob.chi2()
+    print(f"# {g.name}: {g.num_poses} poses, {g.num_points} points, {g.num_edges} edges; initial chi2 {rchi0:.6f}")
+    done, stats = prob.optimize(a.iterations)
+    for s in stats:
+        print(f"iteration= {s['iteration']}\t chi2= {s['chi2']:.6f}\t lambda= {s['lambda']:.6e}\t "
+              f"levenbergIter= {s['levenberg_iterations']}\t pcgIter= {s['iterations_linear_solver']}\t "
+              f"time= {s['time_iteration']:.6f}")
+    if a.stats:
+        total, ks = prob.kernel_stats()
+        print(f"# kernel launches: {total}")
+        for k, (n, ms) in sorted(ks.items(), key=lambda kv: -kv[1][1]):
+            print(f"#   {k:20s} {n:7d} {ms:10.3f} ms")
+    prob.close()
+    return 0 if done > 0 else 2
+
+
+if __name__ == "__main__":
+    sys.exit(main())

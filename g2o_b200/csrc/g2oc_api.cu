@@ -1190,6 +1190,35 @@ int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int*
   return G2OC_OK;
 }
 
+int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* result) {
+  G2OC_TRY(check_ctx(c, true));
+  if (iteration < 0 || !result) {
+    set_error("iteration < 0 or result is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (iteration == 0) G2OC_TRY(reset_pcg(c));
+  g2oc_iteration_stats stv;
+  memset(&stv, 0, sizeof(stv));
+  PhaseTimer tm(c->stream);
+  tm.start();
+  if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, iteration, &stv, result));
+  else G2OC_TRY(gn_iteration(c, iteration, &stv, result));
+  stv.iteration = iteration;
+  stv.result = *result;
+  if (stats) {
+    G2OC_TRY(chi2_to(c, nullptr, &c->sc.p->chi2_plain));
+    DevScalars h;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    stv.chi2 = h.chi2_plain;
+    if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) stv.lambda = h.lambda;
+  }
+  stv.time_iteration = tm.stop();
+  if (stats) *stats = stv;
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G2OC_OK;
+}
+
 int g2oc_chi2(g2oc_ctx* c, double* chi2, double* robust) {
   G2OC_TRY(check_ctx(c, true));
   G2OC_TRY(chi2_to(c, &c->sc.p->chi2_plain, &c->sc.p->chi2_temp));

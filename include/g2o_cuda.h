@@ -22,6 +22,7 @@
  *                                   (g2o/core/sparse_optimizer.cpp:393-455,
  *                                    g2o/core/optimization_algorithm_levenberg.cpp:60-153,
  *                                    g2o/core/optimization_algorithm_gauss_newton.cpp:48-93)
+ *   g2oc_iterate                    OptimizationAlgorithm::solve(iteration, online)
  *   g2oc_chi2 / g2oc_errors         computeActiveErrors + activeChi2 / activeRobustChi2
  *                                   (g2o/core/sparse_optimizer.cpp:78-130)
  *   g2oc_jacobians                  Edge::linearizeOplus (per-edge Jacobians)
@@ -202,6 +203,11 @@ int g2oc_restore_initial_estimates(g2oc_ctx* ctx);
 
 /* optimization: stats may be NULL, else iterations entries */
 int g2oc_optimize(g2oc_ctx* ctx, int iterations, g2oc_iteration_stats* stats, int* iterations_done);
+/* one outer iteration, OptimizationAlgorithm::solve(iteration, false): the
+   per-call form an adapter uses when SparseOptimizer::optimize drives the
+   loop. iteration == 0 starts a run (linear solver init, lambda init) as
+   g2oc_optimize does; stats may be NULL; *result gets G2OC_RESULT_*. */
+int g2oc_iterate(g2oc_ctx* ctx, int iteration, g2oc_iteration_stats* stats, int* result);
 
 /* parity hooks at the current estimate */
 int g2oc_chi2(g2oc_ctx* ctx, double* chi2, double* robust_chi2);

@@ -239,3 +239,31 @@ def test_not_positive_definite_is_reported(backend):
     vals = np.concatenate([np.eye(3).ravel(), 2 * np.eye(3).ravel(), np.eye(3).ravel()])
     st, _, _ = backend.solve_block_system(LINEAR_CHOLESKY, offs, rc, vals, np.ones(6))
     assert st == 4  # G2OC_ERR_NOT_PD
+
+
+def test_iterate_matches_optimize(backend):
+    g = small_ba(seed=9, cams=20, points=800)
+    a = backend.CudaProblem(g)
+    b = backend.CudaProblem(g)
+    _, sa = a.optimize(6)
+    for i in range(6):
+        res, st = b.iterate(i)
+        assert res == 1
+        assert st["chi2"] == sa[i]["chi2"]
+    pa, qa = a.estimates()
+    pb, qb = b.estimates()
+    assert np.array_equal(pa, pb) and np.array_equal(qa, qb)
+
+
+def test_factory_constructed_solver_runs(backend, oracle_lib):
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    g = synth.pose_graph_2d(num_poses=300, num_closures=100, seed=8)
+    opt = backend.SparseOptimizer()
+    opt.set_algorithm(fac.construct("gn_cuda"))
+    opt.set_graph(g.copy())
+    assert opt.initialize_optimization()
+    assert opt.optimize(5) == 5
+    o = oracle_lib.OracleProblem(g, oracle_lib.default_params(algorithm=ALGO_GAUSS_NEWTON,
+                                                              linear_solver=LINEAR_CHOLESKY))
+    o.optimize(5)
+    assert abs(opt.active_chi2() - o.chi2()[0]) <= 1e-8 * o.chi2()[0]
