@@ -14,7 +14,7 @@ HEADERS = ["g2oc_internal.h", "g2o_math.cuh", "reduce.cuh", "ba_kernels.cuh", "p
            "pg_kernels.cuh", "lm_kernels.cuh", "cholesky.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-fopenmp",
          "--expt-relaxed-constexpr", "-ccbin", "/usr/bin/g++"]
 
 
@@ -42,7 +42,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+    cmd = [NVCC] + ARCH + ["-shared", "-ccbin", "/usr/bin/g++", "-o", LIB] + objs + ["-lcudart", "-lgomp"]
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)

@@ -179,6 +179,89 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
   for (int i = 0; i < 3; ++i) b_l[(size_t)l * 3 + i] = bl[i];
 }
 
+// Landmark pass, edge-parallel form (graphs whose landmarks have at most 32
+// edges and whose (camera, landmark) pairs are unique): one warp per chunk of
+// whole landmarks (at most 32 edges, packed on the host), one lane per edge.
+// Edge loads are coalesced and each lane writes its own Hpl block (blocks
+// follow the edge order); H_ll and b_l are summed by a segmented warp scan
+// keyed by landmark (fixed shuffle order), written by the segment's last lane.
+template <typename Real>
+__global__ void ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, int nchunks, const int* e_lm,
+                                 Real* hll, Real* hpl, double* b_l) {
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ch >= nchunks) return;
+  const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
+  const int k = e0 + lane;
+  const bool act = k < e1;
+  Real H[6] = {0, 0, 0, 0, 0, 0};
+  double bl[3] = {0, 0, 0};
+  int key = -1 - lane;  // distinct for idle lanes
+  if (act) {
+    key = e_lm[k];
+    const int2 v = E.v[k];
+    const double4 om = E.om[k];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
+    double Jpd[6], Jcd[12];
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jpd, Jcd);
+    Real Jp[6], Jc[12];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) Jp[i] = (Real)Jpd[i];
+#pragma unroll
+    for (int i = 0; i < 12; ++i) Jc[i] = (Real)Jcd[i];
+    const double we0 = -w * (om.x * e[0] + om.y * e[1]);
+    const double we1 = -w * (om.y * e[0] + om.z * e[1]);
+    const Real o00 = (Real)(w * om.x), o01 = (Real)(w * om.y), o11 = (Real)(w * om.z);
+    Real A0[3], A1[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      A0[i] = Jp[i] * o00 + Jp[3 + i] * o01;
+      A1[i] = Jp[i] * o01 + Jp[3 + i] * o11;
+    }
+    H[0] = A0[0] * Jp[0] + A1[0] * Jp[3];
+    H[1] = A0[0] * Jp[1] + A1[0] * Jp[4];
+    H[2] = A0[0] * Jp[2] + A1[0] * Jp[5];
+    H[3] = A0[1] * Jp[1] + A1[1] * Jp[4];
+    H[4] = A0[1] * Jp[2] + A1[1] * Jp[5];
+    H[5] = A0[2] * Jp[2] + A1[2] * Jp[5];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bl[i] = Jpd[i] * we0 + Jpd[3 + i] * we1;
+    const int blk = E.hpl[k];
+    if (blk >= 0) {
+      Real* o = hpl + (size_t)blk * 18;
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[r * 3 + c] = Jc[r] * A0[c] + Jc[6 + r] * A1[c];
+    }
+  }
+  // segmented inclusive scan by landmark
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ko = __shfl_up_sync(0xffffffffu, key, off);
+    Real Ho[6];
+    double bo[3];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) Ho[i] = __shfl_up_sync(0xffffffffu, H[i], off);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bo[i] = __shfl_up_sync(0xffffffffu, bl[i], off);
+    if (lane >= off && ko == key) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) H[i] += Ho[i];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) bl[i] += bo[i];
+    }
+  }
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  if (act && (lane == 31 || knext != key)) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) hll[(size_t)key * 6 + i] = H[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) b_l[(size_t)key * 3 + i] = bl[i];
+  }
+}
+
 // Camera pass: one CTA per free camera sums H_pp = sum Jc^T Om' Jc (21 unique)
 // and b_p = sum Jc^T we over the camera's edges with a fixed-order block
 // reduction, and writes the full 6x6 block.
@@ -293,7 +376,7 @@ struct Vec2<float> {
 // layout of sys_offset.
 template <typename Real, int THREADS, bool STAGE>
 __global__ void __launch_bounds__(THREADS, 1)
-    schur_rows(const int* hc_ptr, const int* hc_blk, const int* hpl_col, const Real* hpl, const Real* dinv,
+    schur_rows(const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl, const Real* dinv,
                const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs, const int* s_hpp,
                const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l, double* bs) {
   using R2 = typename Vec2<Real>::T;
@@ -301,7 +384,6 @@ __global__ void __launch_bounds__(THREADS, 1)
   __shared__ double red[THREADS / 32][21];
   const int r = blockIdx.x;
   const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // the camera's BD_a = B_a Dinv_l blocks, one thread per block: staged in
   // shared memory, or (cameras with more blocks than shared memory holds)
   // written to the camera-major scratch bdc and read back in place
@@ -309,7 +391,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   for (int t = threadIdx.x; t < na; t += THREADS) {
     const int a = hc_blk[a0 + t];
     const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)a * 18);
-    const Real* Dl = dinv + (size_t)hpl_col[a] * 9;
+    const Real* Dl = dinv + (size_t)hc_col[a0 + t] * 9;
     Real b[18], D[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
@@ -367,22 +449,19 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
     }
   }
-  if (bs && warp == 0) {
+  if (bs) {
+    // reduced right-hand side, spread over the whole CTA (fixed assignment)
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int t = lane; t < na; t += 32) {
-      const double* bl = b_l + (size_t)hpl_col[hc_blk[a0 + t]] * 3;
+    for (int t = threadIdx.x; t < na; t += THREADS) {
+      const double* bl = b_l + (size_t)hc_col[a0 + t] * 3;
       const Real* D = BDa + (size_t)t * 18;
 #pragma unroll
       for (int q = 0; q < 6; ++q) acc[q] += (double)D[q * 3] * bl[0] + (double)D[q * 3 + 1] * bl[1] + (double)D[q * 3 + 2] * bl[2];
     }
+    block_sum_array<double, 6, THREADS>(acc, &red[0][0]);
+    if (threadIdx.x == 0) {
 #pragma unroll
-    for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
-    if (lane < 6) {
-      double v = acc[0];
-#pragma unroll
-      for (int q = 1; q < 6; ++q)
-        if (lane == q) v = acc[q];
-      bs[(size_t)r * 6 + lane] = b_p[(size_t)r * 6 + lane] - v;
+      for (int q = 0; q < 6; ++q) bs[(size_t)r * 6 + q] = b_p[(size_t)r * 6 + q] - acc[q];
     }
   }
   // off-diagonal blocks (the row's diagonal is its first block)

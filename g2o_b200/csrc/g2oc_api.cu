@@ -40,7 +40,8 @@ void set_error(const char* fmt, ...) {
 
 static inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-constexpr int kRedBlocks = 592;  // 4 x 148 SMs: fixed grid of the reductions
+constexpr int kRedBlocks = 592;    // 4 x 148 SMs: fixed grid of the reductions
+constexpr int kChi2Blocks = 2048;  // BA chi2: ~2 edges per thread for the 1M-edge graphs
 constexpr int kPcgChunkMax = 64;
 constexpr int kMixedInnerMaxIter = 256;
 
@@ -91,7 +92,7 @@ struct g2oc_ctx {
   g2oc::DBuf<int2> e_v, c_v;
   g2oc::DBuf<double2> e_z, c_z;
   g2oc::DBuf<double4> e_om, c_om;
-  g2oc::DBuf<int> e_hpl, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, hc_index, s_pair_ptr, s_hpp;
+  g2oc::DBuf<int> e_hpl, e_lm, lm_chunk_ptr, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, hc_col, hc_index, s_pair_ptr, s_hpp;
   g2oc::DBuf<int2> s_pairs;
   // pose-graph edges
   g2oc::DBuf<int2> pe_v;
@@ -345,6 +346,7 @@ struct Engine final : EngineBase {
     A.diag = c->sys_diag.p;
     A.cptr = c->sys_cptr.p;
     A.cblk = c->sys_cblk.p;
+    A.perm = c->sys_perm.p;
     A.val = val;
     return A;
   }
@@ -353,9 +355,15 @@ struct Engine final : EngineBase {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (S.ba) {
-      if (S.Pf > 0) {
-        G2OC_K(K_LANDMARK_PASS) ba_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf,
-                                                                 hll.p, hpl.p, c->b.p + (size_t)S.Cf * 6);
+      if (S.Pf > 0 && S.lm_warp_ok) {
+        const int nch = (int)S.lm_chunk_ptr.size() - 1;
+        G2OC_K(K_LANDMARK_PASS) ba_landmark_warp<Real><<<cdiv(nch, 8), 256, 0, st>>>(
+            c->ba_edges(), c->ba_vertices(), c->lm_chunk_ptr.p, nch, c->e_lm.p, hll.p, hpl.p,
+            c->b.p + (size_t)S.Cf * 6);
+        G2OC_LAUNCH_CHECK();
+      } else if (S.Pf > 0) {
+        G2OC_K(K_LANDMARK_PASS) ba_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
+            c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, hll.p, hpl.p, c->b.p + (size_t)S.Cf * 6);
         G2OC_LAUNCH_CHECK();
       }
       if (S.Cf > 0) {
@@ -419,11 +427,11 @@ struct Engine final : EngineBase {
       auto kern = schur_rows<Real, T, true>;
       G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<S.Cf, T, schur_smem, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
+          c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
     } else {
       G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false><<<S.Cf, T, 0, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
+          c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
     }
     G2OC_LAUNCH_CHECK();
@@ -639,12 +647,12 @@ struct Engine final : EngineBase {
 static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kRedBlocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   else G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   G2OC_LAUNCH_CHECK();
-  return finalize_sum(c, kRedBlocks, 2, out_plain, out_robust);
+  return finalize_sum(c, S.ba ? kChi2Blocks : kRedBlocks, 2, out_plain, out_robust);
 }
 
 static int oplus(g2oc_ctx* c) {
@@ -1013,6 +1021,10 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->e_om.upload(eo, st));
     G2OC_TRY(c->e_hpl.upload(S.e_hpl, st));
     G2OC_TRY(c->l_ptr.upload(S.l_ptr, st));
+    if (S.lm_warp_ok) {
+      G2OC_TRY(c->e_lm.upload(S.e_lm, st));
+      G2OC_TRY(c->lm_chunk_ptr.upload(S.lm_chunk_ptr, st));
+    }
     G2OC_TRY(c->c_ptr.upload(S.c_ptr, st));
     G2OC_TRY(c->c_v.upload(cv, st));
     G2OC_TRY(c->c_z.upload(cz, st));
@@ -1028,9 +1040,13 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->hpl_col.upload(hcl, st));
     G2OC_TRY(c->hc_ptr.upload(S.hc_ptr, st));
     G2OC_TRY(c->hc_blk.upload(S.hc_blk, st));
-    std::vector<int> hcidx(S.hc_blk.size());
-    for (size_t p = 0; p < S.hc_blk.size(); ++p) hcidx[S.hc_blk[p]] = (int)p;
+    std::vector<int> hcidx(S.hc_blk.size()), hccol(S.hc_blk.size());
+    for (size_t p = 0; p < S.hc_blk.size(); ++p) {
+      hcidx[S.hc_blk[p]] = (int)p;
+      hccol[p] = S.hpl_rc[2 * (size_t)S.hc_blk[p] + 1];
+    }
     G2OC_TRY(c->hc_index.upload(hcidx, st));
+    G2OC_TRY(c->hc_col.upload(hccol, st));
     G2OC_TRY(c->s_pair_ptr.upload(S.s_pair_ptr, st));
     std::vector<int2> ab(S.s_pairs.size() / 2);
     for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.s_pairs[2 * i], S.s_pairs[2 * i + 1]);
@@ -1381,7 +1397,9 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
   const int n = nb * bs;
   G2OC_TRY(rhs.upload(std::vector<double>(b, b + n), st));
   G2OC_TRY(xo.alloc(n));
-  SysDev<double> A{nb, nnzb, rp.p, rcl.p, brw.p, dg.p, cp.p, cb.p, val.p};
+  DBuf<int> pm;
+  G2OC_TRY(pm.upload(tmp.sys_perm, st));
+  SysDev<double> A{nb, nnzb, rp.p, rcl.p, brw.p, dg.p, cp.p, cb.p, pm.p, val.p};
   int it = 0, ok = 1;
   if (linear_solver == G2OC_LINEAR_CHOLESKY) {
     CholPlan P;
@@ -1395,7 +1413,7 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
     G2OC_TRY(d1.alloc(n));
     G2OC_TRY(q.alloc(n));
     G2OC_TRY(qrow.alloc(n));
-    G2OC_TRY(tb.alloc((size_t)nnzb * bs));
+    G2OC_TRY(tb.alloc((size_t)nnzb * bs + 1));
     G2OC_TRY(reset_pcg(c));
     if (bs == 3) {
       G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<double, 3><<<cdiv(nb, 128), 128, 0, st>>>(A, mi.p, c->flag.p);

@@ -97,6 +97,9 @@ struct Structure {
   std::vector<int> c_edge;              // camera-major -> device edge
   std::vector<int> hc_ptr, hc_blk;      // Cf + 1 / hpl_nnzb: Hpl blocks by camera row
   std::vector<int> hc_pos;              // per Hpl block: position in its camera's list
+  bool lm_warp_ok = false;              // landmarks <= 32 edges, unique (camera, landmark) pairs
+  std::vector<int> lm_chunk_ptr;        // chunks of whole landmarks, <= 32 edges each
+  std::vector<int> e_lm;                // per device edge of a free landmark: the landmark
   int max_blocks_per_cam = 0;
   // Schur pairs per Schur block in the internal (row-major) order: the
   // co-observing (a, b) pairs of BD_a B_b^T, a as a position in row r's

@@ -33,6 +33,9 @@ struct SysDev {
   const int* diag;   // per row: block of the diagonal
   const int* cptr;   // nb + 1: strictly-upper blocks of column c
   const int* cblk;   //         (block indices, rows ascending)
+  const int* perm;   // per block: index in the column-major pattern (diagonal
+                     // last in each column), where the transposed
+                     // contribution of the block is stored
   const Real* val;   // block values, row-SoA layout (sys_offset)
 };
 
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(THREADS) pcg_rowpass(SysDev<Real> A, const dou
         tj[b] += m * dr[i];
       }
     if (c != r) {
-      double* t = tbuf + (size_t)(rb + j) * BS;
+      double* t = tbuf + (size_t)A.perm[rb + j] * BS;
 #pragma unroll
       for (int b = 0; b < BS; ++b) t[b] = tj[b];
     }
@@ -229,9 +232,11 @@ __global__ void __launch_bounds__(THREADS) pcg_colpass(SysDev<Real> A, const dou
   double acc[BS];
 #pragma unroll
   for (int a = 0; a < BS; ++a) acc[a] = 0.0;
-  const int p1 = A.cptr[c + 1];
-  for (int p = A.cptr[c] + threadIdx.x; p < p1; p += THREADS) {
-    const double* t = tbuf + (size_t)A.cblk[p] * BS;
+  // column c's strictly-upper blocks sit contiguously at column-major
+  // positions [cptr[c] + c, cptr[c + 1] + c) (one diagonal per earlier column)
+  const int p0 = A.cptr[c] + c, p1 = A.cptr[c + 1] + c;
+  for (int p = p0 + threadIdx.x; p < p1; p += THREADS) {
+    const double* t = tbuf + (size_t)p * BS;
 #pragma unroll
     for (int a = 0; a < BS; ++a) acc[a] += t[a];
   }

@@ -9,6 +9,10 @@
 #include <cstdio>
 #include <numeric>
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 #include "g2oc_internal.h"
 
 namespace g2oc {
@@ -66,22 +70,22 @@ void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s) {
   const int nnzb = (int)(rc.size() / 2);
   s.sys_nb = nb;
   s.sys_nnzb = nnzb;
-  // internal order: by (row, col); the column-major pattern lists (col, row)
-  std::vector<uint64_t> keys(nnzb);
-  for (int k = 0; k < nnzb; ++k) keys[k] = (uint64_t)rc[2 * k] * (uint64_t)nb + (uint64_t)rc[2 * k + 1];
-  std::vector<uint32_t> perm;
-  radix_sort(keys, perm);
-  s.sys_perm.assign(perm.begin(), perm.end());
-  s.sys_rptr.assign(nb + 1, 0);
+  // internal order = (row, col): a stable counting sort of the column-major
+  // list by row keeps the columns ascending inside each row
+  std::vector<int> rkey(nnzb), order;
+  for (int k = 0; k < nnzb; ++k) rkey[k] = rc[2 * k];
+  counting_sort(rkey, nb, order, s.sys_rptr);
+  s.sys_perm.assign(order.begin(), order.end());
   s.sys_rcol.resize(nnzb);
   s.sys_brow.resize(nnzb);
   s.sys_diag.assign(nb, -1);
   std::vector<int> ckey;
   std::vector<int> cidx;
+  ckey.reserve(nnzb);
+  cidx.reserve(nnzb);
   for (int k = 0; k < nnzb; ++k) {
-    const int p = (int)perm[k];
+    const int p = order[k];
     const int r = rc[2 * p], c = rc[2 * p + 1];
-    s.sys_rptr[r + 1]++;
     s.sys_rcol[k] = c;
     s.sys_brow[k] = r;
     if (r == c) s.sys_diag[r] = k;
@@ -90,11 +94,10 @@ void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s) {
       cidx.push_back(k);
     }
   }
-  for (int i = 0; i < nb; ++i) s.sys_rptr[i + 1] += s.sys_rptr[i];
-  std::vector<int> order;
-  counting_sort(ckey, nb, order, s.sys_cptr);
-  s.sys_cblk.resize(order.size());
-  for (size_t i = 0; i < order.size(); ++i) s.sys_cblk[i] = cidx[order[i]];
+  std::vector<int> corder;
+  counting_sort(ckey, nb, corder, s.sys_cptr);
+  s.sys_cblk.resize(corder.size());
+  for (size_t i = 0; i < corder.size(); ++i) s.sys_cblk[i] = cidx[corder[i]];
 }
 
 static int build_ba(const g2oc_graph* g, Structure& s) {
@@ -134,23 +137,46 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
   s.Pf = (int)s.free_point_of_l.size();
   s.schur = s.Pf > 0;
   const int na = (int)s.act.size();
-  // device order: (point fixed?, point, camera, insertion)
-  std::vector<int> key(na), ord1, ord2, ptr;
-  for (int k = 0; k < na; ++k) key[k] = g->edge_vertex[2 * s.act[k] + 1];
-  counting_sort(key, C, ord1, ptr);
-  std::vector<int> key2(na);
+  // device order: (point fixed?, point, camera, insertion). Graphs built
+  // point by point with ascending cameras (as g2o's ba_demo does) are already
+  // in that order; detect it and skip the sorts.
+  std::vector<int> key2(na), ptr;
   for (int k = 0; k < na; ++k) {
-    const int v0 = g->edge_vertex[2 * s.act[ord1[k]]];
+    const int v0 = g->edge_vertex[2 * s.act[k]];
     const int l = s.point_l[v0];
     key2[k] = l >= 0 ? l : s.Pf + v0;
   }
-  counting_sort(key2, s.Pf + P, ord2, ptr);
+  bool sorted = true;
+  for (int k = 1; k < na && sorted; ++k) {
+    if (key2[k] < key2[k - 1]) sorted = false;
+    else if (key2[k] == key2[k - 1] && g->edge_vertex[2 * s.act[k] + 1] < g->edge_vertex[2 * s.act[k - 1] + 1])
+      sorted = false;
+  }
   s.dev_edge.resize(na);
   s.dev_of_act.resize(na);
-  for (int k = 0; k < na; ++k) {
-    const int a = ord1[ord2[k]];
-    s.dev_edge[k] = s.act[a];
-    s.dev_of_act[a] = k;
+  if (sorted) {
+    ptr.assign(s.Pf + P + 1, 0);
+    for (int k = 0; k < na; ++k) ptr[key2[k] + 1]++;
+    for (int i = 0; i < s.Pf + P; ++i) ptr[i + 1] += ptr[i];
+    for (int k = 0; k < na; ++k) {
+      s.dev_edge[k] = s.act[k];
+      s.dev_of_act[k] = k;
+    }
+  } else {
+    std::vector<int> key(na), ord1, ord2;
+    for (int k = 0; k < na; ++k) key[k] = g->edge_vertex[2 * s.act[k] + 1];
+    counting_sort(key, C, ord1, ptr);
+    for (int k = 0; k < na; ++k) {
+      const int v0 = g->edge_vertex[2 * s.act[ord1[k]]];
+      const int l = s.point_l[v0];
+      key2[k] = l >= 0 ? l : s.Pf + v0;
+    }
+    counting_sort(key2, s.Pf + P, ord2, ptr);
+    for (int k = 0; k < na; ++k) {
+      const int a = ord1[ord2[k]];
+      s.dev_edge[k] = s.act[a];
+      s.dev_of_act[a] = k;
+    }
   }
   s.l_ptr.assign(ptr.begin(), ptr.begin() + s.Pf + 1);
   // Hpl blocks (column-major over (landmark, camera)); duplicates share a block
@@ -172,6 +198,31 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     s.hb_ptr[l + 1] = (int)(s.hpl_rc.size() / 2);
   }
   const int nhpl = (int)(s.hpl_rc.size() / 2);
+  // warp chunks for the edge-parallel landmark pass
+  {
+    bool ok = true;
+    for (int l = 0; l < s.Pf && ok; ++l) {
+      if (s.l_ptr[l + 1] - s.l_ptr[l] > 32) ok = false;
+      for (int k = s.l_ptr[l] + 1; k < s.l_ptr[l + 1] && ok; ++k)
+        if (s.e_hpl[k] >= 0 && s.e_hpl[k] == s.e_hpl[k - 1]) ok = false;
+    }
+    s.lm_warp_ok = ok && s.Pf > 0;
+    s.lm_chunk_ptr.clear();
+    s.e_lm.clear();
+    if (s.lm_warp_ok) {
+      s.e_lm.resize(s.l_ptr[s.Pf]);
+      s.lm_chunk_ptr.push_back(0);
+      int start = 0;
+      for (int l = 0; l < s.Pf; ++l) {
+        for (int k = s.l_ptr[l]; k < s.l_ptr[l + 1]; ++k) s.e_lm[k] = l;
+        if (s.l_ptr[l + 1] - start > 32) {
+          s.lm_chunk_ptr.push_back(s.l_ptr[l]);
+          start = s.l_ptr[l];
+        }
+      }
+      s.lm_chunk_ptr.push_back(s.l_ptr[s.Pf]);
+    }
+  }
   // camera-major edge list over free cameras
   {
     std::vector<int> ck, idx;
@@ -211,66 +262,125 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     for (int p = s.hc_ptr[h]; p < s.hc_ptr[h + 1]; ++p) s.hc_pos[s.hc_blk[p]] = p - s.hc_ptr[h];
   }
   // Schur pattern: Hpp pattern + co-observing pose pairs (block_solver.hpp:229-266),
-  // with the pair list of each block in landmark order
+  // with the pair list of each off-diagonal block in landmark order. The
+  // diagonal block of each camera is formed from the camera's own Hpl blocks
+  // (no pair list). Rows are bucketed by a counting sort (landmark order kept),
+  // then each row is sorted by column with a stable counting sort.
   s.schur_rc.clear();
   s.s_pair_ptr.clear();
   s.s_pairs.clear();
   s.s_hpp.clear();
+  s.num_pairs = 0;
   if (s.schur) {
-    int64_t np = 0;
-    for (int l = 0; l < s.Pf; ++l) {
-      const int64_t m = s.hb_ptr[l + 1] - s.hb_ptr[l];
-      np += m * (m + 1) / 2;
-    }
-    s.num_pairs = np;
-    const uint64_t Cf = (uint64_t)s.Cf;
-    std::vector<uint64_t> keys;  // row-major: r * Cf + c
-    keys.reserve(np + s.Cf);
-    std::vector<int32_t> pa2;
-    pa2.reserve(2 * np);
+    const int Cf = s.Cf;
+    std::vector<int64_t> rcount(Cf + 1, 0);
     for (int l = 0; l < s.Pf; ++l)
-      for (int a = s.hb_ptr[l]; a < s.hb_ptr[l + 1]; ++a)
-        for (int b = a; b < s.hb_ptr[l + 1]; ++b) {
-          const uint64_t r = (uint64_t)s.hpl_rc[2 * a], c = (uint64_t)s.hpl_rc[2 * b];
-          keys.push_back(r * Cf + c);
-          pa2.push_back(s.hc_pos[a]);
-          pa2.push_back(b);
+      for (int a = s.hb_ptr[l]; a < s.hb_ptr[l + 1]; ++a) rcount[s.hpl_rc[2 * a] + 1] += s.hb_ptr[l + 1] - a - 1;
+    for (int h = 0; h < Cf; ++h) rcount[h + 1] += rcount[h];
+    const int64_t np = rcount[Cf];
+    s.num_pairs = np;
+    std::vector<int32_t> pc(np), pa(np), pb(np);  // column, a (position in row camera list), b
+    {
+      // parallel bucketing: landmark chunks in order, each chunk writes its
+      // own slice of every row, so each row stays in landmark order
+#ifdef _OPENMP
+      const int nt = std::max(1, std::min(omp_get_max_threads(), 32));
+#else
+      const int nt = 1;
+#endif
+      std::vector<int64_t> cnt((size_t)nt * Cf, 0);
+      auto chunk = [&](int t, int& l0, int& l1) {
+        l0 = (int)((int64_t)s.Pf * t / nt);
+        l1 = (int)((int64_t)s.Pf * (t + 1) / nt);
+      };
+#pragma omp parallel for num_threads(nt)
+      for (int t = 0; t < nt; ++t) {
+        int l0, l1;
+        chunk(t, l0, l1);
+        int64_t* ct = cnt.data() + (size_t)t * Cf;
+        for (int l = l0; l < l1; ++l)
+          for (int a = s.hb_ptr[l]; a < s.hb_ptr[l + 1]; ++a) ct[s.hpl_rc[2 * a]] += s.hb_ptr[l + 1] - a - 1;
+      }
+      std::vector<int64_t> start((size_t)nt * Cf);
+      for (int r = 0; r < Cf; ++r) {
+        int64_t o = rcount[r];
+        for (int t = 0; t < nt; ++t) {
+          start[(size_t)t * Cf + r] = o;
+          o += cnt[(size_t)t * Cf + r];
         }
-    for (int h = 0; h < s.Cf; ++h) keys.push_back((uint64_t)h * Cf + h);  // diagonal markers (no pair)
-    std::vector<uint32_t> perm;
-    radix_sort(keys, perm);
-    s.s_pairs.reserve(2 * np);
-    std::vector<int32_t> rm_rc;  // internal (row-major) blocks
-    s.s_pair_ptr.push_back(0);
-    uint64_t prev = ~0ull;
-    for (size_t i = 0; i < keys.size(); ++i) {
-      if (keys[i] != prev) {
-        if (prev != ~0ull) s.s_pair_ptr.push_back((int)(s.s_pairs.size() / 2));
-        prev = keys[i];
-        const int r = (int)(keys[i] / Cf), c = (int)(keys[i] % Cf);
-        rm_rc.push_back(r);
-        rm_rc.push_back(c);
-        s.s_hpp.push_back(r == c ? s.hpp_diag[r] : -1);
       }
-      const uint32_t p = perm[i];
-      if (p < (uint32_t)np) {
-        s.s_pairs.push_back(pa2[2 * (size_t)p]);
-        s.s_pairs.push_back(pa2[2 * (size_t)p + 1]);
+#pragma omp parallel for num_threads(nt)
+      for (int t = 0; t < nt; ++t) {
+        int l0, l1;
+        chunk(t, l0, l1);
+        int64_t* pos = start.data() + (size_t)t * Cf;
+        for (int l = l0; l < l1; ++l)
+          for (int a = s.hb_ptr[l]; a < s.hb_ptr[l + 1]; ++a) {
+            const int r = s.hpl_rc[2 * a];
+            for (int b = a + 1; b < s.hb_ptr[l + 1]; ++b) {
+              const int64_t q = pos[r]++;
+              pc[q] = s.hpl_rc[2 * b];
+              pa[q] = s.hc_pos[a];
+              pb[q] = b;
+            }
+          }
       }
     }
-    s.s_pair_ptr.push_back((int)(s.s_pairs.size() / 2));
-    // column-major pattern (the order of SparseBlockMatrix::blockCols)
-    const size_t nS = rm_rc.size() / 2;
-    std::vector<uint64_t> ck(nS);
-    for (size_t k = 0; k < nS; ++k) ck[k] = (uint64_t)rm_rc[2 * k + 1] * Cf + (uint64_t)rm_rc[2 * k];
-    std::vector<uint32_t> cperm;
-    radix_sort(ck, cperm);
-    s.schur_rc.resize(2 * nS);
-    for (size_t i = 0; i < nS; ++i) {
-      s.schur_rc[2 * i] = rm_rc[2 * (size_t)cperm[i]];
-      s.schur_rc[2 * i + 1] = rm_rc[2 * (size_t)cperm[i] + 1];
+    // per row: stable counting sort by column; blocks = diagonal + distinct columns
+    std::vector<std::vector<int32_t>> row_cols(Cf);
+    std::vector<std::vector<int32_t>> row_cnt(Cf);
+    std::vector<int32_t> sp(2 * np);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int r = 0; r < Cf; ++r) {
+      const int64_t q0 = rcount[r], q1 = rcount[r + 1];
+      std::vector<int32_t> cnt(Cf - r + 1, 0);
+      for (int64_t q = q0; q < q1; ++q) cnt[pc[q] - r + 1]++;
+      std::vector<int32_t>& cols = row_cols[r];
+      std::vector<int32_t>& cc = row_cnt[r];
+      for (int c = r + 1; c < Cf; ++c)
+        if (cnt[c - r + 1]) {
+          cols.push_back(c);
+          cc.push_back(cnt[c - r + 1]);
+        }
+      for (int c = 1; c <= Cf - r; ++c) cnt[c] += cnt[c - 1];
+      for (int64_t q = q0; q < q1; ++q) {
+        const int64_t d = q0 + cnt[pc[q] - r]++;
+        sp[2 * d] = pa[q];
+        sp[2 * d + 1] = pb[q];
+      }
     }
-    build_sym_lists(s.Cf, s.schur_rc, s);  // internal order = row-major = the order above
+    s.s_pairs.swap(sp);
+    // internal (row-major) blocks: per row the diagonal, then the columns
+    std::vector<int32_t> rm;
+    std::vector<int> ptr;
+    ptr.push_back(0);
+    int64_t acc = 0;
+    for (int r = 0; r < Cf; ++r) {
+      rm.push_back(r);
+      rm.push_back(r);
+      s.s_hpp.push_back(s.hpp_diag[r]);
+      ptr.push_back((int)acc);  // the diagonal has no pair list
+      for (size_t i = 0; i < row_cols[r].size(); ++i) {
+        rm.push_back(r);
+        rm.push_back(row_cols[r][i]);
+        s.s_hpp.push_back(-1);
+        acc += row_cnt[r][i];
+        ptr.push_back((int)acc);
+      }
+    }
+    s.s_pair_ptr.swap(ptr);
+    // column-major pattern (the order of SparseBlockMatrix::blockCols):
+    // stable counting sort of the row-major list by column
+    const int nS = (int)(rm.size() / 2);
+    std::vector<int> ckey(nS), corder, cptr;
+    for (int k = 0; k < nS; ++k) ckey[k] = rm[2 * k + 1];
+    counting_sort(ckey, Cf, corder, cptr);
+    s.schur_rc.resize(2 * (size_t)nS);
+    for (int i = 0; i < nS; ++i) {
+      s.schur_rc[2 * i] = rm[2 * (size_t)corder[i]];
+      s.schur_rc[2 * i + 1] = rm[2 * (size_t)corder[i] + 1];
+    }
+    build_sym_lists(Cf, s.schur_rc, s);  // internal order = the row-major order above
   } else {
     build_sym_lists(s.Cf, s.hpp_rc, s);
   }
