@@ -161,7 +161,7 @@ typedef struct g2oc_hessian_info {
   int32_t schur_nnzb;       /* upper blocks incl. diagonal, 0 without Schur */
   int32_t num_active_edges;
   int64_t vector_size;      /* Solver::vectorSize() */
-  int64_t schur_pairs;      /* co-observing Hpl block pairs summed into the Schur blocks */
+  int64_t schur_pairs;      /* co-observing Hpl block pairs (a < b) summed into off-diagonal Schur blocks */
 } g2oc_hessian_info;
 
 /* per-kernel launch count and (when timing is on) summed CUDA-event time */

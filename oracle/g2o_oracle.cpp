@@ -1484,10 +1484,11 @@ int orc_get_hessian_info(orc_problem* p, g2oc_hessian_info* info) {
   info->schur_nnzb = (int)p->schur_rc.size();
   info->num_active_edges = (int)p->act.size();
   info->vector_size = (int64_t)p->b.size();
+  // co-observing Hpl block pairs (a < b) of the off-diagonal Schur blocks
   int64_t np = 0;
   for (int l = 0; l < p->Pf; ++l) {
     const int64_t m = p->hpl_col_ptr[l + 1] - p->hpl_col_ptr[l];
-    np += m * (m + 1) / 2;
+    np += m * (m - 1) / 2;
   }
   info->schur_pairs = np;
   return G2OC_OK;
