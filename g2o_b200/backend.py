@@ -76,6 +76,8 @@ def library() -> C.CDLL:
         "g2oc_restore_initial_estimates": ([vp], C.c_int),
         "g2oc_set_kernel_timing": ([vp, C.c_int], C.c_int),
         "g2oc_get_kernel_stats": ([vp, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)], C.c_int),
+        "g2oc_solve_block_system_static": ([C.c_int, C.c_int32, C.c_int32, C.c_int32, ip, dp, dp, dp, C.c_double,
+                                            C.c_int32, ip], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libg2o_b200.so")
-SOURCES = ["g2oc_api.cu", "structure.cpp"]
+SOURCES = ["g2oc_api.cu", "noalloc.cu", "structure.cpp"]
 HEADERS = ["g2oc_internal.h", "g2o_math.cuh", "reduce.cuh", "ba_kernels.cuh", "pcg_kernels.cuh",
            "pg_kernels.cuh", "lm_kernels.cuh", "cholesky.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

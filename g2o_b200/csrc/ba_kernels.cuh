@@ -62,7 +62,7 @@ __device__ __forceinline__ void ba_edge_error(const BAVertices& V, int2 v, doubl
 
 // computeActiveErrors + activeChi2 / activeRobustChi2
 // (g2o/core/sparse_optimizer.cpp:78-130): partials[2*block] = (chi2, robust)
-__global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials) {
+static __global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials) {
   double c = 0.0, r = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n; k += gridDim.x * blockDim.x) {
     double e[2], Xc[3], chi2, w;
@@ -81,7 +81,7 @@ __global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials) {
 }
 
 // per-edge errors (parity hook)
-__global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
+static __global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= E.n) return;
   double e[2], Xc[3], chi2, w;
@@ -91,7 +91,7 @@ __global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
 }
 
 // per-edge Jacobians in FP64 (parity hook): Jp 2x3, Jc 2x6
-__global__ void ba_jacobians_kernel(BAEdges E, BAVertices V, double* jp, double* jc) {
+static __global__ void ba_jacobians_kernel(BAEdges E, BAVertices V, double* jp, double* jc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= E.n) return;
   const int2 v = E.v[k];
@@ -575,7 +575,7 @@ __global__ void ba_backsub(const int* hb_ptr, const int* hpl_row, int Pf, const 
 // mixed-precision refinement, r = b - (J^T Om' J + lambda I) x, with the
 // Jacobians recomputed in FP64 from the edges (no FP32 Hessian involved).
 // Landmark side: one thread per free landmark over its edges.
-__global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l_ptr, int Pf, const int* pose_h,
+static __global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l_ptr, int Pf, const int* pose_h,
                                     double lambda, const double* b_l, const double* x_p, const double* x_l,
                                     double* r_l) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(THREADS) ba_resid64_camera(BACamEdges CE, BAVe
 // SparseOptimizer::update (sparse_optimizer.cpp:457-468) with
 // VertexSE3Expmap::oplusImpl (g2o/types/sba/vertex_se3_expmap.cpp:48-51):
 // T <- exp(dx) * T; VertexPointXYZ: p <- p + dx (vertex_pointxyz.h:47-50)
-__global__ void ba_oplus(BAVertices V, int Cf, int Pf, const double* x, int* nonfinite) {
+static __global__ void ba_oplus(BAVertices V, int Cf, int Pf, const double* x, int* nonfinite) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < Cf) {
     double u[6];

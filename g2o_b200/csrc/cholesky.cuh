@@ -169,7 +169,7 @@ __global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int
 }
 
 // factor the diagonal tile k in shared memory (lower)
-__global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
+static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
   __shared__ double T[kTile][kTile + 1];
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int*
 // panel: L(i,k) = A(i,k) L(k,k)^-T for the listed tiles i
 constexpr int kTileSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
 
-__global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
+static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
   extern __shared__ double sm_trsm[];
   double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
   double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const
 }
 
 // trailing update: A(i,j) -= L(i,k) L(j,k)^T for the listed pairs; 4x4 per thread
-__global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
+static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
   extern __shared__ double sm_gemm[];
   double (*Li)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm);
   double (*Lj)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm + kTile * (kTile + 1));
@@ -275,19 +275,19 @@ __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const
 }
 
 // permuted right-hand side y(perm) = b
-__global__ void chol_load_rhs(const double* b, const int* perm, int nb, int bs, int n, int np, double* y) {
+static __global__ void chol_load_rhs(const double* b, const int* perm, int nb, int bs, int n, int np, double* y) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) y[perm[t / bs] * bs + t % bs] = b[t];
   else if (t < np) y[t] = 0.0;
 }
 
-__global__ void chol_store_x(const double* y, const int* perm, int bs, int n, double* x) {
+static __global__ void chol_store_x(const double* y, const int* perm, int bs, int n, double* x) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < n) x[t] = y[perm[t / bs] * bs + t % bs];
 }
 
 // L(k,k) y_k = y_k
-__global__ void chol_fwd_diag(const double* A, int np, int k, double* y) {
+static __global__ void chol_fwd_diag(const double* A, int np, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
   if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
@@ -304,7 +304,7 @@ __global__ void chol_fwd_diag(const double* A, int np, int k, double* y) {
 }
 
 // y_i -= L(i,k) y_k for the listed tiles i > k
-__global__ void chol_fwd_update(const double* A, int np, int k, const int* tiles, double* y) {
+static __global__ void chol_fwd_update(const double* A, int np, int k, const int* tiles, double* y) {
   const int ti = tiles[blockIdx.x];
   const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
   __shared__ double yk[kTile];
@@ -319,7 +319,7 @@ __global__ void chol_fwd_update(const double* A, int np, int k, const int* tiles
 }
 
 // L(k,k)^T x_k = y_k
-__global__ void chol_bwd_diag(const double* A, int np, int k, double* y) {
+static __global__ void chol_bwd_diag(const double* A, int np, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
   if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
@@ -336,7 +336,7 @@ __global__ void chol_bwd_diag(const double* A, int np, int k, double* y) {
 }
 
 // y_i -= L(k,i)^T y_k for the listed tiles i < k
-__global__ void chol_bwd_update(const double* A, int np, int k, const int* tiles, double* y) {
+static __global__ void chol_bwd_update(const double* A, int np, int k, const int* tiles, double* y) {
   const int ti = tiles[blockIdx.x];
   const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
   __shared__ double yk[kTile];

@@ -10,7 +10,7 @@
 namespace g2oc {
 
 // lambda_0 = initialLambda if set, else tau * max diag(H); ni = 2
-__global__ void lm_init_lambda(DevScalars* sc, double user_lambda, double tau) {
+static __global__ void lm_init_lambda(DevScalars* sc, double user_lambda, double tau) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     sc->lambda = user_lambda > 0.0 ? user_lambda : tau * sc->max_diag;
     sc->ni = 2.0;
@@ -20,7 +20,7 @@ __global__ void lm_init_lambda(DevScalars* sc, double user_lambda, double tau) {
 // One trial's decision. rho = (chi_current - chi_temp) / (scale + 1e-3);
 // accept: lambda *= max(1/3, min(2/3, 1 - (2 rho - 1)^3)), ni = 2;
 // reject: lambda *= ni, ni *= 2 (estimates restored by the host).
-__global__ void lm_decide(DevScalars* sc) {
+static __global__ void lm_decide(DevScalars* sc) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const bool ok2 = sc->solve_ok != 0;
   double tempChi = sc->chi2_temp;
@@ -45,7 +45,7 @@ __global__ void lm_decide(DevScalars* sc) {
 }
 
 // partial sums of x (lambda x + b) (computeScale)
-__global__ void lm_scale_partials(const double* x, const double* b, int n, const DevScalars* sc, double* partials) {
+static __global__ void lm_scale_partials(const double* x, const double* b, int n, const DevScalars* sc, double* partials) {
   const double lambda = sc->lambda;
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -55,14 +55,14 @@ __global__ void lm_scale_partials(const double* x, const double* b, int n, const
 }
 
 // sum of squares partials (refinement residual norms)
-__global__ void sumsq_partials(const double* a, int n, double* partials) {
+static __global__ void sumsq_partials(const double* a, int n, double* partials) {
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * a[i];
   s = block_sum1(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
-__global__ void axpy_kernel(double* y, const double* x, double a, int n) {
+static __global__ void axpy_kernel(double* y, const double* x, double a, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += a * x[i];
 }

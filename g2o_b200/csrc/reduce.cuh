@@ -101,7 +101,7 @@ __device__ __forceinline__ void block_max(double m, double* out) {
 }
 
 // one block: out[i] = sum_j partials[j * stride + i] for i < stride, in a fixed order
-__global__ void finalize_sum_kernel(const double* partials, int n, int stride, double* out0, double* out1,
+static __global__ void finalize_sum_kernel(const double* partials, int n, int stride, double* out0, double* out1,
                                     double add0) {
   double a = 0.0, b = 0.0;
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -116,7 +116,7 @@ __global__ void finalize_sum_kernel(const double* partials, int n, int stride, d
   }
 }
 
-__global__ void finalize_max_kernel(const double* partials, int n, double* out) {
+static __global__ void finalize_max_kernel(const double* partials, int n, double* out) {
   double m = 0.0;
   for (int j = threadIdx.x; j < n; j += blockDim.x) m = fmax(m, partials[j]);
   block_max(m, out);

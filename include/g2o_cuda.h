@@ -235,6 +235,27 @@ int g2oc_solve_block_system(g2oc_ctx* ctx, int32_t linear_solver, int32_t num_bl
                             const double* values, const double* b, double* x,
                             int32_t* iterations);
 
+/* g2oc_solve_block_system_static: no counterpart in the reference. The
+   block-Jacobi PCG solve of g2oc_solve_block_system (same kernels, same
+   results) for callers that cannot allocate device memory, e.g. code running
+   in a process whose GPU memory is capped or pre-partitioned, under a
+   caller-owned allocator, or in a plugin that must not grow the device
+   footprint. It allocates nothing: its device scratch is one file-scope
+   array of G2OC_STATIC_SCRATCH_BYTES that every GPU loading this library
+   holds until process exit, and its host scratch is file-scope too. Inputs
+   and outputs are the caller's host arrays, as for g2oc_solve_block_system
+   (uniform block size 3 or 6, upper blocks column-major). A system whose
+   scratch exceeds the limit is rejected with G2OC_ERR_INVALID_ARGUMENT. The
+   first call on a device looks up the array's device address (with that
+   device current); make that first call before any CUDA stream capture.
+   Calls share the scratch (later calls overwrite it; host callers are
+   serialized by a mutex) and run on cudaStreamPerThread, returning after the
+   result is copied back. */
+#define G2OC_STATIC_SCRATCH_BYTES (16u << 20)
+int g2oc_solve_block_system_static(int device, int32_t num_block_rows, int32_t block_size, int32_t nnzb,
+                                   const int32_t* block_rc, const double* values, const double* b, double* x,
+                                   double pcg_tolerance, int32_t pcg_max_iterations, int32_t* iterations);
+
 #ifdef __cplusplus
 }
 #endif
