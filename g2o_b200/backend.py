@@ -149,6 +149,15 @@ class CudaProblem:
         self.info = G2ocHessianInfo()
         _check(library().g2oc_get_hessian_info(self._h, C.byref(self.info)))
 
+    def upload(self, graph: Graph):
+        """Replace the graph (g2oc_upload). A graph with the same topology as
+        the current one keeps the index structure and device buffers; only its
+        values are copied."""
+        cg = graph.to_c()
+        _check(library().g2oc_upload(self._h, C.byref(cg)))
+        self.graph, self._cg = graph, cg
+        _check(library().g2oc_get_hessian_info(self._h, C.byref(self.info)))
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             library().g2oc_destroy(self._h)

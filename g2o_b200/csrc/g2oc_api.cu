@@ -5,6 +5,7 @@
 // kernels of ba_kernels.cuh, pg_kernels.cuh, pcg_kernels.cuh,
 // lm_kernels.cuh and cholesky.cuh.
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <memory>
 #include <mutex>
@@ -14,8 +15,11 @@
 #include "ba_kernels.cuh"
 #include "cholesky.cuh"
 #include "g2oc_internal.h"
+#include "io_kernels.cuh"
 #include "lm_kernels.cuh"
 #include "pcg_kernels.cuh"
+#include "pcg_persistent.cuh"
+#include "pcg_tiles.cuh"
 #include "pg_kernels.cuh"
 
 namespace g2oc {
@@ -62,13 +66,14 @@ enum KernelId {
   K_CHI2, K_ERRORS, K_JACOBIANS, K_LANDMARK_PASS, K_CAMERA_PASS, K_SCHUR_LANDMARK, K_SCHUR_BLOCKS, K_SCHUR_RHS,
   K_BACKSUB, K_RESID_CAM, K_RESID_LM, K_OPLUS, K_MAX_DIAG, K_PCG_DIAG_INV, K_PCG_INIT, K_PCG_SPMV, K_PCG_UPDATE,
   K_PCG_CHECK, K_PG_LINEARIZE, K_PG_ASSEMBLE_H, K_PG_ASSEMBLE_B, K_DAMP, K_LM_CONTROL, K_REDUCE, K_AXPY,
-  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_COUNT
+  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_COUNT
 };
 static const char* kKernelNames[K_COUNT] = {
   "chi2", "errors", "jacobians", "ba_landmark_pass", "ba_camera_pass", "schur_landmark", "schur_blocks",
   "schur_rhs", "ba_backsub", "ba_resid_cam", "ba_resid_lm", "oplus", "max_diag", "pcg_diag_inv", "pcg_init",
   "pcg_spmv", "pcg_update", "pcg_check_dn", "pg_linearize", "pg_assemble_h", "pg_assemble_b", "damp_diag",
-  "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db"};
+  "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db", "io_reorder", "pcg_solve", "pcg_solve_tiles",
+  "sys_to_tiles"};
 
 struct PendingTiming {
   int kid;
@@ -100,12 +105,27 @@ struct g2oc_ctx {
   g2oc::DBuf<uint8_t> pe_trans;
   g2oc::DBuf<int> hb_src_ptr, hb_src, bv_src_ptr, bv_src;
   // linear system lists
-  g2oc::DBuf<int> sys_perm, sys_rptr, sys_rcol, sys_brow, sys_diag, sys_cptr, sys_cblk;
+  g2oc::DBuf<int> sys_perm, sys_rptr, sys_rcol, sys_brow, sys_diag, sys_cptr, sys_cblk, sys_chunk_ptr, sys_chunk_row,
+      tile_ij, tile_off, trow_ptr, trow_list, tcol_ptr, tcol_list;
+  int pcg_grid[4] = {0, 0, 0, 0};  // CTAs of the persistent PCG per (storage type, block size)
+  int tile_grid[2] = {0, 0};       // CTAs of the dense-tile PCG per storage type
   // FP64 vectors
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
   g2oc::DBuf<g2oc::DevScalars> sc;
   g2oc::DBuf<g2oc::PcgState> pcg;
   g2oc::DBuf<int> flag;  // nonfinite flag
+  // the caller's arrays as copied (g2oc_graph layout), reordered on the device
+  g2oc::DBuf<double> raw_meas, raw_info, raw_delta, raw_pose, raw_point;
+  g2oc::DBuf<int> src_dev, src_cam;  // input edge of each point-major / camera-major row
+  // topology of the uploaded graph: an upload with the same topology keeps
+  // the structure, the device lists, the engine and the Cholesky plan
+  struct Topology {
+    bool valid = false;
+    int32_t pose_type = 0, num_poses = 0, num_points = 0, edge_type = 0, num_edges = 0;
+    std::vector<int32_t> edge_vertex;
+    std::vector<uint8_t> pose_fixed, point_fixed;
+    bool has_pose_fixed = false, has_point_fixed = false;
+  } topo;
   std::unique_ptr<g2oc::EngineBase> eng;
   std::unique_ptr<g2oc::CholPlan> chol;
   int last_pcg_iterations = 0;
@@ -208,6 +228,20 @@ struct LaunchScope {
 #define G2OC_K(kid) for (::g2oc::LaunchScope _ls(c, ::g2oc::kid); !_ls.done; _ls.done = true)
 
 // ------------------------------------------------------------ PCG driver
+// Form of the PCG solve: one cooperative launch over dense tiles when the
+// matrix is nearly full (6x6 blocks), else one cooperative launch over the
+// sparse blocks. G2OC_PCG=sparse forces the sparse launch, G2OC_PCG=kernels
+// the three-kernels-per-iteration form (host-polled).
+// The variable is read at every solve.
+enum PcgMode { PCG_AUTO = 0, PCG_KERNELS = 1, PCG_SPARSE = 2 };
+static int pcg_mode() {
+  const char* e = getenv("G2OC_PCG");
+  if (e && strcmp(e, "kernels") == 0) return PCG_KERNELS;
+  if (e && strcmp(e, "sparse") == 0) return PCG_SPARSE;
+  return PCG_AUTO;
+}
+static bool kernels_pcg() { return pcg_mode() == PCG_KERNELS; }
+
 template <typename Real, int BS>
 static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs, double* xout,
                    double* r, double* s, double* d0, double* d1, double* q, double* qrow, double* tbuf,
@@ -265,6 +299,135 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const
   return G2OC_OK;
 }
 
+// The whole PCG solve as one cooperative launch (pcg_solve_persistent), one
+// CTA pair per SM; the host reads the state once at the end.
+template <typename Real, int BS>
+static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs,
+                              double* xout, double* r, double* s, double* d, double* tbuf, double* cpart,
+                              bool fixed_d0, int* iters) {
+  cudaStream_t st = c->stream;
+  int& grid = c->pcg_grid[(sizeof(Real) == 4 ? 2 : 0) + (BS == 6 ? 1 : 0)];
+  if (grid == 0) {
+    int per_sm = 0, sms = 0;
+    G2OC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_solve_persistent<Real, BS>,
+                                                                kPcgThreads, 0));
+    G2OC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    grid = (per_sm < 2 ? per_sm : 2) * sms;
+    if (grid > 4096) grid = 4096;  // the per-CTA partials use half of `partials` each
+    if (grid <= 0) {
+      set_error("persistent PCG kernel cannot be resident");
+      return G2OC_ERR_CUDA;
+    }
+  }
+  PcgState host;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  PcgState cfg = host;  // keeps residual_carry and, for correction solves, d0
+  cfg.tolerance = c->prm.pcg_tolerance;
+  cfg.max_iter = c->prm.pcg_max_iterations < 0 ? A.nb * BS : c->prm.pcg_max_iterations;
+  if (sizeof(Real) == 4 && cfg.max_iter > kMixedInnerMaxIter) cfg.max_iter = kMixedInnerMaxIter;
+  cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
+  cfg.fixed_d0 = fixed_d0 ? 1 : 0;
+  cfg.counter = 0;
+  cfg.done = 0;
+  cfg.k = 0;
+  cfg.breakdown = 0;
+  cfg.sync_count = 0;
+  cfg.sync_gen = 0;
+  cfg.sync_error = 0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+  SysDev<Real> a = A;
+  const int* chunk_ptr = c->sys_chunk_ptr.p;
+  const int* chunk_row = c->sys_chunk_row.p;
+  int nchunks = (int)c->S.sys_chunk_row.size();
+  double* part_dq = c->partials.p;
+  double* part_rs = c->partials.p + 4096;
+  PcgState* stp = c->pcg.p;
+  void* args[] = {&a, &chunk_ptr, &chunk_row, &nchunks, &minv, &rhs, &xout, &r, &s, &d, &tbuf, &cpart,
+                  &part_dq, &part_rs, &stp};
+  G2OC_K(K_PCG_SOLVE) {
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_persistent<Real, BS>, dim3(grid),
+                                              dim3(kPcgThreads), args, 0, st));
+  }
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (host.sync_error) {
+    set_error("persistent PCG: a grid barrier wait ran out");
+    return G2OC_ERR_TIMEOUT;
+  }
+  if (!host.done) {
+    set_error("persistent PCG did not report completion");
+    return G2OC_ERR_TIMEOUT;
+  }
+  if (iters) *iters = host.iterations;
+  return G2OC_OK;
+}
+
+// PCG over dense tiles (pcg_solve_tiles), one cooperative launch
+template <typename Real>
+static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* minv, const double* rhs, double* xout,
+                         double* r, double* s, double* dbuf0, double* dbuf1, double* rowpart, double* colpart,
+                         bool fixed_d0, int* iters) {
+  cudaStream_t st = c->stream;
+  int& grid = c->tile_grid[sizeof(Real) == 4 ? 1 : 0];
+  if (grid == 0) {
+    int per_sm = 0, sms = 0;
+    G2OC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_solve_tiles<Real>, kTileThreads, 0));
+    G2OC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    const int cap = sizeof(Real) == 4 ? 3 : 2;
+    grid = (per_sm < cap ? per_sm : cap) * sms;
+    if (grid > 4096) grid = 4096;
+    if (grid <= 0) {
+      set_error("dense-tile PCG kernel cannot be resident");
+      return G2OC_ERR_CUDA;
+    }
+  }
+  PcgState host;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  PcgState cfg = host;
+  cfg.tolerance = c->prm.pcg_tolerance;
+  cfg.max_iter = c->prm.pcg_max_iterations < 0 ? nb * 6 : c->prm.pcg_max_iterations;
+  if (sizeof(Real) == 4 && cfg.max_iter > kMixedInnerMaxIter) cfg.max_iter = kMixedInnerMaxIter;
+  cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
+  cfg.fixed_d0 = fixed_d0 ? 1 : 0;
+  cfg.counter = 0;
+  cfg.done = 0;
+  cfg.k = 0;
+  cfg.breakdown = 0;
+  cfg.sync_count = 0;
+  cfg.sync_gen = 0;
+  cfg.sync_error = 0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+  const int2* tij = reinterpret_cast<const int2*>(c->tile_ij.p);
+  int ntiles = (int)(c->S.tile_ij.size() / 2);
+  const int* trp = c->trow_ptr.p;
+  const int* trl = c->trow_list.p;
+  const int* tcp = c->tcol_ptr.p;
+  const int* tcl = c->tcol_list.p;
+  double* part_dq = c->partials.p;
+  double* part_rs = c->partials.p + 4096;
+  PcgState* stp = c->pcg.p;
+  void* args[] = {&tiles, &tij, &ntiles, &trp, &trl,     &tcp,     &tcl,     &nb,      &minv, &rhs,
+                  &xout,  &r,   &s,      &dbuf0, &dbuf1, &rowpart, &colpart, &part_dq, &part_rs, &stp};
+  G2OC_K(K_PCG_TILES) {
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_tiles<Real>, dim3(grid), dim3(kTileThreads),
+                                              args, 0, st));
+  }
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (host.sync_error) {
+    set_error("dense-tile PCG: a grid barrier wait ran out");
+    return G2OC_ERR_TIMEOUT;
+  }
+  if (!host.done) {
+    set_error("dense-tile PCG did not report completion");
+    return G2OC_ERR_TIMEOUT;
+  }
+  if (iters) *iters = host.iterations;
+  return G2OC_OK;
+}
+
 static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, double* out1, double add0 = 0.0) {
   G2OC_K(K_REDUCE) finalize_sum_kernel<<<1, 256, 0, c->stream>>>(c->partials.p, nparts, stride, out0, out1, add0);
   G2OC_LAUNCH_CHECK();
@@ -298,7 +461,9 @@ struct Engine final : EngineBase {
   g2oc_ctx* c;
   // Hessian
   DBuf<Real> hpp, hll, hpl, bdc, dinv, Sval, sysval;
-  DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf;
+  DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf, cpart, rowpart, colpart;
+  DBuf<Real> tiles;  // dense-tile copy of the system (nearly full 6x6-block matrices), allocated on first use
+  bool tiles_fresh = false;  // tiles hold the matrix of the current solve
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
   size_t schur_smem = 0;
   DBuf<Real> hcontrib;
@@ -333,6 +498,8 @@ struct Engine final : EngineBase {
     G2OC_TRY(q.alloc(n + 1));
     G2OC_TRY(qrow.alloc(n + 1));
     G2OC_TRY(tbuf.alloc((size_t)S.sys_nnzb * pd + 1));
+    G2OC_TRY(cpart.alloc(S.sys_chunk_row.size() * pd + 1));
+
     return G2OC_OK;
   }
 
@@ -455,18 +622,40 @@ struct Engine final : EngineBase {
   int pcg_solve(const Real* val, const double* rhs, double* xout, bool fixed_d0, int* iters) {
     const Structure& S = c->S;
     SysDev<Real> A = sys(val);
+    if (!fixed_d0) tiles_fresh = false;
     if (S.pd == 6) {
       if (!fixed_d0) {
         G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
         G2OC_LAUNCH_CHECK();
       }
-      return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
+      if (kernels_pcg())
+        return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
+      if (S.tile_ok && pcg_mode() == PCG_AUTO) {
+        if (!tiles.p) {
+          const size_t nt = S.tile_ij.size() / 2;
+          G2OC_TRY(tiles.alloc(nt * kTileSize));
+          G2OC_CUDA_TRY(cudaMemsetAsync(tiles.p, 0, tiles.bytes(), c->stream));  // blocks outside the pattern
+          G2OC_TRY(rowpart.alloc(nt * kTileScalars));
+          G2OC_TRY(colpart.alloc(nt * kTileScalars));
+        }
+        if (!fixed_d0 || !tiles_fresh) {  // a correction solve reuses the tiles of its first solve
+          G2OC_K(K_TILE_COPY) sys_to_tiles<Real><<<cdiv((long long)A.nnzb * 6, 256), 256, 0, c->stream>>>(
+              A, c->tile_off.p, tiles.p);
+          G2OC_LAUNCH_CHECK();
+          tiles_fresh = true;
+        }
+        return run_pcg_tiles<Real>(c, tiles.p, A.nb, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, rowpart.p, colpart.p,
+                                   fixed_d0, iters);
+      }
+      return run_pcg_persistent<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0, iters);
     }
     if (!fixed_d0) {
       G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 3><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
       G2OC_LAUNCH_CHECK();
     }
-    return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
+    if (kernels_pcg())
+      return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
+    return run_pcg_persistent<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0, iters);
   }
 
   int chol_solve(const Real* val, const double* rhs, double* xout, int* ok) {
@@ -954,9 +1143,41 @@ int g2oc_set_params(g2oc_ctx* c, const g2oc_params* p) {
   return G2OC_OK;
 }
 
-int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
-  G2OC_TRY(check_ctx(c, false));
-  c->uploaded = false;
+static bool same_topology(const g2oc_ctx::Topology& t, const g2oc_graph* g) {
+  if (!t.valid || t.pose_type != g->pose_type || t.num_poses != g->num_poses || t.num_points != g->num_points ||
+      t.edge_type != g->edge_type || t.num_edges != g->num_edges || !g->edge_vertex)
+    return false;
+  if (t.has_pose_fixed != (g->pose_fixed != nullptr) || t.has_point_fixed != (g->point_fixed != nullptr)) return false;
+  if (!t.edge_vertex.empty() && memcmp(t.edge_vertex.data(), g->edge_vertex, t.edge_vertex.size() * sizeof(int32_t)))
+    return false;
+  if (t.has_pose_fixed && !t.pose_fixed.empty() && memcmp(t.pose_fixed.data(), g->pose_fixed, t.pose_fixed.size()))
+    return false;
+  if (t.has_point_fixed && !t.point_fixed.empty() && memcmp(t.point_fixed.data(), g->point_fixed, t.point_fixed.size()))
+    return false;
+  return true;
+}
+
+static void save_topology(g2oc_ctx::Topology& t, const g2oc_graph* g) {
+  t.pose_type = g->pose_type;
+  t.num_poses = g->num_poses;
+  t.num_points = g->num_points;
+  t.edge_type = g->edge_type;
+  t.num_edges = g->num_edges;
+  t.edge_vertex.assign(g->edge_vertex, g->edge_vertex + 2 * (size_t)g->num_edges);
+  t.has_pose_fixed = g->pose_fixed != nullptr;
+  t.has_point_fixed = g->point_fixed != nullptr;
+  t.pose_fixed.assign(g->pose_fixed ? g->pose_fixed : nullptr, g->pose_fixed ? g->pose_fixed + g->num_poses : nullptr);
+  if (g->point_fixed && g->num_points > 0) t.point_fixed.assign(g->point_fixed, g->point_fixed + g->num_points);
+  else t.point_fixed.clear();
+  t.valid = true;
+}
+
+// Everything that depends on the topology alone (vertex counts and types,
+// fixed flags, edge list): SparseOptimizer::initializeOptimization and
+// BlockSolver::buildStructure (g2o/core/sparse_optimizer.cpp:175-287,
+// g2o/core/block_solver.hpp:110-269), the device index lists and the buffers.
+static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
+  c->topo.valid = false;
   c->eng.reset();
   c->chol.reset();
   Structure& S = c->S;
@@ -964,61 +1185,49 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(build_structure(g, S));
   cudaStream_t st = c->stream;
   const int na = (int)S.act.size();
-  c->f = g->focal_length;
-  c->cx = g->principal_point[0];
-  c->cy = g->principal_point[1];
-  // vertices
   if (S.ba) {
-    std::vector<double> cam((size_t)S.C * 8, 0.0), pt((size_t)S.P * 4, 0.0);
-    for (int i = 0; i < S.C; ++i) {
-      const double* v = g->pose_estimate + (size_t)i * 7;
-      double* o = cam.data() + (size_t)i * 8;
-      o[0] = v[3]; o[1] = v[4]; o[2] = v[5]; o[3] = v[6];
-      o[4] = v[0]; o[5] = v[1]; o[6] = v[2];
-    }
-    for (int i = 0; i < S.P; ++i)
-      for (int k = 0; k < 3; ++k) pt[(size_t)i * 4 + k] = g->point_estimate[(size_t)i * 3 + k];
-    G2OC_TRY(c->pose.upload(cam, st));
-    G2OC_TRY(c->point.upload(pt, st));
-    G2OC_TRY(c->point_bak.alloc(pt.size()));
+    G2OC_TRY(c->pose.alloc((size_t)S.C * 8));
+    G2OC_TRY(c->point.alloc((size_t)S.P * 4));
+    G2OC_TRY(c->point_bak.alloc(c->point.n));
+    G2OC_TRY(c->point_init.alloc(c->point.n));
+    G2OC_TRY(c->raw_pose.alloc((size_t)S.C * 7));
+    G2OC_TRY(c->raw_point.alloc((size_t)S.P * 3));
   } else {
-    std::vector<double> est(g->pose_estimate, g->pose_estimate + (size_t)S.C * S.ped);
-    G2OC_TRY(c->pose.upload(est, st));
+    G2OC_TRY(c->pose.alloc((size_t)S.C * S.ped));
     c->point.release();
     c->point_bak.release();
+    c->point_init.release();
   }
   G2OC_TRY(c->pose_bak.alloc(c->pose.n));
   G2OC_TRY(c->pose_init.alloc(c->pose.n));
-  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose_init.p, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, st));
-  if (c->point.n) {
-    G2OC_TRY(c->point_init.alloc(c->point.n));
-    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point_init.p, c->point.p, c->point.bytes(), cudaMemcpyDeviceToDevice, st));
-  }
   G2OC_TRY(c->oplus_count.alloc(S.C));
-  G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, S.C * sizeof(int), st));
   G2OC_TRY(c->free_pose.upload(S.free_pose_of_h, st));
   G2OC_TRY(c->free_point.upload(S.free_point_of_l, st));
   G2OC_TRY(c->pose_h.upload(S.pose_h, st));
   if (S.ba) G2OC_TRY(c->point_l.upload(S.point_l, st));
   if (S.ba) {
-    std::vector<int2> ev(na), cv(S.c_edge.size());
-    std::vector<double2> ez(na), cz(S.c_edge.size());
-    std::vector<double4> eo(na), co(S.c_edge.size());
+    const size_t nc = S.c_edge.size();
+    std::vector<int2> ev(na), cv(nc);
+    std::vector<int> scam(nc);
     for (int k = 0; k < na; ++k) {
       const int e = S.dev_edge[k];
       ev[k] = make_int2(g->edge_vertex[2 * e], g->edge_vertex[2 * e + 1]);
-      ez[k] = make_double2(g->measurement[2 * e], g->measurement[2 * e + 1]);
-      const double* I = g->information + (size_t)e * 4;
-      eo[k] = make_double4(I[0], I[1], I[3], g->robust_delta ? g->robust_delta[e] : 0.0);
     }
-    for (size_t j = 0; j < S.c_edge.size(); ++j) {
+    for (size_t j = 0; j < nc; ++j) {
       cv[j] = ev[S.c_edge[j]];
-      cz[j] = ez[S.c_edge[j]];
-      co[j] = eo[S.c_edge[j]];
+      scam[j] = S.dev_edge[S.c_edge[j]];
     }
     G2OC_TRY(c->e_v.upload(ev, st));
-    G2OC_TRY(c->e_z.upload(ez, st));
-    G2OC_TRY(c->e_om.upload(eo, st));
+    G2OC_TRY(c->c_v.upload(cv, st));
+    G2OC_TRY(c->src_dev.upload(S.dev_edge, st));
+    G2OC_TRY(c->src_cam.upload(scam, st));
+    G2OC_TRY(c->e_z.alloc(na));
+    G2OC_TRY(c->e_om.alloc(na));
+    G2OC_TRY(c->c_z.alloc(nc));
+    G2OC_TRY(c->c_om.alloc(nc));
+    G2OC_TRY(c->raw_meas.alloc((size_t)S.E * 2));
+    G2OC_TRY(c->raw_info.alloc((size_t)S.E * 4));
+    G2OC_TRY(c->raw_delta.alloc((size_t)S.E));
     G2OC_TRY(c->e_hpl.upload(S.e_hpl, st));
     G2OC_TRY(c->l_ptr.upload(S.l_ptr, st));
     if (S.lm_warp_ok) {
@@ -1026,9 +1235,6 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
       G2OC_TRY(c->lm_chunk_ptr.upload(S.lm_chunk_ptr, st));
     }
     G2OC_TRY(c->c_ptr.upload(S.c_ptr, st));
-    G2OC_TRY(c->c_v.upload(cv, st));
-    G2OC_TRY(c->c_z.upload(cz, st));
-    G2OC_TRY(c->c_om.upload(co, st));
     G2OC_TRY(c->hb_ptr.upload(S.hb_ptr, st));
     const size_t nh = S.hpl_rc.size() / 2;
     std::vector<int> hr(nh), hcl(nh);
@@ -1053,20 +1259,15 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->s_pairs.upload(ab, st));
     G2OC_TRY(c->s_hpp.upload(S.s_hpp, st));
   } else {
-    const int D = S.D, ZD = S.md;
     std::vector<int2> ev(na);
-    std::vector<double> zi((size_t)na * ZD), info((size_t)na * D * D), dl(na);
     for (int k = 0; k < na; ++k) {
       const int e = S.act[k];
       ev[k] = make_int2(g->edge_vertex[2 * e], g->edge_vertex[2 * e + 1]);
-      inverse_measurement(S.edge_type, g->measurement + (size_t)e * ZD, zi.data() + (size_t)k * ZD);
-      memcpy(info.data() + (size_t)k * D * D, g->information + (size_t)e * D * D, D * D * sizeof(double));
-      dl[k] = g->robust_delta ? g->robust_delta[e] : 0.0;
     }
     G2OC_TRY(c->pe_v.upload(ev, st));
-    G2OC_TRY(c->pe_zinv.upload(zi, st));
-    G2OC_TRY(c->pe_info.upload(info, st));
-    G2OC_TRY(c->pe_delta.upload(dl, st));
+    G2OC_TRY(c->pe_zinv.alloc((size_t)na * S.md));
+    G2OC_TRY(c->pe_info.alloc((size_t)na * S.D * S.D));
+    G2OC_TRY(c->pe_delta.alloc(na));
     G2OC_TRY(c->pe_trans.upload(S.pe_trans, st));
     G2OC_TRY(c->hb_src_ptr.upload(S.hb_src_ptr, st));
     G2OC_TRY(c->hb_src.upload(S.hb_src, st));
@@ -1080,6 +1281,16 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(c->sys_diag.upload(S.sys_diag, st));
   G2OC_TRY(c->sys_cptr.upload(S.sys_cptr, st));
   G2OC_TRY(c->sys_cblk.upload(S.sys_cblk, st));
+  G2OC_TRY(c->sys_chunk_ptr.upload(S.sys_chunk_ptr, st));
+  G2OC_TRY(c->sys_chunk_row.upload(S.sys_chunk_row, st));
+  if (S.tile_ok) {
+    G2OC_TRY(c->tile_ij.upload(S.tile_ij, st));
+    G2OC_TRY(c->tile_off.upload(S.tile_off, st));
+    G2OC_TRY(c->trow_ptr.upload(S.trow_ptr, st));
+    G2OC_TRY(c->trow_list.upload(S.trow_list, st));
+    G2OC_TRY(c->tcol_ptr.upload(S.tcol_ptr, st));
+    G2OC_TRY(c->tcol_list.upload(S.tcol_list, st));
+  }
   const int n = c->vec_size();
   G2OC_TRY(c->b.alloc(n));
   G2OC_TRY(c->x.alloc(n));
@@ -1088,11 +1299,101 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(c->xs.alloc((size_t)S.Cf * S.pd));
   G2OC_TRY(c->rhs.alloc((size_t)S.Cf * S.pd));
   G2OC_TRY(c->errbuf.alloc((size_t)na * 36));
-  G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, n * sizeof(double), st));
-  G2OC_CUDA_TRY(cudaMemsetAsync(c->b.p, 0, n * sizeof(double), st));
-  G2OC_TRY(reset_pcg(c));
   G2OC_TRY(make_engine(c));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  save_topology(c->topo, g);
+  return G2OC_OK;
+}
+
+// BA vertex estimates from the caller's layout (copied as-is, reordered on the device)
+static int upload_ba_estimates(g2oc_ctx* c, const double* pose, const double* point) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  if (pose && S.C > 0) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_pose.p, pose, c->raw_pose.bytes(), cudaMemcpyHostToDevice, st));
+    G2OC_K(K_IO) ba_pack_poses<<<cdiv((long long)S.C * 8, 256), 256, 0, st>>>(S.C, c->raw_pose.p, c->pose.p);
+    G2OC_LAUNCH_CHECK();
+  }
+  if (point && S.P > 0) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_point.p, point, c->raw_point.bytes(), cudaMemcpyHostToDevice, st));
+    G2OC_K(K_IO) ba_pack_points<<<cdiv((long long)S.P * 4, 256), 256, 0, st>>>(S.P, c->raw_point.p, c->point.p);
+    G2OC_LAUNCH_CHECK();
+  }
+  return G2OC_OK;
+}
+
+// Everything that depends on the values: estimates, measurements, information
+// matrices, robust kernels, camera parameters.
+static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  const int na = (int)S.act.size();
+  c->f = g->focal_length;
+  c->cx = g->principal_point[0];
+  c->cy = g->principal_point[1];
+  if (S.ba) {
+    G2OC_TRY(upload_ba_estimates(c, g->pose_estimate, g->point_estimate));
+    if (S.E > 0) {
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_meas.p, g->measurement, c->raw_meas.bytes(), cudaMemcpyHostToDevice, st));
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_info.p, g->information, c->raw_info.bytes(), cudaMemcpyHostToDevice, st));
+      if (g->robust_delta)
+        G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_delta.p, g->robust_delta, c->raw_delta.bytes(), cudaMemcpyHostToDevice, st));
+      const int nc = (int)S.c_edge.size();
+      if (na + nc > 0) {
+        G2OC_K(K_IO) ba_gather_edges<<<cdiv((long long)na + nc, 256), 256, 0, st>>>(
+            na, nc, c->src_dev.p, c->src_cam.p, c->raw_meas.p, c->raw_info.p, g->robust_delta ? c->raw_delta.p : nullptr,
+            c->e_z.p, c->e_om.p, c->c_z.p, c->c_om.p);
+        G2OC_LAUNCH_CHECK();
+      }
+    }
+  } else {
+    if (S.C > 0)
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, g->pose_estimate, c->pose.bytes(), cudaMemcpyHostToDevice, st));
+    const int D = S.D, ZD = S.md;
+    std::vector<double> zi((size_t)na * ZD), info((size_t)na * D * D), dl(na);
+#pragma omp parallel for schedule(static) if (na > 65536)
+    for (int k = 0; k < na; ++k) {
+      const int e = S.act[k];
+      inverse_measurement(S.edge_type, g->measurement + (size_t)e * ZD, zi.data() + (size_t)k * ZD);
+      memcpy(info.data() + (size_t)k * D * D, g->information + (size_t)e * D * D, D * D * sizeof(double));
+      dl[k] = g->robust_delta ? g->robust_delta[e] : 0.0;
+    }
+    G2OC_TRY(c->pe_zinv.upload(zi, st));
+    G2OC_TRY(c->pe_info.upload(info, st));
+    G2OC_TRY(c->pe_delta.upload(dl, st));
+  }
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose_init.p, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, st));
+  if (c->point.n)
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point_init.p, c->point.p, c->point.bytes(), cudaMemcpyDeviceToDevice, st));
+  if (S.C > 0) G2OC_CUDA_TRY(cudaMemsetAsync(c->oplus_count.p, 0, S.C * sizeof(int), st));
+  const int n = c->vec_size();
+  if (n > 0) {
+    G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, n * sizeof(double), st));
+    G2OC_CUDA_TRY(cudaMemsetAsync(c->b.p, 0, n * sizeof(double), st));
+  }
+  G2OC_TRY(reset_pcg(c));
+  c->system_built = false;
+  return G2OC_OK;
+}
+
+int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
+  G2OC_TRY(check_ctx(c, false));
+  if (!g) {
+    set_error("graph is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const bool reuse = c->eng && same_topology(c->topo, g);
+  c->uploaded = false;
+  if (reuse) {
+    // the null checks build_structure makes for a new topology
+    if (!g->pose_estimate || !g->measurement || !g->information || (c->S.ba && g->num_points > 0 && !g->point_estimate)) {
+      set_error("graph array is NULL");
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+  } else {
+    G2OC_TRY(upload_topology(c, g));
+  }
+  G2OC_TRY(upload_data(c, g));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
   return G2OC_OK;
 }
@@ -1117,27 +1418,10 @@ int g2oc_get_hessian_info(g2oc_ctx* c, g2oc_hessian_info* info) {
 int g2oc_set_estimates(g2oc_ctx* c, const double* pose, const double* point) {
   G2OC_TRY(check_ctx(c, true));
   const Structure& S = c->S;
-  if (pose) {
-    if (S.ba) {
-      std::vector<double> cam((size_t)S.C * 8, 0.0);
-      for (int i = 0; i < S.C; ++i) {
-        const double* v = pose + (size_t)i * 7;
-        double* o = cam.data() + (size_t)i * 8;
-        o[0] = v[3]; o[1] = v[4]; o[2] = v[5]; o[3] = v[6];
-        o[4] = v[0]; o[5] = v[1]; o[6] = v[2];
-      }
-      G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, cam.data(), c->pose.bytes(), cudaMemcpyHostToDevice, c->stream));
-      G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    } else {
-      G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, pose, c->pose.bytes(), cudaMemcpyHostToDevice, c->stream));
-    }
-  }
-  if (point && S.ba && S.P > 0) {
-    std::vector<double> pt((size_t)S.P * 4, 0.0);
-    for (int i = 0; i < S.P; ++i)
-      for (int k = 0; k < 3; ++k) pt[(size_t)i * 4 + k] = point[(size_t)i * 3 + k];
-    G2OC_CUDA_TRY(cudaMemcpyAsync(c->point.p, pt.data(), c->point.bytes(), cudaMemcpyHostToDevice, c->stream));
-    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (S.ba) {
+    G2OC_TRY(upload_ba_estimates(c, pose, point));
+  } else if (pose && S.C > 0) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, pose, c->pose.bytes(), cudaMemcpyHostToDevice, c->stream));
   }
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->system_built = false;
@@ -1147,27 +1431,23 @@ int g2oc_set_estimates(g2oc_ctx* c, const double* pose, const double* point) {
 int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
   G2OC_TRY(check_ctx(c, true));
   const Structure& S = c->S;
-  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if (pose) {
-    if (S.ba) {
-      std::vector<double> cam((size_t)S.C * 8);
-      G2OC_CUDA_TRY(cudaMemcpy(cam.data(), c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost));
-      for (int i = 0; i < S.C; ++i) {
-        const double* o = cam.data() + (size_t)i * 8;
-        double* v = pose + (size_t)i * 7;
-        v[0] = o[4]; v[1] = o[5]; v[2] = o[6];
-        v[3] = o[0]; v[4] = o[1]; v[5] = o[2]; v[6] = o[3];
-      }
-    } else {
-      G2OC_CUDA_TRY(cudaMemcpy(pose, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost));
+  cudaStream_t st = c->stream;
+  if (S.ba) {
+    // reorder into the caller's layout on the device, then one copy each
+    if (pose && S.C > 0) {
+      G2OC_K(K_IO) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, st>>>(S.C, c->pose.p, c->raw_pose.p);
+      G2OC_LAUNCH_CHECK();
+      G2OC_CUDA_TRY(cudaMemcpyAsync(pose, c->raw_pose.p, c->raw_pose.bytes(), cudaMemcpyDeviceToHost, st));
     }
+    if (point && S.P > 0) {
+      G2OC_K(K_IO) ba_unpack_points<<<cdiv((long long)S.P * 3, 256), 256, 0, st>>>(S.P, c->point.p, c->raw_point.p);
+      G2OC_LAUNCH_CHECK();
+      G2OC_CUDA_TRY(cudaMemcpyAsync(point, c->raw_point.p, c->raw_point.bytes(), cudaMemcpyDeviceToHost, st));
+    }
+  } else if (pose && S.C > 0) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(pose, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost, st));
   }
-  if (point && S.ba && S.P > 0) {
-    std::vector<double> pt((size_t)S.P * 4);
-    G2OC_CUDA_TRY(cudaMemcpy(pt.data(), c->point.p, c->point.bytes(), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < S.P; ++i)
-      for (int k = 0; k < 3; ++k) point[(size_t)i * 3 + k] = pt[(size_t)i * 4 + k];
-  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
   return G2OC_OK;
 }
 

@@ -125,7 +125,19 @@ struct Structure {
   std::vector<int> sys_brow;            // per internal block: row
   std::vector<int> sys_diag;            // per row: internal index of the diagonal
   std::vector<int> sys_cptr, sys_cblk;  // strictly-upper blocks by column, rows ascending
+  std::vector<int> sys_chunk_ptr;       // nb + 1: chunks of row r (kSysChunk blocks each, the last ragged)
+  std::vector<int> sys_chunk_row;       // per chunk: its row
+  // dense tiles (6x6 blocks only): kTileBlocks x kTileBlocks blocks each,
+  // stored scalar-row-major (96 x 96), upper tiles only, diagonal tiles full
+  bool tile_ok = false;
+  std::vector<int> tile_ij;             // 2 per tile: tile row I, tile column J (I <= J)
+  std::vector<int> tile_off;            // per internal block: offset of its (0,0) entry in the tile array
+  std::vector<int> trow_ptr, trow_list; // per tile row I: tiles (I, J)
+  std::vector<int> tcol_ptr, tcol_list; // per tile column J: tiles (I, J), I < J
 };
+
+constexpr int kSysChunk = 32;  // blocks per row chunk = lanes of a warp
+constexpr int kTileBlocks = 16;  // blocks per tile side of the dense path
 
 int build_structure(const g2oc_graph* g, Structure& s);
 // internal row-major order and column lists of a block-symmetric matrix from

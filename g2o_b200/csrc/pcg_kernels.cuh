@@ -65,6 +65,10 @@ struct PcgState {
   int absolute_tolerance;
   int fixed_d0;           // correction solves: keep d0 of the first solve, leave the carry
   int breakdown;          // d.q <= 0 met (the matrix is not positive definite along d)
+  // grid barrier of the persistent solve (zero before its launch)
+  unsigned int sync_count;
+  unsigned int sync_gen;
+  int sync_error;         // a barrier wait ran out of its spin limit
 };
 
 // M^-1: inverse of each diagonal block (computed in FP64)

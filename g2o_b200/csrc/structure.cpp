@@ -66,6 +66,66 @@ void radix_sort(std::vector<uint64_t>& keys, std::vector<uint32_t>& perm) {
 
 }  // namespace
 
+// Dense tiles of kTileBlocks x kTileBlocks blocks for a nearly full matrix:
+// the upper tiles (I <= J) holding at least one block, diagonal tiles stored
+// with both triangles. Chosen when the tiles hold at most 1.25x the blocks of
+// the pattern (plus the lower halves of the diagonal tiles).
+static void build_tiles(int nb, Structure& s) {
+  s.tile_ok = false;
+  s.tile_ij.clear();
+  s.tile_off.clear();
+  s.trow_ptr.clear();
+  s.trow_list.clear();
+  s.tcol_ptr.clear();
+  s.tcol_list.clear();
+  const int nnzb = s.sys_nnzb;
+  if (nb < 2 * kTileBlocks) return;
+  const int nbt = (nb + kTileBlocks - 1) / kTileBlocks;
+  std::vector<int> id((size_t)nbt * nbt, -1);
+  for (int k = 0; k < nnzb; ++k) {
+    const int I = s.sys_brow[k] / kTileBlocks, J = s.sys_rcol[k] / kTileBlocks;
+    id[(size_t)I * nbt + J] = 0;
+  }
+  int nt = 0;
+  for (size_t q = 0; q < id.size(); ++q)
+    if (id[q] == 0) id[q] = nt++;
+  const double stored = (double)nt * kTileBlocks * kTileBlocks;
+  const double allowed = 1.25 * nnzb + (double)nbt * kTileBlocks * kTileBlocks / 2;
+  if (stored > allowed || (long long)nt * kTileBlocks * kTileBlocks * 36 >= (1LL << 31)) return;
+  s.tile_ok = true;
+  s.tile_ij.resize(2 * (size_t)nt);
+  s.trow_ptr.assign(nbt + 1, 0);
+  s.tcol_ptr.assign(nbt + 1, 0);
+  for (int I = 0; I < nbt; ++I)
+    for (int J = I; J < nbt; ++J) {
+      const int t = id[(size_t)I * nbt + J];
+      if (t < 0) continue;
+      s.tile_ij[2 * (size_t)t] = I;
+      s.tile_ij[2 * (size_t)t + 1] = J;
+      s.trow_ptr[I + 1]++;
+      if (J > I) s.tcol_ptr[J + 1]++;
+    }
+  for (int I = 0; I < nbt; ++I) {
+    s.trow_ptr[I + 1] += s.trow_ptr[I];
+    s.tcol_ptr[I + 1] += s.tcol_ptr[I];
+  }
+  s.trow_list.resize(s.trow_ptr[nbt]);
+  s.tcol_list.resize(s.tcol_ptr[nbt]);
+  std::vector<int> rfill(s.trow_ptr.begin(), s.trow_ptr.end() - 1), cfill(s.tcol_ptr.begin(), s.tcol_ptr.end() - 1);
+  for (int t = 0; t < nt; ++t) {
+    const int I = s.tile_ij[2 * (size_t)t], J = s.tile_ij[2 * (size_t)t + 1];
+    s.trow_list[rfill[I]++] = t;
+    if (J > I) s.tcol_list[cfill[J]++] = t;
+  }
+  constexpr int TS = kTileBlocks * 6;  // scalar rows of a tile (6x6 blocks)
+  s.tile_off.resize(nnzb);
+  for (int k = 0; k < nnzb; ++k) {
+    const int r = s.sys_brow[k], c = s.sys_rcol[k];
+    const int t = id[(size_t)(r / kTileBlocks) * nbt + c / kTileBlocks];
+    s.tile_off[k] = t * TS * TS + (r % kTileBlocks) * 6 * TS + (c % kTileBlocks) * 6;
+  }
+}
+
 void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s) {
   const int nnzb = (int)(rc.size() / 2);
   s.sys_nb = nb;
@@ -98,6 +158,14 @@ void build_sym_lists(int nb, const std::vector<int32_t>& rc, Structure& s) {
   counting_sort(ckey, nb, corder, s.sys_cptr);
   s.sys_cblk.resize(corder.size());
   for (size_t i = 0; i < corder.size(); ++i) s.sys_cblk[i] = cidx[corder[i]];
+  // row chunks of at most kSysChunk blocks (one warp each in the persistent PCG)
+  s.sys_chunk_ptr.assign(nb + 1, 0);
+  for (int r = 0; r < nb; ++r)
+    s.sys_chunk_ptr[r + 1] = s.sys_chunk_ptr[r] + (s.sys_rptr[r + 1] - s.sys_rptr[r] + kSysChunk - 1) / kSysChunk;
+  s.sys_chunk_row.resize(s.sys_chunk_ptr[nb]);
+  for (int r = 0; r < nb; ++r)
+    for (int ch = s.sys_chunk_ptr[r]; ch < s.sys_chunk_ptr[r + 1]; ++ch) s.sys_chunk_row[ch] = r;
+  build_tiles(nb, s);
 }
 
 static int build_ba(const g2oc_graph* g, Structure& s) {

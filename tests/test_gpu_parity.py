@@ -106,6 +106,37 @@ def test_ba_pcg_solve_matches_oracle(backend, oracle_lib):
     assert relnorm(xc, xo) < 1e-6
 
 
+@pytest.mark.parametrize("form,kernel", [("", "pcg_solve_tiles"), ("sparse", "pcg_solve"), ("kernels", "pcg_spmv")])
+def test_pcg_forms_match_oracle(backend, oracle_lib, monkeypatch, form, kernel):
+    """The three forms of the PCG solve (dense tiles for a nearly full reduced
+    camera system, the sparse cooperative launch, three kernels per iteration)
+    against the oracle. 90 cameras: a full Schur pattern, 6 tile rows with a
+    ragged last one."""
+    if form:
+        monkeypatch.setenv("G2OC_PCG", form)
+    else:
+        monkeypatch.delenv("G2OC_PCG", raising=False)
+    g = small_ba(seed=21, cams=90, points=7000)
+    o, c = both(backend, oracle_lib, g)
+    o.build_system()
+    c.build_system()
+    for lam in (1e2, 1e-2):
+        so, xo, ito = o.solve(lam)
+        sc, xc, itc = c.solve(lam)
+        assert so == 0 and sc == 0
+        assert abs(itc - ito) <= 1, (itc, ito)
+        assert relnorm(xc, xo) < 1e-6
+    _, ks = c.kernel_stats()
+    assert ks.get(kernel, (0, 0.0))[0] > 0, ks
+    do, so_ = o.optimize(5)
+    dc, sc_ = c.optimize(5)
+    for a, b in zip(sc_, so_):
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"]
+    cm = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED))
+    _, sm = cm.optimize(5)
+    assert abs(sm[-1]["chi2"] - so_[-1]["chi2"]) <= 1e-3 * so_[-1]["chi2"]
+
+
 def test_ba_cholesky_solve_is_exact(backend, oracle_lib):
     g = small_ba()
     o, c = both(backend, oracle_lib, g, linear_solver=LINEAR_CHOLESKY)
@@ -253,6 +284,40 @@ def test_iterate_matches_optimize(backend):
     pa, qa = a.estimates()
     pb, qb = b.estimates()
     assert np.array_equal(pa, pb) and np.array_equal(qa, qb)
+
+
+def test_reupload_keeps_structure_and_matches_fresh_context(backend):
+    """g2oc_upload of a graph with the same topology reuses the index structure
+    and the device buffers; the values (estimates, measurements, information,
+    robust kernels) are all replaced. A changed topology rebuilds."""
+    g = small_ba(seed=13, cams=20, points=800)
+    rng = np.random.default_rng(2)
+    g2 = g.copy()
+    g2.measurement += rng.normal(scale=0.3, size=g2.measurement.shape)
+    g2.information *= rng.uniform(0.5, 2.0, size=(g2.num_edges, 1))
+    g2.point_estimate += rng.normal(scale=0.05, size=g2.point_estimate.shape)
+    g2.pose_estimate[:, :3] += rng.normal(scale=0.01, size=(g2.num_poses, 3))
+    g2.robust_delta = None
+    a = backend.CudaProblem(g)
+    a.optimize(3)
+    for gn in (g2, g):
+        a.upload(gn)
+        b = backend.CudaProblem(gn)
+        assert a.chi2() == b.chi2()
+        _, sa = a.optimize(5)
+        _, sb = b.optimize(5)
+        assert [s["chi2"] for s in sa] == [s["chi2"] for s in sb]
+        for x, y in zip(a.estimates(), b.estimates()):
+            assert np.array_equal(x, y)
+        b.close()
+    g3 = g.copy()
+    g3.point_fixed[::5] = 1
+    a.upload(g3)
+    b = backend.CudaProblem(g3)
+    assert a.info.num_free_points == b.info.num_free_points < g.num_points
+    _, sa = a.optimize(4)
+    _, sb = b.optimize(4)
+    assert [s["chi2"] for s in sa] == [s["chi2"] for s in sb]
 
 
 def test_factory_constructed_solver_runs(backend, oracle_lib):
