@@ -375,7 +375,7 @@ struct Vec2<float> {
 // b_l(a) is formed from the same staged blocks. S is written in the row-SoA
 // layout of sys_offset.
 template <typename Real, int THREADS, bool STAGE>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 3 : 1)
     schur_rows(const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl, const Real* dinv,
                const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs, const int* s_hpp,
                const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l, double* bs) {
@@ -468,29 +468,48 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int half = threadIdx.x & 1;
   for (int j = 1 + (threadIdx.x >> 1); j < nblk; j += THREADS / 2) {
     const int k = rb + j;
-    double acc[18];
+    // pair products summed in the storage type (FP64 on the FP64 path; FP32
+    // on the mixed path, whose S is stored in FP32), added to Hpp in FP64
+    Real acc[18];
 #pragma unroll
-    for (int t = 0; t < 18; ++t) acc[t] = 0.0;
-    const int p1 = pair_ptr[k + 1];
-    for (int p = pair_ptr[k]; p < p1; ++p) {
-      const int2 pr = pairs[p];
-      const Real* D = BDa + (size_t)pr.x * 18 + half * 9;
-      Real d[9];
-#pragma unroll
-      for (int t = 0; t < 9; ++t) d[t] = D[t];
-      const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)pr.y * 18);
-      Real b[18];
+    for (int t = 0; t < 18; ++t) acc[t] = 0;
+    // two pairs per step: their index and Hpl loads are independent, so two
+    // gathers are in flight per thread; accumulation stays in pair order
+    auto load_b = [&](int blk, Real (&b)[18]) {
+      const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
         const R2 v = B2[t];
         b[2 * t] = v.x;
         b[2 * t + 1] = v.y;
       }
+    };
+    auto accum = [&](int a, const Real (&b)[18]) {
+      const Real* D = BDa + (size_t)a * 18 + half * 9;
+      Real d[9];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) d[t] = D[t];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-          acc[i * 6 + c] += (double)(d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2]);
+          acc[i * 6 + c] += d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2];
+    };
+    int p = pair_ptr[k];
+    const int p1 = pair_ptr[k + 1];
+    for (; p + 1 < p1; p += 2) {
+      const int2 pa = pairs[p], pb = pairs[p + 1];
+      Real ba[18], bb[18];
+      load_b(pa.y, ba);
+      load_b(pb.y, bb);
+      accum(pa.x, ba);
+      accum(pb.x, bb);
+    }
+    if (p < p1) {
+      const int2 pa = pairs[p];
+      Real ba[18];
+      load_b(pa.y, ba);
+      accum(pa.x, ba);
     }
     const int hb = s_hpp[k];
 #pragma unroll
@@ -498,7 +517,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
       for (int c = 0; c < 6; ++c) {
         const int e = (half * 3 + i) * 6 + c;
-        double v = -acc[i * 6 + c];
+        double v = -(double)acc[i * 6 + c];
         if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
         Sr[(size_t)e * nblk + j] = (Real)v;
       }
@@ -518,30 +537,27 @@ __global__ void schur_db(const Real* dinv, const double* r_l, int Pf, double* db
 }
 
 // Reduced right-hand side for a given (r_p, r_l) (block_solver.hpp:366-392,
-// 429-433): one warp per free camera, bs = r_p - sum_a B_a db_l(a).
-template <typename Real>
-__global__ void schur_rhs(const int* hc_ptr, const int* hc_blk, const int* hpl_col, int Cf, const Real* hpl,
-                          const double* db, const double* r_p, double* bs) {
-  const int h = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  const int lane = threadIdx.x & 31;
-  if (h >= Cf) return;
+// 429-433): one CTA per free camera, bs = r_p - sum_a B_a db_l(a), threads
+// over the camera's Hpl blocks (camera-major lists), fixed-order reduction.
+template <typename Real, int THREADS>
+__global__ void __launch_bounds__(THREADS) schur_rhs(const int* hc_ptr, const int* hc_blk, const int* hc_col,
+                                                     const Real* hpl, const double* db, const double* r_p,
+                                                     double* bs) {
+  const int h = blockIdx.x;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const int e1 = hc_ptr[h + 1];
-  for (int p = hc_ptr[h] + lane; p < e1; p += 32) {
+  for (int p = hc_ptr[h] + threadIdx.x; p < e1; p += THREADS) {
     const int a = hc_blk[p];
-    const double* d = db + (size_t)hpl_col[a] * 3;
+    const double* d = db + (size_t)hc_col[p] * 3;
     const Real* B = hpl + (size_t)a * 18;
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[q] += (double)B[q * 3] * d[0] + (double)B[q * 3 + 1] * d[1] + (double)B[q * 3 + 2] * d[2];
   }
+  __shared__ double red[THREADS / 32][6];
+  block_sum_array<double, 6, THREADS>(acc, &red[0][0]);
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int q = 0; q < 6; ++q) acc[q] = warp_sum(acc[q]);
-  if (lane < 6) {
-    double v = acc[0];
-#pragma unroll
-    for (int q = 1; q < 6; ++q)
-      if (lane == q) v = acc[q];
-    bs[(size_t)h * 6 + lane] = r_p[(size_t)h * 6 + lane] - v;
+    for (int q = 0; q < 6; ++q) bs[(size_t)h * 6 + q] = r_p[(size_t)h * 6 + q] - acc[q];
   }
 }
 
@@ -569,6 +585,58 @@ __global__ void ba_backsub(const int* hb_ptr, const int* hpl_row, int Pf, const 
 #pragma unroll
   for (int i = 0; i < 3; ++i)
     x_l[(size_t)l * 3 + i] = (double)D[i * 3] * cl[0] + (double)D[i * 3 + 1] * cl[1] + (double)D[i * 3 + 2] * cl[2];
+}
+
+// Back-substitution, one warp per chunk of whole landmarks (lane per edge,
+// each edge of a free camera owns one Hpl block when the chunks exist),
+// segmented warp scan by landmark.
+template <typename Real>
+__global__ void ba_backsub_warp(const int* e_hpl, const int* hpl_row, const int* chunk_ptr, int nchunks,
+                                const int* e_lm, const Real* hpl, const Real* dinv, const double* r_l,
+                                const double* x_p, double* x_l) {
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ch >= nchunks) return;
+  const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
+  const int k = e0 + lane;
+  const bool act = k < e1;
+  double acc[3] = {0, 0, 0};
+  int key = -1 - lane;
+  if (act) {
+    key = e_lm[k];
+    const int blk = e_hpl[k];
+    if (blk >= 0) {
+      const Real* B = hpl + (size_t)blk * 18;
+      const double* xp = x_p + (size_t)hpl_row[blk] * 6;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double t = 0.0;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) t += (double)B[r * 3 + c] * xp[r];
+        acc[c] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ko = __shfl_up_sync(0xffffffffu, key, off);
+    double ao[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ao[i] = __shfl_up_sync(0xffffffffu, acc[i], off);
+    if (lane >= off && ko == key) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) acc[i] += ao[i];
+    }
+  }
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  if (act && (lane == 31 || knext != key)) {
+    const double cl[3] = {r_l[(size_t)key * 3] - acc[0], r_l[(size_t)key * 3 + 1] - acc[1],
+                          r_l[(size_t)key * 3 + 2] - acc[2]};
+    const Real* D = dinv + (size_t)key * 9;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      x_l[(size_t)key * 3 + i] = (double)D[i * 3] * cl[0] + (double)D[i * 3 + 1] * cl[1] + (double)D[i * 3 + 2] * cl[2];
+  }
 }
 
 // Matrix-free FP64 residual of the damped normal equations for the
@@ -607,6 +675,62 @@ static __global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) r_l[(size_t)l * 3 + i] = b_l[(size_t)l * 3 + i] - acc[i];
+}
+
+// Landmark side, one warp per chunk of whole landmarks (<= 32 edges, lane
+// per edge) with a segmented warp scan, as ba_landmark_warp.
+static __global__ void ba_resid64_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, int nchunks,
+                                                const int* e_lm, const int* pose_h, double lambda, const double* b_l,
+                                                const double* x_p, const double* x_l, double* r_l) {
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ch >= nchunks) return;
+  const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
+  const int k = e0 + lane;
+  const bool act = k < e1;
+  double acc[3] = {0, 0, 0};
+  int key = -1 - lane;  // distinct for idle lanes
+  if (act) {
+    key = e_lm[k];
+    const double* xl = x_l + (size_t)key * 3;
+    const int2 v = E.v[k];
+    const double4 om = E.om[k];
+    double e[2], Xc[3], chi2, w;
+    ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
+    double Jp[6], Jc[12];
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    double u0 = Jp[0] * xl[0] + Jp[1] * xl[1] + Jp[2] * xl[2];
+    double u1 = Jp[3] * xl[0] + Jp[4] * xl[1] + Jp[5] * xl[2];
+    const int h = pose_h[v.y];
+    if (h >= 0) {
+      const double* xp = x_p + (size_t)h * 6;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        u0 += Jc[q] * xp[q];
+        u1 += Jc[6 + q] * xp[q];
+      }
+    }
+    const double o0 = w * (om.x * u0 + om.y * u1), o1 = w * (om.y * u0 + om.z * u1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) acc[i] = Jp[i] * o0 + Jp[3 + i] * o1;
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ko = __shfl_up_sync(0xffffffffu, key, off);
+    double ao[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ao[i] = __shfl_up_sync(0xffffffffu, acc[i], off);
+    if (lane >= off && ko == key) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) acc[i] += ao[i];
+    }
+  }
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  if (act && (lane == 31 || knext != key)) {
+    const double* xl = x_l + (size_t)key * 3;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r_l[(size_t)key * 3 + i] = b_l[(size_t)key * 3 + i] - lambda * xl[i] - acc[i];
+  }
 }
 
 // Camera side: one CTA per free camera over its edges, fixed-order reduction.

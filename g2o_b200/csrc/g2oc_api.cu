@@ -55,7 +55,7 @@ struct EngineBase {
   virtual int alloc() = 0;
   virtual int build_system() = 0;
   virtual int max_diag() = 0;  // -> sc.max_diag
-  virtual int solve(double lambda, int* pcg_iters) = 0;  // -> x, sc.solve_ok
+  virtual int solve(double lambda) = 0;  // -> x, sc.solve_ok (PCG iterations: PcgState::total_iterations)
   virtual int get_hessian(double* hpp, double* hll, double* hpl) = 0;
   virtual int schur_export(double lambda, double* S, double* bs) = 0;
 };
@@ -128,8 +128,10 @@ struct g2oc_ctx {
   } topo;
   std::unique_ptr<g2oc::EngineBase> eng;
   std::unique_ptr<g2oc::CholPlan> chol;
-  int last_pcg_iterations = 0;
-  double last_schur_s = 0.0;
+  long long pcg_seen = 0;        // PcgState::total_iterations at the last read
+  double lambda_host = 0.0;      // the device's LM lambda as of the last read
+  bool chi2_carry = false;       // chi2_current / chi2_plain hold the current estimates' values
+  g2oc_iteration_stats* cur_stats = nullptr;  // stats of the iteration in progress
   double last_refine_dn = 0.0;
   long long refine_steps = 0;
   // launch accounting
@@ -149,6 +151,34 @@ struct g2oc_ctx {
     cudaEventCreate(&e);
     return e;
   }
+  // phase times without waiting: events recorded around a phase; the elapsed
+  // time is added to *out (and subtracted from *out2) when the spans are
+  // resolved, at a point where the host waits for the stream anyway
+  struct Span {
+    cudaEvent_t a, b;
+    double* out;
+    double* out2;
+  };
+  std::vector<Span> spans;
+  cudaEvent_t mark() {
+    cudaEvent_t e = event();
+    cudaEventRecord(e, stream);
+    return e;
+  }
+  void span(cudaEvent_t a, double* out, double* out2 = nullptr) { spans.push_back({a, mark(), out, out2}); }
+  void resolve_spans() {
+    if (spans.empty()) return;
+    cudaEventSynchronize(spans.back().b);
+    for (auto& sp : spans) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, sp.a, sp.b);
+      if (sp.out) *sp.out += ms * 1e-3;
+      if (sp.out2) *sp.out2 -= ms * 1e-3;
+      event_pool.push_back(sp.a);
+      event_pool.push_back(sp.b);
+    }
+    spans.clear();
+  }
   void flush_timing() {
     if (pending.empty()) return;
     cudaEventSynchronize(pending.back().b);
@@ -165,6 +195,7 @@ struct g2oc_ctx {
     eng.reset();
     chol.reset();
     flush_timing();
+    resolve_spans();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -242,6 +273,17 @@ static int pcg_mode() {
 }
 static bool kernels_pcg() { return pcg_mode() == PCG_KERNELS; }
 
+// LinearSolverPCG::_maxIter (the system dimension when unset); an FP32-stored
+// system (mixed path) is a correction step of the FP64 refinement, so its
+// iterations are capped and the FP64 residual check decides whether another
+// correction is needed
+template <typename Real>
+static int pcg_max_iter(const g2oc_ctx* c, int n) {
+  int m = c->prm.pcg_max_iterations < 0 ? n : c->prm.pcg_max_iterations;
+  if (sizeof(Real) == 4 && m > kMixedInnerMaxIter) m = kMixedInnerMaxIter;
+  return m;
+}
+
 template <typename Real, int BS>
 static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs, double* xout,
                    double* r, double* s, double* d0, double* d1, double* q, double* qrow, double* tbuf,
@@ -295,6 +337,8 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const
     }
     chunk = chunk * 2 > kPcgChunkMax ? kPcgChunkMax : chunk * 2;
   }
+  G2OC_K(K_PCG_CHECK) pcg_add_total<<<1, 32, 0, st>>>(c->pcg.p);
+  G2OC_LAUNCH_CHECK();
   if (iters) *iters = host.iterations;
   return G2OC_OK;
 }
@@ -304,7 +348,7 @@ static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const
 template <typename Real, int BS>
 static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs,
                               double* xout, double* r, double* s, double* d, double* tbuf, double* cpart,
-                              bool fixed_d0, int* iters) {
+                              bool fixed_d0) {
   cudaStream_t st = c->stream;
   int& grid = c->pcg_grid[(sizeof(Real) == 4 ? 2 : 0) + (BS == 6 ? 1 : 0)];
   if (grid == 0) {
@@ -319,23 +363,10 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
       return G2OC_ERR_CUDA;
     }
   }
-  PcgState host;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-  PcgState cfg = host;  // keeps residual_carry and, for correction solves, d0
-  cfg.tolerance = c->prm.pcg_tolerance;
-  cfg.max_iter = c->prm.pcg_max_iterations < 0 ? A.nb * BS : c->prm.pcg_max_iterations;
-  if (sizeof(Real) == 4 && cfg.max_iter > kMixedInnerMaxIter) cfg.max_iter = kMixedInnerMaxIter;
-  cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
-  cfg.fixed_d0 = fixed_d0 ? 1 : 0;
-  cfg.counter = 0;
-  cfg.done = 0;
-  cfg.k = 0;
-  cfg.breakdown = 0;
-  cfg.sync_count = 0;
-  cfg.sync_gen = 0;
-  cfg.sync_error = 0;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+  double tol = c->prm.pcg_tolerance;
+  int max_iter = pcg_max_iter<Real>(c, A.nb * BS);
+  int abs_tol = c->prm.pcg_absolute_tolerance;
+  int fixed = fixed_d0 ? 1 : 0;
   SysDev<Real> a = A;
   const int* chunk_ptr = c->sys_chunk_ptr.p;
   const int* chunk_row = c->sys_chunk_row.p;
@@ -343,23 +374,13 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
   double* part_dq = c->partials.p;
   double* part_rs = c->partials.p + 4096;
   PcgState* stp = c->pcg.p;
-  void* args[] = {&a, &chunk_ptr, &chunk_row, &nchunks, &minv, &rhs, &xout, &r, &s, &d, &tbuf, &cpart,
-                  &part_dq, &part_rs, &stp};
+  void* args[] = {&a,    &chunk_ptr, &chunk_row, &nchunks, &minv,    &rhs,    &xout, &r,       &s,
+                  &d,    &tbuf,      &cpart,     &part_dq, &part_rs, &stp,    &tol,  &max_iter, &abs_tol,
+                  &fixed};
   G2OC_K(K_PCG_SOLVE) {
     G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_persistent<Real, BS>, dim3(grid),
                                               dim3(kPcgThreads), args, 0, st));
   }
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-  if (host.sync_error) {
-    set_error("persistent PCG: a grid barrier wait ran out");
-    return G2OC_ERR_TIMEOUT;
-  }
-  if (!host.done) {
-    set_error("persistent PCG did not report completion");
-    return G2OC_ERR_TIMEOUT;
-  }
-  if (iters) *iters = host.iterations;
   return G2OC_OK;
 }
 
@@ -367,7 +388,7 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
 template <typename Real>
 static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* minv, const double* rhs, double* xout,
                          double* r, double* s, double* dbuf0, double* dbuf1, double* rowpart, double* colpart,
-                         bool fixed_d0, int* iters) {
+                         bool fixed_d0) {
   cudaStream_t st = c->stream;
   int& grid = c->tile_grid[sizeof(Real) == 4 ? 1 : 0];
   if (grid == 0) {
@@ -382,23 +403,10 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
       return G2OC_ERR_CUDA;
     }
   }
-  PcgState host;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-  PcgState cfg = host;
-  cfg.tolerance = c->prm.pcg_tolerance;
-  cfg.max_iter = c->prm.pcg_max_iterations < 0 ? nb * 6 : c->prm.pcg_max_iterations;
-  if (sizeof(Real) == 4 && cfg.max_iter > kMixedInnerMaxIter) cfg.max_iter = kMixedInnerMaxIter;
-  cfg.absolute_tolerance = c->prm.pcg_absolute_tolerance;
-  cfg.fixed_d0 = fixed_d0 ? 1 : 0;
-  cfg.counter = 0;
-  cfg.done = 0;
-  cfg.k = 0;
-  cfg.breakdown = 0;
-  cfg.sync_count = 0;
-  cfg.sync_gen = 0;
-  cfg.sync_error = 0;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &cfg, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+  double tol = c->prm.pcg_tolerance;
+  int max_iter = pcg_max_iter<Real>(c, nb * 6);
+  int abs_tol = c->prm.pcg_absolute_tolerance;
+  int fixed = fixed_d0 ? 1 : 0;
   const int2* tij = reinterpret_cast<const int2*>(c->tile_ij.p);
   int ntiles = (int)(c->S.tile_ij.size() / 2);
   const int* trp = c->trow_ptr.p;
@@ -408,23 +416,13 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
   double* part_dq = c->partials.p;
   double* part_rs = c->partials.p + 4096;
   PcgState* stp = c->pcg.p;
-  void* args[] = {&tiles, &tij, &ntiles, &trp, &trl,     &tcp,     &tcl,     &nb,      &minv, &rhs,
-                  &xout,  &r,   &s,      &dbuf0, &dbuf1, &rowpart, &colpart, &part_dq, &part_rs, &stp};
+  void* args[] = {&tiles, &tij,     &ntiles,  &trp,     &trl,     &tcp,  &tcl, &nb,       &minv,    &rhs,  &xout,
+                  &r,     &s,       &dbuf0,   &dbuf1,   &rowpart, &colpart,    &part_dq, &part_rs, &stp,  &tol,
+                  &max_iter, &abs_tol, &fixed};
   G2OC_K(K_PCG_TILES) {
     G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_tiles<Real>, dim3(grid), dim3(kTileThreads),
                                               args, 0, st));
   }
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-  if (host.sync_error) {
-    set_error("dense-tile PCG: a grid barrier wait ran out");
-    return G2OC_ERR_TIMEOUT;
-  }
-  if (!host.done) {
-    set_error("dense-tile PCG did not report completion");
-    return G2OC_ERR_TIMEOUT;
-  }
-  if (iters) *iters = host.iterations;
   return G2OC_OK;
 }
 
@@ -433,27 +431,6 @@ static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, doubl
   G2OC_LAUNCH_CHECK();
   return G2OC_OK;
 }
-
-struct PhaseTimer {
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  explicit PhaseTimer(cudaStream_t s) : st(s) {
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-  }
-  ~PhaseTimer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-  void start() { cudaEventRecord(a, st); }
-  double stop() {
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    return ms * 1e-3;
-  }
-};
 
 // ---------------------------------------------------------- the engine
 template <typename Real>
@@ -587,7 +564,8 @@ struct Engine final : EngineBase {
       G2OC_LAUNCH_CHECK();
     }
     if (S.Cf == 0) return G2OC_OK;
-    constexpr int T = 512;
+    // FP32 storage: 256 threads, three CTAs per SM; FP64: 512 threads, one
+    constexpr int T = sizeof(Real) == 4 ? 256 : 512;
     const double* bp = c->b.p;
     const double* bl = c->b.p + (size_t)S.Cf * 6;
     if (stage_in_smem) {
@@ -611,15 +589,15 @@ struct Engine final : EngineBase {
       G2OC_K(K_SCHUR_DB) schur_db<Real><<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(dinv.p, rl, S.Pf, c->db.p);
       G2OC_LAUNCH_CHECK();
     }
-    G2OC_K(K_SCHUR_RHS) schur_rhs<Real><<<cdiv(S.Cf, 4), 128, 0, c->stream>>>(c->hc_ptr.p, c->hc_blk.p, c->hpl_col.p,
-                                                                             S.Cf, hpl.p, c->db.p, rp, bs);
+    G2OC_K(K_SCHUR_RHS) schur_rhs<Real, 256><<<S.Cf, 256, 0, c->stream>>>(c->hc_ptr.p, c->hc_blk.p, c->hc_col.p,
+                                                                         hpl.p, c->db.p, rp, bs);
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
   // fixed_d0: a correction solve of the refinement, stopping at the d0 of
   // the first solve (which set the preconditioner)
-  int pcg_solve(const Real* val, const double* rhs, double* xout, bool fixed_d0, int* iters) {
+  int pcg_solve(const Real* val, const double* rhs, double* xout, bool fixed_d0) {
     const Structure& S = c->S;
     SysDev<Real> A = sys(val);
     if (!fixed_d0) tiles_fresh = false;
@@ -629,7 +607,7 @@ struct Engine final : EngineBase {
         G2OC_LAUNCH_CHECK();
       }
       if (kernels_pcg())
-        return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
+        return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, nullptr);
       if (S.tile_ok && pcg_mode() == PCG_AUTO) {
         if (!tiles.p) {
           const size_t nt = S.tile_ij.size() / 2;
@@ -645,17 +623,17 @@ struct Engine final : EngineBase {
           tiles_fresh = true;
         }
         return run_pcg_tiles<Real>(c, tiles.p, A.nb, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, rowpart.p, colpart.p,
-                                   fixed_d0, iters);
+                                   fixed_d0);
       }
-      return run_pcg_persistent<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0, iters);
+      return run_pcg_persistent<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0);
     }
     if (!fixed_d0) {
       G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 3><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
       G2OC_LAUNCH_CHECK();
     }
     if (kernels_pcg())
-      return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, iters);
-    return run_pcg_persistent<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0, iters);
+      return run_pcg<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, nullptr);
+    return run_pcg_persistent<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0);
   }
 
   int chol_solve(const Real* val, const double* rhs, double* xout, int* ok) {
@@ -669,10 +647,9 @@ struct Engine final : EngineBase {
     return g2oc::chol_solve<Real>(*c->chol, c->stream, sys(val), rhs, xout, ok, &c->kcount[K_CHOLESKY]);
   }
 
-  int solve(double lambda, int* pcg_iters) override {
+  int solve(double lambda) override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    int it_total = 0, it = 0;
     int ok = 1;
     const bool use_chol = c->prm.linear_solver == G2OC_LINEAR_CHOLESKY ||
                           (c->prm.linear_solver == 2 && !S.ba);
@@ -683,27 +660,20 @@ struct Engine final : EngineBase {
         if (S.schur) {
           G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
               hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, dinv.p, nullptr, c->flag.p);
-          G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, c->b.p,
-                                                             c->xs.p, c->x.p);
           G2OC_LAUNCH_CHECK();
+          G2OC_TRY(backsub(c->b.p, c->xs.p, c->x.p));
         }
       }
     } else if (S.ba && S.schur) {
-      PhaseTimer tm(st);
-      tm.start();
+      cudaEvent_t ts = c->cur_stats ? c->mark() : nullptr;
       G2OC_TRY(schur(lambda, c->rhs.p));
       const double* bp = c->b.p;
       const double* bl = c->b.p + (size_t)S.Cf * 6;
-      c->last_schur_s = tm.stop();
+      if (ts) c->span(ts, &c->cur_stats->time_schur_complement, &c->cur_stats->time_linear_solver);
       if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
-      else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false, &it));
-      it_total += it;
+      else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false));
       G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-      if (S.Pf > 0) {
-        G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p, dinv.p, bl, c->xs.p,
-                                                           c->x.p + (size_t)S.Cf * 6);
-        G2OC_LAUNCH_CHECK();
-      }
+      G2OC_TRY(backsub(bl, c->xs.p, c->x.p + (size_t)S.Cf * 6));
       // mixed precision: FP64 iterative refinement on the true residual of
       // the damped normal equations, r = b - (J^T Om' J + lambda I) x, formed
       // matrix-free from the edges in FP64. A correction is solved (FP32
@@ -717,10 +687,16 @@ struct Engine final : EngineBase {
         for (int k = 0; k <= c->prm.refine_max_iterations; ++k) {
           double* rp = c->resid.p;
           double* rl = c->resid.p + (size_t)S.Cf * 6;
-          if (S.Pf > 0)
+          if (S.Pf > 0 && S.lm_warp_ok) {
+            const int nch = (int)S.lm_chunk_ptr.size() - 1;
+            G2OC_K(K_RESID_LM) ba_resid64_landmark_warp<<<cdiv(nch, 8), 256, 0, st>>>(
+                c->ba_edges(), c->ba_vertices(), c->lm_chunk_ptr.p, nch, c->e_lm.p, c->pose_h.p, lambda, bl, c->x.p,
+                c->x.p + (size_t)S.Cf * 6, rl);
+          } else if (S.Pf > 0) {
             G2OC_K(K_RESID_LM) ba_resid64_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(
                 c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, c->pose_h.p, lambda, bl, c->x.p,
                 c->x.p + (size_t)S.Cf * 6, rl);
+          }
           BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
           G2OC_K(K_RESID_CAM) ba_resid64_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p, lambda,
                                                                            bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
@@ -741,16 +717,10 @@ struct Engine final : EngineBase {
           }
           if (!(ps.check_dn > ps.d0) || k == c->prm.refine_max_iterations) break;
           prev = ps.check_dn;
-          G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true, &it));
-          it_total += it;
+          G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true));
           c->refine_steps++;
           G2OC_CUDA_TRY(cudaMemcpyAsync(c->dx.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
-          if (S.Pf > 0) {
-            G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, hpl_row(), S.Pf, hpl.p,
-                                                                               dinv.p, rl, c->xs.p,
-                                                                               c->dx.p + (size_t)S.Cf * 6);
-            G2OC_LAUNCH_CHECK();
-          }
+          G2OC_TRY(backsub(rl, c->xs.p, c->dx.p + (size_t)S.Cf * 6));
           G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, 1.0, n);
           G2OC_LAUNCH_CHECK();
         }
@@ -766,17 +736,31 @@ struct Engine final : EngineBase {
             hpp.p, c->sys_perm.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, nnzb, lambda, sysval.p);
       G2OC_LAUNCH_CHECK();
       if (use_chol) G2OC_TRY(chol_solve(sysval.p, c->b.p, c->x.p, &ok));
-      else G2OC_TRY(pcg_solve(sysval.p, c->b.p, c->x.p, false, &it));
-      it_total += it;
+      else G2OC_TRY(pcg_solve(sysval.p, c->b.p, c->x.p, false));
     }
-    c->last_pcg_iterations = it_total;
-    if (pcg_iters) *pcg_iters = it_total;
-    G2OC_CUDA_TRY(cudaMemcpyAsync(&c->sc.p->solve_ok, &ok, sizeof(int), cudaMemcpyHostToDevice, st));
-    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    G2OC_K(K_LM_CONTROL) set_solve_ok<<<1, 32, 0, st>>>(c->sc.p, ok);
+    G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
   const int* hpl_row() { return c->hpl_row.p; }
+
+  // x_l = Dinv (r_l - sum_a B_a^T x_p(row a)) (block_solver.hpp:449-474)
+  int backsub(const double* rl, const double* xp, double* xl) {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.Pf == 0) return G2OC_OK;
+    if (S.lm_warp_ok) {
+      const int nch = (int)S.lm_chunk_ptr.size() - 1;
+      G2OC_K(K_BACKSUB) ba_backsub_warp<Real><<<cdiv(nch, 8), 256, 0, st>>>(
+          c->e_hpl.p, c->hpl_row.p, c->lm_chunk_ptr.p, nch, c->e_lm.p, hpl.p, dinv.p, rl, xp, xl);
+    } else {
+      G2OC_K(K_BACKSUB) ba_backsub<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(c->hb_ptr.p, c->hpl_row.p, S.Pf, hpl.p,
+                                                                         dinv.p, rl, xp, xl);
+    }
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
 
   template <typename T>
   static void to_double(const std::vector<T>& in, double* out) {
@@ -871,53 +855,70 @@ static int pop(g2oc_ctx* c) {
   return G2OC_OK;
 }
 
-// OptimizationAlgorithmLevenberg::solve (optimization_algorithm_levenberg.cpp:60-153)
+static int reset_pcg(g2oc_ctx* c);
+
+// DevScalars and PcgState after the queued work (the one wait of an LM
+// trial): PCG iterations since the last read go to stv
+static int read_state(g2oc_ctx* c, DevScalars* h, g2oc_iteration_stats* stv) {
+  PcgState ps;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (ps.sync_error) {
+    G2OC_TRY(reset_pcg(c));
+    set_error("PCG: a grid barrier wait ran out");
+    return G2OC_ERR_TIMEOUT;
+  }
+  if (stv) stv->iterations_linear_solver += (int)(ps.total_iterations - c->pcg_seen);
+  c->pcg_seen = ps.total_iterations;
+  c->lambda_host = h->lambda;
+  return G2OC_OK;
+}
+
+// OptimizationAlgorithmLevenberg::solve (optimization_algorithm_levenberg.cpp:60-153).
+// The errors of the state an iteration starts from are those of the trial
+// accepted last (same estimates, same kernel), so their chi2 is carried over
+// instead of recomputed; the host waits for the device once per trial.
 static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
   cudaStream_t st = c->stream;
   DevScalars* sc = c->sc.p;
-  PhaseTimer tm(st);
-  tm.start();
-  G2OC_TRY(chi2_to(c, &sc->chi2_plain, &sc->chi2_current));
-  stv->time_residuals = tm.stop();
-  tm.start();
+  c->cur_stats = stv;
+  cudaEvent_t t0 = c->mark();
+  if (!c->chi2_carry) G2OC_TRY(chi2_to(c, &sc->chi2_plain, &sc->chi2_current));
+  c->span(t0, &stv->time_residuals);
+  t0 = c->mark();
   G2OC_TRY(c->eng->build_system());
   c->system_built = true;
-  stv->time_quadratic_form = tm.stop();
+  c->span(t0, &stv->time_quadratic_form);
+  DevScalars h{};
   if (iteration == 0) {
     G2OC_TRY(c->eng->max_diag());
     G2OC_K(K_LM_CONTROL) lm_init_lambda<<<1, 32, 0, st>>>(sc, c->prm.initial_lambda, c->prm.tau);
     G2OC_LAUNCH_CHECK();
+    G2OC_TRY(read_state(c, &h, stv));
   }
   const int n = c->vec_size();
   double rho = 0;
   int qmax = 0;
-  DevScalars h{};
+  bool accepted = false;
   do {
     G2OC_TRY(push(c));
-    DevScalars cur;
-    G2OC_CUDA_TRY(cudaMemcpyAsync(&cur, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
-    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-    tm.start();
-    int pcg_it = 0;
-    c->last_schur_s = 0.0;
-    G2OC_TRY(c->eng->solve(cur.lambda, &pcg_it));
-    const double tsolve = tm.stop();
-    stv->time_schur_complement += c->last_schur_s;
-    stv->time_linear_solver += tsolve - c->last_schur_s;
-    stv->iterations_linear_solver += pcg_it;
-    tm.start();
+    t0 = c->mark();
+    G2OC_TRY(c->eng->solve(c->lambda_host));
+    c->span(t0, &stv->time_linear_solver);
+    t0 = c->mark();
     G2OC_TRY(oplus(c));
-    stv->time_update += tm.stop();
-    G2OC_TRY(chi2_to(c, nullptr, &sc->chi2_temp));
+    c->span(t0, &stv->time_update);
+    G2OC_TRY(chi2_to(c, &sc->chi2_temp_plain, &sc->chi2_temp));
     G2OC_K(K_LM_CONTROL) lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p);
     G2OC_LAUNCH_CHECK();
     G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &sc->scale, nullptr, 1e-3));
     G2OC_K(K_LM_CONTROL) lm_decide<<<1, 32, 0, st>>>(sc);
     G2OC_LAUNCH_CHECK();
-    G2OC_CUDA_TRY(cudaMemcpyAsync(&h, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, st));
-    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    G2OC_TRY(read_state(c, &h, stv));
     rho = h.rho;
-    if (!h.accept) {
+    accepted = h.accept != 0;
+    if (!accepted) {
       G2OC_TRY(pop(c));
       if (!std::isfinite(h.lambda)) {
         qmax++;
@@ -928,7 +929,11 @@ static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
     qmax++;
     stv->levenberg_iterations = qmax;
   } while (rho < 0 && qmax < c->prm.max_trials_after_failure);
+  c->chi2_carry = accepted;
   stv->lambda = h.lambda;
+  stv->chi2 = h.chi2_current;  // activeRobustChi2 of the state the iteration ends in (G2OBatchStatistics::chi2)
+  c->resolve_spans();
+  c->cur_stats = nullptr;
   if (qmax == c->prm.max_trials_after_failure || rho == 0 || !std::isfinite(h.lambda)) *result = G2OC_RESULT_TERMINATE;
   else *result = G2OC_RESULT_OK;
   return G2OC_OK;
@@ -937,28 +942,27 @@ static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
 // OptimizationAlgorithmGaussNewton::solve (optimization_algorithm_gauss_newton.cpp:48-93)
 static int gn_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
   (void)iteration;
-  PhaseTimer tm(c->stream);
-  tm.start();
+  c->cur_stats = stv;
+  c->chi2_carry = false;
+  cudaEvent_t t0 = c->mark();
   G2OC_TRY(chi2_to(c, &c->sc.p->chi2_plain, &c->sc.p->chi2_current));
-  stv->time_residuals = tm.stop();
-  tm.start();
+  c->span(t0, &stv->time_residuals);
+  t0 = c->mark();
   G2OC_TRY(c->eng->build_system());
   c->system_built = true;
-  stv->time_quadratic_form = tm.stop();
-  tm.start();
-  int it = 0;
-  c->last_schur_s = 0.0;
-  G2OC_TRY(c->eng->solve(0.0, &it));
-  const double tsolve = tm.stop();
-  stv->time_schur_complement = c->last_schur_s;
-  stv->time_linear_solver = tsolve - c->last_schur_s;
-  stv->iterations_linear_solver = it;
-  tm.start();
+  c->span(t0, &stv->time_quadratic_form);
+  t0 = c->mark();
+  G2OC_TRY(c->eng->solve(0.0));
+  c->span(t0, &stv->time_linear_solver);
+  t0 = c->mark();
   G2OC_TRY(oplus(c));
-  stv->time_update = tm.stop();
+  c->span(t0, &stv->time_update);
+  G2OC_TRY(chi2_to(c, nullptr, &c->sc.p->chi2_temp));
   DevScalars h;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  G2OC_TRY(read_state(c, &h, stv));
+  stv->chi2 = h.chi2_temp;  // activeRobustChi2 after the update (G2OBatchStatistics::chi2)
+  c->resolve_spans();
+  c->cur_stats = nullptr;
   *result = h.solve_ok ? G2OC_RESULT_OK : G2OC_RESULT_FAIL;
   return G2OC_OK;
 }
@@ -967,6 +971,7 @@ static int reset_pcg(g2oc_ctx* c) {
   PcgState p{};
   p.residual_carry = -1.0;
   G2OC_CUDA_TRY(cudaMemcpyAsync(c->pcg.p, &p, sizeof(PcgState), cudaMemcpyHostToDevice, c->stream));
+  c->pcg_seen = 0;
   return G2OC_OK;
 }
 
@@ -1377,6 +1382,7 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
 
 int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(check_ctx(c, false));
+  c->chi2_carry = false;
   if (!g) {
     set_error("graph is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
@@ -1417,6 +1423,7 @@ int g2oc_get_hessian_info(g2oc_ctx* c, g2oc_hessian_info* info) {
 
 int g2oc_set_estimates(g2oc_ctx* c, const double* pose, const double* point) {
   G2OC_TRY(check_ctx(c, true));
+  c->chi2_carry = false;
   const Structure& S = c->S;
   if (S.ba) {
     G2OC_TRY(upload_ba_estimates(c, pose, point));
@@ -1463,21 +1470,13 @@ int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int*
   for (int i = 0; i < iterations && result == G2OC_RESULT_OK; ++i) {
     g2oc_iteration_stats stv;
     memset(&stv, 0, sizeof(stv));
-    PhaseTimer tm(c->stream);
-    tm.start();
+    cudaEvent_t t0 = c->mark();
     if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, i, &stv, &result));
     else G2OC_TRY(gn_iteration(c, i, &stv, &result));
     stv.iteration = i;
     stv.result = result;
-    if (stats) {
-      G2OC_TRY(chi2_to(c, nullptr, &c->sc.p->chi2_plain));
-      DevScalars h;
-      G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
-      G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
-      stv.chi2 = h.chi2_plain;
-      if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) stv.lambda = h.lambda;
-    }
-    stv.time_iteration = tm.stop();
+    c->span(t0, &stv.time_iteration);
+    c->resolve_spans();
     if (stats) stats[i] = stv;
     ++it;
   }
@@ -1495,21 +1494,13 @@ int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* r
   if (iteration == 0) G2OC_TRY(reset_pcg(c));
   g2oc_iteration_stats stv;
   memset(&stv, 0, sizeof(stv));
-  PhaseTimer tm(c->stream);
-  tm.start();
+  cudaEvent_t t0 = c->mark();
   if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, iteration, &stv, result));
   else G2OC_TRY(gn_iteration(c, iteration, &stv, result));
   stv.iteration = iteration;
   stv.result = *result;
-  if (stats) {
-    G2OC_TRY(chi2_to(c, nullptr, &c->sc.p->chi2_plain));
-    DevScalars h;
-    G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
-    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    stv.chi2 = h.chi2_plain;
-    if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) stv.lambda = h.lambda;
-  }
-  stv.time_iteration = tm.stop();
+  c->span(t0, &stv.time_iteration);
+  c->resolve_spans();
   if (stats) *stats = stv;
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return G2OC_OK;
@@ -1613,12 +1604,12 @@ int g2oc_solve(g2oc_ctx* c, double lambda, double* x, int32_t* iters) {
     set_error("call g2oc_build_system first");
     return G2OC_ERR_STATE;
   }
-  int it = 0;
-  G2OC_TRY(c->eng->solve(lambda, &it));
+  G2OC_TRY(c->eng->solve(lambda));
   DevScalars h;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  if (iters) *iters = it;
+  g2oc_iteration_stats stv;
+  memset(&stv, 0, sizeof(stv));
+  G2OC_TRY(read_state(c, &h, &stv));
+  if (iters) *iters = stv.iterations_linear_solver;
   if (x) G2OC_CUDA_TRY(cudaMemcpy(x, c->x.p, c->x.bytes(), cudaMemcpyDeviceToHost));
   return h.solve_ok ? G2OC_OK : G2OC_ERR_NOT_PD;
 }
@@ -1721,6 +1712,7 @@ int g2oc_get_stream(g2oc_ctx* c, void** stream) {
 
 int g2oc_restore_initial_estimates(g2oc_ctx* c) {
   G2OC_TRY(check_ctx(c, true));
+  c->chi2_carry = false;
   G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, c->pose_init.p, c->pose.bytes(), cudaMemcpyDeviceToDevice, c->stream));
   if (c->point.n)
     G2OC_CUDA_TRY(cudaMemcpyAsync(c->point.p, c->point_init.p, c->point.bytes(), cudaMemcpyDeviceToDevice, c->stream));

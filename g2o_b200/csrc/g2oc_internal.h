@@ -160,6 +160,7 @@ struct DevScalars {
   double pcg_d0;
   double pcg_dn;
   double refine_rnorm;   // mixed precision: |r| / |b| of the last refinement
+  double chi2_temp_plain;  // activeChi2 after the trial update
   int pcg_iterations;
   int pcg_done;
   int solve_ok;

@@ -35,6 +35,7 @@ static __global__ void lm_decide(DevScalars* sc) {
     sc->lambda *= scaleFactor;
     sc->ni = 2;
     sc->chi2_current = tempChi;
+    sc->chi2_plain = sc->chi2_temp_plain;  // the accepted state's errors are the current ones
     sc->accept = 1;
   } else {
     sc->lambda *= sc->ni;
@@ -42,6 +43,10 @@ static __global__ void lm_decide(DevScalars* sc) {
     sc->accept = 0;
   }
   sc->rho = rho;
+}
+
+static __global__ void set_solve_ok(DevScalars* sc, int ok) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) sc->solve_ok = ok;
 }
 
 // partial sums of x (lambda x + b) (computeScale)

@@ -65,10 +65,13 @@ struct PcgState {
   int absolute_tolerance;
   int fixed_d0;           // correction solves: keep d0 of the first solve, leave the carry
   int breakdown;          // d.q <= 0 met (the matrix is not positive definite along d)
-  // grid barrier of the persistent solve (zero before its launch)
+  // grid barrier of the persistent solve (the count returns to zero after
+  // every barrier; any generation value works)
   unsigned int sync_count;
   unsigned int sync_gen;
   int sync_error;         // a barrier wait ran out of its spin limit
+  int pad;
+  long long total_iterations;  // iterations of all solves since the state was reset
 };
 
 // M^-1: inverse of each diagonal block (computed in FP64)
@@ -323,6 +326,11 @@ __global__ void pcg_update(int nb, const double* minv, const double* d0buf, cons
       }
     }
   }
+}
+
+// iterations of a solve driven from the host, added to the running total
+static __global__ void pcg_add_total(PcgState* st) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) st->total_iterations += st->iterations;
 }
 
 // M-norm r^T M^-1 r of a residual in FP64 -> st->check_dn (refinement check)

@@ -120,23 +120,22 @@ __device__ __forceinline__ double row_precondition(const double* minv, int c, co
   return pick<BS>(rc, lane) * v;
 }
 
-// Solve A x = b from x = 0. State in/out: PcgState (tolerance, max_iter,
-// absolute_tolerance, fixed_d0, d0 for fixed_d0, residual_carry in; dn, d0,
-// iterations, breakdown, done, residual_carry out).
+// Solve A x = b from x = 0. Configuration in the arguments (nothing is
+// written to the state before the launch); state in: d0 (fixed_d0 solves)
+// and residual_carry; out: dn, d0, iterations, breakdown, done,
+// residual_carry, total_iterations.
 template <typename Real, int BS>
 __global__ void __launch_bounds__(kPcgThreads, 2)
     pcg_solve_persistent(SysDev<Real> A, const int* chunk_ptr, const int* chunk_row, int nchunks, const double* minv,
                          const double* b, double* x, double* r, double* s, double* d, double* tbuf, double* cpart,
-                         double* part_dq, double* part_rs, PcgState* st) {
+                         double* part_dq, double* part_rs, PcgState* st, double tol, int max_iter, int abs_tol,
+                         int fixed_d0) {
   __shared__ double red[kPcgWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPcgWarps + warp, GW = gridDim.x * kPcgWarps;
-  const double tol = st->tolerance;
-  const int max_iter = st->max_iter;
-  const bool fixed = st->fixed_d0 != 0;
+  const bool fixed = fixed_d0 != 0;
   const double d0_in = st->d0;
   const double carry = st->residual_carry;
-  const int abs_tol = st->absolute_tolerance;
 
   // r = b, x = 0, s = M^-1 r, d = s, dn = r.s (linear_solver_pcg.hpp:117-137)
   double rs = 0.0;
@@ -271,6 +270,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
     st->iterations = k;
     st->breakdown = breakdown ? 1 : 0;
     st->done = 1;
+    st->total_iterations += k;
     if (!fixed) st->residual_carry = 0.5 * dn;
   }
 }

@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     pcg_solve_tiles(const Real* tiles, const int2* tile_ij, int ntiles, const int* trow_ptr, const int* trow_list,
                     const int* tcol_ptr, const int* tcol_list, int nb, const double* minv, const double* b, double* x,
                     double* r, double* s, double* dbuf0, double* dbuf1, double* rowpart, double* colpart,
-                    double* part_dq, double* part_rs, PcgState* st) {
+                    double* part_dq, double* part_rs, PcgState* st, double tol, int max_iter, int abs_tol,
+                    int fixed_d0) {
   constexpr int BS = 6;
   __shared__ double red[kTileWarps];
   __shared__ double drow[kTileScalars], dcol[kTileScalars];
@@ -87,12 +88,9 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
   const int gw = blockIdx.x * kTileWarps + warp, GW = gridDim.x * kTileWarps;
   const int h = tid / 24, g = tid % 24;  // row group (12 rows), column group (4 columns)
   const int n = nb * BS;
-  const double tol = st->tolerance;
-  const int max_iter = st->max_iter;
-  const bool fixed = st->fixed_d0 != 0;
+  const bool fixed = fixed_d0 != 0;
   const double d0_in = st->d0;
   const double carry = st->residual_carry;
-  const int abs_tol = st->absolute_tolerance;
 
   // r = b, x = 0, s = M^-1 r, d_{-1} = 0, dn = r.s (linear_solver_pcg.hpp:117-137)
   double rs = 0.0;
@@ -232,6 +230,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     st->iterations = k;
     st->breakdown = breakdown ? 1 : 0;
     st->done = 1;
+    st->total_iterations += k;
     if (!fixed) st->residual_carry = 0.5 * dn;
   }
 }
