@@ -681,7 +681,7 @@ struct Engine final : EngineBase {
       // reduced residual's M-norm is above that d0, i.e. while the FP32
       // storage of H / S / Dinv, not the PCG tolerance, limits the step; a
       // correction that raises the residual is undone and ends the loop.
-      if (sizeof(Real) == 4 && ok && !use_chol) {
+      if (sizeof(Real) == 4 && ok && !use_chol && c->prm.refine_max_iterations >= 0) {
         const int n = c->vec_size();
         double prev = -1.0;
         for (int k = 0; k <= c->prm.refine_max_iterations; ++k) {
@@ -1036,6 +1036,8 @@ static const char* kSolvers[][2] = {
     {"lm_cuda_chol", "Levenberg: B200 block solver, FP64, dense Cholesky"},
     {"gn_cuda_mixed", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
     {"lm_cuda_mixed", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
+    {"gn_cuda_mixed_fast", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
+    {"lm_cuda_mixed_fast", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
 };
 
 int g2oc_list_solvers(char* buf, size_t size) {
@@ -1070,9 +1072,10 @@ int g2oc_construct(const char* name, g2oc_params* p) {
   const std::string v = n.size() > 7 ? n.substr(8) : "";
   if (v.empty()) p->linear_solver = 2;  // PCG with Schur, Cholesky without
   else if (v.rfind("chol", 0) == 0) p->linear_solver = G2OC_LINEAR_CHOLESKY;
-  else if (v == "mixed") {
+  else if (v == "mixed" || v == "mixed_fast") {
     p->linear_solver = G2OC_LINEAR_PCG;
     p->precision = G2OC_PREC_MIXED;
+    if (v == "mixed_fast") p->refine_max_iterations = -1;  // the FP32-stored system's solution is the step
   } else p->linear_solver = G2OC_LINEAR_PCG;
   return G2OC_OK;
 }

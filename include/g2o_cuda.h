@@ -131,7 +131,8 @@ typedef struct g2oc_params {
   int32_t max_trials_after_failure;  /* 10 ("maxTrialsAfterFailure" property) */
   double initial_lambda;             /* 0: tau * max diag(H) ("initialLambda" property) */
   double tau;                        /* 1e-5 */
-  int32_t refine_max_iterations;     /* mixed precision: max FP64 refinement corrections per solve (default 2) */
+  int32_t refine_max_iterations;     /* mixed precision: max FP64 refinement corrections per solve (default 2);
+                                        -1: no FP64 residual check, the FP32-stored system's solution is the step */
   double refine_tolerance;           /* reserved (default 1e-10) */
 } g2oc_params;
 

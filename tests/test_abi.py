@@ -67,13 +67,17 @@ def test_library_exports_every_declared_symbol(cuda_lib):
 def test_factory_lists_and_constructs():
     fac = backend.OptimizationAlgorithmFactory.instance()
     names = fac.list_solvers()
-    for n in ["gn_cuda", "lm_cuda", "lm_cuda_pcg6_3", "gn_cuda_pcg3_3", "lm_cuda_chol", "lm_cuda_mixed"]:
+    for n in ["gn_cuda", "lm_cuda", "lm_cuda_pcg6_3", "gn_cuda_pcg3_3", "lm_cuda_chol", "lm_cuda_mixed",
+              "lm_cuda_mixed_fast"]:
         assert n in names
     for n in names:
         p = fac.construct(n)
         assert p is not None, n
         assert p.algorithm == (abi.ALGO_GAUSS_NEWTON if n.startswith("gn") else abi.ALGO_LEVENBERG)
     assert fac.construct("lm_cuda_mixed").precision == abi.PREC_MIXED
+    assert fac.construct("lm_cuda_mixed").refine_max_iterations == 2
+    fast = fac.construct("lm_cuda_mixed_fast")
+    assert fast.precision == abi.PREC_MIXED and fast.refine_max_iterations == -1
     assert fac.construct("gn_cuda_chol").linear_solver == abi.LINEAR_CHOLESKY
     assert fac.construct("gn_cuda_pcg6_3").linear_solver == abi.LINEAR_PCG
     assert fac.construct("non_existing_solver") is None

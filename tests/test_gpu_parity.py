@@ -163,12 +163,16 @@ def test_ba_lm_trajectory(backend, oracle_lib):
     assert np.abs(qc - qo).max() < 1e-4
 
 
-def test_ba_mixed_precision_reaches_fp64_chi2(backend, oracle_lib):
+@pytest.mark.parametrize("refine", [2, -1])
+def test_ba_mixed_precision_reaches_fp64_chi2(backend, oracle_lib, refine):
+    """Mixed precision, with FP64 refinement of every step (refine 2) and
+    with FP32 steps under FP64 LM control only (refine -1), reaches the FP64
+    oracle's 20-iteration chi2 within 1e-6 inside 30 iterations."""
     g = small_ba()
     o = oracle_lib.OracleProblem(g)
     _, so = o.optimize(20)
     target = so[-1]["chi2"]
-    c = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED))
+    c = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED, refine_max_iterations=refine))
     _, sc = c.optimize(30)
     best = min(s["chi2"] for s in sc)
     assert best <= target * (1 + 1e-6), (best, target)
