@@ -106,7 +106,7 @@ struct g2oc_ctx {
   g2oc::DBuf<int> hb_src_ptr, hb_src, bv_src_ptr, bv_src;
   // linear system lists
   g2oc::DBuf<int> sys_perm, sys_rptr, sys_rcol, sys_brow, sys_diag, sys_cptr, sys_cblk, sys_chunk_ptr, sys_chunk_row,
-      tile_ij, tile_off, trow_ptr, trow_list, tcol_ptr, tcol_list;
+      tile_ij, tile_off;
   int pcg_grid[4] = {0, 0, 0, 0};  // CTAs of the persistent PCG per (storage type, block size)
   int tile_grid[2] = {0, 0};       // CTAs of the dense-tile PCG per storage type
   // FP64 vectors
@@ -387,8 +387,7 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
 // PCG over dense tiles (pcg_solve_tiles), one cooperative launch
 template <typename Real>
 static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* minv, const double* rhs, double* xout,
-                         double* r, double* s, double* dbuf0, double* dbuf1, double* rowpart, double* colpart,
-                         bool fixed_d0) {
+                         double* r, double* s, double* dbuf0, double* dbuf1, double* part, bool fixed_d0) {
   cudaStream_t st = c->stream;
   int& grid = c->tile_grid[sizeof(Real) == 4 ? 1 : 0];
   if (grid == 0) {
@@ -409,16 +408,12 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
   int fixed = fixed_d0 ? 1 : 0;
   const int2* tij = reinterpret_cast<const int2*>(c->tile_ij.p);
   int ntiles = (int)(c->S.tile_ij.size() / 2);
-  const int* trp = c->trow_ptr.p;
-  const int* trl = c->trow_list.p;
-  const int* tcp = c->tcol_ptr.p;
-  const int* tcl = c->tcol_list.p;
+  int nbt = (nb + kTileBlocks - 1) / kTileBlocks;
   double* part_dq = c->partials.p;
   double* part_rs = c->partials.p + 4096;
   PcgState* stp = c->pcg.p;
-  void* args[] = {&tiles, &tij,     &ntiles,  &trp,     &trl,     &tcp,  &tcl, &nb,       &minv,    &rhs,  &xout,
-                  &r,     &s,       &dbuf0,   &dbuf1,   &rowpart, &colpart,    &part_dq, &part_rs, &stp,  &tol,
-                  &max_iter, &abs_tol, &fixed};
+  void* args[] = {&tiles, &tij,  &ntiles, &nbt,  &nb,      &minv,    &rhs, &xout,     &r,       &s,
+                  &dbuf0, &dbuf1, &part,  &part_dq, &part_rs, &stp, &tol, &max_iter, &abs_tol, &fixed};
   G2OC_K(K_PCG_TILES) {
     G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_tiles<Real>, dim3(grid), dim3(kTileThreads),
                                               args, 0, st));
@@ -438,7 +433,7 @@ struct Engine final : EngineBase {
   g2oc_ctx* c;
   // Hessian
   DBuf<Real> hpp, hll, hpl, bdc, dinv, Sval, sysval;
-  DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf, cpart, rowpart, colpart;
+  DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf, cpart, tpart;
   DBuf<Real> tiles;  // dense-tile copy of the system (nearly full 6x6-block matrices), allocated on first use
   bool tiles_fresh = false;  // tiles hold the matrix of the current solve
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
@@ -613,8 +608,11 @@ struct Engine final : EngineBase {
           const size_t nt = S.tile_ij.size() / 2;
           G2OC_TRY(tiles.alloc(nt * kTileSize));
           G2OC_CUDA_TRY(cudaMemsetAsync(tiles.p, 0, tiles.bytes(), c->stream));  // blocks outside the pattern
-          G2OC_TRY(rowpart.alloc(nt * kTileScalars));
-          G2OC_TRY(colpart.alloc(nt * kTileScalars));
+          // per block row, one slot of 6 partial sums per tile index (zero
+          // for the tiles outside the pattern)
+          const size_t nbt = (A.nb + kTileBlocks - 1) / kTileBlocks;
+          G2OC_TRY(tpart.alloc((size_t)A.nb * nbt * 6));
+          G2OC_CUDA_TRY(cudaMemsetAsync(tpart.p, 0, tpart.bytes(), c->stream));
         }
         if (!fixed_d0 || !tiles_fresh) {  // a correction solve reuses the tiles of its first solve
           G2OC_K(K_TILE_COPY) sys_to_tiles<Real><<<cdiv((long long)A.nnzb * 6, 256), 256, 0, c->stream>>>(
@@ -622,8 +620,7 @@ struct Engine final : EngineBase {
           G2OC_LAUNCH_CHECK();
           tiles_fresh = true;
         }
-        return run_pcg_tiles<Real>(c, tiles.p, A.nb, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, rowpart.p, colpart.p,
-                                   fixed_d0);
+        return run_pcg_tiles<Real>(c, tiles.p, A.nb, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, tpart.p, fixed_d0);
       }
       return run_pcg_persistent<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0);
     }
@@ -1294,10 +1291,6 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
   if (S.tile_ok) {
     G2OC_TRY(c->tile_ij.upload(S.tile_ij, st));
     G2OC_TRY(c->tile_off.upload(S.tile_off, st));
-    G2OC_TRY(c->trow_ptr.upload(S.trow_ptr, st));
-    G2OC_TRY(c->trow_list.upload(S.trow_list, st));
-    G2OC_TRY(c->tcol_ptr.upload(S.tcol_ptr, st));
-    G2OC_TRY(c->tcol_list.upload(S.tcol_list, st));
   }
   const int n = c->vec_size();
   G2OC_TRY(c->b.alloc(n));

@@ -132,8 +132,6 @@ struct Structure {
   bool tile_ok = false;
   std::vector<int> tile_ij;             // 2 per tile: tile row I, tile column J (I <= J)
   std::vector<int> tile_off;            // per internal block: offset of its (0,0) entry in the tile array
-  std::vector<int> trow_ptr, trow_list; // per tile row I: tiles (I, J)
-  std::vector<int> tcol_ptr, tcol_list; // per tile column J: tiles (I, J), I < J
 };
 
 constexpr int kSysChunk = 32;  // blocks per row chunk = lanes of a warp

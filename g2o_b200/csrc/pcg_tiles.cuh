@@ -11,9 +11,12 @@
 //      cols(J) += Tile^T d(I), per tile; d.q as d(I).Tile d(J) (twice for an
 //      off-diagonal tile);
 //   -- barrier; alpha = dn / d.q
-//   C  one warp per block row r: q_r = its tile-row and tile-column partials,
-//      d_k stored, x_r += alpha d_k, r_r -= alpha q_r, s_r = M_r^-1 r_r,
-//      partial r.s;
+//   C  one warp per block row r: q_r = the sum of its partials, d_k stored,
+//      x_r += alpha d_k, r_r -= alpha q_r, s_r = M_r^-1 r_r, partial r.s.
+//      The partials of block row r are contiguous, one slot per tile index:
+//      slot J holds the row sum of tile (I(r), J), slot I' < I(r) the column
+//      sum of tile (I', I(r)); slots of tiles outside the pattern stay zero;
+//
 //   -- barrier; dn, beta, stop test.
 // The arithmetic is FP64 whatever the storage type of the tiles. Sums run in
 // a fixed order for a given grid size (bit-reproducible on a device).
@@ -74,9 +77,8 @@ __device__ __forceinline__ void load4(const double* p, double (&m)[4]) {
 
 template <typename Real>
 __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
-    pcg_solve_tiles(const Real* tiles, const int2* tile_ij, int ntiles, const int* trow_ptr, const int* trow_list,
-                    const int* tcol_ptr, const int* tcol_list, int nb, const double* minv, const double* b, double* x,
-                    double* r, double* s, double* dbuf0, double* dbuf1, double* rowpart, double* colpart,
+    pcg_solve_tiles(const Real* tiles, const int2* tile_ij, int ntiles, int nbt, int nb, const double* minv,
+                    const double* b, double* x, double* r, double* s, double* dbuf0, double* dbuf1, double* part,
                     double* part_dq, double* part_rs, PcgState* st, double tol, int max_iter, int abs_tol,
                     int fixed_d0) {
   constexpr int BS = 6;
@@ -163,14 +165,16 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
         double v = 0.0;
 #pragma unroll
         for (int q = 0; q < 24; ++q) v += red_row[tid][q];
-        rowpart[(size_t)t * kTileScalars + tid] = v;
+        const int rr = ij.x * kTileBlocks + tid / BS;
+        if (rr < nb) part[((size_t)rr * nbt + ij.y) * BS + tid % BS] = v;
         dq += (ij.x == ij.y ? 1.0 : 2.0) * drow[tid] * v;
       } else if (ij.x != ij.y) {
         const int cc = tid - kTileScalars;
         double v = 0.0;
 #pragma unroll
         for (int q = 0; q < 8; ++q) v += red_col[q][cc];
-        colpart[(size_t)t * kTileScalars + cc] = v;
+        const int rr = ij.y * kTileBlocks + cc / BS;
+        if (rr < nb) part[((size_t)rr * nbt + ij.x) * BS + cc % BS] = v;
       }
       __syncthreads();
     }
@@ -185,17 +189,13 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     // ---- C: block rows
     rs = 0.0;
     for (int c = gw; c < nb; c += GW) {
-      const int I = c / kTileBlocks, lr = (c % kTileBlocks) * BS;
-      const int r0 = __ldg(trow_ptr + I), nr = __ldg(trow_ptr + I + 1) - r0;
-      const int c0 = __ldg(tcol_ptr + I), nc = __ldg(tcol_ptr + I + 1) - c0;
       double q[BS];
 #pragma unroll
       for (int a = 0; a < BS; ++a) q[a] = 0.0;
-      for (int e = lane; e < nr + nc; e += 32) {
-        const double* p = e < nr ? rowpart + (size_t)__ldg(trow_list + r0 + e) * kTileScalars + lr
-                                 : colpart + (size_t)__ldg(tcol_list + c0 + e - nr) * kTileScalars + lr;
+      const double* pr = part + (size_t)c * nbt * BS;
+      for (int e = lane; e < nbt; e += 32) {
 #pragma unroll
-        for (int a = 0; a < BS; ++a) q[a] += __ldcg(p + a);
+        for (int a = 0; a < BS; ++a) q[a] += __ldcg(pr + (size_t)e * BS + a);
       }
       double rc[BS], dk[BS];
 #pragma unroll

@@ -74,10 +74,6 @@ static void build_tiles(int nb, Structure& s) {
   s.tile_ok = false;
   s.tile_ij.clear();
   s.tile_off.clear();
-  s.trow_ptr.clear();
-  s.trow_list.clear();
-  s.tcol_ptr.clear();
-  s.tcol_list.clear();
   const int nnzb = s.sys_nnzb;
   if (nb < 2 * kTileBlocks) return;
   const int nbt = (nb + kTileBlocks - 1) / kTileBlocks;
@@ -94,29 +90,13 @@ static void build_tiles(int nb, Structure& s) {
   if (stored > allowed || (long long)nt * kTileBlocks * kTileBlocks * 36 >= (1LL << 31)) return;
   s.tile_ok = true;
   s.tile_ij.resize(2 * (size_t)nt);
-  s.trow_ptr.assign(nbt + 1, 0);
-  s.tcol_ptr.assign(nbt + 1, 0);
   for (int I = 0; I < nbt; ++I)
     for (int J = I; J < nbt; ++J) {
       const int t = id[(size_t)I * nbt + J];
       if (t < 0) continue;
       s.tile_ij[2 * (size_t)t] = I;
       s.tile_ij[2 * (size_t)t + 1] = J;
-      s.trow_ptr[I + 1]++;
-      if (J > I) s.tcol_ptr[J + 1]++;
     }
-  for (int I = 0; I < nbt; ++I) {
-    s.trow_ptr[I + 1] += s.trow_ptr[I];
-    s.tcol_ptr[I + 1] += s.tcol_ptr[I];
-  }
-  s.trow_list.resize(s.trow_ptr[nbt]);
-  s.tcol_list.resize(s.tcol_ptr[nbt]);
-  std::vector<int> rfill(s.trow_ptr.begin(), s.trow_ptr.end() - 1), cfill(s.tcol_ptr.begin(), s.tcol_ptr.end() - 1);
-  for (int t = 0; t < nt; ++t) {
-    const int I = s.tile_ij[2 * (size_t)t], J = s.tile_ij[2 * (size_t)t + 1];
-    s.trow_list[rfill[I]++] = t;
-    if (J > I) s.tcol_list[cfill[J]++] = t;
-  }
   constexpr int TS = kTileBlocks * 6;  // scalar rows of a tile (6x6 blocks)
   s.tile_off.resize(nnzb);
   for (int k = 0; k < nnzb; ++k) {
