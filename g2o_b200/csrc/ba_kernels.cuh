@@ -375,24 +375,33 @@ struct Vec2<float> {
 // b_l(a) is formed from the same staged blocks. S is written in the row-SoA
 // layout of sys_offset.
 template <typename Real, int THREADS, bool STAGE>
-__global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 3 : 1)
+__global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl, const Real* dinv,
                const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs, const int* s_hpp,
                const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l, double* bs) {
   using R2 = typename Vec2<Real>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[THREADS / 32][21];
+  __shared__ double red[THREADS / 32][27];
   const int r = blockIdx.x;
   const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
-  // the camera's BD_a = B_a Dinv_l blocks, one thread per block: staged in
-  // shared memory, or (cameras with more blocks than shared memory holds)
-  // written to the camera-major scratch bdc and read back in place
+  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
+  Real* Sr = S + (size_t)rb * 36;
+  // One pass over the camera's Hpl blocks B_a, one thread per block: BD_a =
+  // B_a Dinv_l, staged in shared memory (or, for cameras with more blocks
+  // than shared memory holds, written to the camera-major scratch bdc and read
+  // back in place); with B_a still in registers, its diagonal-block term
+  // BD_a B_a^T (upper 21 entries) and its right-hand-side term BD_a b_l.
   Real* BDw = STAGE ? reinterpret_cast<Real*>(smem_raw) : const_cast<Real*>(bdc) + (size_t)a0 * 18;
+  Real dacc[21];
+  double racc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int u = 0; u < 21; ++u) dacc[u] = 0;
   for (int t = threadIdx.x; t < na; t += THREADS) {
     const int a = hc_blk[a0 + t];
+    const int l = hc_col[a0 + t];
     const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)a * 18);
-    const Real* Dl = dinv + (size_t)hc_col[a0 + t] * 9;
-    Real b[18], D[9];
+    const Real* Dl = dinv + (size_t)l * 9;
+    Real b[18], D[9], bd[18];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
       const R2 v = B2[q];
@@ -404,35 +413,33 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 3 : 1)
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) o[i * 3 + c] = b[i * 3] * D[c] + b[i * 3 + 1] * D[3 + c] + b[i * 3 + 2] * D[6 + c];
+      for (int c = 0; c < 3; ++c) {
+        bd[i * 3 + c] = b[i * 3] * D[c] + b[i * 3 + 1] * D[3 + c] + b[i * 3 + 2] * D[6 + c];
+        o[i * 3 + c] = bd[i * 3 + c];
+      }
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int c = i; c < 6; ++c, ++u)
+        dacc[u] += bd[i * 3] * b[c * 3] + bd[i * 3 + 1] * b[c * 3 + 1] + bd[i * 3 + 2] * b[c * 3 + 2];
+    if (bs) {
+      const double* bl = b_l + (size_t)l * 3;
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        racc[q] += (double)bd[q * 3] * bl[0] + (double)bd[q * 3 + 1] * bl[1] + (double)bd[q * 3 + 2] * bl[2];
+    }
   }
   if (!STAGE) __threadfence_block();
-  __syncthreads();
-  const Real* BDa = BDw;
-  // diagonal block
-  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
-  Real* Sr = S + (size_t)rb * 36;
+  // fixed-order CTA sum of the 21 diagonal-block and 6 right-hand-side terms
+  // (block_sum_array ends with a barrier, which also publishes the staged BD)
   {
-    double acc[21];
+    double acc[27];
 #pragma unroll
-    for (int t = 0; t < 21; ++t) acc[t] = 0.0;
-    for (int t = threadIdx.x; t < na; t += THREADS) {
-      const Real* D = BDa + (size_t)t * 18;
-      const Real* B = hpl + (size_t)hc_blk[a0 + t] * 18;
-      Real d[18], b[18];
+    for (int u = 0; u < 21; ++u) acc[u] = (double)dacc[u];
 #pragma unroll
-      for (int q = 0; q < 18; ++q) {
-        d[q] = D[q];
-        b[q] = B[q];
-      }
-      int u = 0;
-#pragma unroll
-      for (int i = 0; i < 6; ++i)
-#pragma unroll
-        for (int c = i; c < 6; ++c, ++u)
-          acc[u] += (double)(d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2]);
-    }
-    block_sum_array<double, 21, THREADS>(acc, &red[0][0]);
+    for (int q = 0; q < 6; ++q) acc[21 + q] = racc[q];
+    block_sum_array<double, 27, THREADS>(acc, &red[0][0]);
     if (threadIdx.x == 0) {
       const int hb = s_hpp[rb];
       int u = 0;
@@ -447,23 +454,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 3 : 1)
             Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
           }
         }
+      if (bs) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) bs[(size_t)r * 6 + q] = b_p[(size_t)r * 6 + q] - acc[21 + q];
+      }
     }
   }
-  if (bs) {
-    // reduced right-hand side, spread over the whole CTA (fixed assignment)
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int t = threadIdx.x; t < na; t += THREADS) {
-      const double* bl = b_l + (size_t)hc_col[a0 + t] * 3;
-      const Real* D = BDa + (size_t)t * 18;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) acc[q] += (double)D[q * 3] * bl[0] + (double)D[q * 3 + 1] * bl[1] + (double)D[q * 3 + 2] * bl[2];
-    }
-    block_sum_array<double, 6, THREADS>(acc, &red[0][0]);
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) bs[(size_t)r * 6 + q] = b_p[(size_t)r * 6 + q] - acc[q];
-    }
-  }
+  const Real* BDa = BDw;
   // off-diagonal blocks (the row's diagonal is its first block)
   const int half = threadIdx.x & 1;
   for (int j = 1 + (threadIdx.x >> 1); j < nblk; j += THREADS / 2) {

@@ -559,8 +559,8 @@ struct Engine final : EngineBase {
       G2OC_LAUNCH_CHECK();
     }
     if (S.Cf == 0) return G2OC_OK;
-    // FP32 storage: 256 threads, three CTAs per SM; FP64: 512 threads, one
-    constexpr int T = sizeof(Real) == 4 ? 256 : 512;
+    // FP32 storage: 384 threads, two CTAs per SM; FP64: 512 threads, one
+    constexpr int T = sizeof(Real) == 4 ? 384 : 512;
     const double* bp = c->b.p;
     const double* bl = c->b.p + (size_t)S.Cf * 6;
     if (stage_in_smem) {
