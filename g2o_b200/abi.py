@@ -26,7 +26,7 @@ G2OC_ERR_NOT_SUPPORTED = 10
 
 ERROR_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "BAD_GRAPH", 3: "CUDA", 4: "NOT_PD", 5: "NAN",
-    6: "STATE", 7: "NO_DEVICE", 8: "UNKNOWN_SOLVER", 9: "TIMEOUT", 10: "NOT_SUPPORTED",
+    6: "STATE", 7: "NO_DEVICE", 8: "UNKNOWN_SOLVER", 9: "TIMEOUT", 10: "NOT_SUPPORTED", 11: "NOT_CONVERGED",
 }
 
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
@@ -104,6 +104,10 @@ class G2ocIterationStats(C.Structure):
 
 class G2ocKernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("total_ms", C.c_double)]
+
+
+class G2ocBackwardStats(C.Structure):
+    _fields_ = [("refinement_steps", C.c_int32), ("pcg_iterations", C.c_int32), ("relative_residual", C.c_double)]
 
 
 class G2ocHessianInfo(C.Structure):

@@ -24,8 +24,8 @@ from typing import List, Optional
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocHessianInfo, G2ocIterationStats, G2ocKernelStat,
-                  G2ocParams, Graph, POSE_DIM, POSE_EST_DIM)
+from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocBackwardStats, G2ocHessianInfo, G2ocIterationStats,
+                  G2ocKernelStat, G2ocParams, Graph, POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libg2o_b200.so")
@@ -71,6 +71,7 @@ def library() -> C.CDLL:
         "g2oc_get_hessian": ([vp, dp, dp, dp, dp], C.c_int),
         "g2oc_schur": ([vp, C.c_double, dp, dp], C.c_int),
         "g2oc_solve": ([vp, C.c_double, dp, ip], C.c_int),
+        "g2oc_backward": ([vp, dp, dp, dp, vp], C.c_int),
         "g2oc_solve_block_system": ([vp, C.c_int32, C.c_int32, ip, C.c_int32, ip, dp, dp, dp, ip], C.c_int),
         "g2oc_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "g2oc_restore_initial_estimates": ([vp], C.c_int),
@@ -276,6 +277,22 @@ class CudaProblem:
         bs = np.empty(i.num_free_poses * pd)
         _check(library().g2oc_schur(self._h, lam, _p(S), _p(bs)))
         return S, bs
+
+    def backward(self, dl_dpose, dl_dpoint):
+        """g2oc_backward: implicit-function-theorem gradients of a loss on the
+        current (converged) estimates with respect to each edge's measurement
+        (num_edges x 2) and the log-scale of its information matrix
+        (num_edges,). dl_dpose (num_poses x 6, [omega, upsilon] of the
+        left-multiplied update) and dl_dpoint (num_points x 3) are dL/dx."""
+        g = self.graph
+        dx = np.ascontiguousarray(np.concatenate([np.asarray(dl_dpose, np.float64).reshape(-1),
+                                                  np.asarray(dl_dpoint, np.float64).reshape(-1)]))
+        dmeas = np.zeros((g.num_edges, 2))
+        dlogw = np.zeros(g.num_edges)
+        st = G2ocBackwardStats()
+        _check(library().g2oc_backward(self._h, _p(dx), _p(dmeas), _p(dlogw), C.byref(st)))
+        return dmeas, dlogw, {"refinement_steps": st.refinement_steps, "pcg_iterations": st.pcg_iterations,
+                              "relative_residual": st.relative_residual}
 
     def solve(self, lam):
         x = np.empty(self.info.vector_size)

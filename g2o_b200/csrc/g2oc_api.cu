@@ -4,6 +4,8 @@
 // per-vertex, per-block and per-vector loop of the iteration runs in the
 // kernels of ba_kernels.cuh, pg_kernels.cuh, pcg_kernels.cuh,
 // lm_kernels.cuh and cholesky.cuh.
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
@@ -12,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint_kernels.cuh"
 #include "ba_kernels.cuh"
 #include "cholesky.cuh"
 #include "g2oc_internal.h"
@@ -48,6 +51,11 @@ constexpr int kRedBlocks = 592;    // 4 x 148 SMs: fixed grid of the reductions
 constexpr int kChi2Blocks = 2048;  // BA chi2: ~2 edges per thread for the 1M-edge graphs
 constexpr int kPcgChunkMax = 64;
 constexpr int kMixedInnerMaxIter = 256;
+// adjoint: outer CG steps, the recurrence's stopping residual |g - H v| / |g|,
+// and the true residual accepted at the end
+constexpr int kAdjointMaxSteps = 100;
+constexpr double kAdjointTolerance = 1e-12;
+constexpr double kAdjointAcceptance = 1e-6;
 
 // --------------------------------------------------------------- engine
 struct EngineBase {
@@ -58,6 +66,9 @@ struct EngineBase {
   virtual int solve(double lambda) = 0;  // -> x, sc.solve_ok (PCG iterations: PcgState::total_iterations)
   virtual int get_hessian(double* hpp, double* hll, double* hpl) = 0;
   virtual int schur_export(double lambda, double* S, double* bs) = 0;
+  // Gauss-Newton solve H x = rhs (lambda 0) with a given device right-hand
+  // side in Hessian order, through the same Schur + PCG / Cholesky path (BA)
+  virtual int solve_rhs(const double* rhs, double* out) = 0;
 };
 
 // kernel identifiers for the launch counters and the optional per-launch
@@ -66,14 +77,14 @@ enum KernelId {
   K_CHI2, K_ERRORS, K_JACOBIANS, K_LANDMARK_PASS, K_CAMERA_PASS, K_SCHUR_LANDMARK, K_SCHUR_BLOCKS, K_SCHUR_RHS,
   K_BACKSUB, K_RESID_CAM, K_RESID_LM, K_OPLUS, K_MAX_DIAG, K_PCG_DIAG_INV, K_PCG_INIT, K_PCG_SPMV, K_PCG_UPDATE,
   K_PCG_CHECK, K_PG_LINEARIZE, K_PG_ASSEMBLE_H, K_PG_ASSEMBLE_B, K_DAMP, K_LM_CONTROL, K_REDUCE, K_AXPY,
-  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_COUNT
+  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_BACKWARD, K_COUNT
 };
 static const char* kKernelNames[K_COUNT] = {
   "chi2", "errors", "jacobians", "ba_landmark_pass", "ba_camera_pass", "schur_landmark", "schur_blocks",
   "schur_rhs", "ba_backsub", "ba_resid_cam", "ba_resid_lm", "oplus", "max_diag", "pcg_diag_inv", "pcg_init",
   "pcg_spmv", "pcg_update", "pcg_check_dn", "pg_linearize", "pg_assemble_h", "pg_assemble_b", "damp_diag",
   "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db", "io_reorder", "pcg_solve", "pcg_solve_tiles",
-  "sys_to_tiles"};
+  "sys_to_tiles", "ba_backward"};
 
 struct PendingTiming {
   int kid;
@@ -111,6 +122,7 @@ struct g2oc_ctx {
   int tile_grid[2] = {0, 0};       // CTAs of the dense-tile PCG per storage type
   // FP64 vectors
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
+  g2oc::DBuf<double> adj_g, adj_v, adj_r, adj_dv, adj_p, adj_q, adj_rold, adj_dmeas, adj_dlogw;  // adjoint
   g2oc::DBuf<g2oc::DevScalars> sc;
   g2oc::DBuf<g2oc::PcgState> pcg;
   g2oc::DBuf<int> flag;  // nonfinite flag
@@ -426,6 +438,8 @@ static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, doubl
   G2OC_LAUNCH_CHECK();
   return G2OC_OK;
 }
+
+static int reset_pcg(g2oc_ctx* c);
 
 // ---------------------------------------------------------- the engine
 template <typename Real>
@@ -789,6 +803,35 @@ struct Engine final : EngineBase {
       to_double(h, hpl_out);
     }
     return G2OC_OK;
+  }
+
+  int solve_rhs(const double* rhs, double* out) override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (!(S.ba && S.schur) || S.Cf == 0) {
+      set_error("the adjoint solve needs a bundle adjustment with free cameras and landmarks");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    const bool use_chol = c->prm.linear_solver == G2OC_LINEAR_CHOLESKY;
+    G2OC_TRY(schur(0.0, nullptr));
+    const double* rp = rhs;
+    const double* rl = rhs + (size_t)S.Cf * 6;
+    G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
+    int ok = 1;
+    if (use_chol) {
+      G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
+      if (!ok) {
+        set_error("adjoint solve: the reduced system is not positive definite");
+        return G2OC_ERR_NOT_PD;
+      }
+    } else {
+      // no carried threshold (LinearSolverPCG::_residual) between these solves
+      static const double kNoCarry = -1.0;
+      G2OC_CUDA_TRY(cudaMemcpyAsync(&c->pcg.p->residual_carry, &kNoCarry, sizeof(double), cudaMemcpyHostToDevice, st));
+      G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false));
+    }
+    G2OC_CUDA_TRY(cudaMemcpyAsync(out, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return backsub(rl, c->xs.p, out + (size_t)S.Cf * 6);
   }
 
   int schur_export(double lambda, double* S_out, double* bs_out) override {
@@ -1608,6 +1651,151 @@ int g2oc_solve(g2oc_ctx* c, double lambda, double* x, int32_t* iters) {
   if (iters) *iters = stv.iterations_linear_solver;
   if (x) G2OC_CUDA_TRY(cudaMemcpy(x, c->x.p, c->x.bytes(), cudaMemcpyDeviceToHost));
   return h.solve_ok ? G2OC_OK : G2OC_ERR_NOT_PD;
+}
+
+// ------------------------------------------------------------ adjoint
+// a . b of device vectors, on the host (one wait)
+static int dev_dot(g2oc_ctx* c, const double* a, const double* b, int n, double* out) {
+  G2OC_K(K_LM_CONTROL) dot_partials<<<kRedBlocks, 256, 0, c->stream>>>(a, b, n, c->partials.p);
+  G2OC_LAUNCH_CHECK();
+  G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &c->sc.p->refine_rnorm, nullptr));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(out, &c->sc.p->refine_rnorm, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G2OC_OK;
+}
+
+// q = H p for the exact Hessian of F at x* (forward-mode dual numbers,
+// adjoint_kernels.cuh)
+static int adj_hessian_product(g2oc_ctx* c, const double* p, double* q) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  if (S.Pf > 0 && S.lm_warp_ok) {
+    const int nch = (int)S.lm_chunk_ptr.size() - 1;
+    G2OC_K(K_BACKWARD) ba_hvp_landmark_warp<<<cdiv(nch, 8), 256, 0, st>>>(
+        c->ba_edges(), c->ba_vertices(), c->lm_chunk_ptr.p, nch, c->e_lm.p, c->pose_h.p, S.Cf, p, q);
+  } else if (S.Pf > 0) {
+    G2OC_K(K_BACKWARD) ba_hvp_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p,
+                                                                        S.Pf, c->pose_h.p, S.Cf, p, q);
+  }
+  BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
+  G2OC_K(K_BACKWARD) ba_hvp_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p, S.Cf, p, q);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
+// preconditioner: the Gauss-Newton Schur solve at x*
+static int adj_precondition(g2oc_ctx* c, const double* r, double* z) {
+  G2OC_TRY(c->eng->build_system());
+  return c->eng->solve_rhs(r, z);
+}
+
+int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL_dlogw, g2oc_backward_stats* stats) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!dL_dx || !dL_dmeas || !dL_dlogw) {
+    set_error("dL_dx, dL_dmeas and dL_dlogw must be given");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const Structure& S = c->S;
+  if (!S.ba || !S.schur || S.Cf == 0) {
+    set_error("g2oc_backward supports bundle adjustment (EdgeProjectXYZ2UV) with free cameras and landmarks");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  cudaStream_t st = c->stream;
+  const int n = c->vec_size();
+  // dL/dx in Hessian order (free cameras, then free landmarks)
+  std::vector<double> g(n);
+  for (int h = 0; h < S.Cf; ++h)
+    for (int a = 0; a < 6; ++a) g[(size_t)h * 6 + a] = dL_dx[(size_t)S.free_pose_of_h[h] * 6 + a];
+  for (int l = 0; l < S.Pf; ++l)
+    for (int a = 0; a < 3; ++a)
+      g[(size_t)S.Cf * 6 + l * 3 + a] = dL_dx[(size_t)S.C * 6 + (size_t)S.free_point_of_l[l] * 3 + a];
+  G2OC_TRY(c->adj_g.upload(g, st));
+  for (auto* bf : {&c->adj_v, &c->adj_r, &c->adj_dv, &c->adj_p, &c->adj_q, &c->adj_rold})
+    G2OC_TRY(bf->alloc(n));
+  const size_t nb = (size_t)n * sizeof(double);
+  // v = H^-1 g by flexible preconditioned conjugate gradients on the exact
+  // Hessian of F (FP64 products by forward-mode differentiation),
+  // preconditioned by the Gauss-Newton Schur solve in the context's
+  // precision and linear solver; Polak-Ribiere beta, since the inner solve
+  // is itself iterative
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->adj_v.p, 0, nb, st));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->adj_r.p, c->adj_g.p, nb, cudaMemcpyDeviceToDevice, st));
+  double gg = 0.0;
+  G2OC_TRY(dev_dot(c, c->adj_g.p, c->adj_g.p, n, &gg));
+  int steps = 0;
+  double rel = gg > 0.0 ? 1.0 : 0.0;
+  G2OC_TRY(reset_pcg(c));
+  if (gg > 0.0) {
+    G2OC_TRY(adj_precondition(c, c->adj_r.p, c->adj_dv.p));  // z
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->adj_p.p, c->adj_dv.p, nb, cudaMemcpyDeviceToDevice, st));
+    double rz = 0.0;
+    G2OC_TRY(dev_dot(c, c->adj_r.p, c->adj_dv.p, n, &rz));
+    while (steps < kAdjointMaxSteps) {
+      G2OC_TRY(adj_hessian_product(c, c->adj_p.p, c->adj_q.p));
+      double pq = 0.0;
+      G2OC_TRY(dev_dot(c, c->adj_p.p, c->adj_q.p, n, &pq));
+      ++steps;
+      if (!(pq > 0.0) || !(rz > 0.0)) break;  // not positive definite along p: not at a minimum
+      const double alpha = rz / pq;
+      G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->adj_v.p, c->adj_p.p, alpha, n);
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->adj_rold.p, c->adj_r.p, nb, cudaMemcpyDeviceToDevice, st));
+      G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->adj_r.p, c->adj_q.p, -alpha, n);
+      G2OC_LAUNCH_CHECK();
+      double rr = 0.0;
+      G2OC_TRY(dev_dot(c, c->adj_r.p, c->adj_r.p, n, &rr));
+      rel = std::sqrt(rr / gg);
+      if (rel <= kAdjointTolerance) break;
+      G2OC_TRY(adj_precondition(c, c->adj_r.p, c->adj_dv.p));
+      double rz_new = 0.0, zr_old = 0.0;
+      G2OC_TRY(dev_dot(c, c->adj_r.p, c->adj_dv.p, n, &rz_new));
+      G2OC_TRY(dev_dot(c, c->adj_rold.p, c->adj_dv.p, n, &zr_old));
+      const double beta = (rz_new - zr_old) / rz;
+      G2OC_K(K_AXPY) xpay_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->adj_p.p, c->adj_dv.p, beta, n);
+      G2OC_LAUNCH_CHECK();
+      rz = rz_new;
+    }
+    // the true residual |g - H v| / |g|
+    G2OC_TRY(adj_hessian_product(c, c->adj_v.p, c->adj_q.p));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->adj_r.p, c->adj_g.p, nb, cudaMemcpyDeviceToDevice, st));
+    G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->adj_r.p, c->adj_q.p, -1.0, n);
+    G2OC_LAUNCH_CHECK();
+    double rr = 0.0;
+    G2OC_TRY(dev_dot(c, c->adj_r.p, c->adj_r.p, n, &rr));
+    rel = std::sqrt(rr / gg);
+  }
+  c->system_built = false;  // the preconditioner rebuilt the engine's H
+  DevScalars h;
+  g2oc_iteration_stats tmp;
+  memset(&tmp, 0, sizeof(tmp));
+  G2OC_TRY(read_state(c, &h, &tmp));
+  // per-edge gradients, caller's edge order (zero for inactive edges)
+  G2OC_TRY(c->adj_dmeas.alloc((size_t)S.E * 2 + 1));
+  G2OC_TRY(c->adj_dlogw.alloc((size_t)S.E + 1));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->adj_dmeas.p, 0, c->adj_dmeas.bytes(), st));
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->adj_dlogw.p, 0, c->adj_dlogw.bytes(), st));
+  const int na = (int)S.act.size();
+  if (na > 0) {
+    G2OC_K(K_BACKWARD) ba_backward_edges<<<cdiv(na, 128), 128, 0, st>>>(
+        c->ba_edges(), c->ba_vertices(), c->pose_h.p, c->point_l.p, S.Cf, c->adj_v.p, c->src_dev.p, c->adj_dmeas.p,
+        c->adj_dlogw.p);
+    G2OC_LAUNCH_CHECK();
+  }
+  if (S.E > 0) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(dL_dmeas, c->adj_dmeas.p, (size_t)S.E * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                  st));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(dL_dlogw, c->adj_dlogw.p, (size_t)S.E * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (stats) {
+    stats->refinement_steps = steps;
+    stats->pcg_iterations = tmp.iterations_linear_solver;
+    stats->relative_residual = rel;
+  }
+  if (rel > kAdjointAcceptance) {
+    set_error("adjoint solve stopped at relative residual %.3e after %d steps", rel, steps);
+    return G2OC_ERR_NOT_CONVERGED;
+  }
+  return G2OC_OK;
 }
 
 int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, const int32_t* offs, int32_t nnzb,

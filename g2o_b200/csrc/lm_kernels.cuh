@@ -67,6 +67,20 @@ static __global__ void sumsq_partials(const double* a, int n, double* partials) 
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
+// partial sums of a . b
+static __global__ void dot_partials(const double* a, const double* b, int n, double* partials) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+  s = block_sum1(s);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// y = x + a * y
+static __global__ void xpay_kernel(double* y, const double* x, double a, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i] + a * y[i];
+}
+
 static __global__ void axpy_kernel(double* y, const double* x, double a, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] += a * x[i];

@@ -292,6 +292,35 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     return g
 
 
+def adjoint_problem(num_cameras=200, num_points=40_000, seed=SEED_BASE + 4, robust=False):
+    """The adjoint instance: the BA generator without outliers (and, unless
+    asked, without a robust kernel), 200 cameras / 40k points by default."""
+    g = bundle_adjustment(num_cameras=num_cameras, num_points=num_points, outlier_ratio=0.0, seed=seed)
+    if not robust:
+        g.robust_delta = None
+    return g
+
+
+def camera_centres(pose_est):
+    """World positions of VertexSE3Expmap cameras (t, q world->camera): -R^T t."""
+    t = pose_est[:, :3]
+    q = pose_est[:, 3:7]  # x y z w
+    R = _quat_to_rot(q)
+    return -np.einsum("nba,nb->na", R, t), R
+
+
+def centre_loss(pose_est, truth_pose):
+    """L = sum_i |c_i - c_i^truth|^2 and dL/dx in the update coordinates of
+    VertexSE3Expmap (T <- exp([omega, upsilon]) T): dL/domega = 0,
+    dL/dupsilon = -2 R (c - c^truth)."""
+    c, R = camera_centres(pose_est)
+    ct, _ = camera_centres(truth_pose)
+    d = c - ct
+    grad = np.zeros((len(pose_est), 6))
+    grad[:, 3:] = -2.0 * np.einsum("nab,nb->na", R, d)
+    return float((d * d).sum()), grad
+
+
 CONFIGS = {
     "pg2d": lambda: pose_graph_2d(),
     "pg3d": lambda: pose_graph_3d(),

@@ -75,6 +75,7 @@ extern "C" {
 #define G2OC_ERR_UNKNOWN_SOLVER 8   /* g2oc_construct: name not registered */
 #define G2OC_ERR_TIMEOUT 9          /* a bounded device-side wait gave up */
 #define G2OC_ERR_NOT_SUPPORTED 10   /* combination not implemented */
+#define G2OC_ERR_NOT_CONVERGED 11   /* an iterative refinement stopped above its tolerance */
 
 /* vertex / edge types (g2o class names) */
 #define G2OC_POSE_SE2 1        /* VertexSE2: estimate (x, y, theta) */
@@ -172,6 +173,13 @@ typedef struct g2oc_kernel_stat {
   double total_ms;
 } g2oc_kernel_stat;
 
+/* outcome of g2oc_backward */
+typedef struct g2oc_backward_stats {
+  int32_t refinement_steps;   /* Gauss-Newton solves applied to the exact-Hessian residual */
+  int32_t pcg_iterations;     /* summed over those solves (0 with Cholesky) */
+  double relative_residual;   /* |dL/dx - H v| / |dL/dx| at the end */
+} g2oc_backward_stats;
+
 typedef struct g2oc_ctx g2oc_ctx;
 
 /* library */
@@ -226,6 +234,26 @@ int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations)
    context's stream; read the per-kernel counts and times and the total count */
 int g2oc_set_kernel_timing(g2oc_ctx* ctx, int enable);
 int g2oc_get_kernel_stats(g2oc_ctx* ctx, g2oc_kernel_stat* out, int capacity, int* count, int64_t* total_launches);
+
+/* Adjoint of the optimum (no counterpart in the reference, which has no
+   differentiation): implicit-function-theorem gradients of a loss L(x*) on the
+   current (converged) estimates x* with respect to each edge's measurement and
+   the log of a scale on its information matrix (Omega_e -> exp(s_e) Omega_e,
+   at s_e = 0). dL_dx is dL/dx in the vertices' update coordinates
+   (VertexSE3Expmap: the 6-vector [omega, upsilon] of T <- exp(.) T; points: 3),
+   in vertex order: num_poses * 6 values, then num_points * 3; entries of fixed
+   or inactive vertices are ignored. With F = 1/2 sum_e rho(e^T Omega e) and
+   G = grad F, one extra solve v = H^-1 dL/dx gives dL/dtheta = -(dG/dtheta)^T v.
+   H is the exact Hessian of F: the context's Gauss-Newton Schur solve (its
+   precision and linear solver) is refined in FP64 against Hessian-vector
+   products taken as central differences of the FP64 gradient. Outputs, in
+   edge order: dL_dmeas (num_edges * 2) and dL_dlogw (num_edges); inactive
+   edges get 0. Bundle adjustment (EDGE_PROJECT_XYZ2UV) only;
+   G2OC_ERR_NOT_SUPPORTED otherwise, G2OC_ERR_NOT_CONVERGED when the
+   refinement stalls (the gradients are still written). The estimates are left
+   unchanged. */
+int g2oc_backward(g2oc_ctx* ctx, const double* dL_dx, double* dL_dmeas, double* dL_dlogw,
+                  g2oc_backward_stats* stats);
 
 /* LinearSolver::solve on a caller block matrix: symmetric, upper blocks given
    column-major as (row, col) block pairs with row-major dense values; block
