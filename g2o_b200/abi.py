@@ -106,6 +106,17 @@ class G2ocKernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("total_ms", C.c_double)]
 
 
+class G2ocWindowStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("trials", C.c_int32), ("result", C.c_int32), ("solve_ok", C.c_int32),
+                ("cholesky_threads", C.c_int32), ("rounds", C.c_int32), ("chi2_initial", C.c_double),
+                ("chi2", C.c_double), ("lambda_", C.c_double)]
+
+    def as_dict(self):
+        return {"iterations": self.iterations, "trials": self.trials, "result": self.result,
+                "solve_ok": self.solve_ok, "cholesky_threads": self.cholesky_threads, "rounds": self.rounds,
+                "chi2_initial": self.chi2_initial, "chi2": self.chi2, "lambda": self.lambda_}
+
+
 class G2ocBackwardStats(C.Structure):
     _fields_ = [("refinement_steps", C.c_int32), ("pcg_iterations", C.c_int32), ("relative_residual", C.c_double)]
 

@@ -24,8 +24,8 @@ from typing import List, Optional
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocBackwardStats, G2ocHessianInfo, G2ocIterationStats,
-                  G2ocKernelStat, G2ocParams, Graph, POSE_DIM, POSE_EST_DIM)
+from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
+                  G2ocIterationStats, G2ocKernelStat, G2ocParams, G2ocWindowStats, Graph, POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libg2o_b200.so")
@@ -72,6 +72,9 @@ def library() -> C.CDLL:
         "g2oc_schur": ([vp, C.c_double, dp, dp], C.c_int),
         "g2oc_solve": ([vp, C.c_double, dp, ip], C.c_int),
         "g2oc_backward": ([vp, dp, dp, dp, vp], C.c_int),
+        "g2oc_upload_windows": ([vp, C.c_int32, vp], C.c_int),
+        "g2oc_optimize_windows": ([vp, C.c_int32, vp], C.c_int),
+        "g2oc_download_window": ([vp, C.c_int32, dp, dp], C.c_int),
         "g2oc_solve_block_system": ([vp, C.c_int32, C.c_int32, ip, C.c_int32, ip, dp, dp, dp, ip], C.c_int),
         "g2oc_get_stream": ([vp, C.POINTER(vp)], C.c_int),
         "g2oc_restore_initial_estimates": ([vp], C.c_int),
@@ -299,6 +302,67 @@ class CudaProblem:
         it = C.c_int32()
         st = library().g2oc_solve(self._h, lam, _p(x), C.byref(it))
         return st, x, it.value
+
+
+class CudaWindows:
+    """Many independent bundle-adjustment windows in one context
+    (g2oc_upload_windows / g2oc_optimize_windows / g2oc_download_window)."""
+
+    def __init__(self, windows, params: Optional[G2ocParams] = None, device: int = 0):
+        self.windows = list(windows)
+        self._h = C.c_void_p()
+        _check(library().g2oc_create(device, C.byref(self._h)))
+        self.params = params or default_params()
+        _check(library().g2oc_set_params(self._h, C.byref(self.params)))
+        self._cg = [w.to_c() for w in self.windows]
+        arr = (G2ocGraph * len(self._cg))(*self._cg)
+        self._arr = arr
+        _check(library().g2oc_upload_windows(self._h, len(self._cg), arr))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            library().g2oc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(library().g2oc_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def restore_initial_estimates(self):
+        _check(library().g2oc_restore_initial_estimates(self._h))
+
+    def optimize(self, iterations):
+        st = (G2ocWindowStats * len(self.windows))()
+        _check(library().g2oc_optimize_windows(self._h, iterations, st))
+        return [s.as_dict() for s in st]
+
+    def estimates(self, w):
+        g = self.windows[w]
+        pose = np.empty((g.num_poses, 7))
+        point = np.empty((max(g.num_points, 1), 3))
+        _check(library().g2oc_download_window(self._h, w, _p(pose), _p(point)))
+        return pose, point[: g.num_points]
+
+    def set_kernel_timing(self, enable: bool):
+        _check(library().g2oc_set_kernel_timing(self._h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        arr = (G2ocKernelStat * 64)()
+        n = C.c_int()
+        tot = C.c_int64()
+        _check(library().g2oc_get_kernel_stats(self._h, arr, 64, C.byref(n), C.byref(tot)))
+        return tot.value, {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 64))}
 
 
 def solve_block_system(linear_solver, block_offsets, block_rc, values, b, params=None, device=0):

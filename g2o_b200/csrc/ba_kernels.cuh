@@ -326,9 +326,10 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
 // row's blocks are contiguous for the Schur row kernel.
 template <typename Real>
 __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_ptr, const int* hc_index, int Pf,
-                               double lambda, Real* dinv, Real* bdc, int* nonfinite) {
+                               double lambda_all, const double* lambda_of, Real* dinv, Real* bdc, int* nonfinite) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= Pf) return;
+  const double lambda = lambda_of ? lambda_of[l] : lambda_all;  // per landmark (batched windows)
   const Real* h = hll + (size_t)l * 6;
   double A[9] = {(double)h[0] + lambda, (double)h[1], (double)h[2],
                  (double)h[1], (double)h[3] + lambda, (double)h[4],
@@ -374,15 +375,22 @@ struct Vec2<float> {
 // With bs != nullptr the reduced right-hand side bs_r = b_r - sum_a BD_a
 // b_l(a) is formed from the same staged blocks. S is written in the row-SoA
 // layout of sys_offset.
-template <typename Real, int THREADS, bool STAGE>
+// G = lanes per off-diagonal block: lane pairs split the block's 6 rows in two
+// halves and the G / 2 pairs of a group split its pair list (partial sums
+// combined by a fixed xor tree). rows: the camera rows of this launch (or
+// nullptr: row = blockIdx.x); the row's G is chosen from its pair-list lengths.
+template <typename Real, int THREADS, bool STAGE, int G = 2>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
-    schur_rows(const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl, const Real* dinv,
-               const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr, const int2* pairs, const int* s_hpp,
-               const Real* hpp, double lambda, Real* S, const double* b_p, const double* b_l, double* bs) {
+    schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
+               const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
+               const int2* pairs, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
+               const double* b_p, const double* b_l, double* bs) {
+  static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per block: a power of two in [2, 32]");
   using R2 = typename Vec2<Real>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[THREADS / 32][27];
-  const int r = blockIdx.x;
+  const int r = rows ? rows[blockIdx.x] : blockIdx.x;
+  const double lambda = lambda_of ? lambda_of[r] : lambda_all;  // per camera row (batched windows)
   const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
   const int rb = rptr[r], nblk = rptr[r + 1] - rb;
   Real* Sr = S + (size_t)rb * 36;
@@ -461,9 +469,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     }
   }
   const Real* BDa = BDw;
-  // off-diagonal blocks (the row's diagonal is its first block)
-  const int half = threadIdx.x & 1;
-  for (int j = 1 + (threadIdx.x >> 1); j < nblk; j += THREADS / 2) {
+  // off-diagonal blocks (the row's diagonal is its first block); the loop
+  // runs the same number of times in every lane, so the group reduction's
+  // shuffles see full warps
+  const int half = threadIdx.x & 1, sub = (threadIdx.x % G) >> 1;
+  for (int j0 = 1; j0 < nblk; j0 += THREADS / G) {
+    const int j = j0 + (int)threadIdx.x / G;
+    const bool valid = j < nblk;
     const int k = rb + j;
     // pair products summed in the storage type (FP64 on the FP64 path; FP32
     // on the mixed path, whose S is stored in FP32), added to Hpp in FP64
@@ -492,10 +504,11 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
         for (int c = 0; c < 6; ++c)
           acc[i * 6 + c] += d[i * 3] * b[c * 3] + d[i * 3 + 1] * b[c * 3 + 1] + d[i * 3 + 2] * b[c * 3 + 2];
     };
-    int p = pair_ptr[k];
-    const int p1 = pair_ptr[k + 1];
-    for (; p + 1 < p1; p += 2) {
-      const int2 pa = pairs[p], pb = pairs[p + 1];
+    constexpr int STEP = G / 2;  // this lane's pairs: p0 + sub, p0 + sub + STEP, ...
+    int p = valid ? pair_ptr[k] + sub : 0;
+    const int p1 = valid ? pair_ptr[k + 1] : 0;
+    for (; p + STEP < p1; p += 2 * STEP) {
+      const int2 pa = pairs[p], pb = pairs[p + STEP];
       Real ba[18], bb[18];
       load_b(pa.y, ba);
       load_b(pb.y, bb);
@@ -508,16 +521,22 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       load_b(pa.y, ba);
       accum(pa.x, ba);
     }
-    const int hb = s_hpp[k];
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
+    for (int off = 2; off < G; off <<= 1)
 #pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        const int e = (half * 3 + i) * 6 + c;
-        double v = -(double)acc[i * 6 + c];
-        if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
-        Sr[(size_t)e * nblk + j] = (Real)v;
-      }
+      for (int t = 0; t < 18; ++t) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
+    if (valid && sub == 0) {
+      const int hb = s_hpp[k];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const int e = (half * 3 + i) * 6 + c;
+          double v = -(double)acc[i * 6 + c];
+          if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
+          Sr[(size_t)e * nblk + j] = (Real)v;
+        }
+    }
   }
 }
 

@@ -16,6 +16,7 @@
 
 #include "adjoint_kernels.cuh"
 #include "ba_kernels.cuh"
+#include "batch_kernels.cuh"
 #include "cholesky.cuh"
 #include "g2oc_internal.h"
 #include "io_kernels.cuh"
@@ -69,6 +70,10 @@ struct EngineBase {
   // Gauss-Newton solve H x = rhs (lambda 0) with a given device right-hand
   // side in Hessian order, through the same Schur + PCG / Cholesky path (BA)
   virtual int solve_rhs(const double* rhs, double* out) = 0;
+  // batched windows: per-window lambda initialisation, and the trial's solve
+  // (Schur with per-vertex damping, dense Cholesky per window, back-substitution)
+  virtual int batch_lambda_init(double user_lambda, double tau) = 0;
+  virtual int batch_solve(bool autotune) = 0;
 };
 
 // kernel identifiers for the launch counters and the optional per-launch
@@ -123,6 +128,27 @@ struct g2oc_ctx {
   // FP64 vectors
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
   g2oc::DBuf<double> adj_g, adj_v, adj_r, adj_dv, adj_p, adj_q, adj_rold, adj_dmeas, adj_dlogw;  // adjoint
+  // batched windows (g2oc_upload_windows): packed into one graph
+  bool batch = false;
+  int nw = 0;
+  std::vector<int> win_cam_h, win_lm_h, win_pose_h, win_point_h;  // nw + 1 each
+  g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
+  g2oc::DBuf<long long> win_mat;
+  g2oc::DBuf<double> win_scratch, lam_c, lam_l;
+  g2oc::DBuf<g2oc::WinState> win_state;
+  g2oc::DBuf<int> win_active;
+  g2oc::DBuf<int> win_list[3];       // windows factored with 128 / 256 / 512 threads
+  int win_list_n[3] = {0, 0, 0};
+  int win_threads_of_class[3] = {0, 0, 0};  // autotuned, per size class (n < 96, < 192, >= 192)
+  std::vector<int> win_threads;      // per window, for the statistics
+  int win_nmax = 0;
+  int win_iterations = 0;
+  int win_rounds = 0;
+  bool win_tuned = false;
+  cudaGraphExec_t win_graph = nullptr;
+  g2oc::WinDev windev() const {
+    return g2oc::WinDev{nw, win_cam.p, win_lm.p, win_edge.p, win_pose.p, win_point.p, win_mat.p};
+  }
   g2oc::DBuf<g2oc::DevScalars> sc;
   g2oc::DBuf<g2oc::PcgState> pcg;
   g2oc::DBuf<int> flag;  // nonfinite flag
@@ -204,6 +230,7 @@ struct g2oc_ctx {
     pending.clear();
   }
   ~g2oc_ctx() {
+    if (win_graph) cudaGraphExecDestroy(win_graph);
     eng.reset();
     chol.reset();
     flush_timing();
@@ -449,6 +476,11 @@ struct Engine final : EngineBase {
   DBuf<Real> hpp, hll, hpl, bdc, dinv, Sval, sysval;
   DBuf<double> minv, r, s, d0, d1, q, qrow, tbuf, cpart, tpart;
   DBuf<Real> tiles;  // dense-tile copy of the system (nearly full 6x6-block matrices), allocated on first use
+  // Schur rows by lanes per off-diagonal block (2 / 8 / 16), from the row's
+  // mean pair-list length (<= 12, <= 40, longer): a structural choice, so a
+  // row gets the same arithmetic whatever else is in the graph
+  DBuf<int> row_list[3];
+  int row_n[3] = {0, 0, 0};
   bool tiles_fresh = false;  // tiles hold the matrix of the current solve
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
   size_t schur_smem = 0;
@@ -465,6 +497,19 @@ struct Engine final : EngineBase {
       G2OC_TRY(hpl.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
       G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
       G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
+      {
+        std::vector<int> lists[3];
+        for (int r = 0; r < S.Cf; ++r) {
+          const int k0 = S.sys_rptr[r], k1 = S.sys_rptr[r + 1];
+          const double pairs = (double)(S.s_pair_ptr[k1] - S.s_pair_ptr[k0]);
+          const double mean = k1 - k0 > 1 ? pairs / (k1 - k0 - 1) : 0.0;
+          lists[mean <= 12.0 ? 0 : mean <= 40.0 ? 1 : 2].push_back(r);
+        }
+        for (int gi = 0; gi < 3; ++gi) {
+          row_n[gi] = (int)lists[gi].size();
+          G2OC_TRY(row_list[gi].upload(lists[gi].empty() ? std::vector<int>{0} : lists[gi], c->stream));
+        }
+      }
       schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
       stage_in_smem = schur_smem <= 190 * 1024;
       if (!stage_in_smem) schur_smem = 0;
@@ -564,29 +609,46 @@ struct Engine final : EngineBase {
 
   // S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T (internal row order) and,
   // when bs != nullptr, the reduced right-hand side of b
-  int schur(double lambda, double* bs) {
+  // lam_c / lam_l: per camera row / per landmark damping (batched windows);
+  // nullptr: lambda for all
+  int schur(double lambda, double* bs, const double* lam_c = nullptr, const double* lam_l = nullptr) {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (S.Pf > 0) {
       G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
-          hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, dinv.p, nullptr, c->flag.p);
+          hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, lam_l, dinv.p, nullptr, c->flag.p);
       G2OC_LAUNCH_CHECK();
     }
     if (S.Cf == 0) return G2OC_OK;
-    // FP32 storage: 384 threads, two CTAs per SM; FP64: 512 threads, one
-    constexpr int T = sizeof(Real) == 4 ? 384 : 512;
     const double* bp = c->b.p;
     const double* bl = c->b.p + (size_t)S.Cf * 6;
+    for (int gi = 0; gi < 3; ++gi) {
+      if (row_n[gi] == 0) continue;
+      const int* rows = row_n[gi] == S.Cf ? nullptr : row_list[gi].p;
+      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
+      else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
+      else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
+    }
+    return G2OC_OK;
+  }
+
+  // schur_rows over a list of camera rows with G lanes per off-diagonal block
+  // (FP32 storage: 384 threads, two CTAs per SM; FP64: 512 threads, one)
+  template <int G>
+  int launch_schur_rows(const int* rows, int nrows, double lambda, const double* lam_c, const double* bp,
+                        const double* bl, double* bs) {
+    constexpr int T = sizeof(Real) == 4 ? 384 : 512;
+    cudaStream_t st = c->stream;
     if (stage_in_smem) {
-      auto kern = schur_rows<Real, T, true>;
+      auto kern = schur_rows<Real, T, true, G>;
       G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
-      G2OC_K(K_SCHUR_BLOCKS) kern<<<S.Cf, T, schur_smem, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
+      G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
+          rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, bp, bl, bs);
     } else {
-      G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false><<<S.Cf, T, 0, st>>>(
-          c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, Sval.p, bp, bl, bs);
+      G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false, G><<<nrows, T, 0, st>>>(
+          rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, bp, bl, bs);
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
@@ -670,7 +732,7 @@ struct Engine final : EngineBase {
       if (S.ba && S.Pf > 0) {
         if (S.schur) {
           G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
-              hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, dinv.p, nullptr, c->flag.p);
+              hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, nullptr, dinv.p, nullptr, c->flag.p);
           G2OC_LAUNCH_CHECK();
           G2OC_TRY(backsub(c->b.p, c->xs.p, c->x.p));
         }
@@ -803,6 +865,95 @@ struct Engine final : EngineBase {
       to_double(h, hpl_out);
     }
     return G2OC_OK;
+  }
+
+  int batch_lambda_init(double user_lambda, double tau) override {
+    G2OC_K(K_LM_CONTROL) win_lambda_init<Real, 256><<<c->nw, 256, 0, c->stream>>>(hpp.p, hll.p, c->windev(),
+                                                                                 c->win_state.p, user_lambda, tau);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  // one launch of the dense per-window solve with THREADS threads per window
+  template <int T>
+  int launch_win_chol(const int* list, int nlist) {
+    if (nlist == 0) return G2OC_OK;
+    const size_t smem = ((size_t)c->win_nmax * (kWinPanel + 1) + c->win_nmax) * sizeof(double);
+    if (smem > 48 * 1024)
+      G2OC_CUDA_TRY(cudaFuncSetAttribute(win_chol_solve<Real, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+    G2OC_K(K_CHOLESKY) win_chol_solve<Real, T><<<nlist, T, smem, c->stream>>>(
+        list, nlist, c->windev(), sys(Sval.p), c->rhs.p, c->xs.p, c->win_scratch.p, c->win_state.p);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+  int launch_win_chol_t(int t, const int* list, int nlist) {
+    if (t == 0) return launch_win_chol<128>(list, nlist);
+    if (t == 1) return launch_win_chol<256>(list, nlist);
+    return launch_win_chol<512>(list, nlist);
+  }
+
+  // Times the dense solve with 128 / 256 / 512 threads per window on each
+  // window-size class (n < 96, < 192, >= 192 unknowns) and keeps the fastest;
+  // the windows are then solved in three launches, one per thread count.
+  int batch_autotune() {
+    const Structure& S = c->S;
+    (void)S;
+    cudaStream_t st = c->stream;
+    std::vector<int> cls[3];
+    for (int w = 0; w < c->nw; ++w) {
+      const int n = 6 * (c->win_cam_h[w + 1] - c->win_cam_h[w]);
+      cls[n < 96 ? 0 : n < 192 ? 1 : 2].push_back(w);
+    }
+    DBuf<int> tmp;
+    cudaEvent_t a, b;
+    G2OC_CUDA_TRY(cudaEventCreate(&a));
+    G2OC_CUDA_TRY(cudaEventCreate(&b));
+    std::vector<int> lists[3];
+    c->win_threads.assign(c->nw, 0);
+    for (int k = 0; k < 3; ++k) {
+      if (cls[k].empty()) continue;
+      G2OC_TRY(tmp.upload(cls[k], st));
+      int best = 1;
+      float best_ms = 1e30f;
+      for (int t = 0; t < 3; ++t) {
+        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));  // warm
+        G2OC_CUDA_TRY(cudaEventRecord(a, st));
+        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));
+        G2OC_CUDA_TRY(cudaEventRecord(b, st));
+        G2OC_CUDA_TRY(cudaEventSynchronize(b));
+        float ms = 0.f;
+        G2OC_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = t;
+        }
+      }
+      c->win_threads_of_class[k] = 128 << best;
+      for (int w : cls[k]) {
+        lists[best].push_back(w);
+        c->win_threads[w] = 128 << best;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    for (int t = 0; t < 3; ++t) {
+      c->win_list_n[t] = (int)lists[t].size();
+      G2OC_TRY(c->win_list[t].upload(lists[t].empty() ? std::vector<int>{0} : lists[t], st));
+    }
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+    c->win_tuned = true;
+    return G2OC_OK;
+  }
+
+  int batch_solve(bool autotune) override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    G2OC_TRY(schur(0.0, c->rhs.p, c->lam_c.p, c->lam_l.p));
+    if (autotune && !c->win_tuned) G2OC_TRY(batch_autotune());
+    for (int t = 0; t < 3; ++t) G2OC_TRY(launch_win_chol_t(t, c->win_list[t].p, c->win_list_n[t]));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return backsub(c->b.p + (size_t)S.Cf * 6, c->xs.p, c->x.p + (size_t)S.Cf * 6);
   }
 
   int solve_rhs(const double* rhs, double* out) override {
@@ -1187,6 +1338,10 @@ int g2oc_set_params(g2oc_ctx* c, const g2oc_params* p) {
   }
   const bool prec_changed = p->precision != c->prm.precision;
   c->prm = *p;
+  if (c->win_graph) {  // the captured window round holds the old parameters
+    cudaGraphExecDestroy(c->win_graph);
+    c->win_graph = nullptr;
+  }
   if (c->uploaded && prec_changed) G2OC_TRY(make_engine(c));
   return G2OC_OK;
 }
@@ -1419,9 +1574,20 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
   return G2OC_OK;
 }
 
+static void drop_windows(g2oc_ctx* c) {
+  c->batch = false;
+  c->nw = 0;
+  c->win_tuned = false;
+  if (c->win_graph) {
+    cudaGraphExecDestroy(c->win_graph);
+    c->win_graph = nullptr;
+  }
+}
+
 int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(check_ctx(c, false));
   c->chi2_carry = false;
+  drop_windows(c);
   if (!g) {
     set_error("graph is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
@@ -1795,6 +1961,297 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
     set_error("adjoint solve stopped at relative residual %.3e after %d steps", rel, steps);
     return G2OC_ERR_NOT_CONVERGED;
   }
+  return G2OC_OK;
+}
+
+// ------------------------------------------------------- batched windows
+int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
+  G2OC_TRY(check_ctx(c, false));
+  if (num_windows <= 0 || !w) {
+    set_error("num_windows must be positive and windows non-NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < num_windows; ++i) {
+    const g2oc_graph& g = w[i];
+    if (g.pose_type != G2OC_POSE_SE3EXPMAP || g.edge_type != G2OC_EDGE_PROJECT_XYZ2UV) {
+      set_error("window %d: batched windows are bundle adjustments (VertexSE3Expmap, EdgeProjectXYZ2UV)", i);
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    if (g.focal_length != w[0].focal_length || g.principal_point[0] != w[0].principal_point[0] ||
+        g.principal_point[1] != w[0].principal_point[1]) {
+      set_error("window %d: every window must use the same camera parameters", i);
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    if (!g.pose_estimate || !g.edge_vertex || !g.measurement || !g.information ||
+        (g.num_points > 0 && !g.point_estimate)) {
+      set_error("window %d: graph array is NULL", i);
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+  }
+  // pack: vertices and edges window after window, vertex indices offset
+  std::vector<int> pose_off(num_windows + 1, 0), point_off(num_windows + 1, 0), edge_off(num_windows + 1, 0);
+  for (int i = 0; i < num_windows; ++i) {
+    pose_off[i + 1] = pose_off[i] + w[i].num_poses;
+    point_off[i + 1] = point_off[i] + w[i].num_points;
+    edge_off[i + 1] = edge_off[i] + w[i].num_edges;
+  }
+  const int C = pose_off[num_windows], P = point_off[num_windows], E = edge_off[num_windows];
+  std::vector<double> pose((size_t)C * 7), point((size_t)P * 3), meas((size_t)E * 2), info((size_t)E * 4), delta(E);
+  std::vector<uint8_t> pf(C, 0), qf(P, 0);
+  std::vector<int32_t> ev((size_t)E * 2);
+  bool robust = false;
+  for (int i = 0; i < num_windows; ++i) {
+    const g2oc_graph& g = w[i];
+    memcpy(pose.data() + (size_t)pose_off[i] * 7, g.pose_estimate, (size_t)g.num_poses * 7 * sizeof(double));
+    if (g.num_points)
+      memcpy(point.data() + (size_t)point_off[i] * 3, g.point_estimate, (size_t)g.num_points * 3 * sizeof(double));
+    if (g.pose_fixed) memcpy(pf.data() + pose_off[i], g.pose_fixed, g.num_poses);
+    if (g.point_fixed) memcpy(qf.data() + point_off[i], g.point_fixed, g.num_points);
+    memcpy(meas.data() + (size_t)edge_off[i] * 2, g.measurement, (size_t)g.num_edges * 2 * sizeof(double));
+    memcpy(info.data() + (size_t)edge_off[i] * 4, g.information, (size_t)g.num_edges * 4 * sizeof(double));
+    for (int e = 0; e < g.num_edges; ++e) {
+      const int v0 = g.edge_vertex[2 * e], v1 = g.edge_vertex[2 * e + 1];
+      if (v0 < 0 || v0 >= g.num_points || v1 < 0 || v1 >= g.num_poses) {
+        set_error("window %d edge %d: vertex index out of range", i, e);
+        return G2OC_ERR_BAD_GRAPH;
+      }
+      ev[2 * ((size_t)edge_off[i] + e)] = v0 + point_off[i];
+      ev[2 * ((size_t)edge_off[i] + e) + 1] = v1 + pose_off[i];
+      delta[edge_off[i] + e] = g.robust_delta ? g.robust_delta[e] : 0.0;
+    }
+    robust |= g.robust_delta != nullptr;
+  }
+  g2oc_graph packed;
+  memset(&packed, 0, sizeof(packed));
+  packed.pose_type = G2OC_POSE_SE3EXPMAP;
+  packed.num_poses = C;
+  packed.pose_estimate = pose.data();
+  packed.pose_fixed = pf.data();
+  packed.num_points = P;
+  packed.point_estimate = point.data();
+  packed.point_fixed = qf.data();
+  packed.edge_type = G2OC_EDGE_PROJECT_XYZ2UV;
+  packed.num_edges = E;
+  packed.edge_vertex = ev.data();
+  packed.measurement = meas.data();
+  packed.information = info.data();
+  packed.robust_delta = robust ? delta.data() : nullptr;
+  packed.focal_length = w[0].focal_length;
+  packed.principal_point[0] = w[0].principal_point[0];
+  packed.principal_point[1] = w[0].principal_point[1];
+  G2OC_TRY(g2oc_upload(c, &packed));
+  const Structure& S = c->S;
+  if (!S.ba || !S.schur) {
+    set_error("batched windows need free landmarks (Schur complement)");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  // window ranges: free cameras and landmarks are numbered in vertex order, so
+  // each window's are contiguous
+  const int nw = num_windows;
+  std::vector<int> wc(nw + 1, 0), wl(nw + 1, 0), we(nw + 1, 0), ofc(std::max(S.Cf, 1)), ofl(std::max(S.Pf, 1)),
+      ofp(std::max(C, 1)), ofq(std::max(P, 1));
+  for (int i = 0; i < nw; ++i) {
+    int nc = 0, nl = 0;
+    for (int v = pose_off[i]; v < pose_off[i + 1]; ++v) {
+      ofp[v] = i;
+      if (S.pose_h[v] >= 0) ofc[S.pose_h[v]] = i, ++nc;
+    }
+    for (int v = point_off[i]; v < point_off[i + 1]; ++v) {
+      ofq[v] = i;
+      if (S.point_l[v] >= 0) ofl[S.point_l[v]] = i, ++nl;
+    }
+    wc[i + 1] = wc[i] + nc;
+    wl[i + 1] = wl[i] + nl;
+  }
+  // device edges of a window must be contiguous (they are, unless a window has
+  // fixed points, whose edges the device order puts after all free landmarks)
+  const int na = (int)S.act.size();
+  std::vector<int> win_of_edge(E);
+  for (int i = 0; i < nw; ++i)
+    for (int e = edge_off[i]; e < edge_off[i + 1]; ++e) win_of_edge[e] = i;
+  int prev = 0;
+  for (int k = 0; k < na; ++k) {
+    const int wi = win_of_edge[S.dev_edge[k]];
+    if (wi < prev) {
+      set_error("batched windows with fixed points are not supported");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    for (int j = prev + 1; j <= wi; ++j) we[j] = k;
+    prev = wi;
+  }
+  for (int j = prev + 1; j <= nw; ++j) we[j] = na;
+  std::vector<long long> mat(nw);
+  long long off = 0;
+  int nmax = 0;
+  for (int i = 0; i < nw; ++i) {
+    const int n = 6 * (wc[i + 1] - wc[i]);
+    mat[i] = off;
+    off += (long long)n * n;
+    nmax = std::max(nmax, n);
+  }
+  cudaStream_t st = c->stream;
+  c->nw = nw;
+  c->win_cam_h = wc;
+  c->win_lm_h = wl;
+  c->win_pose_h = pose_off;
+  c->win_point_h = point_off;
+  c->win_nmax = nmax;
+  G2OC_TRY(c->win_cam.upload(wc, st));
+  G2OC_TRY(c->win_lm.upload(wl, st));
+  G2OC_TRY(c->win_edge.upload(we, st));
+  G2OC_TRY(c->win_pose.upload(pose_off, st));
+  G2OC_TRY(c->win_point.upload(point_off, st));
+  G2OC_TRY(c->win_of_cam.upload(ofc, st));
+  G2OC_TRY(c->win_of_lm.upload(ofl, st));
+  G2OC_TRY(c->win_of_pose.upload(ofp, st));
+  G2OC_TRY(c->win_of_point.upload(ofq, st));
+  G2OC_TRY(c->win_mat.upload(mat, st));
+  G2OC_TRY(c->win_scratch.alloc((size_t)std::max(off, 1LL)));
+  G2OC_TRY(c->lam_c.alloc(std::max(S.Cf, 1)));
+  G2OC_TRY(c->lam_l.alloc(std::max(S.Pf, 1)));
+  G2OC_TRY(c->win_state.alloc(nw));
+  G2OC_TRY(c->win_active.alloc(1));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  c->batch = true;
+  return G2OC_OK;
+}
+
+// one LM round of every unfinished window (only stream-ordered work: this is
+// what the CUDA graph captures)
+static int window_round(g2oc_ctx* c, bool autotune) {
+  const Structure& S = c->S;
+  cudaStream_t st = c->stream;
+  const WinDev W = c->windev();
+  const int n = c->vec_size();
+  G2OC_CUDA_TRY(cudaMemsetAsync(c->win_active.p, 0, sizeof(int), st));
+  G2OC_K(K_CHI2) win_chi2<256><<<c->nw, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 0);
+  G2OC_LAUNCH_CHECK();
+  G2OC_TRY(c->eng->build_system());
+  G2OC_TRY(c->eng->batch_lambda_init(c->prm.initial_lambda, c->prm.tau));
+  G2OC_K(K_LM_CONTROL) win_spread_lambda<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(
+      c->win_of_cam.p, S.Cf, c->win_of_lm.p, S.Pf, c->win_state.p, c->lam_c.p, c->lam_l.p);
+  G2OC_LAUNCH_CHECK();
+  G2OC_TRY(push(c));
+  G2OC_TRY(c->eng->batch_solve(autotune));
+  G2OC_K(K_LM_CONTROL) win_mask_step<<<cdiv(n, 256), 256, 0, st>>>(c->win_of_cam.p, S.Cf, c->win_of_lm.p, S.Pf,
+                                                                    c->win_state.p, c->x.p);
+  G2OC_LAUNCH_CHECK();
+  G2OC_TRY(oplus(c));
+  G2OC_K(K_CHI2) win_chi2<256><<<c->nw, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 1);
+  G2OC_K(K_LM_CONTROL) win_scale<256><<<c->nw, 256, 0, st>>>(c->x.p, c->b.p, S.Cf, W, c->win_state.p);
+  G2OC_K(K_LM_CONTROL) win_decide<<<cdiv(c->nw, 128), 128, 0, st>>>(c->win_state.p, c->nw,
+                                                                    c->prm.max_trials_after_failure, c->win_iterations,
+                                                                    c->win_active.p);
+  G2OC_K(K_LM_CONTROL) win_pop<<<cdiv((long long)S.C * 8 + (long long)S.P * 4, 256), 256, 0, st>>>(
+      c->win_of_pose.p, S.C, c->win_of_point.p, S.P, c->win_state.p, c->pose_bak.p, c->pose.p, c->point_bak.p,
+      c->point.p);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
+int g2oc_optimize_windows(g2oc_ctx* c, int32_t iterations, g2oc_window_stats* stats) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->batch) {
+    set_error("no windows uploaded (g2oc_upload_windows)");
+    return G2OC_ERR_STATE;
+  }
+  if (iterations < 0) {
+    set_error("iterations < 0");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  cudaStream_t st = c->stream;
+  // window states: windows without edges are finished from the start
+  std::vector<WinState> ws0(c->nw);
+  memset(ws0.data(), 0, ws0.size() * sizeof(WinState));
+  std::vector<int> we(c->nw + 1);
+  G2OC_CUDA_TRY(cudaMemcpy(we.data(), c->win_edge.p, we.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < c->nw; ++i) {
+    ws0[i].solve_ok = 1;
+    ws0[i].result = G2OC_RESULT_OK;
+    if (we[i + 1] == we[i] || iterations == 0) ws0[i].done = 1;
+  }
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->win_state.p, ws0.data(), ws0.size() * sizeof(WinState), cudaMemcpyHostToDevice,
+                                st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  const bool timing = c->timing;
+  if (iterations != c->win_iterations && c->win_graph) {
+    cudaGraphExecDestroy(c->win_graph);
+    c->win_graph = nullptr;
+  }
+  c->win_iterations = iterations;
+  const int max_rounds = iterations * std::max(c->prm.max_trials_after_failure, 1);
+  int rounds = 0, active = 1;
+  // first round eagerly (it also tunes the dense solve), then a captured round
+  if (max_rounds > 0) {
+    G2OC_TRY(window_round(c, true));
+    ++rounds;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&active, c->win_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  if (active > 0 && rounds < max_rounds && !c->win_graph) {
+    c->timing = false;  // no per-launch events inside the graph
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    int rs = e == cudaSuccess ? window_round(c, false) : G2OC_ERR_CUDA;
+    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    c->timing = timing;
+    if (e != cudaSuccess || rs != G2OC_OK || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      set_error("capturing the window round failed");
+      return G2OC_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&c->win_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      c->win_graph = nullptr;
+      set_error("instantiating the window round failed: %s", cudaGetErrorString(e));
+      return G2OC_ERR_CUDA;
+    }
+  }
+  // replay the round, checking the count of unfinished windows every few rounds
+  while (active > 0 && rounds < max_rounds) {
+    const int k = std::min(4, max_rounds - rounds);
+    for (int i = 0; i < k; ++i) G2OC_CUDA_TRY(cudaGraphLaunch(c->win_graph, st));
+    rounds += k;
+    G2OC_CUDA_TRY(cudaMemcpyAsync(&active, c->win_active.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  c->system_built = false;
+  c->chi2_carry = false;
+  c->win_rounds = rounds;
+  if (stats) {
+    std::vector<WinState> ws(c->nw);
+    G2OC_CUDA_TRY(cudaMemcpy(ws.data(), c->win_state.p, ws.size() * sizeof(WinState), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c->nw; ++i) {
+      g2oc_window_stats& o = stats[i];
+      o.iterations = ws[i].iteration;
+      o.trials = ws[i].trials;
+      o.result = ws[i].result;
+      o.solve_ok = ws[i].solve_ok;
+      o.cholesky_threads = c->win_threads.empty() ? 0 : c->win_threads[i];
+      o.rounds = rounds;
+      o.chi2_initial = ws[i].chi2_init;
+      o.chi2 = ws[i].chi2_cur;
+      o.lambda = ws[i].lambda;
+    }
+  }
+  return G2OC_OK;
+}
+
+int g2oc_download_window(g2oc_ctx* c, int32_t window, double* pose, double* point) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->batch || window < 0 || window >= c->nw) {
+    set_error("no such window");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const Structure& S = c->S;
+  std::vector<double> ps((size_t)S.C * 7), pt((size_t)std::max(S.P, 1) * 3);
+  G2OC_TRY(g2oc_download(c, ps.data(), pt.data()));
+  const int p0 = c->win_pose_h[window], p1 = c->win_pose_h[window + 1];
+  const int q0 = c->win_point_h[window], q1 = c->win_point_h[window + 1];
+  if (pose) memcpy(pose, ps.data() + (size_t)p0 * 7, (size_t)(p1 - p0) * 7 * sizeof(double));
+  if (point && q1 > q0) memcpy(point, pt.data() + (size_t)q0 * 3, (size_t)(q1 - q0) * 3 * sizeof(double));
   return G2OC_OK;
 }
 

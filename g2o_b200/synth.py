@@ -292,6 +292,21 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     return g
 
 
+def windows(num_windows=512, cameras=(10, 60), points=(500, 8000), obs=(2, 8), seed=SEED_BASE + 1000):
+    """Local bundle-adjustment windows of uneven size: cameras and points
+    log-uniform in the given ranges, each point seen by obs[0]..obs[1] cameras
+    of its window; the BA generator (ring cameras, box points, 1 px noise, 1%
+    outliers, Huber) seeded per window."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for w in range(num_windows):
+        nc = int(round(math.exp(rng.uniform(math.log(cameras[0]), math.log(cameras[1])))))
+        npt = int(round(math.exp(rng.uniform(math.log(points[0]), math.log(points[1])))))
+        out.append(bundle_adjustment(num_cameras=nc, num_points=npt, min_obs=obs[0], max_obs=obs[1],
+                                     seed=seed + 1 + w))
+    return out
+
+
 def adjoint_problem(num_cameras=200, num_points=40_000, seed=SEED_BASE + 4, robust=False):
     """The adjoint instance: the BA generator without outliers (and, unless
     asked, without a robust kernel), 200 cameras / 40k points by default."""

@@ -255,6 +255,36 @@ int g2oc_get_kernel_stats(g2oc_ctx* ctx, g2oc_kernel_stat* out, int capacity, in
 int g2oc_backward(g2oc_ctx* ctx, const double* dL_dx, double* dL_dmeas, double* dL_dlogw,
                   g2oc_backward_stats* stats);
 
+/* Batched windows (no counterpart in the reference, where each window would be
+   its own SparseOptimizer): many independent bundle adjustments
+   (VertexSE3Expmap + VertexPointXYZ + EdgeProjectXYZ2UV, same camera
+   parameters, no fixed points) packed into one context and optimized together.
+   Every window runs OptimizationAlgorithmLevenberg::solve on its own (own
+   lambda, trials, Terminate rules; g2o/core/optimization_algorithm_levenberg.cpp:60-153)
+   with its reduced camera system solved by a dense Cholesky
+   (LinearSolverDense, g2o/solvers/dense/linear_solver_dense.h:57-105), while
+   each kernel runs over all windows; one LM round is captured in a CUDA graph
+   and replayed until every window has finished. The Hessian and Schur
+   complement are formed in the context's precision; the Cholesky is FP64.
+   g2oc_upload_windows replaces the context's graph; g2oc_optimize_windows
+   writes one g2oc_window_stats per window; g2oc_download_window reads one
+   window's estimates (its own vertex numbering). */
+typedef struct g2oc_window_stats {
+  int32_t iterations;        /* LM iterations completed */
+  int32_t trials;            /* LM trials in all */
+  int32_t result;            /* G2OC_RESULT_* of the last iteration */
+  int32_t solve_ok;          /* the last dense factorization succeeded */
+  int32_t cholesky_threads;  /* threads per window of the dense solve (autotuned) */
+  int32_t rounds;            /* rounds the batch ran */
+  double chi2_initial;       /* robust chi2 before the first iteration */
+  double chi2;               /* robust chi2 at the end */
+  double lambda;
+} g2oc_window_stats;
+
+int g2oc_upload_windows(g2oc_ctx* ctx, int32_t num_windows, const g2oc_graph* windows);
+int g2oc_optimize_windows(g2oc_ctx* ctx, int32_t iterations, g2oc_window_stats* stats);
+int g2oc_download_window(g2oc_ctx* ctx, int32_t window, double* pose, double* point);
+
 /* LinearSolver::solve on a caller block matrix: symmetric, upper blocks given
    column-major as (row, col) block pairs with row-major dense values; block
    sizes from block_offsets (num_blocks + 1 entries, scalar offsets). x gets
