@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-iterations", type=int, default=1)
+    ap.add_argument("--config", default="ba", choices=["ba", "windows"],
+                    help="ba: the 1000-camera bundle adjustment (default); windows: 512 batched local BA windows")
     return ap.parse_args()
 
 
@@ -219,6 +221,127 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+WIN_ITERS = 10
+
+
+def run_windows(args):
+    """512 local BA windows (log-uniform 10-60 cameras, 500-8000 points),
+    10 LM iterations each, mixed precision (lm_cuda_mixed_fast), batched in one
+    context per GPU. Multi-GPU: windows assigned to ranks by estimated cost
+    (g2o_b200/shard.py), no communication; value = all ranks' window LM
+    iterations / the slowest rank's device time."""
+    rank, world, local = dist_info()
+    import torch
+    from g2o_b200 import backend, shard, synth
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    sizes = synth.window_sizes()
+    costs = [shard.window_cost(c, p) for c, p in sizes]
+    mine = shard.assign_windows(costs, world)[rank]
+    ws = synth.windows(which=mine)
+    edges = sum(w.num_edges for w in ws)
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    prm = fac.construct("lm_cuda_mixed_fast")
+    t0 = time.perf_counter()
+    cw = backend.CudaWindows(ws, prm, device=local)
+    upload_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(cw.stream(), device=local)
+    for _ in range(max(args.warmup, 1)):
+        cw.restore_initial_estimates()
+        cw.optimize(WIN_ITERS)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters = trials = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        cw.restore_initial_estimates()
+        st = cw.optimize(WIN_ITERS)
+        iters += sum(x["iterations"] for x in st)
+        trials += sum(x["trials"] for x in st)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    threads = sorted({x["cholesky_threads"] for x in st})
+    rounds = st[0]["rounds"] if st else 0
+    tot = [ms, float(iters), float(edges)]
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        u = torch.tensor([float(iters), float(edges)], device=f"cuda:{local}")
+        torch.distributed.all_reduce(u, op=torch.distributed.ReduceOp.SUM)
+        tot = [float(t.item()), float(u[0].item()), float(u[1].item())]
+    ms, iters_all, edges_all = tot
+    value = iters_all / (ms * 1e-3)
+    # end to end through the C-ABI with host buffers, every step: upload of the
+    # windows' values (same topology: structure, tuned solve and captured round
+    # kept), optimize, download of every window's estimates
+    h2d = sum(a.nbytes for w in ws for a in (w.pose_estimate, w.point_estimate, w.edge_vertex, w.measurement,
+                                              w.information, w.robust_delta) if a is not None)
+    d2h = 0
+    e2e_iters = 0
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cw.upload(ws)
+        st2 = cw.optimize(WIN_ITERS)
+        est = cw.estimates_all()
+        e2e_iters += sum(x["iterations"] for x in st2)
+        d2h = sum(p.nbytes + q.nbytes for p, q in est)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    tot = [e2e_s, float(e2e_iters)]
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        u = torch.tensor([float(e2e_iters)], device=f"cuda:{local}")
+        torch.distributed.all_reduce(u, op=torch.distributed.ReduceOp.SUM)
+        tot = [float(t.item()), float(u[0].item())]
+    e2e_value = tot[1] / tot[0]
+    cpu = None
+    if rank == 0 and world == 1:
+        from oracle import oracle
+        sample = [0, 1, 2, 3]
+        t0 = time.perf_counter()
+        its = 0
+        for w in sample:
+            o = oracle.OracleProblem(ws[mine.index(w)] if w in mine else synth.windows(which=[w])[0],
+                                     oracle.default_params(linear_solver=1))
+            _, so = o.optimize(WIN_ITERS)
+            its += len(so)
+        dt = time.perf_counter() - t0
+        cpu = {"value": its / dt, "unit": "window iter/s", "cores": 1, "kind": "port",
+               "sample": f"windows {sample}, 10 LM iterations each (FP64 restatement, Cholesky), {dt:.2f} s"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": "batched local BA: window LM iterations/s (512 windows, 10 LM iterations each)",
+        "value": value, "unit": "window iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32/f64 (FP32 Hessian/Schur storage; FP64 Cholesky, vectors, chi2, LM)",
+        "data": "synthetic (seeded per window: BA generator, log-uniform sizes)",
+        "config": {"workload": "batched_ba_512_windows_10-60cam_500-8000pt_lm10", "windows": 512,
+                   "edges": int(edges_all), "parallelism": f"windows by cost over {world} rank(s)",
+                   "rounds": rounds, "cholesky_threads": threads, "trials_per_window": trials / max(len(ws), 1) /
+                   args.steps, "upload_s": upload_s},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": "window iter/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "upload": "same topology each step: values copied, structure kept",
+                "new_topology_upload_s": upload_s},
+        "cpu_baseline": cpu,
+    }), flush=True)
 
 
 def run_ours(args):
@@ -424,5 +547,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "windows":
+        run_windows(a)
     else:
         run_ours(a)

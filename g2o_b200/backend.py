@@ -314,6 +314,13 @@ class CudaWindows:
         _check(library().g2oc_create(device, C.byref(self._h)))
         self.params = params or default_params()
         _check(library().g2oc_set_params(self._h, C.byref(self.params)))
+        self.upload(self.windows)
+
+    def upload(self, windows):
+        """(Re-)upload the windows. The same windows with new values (same
+        topology) keep the structure, the tuned dense solve and the captured
+        LM round."""
+        self.windows = list(windows)
         self._cg = [w.to_c() for w in self.windows]
         arr = (G2ocGraph * len(self._cg))(*self._cg)
         self._arr = arr
@@ -353,6 +360,20 @@ class CudaWindows:
         point = np.empty((max(g.num_points, 1), 3))
         _check(library().g2oc_download_window(self._h, w, _p(pose), _p(point)))
         return pose, point[: g.num_points]
+
+    def estimates_all(self):
+        """Every window's (pose, point) estimates from one download."""
+        C = sum(g.num_poses for g in self.windows)
+        P = sum(g.num_points for g in self.windows)
+        pose = np.empty((C, 7))
+        point = np.empty((max(P, 1), 3))
+        _check(library().g2oc_download(self._h, _p(pose), _p(point)))
+        out, c0, p0 = [], 0, 0
+        for g in self.windows:
+            out.append((pose[c0:c0 + g.num_poses], point[p0:p0 + g.num_points]))
+            c0 += g.num_poses
+            p0 += g.num_points
+        return out
 
     def set_kernel_timing(self, enable: bool):
         _check(library().g2oc_set_kernel_timing(self._h, 1 if enable else 0))

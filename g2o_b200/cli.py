@@ -2,9 +2,11 @@
 (g2o/apps/g2o_cli/g2o.cpp:133-187) for the synthetic configurations:
 
     python -m g2o_b200.cli --config ba --solver lm_cuda_pcg6_3 -i 20 [-stats]
+    python -m g2o_b200.cli --config windows --windows 64 --solver lm_cuda_mixed_fast -i 10
 
 Prints one line per iteration with chi2, lambda, trial and PCG counts and the
-phase times (the fields of G2OBatchStatistics).
+phase times (the fields of G2OBatchStatistics); for the batched windows, one
+line per window with its iterations, trials and chi2.
 """
 import argparse
 import sys
@@ -16,7 +18,26 @@ CONFIGS = {
     "ba_small": lambda: synth.bundle_adjustment(num_cameras=100, num_points=20000, seed=99),
     "pg2d": lambda: synth.pose_graph_2d(),
     "pg3d": lambda: synth.pose_graph_3d(),
+    "windows": None,  # batched local BA windows (synth.windows), see run_windows
 }
+
+
+def run_windows(a, params):
+    ws = synth.windows(which=list(range(min(max(a.windows, 1), 512))))
+    cw = backend.CudaWindows(ws, params, device=a.device)
+    cw.set_kernel_timing(a.stats)
+    st = cw.optimize(a.iterations)
+    print(f"# {len(ws)} windows, {sum(w.num_edges for w in ws)} edges; {st[0]['rounds']} LM rounds")
+    for w, s in enumerate(st):
+        print(f"window= {w}\t iterations= {s['iterations']}\t trials= {s['trials']}\t chi2_initial= "
+              f"{s['chi2_initial']:.6f}\t chi2= {s['chi2']:.6f}\t choleskyThreads= {s['cholesky_threads']}")
+    if a.stats:
+        total, ks = cw.kernel_stats()
+        print(f"# kernel launches: {total}")
+        for k, (n, ms) in sorted(ks.items(), key=lambda kv: -kv[1][1]):
+            print(f"#   {k:20s} {n:7d} {ms:10.3f} ms")
+    cw.close()
+    return 0
 
 
 def main(argv=None):
@@ -27,6 +48,7 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("-stats", "--stats", action="store_true", help="print per-kernel launch counts and times")
     ap.add_argument("--listSolvers", action="store_true")
+    ap.add_argument("--windows", type=int, default=512, help="windows: how many of the 512 local BA windows")
     a = ap.parse_args(argv)
     fac = backend.OptimizationAlgorithmFactory.instance()
     if a.listSolvers:
@@ -36,6 +58,8 @@ def main(argv=None):
     if params is None:
         print(f"unknown solver {a.solver}", file=sys.stderr)
         return 1
+    if a.config == "windows":
+        return run_windows(a, params)
     g = CONFIGS[a.config]()
     prob = backend.CudaProblem(g, params, device=a.device)
     prob.set_kernel_timing(a.stats)

@@ -104,6 +104,7 @@ struct g2oc_ctx {
   g2oc_params prm{};
   g2oc::Structure S;
   bool uploaded = false;
+  bool last_upload_reused = false;  // the last g2oc_upload kept the structure (same topology)
   bool system_built = false;
   double f = 1, cx = 0, cy = 0;
   // vertex state
@@ -132,6 +133,10 @@ struct g2oc_ctx {
   bool batch = false;
   int nw = 0;
   std::vector<int> win_cam_h, win_lm_h, win_pose_h, win_point_h;  // nw + 1 each
+  // host packing buffers, kept so that a re-upload does not fault in fresh pages
+  std::vector<double> pk_pose, pk_point, pk_meas, pk_info, pk_delta;
+  std::vector<uint8_t> pk_pf, pk_qf;
+  std::vector<int32_t> pk_ev;
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
   g2oc::DBuf<long long> win_mat;
   g2oc::DBuf<double> win_scratch, lam_c, lam_l;
@@ -1594,6 +1599,7 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   }
   const bool reuse = c->eng && same_topology(c->topo, g);
   c->uploaded = false;
+  c->last_upload_reused = false;
   if (reuse) {
     // the null checks build_structure makes for a new topology
     if (!g->pose_estimate || !g->measurement || !g->information || (c->S.ba && g->num_points > 0 && !g->point_estimate)) {
@@ -1606,6 +1612,7 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(upload_data(c, g));
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
+  c->last_upload_reused = reuse;
   return G2OC_OK;
 }
 
@@ -1996,9 +2003,18 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
     edge_off[i + 1] = edge_off[i] + w[i].num_edges;
   }
   const int C = pose_off[num_windows], P = point_off[num_windows], E = edge_off[num_windows];
-  std::vector<double> pose((size_t)C * 7), point((size_t)P * 3), meas((size_t)E * 2), info((size_t)E * 4), delta(E);
-  std::vector<uint8_t> pf(C, 0), qf(P, 0);
-  std::vector<int32_t> ev((size_t)E * 2);
+  std::vector<double>&pose = c->pk_pose, &point = c->pk_point, &meas = c->pk_meas, &info = c->pk_info,
+                     &delta = c->pk_delta;
+  std::vector<uint8_t>&pf = c->pk_pf, &qf = c->pk_qf;
+  std::vector<int32_t>& ev = c->pk_ev;
+  pose.resize((size_t)C * 7);
+  point.resize((size_t)P * 3);
+  meas.resize((size_t)E * 2);
+  info.resize((size_t)E * 4);
+  delta.resize(E);
+  pf.assign(C, 0);
+  qf.assign(P, 0);
+  ev.resize((size_t)E * 2);
   bool robust = false;
   for (int i = 0; i < num_windows; ++i) {
     const g2oc_graph& g = w[i];
@@ -2039,7 +2055,23 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   packed.focal_length = w[0].focal_length;
   packed.principal_point[0] = w[0].principal_point[0];
   packed.principal_point[1] = w[0].principal_point[1];
+  // a re-upload of the same windows (same topology, same window ranges) keeps
+  // the tuned dense-solve schedule and the captured LM round: every device
+  // buffer they use keeps its size and address
+  struct Kept {
+    cudaGraphExec_t graph = nullptr;
+    ~Kept() {
+      if (graph) cudaGraphExecDestroy(graph);
+    }
+  } kept;
+  kept.graph = c->win_graph;
+  c->win_graph = nullptr;
+  const bool was_batch = c->batch, was_tuned = c->win_tuned;
+  const int old_nw = c->nw;
+  const std::vector<int> old_pose = c->win_pose_h, old_point = c->win_point_h;
   G2OC_TRY(g2oc_upload(c, &packed));
+  const bool same_windows = was_batch && c->last_upload_reused && old_nw == num_windows && old_pose == pose_off &&
+                            old_point == point_off;
   const Structure& S = c->S;
   if (!S.ba || !S.schur) {
     set_error("batched windows need free landmarks (Schur complement)");
@@ -2113,6 +2145,11 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   G2OC_TRY(c->win_active.alloc(1));
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));
   c->batch = true;
+  if (same_windows) {
+    c->win_tuned = was_tuned;
+    c->win_graph = kept.graph;
+    kept.graph = nullptr;
+  }
   return G2OC_OK;
 }
 

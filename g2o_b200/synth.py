@@ -292,19 +292,27 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     return g
 
 
-def windows(num_windows=512, cameras=(10, 60), points=(500, 8000), obs=(2, 8), seed=SEED_BASE + 1000):
+def window_sizes(num_windows=512, cameras=(10, 60), points=(500, 8000), seed=SEED_BASE + 1000):
+    """(cameras, points) of each window: log-uniform in the given ranges."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(num_windows):
+        nc = int(round(math.exp(rng.uniform(math.log(cameras[0]), math.log(cameras[1])))))
+        npt = int(round(math.exp(rng.uniform(math.log(points[0]), math.log(points[1])))))
+        out.append((nc, npt))
+    return out
+
+
+def windows(num_windows=512, cameras=(10, 60), points=(500, 8000), obs=(2, 8), seed=SEED_BASE + 1000, which=None):
     """Local bundle-adjustment windows of uneven size: cameras and points
     log-uniform in the given ranges, each point seen by obs[0]..obs[1] cameras
     of its window; the BA generator (ring cameras, box points, 1 px noise, 1%
-    outliers, Huber) seeded per window."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for w in range(num_windows):
-        nc = int(round(math.exp(rng.uniform(math.log(cameras[0]), math.log(cameras[1])))))
-        npt = int(round(math.exp(rng.uniform(math.log(points[0]), math.log(points[1])))))
-        out.append(bundle_adjustment(num_cameras=nc, num_points=npt, min_obs=obs[0], max_obs=obs[1],
-                                     seed=seed + 1 + w))
-    return out
+    outliers, Huber) seeded per window. `which`: the indices to generate
+    (default all); window w is the same whichever others are generated."""
+    sizes = window_sizes(num_windows, cameras, points, seed)
+    idx = range(num_windows) if which is None else which
+    return [bundle_adjustment(num_cameras=sizes[w][0], num_points=sizes[w][1], min_obs=obs[0], max_obs=obs[1],
+                              seed=seed + 1 + w) for w in idx]
 
 
 def adjoint_problem(num_cameras=200, num_points=40_000, seed=SEED_BASE + 4, robust=False):

@@ -85,3 +85,31 @@ def test_windows_rerun_and_iteration_limits(backend, small_windows):
     assert all(s["iterations"] == 0 for s in z)
     p, q = cw.estimates(2)
     assert np.array_equal(p, small_windows[2].pose_estimate)
+
+
+def test_windows_reupload_keeps_round_and_matches_fresh_context(backend, small_windows):
+    """Re-uploading the same windows with new values keeps the captured round
+    and the tuned dense solve; the result equals a fresh context's, bit for
+    bit. New windows (other topology) rebuild everything."""
+    ws = small_windows[:8]
+    cw = backend.CudaWindows(ws)
+    cw.optimize(ITER)
+    moved = []
+    for g in ws:
+        g2 = g.copy()
+        g2.measurement = g2.measurement + 0.25
+        moved.append(g2)
+    cw.upload(moved)
+    a = cw.optimize(ITER)
+    fresh = backend.CudaWindows(moved)
+    b = fresh.optimize(ITER)
+    assert [s["chi2"] for s in a] == [s["chi2"] for s in b]
+    assert [s["trials"] for s in a] == [s["trials"] for s in b]
+    for w in (0, 5):
+        for x, y in zip(cw.estimates(w), fresh.estimates(w)):
+            assert np.array_equal(x, y)
+    other = small_windows[8:12]
+    cw.upload(other)
+    c = cw.optimize(ITER)
+    d = backend.CudaWindows(other).optimize(ITER)
+    assert [s["chi2"] for s in c] == [s["chi2"] for s in d]
