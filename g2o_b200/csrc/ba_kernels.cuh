@@ -11,6 +11,7 @@
 #pragma once
 
 #include "g2o_math.cuh"
+#include "g2oc_internal.h"
 #include "reduce.cuh"
 
 namespace g2oc {
@@ -379,12 +380,16 @@ struct Vec2<float> {
 // halves and the G / 2 pairs of a group split its pair list (partial sums
 // combined by a fixed xor tree). rows: the camera rows of this launch (or
 // nullptr: row = blockIdx.x); the row's G is chosen from its pair-list lengths.
+// tiles != nullptr: S is written straight into the dense tiles of the tile PCG
+// (block k at tile_off[k], scalar rows 96 apart; an off-diagonal block inside
+// a diagonal tile also into its transposed place) instead of the row-SoA.
 template <typename Real, int THREADS, bool STAGE, int G = 2>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
                const int2* pairs, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
-               const double* b_p, const double* b_l, double* bs) {
+               Real* tiles, const int* tile_off, const double* b_p, const double* b_l, double* bs) {
+  constexpr int TS = kTileBlocks * 6;  // scalar row stride of a tile
   static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per block: a power of two in [2, 32]");
   using R2 = typename Vec2<Real>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -450,16 +455,21 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     block_sum_array<double, 27, THREADS>(acc, &red[0][0]);
     if (threadIdx.x == 0) {
       const int hb = s_hpp[rb];
+      Real* Td = tiles ? tiles + tile_off[rb] : nullptr;
       int u = 0;
+#pragma unroll
       for (int i = 0; i < 6; ++i)
+#pragma unroll
         for (int c = i; c < 6; ++c, ++u) {
           double v = -acc[u] + (i == c ? lambda : 0.0);
           if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
-          Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
+          if (Td) Td[i * TS + c] = (Real)v;
+          else Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
           if (c != i) {
             double w = -acc[u];
             if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
-            Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
+            if (Td) Td[c * TS + i] = (Real)w;
+            else Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
           }
         }
       if (bs) {
@@ -483,12 +493,14 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
 #pragma unroll
     for (int t = 0; t < 18; ++t) acc[t] = 0;
     // two pairs per step: their index and Hpl loads are independent, so two
-    // gathers are in flight per thread; accumulation stays in pair order
+    // gathers are in flight per thread; accumulation stays in pair order.
+    // The pair list and S are touched once per pass: streamed (evict-first
+    // loads and stores), so the L2 lines go to the Hpl blocks gathered again
     auto load_b = [&](int blk, Real (&b)[18]) {
       const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
-        const R2 v = B2[t];
+        const R2 v = __ldg(B2 + t);
         b[2 * t] = v.x;
         b[2 * t + 1] = v.y;
       }
@@ -508,7 +520,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     int p = valid ? pair_ptr[k] + sub : 0;
     const int p1 = valid ? pair_ptr[k + 1] : 0;
     for (; p + STEP < p1; p += 2 * STEP) {
-      const int2 pa = pairs[p], pb = pairs[p + STEP];
+      const int2 pa = __ldcs(pairs + p), pb = __ldcs(pairs + p + STEP);
       Real ba[18], bb[18];
       load_b(pa.y, ba);
       load_b(pb.y, bb);
@@ -516,7 +528,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       accum(pb.x, bb);
     }
     if (p < p1) {
-      const int2 pa = pairs[p];
+      const int2 pa = __ldcs(pairs + p);
       Real ba[18];
       load_b(pa.y, ba);
       accum(pa.x, ba);
@@ -527,15 +539,39 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       for (int t = 0; t < 18; ++t) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);
     if (valid && sub == 0) {
       const int hb = s_hpp[k];
+      Real v[18];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
           const int e = (half * 3 + i) * 6 + c;
-          double v = -(double)acc[i * 6 + c];
-          if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + e];
-          Sr[(size_t)e * nblk + j] = (Real)v;
+          double w = -(double)acc[i * 6 + c];
+          if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + e];
+          v[i * 6 + c] = (Real)w;
         }
+      if (tiles) {
+        // this lane's three scalar rows of the block: six contiguous entries each
+        const int off = tile_off[k];
+        Real* T = tiles + off + half * 3 * TS;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int c = 0; c < 6; ++c) __stcs(T + i * TS + c, v[i * 6 + c]);
+        const int cc = rcol[k];
+        if (r / kTileBlocks == cc / kTileBlocks) {
+          Real* base = tiles + (size_t)(off / (TS * TS)) * (TS * TS);
+          const int lr = (r % kTileBlocks) * 6 + half * 3, lc = (cc % kTileBlocks) * 6;
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) __stcs(base + (lc + c) * TS + lr + i, v[i * 6 + c]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int c = 0; c < 6; ++c) __stcs(Sr + (size_t)((half * 3 + i) * 6 + c) * nblk + j, v[i * 6 + c]);
+      }
     }
   }
 }

@@ -487,6 +487,7 @@ struct Engine final : EngineBase {
   DBuf<int> row_list[3];
   int row_n[3] = {0, 0, 0};
   bool tiles_fresh = false;  // tiles hold the matrix of the current solve
+  bool tiles_from_schur = false;  // the last Schur pass wrote the tiles, not the row-SoA values
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
   size_t schur_smem = 0;
   DBuf<Real> hcontrib;
@@ -616,9 +617,14 @@ struct Engine final : EngineBase {
   // when bs != nullptr, the reduced right-hand side of b
   // lam_c / lam_l: per camera row / per landmark damping (batched windows);
   // nullptr: lambda for all
-  int schur(double lambda, double* bs, const double* lam_c = nullptr, const double* lam_l = nullptr) {
+  // to_tiles: write S into the tile PCG's dense tiles (tile_pcg_used())
+  int schur(double lambda, double* bs, const double* lam_c = nullptr, const double* lam_l = nullptr,
+            bool to_tiles = false) {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
+    if (to_tiles) G2OC_TRY(ensure_tiles());
+    tiles_from_schur = to_tiles;
+    if (to_tiles) tiles_fresh = true;
     if (S.Pf > 0) {
       G2OC_K(K_SCHUR_LANDMARK) schur_landmark<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
           hll.p, hpl.p, c->hb_ptr.p, c->hc_index.p, S.Pf, lambda, lam_l, dinv.p, nullptr, c->flag.p);
@@ -630,10 +636,28 @@ struct Engine final : EngineBase {
     for (int gi = 0; gi < 3; ++gi) {
       if (row_n[gi] == 0) continue;
       const int* rows = row_n[gi] == S.Cf ? nullptr : row_list[gi].p;
-      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
-      else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
-      else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs));
+      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
+      else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
+      else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
     }
+    return G2OC_OK;
+  }
+
+  // the PCG of a 6x6-block system runs on dense tiles (nearly full pattern,
+  // automatic PCG form)
+  bool tile_pcg_used() const { return c->S.pd == 6 && c->S.tile_ok && pcg_mode() == PCG_AUTO; }
+
+  int ensure_tiles() {
+    if (tiles.p) return G2OC_OK;
+    const Structure& S = c->S;
+    const size_t nt = S.tile_ij.size() / 2;
+    G2OC_TRY(tiles.alloc(nt * kTileSize));
+    G2OC_CUDA_TRY(cudaMemsetAsync(tiles.p, 0, tiles.bytes(), c->stream));  // blocks outside the pattern
+    // per block row, one slot of 6 partial sums per tile index (zero for the
+    // tiles outside the pattern)
+    const size_t nbt = (S.sys_nb + kTileBlocks - 1) / kTileBlocks;
+    G2OC_TRY(tpart.alloc((size_t)S.sys_nb * nbt * 6));
+    G2OC_CUDA_TRY(cudaMemsetAsync(tpart.p, 0, tpart.bytes(), c->stream));
     return G2OC_OK;
   }
 
@@ -641,19 +665,21 @@ struct Engine final : EngineBase {
   // (FP32 storage: 384 threads, two CTAs per SM; FP64: 512 threads, one)
   template <int G>
   int launch_schur_rows(const int* rows, int nrows, double lambda, const double* lam_c, const double* bp,
-                        const double* bl, double* bs) {
+                        const double* bl, double* bs, bool to_tiles) {
     constexpr int T = sizeof(Real) == 4 ? 384 : 512;
     cudaStream_t st = c->stream;
+    Real* tl = to_tiles ? tiles.p : nullptr;
+    const int* toff = to_tiles ? c->tile_off.p : nullptr;
     if (stage_in_smem) {
       auto kern = schur_rows<Real, T, true, G>;
       G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, bp, bl, bs);
     } else {
       G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false, G><<<nrows, T, 0, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, bp, bl, bs);
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
@@ -676,26 +702,23 @@ struct Engine final : EngineBase {
   int pcg_solve(const Real* val, const double* rhs, double* xout, bool fixed_d0) {
     const Structure& S = c->S;
     SysDev<Real> A = sys(val);
-    if (!fixed_d0) tiles_fresh = false;
+    // direct: the Schur pass wrote this system into the tiles (val unused)
+    const bool direct = tiles_from_schur && val == Sval.p && tile_pcg_used();
+    if (!fixed_d0 && !direct) tiles_fresh = false;
     if (S.pd == 6) {
       if (!fixed_d0) {
-        G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+        if (direct)
+          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv_tiles<Real><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(
+              tiles.p, c->tile_off.p, c->sys_diag.p, A.nb, minv.p, c->flag.p);
+        else
+          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
         G2OC_LAUNCH_CHECK();
       }
       if (kernels_pcg())
         return run_pcg<Real, 6>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, d1.p, q.p, qrow.p, tbuf.p, fixed_d0, nullptr);
-      if (S.tile_ok && pcg_mode() == PCG_AUTO) {
-        if (!tiles.p) {
-          const size_t nt = S.tile_ij.size() / 2;
-          G2OC_TRY(tiles.alloc(nt * kTileSize));
-          G2OC_CUDA_TRY(cudaMemsetAsync(tiles.p, 0, tiles.bytes(), c->stream));  // blocks outside the pattern
-          // per block row, one slot of 6 partial sums per tile index (zero
-          // for the tiles outside the pattern)
-          const size_t nbt = (A.nb + kTileBlocks - 1) / kTileBlocks;
-          G2OC_TRY(tpart.alloc((size_t)A.nb * nbt * 6));
-          G2OC_CUDA_TRY(cudaMemsetAsync(tpart.p, 0, tpart.bytes(), c->stream));
-        }
-        if (!fixed_d0 || !tiles_fresh) {  // a correction solve reuses the tiles of its first solve
+      if (tile_pcg_used()) {
+        G2OC_TRY(ensure_tiles());
+        if (!direct && (!fixed_d0 || !tiles_fresh)) {  // a correction solve reuses the tiles of its first solve
           G2OC_K(K_TILE_COPY) sys_to_tiles<Real><<<cdiv((long long)A.nnzb * 6, 256), 256, 0, c->stream>>>(
               A, c->tile_off.p, tiles.p);
           G2OC_LAUNCH_CHECK();
@@ -744,7 +767,7 @@ struct Engine final : EngineBase {
       }
     } else if (S.ba && S.schur) {
       cudaEvent_t ts = c->cur_stats ? c->mark() : nullptr;
-      G2OC_TRY(schur(lambda, c->rhs.p));
+      G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, !use_chol && tile_pcg_used()));
       const double* bp = c->b.p;
       const double* bl = c->b.p + (size_t)S.Cf * 6;
       if (ts) c->span(ts, &c->cur_stats->time_schur_complement, &c->cur_stats->time_linear_solver);
@@ -969,7 +992,7 @@ struct Engine final : EngineBase {
       return G2OC_ERR_NOT_SUPPORTED;
     }
     const bool use_chol = c->prm.linear_solver == G2OC_LINEAR_CHOLESKY;
-    G2OC_TRY(schur(0.0, nullptr));
+    G2OC_TRY(schur(0.0, nullptr, nullptr, nullptr, !use_chol && tile_pcg_used()));
     const double* rp = rhs;
     const double* rl = rhs + (size_t)S.Cf * 6;
     G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));

@@ -57,6 +57,25 @@ __global__ void sys_to_tiles(SysDev<Real> A, const int* tile_off, Real* tiles) {
   }
 }
 
+// Block-Jacobi preconditioner read from the tiles (the Schur rows wrote the
+// system there directly): the same values as the row-SoA diagonal blocks, so
+// the same inverses as pcg_diag_inv.
+template <typename Real>
+__global__ void pcg_diag_inv_tiles(const Real* tiles, const int* tile_off, const int* diag, int nb, double* minv,
+                                   int* nonfinite) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const Real* T = tiles + tile_off[diag[i]];
+  double M[36], I[36];
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) M[r * 6 + c] = (double)T[r * kTileScalars + c];
+  if (!inverse_gj<double, 6>(M, I)) *nonfinite = 1;
+#pragma unroll
+  for (int k = 0; k < 36; ++k) minv[(size_t)i * 36 + k] = I[k];
+}
+
 // four consecutive entries of a tile row (16-byte aligned), kept in the
 // storage type until they are used
 __device__ __forceinline__ void load4(const float* p, float (&m)[4]) {
