@@ -10,8 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libg2o_b200.so")
 SOURCES = ["g2oc_api.cu", "noalloc.cu", "structure.cpp"]
-HEADERS = ["g2oc_internal.h", "g2o_math.cuh", "reduce.cuh", "ba_kernels.cuh", "pcg_kernels.cuh",
-           "pg_kernels.cuh", "lm_kernels.cuh", "cholesky.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-Xcompiler", "-fopenmp",

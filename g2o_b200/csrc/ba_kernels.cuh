@@ -355,6 +355,18 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
   }
 }
 
+// Dense output of the Schur rows for batched windows: each camera row belongs
+// to one window, whose reduced system is a dense FP64 matrix (n + 1 rows of
+// n, row-major, at M + mat[w]; the last row holds the right-hand side). Only
+// the lower triangle is written: the diagonal blocks whole, each upper block
+// (r, c) transposed into block (c, r).
+struct DenseOut {
+  const int* win_of_cam;  // window of each camera row
+  const int* cam;         // first camera row of each window (nw + 1)
+  const long long* mat;   // offset of each window's matrix in M
+  double* M;              // nullptr: no dense output
+};
+
 template <typename Real>
 struct Vec2;
 template <>
@@ -382,13 +394,14 @@ struct Vec2<float> {
 // nullptr: row = blockIdx.x); the row's G is chosen from its pair-list lengths.
 // tiles != nullptr: S is written straight into the dense tiles of the tile PCG
 // (block k at tile_off[k], scalar rows 96 apart; an off-diagonal block inside
-// a diagonal tile also into its transposed place) instead of the row-SoA.
+// a diagonal tile also into its transposed place) instead of the row-SoA;
+// dn.M != nullptr: into the windows' dense matrices (DenseOut) instead.
 template <typename Real, int THREADS, bool STAGE, int G = 2>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
                const int2* pairs, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
-               Real* tiles, const int* tile_off, const double* b_p, const double* b_l, double* bs) {
+               Real* tiles, const int* tile_off, DenseOut dn, const double* b_p, const double* b_l, double* bs) {
   constexpr int TS = kTileBlocks * 6;  // scalar row stride of a tile
   static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per block: a power of two in [2, 32]");
   using R2 = typename Vec2<Real>::T;
@@ -399,6 +412,15 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
   const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
   const int rb = rptr[r], nblk = rptr[r + 1] - rb;
   Real* Sr = S + (size_t)rb * 36;
+  // dense output: the window's matrix, its row length and this row's first index
+  double* Md = nullptr;
+  int dn_n = 0, dn_h0 = 0;
+  if (dn.M) {
+    const int w = dn.win_of_cam[r];
+    dn_h0 = dn.cam[w];
+    dn_n = 6 * (dn.cam[w + 1] - dn_h0);
+    Md = dn.M + dn.mat[w];
+  }
   // One pass over the camera's Hpl blocks B_a, one thread per block: BD_a =
   // B_a Dinv_l, staged in shared memory (or, for cameras with more blocks
   // than shared memory holds, written to the camera-major scratch bdc and read
@@ -456,6 +478,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     if (threadIdx.x == 0) {
       const int hb = s_hpp[rb];
       Real* Td = tiles ? tiles + tile_off[rb] : nullptr;
+      double* Dd = Md ? Md + (size_t)(r - dn_h0) * 6 * dn_n + (r - dn_h0) * 6 : nullptr;
       int u = 0;
 #pragma unroll
       for (int i = 0; i < 6; ++i)
@@ -464,11 +487,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
           double v = -acc[u] + (i == c ? lambda : 0.0);
           if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
           if (Td) Td[i * TS + c] = (Real)v;
+          else if (Dd) Dd[(size_t)i * dn_n + c] = (double)(Real)v;
           else Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
           if (c != i) {
             double w = -acc[u];
             if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
             if (Td) Td[c * TS + i] = (Real)w;
+            else if (Dd) Dd[(size_t)c * dn_n + i] = (double)(Real)w;
             else Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
           }
         }
@@ -566,6 +591,15 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
 #pragma unroll
             for (int c = 0; c < 6; ++c) __stcs(base + (lc + c) * TS + lr + i, v[i * 6 + c]);
         }
+      } else if (Md) {
+        // block (r, cc) transposed into the lower triangle: entry (3h + i, c)
+        // at row (cc - h0) * 6 + c, column (r - h0) * 6 + 3h + i
+        const int cc = rcol[k];
+        double* D = Md + (size_t)(cc - dn_h0) * 6 * dn_n + (r - dn_h0) * 6 + half * 3;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) D[(size_t)c * dn_n + i] = (double)v[i * 6 + c];
       } else {
 #pragma unroll
         for (int i = 0; i < 3; ++i)

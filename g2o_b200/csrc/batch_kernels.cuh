@@ -122,124 +122,216 @@ static __global__ void win_spread_lambda(const int* win_of_cam, int Cf, const in
   else if (t < Cf + Pf) lam_l[t - Cf] = ws[win_of_lm[t - Cf]].lambda;
 }
 
-constexpr int kWinPanel = 16;  // columns per panel of the window Cholesky
+constexpr int kWinNB = 32;      // panel width of the window Cholesky (one warp)
+constexpr int kWinGroups = 16;  // fixed partial-sum groups of the backward solve
 
-// Dense Cholesky solve of one window's reduced camera system (upper blocks in
-// the row-SoA store, right-hand side bs) into x_p, one CTA per window from the
-// list. The full symmetric matrix is gathered in FP64 into the window's
-// scratch and factored in place, right-looking by panels of kWinPanel
-// columns: the panel is factored in shared memory (one column per step), then
-// the trailing lower triangle takes the panel's rank-kWinPanel update (a warp
-// per row, one read-modify-write per element per panel). The forward and
-// backward substitutions run on one warp. A non-positive pivot sets
-// solve_ok = 0 for the window. Dynamic shared memory: (nmax + 1) * (kWinPanel + 1)
-// doubles.
-template <typename Real, int THREADS>
-__global__ void __launch_bounds__(THREADS) win_chol_solve(const int* wlist, int nlist, WinDev W, SysDev<Real> A,
-                                                           const double* bs, double* xp, double* scratch,
-                                                           WinState* ws) {
+// shared memory of win_chol_solve for windows of at most nmax unknowns: the
+// panel (kWinNB x win_ldt(nmax), column-major), x (nmax) and the group sums
+__host__ __device__ inline int win_ldt(int n) { return (n + 2) & ~1; }
+inline size_t win_chol_smem(int nmax) {
+  return ((size_t)kWinNB * win_ldt(nmax) + nmax + kWinGroups * kWinNB) * sizeof(double);
+}
+
+// Dense Cholesky solve of one window's reduced camera system, one CTA per
+// window from the list (LinearSolverDense: LLT of the damped Schur complement,
+// then the two triangular solves). The matrix is the window's (n + 1) x n
+// block of the scratch, written by the Schur rows (lower triangle; row n =
+// the right-hand side), factored in place, right-looking, by panels of
+// kWinNB columns:
+//   - the panel (rows p0..n, the right-hand side row included) is staged in
+//     shared memory column-major;
+//   - warp 0 factors its diagonal block with the block's rows in registers
+//     (lane i = row i; L_jk broadcast by shuffles, no CTA barrier per column);
+//   - every thread solves one panel row against the diagonal block (the
+//     right-hand-side row gives y = L^-1 b on the way);
+//   - the trailing lower triangle takes the panel's update in 4 x 4 register
+//     tiles, each tile's 16 entries loaded before its products.
+// Then x = L^-T y backwards by blocks of kWinNB: the sums over the rows below
+// a block in kWinGroups fixed row groups, the block's triangle on warp 0.
+// Every sum runs in an order fixed by n alone (not by the CTA size). A
+// non-positive pivot sets solve_ok = 0 for the window and x = 0.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const int* wlist, int nlist, WinDev W, const double* bs,
+                                                           double* xp, double* scratch, WinState* ws) {
   constexpr int WARPS = THREADS / 32;
-  constexpr int PS = kWinPanel + 1;  // panel row stride (padded against bank conflicts)
-  extern __shared__ double sm[];     // panel: n x PS, then the vector (n)
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) double sm[];
   __shared__ int s_ok;
   if ((int)blockIdx.x >= nlist) return;
   const int w = wlist[blockIdx.x];
-  const int h0 = W.cam[w], nb = W.cam[w + 1] - h0, n = nb * 6;
+  const int h0 = W.cam[w], n = 6 * (W.cam[w + 1] - h0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (ws[w].done || n == 0) {
     for (int i = tid; i < n; i += THREADS) xp[(size_t)h0 * 6 + i] = 0.0;
     return;
   }
-  double* P = sm;
-  double* vec = sm + (size_t)n * PS;
+  const int ldt = win_ldt(n);
+  double* PT = sm;                          // PT[k * ldt + i]: panel column k, row p0 + i
+  double* vec = sm + (size_t)kWinNB * ldt;  // x
+  double* grp = vec + n;                    // kWinGroups x kWinNB
   double* M = scratch + W.mat[w];
-  // gather: block k of row r (internal order) -> M rows (r-h0)*6.., cols (c-h0)*6..
-  const int k0 = A.rptr[h0], k1 = A.rptr[h0 + nb];
-  for (long long t = tid; t < (long long)(k1 - k0) * 36; t += THREADS) {
-    const int k = k0 + (int)(t / 36), e = (int)(t % 36);
-    const int r = A.brow[k], c = A.rcol[k];
-    const int rb = A.rptr[r], nblk = A.rptr[r + 1] - rb;
-    const double v = (double)A.val[sys_offset<6>(rb, nblk, k - rb, e)];
-    const int i = (r - h0) * 6 + e / 6, j = (c - h0) * 6 + e % 6;
-    M[(size_t)i * n + j] = v;
-    if (r != c) M[(size_t)j * n + i] = v;  // a diagonal block writes each of its entries once
-  }
+  for (int i = tid; i < n; i += THREADS) M[(size_t)n * n + i] = bs[(size_t)h0 * 6 + i];
   if (tid == 0) s_ok = 1;
   __syncthreads();
-  for (int p0 = 0; p0 < n && s_ok; p0 += kWinPanel) {
-    const int pb = min(kWinPanel, n - p0), m = n - p0;  // panel width, panel rows
-    // the panel (rows p0.., columns p0..p0+pb) into shared memory
-    for (int t = tid; t < m * pb; t += THREADS) {
-      const int i = t / pb, cc = t % pb;
-      P[i * PS + cc] = M[(size_t)(p0 + i) * n + p0 + cc];
+  for (int p0 = 0; p0 < n; p0 += kWinNB) {
+    const int pb = min(kWinNB, n - p0);  // panel width
+    const int m = n + 1 - p0;            // panel rows, the right-hand side row last
+    // stage: row-major global reads (coalesced), entries above the diagonal
+    // and columns past pb as zeros
+    for (int t = tid; t < m * kWinNB; t += THREADS) {
+      const int i = t / kWinNB, k = t % kWinNB;
+      PT[k * ldt + i] = (k < pb && k <= i) ? M[(size_t)(p0 + i) * n + p0 + k] : 0.0;
     }
     __syncthreads();
-    for (int cc = 0; cc < pb; ++cc) {
-      const double d = P[cc * PS + cc];
-      if (!(d > 0.0)) {
-        if (tid == 0) s_ok = 0;
-        break;  // uniform: every thread read the same pivot
-      }
-      const double piv = sqrt(d);
-      for (int i = cc + 1 + tid; i < m; i += THREADS) P[i * PS + cc] /= piv;
-      __syncthreads();
-      if (tid == 0) P[cc * PS + cc] = piv;
-      // the panel's later columns
-      const int rest = pb - cc - 1;
-      for (int t = tid; t < (m - cc - 1) * rest; t += THREADS) {
-        const int i = cc + 1 + t / rest, c2 = cc + 1 + t % rest;
-        if (i >= c2) P[i * PS + c2] -= P[i * PS + cc] * P[c2 * PS + cc];
-      }
-      __syncthreads();
-    }
-    __syncthreads();  // every thread (also one that left the loop at a bad pivot) sees s_ok
-    if (!s_ok) break;
-    // write the factored panel back, then the trailing update
-    for (int t = tid; t < m * pb; t += THREADS) {
-      const int i = t / pb, cc = t % pb;
-      if (i >= cc) M[(size_t)(p0 + i) * n + p0 + cc] = P[i * PS + cc];
-    }
-    for (int i = pb + warp; i < m; i += WARPS) {
-      double li[kWinPanel];
+    // diagonal block on warp 0
+    if (warp == 0) {
+      double a[kWinNB];
 #pragma unroll
-      for (int cc = 0; cc < kWinPanel; ++cc) li[cc] = cc < pb ? P[i * PS + cc] : 0.0;
-      double* Mi = M + (size_t)(p0 + i) * n + p0;
-      for (int j = pb + lane; j <= i; j += 32) {
-        double acc = 0.0;
+      for (int j = 0; j < kWinNB; ++j) a[j] = PT[j * ldt + lane];
+      bool ok = true;
 #pragma unroll
-        for (int cc = 0; cc < kWinPanel; ++cc)
-          if (cc < pb) acc += li[cc] * P[j * PS + cc];
-        Mi[j] -= acc;
+      for (int k = 0; k < kWinNB; ++k) {
+        if (k < pb && ok) {
+          const double d = __shfl_sync(FULL, a[k], k);
+          if (!(d > 0.0)) {
+            ok = false;  // uniform: every lane read the same pivot
+          } else {
+            const double piv = sqrt(d);
+            if (lane == k) a[k] = piv;
+            else if (lane > k) a[k] /= piv;
+#pragma unroll
+            for (int j = k + 1; j < kWinNB; ++j) {
+              const double ljk = __shfl_sync(FULL, a[k], j);
+              if (lane >= j) a[j] -= a[k] * ljk;
+            }
+          }
+        }
+      }
+      if (lane < pb) {
+#pragma unroll
+        for (int j = 0; j < kWinNB; ++j)
+          if (j <= lane) PT[j * ldt + lane] = a[j];
+      }
+      if (!ok && lane == 0) s_ok = 0;
+    }
+    __syncthreads();
+    if (!s_ok) break;  // uniform
+    // panel rows below the diagonal block: x L_JJ^T = a
+    for (int i = pb + tid; i < m; i += THREADS) {
+      double x[kWinNB];
+#pragma unroll
+      for (int j = 0; j < kWinNB; ++j) x[j] = PT[j * ldt + i];
+#pragma unroll
+      for (int k = 0; k < kWinNB; ++k) {
+        if (k < pb) {
+          x[k] /= PT[k * ldt + k];
+#pragma unroll
+          for (int j = k + 1; j < kWinNB; ++j) x[j] -= x[k] * PT[k * ldt + j];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kWinNB; ++j) PT[j * ldt + i] = x[j];
+    }
+    __syncthreads();
+    // the factored panel back (lower part and the right-hand side row)
+    for (int t = tid; t < m * kWinNB; t += THREADS) {
+      const int i = t / kWinNB, k = t % kWinNB;
+      if (k < pb && k <= i) M[(size_t)(p0 + i) * n + p0 + k] = PT[k * ldt + i];
+    }
+    // trailing update: rows pb..m-1 (local), columns pb..m-2, lower part;
+    // 4 x 4 tiles (a, b), b <= a, numbered row-block by row-block
+    const int nc = m - 1 - pb;
+    if (nc > 0) {
+      const int nbc = (nc + 3) / 4, nbr = (m - pb + 3) / 4;
+      const int tri = nbc * (nbc + 1) / 2;
+      const int ntile = tri + (nbr > nbc ? nbc : 0);  // the last row block holds the right-hand side row only
+      for (int t = tid; t < ntile; t += THREADS) {
+        int a, b;
+        if (t < tri) {
+          a = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+          while ((a + 1) * (a + 2) / 2 <= t) ++a;
+          while (a * (a + 1) / 2 > t) --a;
+          b = t - a * (a + 1) / 2;
+        } else {
+          a = nbc;
+          b = t - tri;
+        }
+        const int i0 = pb + 4 * a, j0 = pb + 4 * b;
+        double cv[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = i0 + r, j = j0 + q;
+            cv[r][q] = (i < m && j <= m - 2 && j <= i) ? M[(size_t)(p0 + i) * n + p0 + j] : 0.0;
+          }
+        double acc[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+        for (int k = 0; k < pb; ++k) {
+          const double2 u0 = *reinterpret_cast<const double2*>(PT + k * ldt + i0);
+          const double2 u1 = *reinterpret_cast<const double2*>(PT + k * ldt + i0 + 2);
+          const double2 v0 = *reinterpret_cast<const double2*>(PT + k * ldt + j0);
+          const double2 v1 = *reinterpret_cast<const double2*>(PT + k * ldt + j0 + 2);
+          const double li[4] = {u0.x, u0.y, u1.x, u1.y}, lj[4] = {v0.x, v0.y, v1.x, v1.y};
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[r][q] += li[r] * lj[q];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = i0 + r, j = j0 + q;
+            if (i < m && j <= m - 2 && j <= i) M[(size_t)(p0 + i) * n + p0 + j] = cv[r][q] - acc[r][q];
+          }
       }
     }
     __syncthreads();
   }
-  __syncthreads();
   if (!s_ok) {
     if (tid == 0) ws[w].solve_ok = 0;
     for (int i = tid; i < n; i += THREADS) xp[(size_t)h0 * 6 + i] = 0.0;
     return;
   }
-  // L y = b, then L^T x = y, on warp 0
-  for (int i = tid; i < n; i += THREADS) vec[i] = bs[(size_t)h0 * 6 + i];
-  __syncthreads();
-  if (warp == 0) {
-    for (int k = 0; k < n; ++k) {
-      const double yk = vec[k] / M[(size_t)k * n + k];
-      for (int i = k + 1 + lane; i < n; i += 32) vec[i] -= M[(size_t)i * n + k] * yk;
-      __syncwarp();
-      if (lane == 0) vec[k] = yk;
-      __syncwarp();
+  // x = L^-T y, y = row n; blocks from the last
+  const double* y = M + (size_t)n * n;
+  const int nblk = (n + kWinNB - 1) / kWinNB;
+  for (int J = nblk - 1; J >= 0; --J) {
+    const int q0 = J * kWinNB, qb = min(kWinNB, n - q0), r0 = q0 + qb;
+    // group sums: g covers rows r0 + g, r0 + g + kWinGroups, ...
+    for (int g = warp; g < kWinGroups; g += WARPS) {
+      double acc = 0.0;
+      if (lane < qb)
+        for (int i = r0 + g; i < n; i += kWinGroups) acc += M[(size_t)i * n + q0 + lane] * vec[i];
+      grp[g * kWinNB + lane] = acc;
     }
-    for (int k = n - 1; k >= 0; --k) {
-      double sacc = 0.0;
-      for (int i = k + 1 + lane; i < n; i += 32) sacc += M[(size_t)i * n + k] * vec[i];
-      sacc = warp_sum(sacc);
-      if (lane == 0) vec[k] = (vec[k] - sacc) / M[(size_t)k * n + k];
-      __syncwarp();
+    __syncthreads();
+    if (warp == 0) {
+      double sj = 0.0;
+      if (lane < qb) {
+        sj = y[q0 + lane];
+        for (int g = 0; g < kWinGroups; ++g) sj -= grp[g * kWinNB + lane];
+      }
+      double lc[kWinNB];  // column lane of the block: lc[k] = L(q0 + k, q0 + lane)
+#pragma unroll
+      for (int k = 0; k < kWinNB; ++k)
+        lc[k] = (k < qb && lane <= k) ? M[(size_t)(q0 + k) * n + q0 + lane] : 0.0;
+#pragma unroll
+      for (int k = kWinNB - 1; k >= 0; --k) {
+        if (k < qb) {
+          const double xk = __shfl_sync(FULL, sj / lc[k], k);  // lane k: s_k / L_kk
+          if (lane == k) sj = xk;
+          else if (lane < k) sj -= lc[k] * xk;
+        }
+      }
+      if (lane < qb) vec[q0 + lane] = sj;
     }
+    __syncthreads();
   }
-  __syncthreads();
   for (int i = tid; i < n; i += THREADS) xp[(size_t)h0 * 6 + i] = vec[i];
   if (tid == 0) ws[w].solve_ok = 1;
 }

@@ -150,6 +150,7 @@ struct g2oc_ctx {
   int win_iterations = 0;
   int win_rounds = 0;
   bool win_tuned = false;
+  bool win_sparse = false;  // some window's reduced system has blocks outside its pattern (zeroed each round)
   cudaGraphExec_t win_graph = nullptr;
   g2oc::WinDev windev() const {
     return g2oc::WinDev{nw, win_cam.p, win_lm.p, win_edge.p, win_pose.p, win_point.p, win_mat.p};
@@ -617,9 +618,10 @@ struct Engine final : EngineBase {
   // when bs != nullptr, the reduced right-hand side of b
   // lam_c / lam_l: per camera row / per landmark damping (batched windows);
   // nullptr: lambda for all
-  // to_tiles: write S into the tile PCG's dense tiles (tile_pcg_used())
+  // to_tiles: write S into the tile PCG's dense tiles (tile_pcg_used());
+  // to_windows: into the batched windows' dense matrices
   int schur(double lambda, double* bs, const double* lam_c = nullptr, const double* lam_l = nullptr,
-            bool to_tiles = false) {
+            bool to_tiles = false, bool to_windows = false) {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (to_tiles) G2OC_TRY(ensure_tiles());
@@ -636,9 +638,9 @@ struct Engine final : EngineBase {
     for (int gi = 0; gi < 3; ++gi) {
       if (row_n[gi] == 0) continue;
       const int* rows = row_n[gi] == S.Cf ? nullptr : row_list[gi].p;
-      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
-      else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
-      else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles));
+      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
+      else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
+      else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
     }
     return G2OC_OK;
   }
@@ -665,21 +667,22 @@ struct Engine final : EngineBase {
   // (FP32 storage: 384 threads, two CTAs per SM; FP64: 512 threads, one)
   template <int G>
   int launch_schur_rows(const int* rows, int nrows, double lambda, const double* lam_c, const double* bp,
-                        const double* bl, double* bs, bool to_tiles) {
+                        const double* bl, double* bs, bool to_tiles, bool to_windows) {
     constexpr int T = sizeof(Real) == 4 ? 384 : 512;
     cudaStream_t st = c->stream;
     Real* tl = to_tiles ? tiles.p : nullptr;
     const int* toff = to_tiles ? c->tile_off.p : nullptr;
+    DenseOut dn{c->win_of_cam.p, c->win_cam.p, c->win_mat.p, to_windows ? c->win_scratch.p : nullptr};
     if (stage_in_smem) {
       auto kern = schur_rows<Real, T, true, G>;
       G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp, bl, bs);
     } else {
       G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false, G><<<nrows, T, 0, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp, bl, bs);
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
@@ -906,12 +909,12 @@ struct Engine final : EngineBase {
   template <int T>
   int launch_win_chol(const int* list, int nlist) {
     if (nlist == 0) return G2OC_OK;
-    const size_t smem = ((size_t)c->win_nmax * (kWinPanel + 1) + c->win_nmax) * sizeof(double);
+    const size_t smem = win_chol_smem(c->win_nmax);
     if (smem > 48 * 1024)
-      G2OC_CUDA_TRY(cudaFuncSetAttribute(win_chol_solve<Real, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem));
-    G2OC_K(K_CHOLESKY) win_chol_solve<Real, T><<<nlist, T, smem, c->stream>>>(
-        list, nlist, c->windev(), sys(Sval.p), c->rhs.p, c->xs.p, c->win_scratch.p, c->win_state.p);
+      G2OC_CUDA_TRY(
+          cudaFuncSetAttribute(win_chol_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    G2OC_K(K_CHOLESKY) win_chol_solve<T><<<nlist, T, smem, c->stream>>>(list, nlist, c->windev(), c->rhs.p, c->xs.p,
+                                                                          c->win_scratch.p, c->win_state.p);
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
@@ -934,6 +937,16 @@ struct Engine final : EngineBase {
       cls[n < 96 ? 0 : n < 192 ? 1 : 2].push_back(w);
     }
     DBuf<int> tmp;
+    // the solve factors the windows' matrices in place: every trial starts
+    // from a copy of them, and the copy is put back for the real solve
+    DBuf<double> saved;
+    const size_t mbytes = c->win_scratch.bytes();
+    G2OC_TRY(saved.alloc(c->win_scratch.n));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(saved.p, c->win_scratch.p, mbytes, cudaMemcpyDeviceToDevice, st));
+    auto restore = [&]() -> int {
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->win_scratch.p, saved.p, mbytes, cudaMemcpyDeviceToDevice, st));
+      return G2OC_OK;
+    };
     cudaEvent_t a, b;
     G2OC_CUDA_TRY(cudaEventCreate(&a));
     G2OC_CUDA_TRY(cudaEventCreate(&b));
@@ -945,7 +958,9 @@ struct Engine final : EngineBase {
       int best = 1;
       float best_ms = 1e30f;
       for (int t = 0; t < 3; ++t) {
+        G2OC_TRY(restore());
         G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));  // warm
+        G2OC_TRY(restore());
         G2OC_CUDA_TRY(cudaEventRecord(a, st));
         G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));
         G2OC_CUDA_TRY(cudaEventRecord(b, st));
@@ -965,6 +980,7 @@ struct Engine final : EngineBase {
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    G2OC_TRY(restore());
     for (int t = 0; t < 3; ++t) {
       c->win_list_n[t] = (int)lists[t].size();
       G2OC_TRY(c->win_list[t].upload(lists[t].empty() ? std::vector<int>{0} : lists[t], st));
@@ -977,7 +993,9 @@ struct Engine final : EngineBase {
   int batch_solve(bool autotune) override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    G2OC_TRY(schur(0.0, c->rhs.p, c->lam_c.p, c->lam_l.p));
+    if (c->win_sparse)
+      G2OC_CUDA_TRY(cudaMemsetAsync(c->win_scratch.p, 0, c->win_scratch.bytes(), st));
+    G2OC_TRY(schur(0.0, c->rhs.p, c->lam_c.p, c->lam_l.p, false, true));
     if (autotune && !c->win_tuned) G2OC_TRY(batch_autotune());
     for (int t = 0; t < 3; ++t) G2OC_TRY(launch_win_chol_t(t, c->win_list[t].p, c->win_list_n[t]));
     G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -2135,14 +2153,21 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
     prev = wi;
   }
   for (int j = prev + 1; j <= nw; ++j) we[j] = na;
+  // each window's dense (n + 1) x n matrix: the reduced system's lower
+  // triangle, then the right-hand side row
   std::vector<long long> mat(nw);
   long long off = 0;
   int nmax = 0;
   for (int i = 0; i < nw; ++i) {
     const int n = 6 * (wc[i + 1] - wc[i]);
     mat[i] = off;
-    off += (long long)n * n;
+    off += (long long)n * (n + 1);
     nmax = std::max(nmax, n);
+  }
+  if (win_chol_smem(nmax) > 227 * 1024) {
+    set_error("a window has %d free camera unknowns; the dense window solve takes at most %d", nmax,
+              (int)((227 * 1024 / sizeof(double) - kWinGroups * kWinNB - 2 * kWinNB) / (kWinNB + 1)));
+    return G2OC_ERR_NOT_SUPPORTED;
   }
   cudaStream_t st = c->stream;
   c->nw = nw;
@@ -2151,6 +2176,14 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   c->win_pose_h = pose_off;
   c->win_point_h = point_off;
   c->win_nmax = nmax;
+  // a window whose cameras do not all co-observe has zero blocks in its dense
+  // matrix, which the Schur rows do not write
+  c->win_sparse = false;
+  for (int i = 0; i < nw; ++i) {
+    const int nb = wc[i + 1] - wc[i];
+    const long long blocks = nb > 0 ? (long long)S.sys_rptr[wc[i + 1]] - S.sys_rptr[wc[i]] : 0;
+    if (blocks != (long long)nb * (nb + 1) / 2) c->win_sparse = true;
+  }
   G2OC_TRY(c->win_cam.upload(wc, st));
   G2OC_TRY(c->win_lm.upload(wl, st));
   G2OC_TRY(c->win_edge.upload(we, st));

@@ -113,3 +113,32 @@ def test_windows_reupload_keeps_round_and_matches_fresh_context(backend, small_w
     c = cw.optimize(ITER)
     d = backend.CudaWindows(other).optimize(ITER)
     assert [s["chi2"] for s in c] == [s["chi2"] for s in d]
+
+
+def _merge(g0, g1):
+    """One window made of two independent ones: its reduced camera system has
+    zero blocks between the two camera groups."""
+    from g2o_b200.abi import Graph
+
+    def cat(a, b):
+        return None if a is None else np.concatenate([a, b])
+
+    ev1 = g1.edge_vertex + np.array([g0.num_points, g0.num_poses], dtype=g1.edge_vertex.dtype)
+    return Graph(g0.pose_type, g0.edge_type, cat(g0.pose_estimate, g1.pose_estimate),
+                 np.concatenate([g0.edge_vertex, ev1]), cat(g0.measurement, g1.measurement),
+                 cat(g0.information, g1.information), cat(g0.pose_fixed, g1.pose_fixed),
+                 cat(g0.point_estimate, g1.point_estimate), cat(g0.point_fixed, g1.point_fixed),
+                 cat(g0.robust_delta, g1.robust_delta), g0.focal_length, tuple(g0.principal_point), "merged", {})
+
+
+def test_windows_with_sparse_reduced_system(backend, oracle_lib, small_windows):
+    """Windows whose cameras do not all co-observe (zero blocks in the dense
+    matrix) against the FP64 oracle, batched with full ones."""
+    ws = [_merge(small_windows[0], small_windows[1]), small_windows[2], _merge(small_windows[3], small_windows[4])]
+    cw = backend.CudaWindows(ws)
+    st = cw.optimize(ITER)
+    for w, g in enumerate(ws):
+        so, _ = oracle_run(oracle_lib, g)
+        assert st[w]["iterations"] == len(so)
+        assert st[w]["trials"] == sum(x["levenberg_iterations"] for x in so), w
+        assert abs(st[w]["chi2"] - so[-1]["chi2"]) <= 1e-8 * so[-1]["chi2"], (w, st[w]["chi2"], so[-1]["chi2"])
