@@ -431,9 +431,18 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
   double racc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
   for (int u = 0; u < 21; ++u) dacc[u] = 0;
+  // the next block's indices are loaded while this one's Hpl and Dinv are
+  int a_next = 0, l_next = 0;
+  if ((int)threadIdx.x < na) {
+    a_next = hc_blk[a0 + threadIdx.x];
+    l_next = hc_col[a0 + threadIdx.x];
+  }
   for (int t = threadIdx.x; t < na; t += THREADS) {
-    const int a = hc_blk[a0 + t];
-    const int l = hc_col[a0 + t];
+    const int a = a_next, l = l_next;
+    if (t + THREADS < na) {
+      a_next = hc_blk[a0 + t + THREADS];
+      l_next = hc_col[a0 + t + THREADS];
+    }
     const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)a * 18);
     const Real* Dl = dinv + (size_t)l * 9;
     Real b[18], D[9], bd[18];
@@ -466,40 +475,53 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     }
   }
   if (!STAGE) __threadfence_block();
-  // fixed-order CTA sum of the 21 diagonal-block and 6 right-hand-side terms
-  // (block_sum_array ends with a barrier, which also publishes the staged BD)
+  // fixed-order CTA sum of the 21 diagonal-block and 6 right-hand-side terms:
+  // warp sums, then term u summed over the warps in order by thread u, which
+  // writes its entry (and its mirror) of the diagonal block or of bs. The
+  // barrier also publishes the staged BD.
   {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double acc[27];
 #pragma unroll
     for (int u = 0; u < 21; ++u) acc[u] = (double)dacc[u];
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[21 + q] = racc[q];
-    block_sum_array<double, 27, THREADS>(acc, &red[0][0]);
-    if (threadIdx.x == 0) {
-      const int hb = s_hpp[rb];
-      Real* Td = tiles ? tiles + tile_off[rb] : nullptr;
-      double* Dd = Md ? Md + (size_t)(r - dn_h0) * 6 * dn_n + (r - dn_h0) * 6 : nullptr;
-      int u = 0;
 #pragma unroll
-      for (int i = 0; i < 6; ++i)
+    for (int u = 0; u < 27; ++u) acc[u] = warp_sum(acc[u]);
+    if (lane == 0) {
 #pragma unroll
-        for (int c = i; c < 6; ++c, ++u) {
-          double v = -acc[u] + (i == c ? lambda : 0.0);
-          if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
-          if (Td) Td[i * TS + c] = (Real)v;
-          else if (Dd) Dd[(size_t)i * dn_n + c] = (double)(Real)v;
-          else Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
-          if (c != i) {
-            double w = -acc[u];
-            if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
-            if (Td) Td[c * TS + i] = (Real)w;
-            else if (Dd) Dd[(size_t)c * dn_n + i] = (double)(Real)w;
-            else Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
-          }
+      for (int u = 0; u < 27; ++u) red[warp][u] = acc[u];
+    }
+    __syncthreads();
+    const int u = threadIdx.x;
+    if (u < 27) {
+      double sum = red[0][u];
+#pragma unroll
+      for (int w = 1; w < THREADS / 32; ++w) sum += red[w][u];
+      if (u < 21) {
+        int i = 0, c = u;  // u -> (i, c), i <= c, row by row
+        while (c >= 6 - i) {
+          c -= 6 - i;
+          ++i;
         }
-      if (bs) {
-#pragma unroll
-        for (int q = 0; q < 6; ++q) bs[(size_t)r * 6 + q] = b_p[(size_t)r * 6 + q] - acc[21 + q];
+        c += i;
+        const int hb = s_hpp[rb];
+        Real* Td = tiles ? tiles + tile_off[rb] : nullptr;
+        double* Dd = Md ? Md + (size_t)(r - dn_h0) * 6 * dn_n + (r - dn_h0) * 6 : nullptr;
+        double v = -sum + (i == c ? lambda : 0.0);
+        if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
+        if (Td) Td[i * TS + c] = (Real)v;
+        else if (Dd) Dd[(size_t)i * dn_n + c] = (double)(Real)v;
+        else Sr[(size_t)(i * 6 + c) * nblk] = (Real)v;
+        if (c != i) {
+          double w = -sum;
+          if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
+          if (Td) Td[c * TS + i] = (Real)w;
+          else if (Dd) Dd[(size_t)c * dn_n + i] = (double)(Real)w;
+          else Sr[(size_t)(c * 6 + i) * nblk] = (Real)w;
+        }
+      } else if (bs) {
+        bs[(size_t)r * 6 + (u - 21)] = b_p[(size_t)r * 6 + (u - 21)] - sum;
       }
     }
   }
@@ -544,8 +566,14 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     constexpr int STEP = G / 2;  // this lane's pairs: p0 + sub, p0 + sub + STEP, ...
     int p = valid ? pair_ptr[k] + sub : 0;
     const int p1 = valid ? pair_ptr[k + 1] : 0;
+    // the next step's pair indices are loaded while this step's blocks are
+    int2 na2 = make_int2(0, 0), nb2 = make_int2(0, 0);
+    if (p < p1) na2 = __ldcs(pairs + p);
+    if (p + STEP < p1) nb2 = __ldcs(pairs + p + STEP);
     for (; p + STEP < p1; p += 2 * STEP) {
-      const int2 pa = __ldcs(pairs + p), pb = __ldcs(pairs + p + STEP);
+      const int2 pa = na2, pb = nb2;
+      if (p + 2 * STEP < p1) na2 = __ldcs(pairs + p + 2 * STEP);
+      if (p + 3 * STEP < p1) nb2 = __ldcs(pairs + p + 3 * STEP);
       Real ba[18], bb[18];
       load_b(pa.y, ba);
       load_b(pb.y, bb);
@@ -553,7 +581,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       accum(pb.x, bb);
     }
     if (p < p1) {
-      const int2 pa = __ldcs(pairs + p);
+      const int2 pa = na2;
       Real ba[18];
       load_b(pa.y, ba);
       accum(pa.x, ba);

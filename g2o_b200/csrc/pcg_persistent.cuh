@@ -34,15 +34,21 @@ constexpr int kPcgWarps = kPcgThreads / 32;
 constexpr unsigned int kGridSyncSpinLimit = 1u << 21;
 
 // Grid-wide barrier over the co-resident CTAs of a cooperative launch:
-// arrival counter plus generation number. Returns false (in every thread of
-// the CTA) once any CTA's wait has run out; the caller then returns.
-__device__ __forceinline__ bool grid_barrier(PcgState* st) {
+// arrival counter plus generation number. gen (meaningful in thread 0 only)
+// is the generation the barrier completes from: read once per launch by
+// grid_gen_start (no barrier can complete before every CTA has read it) and
+// counted locally after that, so an arrival costs one atomic and no read of
+// the shared generation. Returns false (in every thread of the CTA) once any
+// CTA's wait has run out; the caller then returns.
+__device__ __forceinline__ unsigned grid_gen_start(const PcgState* st) {
+  return threadIdx.x == 0 ? *reinterpret_cast<const volatile unsigned int*>(&st->sync_gen) : 0u;
+}
+__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = &st->sync_gen;
     volatile int* verr = &st->sync_error;
-    const unsigned int gen = *vgen;
     __threadfence();
     if (atomicAdd(&st->sync_count, 1u) == gridDim.x - 1) {
       atomicExch(&st->sync_count, 0u);
@@ -55,10 +61,11 @@ __device__ __forceinline__ bool grid_barrier(PcgState* st) {
           atomicExch(&st->sync_error, 1);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
     __threadfence();
+    gen += 1;
     s_ok = (*verr == 0);
   }
   __syncthreads();
@@ -136,6 +143,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
   const bool fixed = fixed_d0 != 0;
   const double d0_in = st->d0;
   const double carry = st->residual_carry;
+  unsigned gen = grid_gen_start(st);
 
   // r = b, x = 0, s = M^-1 r, d = s, dn = r.s (linear_solver_pcg.hpp:117-137)
   double rs = 0.0;
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
     }
   }
   cta_partial(rs, part_rs, red);
-  if (!grid_barrier(st)) return;
+  if (!grid_barrier(st, gen)) return;
   double dn = cta_sum_all(part_rs, red);
   double d0 = d0_in;
   if (!fixed) {
@@ -207,7 +215,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
       if (lane < BS) cpart[(size_t)ch * BS + lane] = pick<BS>(acc, lane);
     }
     cta_partial(dq, part_dq, red);
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, gen)) return;
     const double dqs = cta_sum_all(part_dq, red);
     if (!(dqs > 0.0)) {
       // the (rounded) matrix is not positive definite along d: stop with the
@@ -249,7 +257,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
       }
     }
     cta_partial(rs, part_rs, red);
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, gen)) return;
     const double dn_new = cta_sum_all(part_rs, red);
     const double beta = dn_new / dn;
     dn = dn_new;
@@ -261,7 +269,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
         const size_t o = (size_t)c * BS + lane;
         d[o] = __ldcg(s + o) + beta * __ldcg(d + o);
       }
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, gen)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->dn = dn;

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
   const bool fixed = fixed_d0 != 0;
   const double d0_in = st->d0;
   const double carry = st->residual_carry;
+  unsigned gen = grid_gen_start(st);
 
   // r = b, x = 0, s = M^-1 r, d_{-1} = 0, dn = r.s (linear_solver_pcg.hpp:117-137)
   double rs = 0.0;
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     }
   }
   cta_partial<kTileWarps>(rs, part_rs, red);
-  if (!grid_barrier(st)) return;
+  if (!grid_barrier(st, gen)) return;
   double dn = cta_sum_all<kTileWarps>(part_rs, red);
   double d0 = d0_in;
   if (!fixed) {
@@ -197,8 +198,27 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
       }
       __syncthreads();
     }
+    // the first block row of this warp in phase C: its s, d_{k-1}, r, x and
+    // M^-1 row, loaded while the CTAs meet at the barrier (they do not
+    // depend on alpha)
+    double sa = 0.0, da = 0.0, ra = 0.0, xa = 0.0, mrow[BS];
+    auto load_row = [&](int c) {
+      if (lane < BS) {
+        const size_t o = (size_t)c * BS + lane;
+        sa = __ldcg(s + o);
+        da = __ldcg(dprev + o);
+        ra = __ldcg(r + o);
+        xa = __ldcg(x + o);
+        const double* M = minv + (size_t)c * BS * BS + (size_t)lane * BS;
+#pragma unroll
+        for (int b2 = 0; b2 < BS; ++b2) mrow[b2] = M[b2];
+      }
+    };
+#pragma unroll
+    for (int b2 = 0; b2 < BS; ++b2) mrow[b2] = 0.0;
+    if (gw < nb) load_row(gw);
     cta_partial<kTileWarps>(dq, part_dq, red);
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, gen)) return;
     const double dqs = cta_sum_all<kTileWarps>(part_dq, red);
     if (!(dqs > 0.0)) {
       breakdown = true;  // not positive definite along d (see pcg_solve_persistent)
@@ -208,6 +228,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     // ---- C: block rows
     rs = 0.0;
     for (int c = gw; c < nb; c += GW) {
+      if (c != gw) load_row(c);
       double q[BS];
 #pragma unroll
       for (int a = 0; a < BS; ++a) q[a] = 0.0;
@@ -216,26 +237,28 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
 #pragma unroll
         for (int a = 0; a < BS; ++a) q[a] += __ldcg(pr + (size_t)e * BS + a);
       }
-      double rc[BS], dk[BS];
 #pragma unroll
-      for (int a = 0; a < BS; ++a) {
-        q[a] = warp_sum(q[a]);
-        const size_t o = (size_t)c * BS + a;
-        dk[a] = __ldcg(s + o) + beta * __ldcg(dprev + o);
-        rc[a] = __ldcg(r + o) - alpha * q[a];
-      }
-      __syncwarp();  // every lane has read s_c and r_c before the owner lanes rewrite them
-      rs += row_precondition<BS>(minv, c, rc, lane, s);
+      for (int a = 0; a < BS; ++a) q[a] = warp_sum(q[a]);
+      const double qa = pick<BS>(q, lane);
+      const double dka = sa + beta * da;
+      const double rca = ra - alpha * qa;
+      double rc[BS];
+#pragma unroll
+      for (int a = 0; a < BS; ++a) rc[a] = __shfl_sync(0xffffffffu, rca, a);
       if (lane < BS) {
+        double v = 0.0;
+#pragma unroll
+        for (int b2 = 0; b2 < BS; ++b2) v += mrow[b2] * rc[b2];
         const size_t o = (size_t)c * BS + lane;
-        const double dka = pick<BS>(dk, lane);
-        x[o] += alpha * dka;
+        s[o] = v;
+        rs += rca * v;
+        x[o] = xa + alpha * dka;
         dcur[o] = dka;
-        r[o] = pick<BS>(rc, lane);
+        r[o] = rca;
       }
     }
     cta_partial<kTileWarps>(rs, part_rs, red);
-    if (!grid_barrier(st)) return;
+    if (!grid_barrier(st, gen)) return;
     const double dn_new = cta_sum_all<kTileWarps>(part_rs, red);
     beta = dn_new / dn;
     dn = dn_new;
