@@ -16,6 +16,18 @@
 
 namespace g2oc {
 
+// two entries of the storage type in one access
+template <typename Real>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using T = double2;
+};
+template <>
+struct Vec2<float> {
+  using T = float2;
+};
+
 struct BAEdges {
   int n;                  // active edges
   const int2* v;          // (point index, pose index), point-major device order
@@ -183,14 +195,19 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
 // Landmark pass, edge-parallel form (graphs whose landmarks have at most 32
 // edges and whose (camera, landmark) pairs are unique): one warp per chunk of
 // whole landmarks (at most 32 edges, packed on the host), one lane per edge.
-// Edge loads are coalesced and each lane writes its own Hpl block (blocks
-// follow the edge order); H_ll and b_l are summed by a segmented warp scan
-// keyed by landmark (fixed shuffle order), written by the segment's last lane.
+// Edge loads are coalesced. The Hpl blocks of a chunk's edges are one
+// contiguous range (one block per edge of a free camera, numbered in edge
+// order): each lane puts its block in shared memory and the warp stores the
+// range with coalesced pair stores. H_ll and b_l are summed by a segmented
+// warp scan keyed by landmark (fixed shuffle order), written by the segment's
+// last lane. Launched with 256 threads (8 warps).
 template <typename Real>
-__global__ void ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, int nchunks, const int* e_lm,
+__global__ void __launch_bounds__(256) ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, int nchunks, const int* e_lm,
                                  Real* hll, Real* hpl, double* b_l) {
-  const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  using R2 = typename Vec2<Real>::T;
+  __shared__ R2 stage[8][32 * 9];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + wid;
   if (ch >= nchunks) return;
   const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
   const int k = e0 + lane;
@@ -198,6 +215,9 @@ __global__ void ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, 
   Real H[6] = {0, 0, 0, 0, 0, 0};
   double bl[3] = {0, 0, 0};
   int key = -1 - lane;  // distinct for idle lanes
+  const int blk = act ? E.hpl[k] : -1;
+  const unsigned has = __ballot_sync(0xffffffffu, blk >= 0);
+  const int blk0 = (int)__reduce_min_sync(0xffffffffu, blk >= 0 ? (unsigned)blk : 0x7fffffffu);
   if (act) {
     key = e_lm[k];
     const int2 v = E.v[k];
@@ -228,13 +248,20 @@ __global__ void ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, 
     H[5] = A0[2] * Jp[2] + A1[2] * Jp[5];
 #pragma unroll
     for (int i = 0; i < 3; ++i) bl[i] = Jpd[i] * we0 + Jpd[3 + i] * we1;
-    const int blk = E.hpl[k];
     if (blk >= 0) {
-      Real* o = hpl + (size_t)blk * 18;
+      Real hb[18];
 #pragma unroll
       for (int r = 0; r < 6; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) o[r * 3 + c] = Jc[r] * A0[c] + Jc[6 + r] * A1[c];
+        for (int c = 0; c < 3; ++c) hb[r * 3 + c] = Jc[r] * A0[c] + Jc[6 + r] * A1[c];
+      R2* o = &stage[wid][(blk - blk0) * 9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        R2 t;
+        t.x = hb[2 * q];
+        t.y = hb[2 * q + 1];
+        o[q] = t;
+      }
     }
   }
   // segmented inclusive scan by landmark
@@ -261,6 +288,13 @@ __global__ void ba_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, 
 #pragma unroll
     for (int i = 0; i < 3; ++i) b_l[(size_t)key * 3 + i] = bl[i];
   }
+  // the chunk's Hpl range (8-byte aligned in FP32, 16 in FP64), coalesced
+  __syncwarp();
+  const int npair = __popc(has) * 9;
+  if (npair > 0) {
+    R2* out = reinterpret_cast<R2*>(hpl + (size_t)blk0 * 18);
+    for (int i = lane; i < npair; i += 32) out[i] = stage[wid][i];
+  }
 }
 
 // Camera pass: one CTA per free camera sums H_pp = sum Jc^T Om' Jc (21 unique)
@@ -276,11 +310,27 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
 #pragma unroll
   for (int i = 0; i < 6; ++i) bp[i] = 0.0;
   const int j1 = CE.ptr[h + 1];
-  for (int j = CE.ptr[h] + threadIdx.x; j < j1; j += THREADS) {
-    const int2 v = CE.v[j];
-    const double4 om = CE.om[j];
+  // the next edge's record is loaded while this one's point is
+  int j = CE.ptr[h] + threadIdx.x;
+  int2 vn = make_int2(0, 0);
+  double2 zn = make_double2(0.0, 0.0);
+  double4 omn = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (j < j1) {
+    vn = CE.v[j];
+    zn = CE.z[j];
+    omn = CE.om[j];
+  }
+  for (; j < j1; j += THREADS) {
+    const int2 v = vn;
+    const double2 z = zn;
+    const double4 om = omn;
+    if (j + THREADS < j1) {
+      vn = CE.v[j + THREADS];
+      zn = CE.z[j + THREADS];
+      omn = CE.om[j + THREADS];
+    }
     double e[2], Xc[3], chi2, w;
-    ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
+    ba_edge_error(V, v, z, om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
     double Jpd[6], Jcd[12];
     ba_jacobians_from_xc(cam, Xc, V.f, Jpd, Jcd);
@@ -367,16 +417,6 @@ struct DenseOut {
   double* M;              // nullptr: no dense output
 };
 
-template <typename Real>
-struct Vec2;
-template <>
-struct Vec2<double> {
-  using T = double2;
-};
-template <>
-struct Vec2<float> {
-  using T = float2;
-};
 
 // Schur complement by camera rows (block_solver.hpp:343-433): one CTA per
 // free camera r stages the camera's BD_a blocks (contiguous in bdc) in shared
