@@ -59,10 +59,28 @@ __global__ void __launch_bounds__(THREADS) win_chi2(BAEdges E, BAVertices V, Win
   WinState& s = ws[w];
   if (s.done || (which == 0 && s.qmax != 0)) return;
   double r = 0.0;
-  for (int k = W.edge[w] + threadIdx.x; k < W.edge[w + 1]; k += THREADS) {
+  const int k1 = W.edge[w + 1];
+  // the next edge's record is loaded while this one's vertices are
+  int k = W.edge[w] + threadIdx.x;
+  int2 vn = make_int2(0, 0);
+  double2 zn = make_double2(0.0, 0.0);
+  double4 omn = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (k < k1) {
+    vn = E.v[k];
+    zn = E.z[k];
+    omn = E.om[k];
+  }
+  for (; k < k1; k += THREADS) {
+    const int2 v = vn;
+    const double2 z = zn;
+    const double4 om = omn;
+    if (k + THREADS < k1) {
+      vn = E.v[k + THREADS];
+      zn = E.z[k + THREADS];
+      omn = E.om[k + THREADS];
+    }
     double e[2], Xc[3], chi2, wt;
-    const double4 om = E.om[k];
-    ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, wt);
+    ba_edge_error(V, v, z, om, e, Xc, chi2, wt);
     if (om.w > 0.0) {
       double rho[3];
       huber(chi2, om.w, rho);

@@ -144,6 +144,7 @@ struct g2oc_ctx {
   g2oc::DBuf<int> win_active;
   g2oc::DBuf<int> win_list[3];       // windows factored with 128 / 256 / 512 threads
   int win_list_n[3] = {0, 0, 0};
+  int win_list_nmax[3] = {0, 0, 0};  // largest window of each list (its shared memory)
   int win_threads_of_class[3] = {0, 0, 0};  // autotuned, per size class (n < 96, < 192, >= 192)
   std::vector<int> win_threads;      // per window, for the statistics
   int win_nmax = 0;
@@ -506,13 +507,18 @@ struct Engine final : EngineBase {
       G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
       {
         std::vector<int> lists[3];
+        std::vector<double> work(S.Cf);
         for (int r = 0; r < S.Cf; ++r) {
           const int k0 = S.sys_rptr[r], k1 = S.sys_rptr[r + 1];
           const double pairs = (double)(S.s_pair_ptr[k1] - S.s_pair_ptr[k0]);
           const double mean = k1 - k0 > 1 ? pairs / (k1 - k0 - 1) : 0.0;
           lists[mean <= 12.0 ? 0 : mean <= 40.0 ? 1 : 2].push_back(r);
+          work[r] = pairs + 2.0 * (S.hc_ptr[r + 1] - S.hc_ptr[r]);
         }
+        // rows with the most pair products first: the long rows start in
+        // the first wave of CTAs (a row's result does not depend on when it runs)
         for (int gi = 0; gi < 3; ++gi) {
+          std::stable_sort(lists[gi].begin(), lists[gi].end(), [&](int a, int b) { return work[a] > work[b]; });
           row_n[gi] = (int)lists[gi].size();
           G2OC_TRY(row_list[gi].upload(lists[gi].empty() ? std::vector<int>{0} : lists[gi], c->stream));
         }
@@ -637,7 +643,7 @@ struct Engine final : EngineBase {
     const double* bl = c->b.p + (size_t)S.Cf * 6;
     for (int gi = 0; gi < 3; ++gi) {
       if (row_n[gi] == 0) continue;
-      const int* rows = row_n[gi] == S.Cf ? nullptr : row_list[gi].p;
+      const int* rows = row_list[gi].p;
       if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
       else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
       else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
@@ -907,9 +913,9 @@ struct Engine final : EngineBase {
 
   // one launch of the dense per-window solve with THREADS threads per window
   template <int T>
-  int launch_win_chol(const int* list, int nlist) {
+  int launch_win_chol(const int* list, int nlist, int nmax) {
     if (nlist == 0) return G2OC_OK;
-    const size_t smem = win_chol_smem(c->win_nmax);
+    const size_t smem = win_chol_smem(nmax);
     if (smem > 48 * 1024)
       G2OC_CUDA_TRY(
           cudaFuncSetAttribute(win_chol_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -918,10 +924,10 @@ struct Engine final : EngineBase {
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
-  int launch_win_chol_t(int t, const int* list, int nlist) {
-    if (t == 0) return launch_win_chol<128>(list, nlist);
-    if (t == 1) return launch_win_chol<256>(list, nlist);
-    return launch_win_chol<512>(list, nlist);
+  int launch_win_chol_t(int t, const int* list, int nlist, int nmax) {
+    if (t == 0) return launch_win_chol<128>(list, nlist, nmax);
+    if (t == 1) return launch_win_chol<256>(list, nlist, nmax);
+    return launch_win_chol<512>(list, nlist, nmax);
   }
 
   // Times the dense solve with 128 / 256 / 512 threads per window on each
@@ -931,11 +937,21 @@ struct Engine final : EngineBase {
     const Structure& S = c->S;
     (void)S;
     cudaStream_t st = c->stream;
+    // windows largest first within a launch (the long factorizations start
+    // in the first wave)
+    auto wn = [&](int w) { return 6 * (c->win_cam_h[w + 1] - c->win_cam_h[w]); };
+    auto by_size = [&](std::vector<int>& v) {
+      std::stable_sort(v.begin(), v.end(), [&](int a, int b) { return wn(a) > wn(b); });
+    };
     std::vector<int> cls[3];
+    int cls_nmax[3] = {0, 0, 0};
     for (int w = 0; w < c->nw; ++w) {
-      const int n = 6 * (c->win_cam_h[w + 1] - c->win_cam_h[w]);
-      cls[n < 96 ? 0 : n < 192 ? 1 : 2].push_back(w);
+      const int n = wn(w);
+      const int k = n < 96 ? 0 : n < 192 ? 1 : 2;
+      cls[k].push_back(w);
+      cls_nmax[k] = std::max(cls_nmax[k], n);
     }
+    for (auto& v : cls) by_size(v);
     DBuf<int> tmp;
     // the solve factors the windows' matrices in place: every trial starts
     // from a copy of them, and the copy is put back for the real solve
@@ -959,10 +975,10 @@ struct Engine final : EngineBase {
       float best_ms = 1e30f;
       for (int t = 0; t < 3; ++t) {
         G2OC_TRY(restore());
-        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));  // warm
+        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size(), cls_nmax[k]));  // warm
         G2OC_TRY(restore());
         G2OC_CUDA_TRY(cudaEventRecord(a, st));
-        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size()));
+        G2OC_TRY(launch_win_chol_t(t, tmp.p, (int)cls[k].size(), cls_nmax[k]));
         G2OC_CUDA_TRY(cudaEventRecord(b, st));
         G2OC_CUDA_TRY(cudaEventSynchronize(b));
         float ms = 0.f;
@@ -982,7 +998,9 @@ struct Engine final : EngineBase {
     cudaEventDestroy(b);
     G2OC_TRY(restore());
     for (int t = 0; t < 3; ++t) {
+      by_size(lists[t]);
       c->win_list_n[t] = (int)lists[t].size();
+      c->win_list_nmax[t] = lists[t].empty() ? 0 : wn(lists[t][0]);
       G2OC_TRY(c->win_list[t].upload(lists[t].empty() ? std::vector<int>{0} : lists[t], st));
     }
     G2OC_CUDA_TRY(cudaStreamSynchronize(st));
@@ -997,7 +1015,8 @@ struct Engine final : EngineBase {
       G2OC_CUDA_TRY(cudaMemsetAsync(c->win_scratch.p, 0, c->win_scratch.bytes(), st));
     G2OC_TRY(schur(0.0, c->rhs.p, c->lam_c.p, c->lam_l.p, false, true));
     if (autotune && !c->win_tuned) G2OC_TRY(batch_autotune());
-    for (int t = 0; t < 3; ++t) G2OC_TRY(launch_win_chol_t(t, c->win_list[t].p, c->win_list_n[t]));
+    for (int t = 0; t < 3; ++t)
+      G2OC_TRY(launch_win_chol_t(t, c->win_list[t].p, c->win_list_n[t], c->win_list_nmax[t]));
     G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
     return backsub(c->b.p + (size_t)S.Cf * 6, c->xs.p, c->x.p + (size_t)S.Cf * 6);
   }
@@ -2217,7 +2236,7 @@ static int window_round(g2oc_ctx* c, bool autotune) {
   const WinDev W = c->windev();
   const int n = c->vec_size();
   G2OC_CUDA_TRY(cudaMemsetAsync(c->win_active.p, 0, sizeof(int), st));
-  G2OC_K(K_CHI2) win_chi2<256><<<c->nw, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 0);
+  G2OC_K(K_CHI2) win_chi2<1024><<<c->nw, 1024, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 0);
   G2OC_LAUNCH_CHECK();
   G2OC_TRY(c->eng->build_system());
   G2OC_TRY(c->eng->batch_lambda_init(c->prm.initial_lambda, c->prm.tau));
@@ -2230,7 +2249,7 @@ static int window_round(g2oc_ctx* c, bool autotune) {
                                                                     c->win_state.p, c->x.p);
   G2OC_LAUNCH_CHECK();
   G2OC_TRY(oplus(c));
-  G2OC_K(K_CHI2) win_chi2<256><<<c->nw, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 1);
+  G2OC_K(K_CHI2) win_chi2<1024><<<c->nw, 1024, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 1);
   G2OC_K(K_LM_CONTROL) win_scale<256><<<c->nw, 256, 0, st>>>(c->x.p, c->b.p, S.Cf, W, c->win_state.p);
   G2OC_K(K_LM_CONTROL) win_decide<<<cdiv(c->nw, 128), 128, 0, st>>>(c->win_state.p, c->nw,
                                                                     c->prm.max_trials_after_failure, c->win_iterations,
