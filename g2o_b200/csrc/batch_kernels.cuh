@@ -144,10 +144,11 @@ constexpr int kWinNB = 32;      // panel width of the window Cholesky (one warp)
 constexpr int kWinGroups = 16;  // fixed partial-sum groups of the backward solve
 
 // shared memory of win_chol_solve for windows of at most nmax unknowns: the
-// panel (kWinNB x win_ldt(nmax), column-major), x (nmax) and the group sums
+// panel (kWinNB x win_ldt(nmax), column-major), x (nmax), the group sums and
+// the reciprocal pivots (nmax)
 __host__ __device__ inline int win_ldt(int n) { return (n + 2) & ~1; }
 inline size_t win_chol_smem(int nmax) {
-  return ((size_t)kWinNB * win_ldt(nmax) + nmax + kWinGroups * kWinNB) * sizeof(double);
+  return ((size_t)kWinNB * win_ldt(nmax) + 2 * nmax + kWinGroups * kWinNB) * sizeof(double);
 }
 
 // Dense Cholesky solve of one window's reduced camera system, one CTA per
@@ -166,8 +167,11 @@ inline size_t win_chol_smem(int nmax) {
 //     tiles, each tile's 16 entries loaded before its products.
 // Then x = L^-T y backwards by blocks of kWinNB: the sums over the rows below
 // a block in kWinGroups fixed row groups, the block's triangle on warp 0.
-// Every sum runs in an order fixed by n alone (not by the CTA size). A
-// non-positive pivot sets solve_ok = 0 for the window and x = 0.
+// Every sum runs in an order fixed by n alone (not by the CTA size). The
+// pivots' reciprocals 1/L_kk = rsqrt(d_k) are kept, so the long dependent
+// chains (the diagonal block, each panel row, the backward block solves)
+// multiply instead of divide. A non-positive pivot sets solve_ok = 0 for the
+// window and x = 0.
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const int* wlist, int nlist, WinDev W, const double* bs,
                                                            double* xp, double* scratch, WinState* ws) {
@@ -187,6 +191,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
   double* PT = sm;                          // PT[k * ldt + i]: panel column k, row p0 + i
   double* vec = sm + (size_t)kWinNB * ldt;  // x
   double* grp = vec + n;                    // kWinGroups x kWinNB
+  double* invd = grp + kWinGroups * kWinNB; // 1 / L_kk
   double* M = scratch + W.mat[w];
   for (int i = tid; i < n; i += THREADS) M[(size_t)n * n + i] = bs[(size_t)h0 * 6 + i];
   if (tid == 0) s_ok = 1;
@@ -214,9 +219,13 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
           if (!(d > 0.0)) {
             ok = false;  // uniform: every lane read the same pivot
           } else {
-            const double piv = sqrt(d);
-            if (lane == k) a[k] = piv;
-            else if (lane > k) a[k] /= piv;
+            const double inv = rsqrt(d);
+            if (lane == k) {
+              a[k] = d * inv;
+              invd[p0 + k] = inv;
+            } else if (lane > k) {
+              a[k] *= inv;
+            }
 #pragma unroll
             for (int j = k + 1; j < kWinNB; ++j) {
               const double ljk = __shfl_sync(FULL, a[k], j);
@@ -242,7 +251,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
 #pragma unroll
       for (int k = 0; k < kWinNB; ++k) {
         if (k < pb) {
-          x[k] /= PT[k * ldt + k];
+          x[k] *= invd[p0 + k];
 #pragma unroll
           for (int j = k + 1; j < kWinNB; ++j) x[j] -= x[k] * PT[k * ldt + j];
         }
@@ -341,7 +350,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
 #pragma unroll
       for (int k = kWinNB - 1; k >= 0; --k) {
         if (k < qb) {
-          const double xk = __shfl_sync(FULL, sj / lc[k], k);  // lane k: s_k / L_kk
+          const double xk = __shfl_sync(FULL, sj * invd[q0 + k], k);  // lane k: s_k / L_kk
           if (lane == k) sj = xk;
           else if (lane < k) sj -= lc[k] * xk;
         }

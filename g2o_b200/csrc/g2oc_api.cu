@@ -2185,7 +2185,7 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   }
   if (win_chol_smem(nmax) > 227 * 1024) {
     set_error("a window has %d free camera unknowns; the dense window solve takes at most %d", nmax,
-              (int)((227 * 1024 / sizeof(double) - kWinGroups * kWinNB - 2 * kWinNB) / (kWinNB + 1)));
+              (int)((227 * 1024 / sizeof(double) - kWinGroups * kWinNB - 2 * kWinNB) / (kWinNB + 2)));
     return G2OC_ERR_NOT_SUPPORTED;
   }
   cudaStream_t st = c->stream;
