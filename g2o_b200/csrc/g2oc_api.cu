@@ -717,10 +717,10 @@ struct Engine final : EngineBase {
     if (S.pd == 6) {
       if (!fixed_d0) {
         if (direct)
-          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv_tiles<Real><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(
+          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv_tiles<Real><<<cdiv(A.nb, 20), 128, 0, c->stream>>>(
               tiles.p, c->tile_off.p, c->sys_diag.p, A.nb, minv.p, c->flag.p);
         else
-          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<Real, 6><<<cdiv(A.nb, 128), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
+          G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv6_lanes<Real><<<cdiv(A.nb, 20), 128, 0, c->stream>>>(A, minv.p, c->flag.p);
         G2OC_LAUNCH_CHECK();
       }
       if (kernels_pcg())

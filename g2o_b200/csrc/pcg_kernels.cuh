@@ -74,6 +74,91 @@ struct PcgState {
   long long total_iterations;  // iterations of all solves since the state was reset
 };
 
+// Gauss-Jordan inverse with partial pivoting of an N x N matrix held one row
+// per lane by N consecutive lanes (g0: the group's first lane, i: this lane's
+// row): the operations of inverse_gj in the same order, with the rows in
+// registers and the pivot row and swaps by shuffles instead of serial loops
+// over a local array. Every lane of the warp takes part in the shuffles.
+template <int N>
+__device__ __forceinline__ bool inverse_gj_lanes(double (&m)[N], double (&inv)[N], int i, int g0) {
+  constexpr unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int k = 0; k < N; ++k) inv[k] = (k == i) ? 1.0 : 0.0;
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < N; ++c) {
+    // pivot: the first row r >= c with the largest |m(r, c)|
+    int p = c;
+    double best = fabs(__shfl_sync(FULL, m[c], g0 + c));
+#pragma unroll
+    for (int r = c + 1; r < N; ++r) {
+      const double v = fabs(__shfl_sync(FULL, m[c], g0 + r));
+      if (v > best) {
+        best = v;
+        p = r;
+      }
+    }
+    if (best == 0.0) ok = false;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {  // swap rows p and c
+      const double mp = __shfl_sync(FULL, m[k], g0 + p), mc = __shfl_sync(FULL, m[k], g0 + c);
+      const double ip = __shfl_sync(FULL, inv[k], g0 + p), ic = __shfl_sync(FULL, inv[k], g0 + c);
+      if (i == c) {
+        m[k] = mp;
+        inv[k] = ip;
+      } else if (i == p) {
+        m[k] = mc;
+        inv[k] = ic;
+      }
+    }
+    const double iv = 1.0 / __shfl_sync(FULL, m[c], g0 + c);
+    if (i == c) {
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        m[k] *= iv;
+        inv[k] *= iv;
+      }
+    }
+    const double f = m[c];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const double mck = __shfl_sync(FULL, m[k], g0 + c), ick = __shfl_sync(FULL, inv[k], g0 + c);
+      if (i != c) {
+        m[k] -= f * mck;
+        inv[k] -= f * ick;
+      }
+    }
+  }
+  return ok;
+}
+
+// M^-1 of 6x6 diagonal blocks, five blocks per warp (six lanes each, one
+// row per lane; lanes 30 and 31 idle): the inverses of pcg_diag_inv<Real, 6>
+// without its per-thread local arrays. Launch with nb * 32 / 5 threads or more.
+template <typename Real>
+__global__ void pcg_diag_inv6_lanes(SysDev<Real> A, double* minv, int* nonfinite) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int grp = lane / 6, i = lane - 6 * grp;
+  const int blk = gw * 5 + grp;
+  const bool act = grp < 5 && blk < A.nb;
+  double m[6], inv[6];
+  if (act) {
+    const int rb = A.rptr[blk], nblk = A.rptr[blk + 1] - rb, j = A.diag[blk] - rb;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) m[c] = (double)A.val[sys_offset<6>(rb, nblk, j, i * 6 + c)];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) m[c] = (c == i) ? 1.0 : 0.0;
+  }
+  const bool ok = inverse_gj_lanes<6>(m, inv, i, lane - i);
+  if (act) {
+    if (!ok && i == 0) *nonfinite = 1;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) minv[(size_t)blk * 36 + i * 6 + c] = inv[c];
+  }
+}
+
 // M^-1: inverse of each diagonal block (computed in FP64)
 template <typename Real, int BS>
 __global__ void pcg_diag_inv(SysDev<Real> A, double* minv, int* nonfinite) {

@@ -58,22 +58,32 @@ __global__ void sys_to_tiles(SysDev<Real> A, const int* tile_off, Real* tiles) {
 }
 
 // Block-Jacobi preconditioner read from the tiles (the Schur rows wrote the
-// system there directly): the same values as the row-SoA diagonal blocks, so
-// the same inverses as pcg_diag_inv.
+// system there directly): the same values as the row-SoA diagonal blocks and
+// the same inverses as pcg_diag_inv, five blocks per warp, one row per lane
+// (inverse_gj_lanes). Launch with nb * 32 / 5 threads or more.
 template <typename Real>
 __global__ void pcg_diag_inv_tiles(const Real* tiles, const int* tile_off, const int* diag, int nb, double* minv,
                                    int* nonfinite) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb) return;
-  const Real* T = tiles + tile_off[diag[i]];
-  double M[36], I[36];
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int grp = lane / 6, i = lane - 6 * grp;
+  const int blk = gw * 5 + grp;
+  const bool act = grp < 5 && blk < nb;
+  double m[6], inv[6];
+  if (act) {
+    const Real* T = tiles + tile_off[diag[blk]] + (size_t)i * kTileScalars;
 #pragma unroll
-  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 6; ++c) m[c] = (double)T[c];
+  } else {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) M[r * 6 + c] = (double)T[r * kTileScalars + c];
-  if (!inverse_gj<double, 6>(M, I)) *nonfinite = 1;
+    for (int c = 0; c < 6; ++c) m[c] = (c == i) ? 1.0 : 0.0;
+  }
+  const bool ok = inverse_gj_lanes<6>(m, inv, i, lane - i);
+  if (act) {
+    if (!ok && i == 0) *nonfinite = 1;
 #pragma unroll
-  for (int k = 0; k < 36; ++k) minv[(size_t)i * 36 + k] = I[k];
+    for (int c = 0; c < 6; ++c) minv[(size_t)blk * 36 + i * 6 + c] = inv[c];
+  }
 }
 
 // four consecutive entries of a tile row (16-byte aligned), kept in the
