@@ -98,6 +98,41 @@ struct PendingTiming {
 
 }  // namespace g2oc
 
+namespace g2oc {
+// page-locked host array (grown, never shrunk): the windows are packed here so
+// that their upload is one DMA copy per array
+template <typename T>
+struct PinnedVec {
+  T* p = nullptr;
+  size_t n = 0, cap = 0;
+  PinnedVec() = default;
+  PinnedVec(const PinnedVec&) = delete;
+  PinnedVec& operator=(const PinnedVec&) = delete;
+  ~PinnedVec() {
+    if (p) cudaFreeHost(p);
+  }
+  int resize(size_t m) {
+    if (m > cap) {
+      if (p) cudaFreeHost(p);
+      p = nullptr;
+      cap = 0;
+      cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), std::max<size_t>(m, 1) * sizeof(T),
+                                    cudaHostAllocDefault);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        n = 0;
+        set_error("cudaHostAlloc of %zu bytes failed: %s", m * sizeof(T), cudaGetErrorString(e));
+        return G2OC_ERR_CUDA;
+      }
+      cap = m;
+    }
+    n = m;
+    return G2OC_OK;
+  }
+  T* data() { return p; }
+};
+}  // namespace g2oc
+
 struct g2oc_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -133,10 +168,10 @@ struct g2oc_ctx {
   bool batch = false;
   int nw = 0;
   std::vector<int> win_cam_h, win_lm_h, win_pose_h, win_point_h;  // nw + 1 each
-  // host packing buffers, kept so that a re-upload does not fault in fresh pages
-  std::vector<double> pk_pose, pk_point, pk_meas, pk_info, pk_delta;
-  std::vector<uint8_t> pk_pf, pk_qf;
-  std::vector<int32_t> pk_ev;
+  // host packing buffers (page-locked), kept for re-uploads
+  g2oc::PinnedVec<double> pk_pose, pk_point, pk_meas, pk_info, pk_delta;
+  g2oc::PinnedVec<uint8_t> pk_pf, pk_qf;
+  g2oc::PinnedVec<int32_t> pk_ev;
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
   g2oc::DBuf<long long> win_mat;
   g2oc::DBuf<double> win_scratch, lam_c, lam_l;
@@ -2063,39 +2098,55 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
     edge_off[i + 1] = edge_off[i] + w[i].num_edges;
   }
   const int C = pose_off[num_windows], P = point_off[num_windows], E = edge_off[num_windows];
-  std::vector<double>&pose = c->pk_pose, &point = c->pk_point, &meas = c->pk_meas, &info = c->pk_info,
-                     &delta = c->pk_delta;
-  std::vector<uint8_t>&pf = c->pk_pf, &qf = c->pk_qf;
-  std::vector<int32_t>& ev = c->pk_ev;
-  pose.resize((size_t)C * 7);
-  point.resize((size_t)P * 3);
-  meas.resize((size_t)E * 2);
-  info.resize((size_t)E * 4);
-  delta.resize(E);
-  pf.assign(C, 0);
-  qf.assign(P, 0);
-  ev.resize((size_t)E * 2);
+  g2oc::PinnedVec<double>&pose = c->pk_pose, &point = c->pk_point, &meas = c->pk_meas, &info = c->pk_info,
+                          &delta = c->pk_delta;
+  g2oc::PinnedVec<uint8_t>&pf = c->pk_pf, &qf = c->pk_qf;
+  g2oc::PinnedVec<int32_t>& ev = c->pk_ev;
+  G2OC_TRY(pose.resize((size_t)C * 7));
+  G2OC_TRY(point.resize((size_t)P * 3));
+  G2OC_TRY(meas.resize((size_t)E * 2));
+  G2OC_TRY(info.resize((size_t)E * 4));
+  G2OC_TRY(delta.resize(E));
+  G2OC_TRY(pf.resize(C));
+  G2OC_TRY(qf.resize(P));
+  G2OC_TRY(ev.resize((size_t)E * 2));
   bool robust = false;
+  for (int i = 0; i < num_windows; ++i) robust |= w[i].robust_delta != nullptr;
+  // windows in parallel (each writes its own ranges); the first window with
+  // an out-of-range vertex index is reported
+  int bad_window = num_windows, bad_edge = 0;
+#pragma omp parallel for schedule(dynamic, 4)
   for (int i = 0; i < num_windows; ++i) {
     const g2oc_graph& g = w[i];
     memcpy(pose.data() + (size_t)pose_off[i] * 7, g.pose_estimate, (size_t)g.num_poses * 7 * sizeof(double));
     if (g.num_points)
       memcpy(point.data() + (size_t)point_off[i] * 3, g.point_estimate, (size_t)g.num_points * 3 * sizeof(double));
     if (g.pose_fixed) memcpy(pf.data() + pose_off[i], g.pose_fixed, g.num_poses);
+    else memset(pf.data() + pose_off[i], 0, g.num_poses);
     if (g.point_fixed) memcpy(qf.data() + point_off[i], g.point_fixed, g.num_points);
+    else memset(qf.data() + point_off[i], 0, g.num_points);
     memcpy(meas.data() + (size_t)edge_off[i] * 2, g.measurement, (size_t)g.num_edges * 2 * sizeof(double));
     memcpy(info.data() + (size_t)edge_off[i] * 4, g.information, (size_t)g.num_edges * 4 * sizeof(double));
+    int32_t* evw = ev.data() + 2 * (size_t)edge_off[i];
+    double* dw = delta.data() + edge_off[i];
     for (int e = 0; e < g.num_edges; ++e) {
       const int v0 = g.edge_vertex[2 * e], v1 = g.edge_vertex[2 * e + 1];
       if (v0 < 0 || v0 >= g.num_points || v1 < 0 || v1 >= g.num_poses) {
-        set_error("window %d edge %d: vertex index out of range", i, e);
-        return G2OC_ERR_BAD_GRAPH;
+#pragma omp critical(g2oc_bad_window)
+        if (i < bad_window) {
+          bad_window = i;
+          bad_edge = e;
+        }
+        break;
       }
-      ev[2 * ((size_t)edge_off[i] + e)] = v0 + point_off[i];
-      ev[2 * ((size_t)edge_off[i] + e) + 1] = v1 + pose_off[i];
-      delta[edge_off[i] + e] = g.robust_delta ? g.robust_delta[e] : 0.0;
+      evw[2 * e] = v0 + point_off[i];
+      evw[2 * e + 1] = v1 + pose_off[i];
+      dw[e] = g.robust_delta ? g.robust_delta[e] : 0.0;
     }
-    robust |= g.robust_delta != nullptr;
+  }
+  if (bad_window < num_windows) {
+    set_error("window %d edge %d: vertex index out of range", bad_window, bad_edge);
+    return G2OC_ERR_BAD_GRAPH;
   }
   g2oc_graph packed;
   memset(&packed, 0, sizeof(packed));
