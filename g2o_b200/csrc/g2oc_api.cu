@@ -172,6 +172,11 @@ struct g2oc_ctx {
   g2oc::PinnedVec<double> pk_pose, pk_point, pk_meas, pk_info, pk_delta;
   g2oc::PinnedVec<uint8_t> pk_pf, pk_qf;
   g2oc::PinnedVec<int32_t> pk_ev;
+  // the LM / PCG state read once per trial: page-locked, so the copy is a DMA
+  // the host can poll for
+  g2oc::PinnedVec<g2oc::DevScalars> h_sc;
+  g2oc::PinnedVec<g2oc::PcgState> h_pcg;
+  cudaEvent_t ev_read = nullptr;
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
   g2oc::DBuf<long long> win_mat;
   g2oc::DBuf<double> win_scratch, lam_c, lam_l;
@@ -272,6 +277,7 @@ struct g2oc_ctx {
     pending.clear();
   }
   ~g2oc_ctx() {
+    if (ev_read) cudaEventDestroy(ev_read);
     if (win_graph) cudaGraphExecDestroy(win_graph);
     eng.reset();
     chol.reset();
@@ -1151,10 +1157,23 @@ static int reset_pcg(g2oc_ctx* c);
 // DevScalars and PcgState after the queued work (the one wait of an LM
 // trial): PCG iterations since the last read go to stv
 static int read_state(g2oc_ctx* c, DevScalars* h, g2oc_iteration_stats* stv) {
-  PcgState ps;
-  G2OC_CUDA_TRY(cudaMemcpyAsync(h, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
-  G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
-  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (!c->ev_read) {
+    G2OC_TRY(c->h_sc.resize(1));
+    G2OC_TRY(c->h_pcg.resize(1));
+    G2OC_CUDA_TRY(cudaEventCreateWithFlags(&c->ev_read, cudaEventDisableTiming));
+  }
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->h_sc.data(), c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->h_pcg.data(), c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaEventRecord(c->ev_read, c->stream));
+  // the host polls (the trial's work is a few hundred microseconds at most;
+  // a blocking wait would add its wake-up latency to every trial)
+  cudaError_t q;
+  while ((q = cudaEventQuery(c->ev_read)) == cudaErrorNotReady) {
+  }
+  G2OC_CUDA_TRY(q);
+  cudaGetLastError();  // the not-ready answers are not errors of later launches
+  *h = *c->h_sc.data();
+  const PcgState ps = *c->h_pcg.data();
   if (ps.sync_error) {
     G2OC_TRY(reset_pcg(c));
     set_error("PCG: a grid barrier wait ran out");
