@@ -142,3 +142,11 @@ def test_windows_with_sparse_reduced_system(backend, oracle_lib, small_windows):
         assert st[w]["iterations"] == len(so)
         assert st[w]["trials"] == sum(x["levenberg_iterations"] for x in so), w
         assert abs(st[w]["chi2"] - so[-1]["chi2"]) <= 1e-8 * so[-1]["chi2"], (w, st[w]["chi2"], so[-1]["chi2"])
+
+
+def test_window_too_large_for_the_dense_solve_is_rejected(backend):
+    """A window whose reduced camera system does not fit the dense solve's
+    shared memory is refused at upload with NOT_SUPPORTED, not run."""
+    big = synth.bundle_adjustment(num_cameras=150, num_points=400, min_obs=2, max_obs=4, seed=9)
+    with pytest.raises(Exception, match="dense window solve"):
+        backend.CudaWindows([big])
