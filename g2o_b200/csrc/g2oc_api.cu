@@ -69,7 +69,9 @@ struct EngineBase {
   virtual int schur_export(double lambda, double* S, double* bs) = 0;
   // Gauss-Newton solve H x = rhs (lambda 0) with a given device right-hand
   // side in Hessian order, through the same Schur + PCG / Cholesky path (BA)
-  virtual int solve_rhs(const double* rhs, double* out) = 0;
+  // reuse_schur: the Schur complement of the last call still stands (same
+  // linearization, lambda 0); only the reduced right-hand side is formed
+  virtual int solve_rhs(const double* rhs, double* out, bool reuse_schur = false) = 0;
   // batched windows: per-window lambda initialisation, and the trial's solve
   // (Schur with per-vertex damping, dense Cholesky per window, back-substitution)
   virtual int batch_lambda_init(double user_lambda, double tau) = 0;
@@ -164,6 +166,7 @@ struct g2oc_ctx {
   // FP64 vectors
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
   g2oc::DBuf<double> adj_g, adj_v, adj_r, adj_dv, adj_p, adj_q, adj_rold, adj_dmeas, adj_dlogw;  // adjoint
+  bool adj_schur_ready = false;  // the preconditioner's H and Schur complement of this backward call are built
   // batched windows (g2oc_upload_windows): packed into one graph
   bool batch = false;
   int nw = 0;
@@ -1062,7 +1065,7 @@ struct Engine final : EngineBase {
     return backsub(c->b.p + (size_t)S.Cf * 6, c->xs.p, c->x.p + (size_t)S.Cf * 6);
   }
 
-  int solve_rhs(const double* rhs, double* out) override {
+  int solve_rhs(const double* rhs, double* out, bool reuse_schur = false) override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (!(S.ba && S.schur) || S.Cf == 0) {
@@ -1070,7 +1073,7 @@ struct Engine final : EngineBase {
       return G2OC_ERR_NOT_SUPPORTED;
     }
     const bool use_chol = c->prm.linear_solver == G2OC_LINEAR_CHOLESKY;
-    G2OC_TRY(schur(0.0, nullptr, nullptr, nullptr, !use_chol && tile_pcg_used()));
+    if (!reuse_schur) G2OC_TRY(schur(0.0, nullptr, nullptr, nullptr, !use_chol && tile_pcg_used()));
     const double* rp = rhs;
     const double* rl = rhs + (size_t)S.Cf * 6;
     G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
@@ -1970,10 +1973,16 @@ static int adj_hessian_product(g2oc_ctx* c, const double* p, double* q) {
   return G2OC_OK;
 }
 
-// preconditioner: the Gauss-Newton Schur solve at x*
+// preconditioner: the Gauss-Newton Schur solve at x*. The Gauss-Newton
+// system is the same for every application within one
+// backward call (same estimates, lambda 0): H and its Schur complement are
+// built on the first, the later ones form the reduced right-hand side only.
 static int adj_precondition(g2oc_ctx* c, const double* r, double* z) {
+  if (c->adj_schur_ready) return c->eng->solve_rhs(r, z, true);
   G2OC_TRY(c->eng->build_system());
-  return c->eng->solve_rhs(r, z);
+  G2OC_TRY(c->eng->solve_rhs(r, z, false));
+  c->adj_schur_ready = true;
+  return G2OC_OK;
 }
 
 int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL_dlogw, g2oc_backward_stats* stats) {
@@ -2012,6 +2021,7 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
   int steps = 0;
   double rel = gg > 0.0 ? 1.0 : 0.0;
   G2OC_TRY(reset_pcg(c));
+  c->adj_schur_ready = false;
   if (gg > 0.0) {
     G2OC_TRY(adj_precondition(c, c->adj_r.p, c->adj_dv.p));  // z
     G2OC_CUDA_TRY(cudaMemcpyAsync(c->adj_p.p, c->adj_dv.p, nb, cudaMemcpyDeviceToDevice, st));
