@@ -163,8 +163,9 @@ inline size_t win_chol_smem(int nmax) {
 //     (lane i = row i; L_jk broadcast by shuffles, no CTA barrier per column);
 //   - every thread solves one panel row against the diagonal block (the
 //     right-hand-side row gives y = L^-1 b on the way);
-//   - the trailing lower triangle takes the panel's update in 4 x 4 register
-//     tiles, each tile's 16 entries loaded before its products.
+//   - the trailing lower triangle takes the panel's update in 16 x 16 tiles,
+//     one warp each, as FP64 tensor-core products (mma.sync m8n8k4) fed from
+//     the column-major panel.
 // Then x = L^-T y backwards by blocks of kWinNB: the sums over the rows below
 // a block in kWinGroups fixed row groups, the block's triangle on warp 0.
 // Every sum runs in an order fixed by n alone (not by the CTA size). The
@@ -265,14 +266,17 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
       const int i = t / kWinNB, k = t % kWinNB;
       if (k < pb && k <= i) M[(size_t)(p0 + i) * n + p0 + k] = PT[k * ldt + i];
     }
-    // trailing update: rows pb..m-1 (local), columns pb..m-2, lower part;
-    // 4 x 4 tiles (a, b), b <= a, numbered row-block by row-block
+    // trailing update: rows pb..m-1 (local), columns pb..m-2, lower part, in
+    // 16 x 16 tiles (a, b), b <= a, numbered row-block by row-block, one warp
+    // per tile: 2 x 2 FP64 tensor-core products (mma m8n8k4) per 4 columns of
+    // the panel, operands straight from the column-major panel
     const int nc = m - 1 - pb;
     if (nc > 0) {
-      const int nbc = (nc + 3) / 4, nbr = (m - pb + 3) / 4;
+      const int nbc = (nc + 15) / 16, nbr = (m - pb + 15) / 16;
       const int tri = nbc * (nbc + 1) / 2;
       const int ntile = tri + (nbr > nbc ? nbc : 0);  // the last row block holds the right-hand side row only
-      for (int t = tid; t < ntile; t += THREADS) {
+      const int gi = lane >> 2, ti = lane & 3;
+      for (int t = warp; t < ntile; t += WARPS) {
         int a, b;
         if (t < tri) {
           a = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
@@ -283,38 +287,37 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) win_chol_solve(const i
           a = nbc;
           b = t - tri;
         }
-        const int i0 = pb + 4 * a, j0 = pb + 4 * b;
-        double cv[4][4];
+        const int i0 = pb + 16 * a, j0 = pb + 16 * b;
+        double acc[2][2][2];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int u = 0; u < 2; ++u)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int i = i0 + r, j = j0 + q;
-            cv[r][q] = (i < m && j <= m - 2 && j <= i) ? M[(size_t)(p0 + i) * n + p0 + j] : 0.0;
-          }
-        double acc[4][4];
+          for (int v = 0; v < 2; ++v) acc[u][v][0] = acc[u][v][1] = 0.0;
+        for (int k0 = 0; k0 < pb; k0 += 4) {
+          const double* col = PT + (k0 + ti) * ldt;
+          const double fa0 = col[i0 + gi], fa1 = col[i0 + 8 + gi];
+          const double fb0 = col[j0 + gi], fb1 = col[j0 + 8 + gi];
+          const double fa[2] = {fa0, fa1}, fb[2] = {fb0, fb1};
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+          for (int u = 0; u < 2; ++u)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
-        for (int k = 0; k < pb; ++k) {
-          const double2 u0 = *reinterpret_cast<const double2*>(PT + k * ldt + i0);
-          const double2 u1 = *reinterpret_cast<const double2*>(PT + k * ldt + i0 + 2);
-          const double2 v0 = *reinterpret_cast<const double2*>(PT + k * ldt + j0);
-          const double2 v1 = *reinterpret_cast<const double2*>(PT + k * ldt + j0 + 2);
-          const double li[4] = {u0.x, u0.y, u1.x, u1.y}, lj[4] = {v0.x, v0.y, v1.x, v1.y};
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[r][q] += li[r] * lj[q];
+            for (int v = 0; v < 2; ++v)
+              asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                           : "+d"(acc[u][v][0]), "+d"(acc[u][v][1])
+                           : "d"(fa[u]), "d"(fb[v]));
         }
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int u = 0; u < 2; ++u)
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int i = i0 + r, j = j0 + q;
-            if (i < m && j <= m - 2 && j <= i) M[(size_t)(p0 + i) * n + p0 + j] = cv[r][q] - acc[r][q];
-          }
+          for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int i = i0 + 8 * u + gi, j = j0 + 8 * v + 2 * ti + e;
+              if (i < m && j <= m - 2 && j <= i) {
+                double* pm = M + (size_t)(p0 + i) * n + p0 + j;
+                *pm = *pm - acc[u][v][e];
+              }
+            }
       }
     }
     __syncthreads();
