@@ -39,6 +39,12 @@ class G2ocError(RuntimeError):
         self.status = status
 
 
+# g2oc_allreduce_fn: (user, device_ptr, count, dtype, op, stream) -> status
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p)
+RED_SUM, RED_MAX = 0, 1
+DT_F32, DT_F64 = 0, 1
+
+
 def library() -> C.CDLL:
     """Load libg2o_b200.so (raises if it has not been built)."""
     global _LIB
@@ -82,6 +88,7 @@ def library() -> C.CDLL:
         "g2oc_get_kernel_stats": ([vp, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)], C.c_int),
         "g2oc_solve_block_system_static": ([C.c_int, C.c_int32, C.c_int32, C.c_int32, ip, dp, dp, dp, C.c_double,
                                             C.c_int32, ip], C.c_int),
+        "g2oc_set_sharding": ([vp, C.c_int32, C.c_int32, ALLREDUCE_FN, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -142,12 +149,31 @@ class OptimizationAlgorithmFactory:
 class CudaProblem:
     """One device context holding one graph: the C-ABI handle."""
 
-    def __init__(self, graph: Graph, params: Optional[G2ocParams] = None, device: int = 0):
+    def __init__(self, graph: Graph, params: Optional[G2ocParams] = None, device: int = 0, shard=None):
+        """shard = (rank, world, allreduce): this rank's part of a sharded
+        bundle adjustment (g2oc_set_sharding); allreduce(ptr, count, dtype, op,
+        stream) combines count elements at the device address ptr across the
+        ranks in place, ordered on the CUDA stream `stream`."""
         self.graph = graph
         self._h = C.c_void_p()
         _check(library().g2oc_create(device, C.byref(self._h)))
         self.params = params or default_params()
         _check(library().g2oc_set_params(self._h, C.byref(self.params)))
+        self._reduce_cb = None
+        if shard is not None:
+            rank, world, fn = shard
+
+            def cb(user, ptr, count, dtype, op, stream):
+                try:
+                    fn(ptr, int(count), int(dtype), int(op), stream or 0)
+                    return 0
+                except Exception:  # reported to the C side as a failed all-reduce
+                    import traceback
+                    traceback.print_exc()
+                    return 1
+
+            self._reduce_cb = ALLREDUCE_FN(cb)  # kept alive with the context
+            _check(library().g2oc_set_sharding(self._h, rank, world, self._reduce_cb, None))
         self._cg = graph.to_c()
         _check(library().g2oc_upload(self._h, C.byref(self._cg)))
         self.info = G2ocHessianInfo()
@@ -302,6 +328,45 @@ class CudaProblem:
         it = C.c_int32()
         st = library().g2oc_solve(self._h, lam, _p(x), C.byref(it))
         return st, x, it.value
+
+
+def device_tensor(ptr: int, count: int, dtype: int, device: int = 0):
+    """A torch tensor viewing count FP32/FP64 elements at a device address
+    (the buffers g2oc_allreduce_fn is given); no copy."""
+    import torch
+
+    class _View:
+        pass
+
+    v = _View()
+    v.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f4" if dtype == DT_F32 else "<f8",
+                                  "data": (int(ptr), False), "version": 3, "strides": None, "stream": None}
+    return torch.as_tensor(v, device=f"cuda:{device}")
+
+
+def split_points(g: Graph, parts: int):
+    """The shards of a bundle adjustment: every camera, and the points with
+    their edges cut into `parts` contiguous ranges of point index. Returns the
+    sub-graphs and, per part, the original indices of its points."""
+    bounds = [round(i * g.num_points / parts) for i in range(parts + 1)]
+    out = []
+    for r in range(parts):
+        p0, p1 = bounds[r], bounds[r + 1]
+        sel = (g.edge_vertex[:, 0] >= p0) & (g.edge_vertex[:, 0] < p1)
+        ev = g.edge_vertex[sel].copy()
+        ev[:, 0] -= p0
+
+        def pick(a, rows=None):
+            if a is None:
+                return None
+            return a[sel].copy() if rows is None else a[rows].copy()
+
+        sub = Graph(g.pose_type, g.edge_type, g.pose_estimate.copy(), ev, pick(g.measurement), pick(g.information),
+                    None if g.pose_fixed is None else g.pose_fixed.copy(), g.point_estimate[p0:p1].copy(),
+                    None if g.point_fixed is None else g.point_fixed[p0:p1].copy(), pick(g.robust_delta),
+                    g.focal_length, tuple(g.principal_point), f"{g.name}-shard{r}", {})
+        out.append((sub, np.arange(p0, p1)))
+    return out
 
 
 class CudaWindows:

@@ -961,6 +961,32 @@ static __global__ void ba_oplus(BAVertices V, int Cf, int Pf, const double* x, i
 
 // max |diag| over Hpp and H_ll (computeLambdaInit,
 // optimization_algorithm_levenberg.cpp:155-167): partial maxima per block
+// sharded bundle adjustment: the diagonal of this rank's part of Hpp
+template <typename Real>
+__global__ void ba_hpp_diag(const Real* hpp, int Cf, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < Cf * 6) out[t] = (double)hpp[(size_t)(t / 6) * 36 + (t % 6) * 7];
+}
+
+// max |diag H| from the summed Hpp diagonal (all ranks) and this rank's Hll
+template <typename Real>
+__global__ void ba_max_diag_summed(const double* pdiag, int Cf, const Real* hll, int Pf, double* partials) {
+  double m = 0.0;
+  const int n = Cf * 6 + Pf * 3;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double v;
+    if (t < Cf * 6) {
+      v = fabs(pdiag[t]);
+    } else {
+      const int l = (t - Cf * 6) / 3, d = (t - Cf * 6) % 3;
+      const int idx = d == 0 ? 0 : d == 1 ? 3 : 5;
+      v = fabs((double)hll[(size_t)l * 6 + idx]);
+    }
+    m = fmax(m, v);
+  }
+  block_max(m, partials + blockIdx.x);
+}
+
 template <typename Real>
 __global__ void ba_max_diag(const Real* hpp, int Cf, const Real* hll, int Pf, double* partials) {
   double m = 0.0;

@@ -167,6 +167,11 @@ struct g2oc_ctx {
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
   g2oc::DBuf<double> adj_g, adj_v, adj_r, adj_dv, adj_p, adj_q, adj_rold, adj_dmeas, adj_dlogw;  // adjoint
   bool adj_schur_ready = false;  // the preconditioner's H and Schur complement of this backward call are built
+  // sharded bundle adjustment (g2oc_set_sharding)
+  int shard_rank = 0, shard_world = 1;
+  g2oc_allreduce_fn shard_fn = nullptr;
+  void* shard_user = nullptr;
+  g2oc::DBuf<double> shard_diag;  // the summed Hpp diagonal for the initial lambda
   // batched windows (g2oc_upload_windows): packed into one graph
   bool batch = false;
   int nw = 0;
@@ -511,6 +516,18 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
   return G2OC_OK;
 }
 
+// sharded bundle adjustment: combine count elements across the ranks in place
+// through the caller's all-reduce (a no-op for one rank)
+static int shard_reduce(g2oc_ctx* c, void* p, long long count, int dtype, int op) {
+  if (c->shard_world <= 1) return G2OC_OK;
+  const int rc = c->shard_fn(c->shard_user, p, (int64_t)count, dtype, op, (void*)c->stream);
+  if (rc != 0) {
+    set_error("sharded bundle adjustment: the all-reduce returned %d", rc);
+    return G2OC_ERR_STATE;
+  }
+  return G2OC_OK;
+}
+
 static int finalize_sum(g2oc_ctx* c, int nparts, int stride, double* out0, double* out1, double add0 = 0.0) {
   G2OC_K(K_REDUCE) finalize_sum_kernel<<<1, 256, 0, c->stream>>>(c->partials.p, nparts, stride, out0, out1, add0);
   G2OC_LAUNCH_CHECK();
@@ -655,13 +672,23 @@ struct Engine final : EngineBase {
   int max_diag() override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    if (S.ba) G2OC_K(K_MAX_DIAG) ba_max_diag<Real><<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
+    if (S.ba && c->shard_world > 1) {
+      // the lambda of LM iteration 0 takes max |diag H| of the summed Hpp
+      G2OC_TRY(c->shard_diag.alloc((size_t)S.Cf * 6 + 1));
+      G2OC_K(K_MAX_DIAG) ba_hpp_diag<Real><<<cdiv(S.Cf * 6, 256), 256, 0, st>>>(hpp.p, S.Cf, c->shard_diag.p);
+      G2OC_LAUNCH_CHECK();
+      G2OC_TRY(shard_reduce(c, c->shard_diag.p, (long long)S.Cf * 6, G2OC_DT_F64, G2OC_RED_SUM));
+      G2OC_K(K_MAX_DIAG) ba_max_diag_summed<Real><<<kRedBlocks, 256, 0, st>>>(c->shard_diag.p, S.Cf, hll.p, S.Pf,
+                                                                              c->partials.p);
+    } else if (S.ba) {
+      G2OC_K(K_MAX_DIAG) ba_max_diag<Real><<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
+    }
     else if (S.pd == 3) G2OC_K(K_MAX_DIAG) pg_max_diag<Real, 3><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
     else G2OC_K(K_MAX_DIAG) pg_max_diag<Real, 6><<<kRedBlocks, 256, 0, st>>>(hpp.p, c->sys_diag.p, S.Cf, c->partials.p);
     G2OC_LAUNCH_CHECK();
     G2OC_K(K_REDUCE) finalize_max_kernel<<<1, 256, 0, st>>>(c->partials.p, kRedBlocks, &c->sc.p->max_diag);
     G2OC_LAUNCH_CHECK();
-    return G2OC_OK;
+    return shard_reduce(c, &c->sc.p->max_diag, 1, G2OC_DT_F64, G2OC_RED_MAX);
   }
 
   // S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T (internal row order) and,
@@ -685,6 +712,9 @@ struct Engine final : EngineBase {
     if (S.Cf == 0) return G2OC_OK;
     const double* bp = c->b.p;
     const double* bl = c->b.p + (size_t)S.Cf * 6;
+    // sharded: the camera diagonal's lambda is added by rank 0 only (the
+    // ranks' rows are summed); the landmarks' above is every rank's own
+    lambda = (c->shard_world > 1 && c->shard_rank != 0) ? 0.0 : lambda;
     for (int gi = 0; gi < 3; ++gi) {
       if (row_n[gi] == 0) continue;
       const int* rows = row_list[gi].p;
@@ -820,7 +850,20 @@ struct Engine final : EngineBase {
       }
     } else if (S.ba && S.schur) {
       cudaEvent_t ts = c->cur_stats ? c->mark() : nullptr;
-      G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, !use_chol && tile_pcg_used()));
+      if (c->shard_world > 1) {
+        // every rank forms its landmarks' part of S and b_schur (its Hpp and
+        // b_p parts included; the cameras' lambda on rank 0 only, the
+        // landmarks' on every rank) into zeroed tiles, then the ranks sum
+        // them: all hold the same reduced system
+        G2OC_TRY(ensure_tiles());
+        G2OC_CUDA_TRY(cudaMemsetAsync(tiles.p, 0, tiles.bytes(), st));
+        G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, true));
+        G2OC_TRY(shard_reduce(c, tiles.p, (long long)tiles.n, sizeof(Real) == 4 ? G2OC_DT_F32 : G2OC_DT_F64,
+                              G2OC_RED_SUM));
+        G2OC_TRY(shard_reduce(c, c->rhs.p, (long long)S.Cf * 6, G2OC_DT_F64, G2OC_RED_SUM));
+      } else {
+        G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, !use_chol && tile_pcg_used()));
+      }
       const double* bp = c->b.p;
       const double* bl = c->b.p + (size_t)S.Cf * 6;
       if (ts) c->span(ts, &c->cur_stats->time_schur_complement, &c->cur_stats->time_linear_solver);
@@ -1125,7 +1168,9 @@ static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
     G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   else G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   G2OC_LAUNCH_CHECK();
-  return finalize_sum(c, S.ba ? kChi2Blocks : kRedBlocks, 2, out_plain, out_robust);
+  G2OC_TRY(finalize_sum(c, S.ba ? kChi2Blocks : kRedBlocks, 2, out_plain, out_robust));
+  G2OC_TRY(shard_reduce(c, out_plain, 1, G2OC_DT_F64, G2OC_RED_SUM));
+  return shard_reduce(c, out_robust, 1, G2OC_DT_F64, G2OC_RED_SUM);
 }
 
 static int oplus(g2oc_ctx* c) {
@@ -1223,9 +1268,17 @@ static int lm_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
     G2OC_TRY(oplus(c));
     c->span(t0, &stv->time_update);
     G2OC_TRY(chi2_to(c, &sc->chi2_temp_plain, &sc->chi2_temp));
-    G2OC_K(K_LM_CONTROL) lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p);
-    G2OC_LAUNCH_CHECK();
-    G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &sc->scale, nullptr, 1e-3));
+    {
+      // sharded: the camera entries are the same on every rank, their lambda
+      // term (and the 1e-3) counted on rank 0 only; b's camera part is each
+      // rank's share
+      const bool other = c->shard_world > 1 && c->shard_rank != 0;
+      G2OC_K(K_LM_CONTROL) lm_scale_partials<<<kRedBlocks, 256, 0, st>>>(c->x.p, c->b.p, n, sc, c->partials.p,
+                                                                         other ? c->S.Cf * 6 : 0);
+      G2OC_LAUNCH_CHECK();
+      G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &sc->scale, nullptr, other ? 0.0 : 1e-3));
+      G2OC_TRY(shard_reduce(c, &sc->scale, 1, G2OC_DT_F64, G2OC_RED_SUM));
+    }
     G2OC_K(K_LM_CONTROL) lm_decide<<<1, 32, 0, st>>>(sc);
     G2OC_LAUNCH_CHECK();
     G2OC_TRY(read_state(c, &h, stv));
@@ -1507,6 +1560,7 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
   c->chol.reset();
   Structure& S = c->S;
   S = Structure();
+  S.shard_world = c->shard_world;
   G2OC_TRY(build_structure(g, S));
   cudaStream_t st = c->stream;
   const int na = (int)S.act.size();
@@ -1787,12 +1841,44 @@ int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
   return G2OC_OK;
 }
 
+static int check_sharding(g2oc_ctx* c) {
+  if (c->shard_world <= 1) return G2OC_OK;
+  const Structure& S = c->S;
+  if (!S.ba || !S.schur || !S.tile_ok || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY || pcg_mode() != PCG_AUTO ||
+      (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0)) {
+    set_error("sharded mode runs bundle adjustments with >= %d free cameras and landmarks, the PCG solver, FP64 or "
+              "mixed precision without FP64 refinement",
+              2 * kTileBlocks);
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  return G2OC_OK;
+}
+
+int g2oc_set_sharding(g2oc_ctx* c, int32_t rank, int32_t world, g2oc_allreduce_fn allreduce, void* user) {
+  G2OC_TRY(check_ctx(c, false));
+  if (world < 1 || rank < 0 || rank >= world || (world > 1 && !allreduce)) {
+    set_error("sharding: rank %d of %d (an all-reduce is needed for more than one rank)", rank, world);
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (c->uploaded || c->batch) {
+    set_error("g2oc_set_sharding comes before g2oc_upload");
+    return G2OC_ERR_STATE;
+  }
+  c->shard_rank = rank;
+  c->shard_world = world;
+  c->shard_fn = allreduce;
+  c->shard_user = user;
+  c->topo.valid = false;  // the next upload builds the structure for this world size
+  return G2OC_OK;
+}
+
 int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int* done) {
   G2OC_TRY(check_ctx(c, true));
   if (iterations < 0) {
     set_error("iterations < 0");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
+  G2OC_TRY(check_sharding(c));
   G2OC_TRY(reset_pcg(c));  // LinearSolverPCG::init via BlockSolver::init
   int result = G2OC_RESULT_OK;
   int it = 0;
@@ -1987,6 +2073,10 @@ static int adj_precondition(g2oc_ctx* c, const double* r, double* z) {
 
 int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL_dlogw, g2oc_backward_stats* stats) {
   G2OC_TRY(check_ctx(c, true));
+  if (c->shard_world > 1) {
+    set_error("g2oc_backward runs on one rank (no sharding)");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
   if (!dL_dx || !dL_dmeas || !dL_dlogw) {
     set_error("dL_dx, dL_dmeas and dL_dlogw must be given");
     return G2OC_ERR_INVALID_ARGUMENT;
@@ -2098,6 +2188,10 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
 // ------------------------------------------------------- batched windows
 int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   G2OC_TRY(check_ctx(c, false));
+  if (c->shard_world > 1) {
+    set_error("batched windows shard by window (one context per rank), not by landmark");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
   if (num_windows <= 0 || !w) {
     set_error("num_windows must be positive and windows non-NULL");
     return G2OC_ERR_INVALID_ARGUMENT;

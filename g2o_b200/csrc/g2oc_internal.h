@@ -130,6 +130,11 @@ struct Structure {
   // dense tiles (6x6 blocks only): kTileBlocks x kTileBlocks blocks each,
   // stored scalar-row-major (96 x 96), upper tiles only, diagonal tiles full
   bool tile_ok = false;
+  // ranks of a sharded bundle adjustment (> 1: every non-fixed camera is
+  // free whether or not this rank has edges on it, and the tiles cover the
+  // whole upper triangle, so every rank has the same Hessian order and the
+  // same tile layout)
+  int shard_world = 1;
   std::vector<int> tile_ij;             // 2 per tile: tile row I, tile column J (I <= J)
   std::vector<int> tile_off;            // per internal block: offset of its (0,0) entry in the tile array
 };

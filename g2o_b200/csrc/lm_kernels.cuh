@@ -50,11 +50,15 @@ static __global__ void set_solve_ok(DevScalars* sc, int ok) {
 }
 
 // partial sums of x (lambda x + b) (computeScale)
-static __global__ void lm_scale_partials(const double* x, const double* b, int n, const DevScalars* sc, double* partials) {
+// lam_from: first entry the lambda term applies to (0; a sharded bundle
+// adjustment's ranks other than 0 leave the replicated camera entries' term
+// to rank 0)
+static __global__ void lm_scale_partials(const double* x, const double* b, int n, const DevScalars* sc, double* partials,
+                                         int lam_from = 0) {
   const double lambda = sc->lambda;
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    s += x[i] * (lambda * x[i] + b[i]);
+    s += x[i] * ((i >= lam_from ? lambda : 0.0) * x[i] + b[i]);
   s = block_sum1(s);
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }

@@ -82,12 +82,16 @@ static void build_tiles(int nb, Structure& s) {
     const int I = s.sys_brow[k] / kTileBlocks, J = s.sys_rcol[k] / kTileBlocks;
     id[(size_t)I * nbt + J] = 0;
   }
+  if (s.shard_world > 1)  // every rank: the whole upper triangle
+    for (int I = 0; I < nbt; ++I)
+      for (int J = I; J < nbt; ++J) id[(size_t)I * nbt + J] = 0;
   int nt = 0;
   for (size_t q = 0; q < id.size(); ++q)
     if (id[q] == 0) id[q] = nt++;
   const double stored = (double)nt * kTileBlocks * kTileBlocks;
   const double allowed = 1.25 * nnzb + (double)nbt * kTileBlocks * kTileBlocks / 2;
-  if (stored > allowed || (long long)nt * kTileBlocks * kTileBlocks * 36 >= (1LL << 31)) return;
+  if ((long long)nt * kTileBlocks * kTileBlocks * 36 >= (1LL << 31)) return;
+  if (stored > allowed && s.shard_world <= 1) return;
   s.tile_ok = true;
   s.tile_ij.resize(2 * (size_t)nt);
   for (int I = 0; I < nbt; ++I)
@@ -171,6 +175,7 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
   s.point_l.assign(P, -1);
   s.free_pose_of_h.clear();
   s.free_point_of_l.clear();
+  if (s.shard_world > 1) std::fill(pa.begin(), pa.end(), (char)1);
   for (int i = 0; i < C; ++i)
     if (pa[i] && !(pf && pf[i])) {
       s.pose_h[i] = (int)s.free_pose_of_h.size();

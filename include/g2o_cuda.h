@@ -255,6 +255,31 @@ int g2oc_get_kernel_stats(g2oc_ctx* ctx, g2oc_kernel_stat* out, int capacity, in
 int g2oc_backward(g2oc_ctx* ctx, const double* dL_dx, double* dL_dmeas, double* dL_dlogw,
                   g2oc_backward_stats* stats);
 
+/* ---- sharded bundle adjustment (one process per GPU)
+ * Each rank uploads every camera and its own share of the points with their
+ * edges; per LM trial the ranks sum their parts of the reduced camera system
+ * (the Schur complement and its right-hand side, in the dense-tile layout),
+ * of chi2 and of the gain-ratio scale through the caller's all-reduce, and
+ * then take identical steps: the reduced solve is replicated, the landmark
+ * back-substitution and updates stay local. The scheme of
+ * BlockSolver::solve (g2o/core/block_solver.hpp:331-477) with the sum over
+ * landmarks split across ranks; g2o has no distributed counterpart.
+ * allreduce(user, device_ptr, count, dtype, op, stream) must combine count
+ * elements at device_ptr across all ranks in place (G2OC_RED_SUM or
+ * G2OC_RED_MAX; G2OC_DT_F32 or G2OC_DT_F64), ordered after the work already
+ * on `stream` (the context's CUDA stream) and before the work enqueued on it
+ * after the call returns; it returns 0 on success. Every rank calls it at
+ * the same points in the same order. Call before g2oc_upload; supported for
+ * EdgeProjectXYZ2UV graphs with at least 32 free cameras, the PCG linear
+ * solver, FP64 or mixed precision without FP64 refinement
+ * (refine_max_iterations = -1). world = 1 switches it off. */
+#define G2OC_RED_SUM 0
+#define G2OC_RED_MAX 1
+#define G2OC_DT_F32 0
+#define G2OC_DT_F64 1
+typedef int (*g2oc_allreduce_fn)(void* user, void* device_ptr, int64_t count, int32_t dtype, int32_t op, void* stream);
+int g2oc_set_sharding(g2oc_ctx* ctx, int32_t rank, int32_t world, g2oc_allreduce_fn allreduce, void* user);
+
 /* Batched windows (no counterpart in the reference, where each window would be
    its own SparseOptimizer): many independent bundle adjustments
    (VertexSE3Expmap + VertexPointXYZ + EdgeProjectXYZ2UV, same camera
