@@ -54,9 +54,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-iterations", type=int, default=1)
-    ap.add_argument("--config", default="ba", choices=["ba", "windows", "adjoint"],
-                    help="ba: the 1000-camera bundle adjustment (default); windows: 512 batched local BA windows; "
-                         "adjoint: implicit-function-theorem gradients through the converged 200-camera BA")
+    ap.add_argument("--config", default="ba", choices=["ba", "ba_sharded", "windows", "adjoint"],
+                    help="ba: the 1000-camera bundle adjustment (default; one replica per GPU); ba_sharded: the same "
+                         "bundle adjustment split by points over the GPUs (NCCL all-reduce of the reduced camera "
+                         "system per LM trial); windows: 512 batched local BA windows; adjoint: "
+                         "implicit-function-theorem gradients through the converged 200-camera BA")
     return ap.parse_args()
 
 
@@ -342,6 +344,100 @@ def run_windows(args):
                 "d2h_bytes_per_step": int(d2h), "upload": "same topology each step: values copied, structure kept",
                 "new_topology_upload_s": upload_s},
         "cpu_baseline": cpu,
+    }), flush=True)
+
+
+def nccl_reducer(device):
+    """g2oc_allreduce_fn over torch.distributed (NCCL): the context's buffer
+    viewed as a tensor, reduced on the context's stream."""
+    import torch
+    import torch.distributed as dist
+    from g2o_b200 import backend
+
+    def fn(ptr, count, dtype, op, stream):
+        t = backend.device_tensor(ptr, count, dtype, device)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream, device=device)):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM if op == backend.RED_SUM else dist.ReduceOp.MAX)
+
+    return fn
+
+
+def run_ba_sharded(args):
+    """The 1000-camera BA split by points over the ranks (strong scaling: one
+    problem): every rank holds all cameras and 1/N of the points and edges;
+    per LM trial the ranks sum the reduced camera system, b_schur, chi2 and
+    the gain-ratio scale with NCCL and take the same step. value = the LM
+    iterations of the one problem / the slowest rank's device time."""
+    rank, world, local = dist_info()
+    import torch
+    from g2o_b200 import backend
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    g = build_graph()
+    sub = backend.split_points(g, world)[rank][0] if world > 1 else g
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    shard = (rank, world, nccl_reducer(local)) if world > 1 else None
+    prob = backend.CudaProblem(sub, fac.construct("lm_cuda_mixed_fast"), device=local, shard=shard)
+    stream = torch.cuda.ExternalStream(prob.stream(), device=local)
+    for _ in range(max(args.warmup, 1)):
+        prob.restore_initial_estimates()
+        prob.optimize(ITERATIONS)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local)
+    launches0, _ = prob.kernel_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    iters = 0
+    chi2 = None
+    for _ in range(args.steps):
+        prob.restore_initial_estimates()
+        _, st = prob.optimize(ITERATIONS)
+        iters += len(st)
+        chi2 = st[-1]["chi2"]
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    launches1, _ = prob.kernel_stats()
+    ms = e0.elapsed_time(e1)
+    # end to end: this rank's share uploaded from host arrays (same topology), optimized, downloaded
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        prob.upload(sub)
+        prob.optimize(ITERATIONS)
+        pose, point = prob.estimates()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([ms, wall], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, wall = float(t[0].item()), float(t[1].item())
+    prob.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    h2d = sum(a.nbytes for a in (sub.pose_estimate, sub.point_estimate, sub.edge_vertex, sub.measurement,
+                                 sub.information, sub.robust_delta) if a is not None)
+    d2h = pose.nbytes + point.nbytes
+    print(json.dumps({
+        "metric": METRIC, "value": iters / (ms * 1e-3), "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32/f64 (FP32 Hessian/Schur/SpMV storage; FP64 vectors, chi2, LM)",
+        "data": "synthetic (seeded BA generator: ring cameras, box points, 1 px noise, 1% outliers, Huber)",
+        "config": {"workload": WORKLOAD, "iterations_per_step": ITERATIONS, "cameras": g.num_poses,
+                   "points": g.num_points, "edges": g.num_edges, "parallelism": f"points sharded over {world} rank(s)",
+                   "final_chi2": chi2},
+        "clocks": clk,
+        "e2e": {"value": iters / wall, "unit": "iter/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "upload": "same topology each step, per rank its share"},
+        "gpu_launches": launches1 - launches0,
+        "cpu_baseline": None,
+        "cpu_baseline_note": "see the default configuration's line (the same graph on the host cores)",
     }), flush=True)
 
 
@@ -643,5 +739,7 @@ if __name__ == "__main__":
         run_windows(a)
     elif a.config == "adjoint":
         run_adjoint(a)
+    elif a.config == "ba_sharded":
+        run_ba_sharded(a)
     else:
         run_ours(a)
