@@ -68,3 +68,28 @@ def test_assignment_is_deterministic_and_balanced():
         a = shard.assign_windows(costs, world)
         assert a == shard.assign_windows(costs, world)
         assert sorted(w for x in a for w in x) == list(range(100))
+
+
+def test_split_points_partitions_the_bundle_adjustment():
+    """The shards of a sharded bundle adjustment: every camera on every rank,
+    each point and each edge on exactly one, point indices renumbered within
+    the shard, edge data carried along."""
+    import numpy as np
+    from g2o_b200 import backend, synth
+    g = synth.bundle_adjustment(num_cameras=30, num_points=2000, seed=8)
+    for parts in (1, 2, 3):
+        shards = backend.split_points(g, parts)
+        assert sum(s.num_points for s, _ in shards) == g.num_points
+        assert sum(s.num_edges for s, _ in shards) == g.num_edges
+        seen = np.concatenate([idx for _, idx in shards])
+        assert np.array_equal(np.sort(seen), np.arange(g.num_points))
+        for s, idx in shards:
+            assert s.num_poses == g.num_poses and np.array_equal(s.pose_estimate, g.pose_estimate)
+            assert np.array_equal(s.pose_fixed, g.pose_fixed)
+            assert np.array_equal(s.point_estimate, g.point_estimate[idx])
+            orig = s.edge_vertex[:, 0] + idx[0]
+            sel = np.isin(g.edge_vertex[:, 0], idx)
+            assert np.array_equal(orig, g.edge_vertex[sel, 0])
+            assert np.array_equal(s.edge_vertex[:, 1], g.edge_vertex[sel, 1])
+            assert np.array_equal(s.measurement, g.measurement[sel])
+            assert np.array_equal(s.information, g.information[sel])
