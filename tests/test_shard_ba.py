@@ -1,8 +1,8 @@
 """Sharded bundle adjustment (g2oc_set_sharding): every rank holds every
 camera and a share of the points; per LM trial the ranks sum their parts of
 the reduced camera system, chi2 and the gain-ratio scale, then take the same
-step. Run here as two ranks in one process on one GPU: two contexts driven by
-two host threads whose all-reduce meets on the host (each rank's CUDA stream
+step. Run here as two and three ranks in one process on one GPU: contexts driven by
+host threads whose all-reduce meets on the host (each rank's CUDA stream
 is drained before the meeting, no kernel waits for another). The sharded run
 must follow the single-context run of the whole graph: same trial counts,
 chi2 per iteration within 1e-6 relative, camera translations within 1e-6 m and
@@ -85,8 +85,8 @@ def run_sharded(backend, g, make_params, iters, world=2):
     return out, shards, bus.calls
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed_fast"])
-def test_two_shards_follow_the_single_context(backend, precision):
+@pytest.mark.parametrize("precision,world", [("fp64", 2), ("mixed_fast", 2), ("fp64", 3)])
+def test_shards_follow_the_single_context(backend, precision, world):
     g = synth.bundle_adjustment(num_cameras=60, num_points=6000, seed=41)
     fac = backend.OptimizationAlgorithmFactory.instance()
     name = "lm_cuda" if precision == "fp64" else "lm_cuda_mixed_fast"
@@ -94,7 +94,7 @@ def test_two_shards_follow_the_single_context(backend, precision):
     done_ref, st_ref = ref.optimize(ITER)
     pose_ref, point_ref = ref.estimates()
     ref.close()
-    out, shards, calls = run_sharded(backend, g, lambda: fac.construct(name), ITER)
+    out, shards, calls = run_sharded(backend, g, lambda: fac.construct(name), ITER, world)
     # metres, in a 20 m scene: FP64 sums in another order; FP32 storage of H and S
     tol_pose, tol_point = (1e-6, 1e-5) if precision == "fp64" else (2e-5, 2e-4)
     assert calls > 0
@@ -106,8 +106,9 @@ def test_two_shards_follow_the_single_context(backend, precision):
         assert np.abs(pose[:, :3] - pose_ref[:, :3]).max() < tol_pose
         idx = shards[r][1]
         assert np.abs(point - point_ref[idx]).max() < tol_point
-    # both ranks hold the same cameras
-    assert np.array_equal(out[0][2], out[1][2])
+    # every rank holds the same cameras
+    for r in range(1, world):
+        assert np.array_equal(out[0][2], out[r][2])
 
 
 def test_sharding_rejects_unsupported_setups(backend):
