@@ -50,37 +50,25 @@ struct WinDev {
   const long long* mat;  // offset of the window's dense n x n matrix in the scratch
 };
 
-// robust chi2 per window (activeRobustChi2), one CTA per window; into
-// chi2_cur (which = 0, windows at the start of an iteration) or chi2_temp
-// (which = 1)
+// robust chi2 per window (activeRobustChi2) into chi2_cur (which = 0, windows
+// at the start of an iteration) or chi2_temp (which = 1), over edge chunks of
+// at most kWinChi2Chunk edges so that the largest windows do not set the
+// launch's tail: per chunk a CTA's sum, then per window the chunk sums in
+// chunk order (win_chi2_finish).
+constexpr int kWinChi2Chunk = 2048;
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) win_chi2(BAEdges E, BAVertices V, WinDev W, WinState* ws, int which) {
-  const int w = blockIdx.x;
-  WinState& s = ws[w];
+__global__ void __launch_bounds__(THREADS) win_chi2_chunks(BAEdges E, BAVertices V, WinDev W, const int* chunk_w,
+                                                          const int* chunk_e0, const WinState* ws, int which,
+                                                          double* partial) {
+  const int ch = blockIdx.x, w = chunk_w[ch];
+  const WinState& s = ws[w];
   if (s.done || (which == 0 && s.qmax != 0)) return;
+  const int k1 = min(chunk_e0[ch] + kWinChi2Chunk, W.edge[w + 1]);
   double r = 0.0;
-  const int k1 = W.edge[w + 1];
-  // the next edge's record is loaded while this one's vertices are
-  int k = W.edge[w] + threadIdx.x;
-  int2 vn = make_int2(0, 0);
-  double2 zn = make_double2(0.0, 0.0);
-  double4 omn = make_double4(0.0, 0.0, 0.0, 0.0);
-  if (k < k1) {
-    vn = E.v[k];
-    zn = E.z[k];
-    omn = E.om[k];
-  }
-  for (; k < k1; k += THREADS) {
-    const int2 v = vn;
-    const double2 z = zn;
-    const double4 om = omn;
-    if (k + THREADS < k1) {
-      vn = E.v[k + THREADS];
-      zn = E.z[k + THREADS];
-      omn = E.om[k + THREADS];
-    }
+  for (int k = chunk_e0[ch] + threadIdx.x; k < k1; k += THREADS) {
     double e[2], Xc[3], chi2, wt;
-    ba_edge_error(V, v, z, om, e, Xc, chi2, wt);
+    const double4 om = E.om[k];
+    ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, wt);
     if (om.w > 0.0) {
       double rho[3];
       huber(chi2, om.w, rho);
@@ -90,13 +78,22 @@ __global__ void __launch_bounds__(THREADS) win_chi2(BAEdges E, BAVertices V, Win
     }
   }
   r = block_sum1(r);
-  if (threadIdx.x == 0) {
-    if (which == 0) {
-      s.chi2_cur = r;
-      if (s.iteration == 0) s.chi2_init = r;
-    } else {
-      s.chi2_temp = r;
-    }
+  if (threadIdx.x == 0) partial[ch] = r;
+}
+
+static __global__ void win_chi2_finish(const int* win_chunk_ptr, int nw, const double* partial, WinState* ws,
+                                       int which) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nw) return;
+  WinState& s = ws[w];
+  if (s.done || (which == 0 && s.qmax != 0)) return;
+  double r = 0.0;
+  for (int c = win_chunk_ptr[w]; c < win_chunk_ptr[w + 1]; ++c) r += partial[c];
+  if (which == 0) {
+    s.chi2_cur = r;
+    if (s.iteration == 0) s.chi2_init = r;
+  } else {
+    s.chi2_temp = r;
   }
 }
 

@@ -186,6 +186,9 @@ struct g2oc_ctx {
   g2oc::PinnedVec<g2oc::PcgState> h_pcg;
   cudaEvent_t ev_read = nullptr;
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
+  g2oc::DBuf<int> win_chunk_w, win_chunk_e0, win_chunk_ptr;  // chi2 edge chunks (kWinChi2Chunk)
+  g2oc::DBuf<double> win_chunk_sum;
+  int win_nchunks = 0;
   g2oc::DBuf<long long> win_mat;
   g2oc::DBuf<double> win_scratch, lam_c, lam_l;
   g2oc::DBuf<g2oc::WinState> win_state;
@@ -2380,6 +2383,25 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   G2OC_TRY(c->win_cam.upload(wc, st));
   G2OC_TRY(c->win_lm.upload(wl, st));
   G2OC_TRY(c->win_edge.upload(we, st));
+  {
+    std::vector<int> cw, ce0, cptr(nw + 1, 0);
+    for (int i = 0; i < nw; ++i) {
+      for (int e0 = we[i]; e0 < we[i + 1]; e0 += kWinChi2Chunk) {
+        cw.push_back(i);
+        ce0.push_back(e0);
+      }
+      cptr[i + 1] = (int)cw.size();
+    }
+    c->win_nchunks = (int)cw.size();
+    if (cw.empty()) {
+      cw.push_back(0);
+      ce0.push_back(0);
+    }
+    G2OC_TRY(c->win_chunk_w.upload(cw, st));
+    G2OC_TRY(c->win_chunk_e0.upload(ce0, st));
+    G2OC_TRY(c->win_chunk_ptr.upload(cptr, st));
+    G2OC_TRY(c->win_chunk_sum.alloc(cw.size()));
+  }
   G2OC_TRY(c->win_pose.upload(pose_off, st));
   G2OC_TRY(c->win_point.upload(point_off, st));
   G2OC_TRY(c->win_of_cam.upload(ofc, st));
@@ -2402,6 +2424,22 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   return G2OC_OK;
 }
 
+// robust chi2 of every window (which = 0: into chi2_cur at an iteration's
+// start; 1: into chi2_temp after a trial step)
+static int window_chi2(g2oc_ctx* c, int which) {
+  cudaStream_t st = c->stream;
+  if (c->win_nchunks > 0) {
+    G2OC_K(K_CHI2) win_chi2_chunks<512><<<c->win_nchunks, 512, 0, st>>>(
+        c->ba_edges(), c->ba_vertices(), c->windev(), c->win_chunk_w.p, c->win_chunk_e0.p, c->win_state.p, which,
+        c->win_chunk_sum.p);
+    G2OC_LAUNCH_CHECK();
+  }
+  G2OC_K(K_CHI2) win_chi2_finish<<<cdiv(c->nw, 128), 128, 0, st>>>(c->win_chunk_ptr.p, c->nw, c->win_chunk_sum.p,
+                                                                    c->win_state.p, which);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
 // one LM round of every unfinished window (only stream-ordered work: this is
 // what the CUDA graph captures)
 static int window_round(g2oc_ctx* c, bool autotune) {
@@ -2410,7 +2448,7 @@ static int window_round(g2oc_ctx* c, bool autotune) {
   const WinDev W = c->windev();
   const int n = c->vec_size();
   G2OC_CUDA_TRY(cudaMemsetAsync(c->win_active.p, 0, sizeof(int), st));
-  G2OC_K(K_CHI2) win_chi2<1024><<<c->nw, 1024, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 0);
+  G2OC_TRY(window_chi2(c, 0));
   G2OC_LAUNCH_CHECK();
   G2OC_TRY(c->eng->build_system());
   G2OC_TRY(c->eng->batch_lambda_init(c->prm.initial_lambda, c->prm.tau));
@@ -2423,7 +2461,7 @@ static int window_round(g2oc_ctx* c, bool autotune) {
                                                                     c->win_state.p, c->x.p);
   G2OC_LAUNCH_CHECK();
   G2OC_TRY(oplus(c));
-  G2OC_K(K_CHI2) win_chi2<1024><<<c->nw, 1024, 0, st>>>(c->ba_edges(), c->ba_vertices(), W, c->win_state.p, 1);
+  G2OC_TRY(window_chi2(c, 1));
   G2OC_K(K_LM_CONTROL) win_scale<256><<<c->nw, 256, 0, st>>>(c->x.p, c->b.p, S.Cf, W, c->win_state.p);
   G2OC_K(K_LM_CONTROL) win_decide<<<cdiv(c->nw, 128), 128, 0, st>>>(c->win_state.p, c->nw,
                                                                     c->prm.max_trials_after_failure, c->win_iterations,
