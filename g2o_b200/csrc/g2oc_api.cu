@@ -1529,8 +1529,18 @@ static bool same_topology(const g2oc_ctx::Topology& t, const g2oc_graph* g) {
       t.edge_type != g->edge_type || t.num_edges != g->num_edges || !g->edge_vertex)
     return false;
   if (t.has_pose_fixed != (g->pose_fixed != nullptr) || t.has_point_fixed != (g->point_fixed != nullptr)) return false;
-  if (!t.edge_vertex.empty() && memcmp(t.edge_vertex.data(), g->edge_vertex, t.edge_vertex.size() * sizeof(int32_t)))
-    return false;
+  if (!t.edge_vertex.empty()) {
+    // compared in parallel chunks (tens of MB for large graphs)
+    const size_t n = t.edge_vertex.size(), chunk = 1 << 20;
+    const long long nch = (long long)((n + chunk - 1) / chunk);
+    int differ = 0;
+#pragma omp parallel for schedule(static) reduction(| : differ) if (nch > 1)
+    for (long long q = 0; q < nch; ++q) {
+      const size_t a = (size_t)q * chunk, len = std::min(chunk, n - a);
+      if (memcmp(t.edge_vertex.data() + a, g->edge_vertex + a, len * sizeof(int32_t))) differ |= 1;
+    }
+    if (differ) return false;
+  }
   if (t.has_pose_fixed && !t.pose_fixed.empty() && memcmp(t.pose_fixed.data(), g->pose_fixed, t.pose_fixed.size()))
     return false;
   if (t.has_point_fixed && !t.point_fixed.empty() && memcmp(t.point_fixed.data(), g->point_fixed, t.point_fixed.size()))
