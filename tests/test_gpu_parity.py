@@ -336,3 +336,31 @@ def test_factory_constructed_solver_runs(backend, oracle_lib):
                                                               linear_solver=LINEAR_CHOLESKY))
     o.optimize(5)
     assert abs(opt.active_chi2() - o.chi2()[0]) <= 1e-8 * o.chi2()[0]
+
+
+# ------------------------------------------------------------ invalid graphs
+def test_invalid_graphs_are_refused_at_upload(backend):
+    """Graphs the reference would not optimize are refused with BAD_GRAPH at
+    upload (g2oc_upload), not run: a vertex index out of range, no edge at
+    all, and no active edge (every vertex of every edge fixed,
+    allVerticesFixed)."""
+    g = small_ba(cams=10, points=200)
+    bad = g.copy()
+    bad.edge_vertex[5, 1] = g.num_poses  # camera index past the end
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(bad)
+    assert e.value.status == 2
+    empty = g.copy()
+    empty.edge_vertex = empty.edge_vertex[:0].copy()
+    empty.measurement = empty.measurement[:0].copy()
+    empty.information = empty.information[:0].copy()
+    empty.robust_delta = None
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(empty)
+    assert e.value.status == 2
+    fixed = g.copy()
+    fixed.pose_fixed = np.ones(g.num_poses, dtype=np.uint8)
+    fixed.point_fixed = np.ones(g.num_points, dtype=np.uint8)
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(fixed)
+    assert e.value.status == 2
