@@ -117,6 +117,22 @@ class G2ocWindowStats(C.Structure):
                 "chi2_initial": self.chi2_initial, "chi2": self.chi2, "lambda": self.lambda_}
 
 
+class G2ocFileInfo(C.Structure):
+    """g2oc_file_info (include/g2o_io.h)."""
+    _fields_ = [("num_vertices", C.c_int32), ("num_edges", C.c_int32), ("num_parameters", C.c_int32),
+                ("num_fixed", C.c_int32), ("lines", C.c_int32), ("lines_rejected", C.c_int32),
+                ("lines_unsupported", C.c_int32), ("lines_skipped", C.c_int32), ("fix_not_found", C.c_int32),
+                ("first_problem_line", C.c_int32), ("first_problem", C.c_char * 200)]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["first_problem"] = self.first_problem.decode()
+        return d
+
+
+SAVE_ALL, SAVE_VERTEX_SUBSET, SAVE_EDGE_SUBSET = 0, 1, 2
+
+
 class G2ocBackwardStats(C.Structure):
     _fields_ = [("refinement_steps", C.c_int32), ("pcg_iterations", C.c_int32), ("relative_residual", C.c_double)]
 

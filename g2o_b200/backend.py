@@ -89,6 +89,18 @@ def library() -> C.CDLL:
         "g2oc_solve_block_system_static": ([C.c_int, C.c_int32, C.c_int32, C.c_int32, ip, dp, dp, dp, C.c_double,
                                             C.c_int32, ip], C.c_int),
         "g2oc_set_sharding": ([vp, C.c_int32, C.c_int32, ALLREDUCE_FN, vp], C.c_int),
+        "g2oc_file_load": ([C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
+        "g2oc_file_parse": ([C.c_char_p, C.c_size_t, C.c_char_p, C.POINTER(vp)], C.c_int),
+        "g2oc_file_from_graph": ([vp, ip, ip, C.c_int32, C.POINTER(vp)], C.c_int),
+        "g2oc_file_free": ([vp], None),
+        "g2oc_file_get_info": ([vp, vp], C.c_int),
+        "g2oc_file_graph": ([vp, vp], C.c_int),
+        "g2oc_file_vertex_ids": ([vp, ip, ip], C.c_int),
+        "g2oc_file_set_fixed": ([vp, C.c_int32, C.c_int32], C.c_int),
+        "g2oc_file_fix_gauge": ([vp, ip], C.c_int),
+        "g2oc_file_set_robust_huber": ([vp, C.c_double, C.c_int32], C.c_int),
+        "g2oc_file_set_estimates": ([vp, dp, dp], C.c_int),
+        "g2oc_file_save": ([vp, C.c_char_p, C.c_int32, ip, C.c_int32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -98,9 +110,11 @@ def library() -> C.CDLL:
     return L
 
 
-def header_symbols(path: str = HEADER_PATH) -> List[str]:
-    """Function names declared in include/g2o_cuda.h."""
-    text = open(path).read()
+def header_symbols(path: Optional[str] = None) -> List[str]:
+    """Function names declared in include/*.h (or in the one header given)."""
+    inc = os.path.dirname(HEADER_PATH)
+    paths = [path] if path else [os.path.join(inc, f) for f in sorted(os.listdir(inc)) if f.endswith(".h")]
+    text = "".join(open(p).read() for p in paths)
     return sorted(set(re.findall(r"^\s*(?:int|void|const char\*)\s+(g2oc_\w+)\s*\(", text, re.M)))
 
 

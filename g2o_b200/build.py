@@ -9,7 +9,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libg2o_b200.so")
-SOURCES = ["g2oc_api.cu", "noalloc.cu", "structure.cpp"]
+CLI = os.path.join(HERE, "g2o_cuda_cli")
+CLI_SOURCE = "g2o_cuda_cli.cpp"
+SOURCES = ["g2oc_api.cu", "noalloc.cu", "structure.cpp", "g2o_io.cpp"]
 HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -22,12 +24,12 @@ def _newest(paths):
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return False
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    deps.append(os.path.join(HERE, "..", "include", "g2o_cuda.h"))
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS + [CLI_SOURCE]]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("g2o_cuda.h", "g2o_io.h")]
     deps.append(__file__)
-    return os.path.getmtime(LIB) >= _newest(deps)
+    return min(os.path.getmtime(LIB), os.path.getmtime(CLI)) >= _newest(deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -45,6 +47,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
+    # the command-line optimizer, linked against the library next to it
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-o", CLI, os.path.join(CSRC, CLI_SOURCE), "-L" + HERE,
+           "-lg2o_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
     return LIB
 
 

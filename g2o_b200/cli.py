@@ -3,6 +3,10 @@
 
     python -m g2o_b200.cli --config ba --solver lm_cuda_pcg6_3 -i 20 [-stats]
     python -m g2o_b200.cli --config windows --windows 64 --solver lm_cuda_mixed_fast -i 10
+    python -m g2o_b200.cli --input graph.g2o -o graph_opt.g2o --solver lm_cuda -i 20
+
+(g2o_b200/g2o_cuda_cli is the native counterpart for .g2o files, with g2o_cli's
+options.)
 
 Prints one line per iteration with chi2, lambda, trial and PCG counts and the
 phase times (the fields of G2OBatchStatistics); for the batched windows, one
@@ -49,6 +53,8 @@ def main(argv=None):
     ap.add_argument("-stats", "--stats", action="store_true", help="print per-kernel launch counts and times")
     ap.add_argument("--listSolvers", action="store_true")
     ap.add_argument("--windows", type=int, default=512, help="windows: how many of the 512 local BA windows")
+    ap.add_argument("--input", help="a .g2o file to optimize instead of a synthetic configuration")
+    ap.add_argument("-o", "--output", help="with --input: write the optimized graph here")
     a = ap.parse_args(argv)
     fac = backend.OptimizationAlgorithmFactory.instance()
     if a.listSolvers:
@@ -60,7 +66,17 @@ def main(argv=None):
         return 1
     if a.config == "windows":
         return run_windows(a, params)
-    g = CONFIGS[a.config]()
+    gfile = None
+    if a.input:
+        from .g2ofile import G2oFile
+        gfile = G2oFile.load(a.input)
+        gid = gfile.fix_gauge()
+        print(f"# {a.input}: {gfile.info()['num_vertices']} vertices, {gfile.info()['num_edges']} edges"
+              + (f"; gauge fixed at vertex {gid}" if gid >= 0 else ""))
+        g = gfile.graph()
+        g.name = a.input
+    else:
+        g = CONFIGS[a.config]()
     prob = backend.CudaProblem(g, params, device=a.device)
     prob.set_kernel_timing(a.stats)
     chi0, rchi0 = prob.chi2()
@@ -75,6 +91,10 @@ def main(argv=None):
         print(f"# kernel launches: {total}")
         for k, (n, ms) in sorted(ks.items(), key=lambda kv: -kv[1][1]):
             print(f"#   {k:20s} {n:7d} {ms:10.3f} ms")
+    if gfile is not None and a.output:
+        pose, point = prob.estimates()
+        gfile.set_estimates(pose, point)
+        gfile.save(a.output)
     prob.close()
     return 0 if done > 0 else 2
 
