@@ -89,6 +89,8 @@ def library() -> C.CDLL:
         "g2oc_solve_block_system_static": ([C.c_int, C.c_int32, C.c_int32, C.c_int32, ip, dp, dp, dp, C.c_double,
                                             C.c_int32, ip], C.c_int),
         "g2oc_set_sharding": ([vp, C.c_int32, C.c_int32, ALLREDUCE_FN, vp], C.c_int),
+        "g2oc_compute_marginals": ([vp, C.c_int32, ip, dp], C.c_int),
+        "g2oc_solve_pattern_block_system": ([vp, C.c_int32, ip, C.c_int32, ip, dp, C.c_int32, ip, dp], C.c_int),
         "g2oc_file_load": ([C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
         "g2oc_file_parse": ([C.c_char_p, C.c_size_t, C.c_char_p, C.POINTER(vp)], C.c_int),
         "g2oc_file_from_graph": ([vp, ip, ip, C.c_int32, C.POINTER(vp)], C.c_int),
@@ -337,6 +339,15 @@ class CudaProblem:
         return dmeas, dlogw, {"refinement_steps": st.refinement_steps, "pcg_iterations": st.pcg_iterations,
                               "relative_residual": st.relative_residual}
 
+    def compute_marginals(self, block_indices):
+        """Blocks of Hpp^-1 at the current estimates for (row, col) pairs of
+        Hessian block indices (SparseOptimizer::computeMarginals)."""
+        idx = np.ascontiguousarray(np.asarray(block_indices, np.int32).reshape(-1, 2))
+        pd = self.info.pose_dim
+        out = np.zeros((max(len(idx), 1), pd, pd))
+        _check(library().g2oc_compute_marginals(self._h, len(idx), _p(idx, C.c_int32), _p(out)))
+        return out[:len(idx)]
+
     def solve(self, lam):
         x = np.empty(self.info.vector_size)
         it = C.c_int32()
@@ -482,6 +493,26 @@ def solve_block_system(linear_solver, block_offsets, block_rc, values, b, params
         st = L.g2oc_solve_block_system(h, linear_solver, len(offs) - 1, _p(offs, C.c_int32), len(rc),
                                        _p(rc, C.c_int32), _p(vals), _p(bb), _p(x), C.byref(it))
         return st, x, it.value
+    finally:
+        L.g2oc_destroy(h)
+
+
+def solve_pattern_block_system(block_offsets, block_rc, values, block_indices, device=0):
+    """LinearSolver::solvePattern on a caller block matrix: the requested
+    (row, col) blocks of A^-1, row-major."""
+    L = library()
+    h = C.c_void_p()
+    _check(L.g2oc_create(device, C.byref(h)))
+    try:
+        offs = np.ascontiguousarray(block_offsets, np.int32)
+        rc = np.ascontiguousarray(block_rc, np.int32)
+        vals = np.ascontiguousarray(values, np.float64)
+        idx = np.ascontiguousarray(np.asarray(block_indices, np.int32).reshape(-1, 2))
+        bs = int(offs[1] - offs[0])
+        out = np.zeros((max(len(idx), 1), bs, bs))
+        st = L.g2oc_solve_pattern_block_system(h, len(offs) - 1, _p(offs, C.c_int32), len(rc), _p(rc, C.c_int32),
+                                               _p(vals), len(idx), _p(idx, C.c_int32), _p(out))
+        return st, out[:len(idx)]
     finally:
         L.g2oc_destroy(h)
 

@@ -83,8 +83,11 @@ static void rcm_order(int nb, const std::vector<int32_t>& rc, std::vector<int>& 
   for (int i = 0; i < nb; ++i) perm[order[nb - 1 - i]] = i;
 }
 
+// extra: further (row, col) block pairs whose entries the plan must hold
+// (the blocks a selected inverse is asked for), treated as structural
+// nonzeros of the matrix so that the symbolic fill covers them
 static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_t>& rc, bool reorder,
-                           cudaStream_t st) {
+                           cudaStream_t st, const std::vector<int32_t>* extra = nullptr) {
   P.nb = nb;
   P.bs = bs;
   P.n = nb * bs;
@@ -106,6 +109,8 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
       }
   };
   for (size_t k = 0; k < rc.size() / 2; ++k) mark(rc[2 * k], rc[2 * k + 1]);
+  if (extra)
+    for (size_t k = 0; k < extra->size() / 2; ++k) mark((*extra)[2 * k], (*extra)[2 * k + 1]);
   for (int t = 0; t < nt; ++t) nz[(size_t)t * nt + t] = 1;
   P.pnl_ptr.assign(nt + 1, 0);
   P.upd_ptr.assign(nt + 1, 0);
@@ -350,11 +355,10 @@ static __global__ void chol_bwd_update(const double* A, int np, int k, const int
   }
 }
 
+// densify and factor: P.A holds L (lower tiles of the pattern), P.info the pivot flag
 template <typename Real>
-static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const double* rhs, double* xout, int* ok,
-                      long long* nlaunch) {
+static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long long* nl) {
   const int nnzb = S.nnzb;
-  long long nl = 4;  // densify, load_rhs, store_x, + memsets
   const int np = P.np, nt = P.nt;
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
@@ -368,13 +372,22 @@ static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const
     if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k]);
     const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];
     if (nu > 0) chol_gemm<<<nu, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_upd.p + P.upd_ptr[k]);
-    nl += 1 + (np_k > 0) + (nu > 0);
+    *nl += 1 + (np_k > 0) + (nu > 0);
   }
   const cudaError_t e1 = cudaGetLastError();
   if (e1 != cudaSuccess) {
     set_error("cholesky launch: %s", cudaGetErrorString(e1));
     return G2OC_ERR_CUDA;
   }
+  return G2OC_OK;
+}
+
+template <typename Real>
+static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const double* rhs, double* xout, int* ok,
+                      long long* nlaunch) {
+  long long nl = 4;  // densify, load_rhs, store_x, + memsets
+  const int np = P.np, nt = P.nt;
+  G2OC_TRY(chol_factor<Real>(P, st, S, &nl));
   chol_load_rhs<<<(np + 255) / 256, 256, 0, st>>>(rhs, P.d_perm.p, P.nb, P.bs, P.n, np, P.y.p);
   for (int k = 0; k < nt; ++k) {
     chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
@@ -399,6 +412,246 @@ static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const
   G2OC_CUDA_TRY(cudaMemcpyAsync(&info, P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));
   *ok = info == 0;
+  return G2OC_OK;
+}
+
+// ------------------------------------------------------------------------
+// Selected inverse (the marginal covariances of
+// LinearSolver::solvePattern, g2o/core/linear_solver.h:78-90, which g2o's
+// Cholesky solvers compute with MarginalCovarianceCholesky,
+// g2o/core/linear_solver.h:165-173 and g2o/core/marginal_covariance_cholesky.h:42-106). From H = L L^T
+// and L^T Sigma = L^-1 (upper-triangular right side), for tile column J
+// taken from last to first with S_J = {I > J : L(I,J) != 0} and
+// Lh(I,J) = L(I,J) L(J,J)^-1:
+//   Sigma(K,J) = - sum_{I in S_J} Sigma(K,I) Lh(I,J)          (K in S_J)
+//   Sigma(J,J) = L(J,J)^-T L(J,J)^-1 - sum_{I in S_J} Lh(I,J)^T Sigma(I,J)
+// Every Sigma(K,I) needed lies in the filled tile pattern (S_J is a clique
+// of it), so only the pattern's tiles are computed: the tile form of the
+// Takahashi recurrences. Sigma is kept in a dense column-major np x np
+// buffer: lower tiles and full diagonal tiles. L's panel tiles are
+// overwritten by Lh.
+
+// W = L(J,J)^-1 (lower), column c by thread c: forward substitution of e_c
+static __global__ void __launch_bounds__(256) selinv_tri_inv(const double* A, int np, int J, double* W) {
+  extern __shared__ double sm_ti[];
+  double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_ti);
+  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_ti + kTile * (kTile + 1));
+  const size_t jb = (size_t)J * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    L[r][c] = r >= c ? A[(jb + c) * np + jb + r] : 0.0;
+  }
+  __syncthreads();
+  const int c = threadIdx.x;
+  if (c < kTile) {
+    for (int r = 0; r < c; ++r) X[r][c] = 0.0;
+    for (int r = c; r < kTile; ++r) {
+      double v = r == c ? 1.0 : 0.0;
+      for (int t = c; t < r; ++t) v -= L[r][t] * X[t][c];
+      X[r][c] = v / L[r][r];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, cc = e / kTile;
+    W[cc * kTile + r] = X[r][cc];
+  }
+}
+
+// Lh(I,J) = L(I,J) W for the listed tiles I, in place
+static __global__ void __launch_bounds__(256) selinv_panel(double* A, int np, int J, const int* tiles,
+                                                           const double* W) {
+  extern __shared__ double sm_sp[];
+  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_sp);
+  double (*Wt)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_sp + kTile * (kTile + 1));
+  const size_t jb = (size_t)J * kTile, ib = (size_t)tiles[blockIdx.x] * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    X[r][c] = A[(jb + c) * np + ib + r];
+    Wt[r][c] = W[c * kTile + r];
+  }
+  __syncthreads();
+  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int t = 0; t < kTile; ++t) {
+    double x[4], y[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      x[a] = X[tr + 16 * a][t];
+      y[a] = Wt[t][tc + 16 * a];
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) A[(jb + tc + 16 * b) * np + ib + tr + 16 * a] = acc[a][b];
+}
+
+// Sigma tile (K, I) of the stored lower/diagonal tiles, into smem as T[r][c]
+__device__ __forceinline__ void selinv_load_sigma(const double* Sg, int np, int K, int I,
+                                                  double (*T)[kTile + 1]) {
+  const size_t kb = (size_t)K * kTile, ib = (size_t)I * kTile;
+  if (K >= I) {
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int r = e % kTile, c = e / kTile;
+      T[r][c] = Sg[(ib + c) * np + kb + r];
+    }
+  } else {  // Sigma(K,I) = Sigma(I,K)^T
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int c = e % kTile, r = e / kTile;
+      T[r][c] = Sg[(kb + r) * np + ib + c];
+    }
+  }
+}
+
+// Sigma(K,J) = - sum_I Sigma(K,I) Lh(I,J), one CTA per K in S_J
+static __global__ void __launch_bounds__(256) selinv_offdiag(const double* A, double* Sg, int np, int J,
+                                                             const int* tiles, int ntiles) {
+  extern __shared__ double sm_so[];
+  double (*Sk)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_so);
+  double (*Lh)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_so + kTile * (kTile + 1));
+  const int K = tiles[blockIdx.x];
+  const size_t jb = (size_t)J * kTile;
+  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int q = 0; q < ntiles; ++q) {
+    const int I = tiles[q];
+    const size_t ib = (size_t)I * kTile;
+    __syncthreads();
+    selinv_load_sigma(Sg, np, K, I, Sk);
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int r = e % kTile, c = e / kTile;
+      Lh[r][c] = A[(jb + c) * np + ib + r];
+    }
+    __syncthreads();
+    for (int t = 0; t < kTile; ++t) {
+      double x[4], y[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        x[a] = Sk[tr + 16 * a][t];
+        y[a] = Lh[t][tc + 16 * a];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
+    }
+  }
+  const size_t kb = (size_t)K * kTile;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) Sg[(jb + tc + 16 * b) * np + kb + tr + 16 * a] = -acc[a][b];
+}
+
+// Sigma(J,J) = W^T W - sum_I Lh(I,J)^T Sigma(I,J), symmetrized
+static __global__ void __launch_bounds__(256) selinv_diag(const double* A, double* Sg, int np, int J,
+                                                          const int* tiles, int ntiles, const double* W) {
+  extern __shared__ double sm_sd[];
+  double (*P0)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_sd);
+  double (*P1)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_sd + kTile * (kTile + 1));
+  const size_t jb = (size_t)J * kTile;
+  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
+  double acc[4][4] = {};
+  for (int q = -1; q < ntiles; ++q) {
+    __syncthreads();
+    if (q < 0) {
+      for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+        const int r = e % kTile, c = e / kTile;
+        P0[r][c] = W[c * kTile + r];
+        P1[r][c] = -W[c * kTile + r];
+      }
+    } else {
+      const size_t ib = (size_t)tiles[q] * kTile;
+      for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+        const int r = e % kTile, c = e / kTile;
+        P0[r][c] = A[(jb + c) * np + ib + r];   // Lh(I,J)
+        P1[r][c] = Sg[(jb + c) * np + ib + r];  // Sigma(I,J)
+      }
+    }
+    __syncthreads();
+    // acc -= P0^T P1
+    for (int t = 0; t < kTile; ++t) {
+      double x[4], y[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        x[a] = P0[t][tr + 16 * a];
+        y[a] = P1[t][tc + 16 * a];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] -= x[a] * y[b];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) P0[tr + 16 * a][tc + 16 * b] = acc[a][b];
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int r = e % kTile, c = e / kTile;
+    Sg[(jb + c) * np + jb + r] = 0.5 * (P0[r][c] + P0[c][r]);
+  }
+}
+
+// requested blocks (row, col) of H^-1, row-major bs x bs each
+static __global__ void selinv_gather(const double* Sg, int np, const int* perm, int bs, const int2* req, int nreq,
+                                     double* out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int per = bs * bs;
+  if (t >= (long long)nreq * per) return;
+  const int q = (int)(t / per), e = (int)(t % per);
+  const int i = perm[req[q].x] * bs + e / bs, j = perm[req[q].y] * bs + e % bs;
+  out[t] = (i / kTile >= j / kTile) ? Sg[(size_t)j * np + i] : Sg[(size_t)i * np + j];
+}
+
+// the requested blocks of S^-1 (pairs (row, col) of block indices, covered by
+// the plan's extra pairs) into out (device, nreq * bs * bs)
+template <typename Real>
+static int chol_selected_inverse(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const int2* d_req, int nreq,
+                                 double* d_out, int* ok, long long* nlaunch) {
+  long long nl = 2;
+  const int np = P.np, nt = P.nt;
+  G2OC_TRY(chol_factor<Real>(P, st, S, &nl));
+  int info = 0;
+  G2OC_CUDA_TRY(cudaMemcpyAsync(&info, P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  *ok = info == 0;
+  if (!*ok) return G2OC_OK;
+  DBuf<double> Sg, W;
+  G2OC_TRY(Sg.alloc((size_t)np * np));
+  G2OC_TRY(W.alloc((size_t)kTile * kTile));
+  G2OC_CUDA_TRY(cudaMemsetAsync(Sg.p, 0, Sg.bytes(), st));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(selinv_tri_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(selinv_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(selinv_offdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(selinv_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+  for (int J = nt - 1; J >= 0; --J) {
+    const int nj = P.pnl_ptr[J + 1] - P.pnl_ptr[J];
+    const int* tl = P.d_pnl.p + P.pnl_ptr[J];
+    selinv_tri_inv<<<1, 256, kTileSmem, st>>>(P.A.p, np, J, W.p);
+    if (nj > 0) {
+      selinv_panel<<<nj, 256, kTileSmem, st>>>(P.A.p, np, J, tl, W.p);
+      selinv_offdiag<<<nj, 256, kTileSmem, st>>>(P.A.p, Sg.p, np, J, tl, nj);
+    }
+    selinv_diag<<<1, 256, kTileSmem, st>>>(P.A.p, Sg.p, np, J, tl, nj, W.p);
+    nl += 2 + 2 * (nj > 0);
+  }
+  const long long work = (long long)nreq * P.bs * P.bs;
+  if (work > 0) selinv_gather<<<(int)((work + 255) / 256), 256, 0, st>>>(Sg.p, np, P.d_perm.p, P.bs, d_req, nreq, d_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("selected inverse launch: %s", cudaGetErrorString(e));
+    return G2OC_ERR_CUDA;
+  }
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  if (nlaunch) *nlaunch += nl;
   return G2OC_OK;
 }
 

@@ -6,14 +6,15 @@
 //   g2o_cuda_cli [-i N] [-v] [-solver lm_cuda] [-o out.g2o] [-stats f] [-summary f]
 //                [-robustKernel Huber] [-robustKernelWidth w] [-nonSequential]
 //                [-gaugeList 1,2] [-renameTypes A=B,...] [-solverProperties k=v,...]
-//                [-gain g] [-ig n] [-device d] [-listSolvers] [-listRobustKernels]
-//                [-printSolverProperties] graph.g2o | -
+//                [-gain g] [-ig n] [-device d] [-computeMarginals] [-listSolvers]
+//                [-listRobustKernels] [-printSolverProperties] graph.g2o | -
 //
 // Messages go to stderr with g2o_cli's wording; exit codes follow it (1: no
 // vertices or the file cannot be opened, 2: load error, 3: the solver does
 // not suit the graph). Options of g2o_cli outside the device path (-guess,
-// -guessOdometry, -inc, -update, -guiout, -gnudump, -computeMarginals) are
-// refused with exit code 1.
+// -guessOdometry, -inc, -update, -guiout, -gnudump) are refused with exit
+// code 1. -computeMarginals prints the blocks (h, h) and (h-1, h) of Hpp^-1
+// for every free pose h, as g2o_cli does (g2o.cpp:620-652).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -41,10 +42,11 @@ struct Args {
   int device = 0;
   bool list_solvers = false, list_kernels = false, list_types = false, print_properties = false;
   bool marginalize = false;  // accepted: the points of a projection graph are always marginalized
+  bool marginals = false;
 };
 
 const char* const kRefused[] = {"-guess", "-guessOdometry", "-inc", "-update", "-guiout", "-gnudump",
-                                "-computeMarginals", "-gaugeId"};
+                                "-gaugeId"};
 
 int usage(const char* msg) {
   std::cerr << msg << "\nusage: g2o_cuda_cli [options] graph.g2o (see the source header for the options)\n";
@@ -102,6 +104,7 @@ bool parse_args(int argc, char** argv, Args& a, std::string& err) {
     else if (s == "-listTypes") a.list_types = true;
     else if (s == "-printSolverProperties") a.print_properties = true;
     else if (s == "-marginalize") a.marginalize = true;
+    else if (s == "-computeMarginals") a.marginals = true;
     else if (s.size() > 1 && s[0] == '-') {
       err = "unknown option " + s;
       return false;
@@ -370,6 +373,32 @@ int main(int argc, char** argv) {
     if (result == G2OC_RESULT_FAIL || fail) {
       result_iterations = 0;
       if (a.iterations > 0) std::cerr << "Cholesky failed, result might be invalid" << std::endl;
+    } else if (a.marginals) {
+      // free poses in Hessian order: pose ids ascending, fixed ones skipped
+      std::vector<int32_t> ids(graph.num_poses), hid;
+      g2oc_file_vertex_ids(file, ids.data(), nullptr);
+      for (int i = 0; i < graph.num_poses; ++i)
+        if (!(graph.pose_fixed && graph.pose_fixed[i])) hid.push_back(ids[i]);
+      std::vector<int32_t> req;
+      for (int h = 0; h < (int)hid.size(); ++h) {
+        req.push_back(h); req.push_back(h);
+        if (h > 0) { req.push_back(h - 1); req.push_back(h); }
+      }
+      const int pd = hinfo.pose_dim, nreq = (int)req.size() / 2;
+      std::vector<double> blocks((size_t)nreq * pd * pd);
+      if (g2oc_compute_marginals(ctx, nreq, req.data(), blocks.data()) == G2OC_OK) {
+        for (int q = 0; q < nreq; ++q) {
+          const int r = req[2 * q], cc = req[2 * q + 1];
+          if (r == cc) std::cerr << "Vertex id:" << hid[r] << std::endl;
+          std::cerr << "inv block :" << r << ", " << cc << std::endl;
+          for (int i = 0; i < pd; ++i) {
+            for (int j = 0; j < pd; ++j) std::cerr << (j ? " " : "") << blocks[((size_t)q * pd + i) * pd + j];
+            std::cerr << std::endl;
+          }
+        }
+      } else {
+        std::cerr << "computing the marginals failed: " << g2oc_last_error() << std::endl;
+      }
     }
     std::vector<double> pose((size_t)graph.num_poses * (graph.pose_type == G2OC_POSE_SE2 ? 3
                                                         : graph.pose_type == G2OC_POSE_SE3 ? 12 : 7));

@@ -2589,10 +2589,20 @@ int g2oc_download_window(g2oc_ctx* c, int32_t window, double* pose, double* poin
   return G2OC_OK;
 }
 
-int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, const int32_t* offs, int32_t nnzb,
-                            const int32_t* rc, const double* values, const double* b, double* x, int32_t* iters) {
-  G2OC_TRY(check_ctx(c, false));
-  if (nb <= 0 || !offs || nnzb <= 0 || !rc || !values || !b || !x) {
+// a caller's block matrix (upper blocks listed column-major, row-major
+// values) as a device system in the internal row order
+struct CallerSystem {
+  Structure tmp;
+  std::vector<int32_t> rcv;
+  int bs = 0;
+  DBuf<int> rp, rcl, brw, dg, cp, cb, pm;
+  DBuf<double> val;
+  SysDev<double> A;
+};
+
+static int caller_system(cudaStream_t st, int32_t nb, const int32_t* offs, int32_t nnzb, const int32_t* rc,
+                         const double* values, CallerSystem& cs) {
+  if (nb <= 0 || !offs || nnzb <= 0 || !rc || !values) {
     set_error("invalid block system arguments");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
@@ -2606,7 +2616,8 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
     set_error("block size %d not supported (3 or 6)", bs);
     return G2OC_ERR_NOT_SUPPORTED;
   }
-  std::vector<int32_t> rcv(rc, rc + 2 * (size_t)nnzb);
+  cs.bs = bs;
+  cs.rcv.assign(rc, rc + 2 * (size_t)nnzb);
   for (int k = 0; k < nnzb; ++k) {
     const int r = rc[2 * k], cc = rc[2 * k + 1];
     if (r < 0 || cc < 0 || r >= nb || cc >= nb || r > cc ||
@@ -2615,9 +2626,8 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
       return G2OC_ERR_INVALID_ARGUMENT;
     }
   }
-  // the system in the internal (row-major upper) order
-  Structure tmp;
-  build_sym_lists(nb, rcv, tmp);
+  Structure& tmp = cs.tmp;
+  build_sym_lists(nb, cs.rcv, tmp);
   for (int i = 0; i < nb; ++i)
     if (tmp.sys_diag[i] < 0) {
       set_error("diagonal block %d missing", i);
@@ -2630,26 +2640,38 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
     for (size_t e = 0; e < per; ++e)
       vint[(size_t)rb * per + e * nblk + (k - rb)] = values[(size_t)tmp.sys_perm[k] * per + e];
   }
+  G2OC_TRY(cs.rp.upload(tmp.sys_rptr, st));
+  G2OC_TRY(cs.rcl.upload(tmp.sys_rcol, st));
+  G2OC_TRY(cs.brw.upload(tmp.sys_brow, st));
+  G2OC_TRY(cs.dg.upload(tmp.sys_diag, st));
+  G2OC_TRY(cs.cp.upload(tmp.sys_cptr, st));
+  G2OC_TRY(cs.cb.upload(tmp.sys_cblk.empty() ? std::vector<int>{0} : tmp.sys_cblk, st));
+  G2OC_TRY(cs.val.upload(vint, st));
+  G2OC_TRY(cs.pm.upload(tmp.sys_perm, st));
+  cs.A = SysDev<double>{nb, nnzb, cs.rp.p, cs.rcl.p, cs.brw.p, cs.dg.p, cs.cp.p, cs.cb.p, cs.pm.p, cs.val.p};
+  return G2OC_OK;
+}
+
+int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, const int32_t* offs, int32_t nnzb,
+                            const int32_t* rc, const double* values, const double* b, double* x, int32_t* iters) {
+  G2OC_TRY(check_ctx(c, false));
+  if (!b || !x) {
+    set_error("invalid block system arguments");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
   cudaStream_t st = c->stream;
-  DBuf<int> rp, rcl, brw, dg, cp, cb;
-  DBuf<double> val, rhs, xo, mi, r, s, d0, d1, q, qrow, tb;
-  G2OC_TRY(rp.upload(tmp.sys_rptr, st));
-  G2OC_TRY(rcl.upload(tmp.sys_rcol, st));
-  G2OC_TRY(brw.upload(tmp.sys_brow, st));
-  G2OC_TRY(dg.upload(tmp.sys_diag, st));
-  G2OC_TRY(cp.upload(tmp.sys_cptr, st));
-  G2OC_TRY(cb.upload(tmp.sys_cblk.empty() ? std::vector<int>{0} : tmp.sys_cblk, st));
-  G2OC_TRY(val.upload(vint, st));
+  CallerSystem cs;
+  G2OC_TRY(caller_system(st, nb, offs, nnzb, rc, values, cs));
+  const int bs = cs.bs;
+  const SysDev<double>& A = cs.A;
+  DBuf<double> rhs, xo, mi, r, s, d0, d1, q, qrow, tb;
   const int n = nb * bs;
   G2OC_TRY(rhs.upload(std::vector<double>(b, b + n), st));
   G2OC_TRY(xo.alloc(n));
-  DBuf<int> pm;
-  G2OC_TRY(pm.upload(tmp.sys_perm, st));
-  SysDev<double> A{nb, nnzb, rp.p, rcl.p, brw.p, dg.p, cp.p, cb.p, pm.p, val.p};
   int it = 0, ok = 1;
   if (linear_solver == G2OC_LINEAR_CHOLESKY) {
     CholPlan P;
-    G2OC_TRY(chol_plan_build(P, nb, bs, rcv, true, st));
+    G2OC_TRY(chol_plan_build(P, nb, bs, cs.rcv, true, st));
     G2OC_TRY(chol_solve<double>(P, st, A, rhs.p, xo.p, &ok, &c->kcount[K_CHOLESKY]));
   } else {
     G2OC_TRY(mi.alloc((size_t)nb * bs * bs));
@@ -2673,6 +2695,74 @@ int g2oc_solve_block_system(g2oc_ctx* c, int32_t linear_solver, int32_t nb, cons
   G2OC_CUDA_TRY(cudaMemcpy(x, xo.p, n * sizeof(double), cudaMemcpyDeviceToHost));
   if (iters) *iters = it;
   return ok ? G2OC_OK : G2OC_ERR_NOT_PD;
+}
+
+// blocks of the inverse of a caller system (LinearSolver::solvePattern)
+static int solve_pattern(g2oc_ctx* c, CallerSystem& cs, int32_t nb, int32_t nreq, const int32_t* req, double* out) {
+  if (nreq < 0 || (nreq > 0 && (!req || !out))) {
+    set_error("invalid block index arguments");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  std::vector<int32_t> extra(req, req + 2 * (size_t)nreq);
+  std::vector<int2> pairs(nreq > 0 ? nreq : 1, make_int2(0, 0));
+  for (int q = 0; q < nreq; ++q) {
+    const int r = req[2 * q], cc = req[2 * q + 1];
+    if (r < 0 || cc < 0 || r >= nb || cc >= nb) {
+      set_error("block index pair (%d, %d) out of range [0, %d)", r, cc, nb);
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+    pairs[q] = make_int2(r, cc);
+  }
+  cudaStream_t st = c->stream;
+  CholPlan P;
+  G2OC_TRY(chol_plan_build(P, nb, cs.bs, cs.rcv, true, st, &extra));
+  DBuf<int2> d_req;
+  DBuf<double> d_out;
+  G2OC_TRY(d_req.upload(pairs, st));
+  G2OC_TRY(d_out.alloc((size_t)(nreq > 0 ? nreq : 1) * cs.bs * cs.bs));
+  int ok = 1;
+  G2OC_TRY(chol_selected_inverse<double>(P, st, cs.A, d_req.p, nreq, d_out.p, &ok, &c->kcount[K_CHOLESKY]));
+  if (!ok) {
+    set_error("the matrix is not positive definite");
+    return G2OC_ERR_NOT_PD;
+  }
+  if (nreq > 0)
+    G2OC_CUDA_TRY(cudaMemcpy(out, d_out.p, (size_t)nreq * cs.bs * cs.bs * sizeof(double), cudaMemcpyDeviceToHost));
+  return G2OC_OK;
+}
+
+int g2oc_solve_pattern_block_system(g2oc_ctx* c, int32_t nb, const int32_t* offs, int32_t nnzb, const int32_t* rc,
+                                    const double* values, int32_t num_blocks, const int32_t* block_indices,
+                                    double* out) {
+  G2OC_TRY(check_ctx(c, false));
+  CallerSystem cs;
+  G2OC_TRY(caller_system(c->stream, nb, offs, nnzb, rc, values, cs));
+  return solve_pattern(c, cs, nb, num_blocks, block_indices, out);
+}
+
+int g2oc_compute_marginals(g2oc_ctx* c, int32_t num_blocks, const int32_t* block_indices, double* out) {
+  G2OC_TRY(check_ctx(c, true));
+  if (c->shard_world > 1 || c->batch) {
+    set_error("marginals of a sharded bundle adjustment or of batched windows are not supported");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  const Structure& S = c->S;
+  const int nb = S.Cf;
+  if (nb <= 0) {
+    set_error("the graph has no free pose");
+    return G2OC_ERR_BAD_GRAPH;
+  }
+  // H at the current estimates, then its pose part Hpp
+  G2OC_TRY(g2oc_build_system(c));
+  const int pd = S.pd;
+  const size_t nnzb = S.hpp_rc.size() / 2;
+  std::vector<double> hpp(nnzb * pd * pd);
+  G2OC_TRY(c->eng->get_hessian(hpp.data(), nullptr, nullptr));
+  std::vector<int32_t> offs(nb + 1);
+  for (int i = 0; i <= nb; ++i) offs[i] = i * pd;
+  CallerSystem cs;
+  G2OC_TRY(caller_system(c->stream, nb, offs.data(), (int32_t)nnzb, S.hpp_rc.data(), hpp.data(), cs));
+  return solve_pattern(c, cs, nb, num_blocks, block_indices, out);
 }
 
 int g2oc_get_stream(g2oc_ctx* c, void** stream) {

@@ -34,6 +34,11 @@
  *   g2oc_solve                      setLambda + BlockSolver::solve + restoreDiagonal
  *   g2oc_solve_block_system         LinearSolver<MatrixType>::solve(A, x, b)
  *                                   (g2o/core/linear_solver.h:64-65) on a caller block matrix
+ *   g2oc_compute_marginals          SparseOptimizer::computeMarginals -> BlockSolver::computeMarginals
+ *                                   -> LinearSolver::solvePattern on Hpp (g2o/core/sparse_optimizer.cpp:585-610,
+ *                                    g2o/core/block_solver.hpp:478-490, g2o/core/linear_solver.h:78-90, 165-173)
+ *   g2oc_solve_pattern_block_system LinearSolver::solvePattern(spinv, blockIndices, A) on a caller
+ *                                   block matrix
  *   g2oc_download / g2oc_set_estimates   vertex estimate read-back / write
  *
  * Conventions
@@ -227,6 +232,14 @@ int g2oc_get_pattern(g2oc_ctx* ctx, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* s
 int g2oc_get_hessian(g2oc_ctx* ctx, double* hpp, double* hll, double* hpl, double* b);
 int g2oc_schur(g2oc_ctx* ctx, double lambda, double* schur_blocks, double* bschur);
 int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations);
+/* Marginal covariances: blocks of Hpp^-1, Hpp the pose part of H built at the
+   current estimates (no lambda; for bundle adjustment the camera blocks only,
+   as BlockSolver::computeMarginals passes _Hpp). block_indices holds
+   num_blocks pairs (row, col) of Hessian block indices (free poses in
+   Hessian order, as vertex hessianIndex()); out gets num_blocks row-major
+   pose_dim x pose_dim blocks. FP64 selected inversion of the tiled Cholesky
+   factor; G2OC_ERR_NOT_PD when Hpp is not positive definite (a free gauge). */
+int g2oc_compute_marginals(g2oc_ctx* ctx, int32_t num_blocks, const int32_t* block_indices, double* out);
 
 /* instrumentation, the device-side counterpart of G2OBatchStatistics /
    ScopedTictoc (g2o/core/batch_stats.h:40-82, g2o/stuff/tictoc.h:59):
@@ -318,6 +331,12 @@ int g2oc_solve_block_system(g2oc_ctx* ctx, int32_t linear_solver, int32_t num_bl
                             const int32_t* block_offsets, int32_t nnzb, const int32_t* block_rc,
                             const double* values, const double* b, double* x,
                             int32_t* iterations);
+/* LinearSolver::solvePattern on a caller block matrix given as for
+   g2oc_solve_block_system: num_blocks pairs (row, col) of block indices in
+   block_indices, the blocks of A^-1 into out (row-major, num_blocks * bs * bs). */
+int g2oc_solve_pattern_block_system(g2oc_ctx* ctx, int32_t nb, const int32_t* block_offsets, int32_t nnzb,
+                                    const int32_t* block_rc, const double* values, int32_t num_blocks,
+                                    const int32_t* block_indices, double* out);
 
 /* g2oc_solve_block_system_static: no counterpart in the reference. The
    block-Jacobi PCG solve of g2oc_solve_block_system (same kernels, same

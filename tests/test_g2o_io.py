@@ -367,3 +367,15 @@ def test_cli_optimizes_a_bundle_adjustment_file(oracle_lib, tmp_path):
     # GPU/oracle difference; the initial perturbations are 0.05 and 0.1
     np.testing.assert_allclose(res.point_estimate, point, rtol=1e-5, atol=3e-4)
     np.testing.assert_allclose(res.pose_estimate, pose, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.gpu
+def test_cli_compute_marginals(tmp_path):
+    g = synth.pose_graph_2d(num_poses=40, num_closures=10, seed=33)
+    src = tmp_path / "pg.g2o"
+    G2oFile.from_graph(g).save(str(src))
+    r = run_cli("-i", "3", "-solver", "gn_cuda_chol", "-computeMarginals", str(src))
+    assert r.returncode == 0, r.stderr
+    nfree = int((g.pose_fixed == 0).sum())
+    assert r.stderr.count("Vertex id:") == nfree
+    assert r.stderr.count("inv block :") == 2 * nfree - 1
