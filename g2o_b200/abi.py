@@ -30,7 +30,8 @@ ERROR_NAMES = {
 }
 
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
-EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV = 1, 2, 3
+EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ = 1, 2, 3, 4
+BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
 ALGO_GAUSS_NEWTON, ALGO_LEVENBERG = 0, 1
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -38,8 +39,8 @@ RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2
 
 POSE_EST_DIM = {POSE_SE2: 3, POSE_SE3: 12, POSE_SE3EXPMAP: 7}
 POSE_DIM = {POSE_SE2: 3, POSE_SE3: 6, POSE_SE3EXPMAP: 6}
-EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2}
-MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2}
+EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2}
+MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -63,6 +64,7 @@ class G2ocGraph(C.Structure):
         ("robust_delta", _dp),
         ("focal_length", C.c_double),
         ("principal_point", C.c_double * 2),
+        ("focal_length_y", C.c_double),
     ]
 
 
@@ -182,6 +184,7 @@ class Graph:
     principal_point: tuple = (0.0, 0.0)
     name: str = ""
     extra: dict = field(default_factory=dict)
+    focal_length_y: Optional[float] = None  # EdgeSE3ProjectXYZ's fy (None: focal_length)
 
     def __post_init__(self):
         self.pose_estimate = np.ascontiguousarray(self.pose_estimate, dtype=np.float64)
@@ -220,7 +223,8 @@ class Graph:
         return Graph(self.pose_type, self.edge_type, c(self.pose_estimate), c(self.edge_vertex),
                      c(self.measurement), c(self.information), c(self.pose_fixed),
                      c(self.point_estimate), c(self.point_fixed), c(self.robust_delta),
-                     self.focal_length, tuple(self.principal_point), self.name, dict(self.extra))
+                     self.focal_length, tuple(self.principal_point), self.name, dict(self.extra),
+                     self.focal_length_y)
 
     def to_c(self) -> G2ocGraph:
         g = G2ocGraph()
@@ -240,6 +244,7 @@ class Graph:
         g.focal_length = float(self.focal_length)
         g.principal_point[0] = float(self.principal_point[0])
         g.principal_point[1] = float(self.principal_point[1])
+        g.focal_length_y = float(self.focal_length if self.focal_length_y is None else self.focal_length_y)
         # keep the numpy arrays alive as long as the struct
         g._owner = self
         return g

@@ -24,7 +24,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
+from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
                   G2ocIterationStats, G2ocKernelStat, G2ocParams, G2ocWindowStats, Graph, POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -221,7 +221,7 @@ class CudaProblem:
 
     @property
     def is_ba(self):
-        return self.graph.edge_type == EDGE_PROJECT_XYZ2UV
+        return self.graph.edge_type in (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
 
     def set_params(self, params: G2ocParams):
         self.params = params
@@ -389,7 +389,7 @@ def split_points(g: Graph, parts: int):
         sub = Graph(g.pose_type, g.edge_type, g.pose_estimate.copy(), ev, pick(g.measurement), pick(g.information),
                     None if g.pose_fixed is None else g.pose_fixed.copy(), g.point_estimate[p0:p1].copy(),
                     None if g.point_fixed is None else g.point_fixed[p0:p1].copy(), pick(g.robust_delta),
-                    g.focal_length, tuple(g.principal_point), f"{g.name}-shard{r}", {})
+                    g.focal_length, tuple(g.principal_point), f"{g.name}-shard{r}", {}, g.focal_length_y)
         out.append((sub, np.arange(p0, p1)))
     return out
 

@@ -39,29 +39,29 @@ __device__ __forceinline__ Dual dsqrt(Dual a) {
 
 // EdgeProjectXYZ2UV::linearizeOplus (g2o/types/sba/edge_project_xyz2uv.cpp:58-97)
 // on dual numbers, with the camera rotation given as a matrix
-__device__ __forceinline__ void ba_jacobians_dual(const Dual R[9], const Dual Xc[3], double fs, Dual Jp[6],
-                                                  Dual Jc[12]) {
-  const Dual f(fs);
+__device__ __forceinline__ void ba_jacobians_dual(const Dual R[9], const Dual Xc[3], double fxs, double fys,
+                                                  Dual Jp[6], Dual Jc[12]) {
+  const Dual fx(fxs), fy(fys);
   const Dual x = Xc[0], y = Xc[1], z = Xc[2], z2 = z * z;
-  const Dual a02 = -x / z * f, a12 = -y / z * f;
+  const Dual a02 = -x / z * fx, a12 = -y / z * fy;
   const Dual iz = Dual(-1.0) / z;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    Jp[c] = iz * (f * R[c] + a02 * R[6 + c]);
-    Jp[3 + c] = iz * (f * R[3 + c] + a12 * R[6 + c]);
+    Jp[c] = iz * (fx * R[c] + a02 * R[6 + c]);
+    Jp[3 + c] = iz * (fy * R[3 + c] + a12 * R[6 + c]);
   }
-  Jc[0] = x * y / z2 * f;
-  Jc[1] = -(Dual(1.0) + (x * x / z2)) * f;
-  Jc[2] = y / z * f;
-  Jc[3] = Dual(-1.0) / z * f;
+  Jc[0] = x * y / z2 * fx;
+  Jc[1] = -(Dual(1.0) + (x * x / z2)) * fx;
+  Jc[2] = y / z * fx;
+  Jc[3] = Dual(-1.0) / z * fx;
   Jc[4] = Dual(0.0);
-  Jc[5] = x / z2 * f;
-  Jc[6] = (Dual(1.0) + y * y / z2) * f;
-  Jc[7] = -x * y / z2 * f;
-  Jc[8] = -x / z * f;
+  Jc[5] = x / z2 * fx;
+  Jc[6] = (Dual(1.0) + y * y / z2) * fy;
+  Jc[7] = -x * y / z2 * fy;
+  Jc[8] = -x / z * fy;
   Jc[9] = Dual(0.0);
-  Jc[10] = Dual(-1.0) / z * f;
-  Jc[11] = y / z2 * f;
+  Jc[10] = Dual(-1.0) / z * fy;
+  Jc[11] = y / z2 * fy;
 }
 
 // Derivative along p of one edge's gradient terms: gp = d/dt (rho' Jp^T Om e)
@@ -98,8 +98,8 @@ __device__ __forceinline__ void ba_edge_hvp(const BAVertices& V, int2 v, double2
     Rd[3 + c] = Dual(R[3 + c], w2 * R[c] - w0 * R[6 + c]);
     Rd[6 + c] = Dual(R[6 + c], w0 * R[3 + c] - w1 * R[c]);
   }
-  const Dual e0 = Dual(z.x) - (Xd[0] / Xd[2] * Dual(V.f) + Dual(V.cx));
-  const Dual e1 = Dual(z.y) - (Xd[1] / Xd[2] * Dual(V.f) + Dual(V.cy));
+  const Dual e0 = Dual(z.x) - (Xd[0] / Xd[2] * Dual(V.fx) + Dual(V.cx));
+  const Dual e1 = Dual(z.y) - (Xd[1] / Xd[2] * Dual(V.fy) + Dual(V.cy));
   const Dual oe0 = Dual(om.x) * e0 + Dual(om.y) * e1;
   const Dual oe1 = Dual(om.y) * e0 + Dual(om.z) * e1;
   Dual rho1(1.0);
@@ -110,7 +110,7 @@ __device__ __forceinline__ void ba_edge_hvp(const BAVertices& V, int2 v, double2
   }
   const Dual g0 = rho1 * oe0, g1 = rho1 * oe1;
   Dual Jp[6], Jc[12];
-  ba_jacobians_dual(Rd, Xd, V.f, Jp, Jc);
+  ba_jacobians_dual(Rd, Xd, V.fx, V.fy, Jp, Jc);
 #pragma unroll
   for (int i = 0; i < 3; ++i) gp[i] = (Jp[i] * g0 + Jp[3 + i] * g1).d;
 #pragma unroll
@@ -217,7 +217,7 @@ static __global__ void ba_backward_edges(BAEdges E, BAVertices V, const int* pos
   double e[2], Xc[3], chi2, w;
   ba_edge_error(V, vv, E.z[k], om, e, Xc, chi2, w);
   double Jp[6], Jc[12];
-  ba_jacobians_from_xc(V.cam + (size_t)vv.y * 8, Xc, V.f, Jp, Jc);
+  ba_jacobians_from_xc(V.cam + (size_t)vv.y * 8, Xc, V.fx, V.fy, Jp, Jc);
   double u0 = 0.0, u1 = 0.0;
   const int h = pose_h[vv.y], l = point_l[vv.x];
   if (h >= 0) {

@@ -48,7 +48,7 @@ struct BAVertices {
   double* pt;             // P x 4: x y z pad
   const int* free_pose;   // Cf: pose index of Hessian row h
   const int* free_point;  // Pf: point index of landmark l
-  double f, cx, cy;
+  double fx, fy, cx, cy;  // EdgeProjectXYZ2UV: fx = fy = focal_length
 };
 
 // Per-edge residual, robust weight and weighted error in FP64.
@@ -60,8 +60,8 @@ __device__ __forceinline__ void ba_edge_error(const BAVertices& V, int2 v, doubl
   const double* cam = V.cam + (size_t)v.y * 8;
   const double* X = V.pt + (size_t)v.x * 4;
   ba_transform(cam, X, Xc);
-  e[0] = z.x - (Xc[0] / Xc[2] * V.f + V.cx);
-  e[1] = z.y - (Xc[1] / Xc[2] * V.f + V.cy);
+  e[0] = z.x - (Xc[0] / Xc[2] * V.fx + V.cx);
+  e[1] = z.y - (Xc[1] / Xc[2] * V.fy + V.cy);
   const double t0 = om.x * e[0] + om.y * e[1];
   const double t1 = om.y * e[0] + om.z * e[1];
   chi2 = e[0] * t0 + e[1] * t1;
@@ -112,7 +112,7 @@ static __global__ void ba_jacobians_kernel(BAEdges E, BAVertices V, double* jp, 
   double Xc[3];
   ba_transform(cam, V.pt + (size_t)v.x * 4, Xc);
   double Jp[6], Jc[12];
-  ba_jacobians_from_xc(cam, Xc, V.f, Jp, Jc);
+  ba_jacobians_from_xc(cam, Xc, V.fx, V.fy, Jp, Jc);
   for (int i = 0; i < 6; ++i) jp[6 * k + i] = Jp[i];
   for (int i = 0; i < 12; ++i) jc[12 * k + i] = Jc[i];
 }
@@ -140,7 +140,7 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
     double Jpd[6], Jcd[12];
-    ba_jacobians_from_xc(cam, Xc, V.f, Jpd, Jcd);
+    ba_jacobians_from_xc(cam, Xc, V.fx, V.fy, Jpd, Jcd);
     Real Jp[6], Jc[12];
 #pragma unroll
     for (int i = 0; i < 6; ++i) Jp[i] = (Real)Jpd[i];
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) ba_landmark_warp(BAEdges E, BAVertices V,
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jpd[6], Jcd[12];
-    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jpd, Jcd);
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jpd, Jcd);
     Real Jp[6], Jc[12];
 #pragma unroll
     for (int i = 0; i < 6; ++i) Jp[i] = (Real)Jpd[i];
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
     ba_edge_error(V, v, z, om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
     double Jpd[6], Jcd[12];
-    ba_jacobians_from_xc(cam, Xc, V.f, Jpd, Jcd);
+    ba_jacobians_from_xc(cam, Xc, V.fx, V.fy, Jpd, Jcd);
     Real Jc[12];
 #pragma unroll
     for (int i = 0; i < 12; ++i) Jc[i] = (Real)Jcd[i];
@@ -811,7 +811,7 @@ static __global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];
-    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jp, Jc);
     double u0 = Jp[0] * xl[0] + Jp[1] * xl[1] + Jp[2] * xl[2];
     double u1 = Jp[3] * xl[0] + Jp[4] * xl[1] + Jp[5] * xl[2];
     const int h = pose_h[v.y];
@@ -852,7 +852,7 @@ static __global__ void ba_resid64_landmark_warp(BAEdges E, BAVertices V, const i
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];
-    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jp, Jc);
     double u0 = Jp[0] * xl[0] + Jp[1] * xl[1] + Jp[2] * xl[2];
     double u1 = Jp[3] * xl[0] + Jp[4] * xl[1] + Jp[5] * xl[2];
     const int h = pose_h[v.y];
@@ -902,7 +902,7 @@ __global__ void __launch_bounds__(THREADS) ba_resid64_camera(BACamEdges CE, BAVe
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];
-    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.f, Jp, Jc);
+    ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jp, Jc);
     double u0 = 0.0, u1 = 0.0;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {

@@ -197,29 +197,31 @@ G2OC_HD void ba_error(const T* cam, const T* X, const T* z, T f, T cx, T cy, T e
 
 // Jp (2x3) and Jc (2x6, columns omega then upsilon)
 template <typename T>
-G2OC_HD void ba_jacobians_from_xc(const T* cam, const T Xc[3], T f, T Jp[6], T Jc[12]) {
+G2OC_HD void ba_jacobians_from_xc(const T* cam, const T Xc[3], T fx, T fy, T Jp[6], T Jc[12]) {
+  // fx = fy = CameraParameters::focal_length for EdgeProjectXYZ2UV; the
+  // members fx, fy of EdgeSE3ProjectXYZ (g2o/types/sba/edge_project_xyz.cpp:59-93)
   const T x = Xc[0], y = Xc[1], z = Xc[2], z2 = z * z;
   T R[9];
   quat_to_rot(Q4<T>{cam[0], cam[1], cam[2], cam[3]}, R);
-  const T a02 = -x / z * f, a12 = -y / z * f;
+  const T a02 = -x / z * fx, a12 = -y / z * fy;
   const T iz = T(-1) / z;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    Jp[c] = iz * (f * R[c] + a02 * R[6 + c]);
-    Jp[3 + c] = iz * (f * R[3 + c] + a12 * R[6 + c]);
+    Jp[c] = iz * (fx * R[c] + a02 * R[6 + c]);
+    Jp[3 + c] = iz * (fy * R[3 + c] + a12 * R[6 + c]);
   }
-  Jc[0] = x * y / z2 * f;
-  Jc[1] = -(T(1) + (x * x / z2)) * f;
-  Jc[2] = y / z * f;
-  Jc[3] = T(-1) / z * f;
+  Jc[0] = x * y / z2 * fx;
+  Jc[1] = -(T(1) + (x * x / z2)) * fx;
+  Jc[2] = y / z * fx;
+  Jc[3] = T(-1) / z * fx;
   Jc[4] = T(0);
-  Jc[5] = x / z2 * f;
-  Jc[6] = (T(1) + y * y / z2) * f;
-  Jc[7] = -x * y / z2 * f;
-  Jc[8] = -x / z * f;
+  Jc[5] = x / z2 * fx;
+  Jc[6] = (T(1) + y * y / z2) * fy;
+  Jc[7] = -x * y / z2 * fy;
+  Jc[8] = -x / z * fy;
   Jc[9] = T(0);
-  Jc[10] = T(-1) / z * f;
-  Jc[11] = y / z2 * f;
+  Jc[10] = T(-1) / z * fy;
+  Jc[11] = y / z2 * fy;
 }
 
 // --------------------------------------------------------------- SE2 edge

@@ -143,7 +143,7 @@ struct g2oc_ctx {
   bool uploaded = false;
   bool last_upload_reused = false;  // the last g2oc_upload kept the structure (same topology)
   bool system_built = false;
-  double f = 1, cx = 0, cy = 0;
+  double fx = 1, fy = 1, cx = 0, cy = 0;
   // vertex state
   g2oc::DBuf<double> pose, point, pose_bak, point_bak, pose_init, point_init;
   g2oc::DBuf<int> oplus_count, free_pose, free_point, pose_h, point_l;
@@ -185,6 +185,7 @@ struct g2oc_ctx {
   g2oc::PinnedVec<g2oc::DevScalars> h_sc;
   g2oc::PinnedVec<g2oc::PcgState> h_pcg;
   cudaEvent_t ev_read = nullptr;
+  cudaEvent_t coop_done = nullptr;  // completion of this context's last grid-barrier launch
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
   g2oc::DBuf<int> win_chunk_w, win_chunk_e0, win_chunk_ptr;  // chi2 edge chunks (kWinChi2Chunk)
   g2oc::DBuf<double> win_chunk_sum;
@@ -262,6 +263,16 @@ struct g2oc_ctx {
     return e;
   }
   void span(cudaEvent_t a, double* out, double* out2 = nullptr) { spans.push_back({a, mark(), out, out2}); }
+  // forget the recorded spans without writing their times: after a call that
+  // failed half-way their targets (the call's own stats) no longer exist
+  void drop_spans() {
+    for (auto& sp : spans) {
+      event_pool.push_back(sp.a);
+      event_pool.push_back(sp.b);
+    }
+    spans.clear();
+    cur_stats = nullptr;
+  }
   void resolve_spans() {
     if (spans.empty()) return;
     cudaEventSynchronize(spans.back().b);
@@ -289,11 +300,12 @@ struct g2oc_ctx {
   }
   ~g2oc_ctx() {
     if (ev_read) cudaEventDestroy(ev_read);
+    if (coop_done) cudaEventDestroy(coop_done);
     if (win_graph) cudaGraphExecDestroy(win_graph);
     eng.reset();
     chol.reset();
     flush_timing();
-    resolve_spans();
+    drop_spans();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -304,7 +316,8 @@ struct g2oc_ctx {
     V.pt = point.p;
     V.free_pose = free_pose.p;
     V.free_point = free_point.p;
-    V.f = f;
+    V.fx = fx;
+    V.fy = fy;
     V.cx = cx;
     V.cy = cy;
     return V;
@@ -357,6 +370,57 @@ struct LaunchScope {
 #define G2OC_K(kid) for (::g2oc::LaunchScope _ls(c, ::g2oc::kid); !_ls.done; _ls.done = true)
 
 // ------------------------------------------------------------ PCG driver
+// Grid-barrier (cooperative) launches of different contexts on one device
+// run one after another. Each such kernel sizes its grid to fill the GPU and
+// its barrier needs every CTA resident at once, which two of them sharing the
+// SMs (contexts on several host threads, or ranks emulated on one GPU) need
+// not get: each waits for CTAs the other holds until its bounded spin gives
+// up. While more than one context lives on the device, every cooperative
+// launch therefore waits (on the device, cudaStreamWaitEvent) for the
+// previous one of any context; the chain follows the host order of the
+// launches, so it cannot form a cycle. One context alone pays nothing.
+struct CoopChain {
+  std::mutex m;
+  int live = 0;               // contexts on this device
+  const g2oc_ctx* owner = nullptr;
+  cudaEvent_t last = nullptr;  // the owner's coop_done, recorded after its last launch
+};
+static CoopChain g_coop[64];
+
+static void coop_register(g2oc_ctx* c, int delta) {
+  if (c->device < 0 || c->device >= 64) return;
+  CoopChain& ch = g_coop[c->device];
+  std::lock_guard<std::mutex> lk(ch.m);
+  ch.live += delta;
+  if (delta < 0 && ch.owner == c) {
+    ch.owner = nullptr;
+    ch.last = nullptr;
+  }
+}
+
+static int coop_launch(g2oc_ctx* c, const void* fn, int grid, int threads, void** args) {
+  cudaStream_t st = c->stream;
+  if (c->device < 0 || c->device >= 64) {
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+    return G2OC_OK;
+  }
+  CoopChain& ch = g_coop[c->device];
+  std::lock_guard<std::mutex> lk(ch.m);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  G2OC_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
+  if (ch.live <= 1 || cap != cudaStreamCaptureStatusNone) {  // alone, or inside a graph capture
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+    return G2OC_OK;
+  }
+  if (!c->coop_done) G2OC_CUDA_TRY(cudaEventCreateWithFlags(&c->coop_done, cudaEventDisableTiming));
+  if (ch.last && ch.owner != c) G2OC_CUDA_TRY(cudaStreamWaitEvent(st, ch.last, 0));
+  G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+  G2OC_CUDA_TRY(cudaEventRecord(c->coop_done, st));
+  ch.owner = c;
+  ch.last = c->coop_done;
+  return G2OC_OK;
+}
+
 // Form of the PCG solve: one cooperative launch over dense tiles when the
 // matrix is nearly full (6x6 blocks), else one cooperative launch over the
 // sparse blocks. G2OC_PCG=sparse forces the sparse launch, G2OC_PCG=kernels
@@ -447,7 +511,6 @@ template <typename Real, int BS>
 static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs,
                               double* xout, double* r, double* s, double* d, double* tbuf, double* cpart,
                               bool fixed_d0) {
-  cudaStream_t st = c->stream;
   int& grid = c->pcg_grid[(sizeof(Real) == 4 ? 2 : 0) + (BS == 6 ? 1 : 0)];
   if (grid == 0) {
     int per_sm = 0, sms = 0;
@@ -475,10 +538,7 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
   void* args[] = {&a,    &chunk_ptr, &chunk_row, &nchunks, &minv,    &rhs,    &xout, &r,       &s,
                   &d,    &tbuf,      &cpart,     &part_dq, &part_rs, &stp,    &tol,  &max_iter, &abs_tol,
                   &fixed};
-  G2OC_K(K_PCG_SOLVE) {
-    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_persistent<Real, BS>, dim3(grid),
-                                              dim3(kPcgThreads), args, 0, st));
-  }
+  G2OC_K(K_PCG_SOLVE) { G2OC_TRY(coop_launch(c, (const void*)pcg_solve_persistent<Real, BS>, grid, kPcgThreads, args)); }
   return G2OC_OK;
 }
 
@@ -486,7 +546,6 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
 template <typename Real>
 static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* minv, const double* rhs, double* xout,
                          double* r, double* s, double* dbuf0, double* dbuf1, double* part, bool fixed_d0) {
-  cudaStream_t st = c->stream;
   int& grid = c->tile_grid[sizeof(Real) == 4 ? 1 : 0];
   if (grid == 0) {
     int per_sm = 0, sms = 0;
@@ -512,10 +571,7 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
   PcgState* stp = c->pcg.p;
   void* args[] = {&tiles, &tij,  &ntiles, &nbt,  &nb,      &minv,    &rhs, &xout,     &r,       &s,
                   &dbuf0, &dbuf1, &part,  &part_dq, &part_rs, &stp, &tol, &max_iter, &abs_tol, &fixed};
-  G2OC_K(K_PCG_TILES) {
-    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)pcg_solve_tiles<Real>, dim3(grid), dim3(kTileThreads),
-                                              args, 0, st));
-  }
+  G2OC_K(K_PCG_TILES) { G2OC_TRY(coop_launch(c, (const void*)pcg_solve_tiles<Real>, grid, kTileThreads, args)); }
   return G2OC_OK;
 }
 
@@ -1484,6 +1540,7 @@ int g2oc_create(int device, g2oc_ctx** out) {
   G2OC_CUDA_TRY(cudaMemsetAsync(c->flag.p, 0, sizeof(int), c->stream));
   G2OC_TRY(reset_pcg(c.get()));
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  coop_register(c.get(), +1);
   *out = c.release();
   return G2OC_OK;
 }
@@ -1492,6 +1549,7 @@ void g2oc_destroy(g2oc_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  coop_register(c, -1);
   delete c;
 }
 
@@ -1715,7 +1773,8 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
   const int na = (int)S.act.size();
-  c->f = g->focal_length;
+  c->fx = g->focal_length;
+  c->fy = g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? g->focal_length_y : g->focal_length;
   c->cx = g->principal_point[0];
   c->cy = g->principal_point[1];
   if (S.ba) {
@@ -1885,8 +1944,7 @@ int g2oc_set_sharding(g2oc_ctx* c, int32_t rank, int32_t world, g2oc_allreduce_f
   return G2OC_OK;
 }
 
-int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int* done) {
-  G2OC_TRY(check_ctx(c, true));
+static int optimize_impl(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int* done) {
   if (iterations < 0) {
     set_error("iterations < 0");
     return G2OC_ERR_INVALID_ARGUMENT;
@@ -1913,8 +1971,7 @@ int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int*
   return G2OC_OK;
 }
 
-int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* result) {
-  G2OC_TRY(check_ctx(c, true));
+static int iterate_impl(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* result) {
   if (iteration < 0 || !result) {
     set_error("iteration < 0 or result is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
@@ -1932,6 +1989,22 @@ int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* r
   if (stats) *stats = stv;
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return G2OC_OK;
+}
+
+// the iteration paths record phase-time spans aimed at a stats record on
+// their own stack; a failure half-way must not leave those behind
+int g2oc_optimize(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stats, int* done) {
+  G2OC_TRY(check_ctx(c, true));
+  const int st = optimize_impl(c, iterations, stats, done);
+  if (st != G2OC_OK) c->drop_spans();
+  return st;
+}
+
+int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* result) {
+  G2OC_TRY(check_ctx(c, true));
+  const int st = iterate_impl(c, iteration, stats, result);
+  if (st != G2OC_OK) c->drop_spans();
+  return st;
 }
 
 int g2oc_chi2(g2oc_ctx* c, double* chi2, double* robust) {
@@ -2211,11 +2284,15 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   }
   for (int i = 0; i < num_windows; ++i) {
     const g2oc_graph& g = w[i];
-    if (g.pose_type != G2OC_POSE_SE3EXPMAP || g.edge_type != G2OC_EDGE_PROJECT_XYZ2UV) {
-      set_error("window %d: batched windows are bundle adjustments (VertexSE3Expmap, EdgeProjectXYZ2UV)", i);
+    if (g.pose_type != G2OC_POSE_SE3EXPMAP ||
+        (g.edge_type != G2OC_EDGE_PROJECT_XYZ2UV && g.edge_type != G2OC_EDGE_SE3_PROJECT_XYZ)) {
+      set_error("window %d: batched windows are bundle adjustments (VertexSE3Expmap, EdgeProjectXYZ2UV or "
+                "EdgeSE3ProjectXYZ)", i);
       return G2OC_ERR_NOT_SUPPORTED;
     }
-    if (g.focal_length != w[0].focal_length || g.principal_point[0] != w[0].principal_point[0] ||
+    const double fy_i = g.edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? g.focal_length_y : g.focal_length;
+    const double fy_0 = w[0].edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? w[0].focal_length_y : w[0].focal_length;
+    if (g.focal_length != w[0].focal_length || fy_i != fy_0 || g.principal_point[0] != w[0].principal_point[0] ||
         g.principal_point[1] != w[0].principal_point[1]) {
       set_error("window %d: every window must use the same camera parameters", i);
       return G2OC_ERR_NOT_SUPPORTED;
@@ -2293,13 +2370,14 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   packed.num_points = P;
   packed.point_estimate = point.data();
   packed.point_fixed = qf.data();
-  packed.edge_type = G2OC_EDGE_PROJECT_XYZ2UV;
+  packed.edge_type = w[0].edge_type;
   packed.num_edges = E;
   packed.edge_vertex = ev.data();
   packed.measurement = meas.data();
   packed.information = info.data();
   packed.robust_delta = robust ? delta.data() : nullptr;
   packed.focal_length = w[0].focal_length;
+  packed.focal_length_y = w[0].focal_length_y;
   packed.principal_point[0] = w[0].principal_point[0];
   packed.principal_point[1] = w[0].principal_point[1];
   // a re-upload of the same windows (same topology, same window ranges) keeps

@@ -544,8 +544,8 @@ int build_structure(const g2oc_graph* g, Structure& s) {
     set_error("graph is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
-  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 3 ||
+  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 4 ||
       (g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2) ||
       (g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3) ||
       ba != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {

@@ -23,7 +23,7 @@ import math
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3, POSE_SE2, POSE_SE3,
+from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_PROJECT_XYZ, EDGE_SE3, POSE_SE2, POSE_SE3,
                   POSE_SE3EXPMAP, Graph)
 
 SEED_BASE = 20261203
@@ -222,8 +222,11 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
                       box=(10.0, 10.0, 5.0), mean_obs=5.0, min_obs=2, max_obs=20,
                       focal=500.0, width=640, height_px=480, pixel_noise=1.0, outlier_ratio=0.01,
                       pose_noise=(0.05, 0.01), point_noise=0.1, num_fixed=2,
-                      seed=SEED_BASE + 2, chunk=2048):
-    """Ring of inward-looking cameras observing a box of points (ba_demo form)."""
+                      seed=SEED_BASE + 2, chunk=2048, focal_y=None):
+    """Ring of inward-looking cameras observing a box of points (ba_demo form).
+    With focal_y the edges are EdgeSE3ProjectXYZ with fx = focal, fy = focal_y
+    (ORB-SLAM's form); otherwise EdgeProjectXYZ2UV with one focal length."""
+    fy = focal if focal_y is None else focal_y
     rng = np.random.default_rng(seed)
     az = 2 * np.pi * np.arange(num_cameras) / num_cameras
     centers = np.stack([ring_radius * np.cos(az), ring_radius * np.sin(az), np.full(num_cameras, height)], 1)
@@ -240,7 +243,7 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
         z = Xc[..., 2]
         with np.errstate(divide="ignore", invalid="ignore"):
             u = focal * Xc[..., 0] / z + cx
-            v = focal * Xc[..., 1] / z + cy
+            v = fy * Xc[..., 1] / z + cy
         vis = (z > 0.5) & (u >= 0) & (u < width) & (v >= 0) & (v < height_px)
         keys = rng.random(vis.shape)
         keys[~vis] = 2.0
@@ -281,11 +284,11 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     X0 = Xt + rng.normal(0.0, point_noise, size=Xt.shape)
     E = len(pts)
     info = np.tile(np.eye(2).reshape(1, 4), (E, 1))
-    g = Graph(POSE_SE3EXPMAP, EDGE_PROJECT_XYZ2UV, pose_est,
+    g = Graph(POSE_SE3EXPMAP, EDGE_PROJECT_XYZ2UV if focal_y is None else EDGE_SE3_PROJECT_XYZ, pose_est,
               np.stack([pts, cams], 1).astype(np.int32), uv, info, pose_fixed=fixed,
               point_estimate=X0, point_fixed=np.zeros(len(Xt), np.uint8),
               robust_delta=np.full(E, math.sqrt(5.991)), focal_length=focal,
-              principal_point=(cx, cy), name=f"bundle_adjustment_{num_cameras}x{len(Xt)}")
+              principal_point=(cx, cy), name=f"bundle_adjustment_{num_cameras}x{len(Xt)}", focal_length_y=focal_y)
     g.extra["truth_pose"] = np.concatenate([tcw, _rot_to_quat(Rcw)], axis=1)
     g.extra["truth_point"] = Xt
     g.extra["outliers"] = out

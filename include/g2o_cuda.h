@@ -66,7 +66,7 @@
 extern "C" {
 #endif
 
-#define G2OC_ABI_VERSION 1
+#define G2OC_ABI_VERSION 2
 
 /* status codes */
 #define G2OC_OK 0
@@ -90,6 +90,8 @@ extern "C" {
 #define G2OC_EDGE_SE2 1            /* EdgeSE2(VertexSE2, VertexSE2), D=3, measurement (x,y,theta) */
 #define G2OC_EDGE_SE3 2            /* EdgeSE3(VertexSE3, VertexSE3), D=6, measurement Isometry3 (12) */
 #define G2OC_EDGE_PROJECT_XYZ2UV 3 /* EdgeProjectXYZ2UV(VertexPointXYZ, VertexSE3Expmap), D=2 */
+#define G2OC_EDGE_SE3_PROJECT_XYZ 4 /* EdgeSE3ProjectXYZ(VertexPointXYZ, VertexSE3Expmap), D=2, with
+                                     fx = focal_length, fy = focal_length_y, (cx, cy) = principal_point */
 
 /* algorithm / linear solver / precision */
 #define G2OC_ALGO_GAUSS_NEWTON 0
@@ -123,8 +125,9 @@ typedef struct g2oc_graph {
   const double* measurement;   /* num_edges * {3, 12, 2} */
   const double* information;   /* num_edges * D*D, row-major, symmetric */
   const double* robust_delta;  /* num_edges Huber deltas; <= 0 or NULL: no kernel */
-  double focal_length;         /* CameraParameters (PROJECT_XYZ2UV only) */
+  double focal_length;         /* CameraParameters (PROJECT_XYZ2UV); fx of SE3_PROJECT_XYZ */
   double principal_point[2];
+  double focal_length_y;       /* fy of SE3_PROJECT_XYZ (EdgeSE3ProjectXYZ::fy); ignored otherwise */
 } g2oc_graph;
 
 typedef struct g2oc_params {

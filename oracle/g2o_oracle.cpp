@@ -364,20 +364,22 @@ inline SE2v se2_mul(const SE2v& a, const SE2v& b) {
 }
 
 // EdgeProjectXYZ2UV (g2o/types/sba/edge_project_xyz2uv.cpp:50-97), vertex0 =
-// point, vertex1 = camera; CameraParameters::cam_map (parameter_cameraparameters.cpp:59-65)
-void ba_error(const double* cam7, const double* X, const double* z, double f, double cx, double cy,
+// point, vertex1 = camera; CameraParameters::cam_map (parameter_cameraparameters.cpp:59-65),
+// fx = fy = focal_length. EdgeSE3ProjectXYZ (g2o/types/sba/edge_project_xyz.cpp:43-100)
+// is the same with its own fx, fy, cx, cy.
+void ba_error(const double* cam7, const double* X, const double* z, double fx, double fy, double cx, double cy,
               double e[2]) {
   SE3Q T = se3q_load(cam7);
   double Xc[3];
   quat_rotate(T.q, X, Xc);
   Xc[0] += T.t[0]; Xc[1] += T.t[1]; Xc[2] += T.t[2];
-  const double u = Xc[0] / Xc[2] * f + cx;
-  const double v = Xc[1] / Xc[2] * f + cy;
+  const double u = Xc[0] / Xc[2] * fx + cx;
+  const double v = Xc[1] / Xc[2] * fy + cy;
   e[0] = z[0] - u;
   e[1] = z[1] - v;
 }
 
-void ba_jacobians(const double* cam7, const double* X, double f, double Jp[6], double Jc[12]) {
+void ba_jacobians(const double* cam7, const double* X, double fx, double fy, double Jp[6], double Jc[12]) {
   SE3Q T = se3q_load(cam7);
   double Xc[3];
   quat_rotate(T.q, X, Xc);
@@ -385,22 +387,22 @@ void ba_jacobians(const double* cam7, const double* X, double f, double Jp[6], d
   const double x = Xc[0], y = Xc[1], z = Xc[2], z2 = z * z;
   double R[9];
   quat_to_rot(T.q, R);
-  const double tmp[6] = {f, 0, -x / z * f, 0, f, -y / z * f};
+  const double tmp[6] = {fx, 0, -x / z * fx, 0, fy, -y / z * fy};
   for (int r = 0; r < 2; ++r)
     for (int c = 0; c < 3; ++c)
       Jp[r * 3 + c] = -1. / z * (tmp[r * 3] * R[c] + tmp[r * 3 + 1] * R[3 + c] + tmp[r * 3 + 2] * R[6 + c]);
-  Jc[0] = x * y / z2 * f;
-  Jc[1] = -(1 + (x * x / z2)) * f;
-  Jc[2] = y / z * f;
-  Jc[3] = -1. / z * f;
+  Jc[0] = x * y / z2 * fx;
+  Jc[1] = -(1 + (x * x / z2)) * fx;
+  Jc[2] = y / z * fx;
+  Jc[3] = -1. / z * fx;
   Jc[4] = 0;
-  Jc[5] = x / z2 * f;
-  Jc[6] = (1 + y * y / z2) * f;
-  Jc[7] = -x * y / z2 * f;
-  Jc[8] = -x / z * f;
+  Jc[5] = x / z2 * fx;
+  Jc[6] = (1 + y * y / z2) * fy;
+  Jc[7] = -x * y / z2 * fy;
+  Jc[8] = -x / z * fy;
   Jc[9] = 0;
-  Jc[10] = -1. / z * f;
-  Jc[11] = y / z2 * f;
+  Jc[10] = -1. / z * fy;
+  Jc[11] = y / z2 * fy;
 }
 
 // EdgeSE2 (g2o/types/slam2d/edge_se2.h:46-59, edge_se2.cpp:63-83)
@@ -762,7 +764,8 @@ struct orc_problem {
   std::vector<uint8_t> pose_fixed, point_fixed;
   std::vector<int> ev;
   std::vector<double> meas, info, delta;
-  double f = 1, cx = 0, cy = 0;
+  double fx = 1, fy = 1, cx = 0, cy = 0;
+  bool ba = false;  // EdgeProjectXYZ2UV or EdgeSE3ProjectXYZ
   std::vector<int> oplus_count;  // VertexSE3 orthogonalization counter
   // active sets and index mapping (sparse_optimizer.cpp:175-287)
   std::vector<int> act;  // active edge ids
@@ -799,8 +802,8 @@ inline double* point_ptr(orc_problem* p, int i) { return p->point.data() + (size
 void compute_edge_error(orc_problem* p, int e, double* out) {
   const int v0 = p->ev[2 * e], v1 = p->ev[2 * e + 1];
   const double* m = p->meas.data() + (size_t)e * p->md;
-  if (p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV)
-    ba_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->f, p->cx, p->cy, out);
+  if (p->ba)
+    ba_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->fx, p->fy, p->cx, p->cy, out);
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out);
   else
@@ -810,8 +813,8 @@ void compute_edge_error(orc_problem* p, int e, double* out) {
 void compute_edge_jac(orc_problem* p, int e, double* J0, double* J1) {
   const int v0 = p->ev[2 * e], v1 = p->ev[2 * e + 1];
   const double* m = p->meas.data() + (size_t)e * p->md;
-  if (p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV)
-    ba_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->f, J0, J1);
+  if (p->ba)
+    ba_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->fx, p->fy, J0, J1);
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1);
   else
@@ -860,7 +863,7 @@ void active_chi2(orc_problem* p, double* chi2, double* robust) {
 
 int build_structure(orc_problem* p) {
   // active edges: all vertices present, not all fixed (sparse_optimizer.cpp:233-258)
-  const bool ba = p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
+  const bool ba = p->ba;
   std::vector<char> pa(p->C, 0), qa(p->P, 0);
   p->act.clear();
   for (int e = 0; e < p->E; ++e) {
@@ -1036,7 +1039,7 @@ void build_system(orc_problem* p) {
   std::fill(p->b.begin(), p->b.end(), 0.0);
   const int na = (int)p->act.size();
   const int D = p->D, pd = p->pd;
-  const bool ba = p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
+  const bool ba = p->ba;
   const int d0 = ba ? 3 : pd, d1 = pd;
   // linearize in parallel into per-edge buffers, then scatter in edge order
   std::vector<double> J0((size_t)na * D * d0), J1((size_t)na * D * d1);
@@ -1415,8 +1418,8 @@ int orc_set_threads(int n) {
 int orc_create(const g2oc_graph* g, orc_problem** out) {
   if (!g || !out) return G2OC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 3) return G2OC_ERR_BAD_GRAPH;
+  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 4) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2)) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3)) return G2OC_ERR_BAD_GRAPH;
   if (ba != (g->pose_type == G2OC_POSE_SE3EXPMAP)) return G2OC_ERR_BAD_GRAPH;
@@ -1451,7 +1454,9 @@ int orc_create(const g2oc_graph* g, orc_problem** out) {
   p->meas.assign(g->measurement, g->measurement + (size_t)p->E * p->md);
   p->info.assign(g->information, g->information + (size_t)p->E * p->D * p->D);
   if (g->robust_delta) p->delta.assign(g->robust_delta, g->robust_delta + p->E);
-  p->f = g->focal_length;
+  p->ba = ba;
+  p->fx = g->focal_length;
+  p->fy = g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? g->focal_length_y : g->focal_length;
   p->cx = g->principal_point[0];
   p->cy = g->principal_point[1];
   p->oplus_count.assign(p->C, 0);
@@ -1524,7 +1529,7 @@ int orc_errors(orc_problem* p, double* out) {
 
 int orc_jacobians(orc_problem* p, double* j0, double* j1) {
   if (!p || !j0 || !j1) return G2OC_ERR_INVALID_ARGUMENT;
-  const bool ba = p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
+  const bool ba = p->ba;
   const int d0 = ba ? 3 : p->pd, d1 = p->pd, D = p->D;
   for (size_t k = 0; k < p->act.size(); ++k)
     compute_edge_jac(p, p->act[k], j0 + k * D * d0, j1 + k * D * d1);
@@ -1533,7 +1538,7 @@ int orc_jacobians(orc_problem* p, double* j0, double* j1) {
 
 int orc_numeric_jacobians(orc_problem* p, double* j0, double* j1) {
   if (!p || !j0 || !j1) return G2OC_ERR_INVALID_ARGUMENT;
-  const bool ba = p->edge_type == G2OC_EDGE_PROJECT_XYZ2UV;
+  const bool ba = p->ba;
   const int d0 = ba ? 3 : p->pd, d1 = p->pd, D = p->D;
   const double delta = 1e-9, scalar = 1 / (2 * delta);
   for (size_t k = 0; k < p->act.size(); ++k) {

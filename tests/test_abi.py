@@ -24,6 +24,7 @@ int main(void) {
   printf("g2oc_graph %zu\n", sizeof(g2oc_graph));
   F(g2oc_graph, pose_estimate) F(g2oc_graph, num_points) F(g2oc_graph, edge_vertex)
   F(g2oc_graph, robust_delta) F(g2oc_graph, focal_length) F(g2oc_graph, principal_point)
+  F(g2oc_graph, focal_length_y)
   printf("g2oc_params %zu\n", sizeof(g2oc_params));
   F(g2oc_params, pcg_tolerance) F(g2oc_params, initial_lambda) F(g2oc_params, refine_tolerance)
   printf("g2oc_iteration_stats %zu\n", sizeof(g2oc_iteration_stats));
@@ -61,7 +62,7 @@ def test_library_exports_every_declared_symbol(cuda_lib):
     assert len(names) >= 20
     for n in names:
         assert hasattr(cuda_lib, n), n
-    assert cuda_lib.g2oc_abi_version() == 1
+    assert cuda_lib.g2oc_abi_version() == 2
 
 
 def test_factory_lists_and_constructs():

@@ -364,3 +364,54 @@ def test_invalid_graphs_are_refused_at_upload(backend):
     with pytest.raises(backend.G2ocError) as e:
         backend.CudaProblem(fixed)
     assert e.value.status == 2
+
+
+# ------------------------------------------- EdgeSE3ProjectXYZ (fx != fy)
+def test_se3_project_xyz_matches_oracle(backend, oracle_lib):
+    """EdgeSE3ProjectXYZ (g2o/types/sba/edge_project_xyz.cpp:43-100) on the
+    same kernels as EdgeProjectXYZ2UV with its own fx, fy: errors, Jacobians,
+    Hessian and a 20-iteration LM trajectory against the FP64 oracle."""
+    from g2o_b200.abi import EDGE_SE3_PROJECT_XYZ
+    g = small_ba(seed=21, focal_y=455.0)
+    assert g.edge_type == EDGE_SE3_PROJECT_XYZ
+    o, c = both(backend, oracle_lib, g)
+    assert relnorm(c.errors(), o.errors()) < 1e-12
+    j0c, j1c = c.jacobians()
+    j0o, j1o = o.jacobians()
+    assert rel_block_err(j0c, j0o) < 1e-12 and rel_block_err(j1c, j1o) < 1e-12
+    o.build_system()
+    c.build_system()
+    hc, ho = c.hessian(), o.hessian()
+    for a, b in zip(hc[:3], ho[:3]):
+        assert rel_block_err(a, b) < 1e-10
+    do, so = o.optimize(20)
+    dc, sc = c.optimize(20)
+    assert do == dc == 20
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"]
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["chi2"], b["chi2"])
+    # the same graph read as EdgeProjectXYZ2UV (fy := fx) is a different problem
+    g2 = g.copy()
+    g2.focal_length_y = g.focal_length
+    assert abs(backend.CudaProblem(g2).chi2()[0] - c.chi2()[0]) > 1e-3 * c.chi2()[0]
+
+
+def test_se3_project_xyz_windows_and_mixed(backend, oracle_lib):
+    from g2o_b200.abi import EDGE_SE3_PROJECT_XYZ, LINEAR_CHOLESKY
+    ws = [synth.bundle_adjustment(num_cameras=12 + 2 * i, num_points=300 + 50 * i, seed=60 + i, focal_y=455.0,
+                                  num_fixed=1) for i in range(4)]
+    assert all(w.edge_type == EDGE_SE3_PROJECT_XYZ for w in ws)
+    cw = backend.CudaWindows(ws)
+    st = cw.optimize(10)
+    for w, g in enumerate(ws):
+        o = oracle_lib.OracleProblem(g, oracle_lib.default_params(linear_solver=LINEAR_CHOLESKY))
+        _, so = o.optimize(10)
+        assert st[w]["iterations"] == len(so)
+        assert abs(st[w]["chi2"] - so[-1]["chi2"]) <= 1e-8 * so[-1]["chi2"], (w, st[w]["chi2"], so[-1]["chi2"])
+    cw.close()
+    g = small_ba(seed=22, focal_y=455.0)
+    o = oracle_lib.OracleProblem(g)
+    _, so = o.optimize(20)
+    m = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED))
+    _, sm = m.optimize(30)
+    assert min(s["chi2"] for s in sm) <= so[-1]["chi2"] * (1 + 1e-6)

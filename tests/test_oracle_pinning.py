@@ -208,3 +208,25 @@ def test_two_pose_se3_converges(oracle_lib, algo, case):
     pose, _ = p.estimates()
     assert np.abs(pose[1, 9:]).max() < 1e-3
     assert np.abs(np.diag(pose[1, :9].reshape(3, 3)) - 1).max() < 1e-3
+
+
+@pytest.mark.parametrize("focal_y", [None, 455.0])
+def test_projection_jacobians_match_numeric(oracle_lib, focal_y):
+    """EdgeProjectXYZ2UV (fx = fy) and EdgeSE3ProjectXYZ (fx != fy): the
+    analytic Jacobians against central differences with g2o's step 1e-9
+    (BaseFixedSizedEdge::linearizeOplus numeric form,
+    g2o/core/base_fixed_sized_edge.hpp:161-193)."""
+    from g2o_b200 import synth
+    g = synth.bundle_adjustment(num_cameras=12, num_points=400, seed=17, focal_y=focal_y)
+    p = oracle_lib.OracleProblem(g)
+    a0, a1 = p.jacobians()
+    n0, n1 = p.jacobians(numeric=True)
+    for a, n in ((a0, n0), (a1, n1)):
+        assert np.abs(a - n).max() <= 1e-5 * max(1.0, np.abs(a).max())
+    # fx and fy act on their own rows: the v row scales with fy alone
+    if focal_y is not None:
+        g2 = g.copy()
+        g2.focal_length_y = 500.0
+        b0, b1 = oracle_lib.OracleProblem(g2).jacobians()
+        np.testing.assert_allclose(a1[:, 0], b1[:, 0], rtol=1e-12)
+        np.testing.assert_allclose(a1[:, 1], b1[:, 1] * (455.0 / 500.0), rtol=1e-12)
