@@ -32,7 +32,7 @@ ERROR_NAMES = {
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
 EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ = 1, 2, 3, 4
 BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
-ALGO_GAUSS_NEWTON, ALGO_LEVENBERG = 0, 1
+ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG = 0, 1, 2
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2
@@ -81,6 +81,8 @@ class G2ocParams(C.Structure):
         ("tau", C.c_double),
         ("refine_max_iterations", C.c_int32),
         ("refine_tolerance", C.c_double),
+        ("initial_delta", C.c_double),
+        ("lambda_factor", C.c_double),
     ]
 
 
@@ -98,6 +100,8 @@ class G2ocIterationStats(C.Structure):
         ("time_linear_solver", C.c_double),
         ("time_update", C.c_double),
         ("time_iteration", C.c_double),
+        ("trust_radius", C.c_double),
+        ("dogleg_step", C.c_int32),
     ]
 
     def as_dict(self):

@@ -141,6 +141,8 @@ bool apply_properties(const std::string& spec, g2oc_params& p) {
     if (k == "initialLambda") p.initial_lambda = std::atof(v.c_str());
     else if (k == "tau") p.tau = std::atof(v.c_str());
     else if (k == "maxTrialsAfterFailure") p.max_trials_after_failure = std::atoi(v.c_str());
+    else if (k == "initialDelta") p.initial_delta = std::atof(v.c_str());
+    else if (k == "lambdaFactor") p.lambda_factor = std::atof(v.c_str());
     else if (k == "tolerance") p.pcg_tolerance = std::atof(v.c_str());
     else if (k == "maxIterations") p.pcg_max_iterations = std::atoi(v.c_str());
     else if (k == "absoluteTolerance") p.pcg_absolute_tolerance = (v == "1" || v == "true");
@@ -359,6 +361,13 @@ int main(int argc, char** argv) {
                   << (hinfo.num_free_points > 0 ? 1 : 0);
         if (params.algorithm == G2OC_ALGO_LEVENBERG)
           std::cerr << "\t lambda= " << fixed6(s.lambda) << "\t levenbergIter= " << s.levenberg_iterations;
+        if (params.algorithm == G2OC_ALGO_DOGLEG) {
+          // OptimizationAlgorithmDogleg::printVerbose (optimization_algorithm_dogleg.cpp:182-187)
+          static const char* const kStep[] = {"Undefined", "Descent", "GN", "Dogleg"};
+          std::cerr << "\t Delta= " << s.trust_radius << "\t step= " << kStep[s.dogleg_step & 3]
+                    << "\t tries= " << s.levenberg_iterations;
+          if (s.lambda > 0) std::cerr << "\t lambda= " << s.lambda;
+        }
         std::cerr << std::endl;
       }
       if (gain_mode) {

@@ -64,6 +64,9 @@ struct EngineBase {
   virtual int alloc() = 0;
   virtual int build_system() = 0;
   virtual int max_diag() = 0;  // -> sc.max_diag
+  // dst = Hpp src over the Hessian-order vector (landmark part of dst zero):
+  // BlockSolver::multiplyHessian (g2o/core/block_solver.h:96)
+  virtual int multiply_hessian(const double* src, double* dst) = 0;
   virtual int solve(double lambda) = 0;  // -> x, sc.solve_ok (PCG iterations: PcgState::total_iterations)
   virtual int get_hessian(double* hpp, double* hll, double* hpl) = 0;
   virtual int schur_export(double lambda, double* S, double* bs) = 0;
@@ -186,6 +189,11 @@ struct g2oc_ctx {
   g2oc::PinnedVec<g2oc::PcgState> h_pcg;
   cudaEvent_t ev_read = nullptr;
   cudaEvent_t coop_done = nullptr;  // completion of this context's last grid-barrier launch
+  // Dogleg state (OptimizationAlgorithmDogleg's members) and its vectors
+  // (steepest-descent step, Gauss-Newton step, scratch)
+  double dl_delta = 0.0, dl_lambda = 0.0;
+  bool dl_was_pd = true;
+  g2oc::DBuf<double> dl_buf;
   g2oc::DBuf<int> win_cam, win_lm, win_edge, win_pose, win_point, win_of_cam, win_of_lm, win_of_pose, win_of_point;
   g2oc::DBuf<int> win_chunk_w, win_chunk_e0, win_chunk_ptr;  // chi2 edge chunks (kWinChi2Chunk)
   g2oc::DBuf<double> win_chunk_sum;
@@ -725,6 +733,22 @@ struct Engine final : EngineBase {
       }
       G2OC_LAUNCH_CHECK();
     }
+    return G2OC_OK;
+  }
+
+  int multiply_hessian(const double* src, double* dst) override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    const int n = c->vec_size();
+    if (n <= 0) return G2OC_OK;
+    if (S.Cf == 0) {
+      G2OC_CUDA_TRY(cudaMemsetAsync(dst, 0, (size_t)n * sizeof(double), st));
+      return G2OC_OK;
+    }
+    if (S.ba) G2OC_K(K_LM_CONTROL) hpp_mult_diag6<Real><<<cdiv(n, 256), 256, 0, st>>>(S.Cf, hpp.p, src, dst, n);
+    else if (S.pd == 3) G2OC_K(K_LM_CONTROL) hpp_mult_sym<Real, 3><<<cdiv(S.Cf, 128), 128, 0, st>>>(sys(nullptr), hpp.p, src, dst);
+    else G2OC_K(K_LM_CONTROL) hpp_mult_sym<Real, 6><<<cdiv(S.Cf, 128), 128, 0, st>>>(sys(nullptr), hpp.p, src, dst);
+    G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
@@ -1392,6 +1416,164 @@ static int gn_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
   return G2OC_OK;
 }
 
+// a . b of device vectors, on the host (one wait), fixed summation order
+static int dl_dot(g2oc_ctx* c, const double* a, const double* b, int n, double* out) {
+  G2OC_K(K_LM_CONTROL) dot_partials<<<kRedBlocks, 256, 0, c->stream>>>(a, b, n, c->partials.p);
+  G2OC_LAUNCH_CHECK();
+  G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &c->sc.p->refine_rnorm, nullptr));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(out, &c->sc.p->refine_rnorm, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G2OC_OK;
+}
+
+static int dl_combine(g2oc_ctx* c, int n, double a, const double* x, double b, const double* y, double* out) {
+  if (n <= 0) return G2OC_OK;
+  G2OC_K(K_AXPY) dl_axpby<<<cdiv(n, 256), 256, 0, c->stream>>>(n, a, x, b, y, out);
+  G2OC_LAUNCH_CHECK();
+  return G2OC_OK;
+}
+
+// OptimizationAlgorithmDogleg::solve (g2o/core/optimization_algorithm_dogleg.cpp:62-180):
+// steepest-descent step alpha b with alpha = |b|^2 / b^T Hpp b, Gauss-Newton
+// step H^-1 b (damped with lambda once a solve was not positive definite),
+// the dogleg between them inside the trust radius Delta; the step is kept
+// when the gain ratio rho > 0; Delta grows (rho > 0.75) or halves
+// (rho < 0.25). The control runs on the host from device dot products.
+static int dl_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, int* result) {
+  cudaStream_t st = c->stream;
+  DevScalars* sc = c->sc.p;
+  c->cur_stats = stv;
+  const int n = c->vec_size();
+  if (iteration == 0) {
+    c->dl_delta = c->prm.initial_delta;
+    c->dl_lambda = c->prm.initial_lambda > 0 ? c->prm.initial_lambda : 1e-7;
+    c->dl_was_pd = true;
+  }
+  if (c->dl_buf.n < (size_t)3 * n) G2OC_TRY(c->dl_buf.alloc((size_t)3 * n));
+  double* hsd = c->dl_buf.p;
+  double* hgn = c->dl_buf.p + n;
+  double* aux = c->dl_buf.p + 2 * (size_t)n;
+  double* hdl = c->x.p;  // the update oplus applies
+  const double* b = c->b.p;
+  cudaEvent_t t0 = c->mark();
+  G2OC_TRY(chi2_to(c, &sc->chi2_plain, &sc->chi2_current));
+  c->span(t0, &stv->time_residuals);
+  t0 = c->mark();
+  G2OC_TRY(c->eng->build_system());
+  c->system_built = true;
+  c->span(t0, &stv->time_quadratic_form);
+  DevScalars h{};
+  G2OC_TRY(read_state(c, &h, stv));
+  const double current_chi = h.chi2_current;
+  // alpha = |b|^2 / (b^T Hpp b); hsd = alpha b
+  G2OC_TRY(c->eng->multiply_hessian(b, aux));
+  double bb = 0, ab = 0;
+  G2OC_TRY(dl_dot(c, b, b, n, &bb));
+  G2OC_TRY(dl_dot(c, aux, b, n, &ab));
+  const double alpha = bb / ab;
+  G2OC_TRY(dl_combine(c, n, alpha, b, 0.0, nullptr, hsd));
+  double hsd2 = 0;
+  G2OC_TRY(dl_dot(c, hsd, hsd, n, &hsd2));
+  const double hsd_norm = std::sqrt(hsd2);
+  double hgn_norm = -1.0, new_chi = current_chi;
+  bool solved = false, good = false;
+  int tries = 0, step = 0;
+  const int max_trials = c->prm.max_trials_after_failure;
+  do {
+    ++tries;
+    if (!solved) {
+      solved = true;
+      bool ok = false;
+      while (!ok) {
+        t0 = c->mark();
+        G2OC_TRY(c->eng->solve(c->dl_was_pd ? 0.0 : c->dl_lambda));
+        c->span(t0, &stv->time_linear_solver);
+        G2OC_TRY(read_state(c, &h, stv));
+        ok = h.solve_ok != 0;
+        c->dl_was_pd = c->dl_was_pd && ok;
+        if (!c->dl_was_pd) {
+          if (ok) {
+            c->dl_lambda = std::max(1e-12, c->dl_lambda / (0.5 * c->prm.lambda_factor));
+          } else {
+            c->dl_lambda *= c->prm.lambda_factor;
+            if (c->dl_lambda > 1e3) {
+              c->dl_lambda = 1e3;
+              stv->levenberg_iterations = tries;
+              stv->lambda = c->dl_lambda;
+              stv->trust_radius = c->dl_delta;
+              stv->chi2 = current_chi;
+              c->resolve_spans();
+              c->cur_stats = nullptr;
+              *result = G2OC_RESULT_FAIL;
+              return G2OC_OK;
+            }
+          }
+        }
+      }
+      G2OC_CUDA_TRY(cudaMemcpyAsync(hgn, c->x.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      double g2 = 0;
+      G2OC_TRY(dl_dot(c, hgn, hgn, n, &g2));
+      hgn_norm = std::sqrt(g2);
+    }
+    const double delta = c->dl_delta;
+    if (hgn_norm < delta) {
+      G2OC_CUDA_TRY(cudaMemcpyAsync(hdl, hgn, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      step = 2;
+    } else if (hsd_norm > delta) {
+      G2OC_TRY(dl_combine(c, n, delta / hsd_norm, hsd, 0.0, nullptr, hdl));
+      step = 1;
+    } else {
+      G2OC_TRY(dl_combine(c, n, 1.0, hgn, -1.0, hsd, aux));  // b - a
+      double cc = 0, bma2 = 0;
+      G2OC_TRY(dl_dot(c, hsd, aux, n, &cc));
+      G2OC_TRY(dl_dot(c, aux, aux, n, &bma2));
+      double beta;
+      if (cc <= 0.) beta = (-cc + std::sqrt(cc * cc + bma2 * (delta * delta - hsd2))) / bma2;
+      else beta = (delta * delta - hsd2) / (cc + std::sqrt(cc * cc + bma2 * (delta * delta - hsd2)));
+      G2OC_TRY(dl_combine(c, n, 1.0, hsd, beta, aux, hdl));
+      step = 3;
+    }
+    // linear gain -hdl^T Hpp hdl + 2 b^T hdl
+    G2OC_TRY(c->eng->multiply_hessian(hdl, aux));
+    double hh = 0, bh = 0;
+    G2OC_TRY(dl_dot(c, aux, hdl, n, &hh));
+    G2OC_TRY(dl_dot(c, b, hdl, n, &bh));
+    double linear_gain = -1 * hh + 2 * bh;
+    G2OC_TRY(push(c));
+    t0 = c->mark();
+    G2OC_TRY(oplus(c));
+    c->span(t0, &stv->time_update);
+    G2OC_TRY(chi2_to(c, &sc->chi2_temp_plain, &sc->chi2_temp));
+    G2OC_TRY(read_state(c, &h, stv));
+    new_chi = h.chi2_temp;
+    const double nonlinear_gain = current_chi - new_chi;
+    if (std::fabs(linear_gain) < 1e-12) linear_gain = 1e-12;
+    const double rho = nonlinear_gain / linear_gain;
+    if (rho > 0) {
+      good = true;
+    } else {
+      G2OC_TRY(pop(c));
+    }
+    if (rho > 0.75) {
+      double d2 = 0;
+      G2OC_TRY(dl_dot(c, hdl, hdl, n, &d2));
+      c->dl_delta = std::max(c->dl_delta, 3 * std::sqrt(d2));
+    } else if (rho < 0.25) {
+      c->dl_delta *= 0.5;
+    }
+  } while (!good && tries < max_trials);
+  stv->levenberg_iterations = tries;
+  stv->lambda = c->dl_was_pd ? 0.0 : c->dl_lambda;
+  stv->trust_radius = c->dl_delta;
+  stv->dogleg_step = step;
+  stv->chi2 = good ? new_chi : current_chi;  // activeRobustChi2 of the state the iteration ends in
+  c->chi2_carry = false;
+  c->resolve_spans();
+  c->cur_stats = nullptr;
+  *result = (tries == max_trials || !good) ? G2OC_RESULT_TERMINATE : G2OC_RESULT_OK;
+  return G2OC_OK;
+}
+
 static int reset_pcg(g2oc_ctx* c) {
   PcgState p{};
   p.residual_carry = -1.0;
@@ -1445,9 +1627,11 @@ void g2oc_default_params(g2oc_params* p) {
   p->tau = 1e-5;
   p->refine_max_iterations = 2;
   p->refine_tolerance = 1e-10;
+  p->initial_delta = 1e4;
+  p->lambda_factor = 10.0;
 }
 
-// names registered by this library, "<gn|lm>_cuda[_<variant>]"
+// names registered by this library, "<gn|lm|dl>_cuda[_<variant>]"
 static const char* kSolvers[][2] = {
     {"gn_cuda", "Gauss-Newton: B200 block solver, FP64, PCG with Schur / Cholesky without"},
     {"lm_cuda", "Levenberg: B200 block solver, FP64, PCG with Schur / Cholesky without"},
@@ -1463,6 +1647,9 @@ static const char* kSolvers[][2] = {
     {"lm_cuda_mixed", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
     {"gn_cuda_mixed_fast", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
     {"lm_cuda_mixed_fast", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
+    {"dl_cuda", "Dogleg: B200 block solver, FP64, PCG with Schur / Cholesky without"},
+    {"dl_cuda_pcg", "Dogleg: B200 block solver, FP64, block-Jacobi PCG"},
+    {"dl_cuda_chol", "Dogleg: B200 block solver, FP64, dense Cholesky"},
 };
 
 int g2oc_list_solvers(char* buf, size_t size) {
@@ -1493,7 +1680,14 @@ int g2oc_construct(const char* name, g2oc_params* p) {
   }
   const std::string n(name);
   g2oc_default_params(p);
-  p->algorithm = n.substr(0, 2) == "gn" ? G2OC_ALGO_GAUSS_NEWTON : G2OC_ALGO_LEVENBERG;
+  p->algorithm = n.substr(0, 2) == "gn"   ? G2OC_ALGO_GAUSS_NEWTON
+                 : n.substr(0, 2) == "dl" ? G2OC_ALGO_DOGLEG
+                                          : G2OC_ALGO_LEVENBERG;
+  if (p->algorithm == G2OC_ALGO_DOGLEG) {
+    // OptimizationAlgorithmDogleg's properties (optimization_algorithm_dogleg.cpp:44-51)
+    p->max_trials_after_failure = 100;
+    p->initial_lambda = 1e-7;
+  }
   const std::string v = n.size() > 7 ? n.substr(8) : "";
   if (v.empty()) p->linear_solver = 2;  // PCG with Schur, Cholesky without
   else if (v.rfind("chol", 0) == 0) p->linear_solver = G2OC_LINEAR_CHOLESKY;
@@ -1567,8 +1761,9 @@ int g2oc_set_params(g2oc_ctx* c, const g2oc_params* p) {
     set_error("params is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
-  if (p->algorithm < 0 || p->algorithm > 1 || p->linear_solver < 0 || p->linear_solver > 2 || p->precision < 0 ||
-      p->precision > 1 || p->max_trials_after_failure < 1 || p->pcg_tolerance < 0) {
+  if (p->algorithm < 0 || p->algorithm > 2 || p->linear_solver < 0 || p->linear_solver > 2 || p->precision < 0 ||
+      p->precision > 1 || p->max_trials_after_failure < 1 || p->pcg_tolerance < 0 ||
+      (p->algorithm == G2OC_ALGO_DOGLEG && (!(p->initial_delta > 0) || !(p->lambda_factor > 0)))) {
     set_error("invalid parameter value");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
@@ -1917,6 +2112,7 @@ static int check_sharding(g2oc_ctx* c) {
   if (c->shard_world <= 1) return G2OC_OK;
   const Structure& S = c->S;
   if (!S.ba || !S.schur || !S.tile_ok || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY || pcg_mode() != PCG_AUTO ||
+      c->prm.algorithm == G2OC_ALGO_DOGLEG ||
       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0)) {
     set_error("sharded mode runs bundle adjustments with >= %d free cameras and landmarks, the PCG solver, FP64 or "
               "mixed precision without FP64 refinement",
@@ -1958,6 +2154,7 @@ static int optimize_impl(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stat
     memset(&stv, 0, sizeof(stv));
     cudaEvent_t t0 = c->mark();
     if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, i, &stv, &result));
+    else if (c->prm.algorithm == G2OC_ALGO_DOGLEG) G2OC_TRY(dl_iteration(c, i, &stv, &result));
     else G2OC_TRY(gn_iteration(c, i, &stv, &result));
     stv.iteration = i;
     stv.result = result;
@@ -1981,6 +2178,7 @@ static int iterate_impl(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats,
   memset(&stv, 0, sizeof(stv));
   cudaEvent_t t0 = c->mark();
   if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, iteration, &stv, result));
+  else if (c->prm.algorithm == G2OC_ALGO_DOGLEG) G2OC_TRY(dl_iteration(c, iteration, &stv, result));
   else G2OC_TRY(gn_iteration(c, iteration, &stv, result));
   stv.iteration = iteration;
   stv.result = *result;
@@ -2570,6 +2768,10 @@ int g2oc_optimize_windows(g2oc_ctx* c, int32_t iterations, g2oc_window_stats* st
   if (iterations < 0) {
     set_error("iterations < 0");
     return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (c->prm.algorithm != G2OC_ALGO_LEVENBERG) {
+    set_error("batched windows run Levenberg-Marquardt");
+    return G2OC_ERR_NOT_SUPPORTED;
   }
   cudaStream_t st = c->stream;
   // window states: windows without edges are finished from the start

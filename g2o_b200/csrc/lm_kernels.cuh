@@ -5,6 +5,7 @@
 #pragma once
 
 #include "g2oc_internal.h"
+#include "pcg_kernels.cuh"
 #include "reduce.cuh"
 
 namespace g2oc {
@@ -97,6 +98,71 @@ __global__ void damp_diag(const int* diag, int nb, double lambda, Real* dst) {
   const int i = t / BS, d = t % BS;
   Real* v = dst + (size_t)diag[i] * BS * BS + d * (BS + 1);
   *v = (Real)((double)*v + lambda);
+}
+
+// ---------------------------------------------------------------- Dogleg
+// out = a x + b y (x or y NULL: that term is absent), the vector
+// combinations of OptimizationAlgorithmDogleg::solve
+// (g2o/core/optimization_algorithm_dogleg.cpp:99-157)
+static __global__ void dl_axpby(int n, double a, const double* x, double b, const double* y, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = 0.0;
+  if (x) v = a * x[i];
+  if (y) v = x ? v + b * y[i] : b * y[i];
+  out[i] = v;
+}
+
+// y = Hpp x for a pose graph: BlockSolver::multiplyHessian
+// (g2o/core/block_solver.h:96) = SparseBlockMatrix::multiplySymmetricUpperTriangle
+// over the upper blocks, listed by the system's row and column lists, values
+// in the column-major pattern order (perm). One thread per block row; the
+// row's blocks, then the transposed strictly-upper blocks of its column.
+template <typename Real, int BS>
+__global__ void hpp_mult_sym(SysDev<Real> A, const Real* hv, const double* x, double* y) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= A.nb) return;
+  double acc[BS];
+#pragma unroll
+  for (int a = 0; a < BS; ++a) acc[a] = 0.0;
+  for (int k = A.rptr[r]; k < A.rptr[r + 1]; ++k) {
+    const int c = A.rcol[k];
+    const Real* B = hv + (size_t)A.perm[k] * BS * BS;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int b = 0; b < BS; ++b) acc[i] += (double)B[i * BS + b] * x[(size_t)c * BS + b];
+  }
+  for (int p = A.cptr[r]; p < A.cptr[r + 1]; ++p) {
+    const int k = A.cblk[p];
+    const int row = A.brow[k];
+    const Real* B = hv + (size_t)A.perm[k] * BS * BS;
+#pragma unroll
+    for (int i = 0; i < BS; ++i)
+#pragma unroll
+      for (int b = 0; b < BS; ++b) acc[b] += (double)B[i * BS + b] * x[(size_t)row * BS + i];
+  }
+#pragma unroll
+  for (int a = 0; a < BS; ++a) y[(size_t)r * BS + a] = acc[a];
+}
+
+// y = Hpp x for bundle adjustment: Hpp is the cameras' 6x6 diagonal blocks
+// (no pose-pose edges); the landmark part of y is zero, as multiplyHessian
+// touches only the pose part of the vector
+template <typename Real>
+__global__ void hpp_mult_diag6(int nb, const Real* hv, const double* x, double* y, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  if (t >= nb * 6) {
+    y[t] = 0.0;
+    return;
+  }
+  const int h = t / 6, i = t % 6;
+  const Real* B = hv + (size_t)h * 36 + i * 6;
+  double acc = 0.0;
+#pragma unroll
+  for (int b = 0; b < 6; ++b) acc += (double)B[b] * x[(size_t)h * 6 + b];
+  y[t] = acc;
 }
 
 }  // namespace g2oc

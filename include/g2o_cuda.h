@@ -96,6 +96,7 @@ extern "C" {
 /* algorithm / linear solver / precision */
 #define G2OC_ALGO_GAUSS_NEWTON 0
 #define G2OC_ALGO_LEVENBERG 1
+#define G2OC_ALGO_DOGLEG 2 /* OptimizationAlgorithmDogleg (g2o/core/optimization_algorithm_dogleg.cpp:62-180) */
 
 #define G2OC_LINEAR_PCG 0      /* block-Jacobi PCG (LinearSolverPCG semantics) */
 #define G2OC_LINEAR_CHOLESKY 1 /* dense Cholesky of the (reduced) system */
@@ -143,6 +144,10 @@ typedef struct g2oc_params {
   int32_t refine_max_iterations;     /* mixed precision: max FP64 refinement corrections per solve (default 2);
                                         -1: no FP64 residual check, the FP32-stored system's solution is the step */
   double refine_tolerance;           /* reserved (default 1e-10) */
+  double initial_delta;              /* Dogleg "initialDelta": initial trust radius (1e4) */
+  double lambda_factor;              /* Dogleg "lambdaFactor" (10); Dogleg's "initialLambda" is
+                                        initial_lambda (the dl_* names set 1e-7, <= 0 means 1e-7) and
+                                        its "maxTrialsAfterFailure" max_trials_after_failure (100) */
 } g2oc_params;
 
 /* one per outer iteration, the fields of G2OBatchStatistics (g2o/core/batch_stats.h:40-82) */
@@ -159,6 +164,8 @@ typedef struct g2oc_iteration_stats {
   double time_linear_solver;
   double time_update;
   double time_iteration;
+  double trust_radius;            /* Dogleg: Delta after the iteration */
+  int32_t dogleg_step;            /* Dogleg: last step, 0 undefined, 1 steepest descent, 2 Gauss-Newton, 3 dogleg */
 } g2oc_iteration_stats;
 
 typedef struct g2oc_hessian_info {

@@ -789,6 +789,10 @@ struct orc_problem {
   PCGState pcg;
   double lambda = -1, ni = 2;
   int pcg_iters_last = 0;
+  // OptimizationAlgorithmDogleg's members
+  double dl_delta = 0, dl_lambda = 0;
+  bool dl_was_pd = true;
+  int dl_step = 0;
   // backup for LM push/pop
   std::vector<double> pose_bak, point_bak;
   bool system_built = false;
@@ -1369,6 +1373,123 @@ int lm_solve(orc_problem* p, int iteration, g2oc_iteration_stats* st) {
   return G2OC_RESULT_OK;
 }
 
+void multiply_hessian(orc_problem* p, const double* src, double* dest) {
+  // BlockSolver::multiplyHessian (g2o/core/block_solver.h:96):
+  // _Hpp->multiplySymmetricUpperTriangle, the pose part only
+  const int pd = p->pd;
+  std::fill(dest, dest + p->x.size(), 0.0);
+  for (size_t k = 0; k < p->hpp_rc.size(); ++k) {
+    const int r = p->hpp_rc[k].first, c = p->hpp_rc[k].second;
+    const double* B = p->hpp.data() + k * pd * pd;
+    for (int i = 0; i < pd; ++i)
+      for (int j = 0; j < pd; ++j) dest[(size_t)r * pd + i] += B[i * pd + j] * src[(size_t)c * pd + j];
+    if (r != c)
+      for (int i = 0; i < pd; ++i)
+        for (int j = 0; j < pd; ++j) dest[(size_t)c * pd + j] += B[i * pd + j] * src[(size_t)r * pd + i];
+  }
+}
+
+double vdot(const std::vector<double>& a, const std::vector<double>& b) {
+  double s = 0;
+  for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+  return s;
+}
+
+int dl_solve(orc_problem* p, int iteration, g2oc_iteration_stats* st) {
+  // OptimizationAlgorithmDogleg::solve (g2o/core/optimization_algorithm_dogleg.cpp:62-180)
+  const size_t n = p->x.size();
+  if (iteration == 0) {
+    p->dl_delta = p->prm.initial_delta;
+    p->dl_lambda = p->prm.initial_lambda > 0 ? p->prm.initial_lambda : 1e-7;
+    p->dl_was_pd = true;
+  }
+  compute_active_errors(p);
+  double currentChi;
+  active_chi2(p, nullptr, &currentChi);
+  build_system(p);
+  const std::vector<double>& b = p->b;
+  std::vector<double> aux(n), hsd(n), hdl(n), hgn;
+  multiply_hessian(p, b.data(), aux.data());
+  const double bNormSquared = vdot(b, b);
+  const double alpha = bNormSquared / vdot(aux, b);
+  for (size_t i = 0; i < n; ++i) hsd[i] = alpha * b[i];
+  const double hsdSqr = vdot(hsd, hsd);
+  const double hsdNorm = std::sqrt(hsdSqr);
+  double hgnNorm = -1;
+  bool solvedGaussNewton = false, goodStep = false;
+  int numTries = 0;
+  const int maxTrials = p->prm.max_trials_after_failure;
+  do {
+    ++numTries;
+    if (!solvedGaussNewton) {
+      const double minLambda = 1e-12, maxLambda = 1e3;
+      solvedGaussNewton = true;
+      bool solverOk = false;
+      while (!solverOk) {
+        if (!p->dl_was_pd) set_lambda(p, p->dl_lambda);
+        double ts = 0, tl = 0;
+        solverOk = block_solver_solve(p, &ts, &tl);
+        if (st) {
+          st->time_schur_complement += ts;
+          st->time_linear_solver += tl;
+          st->iterations_linear_solver += p->pcg_iters_last;
+        }
+        if (!p->dl_was_pd) restore_diagonal(p);
+        p->dl_was_pd = p->dl_was_pd && solverOk;
+        if (!p->dl_was_pd) {
+          if (solverOk) {
+            p->dl_lambda = std::max(minLambda, p->dl_lambda / (0.5 * p->prm.lambda_factor));
+          } else {
+            p->dl_lambda *= p->prm.lambda_factor;
+            if (p->dl_lambda > maxLambda) {
+              p->dl_lambda = maxLambda;
+              return G2OC_RESULT_FAIL;
+            }
+          }
+        }
+      }
+      hgn = p->x;
+      hgnNorm = std::sqrt(vdot(hgn, hgn));
+    }
+    const double delta = p->dl_delta;
+    if (hgnNorm < delta) {
+      hdl = hgn;
+      p->dl_step = 2;
+    } else if (hsdNorm > delta) {
+      for (size_t i = 0; i < n; ++i) hdl[i] = delta / hsdNorm * hsd[i];
+      p->dl_step = 1;
+    } else {
+      for (size_t i = 0; i < n; ++i) aux[i] = hgn[i] - hsd[i];
+      const double c = vdot(hsd, aux);
+      const double bmaSquaredNorm = vdot(aux, aux);
+      double beta;
+      if (c <= 0.)
+        beta = (-c + std::sqrt(c * c + bmaSquaredNorm * (delta * delta - hsdSqr))) / bmaSquaredNorm;
+      else
+        beta = (delta * delta - hsdSqr) / (c + std::sqrt(c * c + bmaSquaredNorm * (delta * delta - hsdSqr)));
+      for (size_t i = 0; i < n; ++i) hdl[i] = hsd[i] + beta * aux[i];
+      p->dl_step = 3;
+    }
+    multiply_hessian(p, hdl.data(), aux.data());
+    double linearGain = -1 * vdot(aux, hdl) + 2 * vdot(b, hdl);
+    push(p);
+    update(p, hdl.data());
+    compute_active_errors(p);
+    double newChi;
+    active_chi2(p, nullptr, &newChi);
+    const double nonLinearGain = currentChi - newChi;
+    if (std::fabs(linearGain) < 1e-12) linearGain = 1e-12;
+    const double rho = nonLinearGain / linearGain;
+    if (rho > 0) goodStep = true;
+    else pop(p);
+    if (rho > 0.75) p->dl_delta = std::max(p->dl_delta, 3 * std::sqrt(vdot(hdl, hdl)));
+    else if (rho < 0.25) p->dl_delta *= 0.5;
+  } while (!goodStep && numTries < maxTrials);
+  if (st) st->levenberg_iterations = numTries;
+  if (numTries == maxTrials || !goodStep) return G2OC_RESULT_TERMINATE;
+  return G2OC_RESULT_OK;
+}
+
 int gn_solve(orc_problem* p, int iteration, g2oc_iteration_stats* st) {
   // OptimizationAlgorithmGaussNewton::solve (optimization_algorithm_gauss_newton.cpp:48-93)
   (void)iteration;
@@ -1637,10 +1758,16 @@ int orc_optimize(orc_problem* p, int iterations, g2oc_iteration_stats* stats, in
     std::memset(&local, 0, sizeof(local));
     double t = now_s();
     if (p->prm.algorithm == G2OC_ALGO_LEVENBERG) result = lm_solve(p, i, &local);
+    else if (p->prm.algorithm == G2OC_ALGO_DOGLEG) result = dl_solve(p, i, &local);
     else result = gn_solve(p, i, &local);
     local.iteration = i;
     local.result = result;
     local.lambda = p->lambda;
+    if (p->prm.algorithm == G2OC_ALGO_DOGLEG) {
+      local.lambda = p->dl_was_pd ? 0.0 : p->dl_lambda;
+      local.trust_radius = p->dl_delta;
+      local.dogleg_step = p->dl_step;
+    }
     compute_active_errors(p);
     active_chi2(p, nullptr, &local.chi2);
     local.time_iteration = now_s() - t;
@@ -1706,6 +1833,8 @@ void orc_default_params(g2oc_params* p) {
   p->tau = 1e-5;
   p->refine_max_iterations = 2;
   p->refine_tolerance = 1e-10;
+  p->initial_delta = 1e4;  // OptimizationAlgorithmDogleg "initialDelta"
+  p->lambda_factor = 10.;  // "lambdaFactor"
 }
 
 }  // extern "C"

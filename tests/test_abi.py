@@ -27,8 +27,10 @@ int main(void) {
   F(g2oc_graph, focal_length_y)
   printf("g2oc_params %zu\n", sizeof(g2oc_params));
   F(g2oc_params, pcg_tolerance) F(g2oc_params, initial_lambda) F(g2oc_params, refine_tolerance)
+  F(g2oc_params, initial_delta) F(g2oc_params, lambda_factor)
   printf("g2oc_iteration_stats %zu\n", sizeof(g2oc_iteration_stats));
   F(g2oc_iteration_stats, chi2) F(g2oc_iteration_stats, time_iteration)
+  F(g2oc_iteration_stats, trust_radius) F(g2oc_iteration_stats, dogleg_step)
   printf("g2oc_hessian_info %zu\n", sizeof(g2oc_hessian_info));
   F(g2oc_hessian_info, vector_size) F(g2oc_hessian_info, schur_pairs)
   return 0;
@@ -74,13 +76,18 @@ def test_factory_lists_and_constructs():
     for n in names:
         p = fac.construct(n)
         assert p is not None, n
-        assert p.algorithm == (abi.ALGO_GAUSS_NEWTON if n.startswith("gn") else abi.ALGO_LEVENBERG)
+        want = {"gn": abi.ALGO_GAUSS_NEWTON, "lm": abi.ALGO_LEVENBERG, "dl": abi.ALGO_DOGLEG}[n[:2]]
+        assert p.algorithm == want, n
     assert fac.construct("lm_cuda_mixed").precision == abi.PREC_MIXED
     assert fac.construct("lm_cuda_mixed").refine_max_iterations == 2
     fast = fac.construct("lm_cuda_mixed_fast")
     assert fast.precision == abi.PREC_MIXED and fast.refine_max_iterations == -1
     assert fac.construct("gn_cuda_chol").linear_solver == abi.LINEAR_CHOLESKY
     assert fac.construct("gn_cuda_pcg6_3").linear_solver == abi.LINEAR_PCG
+    dl = fac.construct("dl_cuda_chol")
+    # OptimizationAlgorithmDogleg's property defaults (optimization_algorithm_dogleg.cpp:44-51)
+    assert dl.linear_solver == abi.LINEAR_CHOLESKY and dl.max_trials_after_failure == 100
+    assert dl.initial_lambda == 1e-7 and dl.initial_delta == 1e4 and dl.lambda_factor == 10.0
     assert fac.construct("non_existing_solver") is None
     assert fac.construct("") is None
 

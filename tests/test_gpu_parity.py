@@ -415,3 +415,39 @@ def test_se3_project_xyz_windows_and_mixed(backend, oracle_lib):
     m = backend.CudaProblem(g, backend.default_params(precision=PREC_MIXED))
     _, sm = m.optimize(30)
     assert min(s["chi2"] for s in sm) <= so[-1]["chi2"] * (1 + 1e-6)
+
+
+# ------------------------------------------- OptimizationAlgorithmDogleg
+@pytest.mark.parametrize("kind", ["pg2d_chol", "pg3d_chol", "pg3d_pcg", "ba"])
+def test_dogleg_matches_oracle(backend, oracle_lib, kind):
+    """dl_cuda* against the oracle's restatement of
+    OptimizationAlgorithmDogleg::solve (optimization_algorithm_dogleg.cpp:62-180):
+    per iteration the same tries and step type, chi2 and trust radius within
+    1e-8 (FP64), over the iterations before convergence (there the gain
+    ratio is a difference of nearly equal chi2 values and its sign is
+    rounding)."""
+    from g2o_b200.abi import ALGO_DOGLEG
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    if kind == "pg2d_chol":
+        g, name, iters = synth.pose_graph_2d(num_poses=600, num_closures=200, seed=3), "dl_cuda_chol", 4
+    elif kind == "pg3d_chol":
+        g, name, iters = synth.pose_graph_3d(num_rings=4, per_ring=40, radius=10.0, seed=4), "dl_cuda_chol", 4
+    elif kind == "pg3d_pcg":
+        g, name, iters = synth.pose_graph_3d(num_rings=4, per_ring=40, radius=10.0, seed=4), "dl_cuda_pcg", 4
+    else:
+        g, name, iters = small_ba(seed=23), "dl_cuda", 6
+    prm = fac.construct(name)
+    assert prm.algorithm == ALGO_DOGLEG
+    o = oracle_lib.OracleProblem(g, prm)
+    c = backend.CudaProblem(g, prm)
+    do, so = o.optimize(iters)
+    dc, sc = c.optimize(iters)
+    assert do == dc
+    tol = 1e-8 if kind != "pg3d_pcg" else 1e-6
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"], (a, b)
+        assert a["dogleg_step"] == b["dogleg_step"], (a, b)
+        assert abs(a["chi2"] - b["chi2"]) <= tol * b["chi2"], (a["chi2"], b["chi2"])
+        assert abs(a["trust_radius"] - b["trust_radius"]) <= 1e-6 * b["trust_radius"], (a, b)
+    assert sc[-1]["chi2"] < sc[0]["chi2"] or kind == "ba"
+    c.close()
