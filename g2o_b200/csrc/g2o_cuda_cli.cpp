@@ -357,8 +357,8 @@ int main(int argc, char** argv) {
       if (a.verbose) {
         cum += s.time_iteration;
         std::cerr << "iteration= " << i << "\t chi2= " << fixed6(s.chi2) << "\t time= " << s.time_iteration
-                  << "\t cumTime= " << cum << "\t edges= " << hinfo.num_active_edges << "\t schur= "
-                  << (hinfo.num_free_points > 0 ? 1 : 0);
+                  << "\t cumTime= " << cum << "\t edges= " << hinfo.num_active_edges;
+        if (params.algorithm != G2OC_ALGO_DOGLEG) std::cerr << "\t schur= " << (hinfo.num_free_points > 0 ? 1 : 0);
         if (params.algorithm == G2OC_ALGO_LEVENBERG)
           std::cerr << "\t lambda= " << fixed6(s.lambda) << "\t levenbergIter= " << s.levenberg_iterations;
         if (params.algorithm == G2OC_ALGO_DOGLEG) {

@@ -379,3 +379,14 @@ def test_cli_compute_marginals(tmp_path):
     nfree = int((g.pose_fixed == 0).sum())
     assert r.stderr.count("Vertex id:") == nfree
     assert r.stderr.count("inv block :") == 2 * nfree - 1
+
+
+@pytest.mark.gpu
+def test_cli_dogleg_verbose(tmp_path):
+    g = synth.pose_graph_2d(num_poses=60, num_closures=20, seed=34)
+    src = tmp_path / "pg.g2o"
+    G2oFile.from_graph(g).save(str(src))
+    r = run_cli("-i", "5", "-v", "-solver", "dl_cuda_chol", "-o", str(tmp_path / "out.g2o"), str(src))
+    assert r.returncode == 0, r.stderr
+    lines = [x for x in r.stderr.splitlines() if x.startswith("iteration= ")]
+    assert lines and all("Delta= " in x and "step= " in x and "tries= " in x for x in lines)
