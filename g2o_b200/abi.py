@@ -32,7 +32,7 @@ ERROR_NAMES = {
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
 EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ = 1, 2, 3, 4
 BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
-ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG = 0, 1, 2
+ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG, ALGO_STRUCTURE_ONLY = 0, 1, 2, 3
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2

@@ -90,6 +90,7 @@ def library() -> C.CDLL:
                                             C.c_int32, ip], C.c_int),
         "g2oc_set_sharding": ([vp, C.c_int32, C.c_int32, ALLREDUCE_FN, vp], C.c_int),
         "g2oc_compute_marginals": ([vp, C.c_int32, ip, dp], C.c_int),
+        "g2oc_structure_only": ([vp, C.c_int32, C.c_int32], C.c_int),
         "g2oc_solve_pattern_block_system": ([vp, C.c_int32, ip, C.c_int32, ip, dp, C.c_int32, ip, dp], C.c_int),
         "g2oc_file_load": ([C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
         "g2oc_file_parse": ([C.c_char_p, C.c_size_t, C.c_char_p, C.POINTER(vp)], C.c_int),
@@ -338,6 +339,10 @@ class CudaProblem:
         _check(library().g2oc_backward(self._h, _p(dx), _p(dmeas), _p(dlogw), C.byref(st)))
         return dmeas, dlogw, {"refinement_steps": st.refinement_steps, "pcg_iterations": st.pcg_iterations,
                               "relative_residual": st.relative_residual}
+
+    def structure_only(self, num_iters=1, num_max_trials=10):
+        """StructureOnlySolver<3>::calc on every free landmark, cameras fixed."""
+        _check(library().g2oc_structure_only(self._h, int(num_iters), int(num_max_trials)))
 
     def compute_marginals(self, block_indices):
         """Blocks of Hpp^-1 at the current estimates for (row, col) pairs of

@@ -93,6 +93,108 @@ static __global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials)
   block_sum2(c, r, partials + 2 * blockIdx.x);
 }
 
+// ------------------------------------------------------- structure only
+// StructureOnlySolver<3>::calc (g2o/solvers/structure_only/structure_only_solver.h:66-215)
+// for every free landmark, the cameras held fixed: each landmark runs its own
+// small Levenberg-Marquardt on its 3x3 system (mu = 0.01, nu = 2; stop when
+// |b| < 0.001 or after num_max_trials rejected steps), with robust chi2
+// rho[0] and the rho'-weighted quadratic form. Landmarks are independent: one
+// thread each, its edges the landmark's contiguous device range.
+__device__ __forceinline__ double so_robust_chi2(const BAEdges& E, const BAVertices& V, int k0, int k1) {
+  double s = 0.0;
+  for (int k = k0; k < k1; ++k) {
+    double e[2], Xc[3], chi2, w;
+    const double4 om = E.om[k];
+    ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, w);
+    if (om.w > 0.0) {
+      double rho[3];
+      huber(chi2, om.w, rho);
+      s += rho[0];
+    } else {
+      s += chi2;
+    }
+  }
+  return s;
+}
+
+static __global__ void ba_structure_only(BAEdges E, BAVertices V, const int* l_ptr, int Pf, int num_iters,
+                                         int num_max_trials) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= Pf) return;
+  double* X = V.pt + (size_t)V.free_point[l] * 4;
+  const int k0 = l_ptr[l], k1 = l_ptr[l + 1];
+  double chi2 = so_robust_chi2(E, V, k0, k1);
+  double mu = 0.01, nu = 2.0;
+  bool stop = false;
+  for (int ig = 0; ig < num_iters; ++ig) {
+    double H[6] = {0, 0, 0, 0, 0, 0};  // 00 01 02 11 12 22
+    double b[3] = {0, 0, 0};
+    for (int k = k0; k < k1; ++k) {
+      double e[2], Xc[3], c2, w;
+      const int2 v = E.v[k];
+      const double4 om = E.om[k];
+      ba_edge_error(V, v, E.z[k], om, e, Xc, c2, w);
+      double Jp[6], Jc[12];
+      ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jp, Jc);
+      // weightedOmega = rho' Omega, omega_r = -rho' Omega e (constructQuadraticForm)
+      const double w00 = w * om.x, w01 = w * om.y, w11 = w * om.z;
+      const double r0 = -(om.x * e[0] + om.y * e[1]) * w, r1 = -(om.y * e[0] + om.z * e[1]) * w;
+      double WJ[6];  // (rho' Omega) Jp, 2x3
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        WJ[c] = w00 * Jp[c] + w01 * Jp[3 + c];
+        WJ[3 + c] = w01 * Jp[c] + w11 * Jp[3 + c];
+      }
+      H[0] += Jp[0] * WJ[0] + Jp[3] * WJ[3];
+      H[1] += Jp[0] * WJ[1] + Jp[3] * WJ[4];
+      H[2] += Jp[0] * WJ[2] + Jp[3] * WJ[5];
+      H[3] += Jp[1] * WJ[1] + Jp[4] * WJ[4];
+      H[4] += Jp[1] * WJ[2] + Jp[4] * WJ[5];
+      H[5] += Jp[2] * WJ[2] + Jp[5] * WJ[5];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) b[c] += Jp[c] * r0 + Jp[3 + c] * r1;
+    }
+    if (sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) < 0.001) break;
+    int trial = 0;
+    do {
+      // LDL^T of H + mu I
+      const double a00 = H[0] + mu, a11 = H[3] + mu, a22 = H[5] + mu;
+      const double d0 = a00;
+      const double l10 = H[1] / d0, l20 = H[2] / d0;
+      const double d1 = a11 - l10 * l10 * d0;
+      const double l21 = (H[4] - l20 * l10 * d0) / d1;
+      const double d2 = a22 - l20 * l20 * d0 - l21 * l21 * d1;
+      bool good = false;
+      if (d0 > 0.0 && d1 > 0.0 && d2 > 0.0) {
+        const double y0 = b[0], y1 = b[1] - l10 * y0, y2 = b[2] - l20 * y0 - l21 * y1;
+        const double z2 = y2 / d2, z1 = y1 / d1 - l21 * z2, z0 = y0 / d0 - l10 * z1 - l20 * z2;
+        const double old[3] = {X[0], X[1], X[2]};
+        X[0] += z0;
+        X[1] += z1;
+        X[2] += z2;
+        const double new_chi2 = so_robust_chi2(E, V, k0, k1);
+        if (chi2 - new_chi2 > 0.0 && isfinite(new_chi2)) {
+          good = true;
+          chi2 = new_chi2;
+        } else {
+          X[0] = old[0];
+          X[1] = old[1];
+          X[2] = old[2];
+        }
+      }
+      if (good) {
+        mu *= 1.0 / 3.0;
+        nu = 2.0;
+        break;
+      }
+      mu *= nu;
+      nu *= 2.0;
+      if (++trial >= num_max_trials) stop = true;
+    } while (!stop);
+    if (stop) break;
+  }
+}
+
 // per-edge errors (parity hook)
 static __global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;

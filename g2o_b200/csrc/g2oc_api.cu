@@ -1574,6 +1574,36 @@ static int dl_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
   return G2OC_OK;
 }
 
+static int structure_only(g2oc_ctx* c, int num_iters, int num_max_trials) {
+  const Structure& S = c->S;
+  if (!S.ba) {
+    set_error("the structure-only solver optimizes the landmarks of a bundle adjustment");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  if (S.Pf == 0 || num_iters <= 0) return G2OC_OK;
+  G2OC_K(K_OPLUS) ba_structure_only<<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(),
+                                                                              c->l_ptr.p, S.Pf, num_iters,
+                                                                              num_max_trials);
+  G2OC_LAUNCH_CHECK();
+  c->chi2_carry = false;
+  c->system_built = false;
+  return G2OC_OK;
+}
+
+// StructureOnlySolver::solve (structure_only_solver.h:62-65): calc(points, 1)
+static int so_iteration(g2oc_ctx* c, g2oc_iteration_stats* stv, int* result) {
+  cudaEvent_t t0 = c->mark();
+  G2OC_TRY(structure_only(c, 1, c->prm.max_trials_after_failure));
+  c->span(t0, &stv->time_update);
+  G2OC_TRY(chi2_to(c, &c->sc.p->chi2_plain, &c->sc.p->chi2_current));
+  DevScalars h{};
+  G2OC_TRY(read_state(c, &h, stv));
+  stv->chi2 = h.chi2_current;
+  c->resolve_spans();
+  *result = G2OC_RESULT_OK;
+  return G2OC_OK;
+}
+
 static int reset_pcg(g2oc_ctx* c) {
   PcgState p{};
   p.residual_carry = -1.0;
@@ -1650,6 +1680,7 @@ static const char* kSolvers[][2] = {
     {"dl_cuda", "Dogleg: B200 block solver, FP64, PCG with Schur / Cholesky without"},
     {"dl_cuda_pcg", "Dogleg: B200 block solver, FP64, block-Jacobi PCG"},
     {"dl_cuda_chol", "Dogleg: B200 block solver, FP64, dense Cholesky"},
+    {"structure_only_cuda_3", "Optimize the landmark positions (3D), cameras fixed: one small LM per landmark"},
 };
 
 int g2oc_list_solvers(char* buf, size_t size) {
@@ -1680,6 +1711,10 @@ int g2oc_construct(const char* name, g2oc_params* p) {
   }
   const std::string n(name);
   g2oc_default_params(p);
+  if (n == "structure_only_cuda_3") {
+    p->algorithm = G2OC_ALGO_STRUCTURE_ONLY;  // StructureOnlyCreator (g2o/solvers/structure_only/structure_only.cpp)
+    return G2OC_OK;
+  }
   p->algorithm = n.substr(0, 2) == "gn"   ? G2OC_ALGO_GAUSS_NEWTON
                  : n.substr(0, 2) == "dl" ? G2OC_ALGO_DOGLEG
                                           : G2OC_ALGO_LEVENBERG;
@@ -1761,7 +1796,7 @@ int g2oc_set_params(g2oc_ctx* c, const g2oc_params* p) {
     set_error("params is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
-  if (p->algorithm < 0 || p->algorithm > 2 || p->linear_solver < 0 || p->linear_solver > 2 || p->precision < 0 ||
+  if (p->algorithm < 0 || p->algorithm > 3 || p->linear_solver < 0 || p->linear_solver > 2 || p->precision < 0 ||
       p->precision > 1 || p->max_trials_after_failure < 1 || p->pcg_tolerance < 0 ||
       (p->algorithm == G2OC_ALGO_DOGLEG && (!(p->initial_delta > 0) || !(p->lambda_factor > 0)))) {
     set_error("invalid parameter value");
@@ -2112,7 +2147,7 @@ static int check_sharding(g2oc_ctx* c) {
   if (c->shard_world <= 1) return G2OC_OK;
   const Structure& S = c->S;
   if (!S.ba || !S.schur || !S.tile_ok || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY || pcg_mode() != PCG_AUTO ||
-      c->prm.algorithm == G2OC_ALGO_DOGLEG ||
+      c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY ||
       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0)) {
     set_error("sharded mode runs bundle adjustments with >= %d free cameras and landmarks, the PCG solver, FP64 or "
               "mixed precision without FP64 refinement",
@@ -2155,6 +2190,7 @@ static int optimize_impl(g2oc_ctx* c, int iterations, g2oc_iteration_stats* stat
     cudaEvent_t t0 = c->mark();
     if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, i, &stv, &result));
     else if (c->prm.algorithm == G2OC_ALGO_DOGLEG) G2OC_TRY(dl_iteration(c, i, &stv, &result));
+    else if (c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY) G2OC_TRY(so_iteration(c, &stv, &result));
     else G2OC_TRY(gn_iteration(c, i, &stv, &result));
     stv.iteration = i;
     stv.result = result;
@@ -2179,6 +2215,7 @@ static int iterate_impl(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats,
   cudaEvent_t t0 = c->mark();
   if (c->prm.algorithm == G2OC_ALGO_LEVENBERG) G2OC_TRY(lm_iteration(c, iteration, &stv, result));
   else if (c->prm.algorithm == G2OC_ALGO_DOGLEG) G2OC_TRY(dl_iteration(c, iteration, &stv, result));
+  else if (c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY) G2OC_TRY(so_iteration(c, &stv, result));
   else G2OC_TRY(gn_iteration(c, iteration, &stv, result));
   stv.iteration = iteration;
   stv.result = *result;
@@ -2203,6 +2240,21 @@ int g2oc_iterate(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stats, int* r
   const int st = iterate_impl(c, iteration, stats, result);
   if (st != G2OC_OK) c->drop_spans();
   return st;
+}
+
+int g2oc_structure_only(g2oc_ctx* c, int32_t num_iters, int32_t num_max_trials) {
+  G2OC_TRY(check_ctx(c, true));
+  if (num_iters < 0 || num_max_trials < 1) {
+    set_error("num_iters < 0 or num_max_trials < 1");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (c->batch || c->shard_world > 1) {
+    set_error("the structure-only solver runs on a single bundle adjustment context");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  G2OC_TRY(structure_only(c, num_iters, num_max_trials));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G2OC_OK;
 }
 
 int g2oc_chi2(g2oc_ctx* c, double* chi2, double* robust) {

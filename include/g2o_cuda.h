@@ -97,6 +97,8 @@ extern "C" {
 #define G2OC_ALGO_GAUSS_NEWTON 0
 #define G2OC_ALGO_LEVENBERG 1
 #define G2OC_ALGO_DOGLEG 2 /* OptimizationAlgorithmDogleg (g2o/core/optimization_algorithm_dogleg.cpp:62-180) */
+#define G2OC_ALGO_STRUCTURE_ONLY 3 /* StructureOnlySolver<3> (g2o/solvers/structure_only/structure_only_solver.h:57-215):
+                                     every iteration is calc(points, 1, max_trials_after_failure) */
 
 #define G2OC_LINEAR_PCG 0      /* block-Jacobi PCG (LinearSolverPCG semantics) */
 #define G2OC_LINEAR_CHOLESKY 1 /* dense Cholesky of the (reduced) system */
@@ -242,6 +244,11 @@ int g2oc_get_pattern(g2oc_ctx* ctx, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* s
 int g2oc_get_hessian(g2oc_ctx* ctx, double* hpp, double* hll, double* hpl, double* b);
 int g2oc_schur(g2oc_ctx* ctx, double lambda, double* schur_blocks, double* bschur);
 int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations);
+/* StructureOnlySolver<3>::calc(points, num_iters, num_max_trials) on every
+   free landmark of a bundle adjustment, the cameras held fixed: each landmark
+   runs its own Levenberg-Marquardt on its 3x3 system (one thread per
+   landmark). G2OC_ERR_NOT_SUPPORTED for pose graphs. */
+int g2oc_structure_only(g2oc_ctx* ctx, int32_t num_iters, int32_t num_max_trials);
 /* Marginal covariances: blocks of Hpp^-1, Hpp the pose part of H built at the
    current estimates (no lambda; for bundle adjustment the camera blocks only,
    as BlockSolver::computeMarginals passes _Hpp). block_indices holds

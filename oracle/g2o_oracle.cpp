@@ -1490,6 +1490,101 @@ int dl_solve(orc_problem* p, int iteration, g2oc_iteration_stats* st) {
   return G2OC_RESULT_OK;
 }
 
+double so_point_chi2(orc_problem* p, const std::vector<int>& edges) {
+  double s = 0;
+  for (int e : edges) {
+    double er[2];
+    compute_edge_error(p, e, er);
+    const double c = edge_chi2(p, e, er);
+    if (!p->delta.empty() && p->delta[e] > 0) {
+      double rho[3];
+      huber(c, p->delta[e], rho);
+      s += rho[0];
+    } else {
+      s += c;
+    }
+  }
+  return s;
+}
+
+int so_calc(orc_problem* p, int num_iters, int num_max_trials) {
+  // StructureOnlySolver<3>::calc (g2o/solvers/structure_only/structure_only_solver.h:66-215)
+  // over the free landmarks, each with its edges ordered by camera
+  std::vector<std::vector<int>> track(p->P);
+  for (int e : p->act) track[p->ev[2 * e]].push_back(e);
+  for (auto& t : track)
+    std::stable_sort(t.begin(), t.end(), [&](int a, int b) { return p->ev[2 * a + 1] < p->ev[2 * b + 1]; });
+  for (int i = 0; i < p->P; ++i) {
+    if (p->point_l[i] < 0) continue;  // fixed or inactive
+    const std::vector<int>& tr = track[i];
+    double* X = point_ptr(p, i);
+    double chi2 = so_point_chi2(p, tr);
+    double mu = 0.01, nu = 2;
+    bool stop = false;
+    for (int ig = 0; ig < num_iters; ++ig) {
+      double H[9] = {0}, b[3] = {0};
+      for (int e : tr) {
+        double er[2], Jp[6], Jc[12];
+        compute_edge_error(p, e, er);
+        compute_edge_jac(p, e, Jp, Jc);
+        const double* Om = p->info.data() + (size_t)e * 4;
+        double w = 1;
+        if (!p->delta.empty() && p->delta[e] > 0) {
+          double rho[3];
+          huber(edge_chi2(p, e, er), p->delta[e], rho);
+          w = rho[1];
+        }
+        // constructQuadraticForm with robustInformation (base_fixed_sized_edge.hpp:48-63)
+        const double r0 = -(Om[0] * er[0] + Om[1] * er[1]) * w, r1 = -(Om[2] * er[0] + Om[3] * er[1]) * w;
+        for (int a = 0; a < 3; ++a) {
+          b[a] += Jp[a] * r0 + Jp[3 + a] * r1;
+          for (int c = 0; c < 3; ++c)
+            H[a * 3 + c] += w * (Jp[a] * (Om[0] * Jp[c] + Om[1] * Jp[3 + c]) + Jp[3 + a] * (Om[2] * Jp[c] + Om[3] * Jp[3 + c]));
+        }
+      }
+      if (std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]) < 0.001) break;
+      int trial = 0;
+      do {
+        // (H + mu I) delta = b by an LDL^T factorization (Eigen::LDLT in g2o;
+        // isPositive: every pivot positive)
+        const double d0 = H[0] + mu;
+        const double l10 = H[1] / d0, l20 = H[2] / d0;
+        const double d1 = H[4] + mu - l10 * l10 * d0;
+        const double l21 = (H[5] - l20 * l10 * d0) / d1;
+        const double d2 = H[8] + mu - l20 * l20 * d0 - l21 * l21 * d1;
+        const bool positive = d0 > 0 && d1 > 0 && d2 > 0;
+        bool good = false;
+        if (positive) {
+          const double y0 = b[0], y1 = b[1] - l10 * y0, y2 = b[2] - l20 * y0 - l21 * y1;
+          double dp[3];
+          dp[2] = y2 / d2;
+          dp[1] = y1 / d1 - l21 * dp[2];
+          dp[0] = y0 / d0 - l10 * dp[1] - l20 * dp[2];
+          const double old[3] = {X[0], X[1], X[2]};
+          X[0] += dp[0]; X[1] += dp[1]; X[2] += dp[2];
+          const double newChi2 = so_point_chi2(p, tr);
+          if (chi2 - newChi2 > 0 && std::isfinite(newChi2)) {
+            good = true;
+            chi2 = newChi2;
+          } else {
+            X[0] = old[0]; X[1] = old[1]; X[2] = old[2];
+          }
+        }
+        if (good) {
+          mu *= 1. / 3.;
+          nu = 2.;
+          break;
+        }
+        mu *= nu;
+        nu *= 2.;
+        if (++trial >= num_max_trials) stop = true;
+      } while (!stop);
+      if (stop) break;
+    }
+  }
+  return G2OC_RESULT_OK;
+}
+
 int gn_solve(orc_problem* p, int iteration, g2oc_iteration_stats* st) {
   // OptimizationAlgorithmGaussNewton::solve (optimization_algorithm_gauss_newton.cpp:48-93)
   (void)iteration;
@@ -1759,6 +1854,7 @@ int orc_optimize(orc_problem* p, int iterations, g2oc_iteration_stats* stats, in
     double t = now_s();
     if (p->prm.algorithm == G2OC_ALGO_LEVENBERG) result = lm_solve(p, i, &local);
     else if (p->prm.algorithm == G2OC_ALGO_DOGLEG) result = dl_solve(p, i, &local);
+    else if (p->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY) result = so_calc(p, 1, p->prm.max_trials_after_failure);
     else result = gn_solve(p, i, &local);
     local.iteration = i;
     local.result = result;

@@ -76,7 +76,8 @@ def test_factory_lists_and_constructs():
     for n in names:
         p = fac.construct(n)
         assert p is not None, n
-        want = {"gn": abi.ALGO_GAUSS_NEWTON, "lm": abi.ALGO_LEVENBERG, "dl": abi.ALGO_DOGLEG}[n[:2]]
+        want = {"gn": abi.ALGO_GAUSS_NEWTON, "lm": abi.ALGO_LEVENBERG, "dl": abi.ALGO_DOGLEG,
+                "st": abi.ALGO_STRUCTURE_ONLY}[n[:2]]
         assert p.algorithm == want, n
     assert fac.construct("lm_cuda_mixed").precision == abi.PREC_MIXED
     assert fac.construct("lm_cuda_mixed").refine_max_iterations == 2

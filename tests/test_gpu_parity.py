@@ -451,3 +451,32 @@ def test_dogleg_matches_oracle(backend, oracle_lib, kind):
         assert abs(a["trust_radius"] - b["trust_radius"]) <= 1e-6 * b["trust_radius"], (a, b)
     assert sc[-1]["chi2"] < sc[0]["chi2"] or kind == "ba"
     c.close()
+
+
+# ------------------------------------------- StructureOnlySolver<3>
+def test_structure_only_matches_oracle(backend, oracle_lib):
+    """structure_only_cuda_3 (one small LM per landmark, cameras fixed)
+    against the oracle's restatement of StructureOnlySolver<3>::calc
+    (g2o/solvers/structure_only/structure_only_solver.h:66-215)."""
+    from g2o_b200.abi import ALGO_STRUCTURE_ONLY
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    prm = fac.construct("structure_only_cuda_3")
+    assert prm.algorithm == ALGO_STRUCTURE_ONLY
+    g = small_ba(seed=24)
+    o = oracle_lib.OracleProblem(g, prm)
+    c = backend.CudaProblem(g, prm)
+    do, so = o.optimize(3)
+    dc, sc = c.optimize(3)
+    assert do == dc == 3
+    for a, b in zip(sc, so):
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-9 * b["chi2"], (a["chi2"], b["chi2"])
+    (pc, qc), (po, qo) = c.estimates(), o.estimates()
+    assert np.array_equal(pc, g.pose_estimate)  # cameras untouched
+    assert np.abs(qc - qo).max() < 1e-9
+    # the entry point with more inner iterations keeps lowering the chi2
+    before = c.chi2()[1]
+    c.structure_only(num_iters=5, num_max_trials=10)
+    assert c.chi2()[1] <= before
+    c.close()
+    with pytest.raises(backend.G2ocError):
+        backend.CudaProblem(synth.pose_graph_2d(num_poses=50, num_closures=10, seed=2)).structure_only()
