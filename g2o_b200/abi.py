@@ -30,7 +30,7 @@ ERROR_NAMES = {
 }
 
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
-EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ = 1, 2, 3, 4
+EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_SE3_EXPMAP = 1, 2, 3, 4, 5
 BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
 ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG, ALGO_STRUCTURE_ONLY = 0, 1, 2, 3
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
@@ -39,8 +39,8 @@ RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2
 
 POSE_EST_DIM = {POSE_SE2: 3, POSE_SE3: 12, POSE_SE3EXPMAP: 7}
 POSE_DIM = {POSE_SE2: 3, POSE_SE3: 6, POSE_SE3EXPMAP: 6}
-EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2}
-MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2}
+EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 6}
+MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 7}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)

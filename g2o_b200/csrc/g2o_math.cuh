@@ -160,6 +160,96 @@ G2OC_HD SE3Q<T> se3q_mul(const SE3Q<T>& a, const SE3Q<T>& b) {
   return r;
 }
 
+// SE3Quat in the C-ABI's 7-vector (t, q: SE3Quat::toVector) and back
+template <typename T>
+G2OC_HD SE3Q<T> se3q_from7(const T* v) {
+  SE3Q<T> s;
+  s.t[0] = v[0]; s.t[1] = v[1]; s.t[2] = v[2];
+  s.q = Q4<T>{v[3], v[4], v[5], v[6]};
+  return s;
+}
+template <typename T>
+G2OC_HD void se3q_to7(const SE3Q<T>& s, T* v) {
+  v[0] = s.t[0]; v[1] = s.t[1]; v[2] = s.t[2];
+  v[3] = s.q.x; v[4] = s.q.y; v[5] = s.q.z; v[6] = s.q.w;
+}
+
+template <typename T>
+G2OC_HD SE3Q<T> se3q_inverse(const SE3Q<T>& a) {
+  // SE3Quat::inverse (se3quat.h:114-119): conjugate, t' = q' (-t); no renormalization
+  SE3Q<T> r;
+  r.q = Q4<T>{-a.q.x, -a.q.y, -a.q.z, a.q.w};
+  const T mt[3] = {a.t[0] * T(-1), a.t[1] * T(-1), a.t[2] * T(-1)};
+  quat_rotate(r.q, mt, r.t);
+  return r;
+}
+
+template <typename T>
+G2OC_HD void se3q_log(const SE3Q<T>& a, T out[6]) {
+  // SE3Quat::log (se3quat.h:165-199) with deltaR and skew (se3_ops.hpp:27-45)
+  T R[9];
+  quat_to_rot(a.q, R);
+  const T d = T(0.5) * (R[0] + R[4] + R[8] - T(1));
+  const T dR[3] = {R[7] - R[5], R[2] - R[6], R[3] - R[1]};
+  T w[3], k1, k2;
+  if (fabs(d) > T(0.99999)) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) w[i] = T(0.5) * dR[i];
+    k2 = T(1) / T(12);
+  } else {
+    const T theta = acos(d);
+    const T f = theta / (T(2) * sqrt(T(1) - d * d));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) w[i] = f * dR[i];
+    k2 = (T(1) - theta / (T(2) * tan(theta / T(2)))) / (theta * theta);
+  }
+  k1 = T(-0.5);
+  const T O[9] = {T(0), -w[2], w[1], w[2], T(0), -w[0], -w[1], w[0], T(0)};
+  T O2[9], Vi[9];
+  matmul3(O, O, O2);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Vi[i] = k1 * O[i] + k2 * O2[i];
+  Vi[0] += T(1); Vi[4] += T(1); Vi[8] += T(1);
+  out[0] = w[0]; out[1] = w[1]; out[2] = w[2];
+  matvec3(Vi, a.t, out + 3);
+}
+
+template <typename T>
+G2OC_HD void se3q_adj(const SE3Q<T>& a, T sign, T A[36]) {
+  // sign * SE3Quat::adj (se3quat.h:232-240): [[R, 0], [skew(t) R, R]], row-major
+  T R[9], S[9], SR[9];
+  quat_to_rot(a.q, R);
+  const T* t = a.t;
+  S[0] = T(0); S[1] = -t[2]; S[2] = t[1];
+  S[3] = t[2]; S[4] = T(0); S[5] = -t[0];
+  S[6] = -t[1]; S[7] = t[0]; S[8] = T(0);
+  matmul3(S, R, SR);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      A[r * 6 + c] = sign * R[r * 3 + c];
+      A[r * 6 + 3 + c] = T(0) * sign;
+      A[(3 + r) * 6 + c] = sign * SR[r * 3 + c];
+      A[(3 + r) * 6 + 3 + c] = sign * R[r * 3 + c];
+    }
+}
+
+// EdgeSE3Expmap (g2o/types/sba/edge_se3_expmap.cpp:45-72) on 7-vector
+// estimates, C the measurement: e = log(Tj^-1 C Ti);
+// J_i = adj(Tj^-1 C), J_j = -adj(Ti^-1 C^-1)
+template <typename T>
+G2OC_HD void se3exp_error(const T* xi, const T* xj, const T* c7, T e[6]) {
+  const SE3Q<T> Ti = se3q_from7(xi), Tj = se3q_from7(xj), C = se3q_from7(c7);
+  se3q_log(se3q_mul(se3q_mul(se3q_inverse(Tj), C), Ti), e);
+}
+template <typename T>
+G2OC_HD void se3exp_jacobians(const T* xi, const T* xj, const T* c7, T Ji[36], T Jj[36]) {
+  const SE3Q<T> Ti = se3q_from7(xi), Tj = se3q_from7(xj), C = se3q_from7(c7);
+  se3q_adj(se3q_mul(se3q_inverse(Tj), C), T(1), Ji);
+  se3q_adj(se3q_mul(se3q_inverse(Ti), se3q_inverse(C)), T(-1), Jj);
+}
+
 template <typename T>
 G2OC_HD void huber(T e, T delta, T rho[3]) {
   // RobustKernelHuber::robustify (g2o/core/robust_kernel_impl.cpp:60-74)

@@ -722,8 +722,12 @@ struct Engine final : EngineBase {
         G2OC_K(K_PG_ASSEMBLE_B) pg_assemble_b<3><<<cdiv((long long)S.Cf * 3, 128), 128, 0, st>>>(S.Cf, c->bv_src_ptr.p, c->bv_src.p,
                                                                        bcontrib.p, c->b.p);
       } else {
-        G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE3><<<cdiv(n, 64), 64, 0, st>>>(c->pose.p, c->pg_edges(), c->pe_trans.p,
-                                                                      hcontrib.p, bcontrib.p);
+        if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+          G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE3EXPMAP><<<cdiv(n, 64), 64, 0, st>>>(
+              c->pose.p, c->pg_edges(), c->pe_trans.p, hcontrib.p, bcontrib.p);
+        else
+          G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE3><<<cdiv(n, 64), 64, 0, st>>>(
+              c->pose.p, c->pg_edges(), c->pe_trans.p, hcontrib.p, bcontrib.p);
         G2OC_LAUNCH_CHECK();
         const int nnzb = (int)S.hpp_rc.size() / 2;
         G2OC_K(K_PG_ASSEMBLE_H) pg_assemble_h<Real, 6><<<cdiv((long long)nnzb * 6, 128), 128, 0, st>>>(nnzb, c->hb_src_ptr.p, c->hb_src.p,
@@ -1249,6 +1253,8 @@ static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
   if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
+  else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+    G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3EXPMAP><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   else G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   G2OC_LAUNCH_CHECK();
   G2OC_TRY(finalize_sum(c, S.ba ? kChi2Blocks : kRedBlocks, 2, out_plain, out_robust));
@@ -1263,6 +1269,9 @@ static int oplus(g2oc_ctx* c) {
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE2><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
                                                              c->oplus_count.p, c->flag.p);
+  else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+    G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE3EXPMAP><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf,
+                                                                                  c->x.p, c->oplus_count.p, c->flag.p);
   else G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE3><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
                                                                 c->oplus_count.p, c->flag.p);
   G2OC_LAUNCH_CHECK();
@@ -1629,6 +1638,8 @@ static int check_ctx(g2oc_ctx* c, bool need_upload) {
 static void inverse_measurement(int et, const double* m, double* out) {
   if (et == G2OC_EDGE_SE2) {
     se2_inv(m, out);
+  } else if (et == G2OC_EDGE_SE3_EXPMAP) {
+    memcpy(out, m, 7 * sizeof(double));  // EdgeSE3Expmap's error uses the measurement itself
   } else {
     iso_inv(m, out);
   }
@@ -2276,6 +2287,9 @@ int g2oc_errors(g2oc_ctx* c, double* out) {
   if (S.ba) G2OC_K(K_ERRORS) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
+  else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+    G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE3EXPMAP><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(),
+                                                                                                c->errbuf.p);
   else G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE3><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
   G2OC_LAUNCH_CHECK();
   std::vector<double> h((size_t)na * S.D);
@@ -2298,6 +2312,9 @@ int g2oc_jacobians(g2oc_ctx* c, double* j0, double* j1) {
   if (S.ba) G2OC_K(K_JACOBIANS) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
+  else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+    G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE3EXPMAP><<<cdiv(na, 64), 64, 0, c->stream>>>(c->pose.p, c->pg_edges(),
+                                                                                                    a.p, b.p);
   else G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE3><<<cdiv(na, 64), 64, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
   G2OC_LAUNCH_CHECK();
   std::vector<double> ha(a.n), hb(b.n);

@@ -1,5 +1,6 @@
 // pg_kernels.cuh -- device kernels of the pose-graph paths: EdgeSE2 between
-// VertexSE2 and EdgeSE3 between VertexSE3. The Hessian is assembled in two
+// VertexSE2, EdgeSE3 between VertexSE3 and EdgeSE3Expmap between
+// VertexSE3Expmap. The Hessian is assembled in two
 // deterministic passes: one thread per edge writes its contributions
 // (H_00, H_11, H_01 and b_0, b_1 of BaseFixedSizedEdge::constructQuadraticForm,
 // g2o/core/base_fixed_sized_edge.hpp:48-130) to scratch, then one thread per
@@ -25,6 +26,12 @@ struct PGTraits<G2OC_POSE_SE3> {
   static constexpr int EST = 12;
   static constexpr int ZD = 12;
 };
+template <>
+struct PGTraits<G2OC_POSE_SE3EXPMAP> {  // EdgeSE3Expmap between VertexSE3Expmap
+  static constexpr int PD = 6;
+  static constexpr int EST = 7;   // SE3Quat::toVector
+  static constexpr int ZD = 7;    // the measurement C itself (the error uses C, not C^-1)
+};
 
 struct PGEdges {
   int n;
@@ -42,6 +49,7 @@ __device__ __forceinline__ void pg_error(const double* est, const PGEdges& E, in
   const double* xj = est + (size_t)v.y * EST;
   const double* zi = E.zinv + (size_t)k * ZD;
   if (PT == G2OC_POSE_SE2) se2_error(xi, xj, zi, e);
+  else if (PT == G2OC_POSE_SE3EXPMAP) se3exp_error(xi, xj, zi, e);
   else se3_error(xi, xj, zi, e);
 }
 
@@ -99,6 +107,7 @@ __device__ __forceinline__ void pg_jac(const double* est, const PGEdges& E, int 
   const double* xj = est + (size_t)v.y * EST;
   const double* zi = E.zinv + (size_t)k * ZD;
   if (PT == G2OC_POSE_SE2) se2_jacobians(xi, xj, zi, J0, J1);
+  else if (PT == G2OC_POSE_SE3EXPMAP) se3exp_jacobians(xi, xj, zi, J0, J1);
   else se3_jacobians(xi, xj, zi, J0, J1);
 }
 
@@ -241,6 +250,9 @@ __global__ void pg_oplus(double* est, const int* free_pose, int Cf, const double
     X[0] += u[0];
     X[1] += u[1];
     X[2] = normalize_theta(X[2] + u[2]);
+  } else if (PT == G2OC_POSE_SE3EXPMAP) {
+    // VertexSE3Expmap::oplusImpl (g2o/types/sba/vertex_se3_expmap.cpp:48-51): T <- exp(u) T
+    se3q_to7(se3q_mul(se3q_exp(u), se3q_from7(X)), X);
   } else {
     double inc[12], Y[12];
     from_compact_quat(u + 3, inc);

@@ -19,8 +19,10 @@ namespace g2oc {
 
 namespace {
 
-int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 6 : 2; }
-int meas_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : 2; }
+int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP) ? 6 : 2; }
+int meas_dim(int et) {
+  return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : et == G2OC_EDGE_SE3_EXPMAP ? 7 : 2;
+}
 int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
 int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
 
@@ -545,10 +547,10 @@ int build_structure(const g2oc_graph* g, Structure& s) {
     return G2OC_ERR_INVALID_ARGUMENT;
   }
   const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 4 ||
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 5 ||
       (g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2) ||
       (g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3) ||
-      ba != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {
+      (ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {
     set_error("unsupported vertex/edge type combination (pose %d, edge %d)", g->pose_type, g->edge_type);
     return G2OC_ERR_BAD_GRAPH;
   }

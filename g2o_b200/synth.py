@@ -23,7 +23,7 @@ import math
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_PROJECT_XYZ, EDGE_SE3, POSE_SE2, POSE_SE3,
+from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_EXPMAP, EDGE_SE3_PROJECT_XYZ, EDGE_SE3, POSE_SE2, POSE_SE3,
                   POSE_SE3EXPMAP, Graph)
 
 SEED_BASE = 20261203
@@ -203,6 +203,28 @@ def pose_graph_3d(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
               name=f"pose_graph_3d_{n}")
     g.extra["truth"] = _iso12(R, t)
     return g
+
+
+def pose_graph_3d_expmap(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
+    """The 3D pose graph as VertexSE3Expmap / EdgeSE3Expmap: T_i = X_i^-1
+    (world to body) and C_ij = Z_ij^-1, so that log(T_j^-1 C_ij T_i) is the
+    edge error; the information blocks reordered to (rotation, translation),
+    the order of SE3Quat::log."""
+    g = pose_graph_3d(num_rings, per_ring, radius, seed)
+
+    def se3quat_of_inverse(iso):
+        R = iso[:, :9].reshape(-1, 3, 3)
+        t = iso[:, 9:]
+        Rt = np.transpose(R, (0, 2, 1))
+        return np.concatenate([-np.einsum("nab,nb->na", Rt, t), _rot_to_quat(Rt)], axis=1)
+
+    perm = [3, 4, 5, 0, 1, 2]
+    info = g.information.reshape(-1, 6, 6)[:, perm][:, :, perm].reshape(-1, 36)
+    out = Graph(POSE_SE3EXPMAP, EDGE_SE3_EXPMAP, se3quat_of_inverse(g.pose_estimate), g.edge_vertex.copy(),
+                se3quat_of_inverse(g.measurement), info, pose_fixed=g.pose_fixed.copy(),
+                name=g.name.replace("pose_graph_3d", "pose_graph_3d_expmap"))
+    out.extra["truth"] = se3quat_of_inverse(g.extra["truth"])
+    return out
 
 
 # ------------------------------------------------------ bundle adjustment

@@ -90,6 +90,8 @@ extern "C" {
 #define G2OC_EDGE_SE2 1            /* EdgeSE2(VertexSE2, VertexSE2), D=3, measurement (x,y,theta) */
 #define G2OC_EDGE_SE3 2            /* EdgeSE3(VertexSE3, VertexSE3), D=6, measurement Isometry3 (12) */
 #define G2OC_EDGE_PROJECT_XYZ2UV 3 /* EdgeProjectXYZ2UV(VertexPointXYZ, VertexSE3Expmap), D=2 */
+#define G2OC_EDGE_SE3_EXPMAP 5 /* EdgeSE3Expmap(VertexSE3Expmap, VertexSE3Expmap), D=6, measurement
+                                 SE3Quat (7, toVector: the edge's _measurement, not the file's inverse) */
 #define G2OC_EDGE_SE3_PROJECT_XYZ 4 /* EdgeSE3ProjectXYZ(VertexPointXYZ, VertexSE3Expmap), D=2, with
                                      fx = focal_length, fy = focal_length_y, (cx, cy) = principal_point */
 

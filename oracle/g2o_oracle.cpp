@@ -179,6 +179,71 @@ inline SE3Q se3q_mul(const SE3Q& a, const SE3Q& b) {
   return r;
 }
 
+inline SE3Q se3q_inv(const SE3Q& a) {
+  // SE3Quat::inverse (se3quat.h:114-119)
+  SE3Q r;
+  r.q = {-a.q.x, -a.q.y, -a.q.z, a.q.w};
+  const double mt[3] = {-a.t[0], -a.t[1], -a.t[2]};
+  quat_rotate(r.q, mt, r.t);
+  return r;
+}
+
+void se3q_log(const SE3Q& a, double out[6]) {
+  // SE3Quat::log (se3quat.h:165-199), deltaR / skew (se3_ops.hpp:27-45)
+  double R[9];
+  quat_to_rot(a.q, R);
+  const double d = 0.5 * (R[0] + R[4] + R[8] - 1);
+  const double dR[3] = {R[7] - R[5], R[2] - R[6], R[3] - R[1]};
+  double w[3], Vi[9];
+  double O[9], O2[9];
+  if (std::fabs(d) > 0.99999) {
+    for (int i = 0; i < 3; ++i) w[i] = 0.5 * dR[i];
+    const double Om[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
+    std::memcpy(O, Om, sizeof(O));
+    matmul3(O, O, O2);
+    for (int i = 0; i < 9; ++i) Vi[i] = -0.5 * O[i] + (1. / 12.) * O2[i];
+  } else {
+    const double theta = std::acos(d);
+    for (int i = 0; i < 3; ++i) w[i] = theta / (2 * std::sqrt(1 - d * d)) * dR[i];
+    const double Om[9] = {0, -w[2], w[1], w[2], 0, -w[0], -w[1], w[0], 0};
+    std::memcpy(O, Om, sizeof(O));
+    matmul3(O, O, O2);
+    const double k = (1 - theta / (2 * std::tan(theta / 2))) / (theta * theta);
+    for (int i = 0; i < 9; ++i) Vi[i] = -0.5 * O[i] + k * O2[i];
+  }
+  Vi[0] += 1; Vi[4] += 1; Vi[8] += 1;
+  out[0] = w[0]; out[1] = w[1]; out[2] = w[2];
+  matvec3(Vi, a.t, out + 3);
+}
+
+void se3q_adj(const SE3Q& a, double sign, double A[36]) {
+  // SE3Quat::adj (se3quat.h:232-240)
+  double R[9], SR[9];
+  quat_to_rot(a.q, R);
+  const double S[9] = {0, -a.t[2], a.t[1], a.t[2], 0, -a.t[0], -a.t[1], a.t[0], 0};
+  matmul3(S, R, SR);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      A[r * 6 + c] = sign * R[r * 3 + c];
+      A[r * 6 + 3 + c] = 0;
+      A[(3 + r) * 6 + c] = sign * SR[r * 3 + c];
+      A[(3 + r) * 6 + 3 + c] = sign * R[r * 3 + c];
+    }
+}
+
+// EdgeSE3Expmap (g2o/types/sba/edge_se3_expmap.cpp:45-72): vertex0 = i,
+// vertex1 = j, measurement C: e = log(Tj^-1 C Ti), J_i = adj(Tj^-1 C),
+// J_j = -adj(Ti^-1 C^-1)
+void se3exp_error(const double* xi, const double* xj, const double* c7, double e[6]) {
+  const SE3Q Ti = se3q_load(xi), Tj = se3q_load(xj), C = se3q_load(c7);
+  se3q_log(se3q_mul(se3q_mul(se3q_inv(Tj), C), Ti), e);
+}
+void se3exp_jacobians(const double* xi, const double* xj, const double* c7, double Ji[36], double Jj[36]) {
+  const SE3Q Ti = se3q_load(xi), Tj = se3q_load(xj), C = se3q_load(c7);
+  se3q_adj(se3q_mul(se3q_inv(Tj), C), 1.0, Ji);
+  se3q_adj(se3q_mul(se3q_inv(Ti), se3q_inv(C)), -1.0, Jj);
+}
+
 // Isometry3 as R (row-major 9) and t (3): 12 doubles
 struct Iso3 {
   double R[9];
@@ -336,8 +401,10 @@ bool inverse_small(const double* A, int n, double* out) {
 
 // ---------------------------------------------------------- edge functions
 
-int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 6 : 2; }
-int meas_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : 2; }
+int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP) ? 6 : 2; }
+int meas_dim(int et) {
+  return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : et == G2OC_EDGE_SE3_EXPMAP ? 7 : 2;
+}
 int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
 int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
 
@@ -811,7 +878,8 @@ void compute_edge_error(orc_problem* p, int e, double* out) {
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out);
   else
-    se3_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out);
+    p->edge_type == G2OC_EDGE_SE3_EXPMAP ? se3exp_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out)
+                                         : se3_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out);
 }
 
 void compute_edge_jac(orc_problem* p, int e, double* J0, double* J1) {
@@ -822,7 +890,8 @@ void compute_edge_jac(orc_problem* p, int e, double* J0, double* J1) {
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1);
   else
-    se3_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1);
+    p->edge_type == G2OC_EDGE_SE3_EXPMAP ? se3exp_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1)
+                                         : se3_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1);
 }
 
 double edge_chi2(const orc_problem* p, int e, const double* er) {
@@ -1635,10 +1704,10 @@ int orc_create(const g2oc_graph* g, orc_problem** out) {
   if (!g || !out) return G2OC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 4) return G2OC_ERR_BAD_GRAPH;
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 5) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2)) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3)) return G2OC_ERR_BAD_GRAPH;
-  if (ba != (g->pose_type == G2OC_POSE_SE3EXPMAP)) return G2OC_ERR_BAD_GRAPH;
+  if ((ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) return G2OC_ERR_BAD_GRAPH;
   if (g->num_poses < 0 || g->num_points < 0 || g->num_edges <= 0) return G2OC_ERR_BAD_GRAPH;
   if (!g->pose_estimate || !g->edge_vertex || !g->measurement || !g->information) return G2OC_ERR_INVALID_ARGUMENT;
   if (ba && g->num_points > 0 && !g->point_estimate) return G2OC_ERR_INVALID_ARGUMENT;

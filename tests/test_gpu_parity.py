@@ -480,3 +480,33 @@ def test_structure_only_matches_oracle(backend, oracle_lib):
     c.close()
     with pytest.raises(backend.G2ocError):
         backend.CudaProblem(synth.pose_graph_2d(num_poses=50, num_closures=10, seed=2)).structure_only()
+
+
+# ------------------------------------------- EdgeSE3Expmap pose graph
+@pytest.mark.parametrize("linear", ["chol", "pcg"])
+def test_se3_expmap_pose_graph_matches_oracle(backend, oracle_lib, linear):
+    """EdgeSE3Expmap between VertexSE3Expmap (g2o/types/sba/edge_se3_expmap.cpp)
+    on the pose-graph kernels: errors 1e-12, Jacobians and Hessian 1e-10, a
+    10-iteration LM trajectory (trial counts equal, chi2 1e-7; PCG 1e-6)."""
+    from g2o_b200.abi import EDGE_SE3_EXPMAP
+    g = synth.pose_graph_3d_expmap(num_rings=4, per_ring=40, radius=10.0, seed=4)
+    assert g.edge_type == EDGE_SE3_EXPMAP
+    lin = LINEAR_CHOLESKY if linear == "chol" else LINEAR_PCG
+    o, c = both(backend, oracle_lib, g, algorithm=ALGO_LEVENBERG, linear_solver=lin)
+    for a, b in zip(o.pattern(), c.pattern()):
+        assert np.array_equal(a, b)
+    assert relnorm(c.errors(), o.errors()) < 1e-12
+    j = c.jacobians(), o.jacobians()
+    assert rel_block_err(j[0][0], j[1][0]) < 1e-10 and rel_block_err(j[0][1], j[1][1]) < 1e-10
+    o.build_system()
+    c.build_system()
+    assert rel_block_err(c.hessian()[0], o.hessian()[0]) < 1e-10
+    do, so = o.optimize(10)
+    dc, sc = c.optimize(10)
+    assert do == dc
+    tol = 1e-7 if linear == "chol" else 1e-6
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"]
+        assert abs(a["chi2"] - b["chi2"]) <= tol * b["chi2"], (a["chi2"], b["chi2"])
+    assert sc[-1]["chi2"] < sc[0]["chi2"]
+    c.close()

@@ -230,3 +230,61 @@ def test_projection_jacobians_match_numeric(oracle_lib, focal_y):
         b0, b1 = oracle_lib.OracleProblem(g2).jacobians()
         np.testing.assert_allclose(a1[:, 0], b1[:, 0], rtol=1e-12)
         np.testing.assert_allclose(a1[:, 1], b1[:, 1] * (455.0 / 500.0), rtol=1e-12)
+
+
+def test_edge_se3_expmap_error_and_jacobians(oracle_lib):
+    """EdgeSE3Expmap (g2o/types/sba/edge_se3_expmap.cpp:45-72): with T_i = I
+    and C = I the error log(T_j^-1 C T_i) of T_j = exp(u)^-1 is u itself
+    (SE3Quat::log inverts SE3Quat::exp, se3quat.h:165-230); g2o's analytic
+    Jacobians (adjoints, without the left Jacobian of the log) match central
+    differences to first order in the error."""
+    from g2o_b200.abi import EDGE_SE3_EXPMAP, POSE_SE3EXPMAP
+    rng = np.random.default_rng(7)
+    n = 200
+    us = rng.normal(0, 0.6, (n, 6))
+    poses, meas = [], []
+    for u in us:
+        R = _rodrigues(u[:3])
+        theta = np.linalg.norm(u[:3])
+        K = _skew(u[:3])
+        V = np.eye(3) + (1 - np.cos(theta)) / theta ** 2 * K + (theta - np.sin(theta)) / theta ** 3 * K @ K
+        t = V @ u[3:]
+        Rt = R.T  # T_j = exp(u)^-1 = (R^T, -R^T t)
+        poses += [[0, 0, 0, 0, 0, 0, 1], list(-Rt @ t) + list(_quat_xyzw(Rt))]
+        meas.append([0, 0, 0, 0, 0, 0, 1])
+    g = Graph(POSE_SE3EXPMAP, EDGE_SE3_EXPMAP, np.array(poses), np.arange(2 * n).reshape(n, 2),
+              np.array(meas, float), np.tile(np.eye(6).reshape(1, 36), (n, 1)))
+    p = oracle_lib.OracleProblem(g)
+    np.testing.assert_allclose(p.errors().reshape(n, 6), us, rtol=0, atol=1e-9)
+    # near zero error the adjoints are the derivatives
+    small = us * 1e-4
+    poses2 = []
+    for u in small:
+        R = _rodrigues(u[:3])
+        poses2 += [[0, 0, 0, 0, 0, 0, 1], list(-R.T @ u[3:]) + list(_quat_xyzw(R.T))]
+    g2 = Graph(POSE_SE3EXPMAP, EDGE_SE3_EXPMAP, np.array(poses2), g.edge_vertex, g.measurement, g.information)
+    p2 = oracle_lib.OracleProblem(g2)
+    a0, a1 = p2.jacobians()
+    n0, n1 = p2.jacobians(numeric=True)
+    assert np.abs(a0 - n0).max() < 1e-3 and np.abs(a1 - n1).max() < 1e-3
+
+
+def _skew(w):
+    return np.array([[0, -w[2], w[1]], [w[2], 0, -w[0]], [-w[1], w[0], 0]])
+
+
+def _rodrigues(w):
+    th = np.linalg.norm(w)
+    K = _skew(w)
+    if th < 1e-12:
+        return np.eye(3) + K
+    return np.eye(3) + np.sin(th) / th * K + (1 - np.cos(th)) / th ** 2 * K @ K
+
+
+def _quat_xyzw(R):
+    w = 0.5 * np.sqrt(max(1.0 + R[0, 0] + R[1, 1] + R[2, 2], 0.0))
+    x = 0.5 * np.sqrt(max(1.0 + R[0, 0] - R[1, 1] - R[2, 2], 0.0)) * np.sign(R[2, 1] - R[1, 2] or 1.0)
+    y = 0.5 * np.sqrt(max(1.0 - R[0, 0] + R[1, 1] - R[2, 2], 0.0)) * np.sign(R[0, 2] - R[2, 0] or 1.0)
+    z = 0.5 * np.sqrt(max(1.0 - R[0, 0] - R[1, 1] + R[2, 2], 0.0)) * np.sign(R[1, 0] - R[0, 1] or 1.0)
+    q = np.array([x, y, z, w])
+    return q / np.linalg.norm(q)
