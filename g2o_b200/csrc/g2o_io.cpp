@@ -22,17 +22,19 @@ using g2oc::set_error;
 namespace {
 
 enum Kind : int8_t { kNone = 0, kSE2 = 1, kSE3 = 2, kExpmap = 3, kXYZ = 4 };
-enum EKind : int8_t { eSE2 = G2OC_EDGE_SE2, eSE3 = G2OC_EDGE_SE3, eProj = G2OC_EDGE_PROJECT_XYZ2UV };
+enum EKind : int8_t { eSE2 = G2OC_EDGE_SE2, eSE3 = G2OC_EDGE_SE3, eProj = G2OC_EDGE_PROJECT_XYZ2UV,
+                      eSE3Exp = G2OC_EDGE_SE3_EXPMAP };
 
 const char* const kVertexTag[5] = {"", "VERTEX_SE2", "VERTEX_SE3:QUAT", "VERTEX_SE3:EXPMAP", "VERTEX_TRACKXYZ"};
-const char* const kEdgeTag[4] = {"", "EDGE_SE2", "EDGE_SE3:QUAT", "EDGE_PROJECT_XYZ2UV:EXPMAP"};
+// indexed by G2OC_EDGE_*; EdgeSE3ProjectXYZ has no file form with its intrinsics
+const char* const kEdgeTag[6] = {"", "EDGE_SE2", "EDGE_SE3:QUAT", "EDGE_PROJECT_XYZ2UV:EXPMAP", "", "EDGE_SE3:EXPMAP"};
 const char* const kCameraTag = "PARAMS_CAMERAPARAMETERS";
 
 // estimate doubles per vertex kind in the C-ABI layout
 int est_dim(int k) { return k == kSE2 ? 3 : k == kSE3 ? 12 : k == kExpmap ? 7 : 3; }
 int vertex_dim(int k) { return k == kSE2 || k == kXYZ ? 3 : 6; }
-int meas_dim(int e) { return e == eSE2 ? 3 : e == eSE3 ? 12 : 2; }
-int err_dim(int e) { return e == eSE2 ? 3 : e == eSE3 ? 6 : 2; }
+int meas_dim(int e) { return e == eSE2 ? 3 : e == eSE3 ? 12 : e == eSE3Exp ? 7 : 2; }
+int err_dim(int e) { return e == eSE2 ? 3 : (e == eSE3 || e == eSE3Exp) ? 6 : 2; }
 
 struct Vtx {
   int32_t id;
@@ -185,8 +187,8 @@ std::string trim(const std::string& s) {
 bool known_tag(const std::string& t) {
   for (int k = 1; k <= 4; ++k)
     if (t == kVertexTag[k]) return true;
-  for (int k = 1; k <= 3; ++k)
-    if (t == kEdgeTag[k]) return true;
+  for (int k = 1; k <= 5; ++k)
+    if (kEdgeTag[k][0] && t == kEdgeTag[k]) return true;
   return t == kCameraTag;
 }
 
@@ -298,8 +300,8 @@ void g2oc_file::parse_line(Line L, int lineno) {
   int vk = kNone, ek = 0;
   for (int k = 1; k <= 4; ++k)
     if (tag == kVertexTag[k]) vk = k;
-  for (int k = 1; k <= 3; ++k)
-    if (tag == kEdgeTag[k]) ek = k;
+  for (int k = 1; k <= 5; ++k)
+    if (kEdgeTag[k][0] && tag == kEdgeTag[k]) ek = k;
   if (vk != kNone) {
     int32_t id;
     double v[7];
@@ -361,7 +363,8 @@ void g2oc_file::parse_line(Line L, int lineno) {
     }
     const int k0 = vtx[i0->second].kind, k1 = vtx[i1->second].kind;
     const bool types_ok = (ek == eSE2 && k0 == kSE2 && k1 == kSE2) || (ek == eSE3 && k0 == kSE3 && k1 == kSE3) ||
-                          (ek == eProj && k0 == kXYZ && k1 == kExpmap);
+                          (ek == eProj && k0 == kXYZ && k1 == kExpmap) ||
+                          (ek == eSE3Exp && k0 == kExpmap && k1 == kExpmap);
     if (!types_ok) {
       info.lines_rejected++;
       problem(lineno, tag, "vertex types do not match the edge");
@@ -376,7 +379,7 @@ void g2oc_file::parse_line(Line L, int lineno) {
     const int D = err_dim(ek), M = meas_dim(ek);
     double m[7];
     double I[36];
-    const int nm = ek == eSE2 ? 3 : ek == eSE3 ? 7 : 2;
+    const int nm = ek == eSE2 ? 3 : (ek == eSE3 || ek == eSE3Exp) ? 7 : 2;
     if (!L.nums(m, nm) || !L.info(I, D)) {
       info.lines_rejected++;
       problem(lineno, tag, "missing or invalid numbers");
@@ -398,6 +401,13 @@ void g2oc_file::parse_line(Line L, int lineno) {
       quat_normalize(q);
       quat_to_rot(q[0], q[1], q[2], q[3], d);
       d[9] = m[0]; d[10] = m[1]; d[11] = m[2];
+    } else if (ek == eSE3Exp) {
+      // EdgeSE3Expmap::read: setMeasurement(SE3Quat(meas).inverse()) (edge_se3_expmap.cpp:33-38)
+      double q[4] = {m[3], m[4], m[5], m[6]};
+      if (q[3] < 0) for (double& cq : q) cq *= -1;
+      quat_normalize(q);
+      const double s7[7] = {m[0], m[1], m[2], q[0], q[1], q[2], q[3]};
+      se3quat_inverse(s7, d);
     } else {
       for (int i = 0; i < M; ++i) d[i] = m[i];
     }
@@ -444,7 +454,7 @@ int g2oc_file::build_view() {
     set_error("the graph has no edge");
     return G2OC_ERR_BAD_GRAPH;
   }
-  const int pk = et == eSE2 ? kSE2 : et == eSE3 ? kSE3 : kExpmap;
+  const int pk = et == eSE2 ? kSE2 : et == eSE3 ? kSE3 : kExpmap;  // projection and SE3Expmap edges: VertexSE3Expmap
   focal = 1.0; pp[0] = pp[1] = 0.0;
   if (et == eProj) {
     const Cam& c0 = params.at(edg[0].param);
@@ -543,6 +553,10 @@ void g2oc_file::write_edge(std::string& s, const Edg& e) const {
   if (e.kind == eSE3) {
     double w[7];
     iso_to_qt(d, w);
+    for (double x : w) put(s, x);
+  } else if (e.kind == eSE3Exp) {
+    double w[7];
+    se3quat_inverse(d, w);  // EdgeSE3Expmap::write: measurement().inverse().toVector()
     for (double x : w) put(s, x);
   } else {
     for (int i = 0; i < M; ++i) put(s, d[i]);
@@ -660,7 +674,8 @@ int g2oc_file_from_graph(const g2oc_graph* g, const int32_t* pose_ids, const int
   int vk, ek = g->edge_type;
   if (g->pose_type == G2OC_POSE_SE2 && ek == G2OC_EDGE_SE2) vk = kSE2;
   else if (g->pose_type == G2OC_POSE_SE3 && ek == G2OC_EDGE_SE3) vk = kSE3;
-  else if (g->pose_type == G2OC_POSE_SE3EXPMAP && ek == G2OC_EDGE_PROJECT_XYZ2UV) vk = kExpmap;
+  else if (g->pose_type == G2OC_POSE_SE3EXPMAP && (ek == G2OC_EDGE_PROJECT_XYZ2UV || ek == G2OC_EDGE_SE3_EXPMAP))
+    vk = kExpmap;
   else {
     set_error("g2oc_file_from_graph: pose type %d does not go with edge type %d", g->pose_type, ek);
     return G2OC_ERR_INVALID_ARGUMENT;

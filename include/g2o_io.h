@@ -14,6 +14,8 @@
  *   VERTEX_SE3:EXPMAP              VertexSE3Expmap     id  (inverse of the estimate) tx ty tz qx qy qz qw
  *   VERTEX_TRACKXYZ                VertexPointXYZ      id x y z
  *   EDGE_PROJECT_XYZ2UV:EXPMAP     EdgeProjectXYZ2UV   id_point id_camera param_id u v  I (3, upper)
+ *   EDGE_SE3:EXPMAP                EdgeSE3Expmap       id0 id1 (inverse of the measurement) tx ty tz qx qy qz qw
+ *                                                      I (21, upper)
  *   PARAMS_CAMERAPARAMETERS        CameraParameters    id f cx cy baseline
  *   FIX                                                id id ...
  *
@@ -26,6 +28,7 @@
  *                                      edge_se2.cpp:38-45, slam3d/vertex_se3.cpp:46-51,
  *                                      edge_se3.cpp:43-53, slam3d/vertex_pointxyz.cpp:40-42,
  *                                      sba/vertex_se3_expmap.cpp:35-40, sba/edge_project_xyz2uv.cpp:38-42,
+ *                                      sba/edge_se3_expmap.cpp:33-43,
  *                                      sba/parameter_cameraparameters.cpp:43-49) and the
  *                                      "-renameTypes" lookup (optimizable_graph.cpp:619-644)
  *   g2oc_file_from_graph               a graph built in code (OptimizableGraph::addVertex /

@@ -15,6 +15,7 @@ Follows (paths relative to the g2o source tree):
   VertexSE3Expmap read, write           g2o/types/sba/vertex_se3_expmap.cpp:35-44
   SE3Quat(Vector7), inverse, normalizeRotation   g2o/types/slam3d/se3quat.h:64-86, 114-119, 251-256
   EdgeProjectXYZ2UV read, write         g2o/types/sba/edge_project_xyz2uv.cpp:38-48
+  EdgeSE3Expmap read, write             g2o/types/sba/edge_se3_expmap.cpp:33-43
   CameraParameters read, write          g2o/types/sba/parameter_cameraparameters.cpp:33-57
   gaugeFreedom / findGauge              g2o/core/sparse_optimizer.cpp:132-173
 
@@ -28,10 +29,12 @@ import re
 
 import numpy as np
 
-from g2o_b200.abi import EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3, POSE_SE2, POSE_SE3, POSE_SE3EXPMAP, Graph
+from g2o_b200.abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3, EDGE_SE3_EXPMAP, POSE_SE2, POSE_SE3,
+                          POSE_SE3EXPMAP, Graph)
 
 VERTEX_TAGS = {"VERTEX_SE2": "se2", "VERTEX_SE3:QUAT": "se3", "VERTEX_SE3:EXPMAP": "expmap", "VERTEX_TRACKXYZ": "xyz"}
-EDGE_TAGS = {"EDGE_SE2": "se2", "EDGE_SE3:QUAT": "se3", "EDGE_PROJECT_XYZ2UV:EXPMAP": "proj"}
+EDGE_TAGS = {"EDGE_SE2": "se2", "EDGE_SE3:QUAT": "se3", "EDGE_PROJECT_XYZ2UV:EXPMAP": "proj",
+             "EDGE_SE3:EXPMAP": "se3exp"}
 CAMERA_TAG = "PARAMS_CAMERAPARAMETERS"
 TAG_OF_VERTEX = {v: k for k, v in VERTEX_TAGS.items()}
 TAG_OF_EDGE = {v: k for k, v in EDGE_TAGS.items()}
@@ -219,7 +222,7 @@ def parse(text: str, renamed_types: str = None) -> TextGraph:
                 continue
             k0, k1 = g.vertices[i0][0], g.vertices[i1][0]
             ok = (kind == "se2" and k0 == k1 == "se2") or (kind == "se3" and k0 == k1 == "se3") or \
-                 (kind == "proj" and k0 == "xyz" and k1 == "expmap")
+                 (kind == "proj" and k0 == "xyz" and k1 == "expmap") or (kind == "se3exp" and k0 == k1 == "expmap")
             if not ok:
                 g._problem(lineno, "lines_rejected")
                 continue
@@ -229,7 +232,7 @@ def parse(text: str, renamed_types: str = None) -> TextGraph:
                 if pid is None:
                     g._problem(lineno, "lines_rejected")
                     continue
-            nm, D = {"se2": (3, 3), "se3": (7, 6), "proj": (2, 2)}[kind]
+            nm, D = {"se2": (3, 3), "se3": (7, 6), "proj": (2, 2), "se3exp": (7, 6)}[kind]
             m = [_num(nxt()) for _ in range(nm)]
             up = [_num(nxt()) for _ in range(D * (D + 1) // 2)]
             if None in m or None in up or (kind == "proj" and pid not in g.params):
@@ -244,6 +247,11 @@ def parse(text: str, renamed_types: str = None) -> TextGraph:
             if kind == "se3":
                 q = quat_normalize(m[3:7])
                 m = quat_to_rot(*q) + m[:3]
+            elif kind == "se3exp":
+                q = m[3:7]
+                if q[3] < 0:
+                    q = [c * -1 for c in q]
+                m = se3quat_inverse(m[:3] + quat_normalize(q))
             g.edges.append([kind, i0, i1, pid, m, info, 0.0])
             continue
         if tag.startswith("VERTEX_") or tag.startswith("EDGE_"):
@@ -261,7 +269,7 @@ def to_graph(g: TextGraph):
     if len(kinds) != 1:
         return None
     ek = kinds.pop()
-    pk = {"se2": "se2", "se3": "se3", "proj": "expmap"}[ek]
+    pk = {"se2": "se2", "se3": "se3", "proj": "expmap", "se3exp": "expmap"}[ek]
     pose_ids = sorted(v for v, r in g.vertices.items() if r[0] == pk)
     point_ids = sorted(v for v, r in g.vertices.items() if r[0] == "xyz") if ek == "proj" else []
     pidx = {v: i for i, v in enumerate(pose_ids)}
@@ -277,7 +285,7 @@ def to_graph(g: TextGraph):
                   point_fixed=np.array([g.vertices[v][2] for v in point_ids], dtype=np.uint8),
                   focal_length=cam[0], principal_point=(cam[1], cam[2]))
     gr = Graph({"se2": POSE_SE2, "se3": POSE_SE3, "expmap": POSE_SE3EXPMAP}[pk],
-               {"se2": EDGE_SE2, "se3": EDGE_SE3, "proj": EDGE_PROJECT_XYZ2UV}[ek],
+               {"se2": EDGE_SE2, "se3": EDGE_SE3, "proj": EDGE_PROJECT_XYZ2UV, "se3exp": EDGE_SE3_EXPMAP}[ek],
                np.array([g.vertices[v][1] for v in pose_ids], dtype=np.float64),
                np.array(ev, dtype=np.int32).reshape(-1, 2),
                np.array([e[4] for e in g.edges], dtype=np.float64),
@@ -321,8 +329,8 @@ def _edge_line(e):
     s = TAG_OF_EDGE[kind] + " " + "%d %d " % (i0, i1)
     if kind == "proj":
         s += "%d " % pid
-    s += "".join(_f(x) for x in (iso_to_qt(m) if kind == "se3" else m))
-    D = {"se2": 3, "se3": 6, "proj": 2}[kind]
+    s += "".join(_f(x) for x in (iso_to_qt(m) if kind == "se3" else se3quat_inverse(m) if kind == "se3exp" else m))
+    D = {"se2": 3, "se3": 6, "proj": 2, "se3exp": 6}[kind]
     s += "".join(_f(info[i * D + j]) for i in range(D) for j in range(i, D))
     return s + "\n"
 
@@ -352,7 +360,7 @@ def from_graph(gr: Graph, pose_ids=None, point_ids=None, param_id: int = 0) -> T
     """A TextGraph holding a graph built in code (g2oc_file_from_graph)."""
     g = TextGraph()
     pk = {POSE_SE2: "se2", POSE_SE3: "se3", POSE_SE3EXPMAP: "expmap"}[gr.pose_type]
-    ek = {EDGE_SE2: "se2", EDGE_SE3: "se3", EDGE_PROJECT_XYZ2UV: "proj"}[gr.edge_type]
+    ek = {EDGE_SE2: "se2", EDGE_SE3: "se3", EDGE_PROJECT_XYZ2UV: "proj", EDGE_SE3_EXPMAP: "se3exp"}[gr.edge_type]
     P, N = gr.num_poses, gr.num_points
     pid = list(range(P)) if pose_ids is None else [int(v) for v in pose_ids]
     qid = list(range(P, P + N)) if point_ids is None else [int(v) for v in point_ids]

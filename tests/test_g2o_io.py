@@ -98,7 +98,8 @@ def test_save_subset_edges(three_pose_loop, tmp_path):
 def graphs():
     return [("pg2d", synth.pose_graph_2d(num_poses=80, num_closures=30, seed=11)),
             ("pg3d", synth.pose_graph_3d(num_rings=3, per_ring=25, radius=8.0, seed=12)),
-            ("ba", synth.bundle_adjustment(num_cameras=10, num_points=250, seed=13))]
+            ("ba", synth.bundle_adjustment(num_cameras=10, num_points=250, seed=13)),
+            ("pg3d_expmap", synth.pose_graph_3d_expmap(num_rings=3, per_ring=25, radius=8.0, seed=14))]
 
 
 @pytest.mark.parametrize("name,g", graphs(), ids=[n for n, _ in graphs()])
