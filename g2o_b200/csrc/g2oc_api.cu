@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstdio>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -35,6 +36,24 @@ void set_error(const char* fmt, ...) {
   va_start(ap, fmt);
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
+}
+
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`, never
+// lower it. The limit belongs to the function (per device, process-wide):
+// contexts on several host threads sizing it for their own launches must not
+// lower it between another thread's setting and that thread's launch, which
+// then fails with "invalid argument".
+static int raise_dyn_smem(const void* fn, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<int, const void*>, size_t> applied;
+  int dev = 0;
+  G2OC_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(m);
+  size_t& cur = applied[std::make_pair(dev, fn)];
+  if (bytes <= cur) return G2OC_OK;
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+  return G2OC_OK;
 }
 
 #define G2OC_LAUNCH_CHECK()                                                             \
@@ -842,7 +861,7 @@ struct Engine final : EngineBase {
     DenseOut dn{c->win_of_cam.p, c->win_cam.p, c->win_mat.p, to_windows ? c->win_scratch.p : nullptr};
     if (stage_in_smem) {
       auto kern = schur_rows<Real, T, true, G>;
-      G2OC_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+      G2OC_TRY(raise_dyn_smem((const void*)kern, schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp, bl, bs);
@@ -1090,9 +1109,7 @@ struct Engine final : EngineBase {
   int launch_win_chol(const int* list, int nlist, int nmax) {
     if (nlist == 0) return G2OC_OK;
     const size_t smem = win_chol_smem(nmax);
-    if (smem > 48 * 1024)
-      G2OC_CUDA_TRY(
-          cudaFuncSetAttribute(win_chol_solve<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem > 48 * 1024) G2OC_TRY(raise_dyn_smem((const void*)win_chol_solve<T>, smem));
     G2OC_K(K_CHOLESKY) win_chol_solve<T><<<nlist, T, smem, c->stream>>>(list, nlist, c->windev(), c->rhs.p, c->xs.p,
                                                                           c->win_scratch.p, c->win_state.p);
     G2OC_LAUNCH_CHECK();

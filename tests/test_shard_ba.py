@@ -79,9 +79,11 @@ def run_sharded(backend, g, make_params, iters, world=2):
         t.start()
     for t in th:
         t.join(timeout=600)
-    for r in range(world):
-        if isinstance(out[r], Exception):
-            raise out[r]
+    errs = [out[r] for r in range(world) if isinstance(out[r], Exception)]
+    if errs:
+        # the rank that failed first, not the ones whose all-reduce it broke
+        first = [e for e in errs if "all-reduce returned" not in str(e)]
+        raise (first or errs)[0]
     return out, shards, bus.calls
 
 
