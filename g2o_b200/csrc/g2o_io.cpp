@@ -614,13 +614,31 @@ std::string g2oc_file::write(int mode, const int32_t* ids, int32_t n, int& statu
     status = G2OC_ERR_INVALID_ARGUMENT;
     return s;
   }
-  std::vector<int32_t> order;
+  std::vector<int32_t> order, eorder;
   for (int32_t i = 0; i < (int32_t)vtx.size(); ++i)
     if (vsel[i]) order.push_back(i);
   std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return vtx[a].id < vtx[b].id; });
-  for (int32_t i : order) write_vertex(s, vtx[i]);
-  for (size_t k = 0; k < edg.size(); ++k)
-    if (esel[k]) write_edge(s, edg[k]);
+  for (int32_t k = 0; k < (int32_t)edg.size(); ++k)
+    if (esel[k]) eorder.push_back(k);
+  // the lines are formatted in parallel chunks and joined in order: the text
+  // is the sequential text
+  auto emit = [&](const std::vector<int32_t>& items, bool vertices) {
+    const int64_t n = (int64_t)items.size();
+    const int64_t per = 8192;
+    const int64_t nchunks = (n + per - 1) / per;
+    std::vector<std::string> parts(nchunks);
+#pragma omp parallel for schedule(dynamic)
+    for (int64_t ch = 0; ch < nchunks; ++ch) {
+      std::string& out = parts[ch];
+      for (int64_t i = ch * per; i < std::min(n, (ch + 1) * per); ++i) {
+        if (vertices) write_vertex(out, vtx[items[i]]);
+        else write_edge(out, edg[items[i]]);
+      }
+    }
+    for (const std::string& part : parts) s += part;
+  };
+  emit(order, true);
+  emit(eorder, false);
   return s;
 }
 
