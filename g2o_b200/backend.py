@@ -559,6 +559,11 @@ class SparseOptimizer:
             self.graph.point_estimate[...] = point
         return done
 
+    def compute_marginals(self, block_indices):
+        """SparseOptimizer::computeMarginals (sparse_optimizer.cpp:585-610):
+        blocks of Hpp^-1 for (row, col) pairs of Hessian block indices."""
+        return self._problem.compute_marginals(block_indices)
+
     def active_chi2(self) -> float:
         return self._problem.chi2()[0]
 
