@@ -653,9 +653,11 @@ struct Engine final : EngineBase {
       G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
       G2OC_TRY(Sval.alloc((size_t)S.schur_rc.size() / 2 * 36 + 1));
       {
+        // Schur rows by mean pair count, longest first (no Schur complement
+        // when every landmark is fixed: the lists stay empty)
         std::vector<int> lists[3];
         std::vector<double> work(S.Cf);
-        for (int r = 0; r < S.Cf; ++r) {
+        for (int r = 0; r < (S.schur ? S.Cf : 0); ++r) {
           const int k0 = S.sys_rptr[r], k1 = S.sys_rptr[r + 1];
           const double pairs = (double)(S.s_pair_ptr[k1] - S.s_pair_ptr[k0]);
           const double mean = k1 - k0 > 1 ? pairs / (k1 - k0 - 1) : 0.0;

@@ -510,3 +510,25 @@ def test_se3_expmap_pose_graph_matches_oracle(backend, oracle_lib, linear):
         assert abs(a["chi2"] - b["chi2"]) <= tol * b["chi2"], (a["chi2"], b["chi2"])
     assert sc[-1]["chi2"] < sc[0]["chi2"]
     c.close()
+
+
+def test_pose_only_projection_edges(backend, oracle_lib):
+    """EdgeSE3ProjectXYZOnlyPose (g2o/types/sba/edge_project_xyz_onlypose.cpp)
+    is EdgeSE3ProjectXYZ with the point a constant: with every point fixed the
+    BA path solves the cameras alone (no Schur complement), as ORB-SLAM's
+    pose-only optimization does; LM trajectory against the oracle."""
+    g = small_ba(seed=25, cams=12, points=1500, focal_y=455.0)
+    g.point_fixed[:] = 1
+    g.pose_fixed[:] = 0
+    o, c = both(backend, oracle_lib, g, algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_CHOLESKY)
+    assert c.info.num_free_points == 0 and c.info.schur_nnzb == 0
+    do, so = o.optimize(10)
+    dc, sc = c.optimize(10)
+    assert do == dc
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"]
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-8 * b["chi2"], (a["chi2"], b["chi2"])
+    (pc, qc), (po, qo) = c.estimates(), o.estimates()
+    assert np.abs(pc - po).max() < 1e-8
+    assert np.array_equal(qc, g.point_estimate)
+    c.close()
