@@ -406,3 +406,30 @@ def test_cli_lists_the_new_algorithms_and_round_trips_se3_expmap(tmp_path):
     # what g2o writes after reading it back (pose 0 was fixed already); not
     # the input bytes: the six-digit quaternions are not unit length
     assert out.read_text() == gt.write(gt.parse(src.read_text()))
+
+
+def test_file_entry_points_refuse_bad_arguments(tmp_path, three_pose_loop):
+    from g2o_b200.backend import library
+    L = library()
+    with pytest.raises(G2ocError) as e:
+        three_pose_loop.save(str(tmp_path / "x.g2o"), mode=7)
+    assert e.value.status == abi.G2OC_ERR_INVALID_ARGUMENT
+    with pytest.raises(G2ocError):
+        three_pose_loop.save(str(tmp_path / "x.g2o"), mode=SAVE_VERTEX_SUBSET, ids=[0, 99])
+    with pytest.raises(G2ocError):
+        three_pose_loop.save(str(tmp_path / "x.g2o"), mode=SAVE_EDGE_SUBSET, ids=[3])
+    with pytest.raises(G2ocError):
+        three_pose_loop.save("/nonexistent/dir/x.g2o")
+    bad = abi.Graph(abi.POSE_SE2, abi.EDGE_SE2, np.zeros((2, 3)), [[0, 5]], np.zeros((1, 3)),
+                    np.eye(3).reshape(1, 9))
+    with pytest.raises(G2ocError):
+        G2oFile.from_graph(bad)
+    mismatched = abi.Graph(abi.POSE_SE2, abi.EDGE_SE3, np.zeros((2, 3)), [[0, 1]], np.zeros((1, 12)),
+                           np.eye(6).reshape(1, 36))
+    with pytest.raises(G2ocError):
+        G2oFile.from_graph(mismatched)
+    with pytest.raises(G2ocError):
+        G2oFile.from_graph(abi.Graph(abi.POSE_SE2, abi.EDGE_SE2, np.zeros((2, 3)), [[0, 1]], np.zeros((1, 3)),
+                                     np.eye(3).reshape(1, 9)), pose_ids=[4, 4])
+    assert L.g2oc_file_get_info(None, None) == abi.G2OC_ERR_INVALID_ARGUMENT
+    assert L.g2oc_file_graph(None, None) == abi.G2OC_ERR_INVALID_ARGUMENT
