@@ -230,6 +230,19 @@ class Graph:
                      self.focal_length, tuple(self.principal_point), self.name, dict(self.extra),
                      self.focal_length_y)
 
+    def digest(self) -> str:
+        """SHA-256 of the graph's types, arrays and intrinsics: equal digests
+        mean the same optimization problem, bit for bit."""
+        import hashlib
+        h = hashlib.sha256()
+        h.update(np.array([self.pose_type, self.edge_type], np.int64).tobytes())
+        for a in (self.pose_estimate, self.edge_vertex, self.measurement, self.information, self.pose_fixed,
+                  self.point_estimate, self.point_fixed, self.robust_delta):
+            h.update(b"-" if a is None else np.ascontiguousarray(a).tobytes())
+        fy = self.focal_length if self.focal_length_y is None else self.focal_length_y
+        h.update(np.array([self.focal_length, fy, *self.principal_point], np.float64).tobytes())
+        return h.hexdigest()
+
     def to_c(self) -> G2ocGraph:
         g = G2ocGraph()
         g.pose_type = self.pose_type

@@ -25,7 +25,8 @@ from typing import List, Optional
 import numpy as np
 
 from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
-                  G2ocIterationStats, G2ocKernelStat, G2ocParams, G2ocWindowStats, Graph, POSE_DIM, POSE_EST_DIM)
+                  G2ocIterationStats, G2ocKernelStat, G2ocParams, G2ocWindowStats, Graph, LINEAR_CHOLESKY, LINEAR_PCG,
+                  POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libg2o_b200.so")
@@ -77,6 +78,8 @@ def library() -> C.CDLL:
         "g2oc_get_hessian": ([vp, dp, dp, dp, dp], C.c_int),
         "g2oc_schur": ([vp, C.c_double, dp, dp], C.c_int),
         "g2oc_solve": ([vp, C.c_double, dp, ip], C.c_int),
+        "g2oc_solver_init": ([vp], C.c_int),
+        "g2oc_multiply_hessian": ([vp, dp, dp], C.c_int),
         "g2oc_backward": ([vp, dp, dp, dp, vp], C.c_int),
         "g2oc_upload_windows": ([vp, C.c_int32, vp], C.c_int),
         "g2oc_optimize_windows": ([vp, C.c_int32, vp], C.c_int),
@@ -358,6 +361,144 @@ class CudaProblem:
         it = C.c_int32()
         st = library().g2oc_solve(self._h, lam, _p(x), C.byref(it))
         return st, x, it.value
+
+    def solver_init(self):
+        """BlockSolver::init -> LinearSolver::init: the next PCG solve carries
+        no residual from the previous one."""
+        _check(library().g2oc_solver_init(self._h))
+
+    def multiply_hessian(self, src):
+        """BlockSolverBase::multiplyHessian: Hpp src (pose part, Hessian order)."""
+        src = np.ascontiguousarray(src, np.float64)
+        dest = np.empty_like(src)
+        _check(library().g2oc_multiply_hessian(self._h, _p(src), _p(dest)))
+        return dest
+
+
+class LinearSolverCudaPCG:
+    """LinearSolverPCG's role (g2o/solvers/pcg/linear_solver_pcg.h:44-110):
+    block-Jacobi PCG. Inside a BlockSolverCuda it solves the reduced system on
+    the device; solve() is LinearSolver<MatrixType>::solve(A, x, b)
+    (g2o/core/linear_solver.h:64-65) on a caller block matrix."""
+
+    kind = LINEAR_PCG
+
+    def __init__(self, tolerance=1e-6, max_iterations=-1, absolute_tolerance=True):
+        self.tolerance = tolerance
+        self.max_iterations = max_iterations
+        self.absolute_tolerance = absolute_tolerance
+
+    def params(self, **kw):
+        return default_params(linear_solver=self.kind, pcg_tolerance=self.tolerance,
+                              pcg_max_iterations=self.max_iterations,
+                              pcg_absolute_tolerance=1 if self.absolute_tolerance else 0, **kw)
+
+    def solve(self, block_offsets, block_rc, values, b, device=0):
+        st, x, it = solve_block_system(self.kind, block_offsets, block_rc, values, b, self.params(), device)
+        return st == 0, x
+
+
+class LinearSolverCudaCholesky(LinearSolverCudaPCG):
+    """LinearSolverEigen / LinearSolverDense's role
+    (g2o/solvers/eigen/linear_solver_eigen.h:94-191,
+    g2o/solvers/dense/linear_solver_dense.h:57-105): FP64 tiled Cholesky."""
+
+    kind = LINEAR_CHOLESKY
+
+    def __init__(self):
+        super().__init__()
+
+
+class BlockSolverCuda:
+    """The Solver interface of g2o's BlockSolver (g2o/core/solver.h:44-153,
+    g2o/core/block_solver.h:96-149) over one device context, for an
+    OptimizationAlgorithm that drives the solve itself (the algorithm updates
+    the host vertices and computes the errors between solves). The graph is
+    uploaded by build_structure and the estimates pushed before each
+    build_system; the Hessian stays on the device and only b and x cross."""
+
+    def __init__(self, linear_solver: LinearSolverCudaPCG, device: int = 0, **params):
+        self.linear_solver = linear_solver
+        self.device = device
+        self._params = linear_solver.params(**params)
+        self._prob: Optional[CudaProblem] = None
+        self._lambda = 0.0
+        self._schur = True
+        self._b = None
+        self._x = None
+
+    # Solver::init / buildStructure / updateStructure
+    def init(self, graph: Graph, online: bool = False) -> bool:
+        self.graph = graph
+        if self._prob is not None:
+            self._prob.solver_init()
+        return True
+
+    def build_structure(self, zero_blocks: bool = False) -> bool:
+        if self._prob is None:
+            self._prob = CudaProblem(self.graph, self._params, device=self.device)
+        else:
+            self._prob.upload(self.graph)
+        self._prob.solver_init()
+        n = self._prob.info.vector_size
+        self._x = np.zeros(n)
+        self._b = np.zeros(n)
+        return True
+
+    def update_structure(self, vset, edges) -> bool:
+        return False  # incremental structure updates are not supported (as in LinearSolverPCG-based solvers)
+
+    # Solver::buildSystem at the host estimates
+    def build_system(self, pose_estimate, point_estimate=None) -> bool:
+        self._prob.set_estimates(pose_estimate, point_estimate)
+        self._prob.build_system()
+        self._b = self._prob.hessian()[3]
+        return True
+
+    # Solver::setLambda / solve / restoreDiagonal
+    def set_lambda(self, lam: float, backup: bool = False) -> bool:
+        self._lambda = float(lam)
+        return True
+
+    def solve(self) -> bool:
+        st, x, self.pcg_iterations = self._prob.solve(self._lambda)
+        self._x = x
+        return st == 0
+
+    def restore_diagonal(self):
+        self._lambda = 0.0
+
+    def x(self):
+        return self._x
+
+    def b(self):
+        return self._b
+
+    def hessian(self):
+        return self._prob.hessian()
+
+    def pattern(self):
+        return self._prob.pattern()
+
+    def multiply_hessian(self, src):
+        return self._prob.multiply_hessian(src)
+
+    def compute_marginals(self, block_indices):
+        return self._prob.compute_marginals(block_indices)
+
+    def supports_schur(self) -> bool:
+        return True
+
+    def schur(self) -> bool:
+        return self._schur
+
+    def set_schur(self, s: bool):
+        self._schur = bool(s)
+
+    def close(self):
+        if self._prob is not None:
+            self._prob.close()
+            self._prob = None
 
 
 def device_tensor(ptr: int, count: int, dtype: int, device: int = 0):

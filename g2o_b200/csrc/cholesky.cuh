@@ -382,12 +382,11 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
   return G2OC_OK;
 }
 
-template <typename Real>
-static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const double* rhs, double* xout, int* ok,
-                      long long* nlaunch) {
-  long long nl = 4;  // densify, load_rhs, store_x, + memsets
+// forward and backward substitution with the factor chol_factor left in P.A
+// (a refinement's correction solve reuses it)
+static int chol_resolve(CholPlan& P, cudaStream_t st, const double* rhs, double* xout, long long* nlaunch) {
+  long long nl = 2;  // load_rhs, store_x
   const int np = P.np, nt = P.nt;
-  G2OC_TRY(chol_factor<Real>(P, st, S, &nl));
   chol_load_rhs<<<(np + 255) / 256, 256, 0, st>>>(rhs, P.d_perm.p, P.nb, P.bs, P.n, np, P.y.p);
   for (int k = 0; k < nt; ++k) {
     chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
@@ -407,6 +406,16 @@ static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const
     set_error("cholesky solve launch: %s", cudaGetErrorString(e2));
     return G2OC_ERR_CUDA;
   }
+  if (nlaunch) *nlaunch += nl;
+  return G2OC_OK;
+}
+
+template <typename Real>
+static int chol_solve(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, const double* rhs, double* xout, int* ok,
+                      long long* nlaunch) {
+  long long nl = 2;  // densify + memsets
+  G2OC_TRY(chol_factor<Real>(P, st, S, &nl));
+  G2OC_TRY(chol_resolve(P, st, rhs, xout, &nl));
   if (nlaunch) *nlaunch += nl - 1;
   int info = 0;
   G2OC_CUDA_TRY(cudaMemcpyAsync(&info, P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));

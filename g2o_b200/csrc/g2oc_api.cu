@@ -106,14 +106,15 @@ enum KernelId {
   K_CHI2, K_ERRORS, K_JACOBIANS, K_LANDMARK_PASS, K_CAMERA_PASS, K_SCHUR_LANDMARK, K_SCHUR_BLOCKS, K_SCHUR_RHS,
   K_BACKSUB, K_RESID_CAM, K_RESID_LM, K_OPLUS, K_MAX_DIAG, K_PCG_DIAG_INV, K_PCG_INIT, K_PCG_SPMV, K_PCG_UPDATE,
   K_PCG_CHECK, K_PG_LINEARIZE, K_PG_ASSEMBLE_H, K_PG_ASSEMBLE_B, K_DAMP, K_LM_CONTROL, K_REDUCE, K_AXPY,
-  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_BACKWARD, K_COUNT
+  K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_BACKWARD, K_PG_RESID,
+  K_COUNT
 };
 static const char* kKernelNames[K_COUNT] = {
   "chi2", "errors", "jacobians", "ba_landmark_pass", "ba_camera_pass", "schur_landmark", "schur_blocks",
   "schur_rhs", "ba_backsub", "ba_resid_cam", "ba_resid_lm", "oplus", "max_diag", "pcg_diag_inv", "pcg_init",
   "pcg_spmv", "pcg_update", "pcg_check_dn", "pg_linearize", "pg_assemble_h", "pg_assemble_b", "damp_diag",
   "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db", "io_reorder", "pcg_solve", "pcg_solve_tiles",
-  "sys_to_tiles", "ba_backward"};
+  "sys_to_tiles", "ba_backward", "pg_resid64"};
 
 struct PendingTiming {
   int kid;
@@ -473,11 +474,22 @@ static int pcg_max_iter(const g2oc_ctx* c, int n) {
   return m;
 }
 
+// The per-CTA partial sums: the multi-kernel PCG's column pass runs one CTA per
+// block row and writes one slot each, so the buffer grows with the system (it
+// never shrinks; the stream is drained first because queued kernels may still
+// read the old buffer).
+static int ensure_partials(g2oc_ctx* c, size_t slots) {
+  if (c->partials.n >= slots) return G2OC_OK;
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return c->partials.alloc(slots);
+}
+
 template <typename Real, int BS>
 static int run_pcg(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs, double* xout,
                    double* r, double* s, double* d0, double* d1, double* q, double* qrow, double* tbuf,
                    bool fixed_d0, int* iters) {
   cudaStream_t st = c->stream;
+  G2OC_TRY(ensure_partials(c, (size_t)A.nb));
   PcgState host;
   G2OC_CUDA_TRY(cudaMemcpyAsync(&host, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
   G2OC_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1042,9 +1054,63 @@ struct Engine final : EngineBase {
       G2OC_LAUNCH_CHECK();
       if (use_chol) G2OC_TRY(chol_solve(sysval.p, c->b.p, c->x.p, &ok));
       else G2OC_TRY(pcg_solve(sysval.p, c->b.p, c->x.p, false));
+      if (sizeof(Real) == 4 && ok && use_chol && !S.ba && c->prm.refine_max_iterations >= 0)
+        G2OC_TRY(refine_pose_graph(lambda));
     }
     G2OC_K(K_LM_CONTROL) set_solve_ok<<<1, 32, 0, st>>>(c->sc.p, ok);
     G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  // Mixed precision on the pose graphs (FP32 Hessian, FP64 Cholesky of it):
+  // FP64 iterative refinement on the true residual of the damped system,
+  // r = b - (J^T Om' J + lambda I) x, formed matrix-free from the edges in
+  // FP64 (pg_hx_contrib). While |r| / |b| is above refine_tolerance a
+  // correction is solved with the same factor, up to refine_max_iterations;
+  // a correction that does not reduce the residual is undone and ends the loop.
+  int refine_pose_graph(double lambda) {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    const int n = c->vec_size();
+    const int ne = (int)S.act.size();
+    double prev = -1.0;
+    for (int k = 0;; ++k) {
+      if (S.pose_type == G2OC_POSE_SE2) {
+        G2OC_K(K_PG_RESID) pg_hx_contrib<G2OC_POSE_SE2><<<cdiv(ne, 128), 128, 0, st>>>(
+            c->pose.p, c->pg_edges(), c->pose_h.p, c->x.p, bcontrib.p);
+        G2OC_K(K_PG_RESID) pg_assemble_b<3><<<cdiv((long long)S.Cf * 3, 128), 128, 0, st>>>(
+            S.Cf, c->bv_src_ptr.p, c->bv_src.p, bcontrib.p, c->xs.p);
+      } else {
+        if (S.pose_type == G2OC_POSE_SE3EXPMAP)
+          G2OC_K(K_PG_RESID) pg_hx_contrib<G2OC_POSE_SE3EXPMAP><<<cdiv(ne, 64), 64, 0, st>>>(
+              c->pose.p, c->pg_edges(), c->pose_h.p, c->x.p, bcontrib.p);
+        else
+          G2OC_K(K_PG_RESID) pg_hx_contrib<G2OC_POSE_SE3><<<cdiv(ne, 64), 64, 0, st>>>(
+              c->pose.p, c->pg_edges(), c->pose_h.p, c->x.p, bcontrib.p);
+        G2OC_K(K_PG_RESID) pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(
+            S.Cf, c->bv_src_ptr.p, c->bv_src.p, bcontrib.p, c->xs.p);
+      }
+      G2OC_K(K_PG_RESID) pg_resid_finish<<<kRedBlocks, 256, 0, st>>>(n, c->b.p, c->xs.p, c->x.p, lambda,
+                                                                     c->resid.p, c->partials.p);
+      G2OC_LAUNCH_CHECK();
+      G2OC_TRY(finalize_sum(c, kRedBlocks, 2, &c->sc.p->refine_rnorm, &c->sc.p->refine_bnorm));
+      double rb[2];
+      G2OC_CUDA_TRY(cudaMemcpyAsync(rb, &c->sc.p->refine_rnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+      const double rel = rb[1] > 0.0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+      c->last_refine_dn = rel;
+      if (prev >= 0.0 && !(rel < prev)) {
+        G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, -1.0, n);
+        G2OC_LAUNCH_CHECK();
+        break;
+      }
+      if (!(rel > c->prm.refine_tolerance) || k == c->prm.refine_max_iterations) break;
+      prev = rel;
+      G2OC_TRY(chol_resolve(*c->chol, st, c->resid.p, c->dx.p, &c->kcount[K_CHOLESKY]));
+      c->refine_steps++;
+      G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, 1.0, n);
+      G2OC_LAUNCH_CHECK();
+    }
     return G2OC_OK;
   }
 
@@ -1707,6 +1773,10 @@ static const char* kSolvers[][2] = {
     {"lm_cuda_mixed", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
     {"gn_cuda_mixed_fast", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
     {"lm_cuda_mixed_fast", "Levenberg: B200 block solver, FP32 Hessian/Schur/PCG steps, FP64 errors and control"},
+    {"gn_cuda_chol_mixed", "Gauss-Newton: B200 block solver, FP32 Hessian, FP64 Cholesky, FP64 refinement"},
+    {"lm_cuda_chol_mixed", "Levenberg: B200 block solver, FP32 Hessian, FP64 Cholesky, FP64 refinement"},
+    {"gn_cuda_chol_mixed_fast", "Gauss-Newton: B200 block solver, FP32 Hessian, FP64 Cholesky of it"},
+    {"lm_cuda_chol_mixed_fast", "Levenberg: B200 block solver, FP32 Hessian, FP64 Cholesky of it"},
     {"dl_cuda", "Dogleg: B200 block solver, FP64, PCG with Schur / Cholesky without"},
     {"dl_cuda_pcg", "Dogleg: B200 block solver, FP64, block-Jacobi PCG"},
     {"dl_cuda_chol", "Dogleg: B200 block solver, FP64, dense Cholesky"},
@@ -1755,7 +1825,13 @@ int g2oc_construct(const char* name, g2oc_params* p) {
   }
   const std::string v = n.size() > 7 ? n.substr(8) : "";
   if (v.empty()) p->linear_solver = 2;  // PCG with Schur, Cholesky without
-  else if (v.rfind("chol", 0) == 0) p->linear_solver = G2OC_LINEAR_CHOLESKY;
+  else if (v.rfind("chol", 0) == 0) {
+    p->linear_solver = G2OC_LINEAR_CHOLESKY;
+    // FP32 Hessian, FP64 factorization of it; FP64 refinement of every step
+    // on pose graphs unless _fast
+    if (v == "chol_mixed" || v == "chol_mixed_fast") p->precision = G2OC_PREC_MIXED;
+    if (v == "chol_mixed_fast") p->refine_max_iterations = -1;
+  }
   else if (v == "mixed" || v == "mixed_fast") {
     p->linear_solver = G2OC_LINEAR_PCG;
     p->precision = G2OC_PREC_MIXED;
@@ -2399,6 +2475,37 @@ int g2oc_solve(g2oc_ctx* c, double lambda, double* x, int32_t* iters) {
   if (iters) *iters = stv.iterations_linear_solver;
   if (x) G2OC_CUDA_TRY(cudaMemcpy(x, c->x.p, c->x.bytes(), cudaMemcpyDeviceToHost));
   return h.solve_ok ? G2OC_OK : G2OC_ERR_NOT_PD;
+}
+
+int g2oc_solver_init(g2oc_ctx* c) {
+  G2OC_TRY(check_ctx(c, true));
+  G2OC_TRY(reset_pcg(c));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G2OC_OK;
+}
+
+int g2oc_multiply_hessian(g2oc_ctx* c, const double* src, double* dest) {
+  G2OC_TRY(check_ctx(c, true));
+  if (!c->system_built) {
+    set_error("call g2oc_build_system first");
+    return G2OC_ERR_STATE;
+  }
+  if (!src || !dest) {
+    set_error("src or dest is NULL");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  const Structure& S = c->S;
+  const size_t np = (size_t)S.Cf * S.pd;
+  if (np == 0) return G2OC_OK;
+  cudaStream_t st = c->stream;
+  // src in the first np entries of the residual scratch, the product in dx
+  // (both hold the whole Hessian-order vector; the product's landmark part
+  // is zero and not returned)
+  G2OC_CUDA_TRY(cudaMemcpyAsync(c->resid.p, src, np * sizeof(double), cudaMemcpyHostToDevice, st));
+  G2OC_TRY(c->eng->multiply_hessian(c->resid.p, c->dx.p));
+  G2OC_CUDA_TRY(cudaMemcpyAsync(dest, c->dx.p, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+  return G2OC_OK;
 }
 
 // ------------------------------------------------------------ adjoint

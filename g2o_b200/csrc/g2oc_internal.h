@@ -163,6 +163,7 @@ struct DevScalars {
   double pcg_d0;
   double pcg_dn;
   double refine_rnorm;   // mixed precision: |r| / |b| of the last refinement
+  double refine_bnorm;   // pose-graph refinement: |b|^2 beside |r|^2 in refine_rnorm
   double chi2_temp_plain;  // activeChi2 after the trial update
   int pcg_iterations;
   int pcg_done;

@@ -216,6 +216,13 @@ extern "C" int g2oc_solve_block_system_static(int device, int32_t num_block_rows
     return G2OC_ERR_INVALID_ARGUMENT;
   }
   std::lock_guard<std::mutex> lock(g_static_mutex);
+  // the caller's current device is put back on every return
+  int caller_device = -1;
+  G2OC_CUDA_TRY(cudaGetDevice(&caller_device));
+  struct RestoreDevice {
+    int d;
+    ~RestoreDevice() { cudaSetDevice(d); }
+  } restore{caller_device};
   G2OC_CUDA_TRY(cudaSetDevice(device));
   if (!g_scratch_ptr[device]) {
     // once per device, with the device current: the device address of the
@@ -226,7 +233,12 @@ extern "C" int g2oc_solve_block_system_static(int device, int32_t num_block_rows
   }
   unsigned char* arena = (unsigned char*)g_scratch_ptr[device];
   const cudaStream_t st = cudaStreamPerThread;
-  if (block_size == 3)
-    return static_solve<3>(st, arena, nb, nnzb, block_rc, values, b, x, pcg_tolerance, pcg_max_iterations, iterations);
-  return static_solve<6>(st, arena, nb, nnzb, block_rc, values, b, x, pcg_tolerance, pcg_max_iterations, iterations);
+  const int rc =
+      block_size == 3
+          ? static_solve<3>(st, arena, nb, nnzb, block_rc, values, b, x, pcg_tolerance, pcg_max_iterations, iterations)
+          : static_solve<6>(st, arena, nb, nnzb, block_rc, values, b, x, pcg_tolerance, pcg_max_iterations, iterations);
+  // a failed call may have left kernels queued that still use the shared
+  // arena: drain them before the lock lets the next caller in
+  if (rc != G2OC_OK) cudaStreamSynchronize(st);
+  return rc;
 }

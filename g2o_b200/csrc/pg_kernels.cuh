@@ -198,6 +198,79 @@ __global__ void pg_linearize(const double* est, PGEdges E, const uint8_t* trans,
   }
 }
 
+// Mixed-precision refinement of the pose graphs: the Gauss-Newton Hessian
+// times a vector, matrix-free and in FP64 from the edges (FP64 Jacobians at
+// the current estimates, the same robust weight rho' as pg_linearize). Per
+// edge, with u = J0 x_i + J1 x_j (a fixed vertex contributes 0) and
+// g = rho' Om u: slot 0 = J0^T g, slot 1 = J1^T g, summed per pose by
+// pg_assemble_b in the gradient's order.
+template <int PT>
+__global__ void pg_hx_contrib(const double* est, PGEdges E, const int* pose_h, const double* x, double* out) {
+  constexpr int D = PGTraits<PT>::PD;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= E.n) return;
+  double e[6], J0[36], J1[36];
+  pg_error<PT>(est, E, k, e);
+  pg_jac<PT>(est, E, k, J0, J1);
+  const double* I = E.info + (size_t)k * D * D;
+  double w = 1.0;
+  const double dl = E.delta ? E.delta[k] : 0.0;
+  if (dl > 0.0) {
+    double rho[3];
+    huber(pg_chi2_of<PT>(E, k, e), dl, rho);
+    w = rho[1];
+  }
+  const int2 v = E.v[k];
+  const int h0 = pose_h[v.x], h1 = pose_h[v.y];
+  double xi[6], xj[6];
+#pragma unroll
+  for (int q = 0; q < D; ++q) {
+    xi[q] = h0 >= 0 ? x[(size_t)h0 * D + q] : 0.0;
+    xj[q] = h1 >= 0 ? x[(size_t)h1 * D + q] : 0.0;
+  }
+  double u[6], g[6];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) t += J0[i * D + q] * xi[q] + J1[i * D + q] * xj[q];
+    u[i] = t;
+  }
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) t += I[i * D + q] * u[q];
+    g[i] = w * t;
+  }
+  double* o = out + (size_t)k * 2 * D;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      s0 += J0[q * D + i] * g[q];
+      s1 += J1[q * D + i] * g[q];
+    }
+    o[i] = s0;
+    o[D + i] = s1;
+  }
+}
+
+// r = b - (H x + lambda x); per-CTA partial sums of |r|^2 and |b|^2 at
+// partials[2 * block], partials[2 * block + 1]
+__global__ void pg_resid_finish(int n, const double* b, const double* hx, const double* x, double lambda, double* r,
+                                double* partials) {
+  double rr = 0.0, bb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = b[i] - hx[i] - lambda * x[i];
+    r[i] = v;
+    rr += v * v;
+    bb += b[i] * b[i];
+  }
+  block_sum2(rr, bb, partials + 2 * blockIdx.x);
+}
+
 // Hpp block (row r of block blk) = sum of its contributions in edge order
 template <typename Real, int D>
 __global__ void pg_assemble_h(int nnzb, const int* src_ptr, const int* src, const Real* hcontrib, Real* hpp) {

@@ -32,6 +32,9 @@
  *   g2oc_schur                      BlockSolver::setLambda + the Schur part of
  *                                   BlockSolver::solve (g2o/core/block_solver.hpp:331-448, 567-606)
  *   g2oc_solve                      setLambda + BlockSolver::solve + restoreDiagonal
+ *   g2oc_solver_init                BlockSolver::init -> LinearSolver::init
+ *                                   (g2o/core/block_solver.hpp:609-616)
+ *   g2oc_multiply_hessian           BlockSolverBase::multiplyHessian (g2o/core/block_solver.h:96)
  *   g2oc_solve_block_system         LinearSolver<MatrixType>::solve(A, x, b)
  *                                   (g2o/core/linear_solver.h:64-65) on a caller block matrix
  *   g2oc_compute_marginals          SparseOptimizer::computeMarginals -> BlockSolver::computeMarginals
@@ -246,6 +249,21 @@ int g2oc_get_pattern(g2oc_ctx* ctx, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* s
 int g2oc_get_hessian(g2oc_ctx* ctx, double* hpp, double* hll, double* hpl, double* b);
 int g2oc_schur(g2oc_ctx* ctx, double lambda, double* schur_blocks, double* bschur);
 int g2oc_solve(g2oc_ctx* ctx, double lambda, double* x, int32_t* pcg_iterations);
+/* The Solver calls of a BlockSolverCuda adapter (g2o/core/solver.h:44-153,
+   g2o/core/block_solver.h:96-149) map onto this ABI as: buildStructure ->
+   g2oc_upload; buildSystem -> g2oc_set_estimates + g2oc_build_system;
+   setLambda + solve + restoreDiagonal -> g2oc_solve(lambda) (lambda is added
+   to a copy of the diagonal; the stored Hessian never changes, so nothing is
+   left to restore); Solver::b() and saveHessian -> g2oc_get_hessian.
+   BlockSolver::init -> LinearSolver::init (g2o/core/block_solver.hpp:609-616,
+   g2o/solvers/pcg/linear_solver_pcg.h:54-59): forget the PCG residual that
+   the next solve's stopping rule would carry over from the previous one. */
+int g2oc_solver_init(g2oc_ctx* ctx);
+/* BlockSolverBase::multiplyHessian(dest, src) (g2o/core/block_solver.h:96,
+   _Hpp->multiplySymmetricUpperTriangle): dest = Hpp src, Hpp the pose part of
+   the last g2oc_build_system; src and dest hold num_free_poses * pose_dim
+   doubles in Hessian order. */
+int g2oc_multiply_hessian(g2oc_ctx* ctx, const double* src, double* dest);
 /* StructureOnlySolver<3>::calc(points, num_iters, num_max_trials) on every
    free landmark of a bundle adjustment, the cameras held fixed: each landmark
    runs its own Levenberg-Marquardt on its 3x3 system (one thread per
@@ -372,7 +390,12 @@ int g2oc_solve_pattern_block_system(g2oc_ctx* ctx, int32_t nb, const int32_t* bl
    device current); make that first call before any CUDA stream capture.
    Calls share the scratch (later calls overwrite it; host callers are
    serialized by a mutex) and run on cudaStreamPerThread, returning after the
-   result is copied back. */
+   result is copied back, or, on an error, after the work already queued has
+   finished. The stopping rule always uses the absolute tolerance (g2o's
+   default, LinearSolverPCG absoluteTolerance = true): the result equals
+   g2oc_solve_block_system's under a context whose pcg_absolute_tolerance is
+   1. The device is made current for the call and the caller's current
+   device is restored before returning. */
 #define G2OC_STATIC_SCRATCH_BYTES (16u << 20)
 int g2oc_solve_block_system_static(int device, int32_t num_block_rows, int32_t block_size, int32_t nnzb,
                                    const int32_t* block_rc, const double* values, const double* b, double* x,

@@ -1900,6 +1900,14 @@ int orc_schur(orc_problem* p, double lambda, double* S, double* bs) {
   return G2OC_OK;
 }
 
+int orc_update(orc_problem* p, const double* x) {
+  // SparseOptimizer::update (sparse_optimizer.cpp:457-468) with a caller step
+  // in Hessian order: the host side of an algorithm that drives a Solver
+  if (!p || !x) return G2OC_ERR_INVALID_ARGUMENT;
+  update(p, x);
+  return G2OC_OK;
+}
+
 int orc_solve(orc_problem* p, double lambda, double* x, int32_t* iters) {
   if (!p) return G2OC_ERR_INVALID_ARGUMENT;
   if (!p->system_built) return G2OC_ERR_STATE;

@@ -49,6 +49,8 @@ int orc_get_pattern(orc_problem* p, int32_t* hpp_rc, int32_t* hpl_rc, int32_t* s
 int orc_get_hessian(orc_problem* p, double* hpp, double* hll, double* hpl, double* b);
 int orc_schur(orc_problem* p, double lambda, double* schur_blocks, double* bschur);
 int orc_solve(orc_problem* p, double lambda, double* x, int32_t* pcg_iterations);
+/* SparseOptimizer::update(x): oplus of every free vertex by its part of x (Hessian order) */
+int orc_update(orc_problem* p, const double* x);
 int orc_solve_block_system(int32_t linear_solver, const g2oc_params* params, int32_t num_block_rows,
                            const int32_t* block_offsets, int32_t nnzb, const int32_t* block_rc,
                            const double* values, const double* b, double* x, int32_t* iterations);

@@ -53,6 +53,7 @@ def lib():
         L.orc_get_hessian.argtypes = [vp, dp, dp, dp, dp]
         L.orc_schur.argtypes = [vp, C.c_double, dp, dp]
         L.orc_solve.argtypes = [vp, C.c_double, dp, ip]
+        L.orc_update.argtypes = [vp, dp]
         L.orc_solve_block_system.argtypes = [C.c_int32, C.c_void_p, C.c_int32, ip, C.c_int32, ip, dp, dp, dp, ip]
         L.orc_huber.argtypes = [C.c_double, C.c_double, dp]
         L.orc_huber.restype = None
@@ -189,6 +190,11 @@ class OracleProblem:
         it = C.c_int32()
         st = lib().orc_solve(self._h, lam, _p(x), C.byref(it))
         return st, x, it.value
+
+    def update(self, x):
+        """SparseOptimizer::update(x) on the oracle's vertices."""
+        x = np.ascontiguousarray(x, np.float64)
+        _check(lib().orc_update(self._h, _p(x)), "update")
 
 
 def solve_block_system(linear_solver, block_offsets, block_rc, values, b, params=None):

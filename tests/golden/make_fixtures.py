@@ -62,7 +62,9 @@ def parse(src):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <g2o source tree>")
+    root = sys.argv[1]
     data = parse(os.path.join(root, "unit_test/solver/sparse_system_helper.cpp"))
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sparse_system_36.json")
     with open(out, "w") as f:

@@ -110,3 +110,34 @@ def test_create_without_device_reports_no_device(cuda_lib):
     st = cuda_lib.g2oc_create(0, C.byref(h))
     assert st == abi.G2OC_ERR_NO_DEVICE
     assert not h.value
+
+
+def test_static_block_solve_rejects_argument_errors_before_the_device(cuda_lib):
+    # g2oc_solve_block_system_static checks its arguments and the host-scratch
+    # bound before it touches a device, so these run without a GPU
+    import numpy as np
+
+    def call(nb, bs, rc, vals, b, device=0):
+        x = np.zeros_like(b)
+        it = C.c_int32()
+        rc = np.ascontiguousarray(rc, np.int32)
+        return cuda_lib.g2oc_solve_block_system_static(
+            device, nb, bs, len(rc), rc.ctypes.data_as(C.POINTER(C.c_int32)),
+            vals.ctypes.data_as(C.POINTER(C.c_double)), b.ctypes.data_as(C.POINTER(C.c_double)),
+            x.ctypes.data_as(C.POINTER(C.c_double)), 1e-6, -1, C.byref(it))
+
+    # a full upper pattern of 1300 block rows: 845,650 blocks, past the host
+    # list bound (5 * nnzb + 4 * nb + 8 ints of 4 Mi)
+    nb = 1300
+    cols = np.repeat(np.arange(nb), np.arange(1, nb + 1))
+    rows = np.concatenate([np.arange(c + 1) for c in range(nb)])
+    rc = np.stack([rows, cols], axis=1)
+    vals = np.zeros(len(rc) * 9)
+    b = np.ones(nb * 3)
+    assert call(nb, 3, rc, vals, b) == abi.G2OC_ERR_INVALID_ARGUMENT
+    assert b"static scratch" in cuda_lib.g2oc_last_error()
+    # lower-triangle block, unsupported block size, bad device
+    small = np.array([[1, 0]], np.int32)
+    assert call(2, 3, small, np.zeros(9), np.ones(6)) == abi.G2OC_ERR_INVALID_ARGUMENT
+    assert call(1, 4, np.array([[0, 0]]), np.zeros(16), np.ones(4)) == abi.G2OC_ERR_INVALID_ARGUMENT
+    assert call(1, 3, np.array([[0, 0]]), np.eye(3).ravel(), np.ones(3), device=-1) == abi.G2OC_ERR_INVALID_ARGUMENT

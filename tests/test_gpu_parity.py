@@ -268,6 +268,44 @@ def test_reference_block_system_on_gpu(backend):
     assert st == 0 and it > 0 and is_approx(sol, x, 1e-6)
 
 
+def test_pcg_block_system_above_16384_block_rows(backend):
+    """The multi-kernel PCG's column pass writes one partial sum per block row;
+    a block-tridiagonal SPD system of 20,000 3x3 block rows (past the 16,384
+    slots a context starts with) solves to the direct solution."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    rng = np.random.default_rng(11)
+    nb, bs = 20000, 3
+    rc, vals = [], []
+    for c in range(nb):
+        if c > 0:
+            rc.append((c - 1, c))
+            vals.append(rng.uniform(-1, 1, (bs, bs)))
+        M = rng.uniform(-1, 1, (bs, bs))
+        rc.append((c, c))
+        vals.append(M @ M.T + 8 * np.eye(bs))
+    rc = np.array(rc, np.int32)
+    vals = np.stack(vals)
+    offs = np.arange(nb + 1, dtype=np.int32) * bs
+    rows, cols, data = [], [], []
+    for (r, c), M in zip(rc, vals):
+        ii, jj = np.meshgrid(np.arange(bs) + r * bs, np.arange(bs) + c * bs, indexing="ij")
+        rows += [ii.ravel()]
+        cols += [jj.ravel()]
+        data += [M.ravel()]
+        if r != c:
+            rows += [jj.ravel()]
+            cols += [ii.ravel()]
+            data += [M.ravel()]
+    A = sp.csr_matrix((np.concatenate(data), (np.concatenate(rows), np.concatenate(cols))), shape=(nb * bs,) * 2)
+    b = rng.normal(size=nb * bs)
+    x_ref = spl.spsolve(A.tocsc(), b)
+    prm = backend.default_params(pcg_tolerance=1e-24, pcg_max_iterations=300)
+    st, x, it = backend.solve_block_system(LINEAR_PCG, offs, rc, vals.ravel(), b, prm)
+    assert st == 0 and it > 0
+    assert relnorm(x, x_ref) < 1e-9, relnorm(x, x_ref)
+
+
 def test_not_positive_definite_is_reported(backend):
     offs = np.array([0, 3, 6], np.int32)
     rc = np.array([[0, 0], [0, 1], [1, 1]], np.int32)

@@ -57,6 +57,11 @@ def cases():
     yield "reference_36x36", offs, rc, vals, b
     o, rc2, v2, b2, _ = random_spd_system(150, 6, 0.2, seed=3)
     yield "random_150x6", o, rc2, v2, b2
+    # a full upper pattern of 130 block rows has nnzb = 8515 >= 64 * nb: the
+    # 256-thread (wide) row and column passes
+    o3, rc3, v3, b3, _ = random_spd_system(130, 6, 1.0, seed=5)
+    assert len(rc3) >= 64 * 130
+    yield "dense_130x6", o3, rc3, v3, b3
 
 
 @pytest.mark.parametrize("tol,maxit", [(1e-6, -1), (1e-20, 200)])
@@ -72,6 +77,30 @@ def test_static_entry_point_matches_allocating_one(tol, maxit):
             assert st == 0, (name, call, L.g2oc_last_error())
             assert it == it_ref, (name, call, it, it_ref)
             assert np.linalg.norm(x - x_ref) <= TOL * np.linalg.norm(x_ref), (name, call)
+
+
+def test_static_entry_point_solves_reference_fixture():
+    # the reference's 36x36 system: the solution within its test's
+    # isApprox(1e-6) (unit_test/solver/linear_solver_test.cpp:84-101), twice
+    from g2o_b200 import backend
+    from tests.test_oracle_pinning import is_approx, load_sparse_system
+    L = backend.library()
+    offs, rc, vals, b, x_ref, _ = load_sparse_system()
+    for call in range(2):
+        st, x, it = static_solve(L, offs, rc, vals, b, 1e-20, 200)
+        assert st == 0 and it > 0, (call, L.g2oc_last_error())
+        assert is_approx(x, x_ref, 1e-6), call
+
+
+def test_static_entry_point_keeps_the_callers_device():
+    import torch
+    from g2o_b200 import backend
+    L = backend.library()
+    torch.cuda.set_device(0)
+    offs, rc, vals, b, _ = random_spd_system(20, 3, 0.3, seed=9)[:5]
+    st, _, _ = static_solve(L, offs, rc, vals, b, 1e-6, -1)
+    assert st == 0
+    assert torch.cuda.current_device() == 0
 
 
 def test_static_entry_point_rejects_oversized_systems():
