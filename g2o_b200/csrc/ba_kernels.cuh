@@ -507,6 +507,69 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
   }
 }
 
+// One 6x3 Hpl block (18 values, row-major) into both lanes of a lane pair
+// (lanes 2j, 2j+1: half = lane & 1), each lane loading about half of it and
+// the halves exchanged by shuffles. FP32 blocks are 72 bytes at a 72-byte
+// stride: 16-byte aligned when the block index is even, 8-byte aligned when
+// odd, so the loads are float4 where the alignment allows. FP64 blocks (144
+// bytes) are nine 16-byte words split 5 / 4. Every value is loaded by exactly
+// one lane and the other lane's slot holds 0, so the exchange is an exact
+// add of zero. Both lanes must call it with the same block (warp-uniform
+// control over the pair).
+__device__ __forceinline__ void load_block_pair(const float* hpl, int blk, int half, float (&b)[18]) {
+  const float* base = hpl + (size_t)blk * 18;
+#pragma unroll
+  for (int t = 0; t < 18; ++t) b[t] = 0.0f;
+  if ((blk & 1) == 0) {
+    // float4 at 0, 4, 8, 12 and float2 at 16
+    if (half == 0) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(base));
+      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 8));
+      const float2 w = __ldg(reinterpret_cast<const float2*>(base + 16));
+      b[0] = u.x; b[1] = u.y; b[2] = u.z; b[3] = u.w;
+      b[8] = v.x; b[9] = v.y; b[10] = v.z; b[11] = v.w;
+      b[16] = w.x; b[17] = w.y;
+    } else {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 4));
+      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 12));
+      b[4] = u.x; b[5] = u.y; b[6] = u.z; b[7] = u.w;
+      b[12] = v.x; b[13] = v.y; b[14] = v.z; b[15] = v.w;
+    }
+  } else {
+    // float2 at 0 and float4 at 2, 6, 10, 14
+    if (half == 0) {
+      const float2 w = __ldg(reinterpret_cast<const float2*>(base));
+      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 2));
+      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 10));
+      b[0] = w.x; b[1] = w.y;
+      b[2] = u.x; b[3] = u.y; b[4] = u.z; b[5] = u.w;
+      b[10] = v.x; b[11] = v.y; b[12] = v.z; b[13] = v.w;
+    } else {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 6));
+      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 14));
+      b[6] = u.x; b[7] = u.y; b[8] = u.z; b[9] = u.w;
+      b[14] = v.x; b[15] = v.y; b[16] = v.z; b[17] = v.w;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(0xffffffffu, b[t], 1);
+}
+
+__device__ __forceinline__ void load_block_pair(const double* hpl, int blk, int half, double (&b)[18]) {
+  const double2* base = reinterpret_cast<const double2*>(hpl + (size_t)blk * 18);
+#pragma unroll
+  for (int t = 0; t < 18; ++t) b[t] = 0.0;
+#pragma unroll
+  for (int q = 0; q < 9; ++q)
+    if ((q & 1) == half) {
+      const double2 v = __ldg(base + q);
+      b[2 * q] = v.x;
+      b[2 * q + 1] = v.y;
+    }
+#pragma unroll
+  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(0xffffffffu, b[t], 1);
+}
+
 // Dense output of the Schur rows for batched windows: each camera row belongs
 // to one window, whose reduced system is a dense FP64 matrix (n + 1 rows of
 // n, row-major, at M + mat[w]; the last row holds the right-hand side). Only
@@ -538,7 +601,7 @@ struct DenseOut {
 // (block k at tile_off[k], scalar rows 96 apart; an off-diagonal block inside
 // a diagonal tile also into its transposed place) instead of the row-SoA;
 // dn.M != nullptr: into the windows' dense matrices (DenseOut) instead.
-template <typename Real, int THREADS, bool STAGE, int G = 2>
+template <typename Real, int THREADS, bool STAGE, int G = 2, bool COOP = false>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
@@ -686,6 +749,10 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     // The pair list and S are touched once per pass: streamed (evict-first
     // loads and stores), so the L2 lines go to the Hpl blocks gathered again
     auto load_b = [&](int blk, Real (&b)[18]) {
+      if (COOP) {
+        load_block_pair(hpl, blk, half, b);
+        return;
+      }
       const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
 #pragma unroll
       for (int t = 0; t < 9; ++t) {

@@ -25,6 +25,7 @@
 #include "pcg_kernels.cuh"
 #include "pcg_persistent.cuh"
 #include "pcg_tiles.cuh"
+#include "tc_chol.cuh"
 #include "pg_kernels.cuh"
 
 namespace g2oc {
@@ -107,14 +108,14 @@ enum KernelId {
   K_BACKSUB, K_RESID_CAM, K_RESID_LM, K_OPLUS, K_MAX_DIAG, K_PCG_DIAG_INV, K_PCG_INIT, K_PCG_SPMV, K_PCG_UPDATE,
   K_PCG_CHECK, K_PG_LINEARIZE, K_PG_ASSEMBLE_H, K_PG_ASSEMBLE_B, K_DAMP, K_LM_CONTROL, K_REDUCE, K_AXPY,
   K_CHOLESKY, K_PCG_COLPASS, K_SCHUR_DB, K_IO, K_PCG_SOLVE, K_PCG_TILES, K_TILE_COPY, K_BACKWARD, K_PG_RESID,
-  K_COUNT
+  K_TC_EXPAND, K_TC_POTRF, K_TC_TILES, K_TC_SOLVE, K_COUNT
 };
 static const char* kKernelNames[K_COUNT] = {
   "chi2", "errors", "jacobians", "ba_landmark_pass", "ba_camera_pass", "schur_landmark", "schur_blocks",
   "schur_rhs", "ba_backsub", "ba_resid_cam", "ba_resid_lm", "oplus", "max_diag", "pcg_diag_inv", "pcg_init",
   "pcg_spmv", "pcg_update", "pcg_check_dn", "pg_linearize", "pg_assemble_h", "pg_assemble_b", "damp_diag",
   "lm_control", "reduce", "axpy", "cholesky", "pcg_colpass", "schur_db", "io_reorder", "pcg_solve", "pcg_solve_tiles",
-  "sys_to_tiles", "ba_backward", "pg_resid64"};
+  "sys_to_tiles", "ba_backward", "pg_resid64", "tc_expand", "tc_potrf", "tc_tiles", "tc_solve"};
 
 struct PendingTiming {
   int kid;
@@ -463,6 +464,16 @@ static int pcg_mode() {
 }
 static bool kernels_pcg() { return pcg_mode() == PCG_KERNELS; }
 
+// Schur rows: the two lanes of a block pair share each Hpl block load
+// (G2OC_SCHUR_COOP=0: each lane loads the whole block)
+static bool schur_coop() {
+  static const int v = [] {
+    const char* e = getenv("G2OC_SCHUR_COOP");
+    return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
 // LinearSolverPCG::_maxIter (the system dimension when unset); an FP32-stored
 // system (mixed path) is a correction step of the FP64 refinement, so its
 // iterations are capped and the FP64 residual check decides whether another
@@ -653,6 +664,7 @@ struct Engine final : EngineBase {
   size_t schur_smem = 0;
   DBuf<Real> hcontrib;
   DBuf<double> bcontrib;
+  std::unique_ptr<TcChol> tc;  // tensor-core Cholesky of the reduced camera system (mixed precision)
   explicit Engine(g2oc_ctx* ctx) : c(ctx) {}
 
   int alloc() override {
@@ -874,7 +886,7 @@ struct Engine final : EngineBase {
     const int* toff = to_tiles ? c->tile_off.p : nullptr;
     DenseOut dn{c->win_of_cam.p, c->win_cam.p, c->win_mat.p, to_windows ? c->win_scratch.p : nullptr};
     if (stage_in_smem) {
-      auto kern = schur_rows<Real, T, true, G>;
+      auto kern = schur_coop() ? schur_rows<Real, T, true, G, true> : schur_rows<Real, T, true, G, false>;
       G2OC_TRY(raise_dyn_smem((const void*)kern, schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
@@ -940,6 +952,86 @@ struct Engine final : EngineBase {
     return run_pcg_persistent<Real, 3>(c, A, minv.p, rhs, xout, r.p, s.p, d0.p, tbuf.p, cpart.p, fixed_d0);
   }
 
+  // a . b of two device vectors of length n, read on the host (one wait)
+  int dev_dot_host(const double* a, const double* b, int n, double* out) {
+    G2OC_K(K_LM_CONTROL) dot_partials<<<kRedBlocks, 256, 0, c->stream>>>(a, b, n, c->partials.p);
+    G2OC_LAUNCH_CHECK();
+    G2OC_TRY(finalize_sum(c, kRedBlocks, 1, &c->sc.p->refine_bnorm, nullptr));
+    G2OC_CUDA_TRY(cudaMemcpyAsync(out, &c->sc.p->refine_bnorm, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return G2OC_OK;
+  }
+
+  // the Cholesky of a nearly full reduced camera system in mixed precision:
+  // the tensor-core factorization of tc_chol.cuh (S written into the dense
+  // tiles by the Schur pass)
+  bool tc_chol_used() const {
+    const Structure& S = c->S;
+    return sizeof(Real) == 4 && S.ba && S.schur && S.pd == 6 && S.tile_ok &&
+           c->prm.linear_solver == G2OC_LINEAR_CHOLESKY && c->shard_world <= 1;
+  }
+
+  int tc_factor(int* ok) {
+    if constexpr (sizeof(Real) != 4) {
+      set_error("the tensor-core Cholesky factors FP32-stored systems");
+      return G2OC_ERR_NOT_SUPPORTED;
+    } else {
+      const Structure& S = c->S;
+      cudaStream_t st = c->stream;
+      if (!tc) {
+        std::unique_ptr<TcChol> P(new TcChol());
+        const int nbt = (S.sys_nb + kTileBlocks - 1) / kTileBlocks;
+        G2OC_TRY(tc_chol_plan(*P, S.sys_nb * 6, nbt, S.tile_ij, st));
+        tc = std::move(P);
+      }
+      G2OC_TRY(tc_chol_attributes());
+      TcChol& P = *tc;
+      G2OC_CUDA_TRY(cudaMemsetAsync(P.info.p, 0, sizeof(int), st));
+      G2OC_CUDA_TRY(cudaMemsetAsync(P.err.p, 0, sizeof(int), st));
+      const long long total = (long long)P.np * P.np;
+      G2OC_K(K_TC_EXPAND) tc_expand_tiles<<<cdiv(total, 256), 256, 0, st>>>(tiles.p, P.tile_index.p, P.nbt, P.n,
+                                                                           P.np, P.A.p);
+      for (int k = 0; k < P.nt; ++k) {
+        float* Wk = P.W.p + (size_t)k * kTc * kTc;
+        G2OC_K(K_TC_POTRF) tc_potrf<<<1, 512, kTcPotrfSmem, st>>>(P.A.p, P.np, k, Wk, P.info.p);
+        const int p0 = P.list_ptr[2 * k], p1 = P.list_ptr[2 * k + 1], p2 = P.list_ptr[2 * k + 2];
+        if (p1 > p0)
+          G2OC_K(K_TC_TILES) tc_tiles<<<p1 - p0, 128, kTcSmem, st>>>(P.A.p, P.np, k, P.lists.p + p0, Wk, P.err.p);
+        if (p2 > p1)
+          G2OC_K(K_TC_TILES) tc_tiles<<<p2 - p1, 128, kTcSmem, st>>>(P.A.p, P.np, k, P.lists.p + p1, Wk, P.err.p);
+      }
+      G2OC_LAUNCH_CHECK();
+      int h[2];
+      G2OC_CUDA_TRY(cudaMemcpyAsync(&h[0], P.info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      G2OC_CUDA_TRY(cudaMemcpyAsync(&h[1], P.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+      G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+      if (h[1]) {
+        set_error("tensor-core Cholesky: a bounded wait for the tile products gave up");
+        return G2OC_ERR_TIMEOUT;
+      }
+      *ok = h[0] == 0;
+      return G2OC_OK;
+    }
+  }
+
+  // x = S^-1 rhs with the factor of tc_factor (FP64 substitutions)
+  int tc_resolve(const double* rhs, double* xout) {
+    TcChol& P = *tc;
+    cudaStream_t st = c->stream;
+    G2OC_K(K_TC_SOLVE) tc_load_rhs<<<cdiv(P.np, 256), 256, 0, st>>>(rhs, P.n, P.np, P.y.p);
+    for (int k = 0; k < P.nt; ++k) {
+      G2OC_K(K_TC_SOLVE) tc_apply_w<<<1, kTc, 0, st>>>(P.W.p + (size_t)k * kTc * kTc, P.y.p, k, false);
+      if (k + 1 < P.nt) G2OC_K(K_TC_SOLVE) tc_fwd_update<<<P.nt - k - 1, kTc, 0, st>>>(P.A.p, P.np, k, P.y.p);
+    }
+    for (int k = P.nt - 1; k >= 0; --k) {
+      G2OC_K(K_TC_SOLVE) tc_apply_w<<<1, kTc, 0, st>>>(P.W.p + (size_t)k * kTc * kTc, P.y.p, k, true);
+      if (k > 0) G2OC_K(K_TC_SOLVE) tc_bwd_update<<<k, kTc, 0, st>>>(P.A.p, P.np, k, P.y.p);
+    }
+    G2OC_LAUNCH_CHECK();
+    G2OC_CUDA_TRY(cudaMemcpyAsync(xout, P.y.p, (size_t)P.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return G2OC_OK;
+  }
+
   int chol_solve(const Real* val, const double* rhs, double* xout, int* ok) {
     const Structure& S = c->S;
     if (!c->chol) {
@@ -982,13 +1074,20 @@ struct Engine final : EngineBase {
                               G2OC_RED_SUM));
         G2OC_TRY(shard_reduce(c, c->rhs.p, (long long)S.Cf * 6, G2OC_DT_F64, G2OC_RED_SUM));
       } else {
-        G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, !use_chol && tile_pcg_used()));
+        G2OC_TRY(schur(lambda, c->rhs.p, nullptr, nullptr, (!use_chol && tile_pcg_used()) || tc_chol_used()));
       }
       const double* bp = c->b.p;
       const double* bl = c->b.p + (size_t)S.Cf * 6;
       if (ts) c->span(ts, &c->cur_stats->time_schur_complement, &c->cur_stats->time_linear_solver);
-      if (use_chol) G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
-      else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false));
+      const bool tc_chol = use_chol && tc_chol_used();
+      if (tc_chol) {
+        G2OC_TRY(tc_factor(&ok));
+        G2OC_TRY(tc_resolve(c->rhs.p, c->xs.p));
+      } else if (use_chol) {
+        G2OC_TRY(chol_solve(Sval.p, c->rhs.p, c->xs.p, &ok));
+      } else {
+        G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, false));
+      }
       G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
       G2OC_TRY(backsub(bl, c->xs.p, c->x.p + (size_t)S.Cf * 6));
       // mixed precision: FP64 iterative refinement on the true residual of
@@ -998,9 +1097,14 @@ struct Engine final : EngineBase {
       // reduced residual's M-norm is above that d0, i.e. while the FP32
       // storage of H / S / Dinv, not the PCG tolerance, limits the step; a
       // correction that raises the residual is undone and ends the loop.
-      if (sizeof(Real) == 4 && ok && !use_chol && c->prm.refine_max_iterations >= 0) {
+      // With the tensor-core Cholesky the same loop runs with corrections
+      // from the kept factor, stopping when |r_s| / |b_s| of the reduced
+      // system is at or below refine_tolerance.
+      if (sizeof(Real) == 4 && ok && (!use_chol || tc_chol) && c->prm.refine_max_iterations >= 0) {
         const int n = c->vec_size();
         double prev = -1.0;
+        double bs2 = 0.0;
+        if (tc_chol) G2OC_TRY(dev_dot_host(c->rhs.p, c->rhs.p, S.Cf * 6, &bs2));
         for (int k = 0; k <= c->prm.refine_max_iterations; ++k) {
           double* rp = c->resid.p;
           double* rl = c->resid.p + (size_t)S.Cf * 6;
@@ -1019,22 +1123,33 @@ struct Engine final : EngineBase {
                                                                            bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
           G2OC_LAUNCH_CHECK();
           G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
-          G2OC_K(K_PCG_CHECK) pcg_check_dn<6><<<cdiv(S.Cf, 128), 128, 0, st>>>(S.Cf, minv.p, c->rhs.p, c->partials.p,
-                                                                               c->pcg.p);
-          G2OC_LAUNCH_CHECK();
-          PcgState ps;
-          G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-          G2OC_CUDA_TRY(cudaStreamSynchronize(st));
-          c->last_refine_dn = ps.check_dn;
-          if (prev >= 0.0 && !(ps.check_dn < prev)) {
+          double check = 0.0, bound = 0.0;
+          if (tc_chol) {
+            double rs2 = 0.0;
+            G2OC_TRY(dev_dot_host(c->rhs.p, c->rhs.p, S.Cf * 6, &rs2));
+            check = bs2 > 0.0 ? std::sqrt(rs2 / bs2) : 0.0;
+            bound = c->prm.refine_tolerance;
+          } else {
+            G2OC_K(K_PCG_CHECK) pcg_check_dn<6><<<cdiv(S.Cf, 128), 128, 0, st>>>(S.Cf, minv.p, c->rhs.p,
+                                                                                 c->partials.p, c->pcg.p);
+            G2OC_LAUNCH_CHECK();
+            PcgState ps;
+            G2OC_CUDA_TRY(cudaMemcpyAsync(&ps, c->pcg.p, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+            G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+            check = ps.check_dn;
+            bound = ps.d0;
+          }
+          c->last_refine_dn = check;
+          if (prev >= 0.0 && !(check < prev)) {
             // the last correction did not reduce the true residual: undo it
             G2OC_K(K_AXPY) axpy_kernel<<<cdiv(n, 256), 256, 0, st>>>(c->x.p, c->dx.p, -1.0, n);
             G2OC_LAUNCH_CHECK();
             break;
           }
-          if (!(ps.check_dn > ps.d0) || k == c->prm.refine_max_iterations) break;
-          prev = ps.check_dn;
-          G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true));
+          if (!(check > bound) || k == c->prm.refine_max_iterations) break;
+          prev = check;
+          if (tc_chol) G2OC_TRY(tc_resolve(c->rhs.p, c->xs.p));
+          else G2OC_TRY(pcg_solve(Sval.p, c->rhs.p, c->xs.p, true));
           c->refine_steps++;
           G2OC_CUDA_TRY(cudaMemcpyAsync(c->dx.p, c->xs.p, (size_t)S.Cf * 6 * sizeof(double), cudaMemcpyDeviceToDevice, st));
           G2OC_TRY(backsub(rl, c->xs.p, c->dx.p + (size_t)S.Cf * 6));

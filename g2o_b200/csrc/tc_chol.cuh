@@ -1,0 +1,418 @@
+// tc_chol.cuh -- dense Cholesky of a nearly full reduced camera system on the
+// 5th-generation tensor cores: the role of LinearSolverDense
+// (g2o/solvers/dense/linear_solver_dense.h:57-105) when the Schur complement
+// of a bundle adjustment is dense enough that a direct factorization is
+// GEMM-shaped.
+//
+// Storage: the system is expanded into a dense FP32 column-major np x np
+// matrix (np a multiple of 128; the padding is the identity), lower triangle.
+// Right-looking blocked factorization in 128 x 128 tiles; per step k:
+//   tc_potrf:  the diagonal tile is factored in FP64 in shared memory (one
+//              CTA) and W(k) = L(k,k)^-1 is formed; L(k,k) and W(k) are
+//              stored in FP32;
+//   tc_tiles:  panel L(i,k) = A(i,k) W(k)^T and trailing update
+//              A(i,j) -= L(i,k) L(j,k)^T, one CTA per 128 x 128 output tile,
+//              as tcgen05.mma kind::tf32 products (M = N = 128, K = 8 per
+//              instruction) issued by one thread, operands in shared memory,
+//              the FP32 accumulator in tensor memory (128 lanes x 128
+//              columns), read back with tcgen05.ld for the epilogue.
+// Each operand value x is split into hi = tf32(x) and lo = tf32(x - hi) and
+// a product is formed as hi*hi + hi*lo + lo*hi (three MMAs per K step), which
+// gives FP32-level accuracy; accumulation is FP32 in tensor memory.
+// Solves use the factor in FP64 arithmetic: y(k) = W(k) (y(k)) then the
+// updates of the other tiles, forward and backward. The caller refines the
+// solution on its true FP64 residual.
+//
+// Shared-memory operand layout (no swizzle, MN-major canonical form of the
+// UMMA descriptor): element (i, j) of a 128 (M or N) x 64 (K) FP32 tile at
+// byte (i % 4) * 4 + (j % 8) * 16 + (i / 4) * 128 + (j / 8) * 4096: core
+// matrices of 4 MN x 8 K (128 bytes), MN groups 128 bytes apart (stride byte
+// offset), K groups 4096 bytes apart (leading byte offset).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "g2oc_internal.h"
+
+namespace g2oc {
+
+constexpr int kTc = 128;           // tile edge
+constexpr int kTcK = 64;           // K per staged chunk
+constexpr int kTcOpBytes = kTc * kTcK * 4;        // one operand tile (hi or lo): 32 KB
+constexpr int kTcSmem = 4 * kTcOpBytes + 1024;    // A hi/lo, B hi/lo, barrier and TMEM address
+constexpr long long kTcSpinLimit = 1ll << 26;     // bounded waits (tens of ms at worst)
+constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + kTc) * sizeof(double);
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t tc_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ float tc_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// UMMA shared-memory descriptor: start address, leading / stride byte
+// offsets (16-byte units), version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// instruction descriptor: kind::tf32, D in FP32, A and B TF32, both MN-major,
+// N = 128 (bits 17-22: N >> 3), M = 128 (bits 24-28: M >> 4)
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+                              ((uint32_t)(kTc >> 3) << 17) | ((uint32_t)(kTc >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// wait for phase `parity` of the barrier, at most kTcSpinLimit polls; false
+// when the limit ran out
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kTcSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(r[t]);
+}
+
+// stage a 128 (MN) x 64 (K) FP32 sub-tile of a column-major matrix (column
+// j of the sub-tile at G + j * ld, 16-byte aligned) as hi / lo TF32 parts.
+// Warp w writes 512 contiguous bytes (four MN groups x eight K columns) and
+// reads four 64-byte runs of each of eight columns.
+__device__ __forceinline__ void tc_stage(const float* G, size_t ld, unsigned char* hi, unsigned char* lo) {
+  for (int q = threadIdx.x; q < kTc * kTcK / 4; q += blockDim.x) {
+    const int lane = q & 31, w = q >> 5;
+    const int j = (w & 7) * 8 + (lane & 7);
+    const int g = (w >> 3) * 4 + (lane >> 3);
+    const float4 v = *reinterpret_cast<const float4*>(G + (size_t)j * ld + g * 4);
+    float4 h, l;
+    h.x = tc_tf32(v.x);
+    h.y = tc_tf32(v.y);
+    h.z = tc_tf32(v.z);
+    h.w = tc_tf32(v.w);
+    l.x = tc_tf32(v.x - h.x);
+    l.y = tc_tf32(v.y - h.y);
+    l.z = tc_tf32(v.z - h.z);
+    l.w = tc_tf32(v.w - h.w);
+    const uint32_t off = (uint32_t)g * 128 + (uint32_t)(j & 7) * 16 + (uint32_t)(j >> 3) * 4096;
+    *reinterpret_cast<float4*>(hi + off) = h;
+    *reinterpret_cast<float4*>(lo + off) = l;
+  }
+}
+
+// ------------------------------------------------------------ tile products
+// One CTA (128 threads, one warpgroup) per output tile:
+//   panel  (ij.y < 0):  L(i,k) = A(i,k) W(k)^T          (ij.x = i)
+//   update (ij.y >= 0): A(i,j) -= L(i,k) L(j,k)^T       (i = ij.x, j = ij.y)
+// P = X Y^T with X the 128 x 128 left operand and Y the right one (both
+// column-major, leading dimension ldx / ldy), formed over two K chunks of 64.
+// *err is set when a bounded wait gives up (the tile is then left unchanged).
+static __global__ void __launch_bounds__(128, 1)
+    tc_tiles(float* A, int np, int k, const int2* list, const float* Wk, int* err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned char* a_hi = tc_smem;
+  unsigned char* a_lo = tc_smem + kTcOpBytes;
+  unsigned char* b_hi = tc_smem + 2 * kTcOpBytes;
+  unsigned char* b_lo = tc_smem + 3 * kTcOpBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tc_smem + 4 * kTcOpBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + 4 * kTcOpBytes + 64);
+  const int2 ij = list[blockIdx.x];
+  const bool panel = ij.y < 0;
+  const size_t kb = (size_t)k * kTc;
+  const float* X = A + kb * np + (size_t)ij.x * kTc;           // A(i,k) or L(i,k)
+  const float* Y = panel ? Wk : A + kb * np + (size_t)ij.y * kTc;  // W(k) or L(j,k)
+  const size_t ldy = panel ? (size_t)kTc : (size_t)np;
+  float* D = A + (panel ? kb : (size_t)ij.y * kTc) * np + (size_t)ij.x * kTc;
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(tmem_slot)),
+                 "r"(kTc));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t mb = tc_smem_addr(mbar);
+  bool ok = true;
+  for (int ch = 0; ch < kTc / kTcK && ok; ++ch) {
+    tc_stage(X + (size_t)ch * kTcK * np, np, a_hi, a_lo);
+    tc_stage(Y + (size_t)ch * kTcK * ldy, ldy, b_hi, b_lo);
+    // the generic-proxy stores must be visible to the tensor core's reads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tc_fence_after();
+      const uint32_t ah = tc_smem_addr(a_hi), al = tc_smem_addr(a_lo);
+      const uint32_t bh = tc_smem_addr(b_hi), bl = tc_smem_addr(b_lo);
+#pragma unroll
+      for (int kg = 0; kg < kTcK / 8; ++kg) {
+        const uint32_t o = (uint32_t)kg * 4096;
+        tc_mma(tmem, tc_desc(ah + o, 4096, 128), tc_desc(bh + o, 4096, 128), (ch > 0 || kg > 0) ? 1u : 0u);
+        tc_mma(tmem, tc_desc(ah + o, 4096, 128), tc_desc(bl + o, 4096, 128), 1u);
+        tc_mma(tmem, tc_desc(al + o, 4096, 128), tc_desc(bh + o, 4096, 128), 1u);
+      }
+      tc_commit(mb);
+    }
+    // every thread waits for the products of this chunk before the operand
+    // tiles are overwritten (or the accumulator is read); the outcome is
+    // made uniform over the CTA so every thread takes the same path
+    ok = __syncthreads_and(tc_wait(mb, (uint32_t)(ch & 1)) ? 1 : 0) != 0;
+  }
+  tc_fence_after();
+  if (!ok) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+  } else {
+    // epilogue: thread (warp w, lane t) holds row m = 32 w + t of P
+    const int m = threadIdx.x;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < kTc; c0 += 16) {
+      float v[16];
+      tc_ld16(lane_base + (uint32_t)c0, v);
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        float* d = D + (size_t)(c0 + t) * np + m;
+        if (panel) *d = v[t];
+        else *d -= v[t];
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTc));
+  }
+}
+
+// ------------------------------------------------------------ diagonal tile
+// Factor the diagonal tile k in FP64 (lower), write L(k,k) back in FP32 and
+// W(k) = L(k,k)^-1 (FP32, column-major 128 x 128, zero above the diagonal)
+// to Wk. A non-positive pivot sets *info (the pivot is replaced by 1 so the
+// arithmetic stays finite). 512 threads; the factor's column j is finished
+// by one sweep (pivot, scaled column, trailing rank-1 update of the lower
+// triangle).
+static __global__ void __launch_bounds__(512, 1) tc_potrf(float* A, int np, int k, float* Wk, int* info) {
+  extern __shared__ double tcp_smem[];
+  double* T = tcp_smem;                 // 128 x 129, column-major: T[j * 129 + i]
+  double* wd = tcp_smem + kTc * (kTc + 1);  // reciprocal pivots
+  constexpr int LD = kTc + 1;
+  const size_t kb = (size_t)k * kTc;
+  for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
+    const int i = e % kTc, j = e / kTc;
+    if (i >= j) T[j * LD + i] = (double)A[(kb + j) * np + kb + i];
+  }
+  __syncthreads();
+  for (int j = 0; j < kTc; ++j) {
+    if (threadIdx.x == 0) {
+      double d = T[j * LD + j];
+      if (!(d > 0.0)) {
+        atomicExch(info, 1);
+        d = 1.0;
+      }
+      const double s = sqrt(d);
+      T[j * LD + j] = s;
+      wd[j] = 1.0 / s;
+    }
+    __syncthreads();
+    const double r = wd[j];
+    for (int i = j + 1 + threadIdx.x; i < kTc; i += blockDim.x) T[j * LD + i] *= r;
+    __syncthreads();
+    const int m = kTc - j - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = j + 1 + e % m, c = j + 1 + e / m;
+      if (i >= c) T[c * LD + i] -= T[j * LD + i] * T[j * LD + c];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
+    const int i = e % kTc, j = e / kTc;
+    if (i >= j) A[(kb + j) * np + kb + i] = (float)T[j * LD + i];
+  }
+  // W = L^-1, column c by thread c (forward substitution of e_c); W(l, c)
+  // for l > c kept in the free upper triangle of T at (row c, column l)
+  if (threadIdx.x < kTc) {
+    const int c = threadIdx.x;
+    for (int i = 0; i < kTc; ++i) {
+      double v;
+      if (i < c) {
+        v = 0.0;
+      } else if (i == c) {
+        v = wd[c];
+      } else {
+        double acc = T[c * LD + i] * wd[c];  // L(i,c) W(c,c)
+        for (int l = c + 1; l < i; ++l) acc += T[l * LD + i] * T[l * LD + c];
+        v = -acc * wd[i];
+        T[i * LD + c] = v;
+      }
+      Wk[(size_t)c * kTc + i] = (float)v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ solves
+// y(k) = W(k) y(k) (128 threads, FP64)
+static __global__ void tc_apply_w(const float* Wk, double* y, int k, bool transpose) {
+  __shared__ double v[kTc];
+  const int r = threadIdx.x;
+  v[r] = y[(size_t)k * kTc + r];
+  __syncthreads();
+  double acc = 0.0;
+  if (!transpose) {
+    for (int c = 0; c <= r; ++c) acc += (double)Wk[(size_t)c * kTc + r] * v[c];
+  } else {
+    for (int c = r; c < kTc; ++c) acc += (double)Wk[(size_t)r * kTc + c] * v[c];
+  }
+  y[(size_t)k * kTc + r] = acc;
+}
+
+// forward update: y(i) -= L(i,k) y(k) for the tiles i > k (CTA per tile,
+// thread per row, columns in order)
+static __global__ void tc_fwd_update(const float* A, int np, int k, double* y) {
+  __shared__ double v[kTc];
+  const int i = k + 1 + blockIdx.x, r = threadIdx.x;
+  v[r] = y[(size_t)k * kTc + r];
+  __syncthreads();
+  const float* L = A + (size_t)k * kTc * np + (size_t)i * kTc + r;
+  double acc = 0.0;
+  for (int c = 0; c < kTc; ++c) acc += (double)L[(size_t)c * np] * v[c];
+  y[(size_t)i * kTc + r] -= acc;
+}
+
+// backward update: y(l) -= L(k,l)^T x(k) for the tiles l < k (CTA per tile;
+// warp per group of columns, lanes over the rows, fixed-order shuffle sums)
+static __global__ void tc_bwd_update(const float* A, int np, int k, double* y) {
+  __shared__ double v[kTc];
+  const int l = blockIdx.x;
+  v[threadIdx.x] = y[(size_t)k * kTc + threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c = warp; c < kTc; c += blockDim.x >> 5) {
+    const float* col = A + ((size_t)l * kTc + c) * np + (size_t)k * kTc;
+    double acc = 0.0;
+    for (int r = lane; r < kTc; r += 32) acc += (double)col[r] * v[r];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[(size_t)l * kTc + c] -= acc;
+  }
+}
+
+// ------------------------------------------------------------ expansion
+// dense FP32 column-major lower triangle of the system held in the dense
+// 96 x 96 tiles of the tile PCG (kTileBlocks 6x6 blocks per tile edge; tile
+// (R, C), R <= C, row-major; tile_index[R * nbt + C] = its index or -1),
+// identity on the padding (rows n .. np-1)
+static __global__ void tc_expand_tiles(const float* tiles, const int* tile_index, int nbt, int n, int np, float* A) {
+  constexpr int TS = kTileBlocks * 6;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)np * np) return;
+  const int j = (int)(t / np), i = (int)(t % np);  // column j, row i; only i >= j is written and read
+  if (i < j) return;
+  float v = 0.0f;
+  if (i < n) {
+    // S(i, j) = S(j, i): row j, column i of the upper storage
+    const int R = j / TS, C = i / TS;
+    const int ti = tile_index[R * nbt + C];
+    if (ti >= 0) v = tiles[(size_t)ti * TS * TS + (size_t)(j % TS) * TS + (i % TS)];
+  } else if (i == j) {
+    v = 1.0f;
+  }
+  A[t] = v;
+}
+
+static __global__ void tc_load_rhs(const double* b, int n, int np, double* y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < np) y[t] = t < n ? b[t] : 0.0;
+}
+
+// ------------------------------------------------------------ host driver
+struct TcChol {
+  int n = 0, np = 0, nt = 0, nbt = 0;
+  DBuf<float> A, W;
+  DBuf<double> y;
+  DBuf<int> info, err, tile_index;
+  DBuf<int2> lists;                 // per step: panel tiles then update pairs
+  std::vector<int> list_ptr;        // per step: [panel start, update start, end)
+};
+
+static int tc_chol_plan(TcChol& P, int n, int nbt_tiles, const std::vector<int32_t>& tile_ij, cudaStream_t st) {
+  P.n = n;
+  P.nt = (n + kTc - 1) / kTc;
+  P.np = P.nt * kTc;
+  P.nbt = nbt_tiles;
+  std::vector<int> index((size_t)nbt_tiles * nbt_tiles, -1);
+  for (size_t t = 0; t < tile_ij.size() / 2; ++t) index[(size_t)tile_ij[2 * t] * nbt_tiles + tile_ij[2 * t + 1]] = (int)t;
+  G2OC_TRY(P.tile_index.upload(index, st));
+  std::vector<int2> L;
+  P.list_ptr.assign(2 * P.nt + 1, 0);
+  for (int k = 0; k < P.nt; ++k) {
+    P.list_ptr[2 * k] = (int)L.size();
+    for (int i = k + 1; i < P.nt; ++i) L.push_back(make_int2(i, -1));
+    P.list_ptr[2 * k + 1] = (int)L.size();
+    for (int j = k + 1; j < P.nt; ++j)
+      for (int i = j; i < P.nt; ++i) L.push_back(make_int2(i, j));
+  }
+  P.list_ptr[2 * P.nt] = (int)L.size();
+  if (L.empty()) L.push_back(make_int2(0, 0));
+  G2OC_TRY(P.lists.upload(L, st));
+  G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
+  G2OC_TRY(P.W.alloc((size_t)P.nt * kTc * kTc));
+  G2OC_TRY(P.y.alloc(P.np));
+  G2OC_TRY(P.info.alloc(1));
+  G2OC_TRY(P.err.alloc(1));
+  return G2OC_OK;
+}
+
+// dynamic shared memory of the two large kernels (once per process)
+static int tc_chol_attributes() {
+  static bool done = false;
+  if (done) return G2OC_OK;
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(tc_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcPotrfSmem));
+  done = true;
+  return G2OC_OK;
+}
+
+}  // namespace g2oc

@@ -148,6 +148,46 @@ def test_ba_cholesky_solve_is_exact(backend, oracle_lib):
     assert relnorm(xc, xo) < 1e-9
 
 
+@pytest.mark.parametrize("cams,points", [(64, 4000), (140, 6000)])
+def test_ba_tensor_core_cholesky_solve(backend, oracle_lib, cams, points):
+    """lm_cuda_chol_mixed on a bundle adjustment whose reduced camera system
+    is nearly full: the tensor-core Cholesky (tcgen05 3xTF32 tile products,
+    FP64 diagonal tiles) of the FP32-stored Schur complement, refined on the
+    FP64 residual, solves the damped system to 1e-9 of the oracle's FP64
+    Cholesky solve (LinearSolverDense's role)."""
+    g = small_ba(seed=23, cams=cams, points=points)
+    prm = backend.OptimizationAlgorithmFactory.instance().construct("lm_cuda_chol_mixed")
+    prm.refine_max_iterations = 10
+    prm.refine_tolerance = 1e-14
+    c = backend.CudaProblem(g, prm)
+    o = oracle_lib.OracleProblem(g, oracle_lib.default_params(linear_solver=LINEAR_CHOLESKY))
+    c.build_system()
+    o.build_system()
+    for lam in (1e-2, 1.0):
+        st, xc, _ = c.solve(lam)
+        so, xo, _ = o.solve(lam)
+        assert st == 0 and so == 0
+        assert relnorm(xc, xo) < 1e-9, (lam, relnorm(xc, xo))
+    _, ks = c.kernel_stats()
+    assert ks["tc_tiles"][0] > 0 and ks["tc_potrf"][0] > 0
+    c.close()
+
+
+def test_ba_tensor_core_cholesky_lm_trajectory(backend, oracle_lib):
+    """LM over the tensor-core Cholesky with FP64 refinement of every step
+    follows the oracle's FP64 Cholesky trajectory: the same trials and chi2
+    within 1e-6 per iteration."""
+    g = small_ba(seed=29, cams=64, points=4000)
+    o = oracle_lib.OracleProblem(g, oracle_lib.default_params(linear_solver=LINEAR_CHOLESKY))
+    c = backend.CudaProblem(g, backend.OptimizationAlgorithmFactory.instance().construct("lm_cuda_chol_mixed"))
+    _, so = o.optimize(10)
+    _, sc = c.optimize(10)
+    c.close()
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"], a["iteration"]
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
+
+
 def test_ba_lm_trajectory(backend, oracle_lib):
     g = small_ba()
     o, c = both(backend, oracle_lib, g)
