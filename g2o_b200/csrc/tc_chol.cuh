@@ -405,14 +405,4 @@ static int tc_chol_plan(TcChol& P, int n, int nbt_tiles, const std::vector<int32
   return G2OC_OK;
 }
 
-// dynamic shared memory of the two large kernels (once per process)
-static int tc_chol_attributes() {
-  static bool done = false;
-  if (done) return G2OC_OK;
-  G2OC_CUDA_TRY(cudaFuncSetAttribute(tc_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-  G2OC_CUDA_TRY(cudaFuncSetAttribute(tc_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcPotrfSmem));
-  done = true;
-  return G2OC_OK;
-}
-
 }  // namespace g2oc
