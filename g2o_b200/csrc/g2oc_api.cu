@@ -264,6 +264,10 @@ struct g2oc_ctx {
   // launch accounting
   bool timing = false;
   long long kcount[g2oc::K_COUNT] = {};
+  // grid-barrier arrivals expected beyond the grid: 0, or 1 when the context
+  // was created with G2OC_TEST_BARRIER_EXTRA set (every bounded barrier wait
+  // of the persistent PCG then runs out: the test of that path)
+  unsigned barrier_extra = 0;
   double ktime_ms[g2oc::K_COUNT] = {};
   long long chol_launches = 0;
   std::vector<cudaEvent_t> event_pool;
@@ -596,9 +600,10 @@ static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* 
   double* part_dq = c->partials.p;
   double* part_rs = c->partials.p + 4096;
   PcgState* stp = c->pcg.p;
+  unsigned extra = c->barrier_extra;
   void* args[] = {&a,    &chunk_ptr, &chunk_row, &nchunks, &minv,    &rhs,    &xout, &r,       &s,
                   &d,    &tbuf,      &cpart,     &part_dq, &part_rs, &stp,    &tol,  &max_iter, &abs_tol,
-                  &fixed};
+                  &fixed, &extra};
   G2OC_K(K_PCG_SOLVE) { G2OC_TRY(coop_launch(c, (const void*)pcg_solve_persistent<Real, BS>, grid, kPcgThreads, args)); }
   return G2OC_OK;
 }
@@ -630,8 +635,9 @@ static int run_pcg_tiles(g2oc_ctx* c, const Real* tiles, int nb, const double* m
   double* part_dq = c->partials.p;
   double* part_rs = c->partials.p + 4096;
   PcgState* stp = c->pcg.p;
+  unsigned extra = c->barrier_extra;
   void* args[] = {&tiles, &tij,  &ntiles, &nbt,  &nb,      &minv,    &rhs, &xout,     &r,       &s,
-                  &dbuf0, &dbuf1, &part,  &part_dq, &part_rs, &stp, &tol, &max_iter, &abs_tol, &fixed};
+                  &dbuf0, &dbuf1, &part,  &part_dq, &part_rs, &stp, &tol, &max_iter, &abs_tol, &fixed, &extra};
   G2OC_K(K_PCG_TILES) { G2OC_TRY(coop_launch(c, (const void*)pcg_solve_tiles<Real>, grid, kTileThreads, args)); }
   return G2OC_OK;
 }
@@ -2044,6 +2050,7 @@ int g2oc_create(int device, g2oc_ctx** out) {
   G2OC_CUDA_TRY(cudaSetDevice(device));
   std::unique_ptr<g2oc_ctx> c(new g2oc_ctx());
   c->device = device;
+  if (const char* e = getenv("G2OC_TEST_BARRIER_EXTRA")) c->barrier_extra = atoi(e) > 0 ? 1u : 0u;
   G2OC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   g2oc_default_params(&c->prm);
   G2OC_TRY(c->sc.alloc(1));

@@ -39,18 +39,21 @@ constexpr unsigned int kGridSyncSpinLimit = 1u << 21;
 // grid_gen_start (no barrier can complete before every CTA has read it) and
 // counted locally after that, so an arrival costs one atomic and no read of
 // the shared generation. Returns false (in every thread of the CTA) once any
-// CTA's wait has run out; the caller then returns.
+// CTA's wait has run out; the caller then returns. extra: arrivals expected
+// beyond the grid (0; a context created with G2OC_TEST_BARRIER_EXTRA set
+// passes 1, so that no barrier completes and every wait runs out: the test
+// of the bounded wait and of the status the host reads back).
 __device__ __forceinline__ unsigned grid_gen_start(const PcgState* st) {
   return threadIdx.x == 0 ? *reinterpret_cast<const volatile unsigned int*>(&st->sync_gen) : 0u;
 }
-__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen) {
+__device__ __forceinline__ bool grid_barrier(PcgState* st, unsigned& gen, unsigned extra) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned int* vgen = &st->sync_gen;
     volatile int* verr = &st->sync_error;
     __threadfence();
-    if (atomicAdd(&st->sync_count, 1u) == gridDim.x - 1) {
+    if (atomicAdd(&st->sync_count, 1u) == gridDim.x - 1 + extra) {
       atomicExch(&st->sync_count, 0u);
       __threadfence();
       atomicAdd(&st->sync_gen, 1u);
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
     pcg_solve_persistent(SysDev<Real> A, const int* chunk_ptr, const int* chunk_row, int nchunks, const double* minv,
                          const double* b, double* x, double* r, double* s, double* d, double* tbuf, double* cpart,
                          double* part_dq, double* part_rs, PcgState* st, double tol, int max_iter, int abs_tol,
-                         int fixed_d0) {
+                         int fixed_d0, unsigned barrier_extra) {
   __shared__ double red[kPcgWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPcgWarps + warp, GW = gridDim.x * kPcgWarps;
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
     }
   }
   cta_partial(rs, part_rs, red);
-  if (!grid_barrier(st, gen)) return;
+  if (!grid_barrier(st, gen, barrier_extra)) return;
   double dn = cta_sum_all(part_rs, red);
   double d0 = d0_in;
   if (!fixed) {
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
       if (lane < BS) cpart[(size_t)ch * BS + lane] = pick<BS>(acc, lane);
     }
     cta_partial(dq, part_dq, red);
-    if (!grid_barrier(st, gen)) return;
+    if (!grid_barrier(st, gen, barrier_extra)) return;
     const double dqs = cta_sum_all(part_dq, red);
     if (!(dqs > 0.0)) {
       // the (rounded) matrix is not positive definite along d: stop with the
@@ -257,7 +260,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
       }
     }
     cta_partial(rs, part_rs, red);
-    if (!grid_barrier(st, gen)) return;
+    if (!grid_barrier(st, gen, barrier_extra)) return;
     const double dn_new = cta_sum_all(part_rs, red);
     const double beta = dn_new / dn;
     dn = dn_new;
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2)
         const size_t o = (size_t)c * BS + lane;
         d[o] = __ldcg(s + o) + beta * __ldcg(d + o);
       }
-    if (!grid_barrier(st, gen)) return;
+    if (!grid_barrier(st, gen, barrier_extra)) return;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->dn = dn;

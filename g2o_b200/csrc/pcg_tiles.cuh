@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     pcg_solve_tiles(const Real* tiles, const int2* tile_ij, int ntiles, int nbt, int nb, const double* minv,
                     const double* b, double* x, double* r, double* s, double* dbuf0, double* dbuf1, double* part,
                     double* part_dq, double* part_rs, PcgState* st, double tol, int max_iter, int abs_tol,
-                    int fixed_d0) {
+                    int fixed_d0, unsigned barrier_extra) {
   constexpr int BS = 6;
   __shared__ double red[kTileWarps];
   __shared__ double drow[kTileScalars], dcol[kTileScalars];
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     }
   }
   cta_partial<kTileWarps>(rs, part_rs, red);
-  if (!grid_barrier(st, gen)) return;
+  if (!grid_barrier(st, gen, barrier_extra)) return;
   double dn = cta_sum_all<kTileWarps>(part_rs, red);
   double d0 = d0_in;
   if (!fixed) {
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
     for (int b2 = 0; b2 < BS; ++b2) mrow[b2] = 0.0;
     if (gw < nb) load_row(gw);
     cta_partial<kTileWarps>(dq, part_dq, red);
-    if (!grid_barrier(st, gen)) return;
+    if (!grid_barrier(st, gen, barrier_extra)) return;
     const double dqs = cta_sum_all<kTileWarps>(part_dq, red);
     if (!(dqs > 0.0)) {
       breakdown = true;  // not positive definite along d (see pcg_solve_persistent)
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(kTileThreads, sizeof(Real) == 4 ? 3 : 2)
       }
     }
     cta_partial<kTileWarps>(rs, part_rs, red);
-    if (!grid_barrier(st, gen)) return;
+    if (!grid_barrier(st, gen, barrier_extra)) return;
     const double dn_new = cta_sum_all<kTileWarps>(part_rs, red);
     beta = dn_new / dn;
     dn = dn_new;

@@ -346,6 +346,30 @@ def test_pcg_block_system_above_16384_block_rows(backend):
     assert relnorm(x, x_ref) < 1e-9, relnorm(x, x_ref)
 
 
+@pytest.mark.parametrize("cams", [40, 64])
+def test_grid_barrier_wait_runs_out_and_reports_timeout(backend, monkeypatch, cams):
+    """The persistent PCG's grid barriers wait a bounded time. A context
+    created with G2OC_TEST_BARRIER_EXTRA expects one arrival more than the
+    grid launches, so no barrier completes: every wait runs out, the kernel
+    returns, and the host reports G2OC_ERR_TIMEOUT (no trap, no hang). The
+    device stays usable: the same context's state is reset, and another
+    context optimizes the same graph normally. 40 cameras: the sparse
+    persistent solve; 64: the dense-tile solve."""
+    from g2o_b200.abi import G2OC_ERR_TIMEOUT
+    g = small_ba(seed=31, cams=cams, points=3000)
+    monkeypatch.setenv("G2OC_TEST_BARRIER_EXTRA", "1")
+    bad = backend.CudaProblem(g)
+    monkeypatch.delenv("G2OC_TEST_BARRIER_EXTRA")
+    with pytest.raises(backend.G2ocError) as ei:
+        bad.optimize(1)
+    assert ei.value.status == G2OC_ERR_TIMEOUT
+    bad.close()
+    good = backend.CudaProblem(g)
+    done, st = good.optimize(2)
+    good.close()
+    assert done == 2 and st[-1]["chi2"] < st[0]["chi2"] * 10
+
+
 def test_not_positive_definite_is_reported(backend):
     offs = np.array([0, 3, 6], np.int32)
     rc = np.array([[0, 0], [0, 1], [1, 1]], np.int32)
