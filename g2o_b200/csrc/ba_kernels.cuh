@@ -514,8 +514,9 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
 // odd, so the loads are float4 where the alignment allows. FP64 blocks (144
 // bytes) are nine 16-byte words split 5 / 4. Every value is loaded by exactly
 // one lane and the other lane's slot holds 0, so the exchange is an exact
-// add of zero. Both lanes must call it with the same block (warp-uniform
-// control over the pair).
+// add of zero. Both lanes of the pair call it together with the same block;
+// the exchange names only those two lanes (other lane pairs of the warp may
+// have left their pair loops already).
 __device__ __forceinline__ void load_block_pair(const float* hpl, int blk, int half, float (&b)[18]) {
   const float* base = hpl + (size_t)blk * 18;
 #pragma unroll
@@ -551,8 +552,9 @@ __device__ __forceinline__ void load_block_pair(const float* hpl, int blk, int h
       b[14] = v.x; b[15] = v.y; b[16] = v.z; b[17] = v.w;
     }
   }
+  const unsigned pair_mask = 3u << (threadIdx.x & 30);
 #pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(0xffffffffu, b[t], 1);
+  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(pair_mask, b[t], 1);
 }
 
 __device__ __forceinline__ void load_block_pair(const double* hpl, int blk, int half, double (&b)[18]) {
@@ -566,8 +568,9 @@ __device__ __forceinline__ void load_block_pair(const double* hpl, int blk, int 
       b[2 * q] = v.x;
       b[2 * q + 1] = v.y;
     }
+  const unsigned pair_mask = 3u << (threadIdx.x & 30);
 #pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(0xffffffffu, b[t], 1);
+  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(pair_mask, b[t], 1);
 }
 
 // Dense output of the Schur rows for batched windows: each camera row belongs

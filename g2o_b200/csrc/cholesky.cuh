@@ -35,9 +35,15 @@ struct CholPlan {
   std::vector<int> bwd_ptr, bwd;     // per k: tiles i < k with L(k,i) != 0
   DBuf<int> d_perm, d_pnl, d_bwd;
   DBuf<int2> d_upd;
+  DBuf<int> d_pnl_ptr, d_upd_ptr, d_bwd_ptr;
   DBuf<double> A, y;
   DBuf<int> info;
+  // every step has at most kCholSingleWidth panel tiles plus trailing
+  // updates: the whole plan runs in one CTA (chol_factor_single)
+  bool single = false;
 };
+
+constexpr int kCholSingleWidth = 24;
 
 // reverse Cuthill-McKee on the block graph
 static void rcm_order(int nb, const std::vector<int32_t>& rc, std::vector<int>& perm) {
@@ -138,6 +144,13 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
       if (nz[(size_t)k * nt + i]) P.bwd.push_back(i);
     P.bwd_ptr[k + 1] = (int)P.bwd.size();
   }
+  int width = 0;
+  for (int k = 0; k < nt; ++k)
+    width = std::max(width, P.pnl_ptr[k + 1] - P.pnl_ptr[k] + P.upd_ptr[k + 1] - P.upd_ptr[k]);
+  P.single = width <= kCholSingleWidth;
+  G2OC_TRY(P.d_pnl_ptr.upload(P.pnl_ptr, st));
+  G2OC_TRY(P.d_upd_ptr.upload(P.upd_ptr, st));
+  G2OC_TRY(P.d_bwd_ptr.upload(P.bwd_ptr, st));
   G2OC_TRY(P.d_perm.upload(P.perm, st));
   G2OC_TRY(P.d_pnl.upload(P.pnl.empty() ? std::vector<int>{0} : P.pnl, st));
   G2OC_TRY(P.d_upd.upload(P.upd.empty() ? std::vector<int2>{make_int2(0, 0)} : P.upd, st));
@@ -173,9 +186,9 @@ __global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int
   }
 }
 
-// factor the diagonal tile k in shared memory (lower)
-static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
-  __shared__ double T[kTile][kTile + 1];
+// factor the diagonal tile k in shared memory (lower); T: kTile x (kTile+1)
+// doubles of shared memory
+__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double (*T)[kTile + 1], int* info) {
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
@@ -205,14 +218,16 @@ static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int 
   }
 }
 
+static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
+  __shared__ double T[kTile][kTile + 1];
+  chol_potrf_tile(A, np, k, T, info);
+}
+
 // panel: L(i,k) = A(i,k) L(k,k)^-T for the listed tiles i
 constexpr int kTileSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
 
-static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
-  extern __shared__ double sm_trsm[];
-  double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
-  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
-  const int ti = tiles[blockIdx.x];
+__device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti, double (*L)[kTile + 1],
+                                               double (*X)[kTile + 1]) {
   const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
@@ -220,9 +235,9 @@ static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k
     X[r][c] = A[(kb + c) * np + ib + r];
   }
   __syncthreads();
-  // each of 4 thread groups handles 16 rows; within a row the columns are sequential
+  // each row's columns in sequence; rows in parallel
   const int row = threadIdx.x % kTile;
-  const int grp = threadIdx.x / kTile;  // 0..3
+  const int grp = threadIdx.x / kTile;
   if (grp == 0) {
     for (int c = 0; c < kTile; ++c) {
       double v = X[row][c];
@@ -237,12 +252,16 @@ static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k
   }
 }
 
-// trailing update: A(i,j) -= L(i,k) L(j,k)^T for the listed pairs; 4x4 per thread
-static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
-  extern __shared__ double sm_gemm[];
-  double (*Li)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm);
-  double (*Lj)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm + kTile * (kTile + 1));
-  const int2 ij = pairs[blockIdx.x];
+static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
+  extern __shared__ double sm_trsm[];
+  double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
+  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
+  chol_trsm_tile(A, np, k, tiles[blockIdx.x], L, X);
+}
+
+// trailing update: A(i,j) -= L(i,k) L(j,k)^T; 4x4 per thread (256 threads)
+__device__ __forceinline__ void chol_gemm_tile(double* A, int np, int k, int2 ij, double (*Li)[kTile + 1],
+                                               double (*Lj)[kTile + 1]) {
   const size_t kb = (size_t)k * kTile, ib = (size_t)ij.x * kTile, jb = (size_t)ij.y * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
@@ -277,6 +296,40 @@ static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k
       if (diag && r < c) continue;
       A[(jb + c) * np + ib + r] -= acc[a][b];
     }
+}
+
+static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
+  extern __shared__ double sm_gemm[];
+  double (*Li)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm);
+  double (*Lj)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm + kTile * (kTile + 1));
+  chol_gemm_tile(A, np, k, pairs[blockIdx.x], Li, Lj);
+}
+
+// The whole factorization in one CTA of 256 threads, for plans whose steps
+// are narrow (the pose graphs after reverse Cuthill-McKee: a banded tile
+// pattern, a few panel tiles and trailing updates per step). The
+// multi-launch form spends such a plan in the launch latency of its n / 64
+// strictly sequential steps; here the steps run back to back with the same
+// tile algorithms (same arithmetic, same order), the tiles passing through
+// shared memory and the factor staying in the dense buffer.
+static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int np, int nt, const int* pnl_ptr,
+                                                                 const int* pnl, const int* upd_ptr,
+                                                                 const int2* upd, int* info) {
+  extern __shared__ double sm_single[];
+  double (*B0)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single);
+  double (*B1)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single + kTile * (kTile + 1));
+  for (int k = 0; k < nt; ++k) {
+    chol_potrf_tile(A, np, k, B0, info);
+    __syncthreads();
+    for (int p = pnl_ptr[k]; p < pnl_ptr[k + 1]; ++p) {
+      chol_trsm_tile(A, np, k, pnl[p], B0, B1);
+      __syncthreads();
+    }
+    for (int p = upd_ptr[k]; p < upd_ptr[k + 1]; ++p) {
+      chol_gemm_tile(A, np, k, upd[p], B0, B1);
+      __syncthreads();
+    }
+  }
 }
 
 // permuted right-hand side y(perm) = b
@@ -355,6 +408,101 @@ static __global__ void chol_bwd_update(const double* A, int np, int k, const int
   }
 }
 
+// Both substitutions of a single-CTA plan in one CTA of 256 threads: per
+// diagonal tile, warp 0 solves the 64 x 64 triangle from shared memory with
+// shuffles (lane l holds rows l and l + 32; a column's pivot division by its
+// owner, then the update of the rows below in column order, as
+// chol_fwd_diag), then the tiles the step updates take their products in
+// parallel (four tiles at a time, one thread per row or column).
+static __global__ void __launch_bounds__(256) chol_solve_single(const double* A, int np, int nt, const int* pnl_ptr,
+                                                                const int* pnl, const int* bwd_ptr, const int* bwd,
+                                                                double* y) {
+  __shared__ double L[kTile][kTile + 1];
+  __shared__ double v[kTile];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < nt; ++k) {
+    const size_t kb = (size_t)k * kTile;
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int r = e % kTile, c = e / kTile;
+      L[r][c] = r >= c ? A[(kb + c) * np + kb + r] : 0.0;
+    }
+    if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+    __syncthreads();
+    if (warp == 0) {
+      double a0 = v[lane], a1 = v[lane + 32];
+      for (int t = 0; t < kTile; ++t) {
+        const bool lo = t < 32;
+        const int owner = t & 31;
+        double mine = lo ? a0 : a1;
+        if (lane == owner) mine = mine / L[t][t];
+        const double xt = __shfl_sync(0xffffffffu, mine, owner);
+        if (lane == owner) {
+          if (lo) a0 = xt;
+          else a1 = xt;
+        }
+        if (lane > t) a0 -= L[lane][t] * xt;
+        if (lane + 32 > t) a1 -= L[lane + 32][t] * xt;
+      }
+      v[lane] = a0;
+      v[lane + 32] = a1;
+    }
+    __syncthreads();
+    if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+    const int np_k = pnl_ptr[k + 1] - pnl_ptr[k];
+    for (int q0 = 0; q0 < np_k; q0 += 4) {
+      const int q = q0 + (int)threadIdx.x / kTile, r = threadIdx.x % kTile;
+      if (q < np_k) {
+        const size_t ib = (size_t)pnl[pnl_ptr[k] + q] * kTile;
+        double s = 0.0;
+        for (int t = 0; t < kTile; ++t) s += A[(kb + t) * np + ib + r] * v[t];
+        y[ib + r] -= s;
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = nt - 1; k >= 0; --k) {
+    const size_t kb = (size_t)k * kTile;
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int r = e % kTile, c = e / kTile;
+      L[r][c] = r >= c ? A[(kb + c) * np + kb + r] : 0.0;
+    }
+    if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+    __syncthreads();
+    if (warp == 0) {
+      // L^T x = v: column t of L^T is row t of L, the rows above t in turn
+      double a0 = v[lane], a1 = v[lane + 32];
+      for (int t = kTile - 1; t >= 0; --t) {
+        const bool lo = t < 32;
+        const int owner = t & 31;
+        double mine = lo ? a0 : a1;
+        if (lane == owner) mine = mine / L[t][t];
+        const double xt = __shfl_sync(0xffffffffu, mine, owner);
+        if (lane == owner) {
+          if (lo) a0 = xt;
+          else a1 = xt;
+        }
+        if (lane < t) a0 -= L[t][lane] * xt;
+        if (lane + 32 < t) a1 -= L[t][lane + 32] * xt;
+      }
+      v[lane] = a0;
+      v[lane + 32] = a1;
+    }
+    __syncthreads();
+    if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+    const int nb_k = bwd_ptr[k + 1] - bwd_ptr[k];
+    for (int q0 = 0; q0 < nb_k; q0 += 4) {
+      const int q = q0 + (int)threadIdx.x / kTile, c = threadIdx.x % kTile;
+      if (q < nb_k) {
+        const size_t ib = (size_t)bwd[bwd_ptr[k] + q] * kTile;
+        double s = 0.0;
+        for (int t = 0; t < kTile; ++t) s += A[(ib + c) * np + kb + t] * v[t];
+        y[ib + c] -= s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // densify and factor: P.A holds L (lower tiles of the pattern), P.info the pivot flag
 template <typename Real>
 static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long long* nl) {
@@ -366,7 +514,13 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
   G2OC_CUDA_TRY(cudaMemsetAsync(P.info.p, 0, sizeof(int), st));
   const long long work = (long long)nnzb * P.bs * P.bs + (np - P.n);
   chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.bs, P.d_perm.p, P.n, np, P.A.p);
-  for (int k = 0; k < nt; ++k) {
+  if (P.single) {
+    G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_factor_single, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    chol_factor_single<<<1, 256, kTileSmem, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p, P.d_upd.p,
+                                                  P.info.p);
+    *nl += 1;
+  }
+  for (int k = 0; k < (P.single ? 0 : nt); ++k) {
     chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.info.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k]);
@@ -388,13 +542,17 @@ static int chol_resolve(CholPlan& P, cudaStream_t st, const double* rhs, double*
   long long nl = 2;  // load_rhs, store_x
   const int np = P.np, nt = P.nt;
   chol_load_rhs<<<(np + 255) / 256, 256, 0, st>>>(rhs, P.d_perm.p, P.nb, P.bs, P.n, np, P.y.p);
-  for (int k = 0; k < nt; ++k) {
+  if (P.single) {
+    chol_solve_single<<<1, 256, 0, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_bwd_ptr.p, P.d_bwd.p, P.y.p);
+    nl += 1;
+  }
+  for (int k = 0; k < (P.single ? 0 : nt); ++k) {
     chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_fwd_update<<<np_k, kTile, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
     nl += 1 + (np_k > 0);
   }
-  for (int k = nt - 1; k >= 0; --k) {
+  for (int k = (P.single ? -1 : nt - 1); k >= 0; --k) {
     chol_bwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
     const int nbk = P.bwd_ptr[k + 1] - P.bwd_ptr[k];
     if (nbk > 0) chol_bwd_update<<<nbk, kTile, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
