@@ -23,11 +23,14 @@
 // updates of the other tiles, forward and backward. The caller refines the
 // solution on its true FP64 residual.
 //
-// Shared-memory operand layout (no swizzle, MN-major canonical form of the
+// Shared-memory operand layout (no swizzle, K-major canonical form of the
 // UMMA descriptor): element (i, j) of a 128 (M or N) x 64 (K) FP32 tile at
-// byte (i % 4) * 4 + (j % 8) * 16 + (i / 4) * 128 + (j / 8) * 4096: core
-// matrices of 4 MN x 8 K (128 bytes), MN groups 128 bytes apart (stride byte
-// offset), K groups 4096 bytes apart (leading byte offset).
+// byte (i % 8) * 16 + (j % 4) * 4 + (i / 8) * 128 + (j / 4) * 2048: core
+// matrices of 8 rows x 4 K values (16 bytes per row, 128 bytes), row groups
+// 128 bytes apart (stride byte offset), K groups 2048 bytes apart (leading
+// byte offset); one MMA (K = 8) spans two K groups. (The MN-major form of
+// the descriptor gave a zero product for kind::tf32 on this hardware, so the
+// operands are transposed into K-major order while they are staged.)
 #pragma once
 
 #include <cstdint>
@@ -63,10 +66,10 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
   return d;
 }
 
-// instruction descriptor: kind::tf32, D in FP32, A and B TF32, both MN-major,
+// instruction descriptor: kind::tf32, D in FP32, A and B TF32, both K-major,
 // N = 128 (bits 17-22: N >> 3), M = 128 (bits 24-28: M >> 4)
-constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
-                              ((uint32_t)(kTc >> 3) << 17) | ((uint32_t)(kTc >> 4) << 24);
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTc >> 3) << 17) |
+                              ((uint32_t)(kTc >> 4) << 24);
 
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
   asm volatile(
@@ -114,27 +117,26 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // stage a 128 (MN) x 64 (K) FP32 sub-tile of a column-major matrix (column
-// j of the sub-tile at G + j * ld, 16-byte aligned) as hi / lo TF32 parts.
-// Warp w writes 512 contiguous bytes (four MN groups x eight K columns) and
-// reads four 64-byte runs of each of eight columns.
+// j of the sub-tile at G + j * ld, 16-byte aligned) as hi / lo TF32 parts in
+// the K-major layout above. Each thread reads four consecutive rows of one
+// column (a warp: four 64-byte runs of each of eight columns) and writes
+// them to the four rows' K slots.
 __device__ __forceinline__ void tc_stage(const float* G, size_t ld, unsigned char* hi, unsigned char* lo) {
   for (int q = threadIdx.x; q < kTc * kTcK / 4; q += blockDim.x) {
     const int lane = q & 31, w = q >> 5;
     const int j = (w & 7) * 8 + (lane & 7);
     const int g = (w >> 3) * 4 + (lane >> 3);
     const float4 v = *reinterpret_cast<const float4*>(G + (size_t)j * ld + g * 4);
-    float4 h, l;
-    h.x = tc_tf32(v.x);
-    h.y = tc_tf32(v.y);
-    h.z = tc_tf32(v.z);
-    h.w = tc_tf32(v.w);
-    l.x = tc_tf32(v.x - h.x);
-    l.y = tc_tf32(v.y - h.y);
-    l.z = tc_tf32(v.z - h.z);
-    l.w = tc_tf32(v.w - h.w);
-    const uint32_t off = (uint32_t)g * 128 + (uint32_t)(j & 7) * 16 + (uint32_t)(j >> 3) * 4096;
-    *reinterpret_cast<float4*>(hi + off) = h;
-    *reinterpret_cast<float4*>(lo + off) = l;
+    const float x[4] = {v.x, v.y, v.z, v.w};
+    const uint32_t kofs = (uint32_t)(j & 3) * 4 + (uint32_t)(j >> 2) * 2048;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = g * 4 + c;
+      const uint32_t off = (uint32_t)(i & 7) * 16 + (uint32_t)(i >> 3) * 128 + kofs;
+      const float h = tc_tf32(x[c]);
+      *reinterpret_cast<float*>(hi + off) = h;
+      *reinterpret_cast<float*>(lo + off) = tc_tf32(x[c] - h);
+    }
   }
 }
 
@@ -190,9 +192,9 @@ static __global__ void __launch_bounds__(128, 1)
 #pragma unroll
       for (int kg = 0; kg < kTcK / 8; ++kg) {
         const uint32_t o = (uint32_t)kg * 4096;
-        tc_mma(tmem, tc_desc(ah + o, 4096, 128), tc_desc(bh + o, 4096, 128), (ch > 0 || kg > 0) ? 1u : 0u);
-        tc_mma(tmem, tc_desc(ah + o, 4096, 128), tc_desc(bl + o, 4096, 128), 1u);
-        tc_mma(tmem, tc_desc(al + o, 4096, 128), tc_desc(bh + o, 4096, 128), 1u);
+        tc_mma(tmem, tc_desc(ah + o, 2048, 128), tc_desc(bh + o, 2048, 128), (ch > 0 || kg > 0) ? 1u : 0u);
+        tc_mma(tmem, tc_desc(ah + o, 2048, 128), tc_desc(bl + o, 2048, 128), 1u);
+        tc_mma(tmem, tc_desc(al + o, 2048, 128), tc_desc(bh + o, 2048, 128), 1u);
       }
       tc_commit(mb);
     }

@@ -30,6 +30,85 @@ SEED_BASE = 20261203
 
 
 # ------------------------------------------------------------------ helpers
+# sin / cos from +, -, *, / and rint only. Each of those is one IEEE-754
+# operation with a correctly rounded result, so the generated graphs are the
+# same bits on every CPU; numpy's own float64 sin / cos dispatch to SIMD
+# kernels chosen by the CPU's features, whose last bits differ between
+# machines (and a last-bit change can flip a visibility decision of the BA
+# generator). Range reduction by a two-part pi/2, then the Taylor series to
+# r^17 on |r| <= pi/4 (truncation error below 1e-16).
+_HALF_PI_HI = 1.5707963267948966
+_HALF_PI_LO = 6.123233995736766e-17
+_SIN_C = [(-1.0) ** k / math.factorial(2 * k + 1) for k in range(9)]
+_COS_C = [(-1.0) ** k / math.factorial(2 * k) for k in range(10)]
+
+
+def _sincos(x):
+    x = np.asarray(x, dtype=np.float64)
+    k = np.rint(x / _HALF_PI_HI)
+    r = (x - k * _HALF_PI_HI) - k * _HALF_PI_LO
+    r2 = r * r
+    s = np.full_like(r, _SIN_C[-1])
+    for c in reversed(_SIN_C[:-1]):
+        s = s * r2 + c
+    s = s * r
+    c_ = np.full_like(r, _COS_C[-1])
+    for c in reversed(_COS_C[:-1]):
+        c_ = c_ * r2 + c
+    q = np.mod(k, 4.0)
+    sin = np.where(q == 0, s, np.where(q == 1, c_, np.where(q == 2, -s, -c_)))
+    cos = np.where(q == 0, c_, np.where(q == 1, -s, np.where(q == 2, -c_, s)))
+    return sin, cos
+
+
+def _sin(x):
+    return _sincos(x)[0]
+
+
+def _cos(x):
+    return _sincos(x)[1]
+
+
+def _geometric(rng, p, size, kmax):
+    """Geometric draws P(K = k) = (1 - p)^(k - 1) p, truncated at kmax: one
+    uniform draw compared with the tails P(K > j) = (1 - p)^j, formed by
+    products only (the same bits on every CPU)."""
+    u = rng.random(size)
+    k = np.ones(size, dtype=np.int64)
+    q = 1.0
+    for _ in range(1, kmax):
+        q = q * (1.0 - p)
+        k += (u < q)
+    return k
+
+# small-matrix products and norms written out elementwise, in a fixed order
+# (numpy's matmul / einsum / norm pick BLAS or SIMD kernels by CPU)
+def _mm(A, B):
+    """(..., 3, 3) x (..., 3, 3)"""
+    return np.stack([np.stack([(A[..., i, 0] * B[..., 0, j] + A[..., i, 1] * B[..., 1, j]) + A[..., i, 2] * B[..., 2, j]
+                               for j in range(3)], -1) for i in range(3)], -2)
+
+
+def _mv(A, v):
+    """(..., 3, 3) x (..., 3)"""
+    return np.stack([(A[..., i, 0] * v[..., 0] + A[..., i, 1] * v[..., 1]) + A[..., i, 2] * v[..., 2]
+                     for i in range(3)], -1)
+
+
+def _mtv(A, v):
+    """(..., 3, 3)^T x (..., 3)"""
+    return np.stack([(A[..., 0, i] * v[..., 0] + A[..., 1, i] * v[..., 1]) + A[..., 2, i] * v[..., 2]
+                     for i in range(3)], -1)
+
+
+def _norm(v):
+    """Euclidean norm over the last axis (3 or 4 entries)."""
+    acc = v[..., 0] * v[..., 0]
+    for i in range(1, v.shape[-1]):
+        acc = acc + v[..., i] * v[..., i]
+    return np.sqrt(acc)
+
+
 def _wrap(a):
     return (a + np.pi) % (2 * np.pi) - np.pi
 
@@ -47,7 +126,7 @@ def _rot_to_quat(R):
     y = np.copysign(y, R[..., 0, 2] - R[..., 2, 0])
     z = np.copysign(z, R[..., 1, 0] - R[..., 0, 1])
     q[..., 0], q[..., 1], q[..., 2], q[..., 3] = x, y, z, w
-    q /= np.linalg.norm(q, axis=-1, keepdims=True)
+    q /= _norm(q)[..., None]
     return q
 
 
@@ -69,21 +148,21 @@ def _quat_to_rot(q):
 def _axis_angle(v):
     """Rodrigues: rotation vectors (..., 3) -> matrices."""
     v = np.asarray(v, dtype=np.float64)
-    th = np.linalg.norm(v, axis=-1)[..., None, None]
+    th = _norm(v)[..., None, None]
     K = np.zeros(v.shape[:-1] + (3, 3))
     K[..., 0, 1], K[..., 0, 2] = -v[..., 2], v[..., 1]
     K[..., 1, 0], K[..., 1, 2] = v[..., 2], -v[..., 0]
     K[..., 2, 0], K[..., 2, 1] = -v[..., 1], v[..., 0]
     with np.errstate(invalid="ignore", divide="ignore"):
-        a = np.where(th > 1e-12, np.sin(th) / th, 1.0)
-        b = np.where(th > 1e-12, (1 - np.cos(th)) / (th * th), 0.5)
-    return np.eye(3) + a * K + b * (K @ K)
+        a = np.where(th > 1e-12, _sin(th) / th, 1.0)
+        b = np.where(th > 1e-12, (1 - _cos(th)) / (th * th), 0.5)
+    return np.eye(3) + a * K + b * _mm(K, K)
 
 
 def _compact_quat_noise(rng, n, sigma):
     """Rotation matrices from a quaternion whose vector part is N(0, sigma)."""
     qv = rng.normal(0.0, sigma, size=(n, 3))
-    w = np.sqrt(np.maximum(1.0 - np.sum(qv * qv, axis=1), 0.0))
+    w = np.sqrt(np.maximum(1.0 - _norm(qv) ** 2, 0.0))
     return _quat_to_rot(np.concatenate([qv, w[:, None]], axis=1))
 
 
@@ -125,7 +204,7 @@ def pose_graph_2d(num_poses=3500, num_closures=2000, seed=SEED_BASE + 0):
     # true relative poses Xi^-1 Xj
     i, j = pairs[:, 0], pairs[:, 1]
     d = pos[j] - pos[i]
-    c, s = np.cos(th[i]), np.sin(th[i])
+    c, s = _cos(th[i]), _sin(th[i])
     rel = np.stack([c * d[:, 0] + s * d[:, 1], -s * d[:, 0] + c * d[:, 1], _wrap(th[j] - th[i])], 1)
     sig = np.array([0.05, 0.05, 0.01])
     meas = rel + rng.normal(0.0, 1.0, size=rel.shape) * sig
@@ -158,8 +237,8 @@ def pose_graph_3d(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
         for j in range(per_ring):
             az = 2 * np.pi * j / per_ring
             idx = k * per_ring + j
-            t[idx] = radius * np.array([np.sin(pol) * np.cos(az), np.sin(pol) * np.sin(az), np.cos(pol)])
-            R[idx] = _axis_angle(np.array([0.0, 0.0, az + np.pi / 2])) @ _axis_angle(np.array([pol - np.pi / 2, 0, 0]))
+            t[idx] = radius * np.array([_sin(pol) * _cos(az), _sin(pol) * _sin(az), _cos(pol)])
+            R[idx] = _mm(_axis_angle(np.array([0.0, 0.0, az + np.pi / 2])), _axis_angle(np.array([pol - np.pi / 2, 0, 0])))
     edges = []
     for k in range(num_rings):
         base = k * per_ring
@@ -175,18 +254,18 @@ def pose_graph_3d(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
         a, b = k * per_ring, (k + 1) * per_ring
         nxt = t[b:b + per_ring]
         for j in range(per_ring):
-            jj = int(np.argmin(np.linalg.norm(nxt - t[a + j], axis=1)))
+            jj = int(np.argmin(_norm(nxt - t[a + j])))
             edges.append((a + j, b + jj))
     edges = np.array(edges, dtype=np.int64)
     i, j = edges[:, 0], edges[:, 1]
     Rt = np.transpose(R[i], (0, 2, 1))
-    relR = Rt @ R[j]
-    relt = np.einsum("nab,nb->na", Rt, t[j] - t[i])
+    relR = _mm(Rt, R[j])
+    relt = _mv(Rt, t[j] - t[i])
     sig_t, sig_r = 0.01, 0.005
     nR = _compact_quat_noise(rng, len(edges), sig_r)
     nt = rng.normal(0.0, sig_t, size=(len(edges), 3))
-    mR = relR @ nR
-    mt = relt + np.einsum("nab,nb->na", relR, nt)
+    mR = _mm(relR, nR)
+    mt = relt + _mv(relR, nt)
     meas = _iso12(mR, mt)
     info = np.tile(np.diag([1 / sig_t ** 2] * 3 + [1 / (sig_r ** 2)] * 3).reshape(1, 36), (len(edges), 1))
     # initial guess: compose the noisy chain
@@ -195,8 +274,8 @@ def pose_graph_3d(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE + 1):
     eR[0], et[0] = R[0], t[0]
     for k in range(odo):
         a, b = edges[k]
-        eR[b] = eR[a] @ mR[k]
-        et[b] = et[a] + eR[a] @ mt[k]
+        eR[b] = _mm(eR[a], mR[k])
+        et[b] = et[a] + _mv(eR[a], mt[k])
     fixed = np.zeros(n, np.uint8)
     fixed[0] = 1
     g = Graph(POSE_SE3, EDGE_SE3, _iso12(eR, et), edges.astype(np.int32), meas, info, pose_fixed=fixed,
@@ -216,7 +295,7 @@ def pose_graph_3d_expmap(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE
         R = iso[:, :9].reshape(-1, 3, 3)
         t = iso[:, 9:]
         Rt = np.transpose(R, (0, 2, 1))
-        return np.concatenate([-np.einsum("nab,nb->na", Rt, t), _rot_to_quat(Rt)], axis=1)
+        return np.concatenate([-_mv(Rt, t), _rot_to_quat(Rt)], axis=1)
 
     perm = [3, 4, 5, 0, 1, 2]
     info = g.information.reshape(-1, 6, 6)[:, perm][:, :, perm].reshape(-1, 36)
@@ -230,13 +309,13 @@ def pose_graph_3d_expmap(num_rings=10, per_ring=250, radius=50.0, seed=SEED_BASE
 # ------------------------------------------------------ bundle adjustment
 def _look_at(centers, target):
     fwd = target[None, :] - centers
-    fwd /= np.linalg.norm(fwd, axis=1, keepdims=True)
+    fwd /= _norm(fwd)[:, None]
     up = np.array([0.0, 0.0, 1.0])
     x = np.cross(fwd, up)
-    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    x /= _norm(x)[:, None]
     y = np.cross(fwd, x)
     Rcw = np.stack([x, y, fwd], axis=1)  # rows: camera axes in world
-    tcw = -np.einsum("nab,nb->na", Rcw, centers)
+    tcw = -_mv(Rcw, centers)
     return Rcw, tcw
 
 
@@ -251,17 +330,18 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     fy = focal if focal_y is None else focal_y
     rng = np.random.default_rng(seed)
     az = 2 * np.pi * np.arange(num_cameras) / num_cameras
-    centers = np.stack([ring_radius * np.cos(az), ring_radius * np.sin(az), np.full(num_cameras, height)], 1)
+    centers = np.stack([ring_radius * _cos(az), ring_radius * _sin(az), np.full(num_cameras, height)], 1)
     Rcw, tcw = _look_at(centers, np.array([0.0, 0.0, box[2] / 2]))
     X = np.stack([rng.uniform(-box[0], box[0], num_points), rng.uniform(-box[1], box[1], num_points),
                   rng.uniform(0.0, box[2], num_points)], 1)
     cx, cy = width / 2.0, height_px / 2.0
-    kdraw = np.clip(rng.geometric(1.0 / mean_obs, size=num_points), min_obs, max_obs)
+    kdraw = np.clip(_geometric(rng, 1.0 / mean_obs, num_points, max_obs), min_obs, max_obs)
     pts, cams, uvs = [], [], []
-    Rm = np.ascontiguousarray(Rcw.reshape(num_cameras * 3, 3).T)
     for s in range(0, num_points, chunk):
         Xs = X[s:s + chunk]
-        Xc = (Xs @ Rm).reshape(Xs.shape[0], num_cameras, 3) + tcw[None, :, :]
+        # camera coordinates of every point of the chunk in every camera
+        Xc = np.stack([((Xs[:, None, 0] * Rcw[None, :, i, 0] + Xs[:, None, 1] * Rcw[None, :, i, 1])
+                        + Xs[:, None, 2] * Rcw[None, :, i, 2]) + tcw[None, :, i] for i in range(3)], -1)
         z = Xc[..., 2]
         with np.errstate(divide="ignore", invalid="ignore"):
             u = focal * Xc[..., 0] / z + cx
@@ -297,8 +377,8 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     # initial guess
     dR = _axis_angle(rng.normal(0.0, pose_noise[1], size=(num_cameras, 3)))
     dt = rng.normal(0.0, pose_noise[0], size=(num_cameras, 3))
-    R0 = dR @ Rcw
-    t0 = np.einsum("nab,nb->na", dR, tcw) + dt
+    R0 = _mm(dR, Rcw)
+    t0 = _mv(dR, tcw) + dt
     fixed = np.zeros(num_cameras, np.uint8)
     fixed[:num_fixed] = 1
     R0[:num_fixed], t0[:num_fixed] = Rcw[:num_fixed], tcw[:num_fixed]
@@ -354,7 +434,7 @@ def camera_centres(pose_est):
     t = pose_est[:, :3]
     q = pose_est[:, 3:7]  # x y z w
     R = _quat_to_rot(q)
-    return -np.einsum("nba,nb->na", R, t), R
+    return -_mtv(R, t), R
 
 
 def centre_loss(pose_est, truth_pose):
@@ -365,7 +445,7 @@ def centre_loss(pose_est, truth_pose):
     ct, _ = camera_centres(truth_pose)
     d = c - ct
     grad = np.zeros((len(pose_est), 6))
-    grad[:, 3:] = -2.0 * np.einsum("nab,nb->na", R, d)
+    grad[:, 3:] = -2.0 * _mv(R, d)
     return float((d * d).sum()), grad
 
 
