@@ -875,15 +875,17 @@ __global__ void __launch_bounds__(THREADS, 1)
     schur_rows_staged(const int* units, const int* hc_ptr, const int* hc_blk, const int* hc_col, const float* hpl,
                       const float* dinv, const int* rptr, const int* rcol, const int* pair_ptr, const int32_t* stage,
                       const int32_t* pairs16, const int* s_hpp, const float* hpp, double lambda, float* S,
-                      float* tiles, const int* tile_off, int bd_floats, int chunk, const double* b_p,
-                      const double* b_l, double* bs) {
+                      float* tiles, const int* tile_off, int bd_floats, int pairs_cap, int chunk,
+                      const double* b_p, const double* b_l, double* bs) {
   constexpr int TS = kTileBlocks * 6;
   constexpr int NP = THREADS / 2;  // lane pairs
+  constexpr int STAGE_ILP = 8;     // staged words in flight per thread
   static_assert(NP * NQ == kStagedUnitBlocks, "a unit's blocks are the lane pairs' blocks");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[THREADS / 32][27];
   float* BDs = reinterpret_cast<float*>(smem_raw);
-  float* Us = BDs + bd_floats;
+  int32_t* Ps = reinterpret_cast<int32_t*>(BDs + bd_floats);  // the unit's pair entries
+  float* Us = reinterpret_cast<float*>(Ps + pairs_cap);
   const int* U = units + 5 * (size_t)blockIdx.x;
   const int r = U[0], j0 = U[1], j1 = U[2], ubase = U[3], nu = U[4];
   const bool first = j0 == 1;
@@ -973,34 +975,50 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
   // ---- phase 2: off-diagonal blocks from staged operands
   const int lp = threadIdx.x >> 1, half = threadIdx.x & 1;
+  // the unit's pair entries (its blocks' lists, contiguous) into shared memory
+  const int pbase = pair_ptr[rb + j0];
+  for (int i = threadIdx.x; i < nu; i += THREADS) Ps[i] = __ldg(pairs16 + pbase + i);
   float acc[NQ][18];
   int p[NQ], pe[NQ];
-  int32_t cur[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
 #pragma unroll
     for (int t = 0; t < 18; ++t) acc[q][t] = 0.0f;
     const int j = j0 + lp + q * NP;
-    p[q] = j < j1 ? pair_ptr[rb + j] : 0;
-    pe[q] = j < j1 ? pair_ptr[rb + j + 1] : 0;
-    cur[q] = p[q] < pe[q] ? pairs16[p[q]] : 0;
+    p[q] = j < j1 ? pair_ptr[rb + j] - pbase : 0;
+    pe[q] = j < j1 ? pair_ptr[rb + j + 1] - pbase : 0;
   }
+  const float2* hpl2 = reinterpret_cast<const float2*>(hpl);
   for (int u0 = 0; u0 < nu; u0 += chunk) {
     const int u1 = min(u0 + chunk, nu);
-    __syncthreads();  // the previous chunk's readers (and phase 1's BD writers) are done
+    __syncthreads();  // the previous chunk's readers (and phase 1's BD, the pair entries) are done
     const int words = (u1 - u0) * 9;
-    for (int w = threadIdx.x; w < words; w += THREADS) {
-      const int bl = w / 9, t = w - bl * 9;
-      const int b = __ldg(stage + ubase + u0 + bl);
-      reinterpret_cast<float2*>(Us)[w] = __ldg(reinterpret_cast<const float2*>(hpl + (size_t)b * 18) + t);
+    for (int w0 = threadIdx.x; w0 < words; w0 += THREADS * STAGE_ILP) {
+      int bidx[STAGE_ILP];
+      float2 val[STAGE_ILP];
+#pragma unroll
+      for (int t = 0; t < STAGE_ILP; ++t) {
+        const int w = w0 + t * THREADS;
+        bidx[t] = w < words ? __ldg(stage + ubase + u0 + w / 9) : 0;
+      }
+#pragma unroll
+      for (int t = 0; t < STAGE_ILP; ++t) {
+        const int w = w0 + t * THREADS;
+        if (w < words) val[t] = __ldg(hpl2 + (size_t)bidx[t] * 9 + (w % 9));
+      }
+#pragma unroll
+      for (int t = 0; t < STAGE_ILP; ++t) {
+        const int w = w0 + t * THREADS;
+        if (w < words) reinterpret_cast<float2*>(Us)[w] = val[t];
+      }
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
-      while (p[q] < pe[q] && (cur[q] & 0xFFFF) < u1) {
-        const int a = cur[q] >> 16, ub = (cur[q] & 0xFFFF) - u0;
+      while (p[q] < pe[q] && (Ps[p[q]] & 0xFFFF) < u1) {
+        const int32_t cur = Ps[p[q]];
+        const int a = cur >> 16, ub = (cur & 0xFFFF) - u0;
         ++p[q];
-        cur[q] = p[q] < pe[q] ? __ldg(pairs16 + p[q]) : 0;
         const float* D = BDs + (size_t)a * 18 + half * 9;
         const float2* Bq = reinterpret_cast<const float2*>(Us) + (size_t)ub * 9;
         float d[9];

@@ -479,12 +479,14 @@ static bool schur_staged() {
   return v != 0;
 }
 
-// Schur rows: the two lanes of a block pair share each Hpl block load
-// (G2OC_SCHUR_COOP=0: each lane loads the whole block)
+// Schur rows: each lane of a block pair loads the whole Hpl block (the
+// default: measured faster on the BA configuration, 240 vs 262 us per
+// launch); G2OC_SCHUR_COOP=1 has the two lanes split each load and exchange
+// halves by shuffle
 static bool schur_coop() {
   static const int v = [] {
     const char* e = getenv("G2OC_SCHUR_COOP");
-    return e ? atoi(e) : 1;
+    return e ? atoi(e) : 0;
   }();
   return v != 0;
 }
@@ -683,7 +685,7 @@ struct Engine final : EngineBase {
   // row's BD blocks and of one chunk of staged Hpl blocks
   static constexpr int kStagedThreads = 512, kStagedNQ = 3;
   bool staged = false;
-  int staged_bd_floats = 0, staged_chunk = 0, staged_n = 0;
+  int staged_bd_floats = 0, staged_pairs_cap = 0, staged_chunk = 0, staged_n = 0;
   DBuf<int> staged_units;  // the 2-lane rows' units (5 ints each), largest first
   std::vector<int> two_lane_rows;
   DBuf<Real> hcontrib;
@@ -729,7 +731,11 @@ struct Engine final : EngineBase {
         // its units run largest staged list first
         const long long budget = 227 * 1024 - 8 * 1024;
         staged_bd_floats = ((S.max_blocks_per_cam * 18 + 3) / 4) * 4;
-        const long long left = budget - (long long)staged_bd_floats * 4;
+        staged_pairs_cap = 0;
+        for (size_t u = 0; u < S.s_units.size() / 5; ++u)
+          staged_pairs_cap = std::max(staged_pairs_cap, S.s_units[5 * u + 4]);
+        staged_pairs_cap = (staged_pairs_cap + 3) / 4 * 4;
+        const long long left = budget - (long long)staged_bd_floats * 4 - (long long)staged_pairs_cap * 4;
         staged_chunk = (int)std::min<long long>(4096, left > 0 ? left / 72 : 0);
         staged = sizeof(Real) == 4 && !S.s_pairs16.empty() && staged_chunk >= 256;
         if (staged) {
@@ -958,12 +964,13 @@ struct Engine final : EngineBase {
       return G2OC_ERR_NOT_SUPPORTED;
     } else {
       auto kern = schur_rows_staged<kStagedThreads, kStagedNQ>;
-      const size_t smem = ((size_t)staged_bd_floats + (size_t)staged_chunk * 18) * sizeof(float);
+      const size_t smem = ((size_t)staged_bd_floats + (size_t)staged_pairs_cap + (size_t)staged_chunk * 18) * 4;
       G2OC_TRY(raise_dyn_smem((const void*)kern, smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<staged_n, kStagedThreads, smem, c->stream>>>(
           staged_units.p, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_stage.p, c->s_pairs16.p, c->s_hpp.p, hpp.p, lambda, Sval.p,
-          to_tiles ? tiles.p : nullptr, to_tiles ? c->tile_off.p : nullptr, staged_bd_floats, staged_chunk, bp, bl, bs);
+          to_tiles ? tiles.p : nullptr, to_tiles ? c->tile_off.p : nullptr, staged_bd_floats, staged_pairs_cap,
+          staged_chunk, bp, bl, bs);
       G2OC_LAUNCH_CHECK();
       return G2OC_OK;
     }
