@@ -5,8 +5,10 @@ and against the oracle trajectories committed in tests/golden/oracle_targets.jso
 
 * BA, 1000 cameras / 200,000 points / ~1.03M edges, LM + Schur + PCG, 20
   iterations, FP64: the same number of LM trials in every iteration, robust
-  chi2 within 1e-6 relative per iteration, camera and point estimates within
-  the stated absolute bounds. The mixed forms (FP64 refinement of every step,
+  chi2 within 1e-6 relative per iteration, camera translations within 5e-5 m
+  and quaternions within 5e-5 (cameras on a 30 m ring: 2e-6 relative; both
+  sides solve with PCG to the 1e-6 stopping rule, so each step differs at
+  that level), points within 1e-4 m. The mixed forms (FP64 refinement of every step,
   and FP32 steps under FP64 LM control) reach the oracle's 20-iteration chi2
   within 1e-6 relative.
 * 2D pose graph, 3500 poses, Gauss-Newton + Cholesky, 10 iterations: chi2
@@ -80,8 +82,8 @@ def test_ba_full_size_fp64_matches_oracle(backend, ba_graph, ba_oracle, targets)
         assert rel <= 1e-6, (a["iteration"], a["chi2"], b["chi2"])
     pc, qc = c.estimates()
     c.close()
-    # cameras: rotation (quaternion xyz) and translation; points in metres
-    assert np.abs(pc - po).max() < 1e-5, np.abs(pc - po).max()
+    # cameras: translation (m) and quaternion; points in metres
+    assert np.abs(pc - po).max() < 5e-5, np.abs(pc - po).max()
     assert np.abs(qc - qo).max() < 1e-4, np.abs(qc - qo).max()
     print(f"BA full size: worst per-iteration chi2 difference {worst:.2e}, "
           f"pose {np.abs(pc - po).max():.2e}, point {np.abs(qc - qo).max():.2e}")
