@@ -20,6 +20,7 @@
 
 #include "g2oc_internal.h"
 #include "pcg_kernels.cuh"
+#include "tile_potrf.cuh"
 
 namespace g2oc {
 
@@ -37,6 +38,7 @@ struct CholPlan {
   DBuf<int2> d_upd;
   DBuf<int> d_pnl_ptr, d_upd_ptr, d_bwd_ptr;
   DBuf<double> A, y;
+  DBuf<double> W;  // W(k) = L(k,k)^-1 per diagonal tile (multi-launch form)
   DBuf<int> info;
   // every step has at most kCholSingleWidth panel tiles plus trailing
   // updates: the whole plan runs in one CTA (chol_factor_single)
@@ -157,6 +159,7 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
   G2OC_TRY(P.d_bwd.upload(P.bwd.empty() ? std::vector<int>{0} : P.bwd, st));
   G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
   G2OC_TRY(P.y.alloc(P.np));
+  G2OC_TRY(P.W.alloc(P.single ? (size_t)1 : (size_t)nt * kTile * kTile));
   G2OC_TRY(P.info.alloc(1));
   return G2OC_OK;
 }
@@ -186,77 +189,76 @@ __global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int
   }
 }
 
-// factor the diagonal tile k in shared memory (lower); T: kTile x (kTile+1)
-// doubles of shared memory
-__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double (*T)[kTile + 1], int* info) {
+// factor the diagonal tile k in shared memory (lower; T: kTile x (kTile+1)
+// doubles, buf: 2 kTile doubles) and form W = L(k,k)^-1 into W (column-major,
+// leading dimension ldw: shared or global memory); 256 threads
+__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double (*T)[kTile + 1], double* buf,
+                                                double* W, int ldw, int* info) {
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
-    T[i][j] = A[(base + j) * np + base + i];
+    if (i >= j) T[i][j] = A[(base + j) * np + base + i];
   }
   __syncthreads();
-  for (int j = 0; j < kTile; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = T[j][j];
-      if (!(d > 0.0)) *info = 1;
-      T[j][j] = sqrt(d > 0.0 ? d : 1.0);
-    }
-    __syncthreads();
-    const double piv = T[j][j];
-    for (int i = j + 1 + threadIdx.x; i < kTile; i += blockDim.x) T[i][j] /= piv;
-    __syncthreads();
-    const int m = kTile - j - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = j + 1 + e % m, c = j + 1 + e / m;
-      if (i >= c) T[i][c] -= T[i][j] * T[c][j];
-    }
-    __syncthreads();
-  }
+  tile_potrf_inv<kTile, 16, 16, double>(&T[0][0], kTile + 1, buf, info, W, ldw);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
     if (i >= j) A[(base + j) * np + base + i] = T[i][j];
   }
 }
 
-static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, int* info) {
+// W(k) of every diagonal tile, kTile x kTile column-major, at W + k kTile^2
+static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, int* info) {
   __shared__ double T[kTile][kTile + 1];
-  chol_potrf_tile(A, np, k, T, info);
+  __shared__ double buf[2 * kTile];
+  chol_potrf_tile(A, np, k, T, buf, W + (size_t)k * kTile * kTile, kTile, info);
 }
 
-// panel: L(i,k) = A(i,k) L(k,k)^-T for the listed tiles i
 constexpr int kTileSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
+// chol_factor_single: two operand tiles, W and the column buffer
+constexpr int kTileSmemSingle = 3 * kTile * (kTile + 1) * (int)sizeof(double) + 2 * kTile * (int)sizeof(double);
 
-__device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti, double (*L)[kTile + 1],
+// panel: L(i,k) = A(i,k) L(k,k)^-T = A(i,k) W^T for the tile i, with
+// Ws[c][r] = W(r, c) in shared memory; 4 x 4 outputs per thread (256 threads)
+__device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti, const double (*Ws)[kTile + 1],
                                                double (*X)[kTile + 1]) {
   const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
-    L[r][c] = A[(kb + c) * np + kb + r];
     X[r][c] = A[(kb + c) * np + ib + r];
   }
   __syncthreads();
-  // each row's columns in sequence; rows in parallel
-  const int row = threadIdx.x % kTile;
-  const int grp = threadIdx.x / kTile;
-  if (grp == 0) {
-    for (int c = 0; c < kTile; ++c) {
-      double v = X[row][c];
-      for (int t = 0; t < c; ++t) v -= X[row][t] * L[c][t];
-      X[row][c] = v / L[c][c];
+  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int t = 0; t < kTile; ++t) {
+    double x[4], w[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      x[a] = X[tr + 16 * a][t];
+      w[a] = Ws[t][tc + 16 * a];  // W(c, t)
     }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * w[b];
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-    const int r = e % kTile, c = e / kTile;
-    A[(kb + c) * np + ib + r] = X[r][c];
-  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) A[(kb + tc + 16 * b) * np + ib + tr + 16 * a] = acc[a][b];
 }
 
-static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles) {
+static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles, const double* W) {
   extern __shared__ double sm_trsm[];
-  double (*L)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
+  double (*Ws)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
   double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
-  chol_trsm_tile(A, np, k, tiles[blockIdx.x], L, X);
+  const double* Wk = W + (size_t)k * kTile * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Ws[e / kTile][e % kTile] = Wk[e];
+  chol_trsm_tile(A, np, k, tiles[blockIdx.x], Ws, X);
 }
 
 // trailing update: A(i,j) -= L(i,k) L(j,k)^T; 4x4 per thread (256 threads)
@@ -311,18 +313,21 @@ static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k
 // multi-launch form spends such a plan in the launch latency of its n / 64
 // strictly sequential steps; here the steps run back to back with the same
 // tile algorithms (same arithmetic, same order), the tiles passing through
-// shared memory and the factor staying in the dense buffer.
+// shared memory, W(k) staying in shared memory and the factor in the dense
+// buffer.
 static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int np, int nt, const int* pnl_ptr,
                                                                  const int* pnl, const int* upd_ptr,
                                                                  const int2* upd, int* info) {
   extern __shared__ double sm_single[];
   double (*B0)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single);
   double (*B1)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single + kTile * (kTile + 1));
+  double (*Ws)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single + 2 * kTile * (kTile + 1));
+  double* buf = sm_single + 3 * kTile * (kTile + 1);
   for (int k = 0; k < nt; ++k) {
-    chol_potrf_tile(A, np, k, B0, info);
+    chol_potrf_tile(A, np, k, B0, buf, &Ws[0][0], kTile + 1, info);
     __syncthreads();
     for (int p = pnl_ptr[k]; p < pnl_ptr[k + 1]; ++p) {
-      chol_trsm_tile(A, np, k, pnl[p], B0, B1);
+      chol_trsm_tile(A, np, k, pnl[p], Ws, B1);
       __syncthreads();
     }
     for (int p = upd_ptr[k]; p < upd_ptr[k + 1]; ++p) {
@@ -344,21 +349,17 @@ static __global__ void chol_store_x(const double* y, const int* perm, int bs, in
   if (t < n) x[t] = y[perm[t / bs] * bs + t % bs];
 }
 
-// L(k,k) y_k = y_k
-static __global__ void chol_fwd_diag(const double* A, int np, int k, double* y) {
+// L(k,k) y_k = y_k as y_k = W(k) y_k (thread per row)
+static __global__ void chol_fwd_diag(const double* W, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
-  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+  const double* Wk = W + kb * kTile;
+  const int r = threadIdx.x;
+  v[r] = y[kb + r];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int r = 0; r < kTile; ++r) {
-      double s = v[r];
-      for (int t = 0; t < r; ++t) s -= A[(kb + t) * np + kb + r] * v[t];
-      v[r] = s / A[(kb + r) * np + kb + r];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+  double s = 0.0;
+  for (int c = 0; c <= r; ++c) s += Wk[(size_t)c * kTile + r] * v[c];
+  y[kb + r] = s;
 }
 
 // y_i -= L(i,k) y_k for the listed tiles i > k
@@ -376,21 +377,17 @@ static __global__ void chol_fwd_update(const double* A, int np, int k, const int
   }
 }
 
-// L(k,k)^T x_k = y_k
-static __global__ void chol_bwd_diag(const double* A, int np, int k, double* y) {
+// L(k,k)^T x_k = y_k as y_k = W(k)^T y_k (thread per row)
+static __global__ void chol_bwd_diag(const double* W, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
-  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+  const double* Wk = W + kb * kTile;
+  const int r = threadIdx.x;
+  v[r] = y[kb + r];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int r = kTile - 1; r >= 0; --r) {
-      double s = v[r];
-      for (int t = r + 1; t < kTile; ++t) s -= A[(kb + r) * np + kb + t] * v[t];
-      v[r] = s / A[(kb + r) * np + kb + r];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
+  double s = 0.0;
+  for (int c = r; c < kTile; ++c) s += Wk[(size_t)r * kTile + c] * v[c];
+  y[kb + r] = s;
 }
 
 // y_i -= L(k,i)^T y_k for the listed tiles i < k
@@ -515,15 +512,16 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
   const long long work = (long long)nnzb * P.bs * P.bs + (np - P.n);
   chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.bs, P.d_perm.p, P.n, np, P.A.p);
   if (P.single) {
-    G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_factor_single, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
-    chol_factor_single<<<1, 256, kTileSmem, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p, P.d_upd.p,
+    G2OC_CUDA_TRY(
+        cudaFuncSetAttribute(chol_factor_single, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemSingle));
+    chol_factor_single<<<1, 256, kTileSmemSingle, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p, P.d_upd.p,
                                                   P.info.p);
     *nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
-    chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.info.p);
+    chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.W.p, P.info.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
-    if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k]);
+    if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.W.p);
     const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];
     if (nu > 0) chol_gemm<<<nu, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_upd.p + P.upd_ptr[k]);
     *nl += 1 + (np_k > 0) + (nu > 0);
@@ -547,13 +545,13 @@ static int chol_resolve(CholPlan& P, cudaStream_t st, const double* rhs, double*
     nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
-    chol_fwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
+    chol_fwd_diag<<<1, kTile, 0, st>>>(P.W.p, k, P.y.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_fwd_update<<<np_k, kTile, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
     nl += 1 + (np_k > 0);
   }
   for (int k = (P.single ? -1 : nt - 1); k >= 0; --k) {
-    chol_bwd_diag<<<1, kTile, 0, st>>>(P.A.p, np, k, P.y.p);
+    chol_bwd_diag<<<1, kTile, 0, st>>>(P.W.p, k, P.y.p);
     const int nbk = P.bwd_ptr[k + 1] - P.bwd_ptr[k];
     if (nbk > 0) chol_bwd_update<<<nbk, kTile, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
     nl += 1 + (nbk > 0);

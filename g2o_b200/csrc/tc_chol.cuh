@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "g2oc_internal.h"
+#include "tile_potrf.cuh"
 
 namespace g2oc {
 
@@ -45,7 +46,7 @@ constexpr int kTcK = 64;           // K per staged chunk
 constexpr int kTcOpBytes = kTc * kTcK * 4;        // one operand tile (hi or lo): 32 KB
 constexpr int kTcSmem = 4 * kTcOpBytes + 1024;    // A hi/lo, B hi/lo, barrier and TMEM address
 constexpr long long kTcSpinLimit = 1ll << 26;     // bounded waits (tens of ms at worst)
-constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + kTc) * sizeof(double);
+constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + 2 * kTc) * sizeof(double);
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t tc_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -233,64 +234,25 @@ static __global__ void __launch_bounds__(128, 1)
 // Factor the diagonal tile k in FP64 (lower), write L(k,k) back in FP32 and
 // W(k) = L(k,k)^-1 (FP32, column-major 128 x 128, zero above the diagonal)
 // to Wk. A non-positive pivot sets *info (the pivot is replaced by 1 so the
-// arithmetic stays finite). 512 threads; the factor's column j is finished
-// by one sweep (pivot, scaled column, trailing rank-1 update of the lower
-// triangle).
+// arithmetic stays finite). 512 threads as a 32 x 16 grid, each holding a
+// 4 x 8 interleaved sub-block of the tile in registers (tile_potrf_inv).
 static __global__ void __launch_bounds__(512, 1) tc_potrf(float* A, int np, int k, float* Wk, int* info) {
   extern __shared__ double tcp_smem[];
-  double* T = tcp_smem;                 // 128 x 129, column-major: T[j * 129 + i]
-  double* wd = tcp_smem + kTc * (kTc + 1);  // reciprocal pivots
   constexpr int LD = kTc + 1;
+  double* T = tcp_smem;                 // 128 x 129, row-major: T[i * 129 + j]
+  double* buf = tcp_smem + kTc * LD;    // two column vectors
   const size_t kb = (size_t)k * kTc;
   for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
     const int i = e % kTc, j = e / kTc;
-    if (i >= j) T[j * LD + i] = (double)A[(kb + j) * np + kb + i];
+    if (i >= j) T[i * LD + j] = (double)A[(kb + j) * np + kb + i];
   }
   __syncthreads();
-  for (int j = 0; j < kTc; ++j) {
-    if (threadIdx.x == 0) {
-      double d = T[j * LD + j];
-      if (!(d > 0.0)) {
-        atomicExch(info, 1);
-        d = 1.0;
-      }
-      const double s = sqrt(d);
-      T[j * LD + j] = s;
-      wd[j] = 1.0 / s;
-    }
-    __syncthreads();
-    const double r = wd[j];
-    for (int i = j + 1 + threadIdx.x; i < kTc; i += blockDim.x) T[j * LD + i] *= r;
-    __syncthreads();
-    const int m = kTc - j - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = j + 1 + e % m, c = j + 1 + e / m;
-      if (i >= c) T[c * LD + i] -= T[j * LD + i] * T[j * LD + c];
-    }
-    __syncthreads();
-  }
+  int bad = 0;
+  tile_potrf_inv<kTc, 32, 16, float>(T, LD, buf, &bad, Wk, kTc);
+  if (threadIdx.x == 0 && bad) atomicExch(info, 1);
   for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
     const int i = e % kTc, j = e / kTc;
-    if (i >= j) A[(kb + j) * np + kb + i] = (float)T[j * LD + i];
-  }
-  // W = L^-1, column c by thread c (forward substitution of e_c); W(l, c)
-  // for l > c kept in the free upper triangle of T at (row c, column l)
-  if (threadIdx.x < kTc) {
-    const int c = threadIdx.x;
-    for (int i = 0; i < kTc; ++i) {
-      double v;
-      if (i < c) {
-        v = 0.0;
-      } else if (i == c) {
-        v = wd[c];
-      } else {
-        double acc = T[c * LD + i] * wd[c];  // L(i,c) W(c,c)
-        for (int l = c + 1; l < i; ++l) acc += T[l * LD + i] * T[l * LD + c];
-        v = -acc * wd[i];
-        T[i * LD + c] = v;
-      }
-      Wk[(size_t)c * kTc + i] = (float)v;
-    }
+    if (i >= j) A[(kb + j) * np + kb + i] = (float)T[i * LD + j];
   }
 }
 
