@@ -57,6 +57,7 @@ sys.path.insert(0, ROOT)
 ITERATIONS = 20
 METRIC = "BA LM iter/s, time to FP64 chi2+-1e-6 (mixed vs FP64 GPU); edges/s linearize"
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 WORKLOAD = "bundle_adjustment_1000cam_200000pt_1.03Medges_huber_lm20"
 
 
@@ -796,6 +797,57 @@ def run_pg(args):
     }), flush=True)
 
 
+def tf32_peak():
+    """Dense TF32 tensor rate: half of the measured bf16 GEMM rate (the
+    nominal B200 ratio, 1.1 vs 2.25 PFLOP/s)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["bf16_tflops"]) / 2, "half of measured bf16"
+    return FALLBACK_BF16_TFLOPS / 2, "half of fallback bf16"
+
+
+def dense_cholesky_line(backend, fac, g, device, pcg_stats, iterations=3):
+    """The reduced camera system (n = 6 x free cameras) factored densely on
+    the tensor cores (lm_cuda_chol_mixed: 128 x 128 tiles, 3xTF32 tile
+    products, FP64 refinement) beside the PCG form of the headline
+    (lm_cuda_mixed_fast) over the same first LM iterations from the same
+    start: device ms per iteration and chi2, and the tile products' tensor
+    rate (issued MMA flops: 3 products x 2 x 128^3 per output tile)."""
+    pc = backend.CudaProblem(g, fac.construct("lm_cuda_chol_mixed"), device=device)
+    pc.optimize(1)  # plan, buffers
+    pc.restore_initial_estimates()
+    _, st = pc.optimize(iterations)
+    ms_it = sum(s["time_iteration"] for s in st) * 1e3 / len(st)
+    pc.restore_initial_estimates()
+    _, k0 = pc.kernel_stats()
+    pc.set_kernel_timing(True)
+    _, st_t = pc.optimize(iterations)
+    pc.set_kernel_timing(False)
+    _, k1 = pc.kernel_stats()
+    pc.close()
+    d = {k: (k1[k][0] - k0.get(k, (0, 0.0))[0], k1[k][1] - k0.get(k, (0, 0.0))[1]) for k in k1}
+    n = 6 * (g.num_poses - int(g.pose_fixed.sum()))
+    nt = (n + 127) // 128
+    factorizations = d.get("tc_expand", (0, 0.0))[0]
+    tiles_per_factor = sum(m + m * (m + 1) // 2 for m in range(1, nt))
+    mma_flops = factorizations * tiles_per_factor * 3 * 2 * 128 ** 3
+    tiles_ms = d.get("tc_tiles", (0, 0.0))[1]
+    peak, kind = tf32_peak()
+    achieved = mma_flops / (tiles_ms * 1e-3) / 1e12 if tiles_ms > 0 else None
+    pcg_ms = sum(s["time_iteration"] for s in pcg_stats[:iterations]) * 1e3 / min(iterations, len(pcg_stats))
+    return {
+        "solver": "lm_cuda_chol_mixed", "iterations": len(st), "n": n, "tiles_128": nt,
+        "ms_per_iteration": ms_it, "chi2": [s["chi2"] for s in st],
+        "pcg_form": {"solver": "lm_cuda_mixed_fast", "ms_per_iteration": pcg_ms,
+                     "chi2": [s["chi2"] for s in pcg_stats[:iterations]]},
+        "factorizations": factorizations,
+        "kernels_ms": {k: round(v[1], 3) for k, v in sorted(d.items(), key=lambda kv: -kv[1][1]) if v[0] > 0},
+        "tc_tiles": {"mma_tflop_per_factorization": tiles_per_factor * 3 * 2 * 128 ** 3 / 1e12,
+                     "achieved_tflops": achieved, "peak_tflops": peak, "peak_kind": kind,
+                     "frac": achieved / peak if achieved else None},
+    }
+
+
 def run_ours(args):
     rank, world, local = dist_info()
     import numpy as np
@@ -969,6 +1021,8 @@ def run_ours(args):
                 "new_topology_upload_s": structure_upload_s})
     pm.close()
 
+    dense = dense_cholesky_line(backend, fac, g, device, stm) if world == 1 else None
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baselines(g, args.cpu_sample_iterations)
@@ -1000,6 +1054,7 @@ def run_ours(args):
                           if len(str_) >= ITERATIONS else None,
                           "time_to_target_speedup_vs_fp64": (t64_to / tr_to) if (tr_to and t64_to) else None},
         "linearize_edges_per_s": edges_per_s,
+        "dense_cholesky": dense,
         "roofline": roof,
         "kernels": kernel_table,
         "gpu_launches": int(launches_value),

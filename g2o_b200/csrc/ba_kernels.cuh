@@ -507,72 +507,6 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
   }
 }
 
-// One 6x3 Hpl block (18 values, row-major) into both lanes of a lane pair
-// (lanes 2j, 2j+1: half = lane & 1), each lane loading about half of it and
-// the halves exchanged by shuffles. FP32 blocks are 72 bytes at a 72-byte
-// stride: 16-byte aligned when the block index is even, 8-byte aligned when
-// odd, so the loads are float4 where the alignment allows. FP64 blocks (144
-// bytes) are nine 16-byte words split 5 / 4. Every value is loaded by exactly
-// one lane and the other lane's slot holds 0, so the exchange is an exact
-// add of zero. Both lanes of the pair call it together with the same block;
-// the exchange names only those two lanes (other lane pairs of the warp may
-// have left their pair loops already).
-__device__ __forceinline__ void load_block_pair(const float* hpl, int blk, int half, float (&b)[18]) {
-  const float* base = hpl + (size_t)blk * 18;
-#pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] = 0.0f;
-  if ((blk & 1) == 0) {
-    // float4 at 0, 4, 8, 12 and float2 at 16
-    if (half == 0) {
-      const float4 u = __ldg(reinterpret_cast<const float4*>(base));
-      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 8));
-      const float2 w = __ldg(reinterpret_cast<const float2*>(base + 16));
-      b[0] = u.x; b[1] = u.y; b[2] = u.z; b[3] = u.w;
-      b[8] = v.x; b[9] = v.y; b[10] = v.z; b[11] = v.w;
-      b[16] = w.x; b[17] = w.y;
-    } else {
-      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 4));
-      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 12));
-      b[4] = u.x; b[5] = u.y; b[6] = u.z; b[7] = u.w;
-      b[12] = v.x; b[13] = v.y; b[14] = v.z; b[15] = v.w;
-    }
-  } else {
-    // float2 at 0 and float4 at 2, 6, 10, 14
-    if (half == 0) {
-      const float2 w = __ldg(reinterpret_cast<const float2*>(base));
-      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 2));
-      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 10));
-      b[0] = w.x; b[1] = w.y;
-      b[2] = u.x; b[3] = u.y; b[4] = u.z; b[5] = u.w;
-      b[10] = v.x; b[11] = v.y; b[12] = v.z; b[13] = v.w;
-    } else {
-      const float4 u = __ldg(reinterpret_cast<const float4*>(base + 6));
-      const float4 v = __ldg(reinterpret_cast<const float4*>(base + 14));
-      b[6] = u.x; b[7] = u.y; b[8] = u.z; b[9] = u.w;
-      b[14] = v.x; b[15] = v.y; b[16] = v.z; b[17] = v.w;
-    }
-  }
-  const unsigned pair_mask = 3u << (threadIdx.x & 30);
-#pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(pair_mask, b[t], 1);
-}
-
-__device__ __forceinline__ void load_block_pair(const double* hpl, int blk, int half, double (&b)[18]) {
-  const double2* base = reinterpret_cast<const double2*>(hpl + (size_t)blk * 18);
-#pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] = 0.0;
-#pragma unroll
-  for (int q = 0; q < 9; ++q)
-    if ((q & 1) == half) {
-      const double2 v = __ldg(base + q);
-      b[2 * q] = v.x;
-      b[2 * q + 1] = v.y;
-    }
-  const unsigned pair_mask = 3u << (threadIdx.x & 30);
-#pragma unroll
-  for (int t = 0; t < 18; ++t) b[t] += __shfl_xor_sync(pair_mask, b[t], 1);
-}
-
 // Dense output of the Schur rows for batched windows: each camera row belongs
 // to one window, whose reduced system is a dense FP64 matrix (n + 1 rows of
 // n, row-major, at M + mat[w]; the last row holds the right-hand side). Only
@@ -604,7 +538,7 @@ struct DenseOut {
 // (block k at tile_off[k], scalar rows 96 apart; an off-diagonal block inside
 // a diagonal tile also into its transposed place) instead of the row-SoA;
 // dn.M != nullptr: into the windows' dense matrices (DenseOut) instead.
-template <typename Real, int THREADS, bool STAGE, int G = 2, bool COOP = false>
+template <typename Real, int THREADS, bool STAGE, int G = 2>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
@@ -752,10 +686,6 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     // The pair list and S are touched once per pass: streamed (evict-first
     // loads and stores), so the L2 lines go to the Hpl blocks gathered again
     auto load_b = [&](int blk, Real (&b)[18]) {
-      if (COOP) {
-        load_block_pair(hpl, blk, half, b);
-        return;
-      }
       const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
@@ -846,237 +776,6 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
 #pragma unroll
           for (int c = 0; c < 6; ++c) __stcs(Sr + (size_t)((half * 3 + i) * 6 + c) * nblk + j, v[i * 6 + c]);
       }
-    }
-  }
-}
-
-// Staged Schur rows (FP32 storage, rows whose pair lists are short): the
-// same S(r, .) and b_schur as schur_rows with two lanes per block, but the
-// off-diagonal pair products read both operands from shared memory. Phase 1
-// is schur_rows' first pass (BD_a = B_a Dinv_l of the row's landmarks
-// staged in shared memory, the diagonal block and the reduced right-hand
-// side by a fixed CTA tree). Phase 2 copies the row's Hpl blocks B_b in
-// landmark order (stage: per row, the blocks of its pairs; a landmark's
-// blocks of the cameras after r are contiguous in Hpl, so the copy is a
-// stream of adjacent 8-byte words) into shared memory in chunks of `chunk`
-// blocks, then every lane pair (half = rows 0-2 / 3-5 of the block) adds the
-// pairs of its blocks that fall in the chunk, in landmark order, so each
-// block's sum has the same order as in schur_rows. A CTA runs one unit: a
-// row's off-diagonal blocks [j0, j1) (units[5 u .. 5 u + 4] = row, j0, j1,
-// start and length of the unit's staged list); lane pair lp owns blocks
-// j0 + lp + q * (THREADS / 2), q < NQ, with FP32 accumulators in registers.
-// Every unit of a row forms the row's BD; the first (j0 == 1) also writes
-// the diagonal block and the reduced right-hand side. pairs16: per pair
-// (a << 16) | (position of B_b in its unit's staged list). The outputs are
-// written as schur_rows writes them (dense tiles, or the row-SoA of
-// sys_offset).
-template <int THREADS, int NQ>
-__global__ void __launch_bounds__(THREADS, 1)
-    schur_rows_staged(const int* units, const int* hc_ptr, const int* hc_blk, const int* hc_col, const float* hpl,
-                      const float* dinv, const int* rptr, const int* rcol, const int* pair_ptr, const int32_t* stage,
-                      const int32_t* pairs16, const int* s_hpp, const float* hpp, double lambda, float* S,
-                      float* tiles, const int* tile_off, int bd_floats, int pairs_cap, int chunk,
-                      const double* b_p, const double* b_l, double* bs) {
-  constexpr int TS = kTileBlocks * 6;
-  constexpr int NP = THREADS / 2;  // lane pairs
-  constexpr int STAGE_ILP = 8;     // staged words in flight per thread
-  static_assert(NP * NQ == kStagedUnitBlocks, "a unit's blocks are the lane pairs' blocks");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[THREADS / 32][27];
-  float* BDs = reinterpret_cast<float*>(smem_raw);
-  int32_t* Ps = reinterpret_cast<int32_t*>(BDs + bd_floats);  // the unit's pair entries
-  float* Us = reinterpret_cast<float*>(Ps + pairs_cap);
-  const int* U = units + 5 * (size_t)blockIdx.x;
-  const int r = U[0], j0 = U[1], j1 = U[2], ubase = U[3], nu = U[4];
-  const bool first = j0 == 1;
-  const int a0 = hc_ptr[r], na = hc_ptr[r + 1] - a0;
-  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
-  float* Sr = S + (size_t)rb * 36;
-  // ---- phase 1 (as schur_rows): BD, diagonal block, reduced RHS
-  float dacc[21];
-  double racc[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int u = 0; u < 21; ++u) dacc[u] = 0.0f;
-  for (int t = threadIdx.x; t < na; t += THREADS) {
-    const int a = hc_blk[a0 + t], l = hc_col[a0 + t];
-    const float2* B2 = reinterpret_cast<const float2*>(hpl + (size_t)a * 18);
-    const float* Dl = dinv + (size_t)l * 9;
-    float b[18], D[9], bd[18];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const float2 v = B2[q];
-      b[2 * q] = v.x;
-      b[2 * q + 1] = v.y;
-      D[q] = Dl[q];
-    }
-    float* o = BDs + (size_t)t * 18;
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        bd[i * 3 + c] = b[i * 3] * D[c] + b[i * 3 + 1] * D[3 + c] + b[i * 3 + 2] * D[6 + c];
-        o[i * 3 + c] = bd[i * 3 + c];
-      }
-    int u = 0;
-#pragma unroll
-    for (int i = 0; i < 6; ++i)
-#pragma unroll
-      for (int c = i; c < 6; ++c, ++u)
-        dacc[u] += bd[i * 3] * b[c * 3] + bd[i * 3 + 1] * b[c * 3 + 1] + bd[i * 3 + 2] * b[c * 3 + 2];
-    if (bs && first) {
-      const double* bl = b_l + (size_t)l * 3;
-#pragma unroll
-      for (int q = 0; q < 6; ++q)
-        racc[q] += (double)bd[q * 3] * bl[0] + (double)bd[q * 3 + 1] * bl[1] + (double)bd[q * 3 + 2] * bl[2];
-    }
-  }
-  if (first) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double acc[27];
-#pragma unroll
-    for (int u = 0; u < 21; ++u) acc[u] = (double)dacc[u];
-#pragma unroll
-    for (int q = 0; q < 6; ++q) acc[21 + q] = racc[q];
-#pragma unroll
-    for (int u = 0; u < 27; ++u) acc[u] = warp_sum(acc[u]);
-    if (lane == 0) {
-#pragma unroll
-      for (int u = 0; u < 27; ++u) red[warp][u] = acc[u];
-    }
-    __syncthreads();
-    const int u = threadIdx.x;
-    if (u < 27) {
-      double sum = red[0][u];
-#pragma unroll
-      for (int w = 1; w < THREADS / 32; ++w) sum += red[w][u];
-      if (u < 21) {
-        int i = 0, c = u;
-        while (c >= 6 - i) {
-          c -= 6 - i;
-          ++i;
-        }
-        c += i;
-        const int hb = s_hpp[rb];
-        float* Td = tiles ? tiles + tile_off[rb] : nullptr;
-        double v = -sum + (i == c ? lambda : 0.0);
-        if (hb >= 0) v += (double)hpp[(size_t)hb * 36 + i * 6 + c];
-        if (Td) Td[i * TS + c] = (float)v;
-        else Sr[(size_t)(i * 6 + c) * nblk] = (float)v;
-        if (c != i) {
-          double w = -sum;
-          if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + c * 6 + i];
-          if (Td) Td[c * TS + i] = (float)w;
-          else Sr[(size_t)(c * 6 + i) * nblk] = (float)w;
-        }
-      } else if (bs) {
-        bs[(size_t)r * 6 + (u - 21)] = b_p[(size_t)r * 6 + (u - 21)] - sum;
-      }
-    }
-  }
-  // ---- phase 2: off-diagonal blocks from staged operands
-  const int lp = threadIdx.x >> 1, half = threadIdx.x & 1;
-  // the unit's pair entries (its blocks' lists, contiguous) into shared memory
-  const int pbase = pair_ptr[rb + j0];
-  for (int i = threadIdx.x; i < nu; i += THREADS) Ps[i] = __ldg(pairs16 + pbase + i);
-  float acc[NQ][18];
-  int p[NQ], pe[NQ];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-#pragma unroll
-    for (int t = 0; t < 18; ++t) acc[q][t] = 0.0f;
-    const int j = j0 + lp + q * NP;
-    p[q] = j < j1 ? pair_ptr[rb + j] - pbase : 0;
-    pe[q] = j < j1 ? pair_ptr[rb + j + 1] - pbase : 0;
-  }
-  const float2* hpl2 = reinterpret_cast<const float2*>(hpl);
-  for (int u0 = 0; u0 < nu; u0 += chunk) {
-    const int u1 = min(u0 + chunk, nu);
-    __syncthreads();  // the previous chunk's readers (and phase 1's BD, the pair entries) are done
-    const int words = (u1 - u0) * 9;
-    for (int w0 = threadIdx.x; w0 < words; w0 += THREADS * STAGE_ILP) {
-      int bidx[STAGE_ILP];
-      float2 val[STAGE_ILP];
-#pragma unroll
-      for (int t = 0; t < STAGE_ILP; ++t) {
-        const int w = w0 + t * THREADS;
-        bidx[t] = w < words ? __ldg(stage + ubase + u0 + w / 9) : 0;
-      }
-#pragma unroll
-      for (int t = 0; t < STAGE_ILP; ++t) {
-        const int w = w0 + t * THREADS;
-        if (w < words) val[t] = __ldg(hpl2 + (size_t)bidx[t] * 9 + (w % 9));
-      }
-#pragma unroll
-      for (int t = 0; t < STAGE_ILP; ++t) {
-        const int w = w0 + t * THREADS;
-        if (w < words) reinterpret_cast<float2*>(Us)[w] = val[t];
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      while (p[q] < pe[q] && (Ps[p[q]] & 0xFFFF) < u1) {
-        const int32_t cur = Ps[p[q]];
-        const int a = cur >> 16, ub = (cur & 0xFFFF) - u0;
-        ++p[q];
-        const float* D = BDs + (size_t)a * 18 + half * 9;
-        const float2* Bq = reinterpret_cast<const float2*>(Us) + (size_t)ub * 9;
-        float d[9];
-#pragma unroll
-        for (int t = 0; t < 9; ++t) d[t] = D[t];
-        // B row c (3 values) for c = 0..5, two columns at a time from float2 words
-#pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-          // rows 2cc and 2cc+1 of B are floats 6cc .. 6cc+5 = words 3cc .. 3cc+2
-          const float2 w0 = Bq[3 * cc], w1 = Bq[3 * cc + 1], w2 = Bq[3 * cc + 2];
-          const float x0[3] = {w0.x, w0.y, w1.x}, x1[3] = {w1.y, w2.x, w2.y};
-#pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            acc[q][i * 6 + 2 * cc] += d[i * 3] * x0[0] + d[i * 3 + 1] * x0[1] + d[i * 3 + 2] * x0[2];
-            acc[q][i * 6 + 2 * cc + 1] += d[i * 3] * x1[0] + d[i * 3 + 1] * x1[1] + d[i * 3 + 2] * x1[2];
-          }
-        }
-      }
-    }
-  }
-  // ---- outputs
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    const int j = j0 + lp + q * NP;
-    if (j >= j1) continue;
-    const int k = rb + j;
-    const int hb = s_hpp[k];
-    float v[18];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int c = 0; c < 6; ++c) {
-        const int e = (half * 3 + i) * 6 + c;
-        double w = -(double)acc[q][i * 6 + c];
-        if (hb >= 0) w += (double)hpp[(size_t)hb * 36 + e];
-        v[i * 6 + c] = (float)w;
-      }
-    if (tiles) {
-      const int off = tile_off[k];
-      float* T = tiles + off + half * 3 * TS;
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) __stcs(T + i * TS + c, v[i * 6 + c]);
-      const int cc = rcol[k];
-      if (r / kTileBlocks == cc / kTileBlocks) {
-        float* base = tiles + (size_t)(off / (TS * TS)) * (TS * TS);
-        const int lr = (r % kTileBlocks) * 6 + half * 3, lc = (cc % kTileBlocks) * 6;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int c = 0; c < 6; ++c) __stcs(base + (lc + c) * TS + lr + i, v[i * 6 + c]);
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) __stcs(Sr + (size_t)((half * 3 + i) * 6 + c) * nblk + j, v[i * 6 + c]);
     }
   }
 }

@@ -189,6 +189,14 @@ __global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int
   }
 }
 
+// asynchronous 8-byte global -> shared copies (every load of a tile in
+// flight at once, instead of one round trip per loop step)
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // factor the diagonal tile k in shared memory (lower; T: kTile x (kTile+1)
 // doubles, buf: 2 kTile doubles) and form W = L(k,k)^-1 into W (column-major,
 // leading dimension ldw: shared or global memory); 256 threads
@@ -197,8 +205,9 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
-    if (i >= j) T[i][j] = A[(base + j) * np + base + i];
+    if (i >= j) cp_async8(&T[i][j], A + (base + j) * np + base + i);
   }
+  cp_async_wait_all();
   __syncthreads();
   tile_potrf_inv<kTile, 16, 16, double>(&T[0][0], kTile + 1, buf, info, W, ldw);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
@@ -225,8 +234,9 @@ __device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti,
   const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
-    X[r][c] = A[(kb + c) * np + ib + r];
+    cp_async8(&X[r][c], A + (kb + c) * np + ib + r);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
   double acc[4][4];
@@ -267,9 +277,10 @@ __device__ __forceinline__ void chol_gemm_tile(double* A, int np, int k, int2 ij
   const size_t kb = (size_t)k * kTile, ib = (size_t)ij.x * kTile, jb = (size_t)ij.y * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
-    Li[r][c] = A[(kb + c) * np + ib + r];
-    Lj[r][c] = A[(kb + c) * np + jb + r];
+    cp_async8(&Li[r][c], A + (kb + c) * np + ib + r);
+    cp_async8(&Lj[r][c], A + (kb + c) * np + jb + r);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
   double acc[4][4];
@@ -421,9 +432,10 @@ static __global__ void __launch_bounds__(256) chol_solve_single(const double* A,
     const size_t kb = (size_t)k * kTile;
     for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
       const int r = e % kTile, c = e / kTile;
-      L[r][c] = r >= c ? A[(kb + c) * np + kb + r] : 0.0;
+      if (r >= c) cp_async8(&L[r][c], A + (kb + c) * np + kb + r);  // the substitutions read the lower triangle
     }
     if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+    cp_async_wait_all();
     __syncthreads();
     if (warp == 0) {
       double a0 = v[lane], a1 = v[lane + 32];
@@ -461,9 +473,10 @@ static __global__ void __launch_bounds__(256) chol_solve_single(const double* A,
     const size_t kb = (size_t)k * kTile;
     for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
       const int r = e % kTile, c = e / kTile;
-      L[r][c] = r >= c ? A[(kb + c) * np + kb + r] : 0.0;
+      if (r >= c) cp_async8(&L[r][c], A + (kb + c) * np + kb + r);  // the substitutions read the lower triangle
     }
     if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
+    cp_async_wait_all();
     __syncthreads();
     if (warp == 0) {
       // L^T x = v: column t of L^T is row t of L, the rows above t in turn

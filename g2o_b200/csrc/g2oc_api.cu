@@ -177,7 +177,6 @@ struct g2oc_ctx {
   g2oc::DBuf<double4> e_om, c_om;
   g2oc::DBuf<int> e_hpl, e_lm, lm_chunk_ptr, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, hc_col, hc_index, s_pair_ptr, s_hpp;
   g2oc::DBuf<int2> s_pairs;
-  g2oc::DBuf<int32_t> s_stage, s_pairs16;  // staged Schur rows (schur_rows_staged)
   // pose-graph edges
   g2oc::DBuf<int2> pe_v;
   g2oc::DBuf<double> pe_zinv, pe_info, pe_delta;
@@ -469,26 +468,14 @@ static int pcg_mode() {
 }
 static bool kernels_pcg() { return pcg_mode() == PCG_KERNELS; }
 
-// Schur rows of the FP32 path with short pair lists: staged operands
-// (schur_rows_staged; G2OC_SCHUR_STAGED=0: schur_rows)
-static bool schur_staged() {
+// order of the Schur rows in their launches: 0 by pair work (longest
+// first), 1 by camera index
+static int schur_row_order() {
   static const int v = [] {
-    const char* e = getenv("G2OC_SCHUR_STAGED");
-    return e ? atoi(e) : 1;
-  }();
-  return v != 0;
-}
-
-// Schur rows: each lane of a block pair loads the whole Hpl block (the
-// default: measured faster on the BA configuration, 240 vs 262 us per
-// launch); G2OC_SCHUR_COOP=1 has the two lanes split each load and exchange
-// halves by shuffle
-static bool schur_coop() {
-  static const int v = [] {
-    const char* e = getenv("G2OC_SCHUR_COOP");
+    const char* e = getenv("G2OC_SCHUR_ROW_ORDER");
     return e ? atoi(e) : 0;
   }();
-  return v != 0;
+  return v;
 }
 
 // LinearSolverPCG::_maxIter (the system dimension when unset); an FP32-stored
@@ -681,13 +668,6 @@ struct Engine final : EngineBase {
   bool tiles_from_schur = false;  // the last Schur pass wrote the tiles, not the row-SoA values
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
   size_t schur_smem = 0;
-  // schur_rows_staged (FP32, the 2-lane row class): shared memory of the
-  // row's BD blocks and of one chunk of staged Hpl blocks
-  static constexpr int kStagedThreads = 512, kStagedNQ = 3;
-  bool staged = false;
-  int staged_bd_floats = 0, staged_pairs_cap = 0, staged_chunk = 0, staged_n = 0;
-  DBuf<int> staged_units;  // the 2-lane rows' units (5 ints each), largest first
-  std::vector<int> two_lane_rows;
   DBuf<Real> hcontrib;
   DBuf<double> bcontrib;
   std::unique_ptr<TcChol> tc;  // tensor-core Cholesky of the reduced camera system (mixed precision)
@@ -715,44 +695,20 @@ struct Engine final : EngineBase {
           work[r] = pairs + 2.0 * (S.hc_ptr[r + 1] - S.hc_ptr[r]);
         }
         // rows with the most pair products first: the long rows start in
-        // the first wave of CTAs (a row's result does not depend on when it runs)
+        // the first wave of CTAs (a row's result does not depend on when it
+        // runs); G2OC_SCHUR_ROW_ORDER=1 keeps camera order instead, so the
+        // rows in flight together are neighbours whose co-observed landmarks
+        // (and so the gathered Hpl blocks) largely coincide
+        const bool by_work = schur_row_order() == 0;
         for (int gi = 0; gi < 3; ++gi) {
-          std::stable_sort(lists[gi].begin(), lists[gi].end(), [&](int a, int b) { return work[a] > work[b]; });
+          if (by_work)
+            std::stable_sort(lists[gi].begin(), lists[gi].end(), [&](int a, int b) { return work[a] > work[b]; });
           row_n[gi] = (int)lists[gi].size();
           G2OC_TRY(row_list[gi].upload(lists[gi].empty() ? std::vector<int>{0} : lists[gi], c->stream));
         }
-        two_lane_rows = lists[0];
       }
       schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
       stage_in_smem = schur_smem <= 190 * 1024;
-      {
-        // the staged kernel (2-lane rows): the row's BD (max blocks per
-        // camera) and a chunk of at least 256 staged blocks in shared memory;
-        // its units run largest staged list first
-        const long long budget = 227 * 1024 - 8 * 1024;
-        staged_bd_floats = ((S.max_blocks_per_cam * 18 + 3) / 4) * 4;
-        staged_pairs_cap = 0;
-        for (size_t u = 0; u < S.s_units.size() / 5; ++u)
-          staged_pairs_cap = std::max(staged_pairs_cap, S.s_units[5 * u + 4]);
-        staged_pairs_cap = (staged_pairs_cap + 3) / 4 * 4;
-        const long long left = budget - (long long)staged_bd_floats * 4 - (long long)staged_pairs_cap * 4;
-        staged_chunk = (int)std::min<long long>(4096, left > 0 ? left / 72 : 0);
-        staged = sizeof(Real) == 4 && !S.s_pairs16.empty() && staged_chunk >= 256;
-        if (staged) {
-          std::vector<char> two_lane(S.Cf, 0);
-          for (int r : two_lane_rows) two_lane[r] = 1;
-          std::vector<int> order;
-          for (int u = 0; u < (int)S.s_units.size() / 5; ++u)
-            if (two_lane[S.s_units[5 * u]]) order.push_back(u);
-          std::stable_sort(order.begin(), order.end(),
-                           [&](int a, int b) { return S.s_units[5 * a + 4] > S.s_units[5 * b + 4]; });
-          std::vector<int> un;
-          un.reserve(order.size() * 5);
-          for (int u : order) un.insert(un.end(), S.s_units.begin() + 5 * u, S.s_units.begin() + 5 * u + 5);
-          staged_n = (int)order.size();
-          G2OC_TRY(staged_units.upload(un.empty() ? std::vector<int>(5, 0) : un, c->stream));
-        }
-      }
       if (!stage_in_smem) schur_smem = 0;
       if (!stage_in_smem) G2OC_TRY(bdc.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
       G2OC_TRY(c->db.alloc((size_t)S.Pf * 3 + 1));
@@ -905,9 +861,7 @@ struct Engine final : EngineBase {
     for (int gi = 0; gi < 3; ++gi) {
       if (row_n[gi] == 0) continue;
       const int* rows = row_list[gi].p;
-      if (gi == 0 && staged && !to_windows && !lam_c && schur_staged())
-        G2OC_TRY(launch_schur_rows_staged(lambda, bp, bl, bs, to_tiles));
-      else if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
+      if (gi == 0) G2OC_TRY(launch_schur_rows<2>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
       else if (gi == 1) G2OC_TRY(launch_schur_rows<8>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
       else G2OC_TRY(launch_schur_rows<16>(rows, row_n[gi], lambda, lam_c, bp, bl, bs, to_tiles, to_windows));
     }
@@ -943,7 +897,7 @@ struct Engine final : EngineBase {
     const int* toff = to_tiles ? c->tile_off.p : nullptr;
     DenseOut dn{c->win_of_cam.p, c->win_cam.p, c->win_mat.p, to_windows ? c->win_scratch.p : nullptr};
     if (stage_in_smem) {
-      auto kern = schur_coop() ? schur_rows<Real, T, true, G, true> : schur_rows<Real, T, true, G, false>;
+      auto kern = schur_rows<Real, T, true, G>;
       G2OC_TRY(raise_dyn_smem((const void*)kern, schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
@@ -955,25 +909,6 @@ struct Engine final : EngineBase {
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
-  }
-
-  int launch_schur_rows_staged(double lambda, const double* bp, const double* bl, double* bs, bool to_tiles) {
-    if (staged_n == 0) return G2OC_OK;
-    if constexpr (sizeof(Real) != 4) {
-      set_error("the staged Schur rows are for FP32 storage");
-      return G2OC_ERR_NOT_SUPPORTED;
-    } else {
-      auto kern = schur_rows_staged<kStagedThreads, kStagedNQ>;
-      const size_t smem = ((size_t)staged_bd_floats + (size_t)staged_pairs_cap + (size_t)staged_chunk * 18) * 4;
-      G2OC_TRY(raise_dyn_smem((const void*)kern, smem));
-      G2OC_K(K_SCHUR_BLOCKS) kern<<<staged_n, kStagedThreads, smem, c->stream>>>(
-          staged_units.p, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_stage.p, c->s_pairs16.p, c->s_hpp.p, hpp.p, lambda, Sval.p,
-          to_tiles ? tiles.p : nullptr, to_tiles ? c->tile_off.p : nullptr, staged_bd_floats, staged_pairs_cap,
-          staged_chunk, bp, bl, bs);
-      G2OC_LAUNCH_CHECK();
-      return G2OC_OK;
-    }
   }
 
   int schur_rhs_from(const double* rp, const double* rl, double* bs) {
@@ -2236,13 +2171,6 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
     std::vector<int2> ab(S.s_pairs.size() / 2);
     for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.s_pairs[2 * i], S.s_pairs[2 * i + 1]);
     G2OC_TRY(c->s_pairs.upload(ab, st));
-    if (!S.s_pairs16.empty()) {
-      G2OC_TRY(c->s_stage.upload(S.s_stage, st));
-      G2OC_TRY(c->s_pairs16.upload(S.s_pairs16, st));
-    } else {
-      c->s_stage.release();
-      c->s_pairs16.release();
-    }
     G2OC_TRY(c->s_hpp.upload(S.s_hpp, st));
   } else {
     std::vector<int2> ev(na);

@@ -108,17 +108,6 @@ struct Structure {
   std::vector<int32_t> s_pairs;         // 2 per pair
   std::vector<int> s_hpp;               // per internal Schur block: Hpp block or -1
   int64_t num_pairs = 0;
-  // the staged form of the same pairs (schur_rows_staged): each row's
-  // off-diagonal blocks in units of at most kStagedUnitBlocks consecutive
-  // blocks; per unit the Hpl blocks B_b of its pairs in landmark order
-  // (s_stage; a unit's list is contiguous and the row's units follow each
-  // other inside the row's pair range), and per pair (position a in the
-  // row's camera list) << 16 | (position of its B_b in the unit's list).
-  // s_units: 5 per unit (row, first block, end block, list start, list
-  // length). Empty when a row has 65536 or more landmarks or pairs.
-  std::vector<int32_t> s_stage;
-  std::vector<int32_t> s_pairs16;
-  std::vector<int32_t> s_units;
 
   // ---- pose graphs (EdgeSE2 / EdgeSE3): device edge order = active order
   std::vector<int> pe_blk;              // 3 per active edge: Hpp block of (v0,v0), (v1,v1), (v0,v1) or -1
@@ -151,7 +140,6 @@ struct Structure {
 };
 
 constexpr int kSysChunk = 32;  // blocks per row chunk = lanes of a warp
-constexpr int kStagedUnitBlocks = 768;  // off-diagonal blocks per staged Schur unit (lane pairs x blocks each)
 constexpr int kTileBlocks = 16;  // blocks per tile side of the dense path
 
 int build_structure(const g2oc_graph* g, Structure& s);

@@ -324,9 +324,6 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
   s.schur_rc.clear();
   s.s_pair_ptr.clear();
   s.s_pairs.clear();
-  s.s_stage.clear();
-  s.s_pairs16.clear();
-  s.s_units.clear();
   s.s_hpp.clear();
   s.num_pairs = 0;
   if (s.schur) {
@@ -388,14 +385,6 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     std::vector<std::vector<int32_t>> row_cols(Cf);
     std::vector<std::vector<int32_t>> row_cnt(Cf);
     std::vector<int32_t> sp(2 * np);
-    // staged form: per unit of consecutive blocks, the unit's Hpl blocks in
-    // landmark order (the bucketing order) and, per sorted pair,
-    // (a << 16) | position in its unit's list
-    bool staged_ok = true;
-    for (int r = 0; r < Cf && staged_ok; ++r)
-      if (rcount[r + 1] - rcount[r] >= 65536 || s.hc_ptr[r + 1] - s.hc_ptr[r] >= 65536) staged_ok = false;
-    std::vector<int32_t> st16(staged_ok ? np : 0), stage(staged_ok ? np : 0);
-    std::vector<std::vector<int32_t>> row_units(Cf);
 #pragma omp parallel for schedule(dynamic, 8)
     for (int r = 0; r < Cf; ++r) {
       const int64_t q0 = rcount[r], q1 = rcount[r + 1];
@@ -408,44 +397,14 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
           cols.push_back(c);
           cc.push_back(cnt[c - r + 1]);
         }
-      // units: blocks 1 + u * kStagedUnitBlocks .. (block j = 1 + index in cols)
-      std::vector<int32_t> col_unit, unit_fill;
-      if (staged_ok) {
-        const int nunit = std::max<int>(1, ((int)cols.size() + kStagedUnitBlocks - 1) / kStagedUnitBlocks);
-        col_unit.assign(Cf - r + 1, 0);
-        std::vector<int64_t> ustart(nunit + 1, 0);
-        for (size_t i = 0; i < cols.size(); ++i) {
-          const int u = (int)(i / kStagedUnitBlocks);
-          col_unit[cols[i] - r] = u;
-          ustart[u + 1] += cc[i];
-        }
-        for (int u = 0; u < nunit; ++u) ustart[u + 1] += ustart[u];
-        std::vector<int32_t>& U = row_units[r];
-        for (int u = 0; u < nunit; ++u) {
-          const int j0 = 1 + u * kStagedUnitBlocks;
-          const int j1 = 1 + std::min<int>((int)cols.size(), (u + 1) * kStagedUnitBlocks);
-          U.insert(U.end(), {r, j0, j1, (int32_t)(q0 + ustart[u]), (int32_t)(ustart[u + 1] - ustart[u])});
-        }
-        unit_fill.assign(nunit, 0);
-      }
       for (int c = 1; c <= Cf - r; ++c) cnt[c] += cnt[c - 1];
       for (int64_t q = q0; q < q1; ++q) {
         const int64_t d = q0 + cnt[pc[q] - r]++;
         sp[2 * d] = pa[q];
         sp[2 * d + 1] = pb[q];
-        if (staged_ok) {
-          const int u = col_unit[pc[q] - r];
-          const int pos = unit_fill[u]++;
-          st16[d] = (pa[q] << 16) | pos;
-          stage[row_units[r][5 * u + 3] + pos] = pb[q];
-        }
       }
     }
-    if (staged_ok)
-      for (int r = 0; r < Cf; ++r) s.s_units.insert(s.s_units.end(), row_units[r].begin(), row_units[r].end());
     s.s_pairs.swap(sp);
-    s.s_stage.swap(stage);
-    s.s_pairs16.swap(st16);
     // internal (row-major) blocks: per row the diagonal, then the columns
     std::vector<int32_t> rm;
     std::vector<int> ptr;

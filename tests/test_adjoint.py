@@ -22,6 +22,7 @@ pytestmark = pytest.mark.gpu
 
 FD_STEP = 1e-4
 FD_TOL = 1e-4
+REOPT_ITERATIONS = 30
 DENSE_TOL = 1e-6
 
 
@@ -38,7 +39,7 @@ def converge(backend, g):
     c = backend.CudaProblem(g, fac.construct("lm_cuda_chol"))
     c.optimize(30)
     c.set_params(fac.construct("gn_cuda_chol"))
-    c.optimize(10)
+    c.optimize(REOPT_ITERATIONS)
     pose, point = c.estimates()
     return c, pose, point
 
@@ -145,9 +146,13 @@ class ConvergedLoss:
 
 
 def loss_after_reopt(backend, c, g2, pose, point):
+    # Gauss-Newton on a robust cost converges linearly (its Hessian keeps
+    # rho' where the exact one has rho' + 2 rho'' s along the residual of an
+    # edge in Huber's linear regime), so the shift of the optimum is resolved
+    # to the finite-difference accuracy only after a few tens of iterations
     c.upload(g2)  # same topology: values only
     c.set_estimates(pose, point)
-    c.optimize(8)
+    c.optimize(REOPT_ITERATIONS)
     p, _ = c.estimates()
     return synth.centre_loss(p, g2.extra["truth_pose"])[0]
 
