@@ -538,11 +538,13 @@ struct DenseOut {
 // (block k at tile_off[k], scalar rows 96 apart; an off-diagonal block inside
 // a diagonal tile also into its transposed place) instead of the row-SoA;
 // dn.M != nullptr: into the windows' dense matrices (DenseOut) instead.
+// block_order (or nullptr: storage order): per row, the off-diagonal block j
+// that the q-th lane group of a round takes, block_order[rptr[r] + q].
 template <typename Real, int THREADS, bool STAGE, int G = 2>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
-               const int2* pairs, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
+               const int2* pairs, const int* block_order, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
                Real* tiles, const int* tile_off, DenseOut dn, const double* b_p, const double* b_l, double* bs) {
   constexpr int TS = kTileBlocks * 6;  // scalar row stride of a tile
   static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per block: a power of two in [2, 32]");
@@ -673,8 +675,9 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
   // shuffles see full warps
   const int half = threadIdx.x & 1, sub = (threadIdx.x % G) >> 1;
   for (int j0 = 1; j0 < nblk; j0 += THREADS / G) {
-    const int j = j0 + (int)threadIdx.x / G;
-    const bool valid = j < nblk;
+    const int q = j0 + (int)threadIdx.x / G;
+    const bool valid = q < nblk;
+    const int j = (valid && block_order) ? block_order[rb + q] : q;
     const int k = rb + j;
     // pair products summed in the storage type (FP64 on the FP64 path; FP32
     // on the mixed path, whose S is stored in FP32), added to Hpp in FP64

@@ -478,6 +478,16 @@ static int schur_row_order() {
   return v;
 }
 
+// order of a Schur row's off-diagonal blocks over its lane groups: 1 by
+// pair count dealt in alternating rounds (the default), 0 storage order
+static int schur_block_order() {
+  static const int v = [] {
+    const char* e = getenv("G2OC_SCHUR_BLOCK_ORDER");
+    return e ? atoi(e) : 1;
+  }();
+  return v;
+}
+
 // LinearSolverPCG::_maxIter (the system dimension when unset); an FP32-stored
 // system (mixed path) is a correction step of the FP64 refinement, so its
 // iterations are capped and the FP64 residual check decides whether another
@@ -663,6 +673,7 @@ struct Engine final : EngineBase {
   // mean pair-list length (<= 12, <= 40, longer): a structural choice, so a
   // row gets the same arithmetic whatever else is in the graph
   DBuf<int> row_list[3];
+  DBuf<int> block_order;  // per row: its off-diagonal blocks in processing order (empty: j order)
   int row_n[3] = {0, 0, 0};
   bool tiles_fresh = false;  // tiles hold the matrix of the current solve
   bool tiles_from_schur = false;  // the last Schur pass wrote the tiles, not the row-SoA values
@@ -705,6 +716,34 @@ struct Engine final : EngineBase {
             std::stable_sort(lists[gi].begin(), lists[gi].end(), [&](int a, int b) { return work[a] > work[b]; });
           row_n[gi] = (int)lists[gi].size();
           G2OC_TRY(row_list[gi].upload(lists[gi].empty() ? std::vector<int>{0} : lists[gi], c->stream));
+        }
+        // the order in which a row's off-diagonal blocks go to its lane
+        // groups: by pair count, most first, dealt in rounds of one block per
+        // group with the direction reversed every round, so the blocks a warp
+        // runs side by side have nearly equal pair counts (a warp takes as
+        // long as its longest block) and the groups' totals even out
+        if (schur_block_order() != 0 && S.schur) {
+          std::vector<int> ord(S.schur_rc.size() / 2 + 1, 0);
+          std::vector<int> js;
+          for (int gi = 0; gi < 3; ++gi) {
+            const int groups = (sizeof(Real) == 4 ? 384 : 512) / (gi == 0 ? 2 : gi == 1 ? 8 : 16);
+            for (int r : lists[gi]) {
+              const int rb = S.sys_rptr[r], nb = S.sys_rptr[r + 1] - rb;
+              js.resize(std::max(nb - 1, 0));
+              for (int j = 1; j < nb; ++j) js[j - 1] = j;
+              std::stable_sort(js.begin(), js.end(), [&](int a, int b) {
+                return S.s_pair_ptr[rb + a + 1] - S.s_pair_ptr[rb + a] > S.s_pair_ptr[rb + b + 1] - S.s_pair_ptr[rb + b];
+              });
+              for (int q0 = 0; q0 < nb - 1; q0 += groups) {
+                const int q1 = std::min(nb - 1, q0 + groups);
+                if ((q0 / groups) & 1) std::reverse(js.begin() + q0, js.begin() + q1);
+              }
+              for (int q = 0; q < nb - 1; ++q) ord[rb + 1 + q] = js[q];
+            }
+          }
+          G2OC_TRY(block_order.upload(ord, c->stream));
+        } else {
+          block_order.release();
         }
       }
       schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
@@ -901,11 +940,13 @@ struct Engine final : EngineBase {
       G2OC_TRY(raise_dyn_smem((const void*)kern, schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, block_order.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp,
+          bl, bs);
     } else {
       G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false, G><<<nrows, T, 0, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
-          c->s_pair_ptr.p, c->s_pairs.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp, bl, bs);
+          c->s_pair_ptr.p, c->s_pairs.p, block_order.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp,
+          bl, bs);
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
