@@ -38,7 +38,7 @@ struct CholPlan {
   DBuf<int2> d_upd;
   DBuf<int> d_pnl_ptr, d_upd_ptr, d_bwd_ptr;
   DBuf<double> A, y;
-  DBuf<double> W;  // W(k) = L(k,k)^-1 per diagonal tile (multi-launch form)
+  DBuf<double> W;  // W(k) = L(k,k)^-1 per diagonal tile
   DBuf<int> info;
   // every step has at most kCholSingleWidth panel tiles plus trailing
   // updates: the whole plan runs in one CTA (chol_factor_single)
@@ -159,7 +159,7 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
   G2OC_TRY(P.d_bwd.upload(P.bwd.empty() ? std::vector<int>{0} : P.bwd, st));
   G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
   G2OC_TRY(P.y.alloc(P.np));
-  G2OC_TRY(P.W.alloc(P.single ? (size_t)1 : (size_t)nt * kTile * kTile));
+  G2OC_TRY(P.W.alloc((size_t)nt * kTile * kTile));
   G2OC_TRY(P.info.alloc(1));
   return G2OC_OK;
 }
@@ -197,125 +197,145 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// factor the diagonal tile k in shared memory (lower; T: kTile x (kTile+1)
-// doubles, buf: 2 kTile doubles) and form W = L(k,k)^-1 into W (column-major,
-// leading dimension ldw: shared or global memory); 256 threads
-__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double (*T)[kTile + 1], double* buf,
-                                                double* W, int ldw, int* info) {
+// Operand tiles of the tile products in shared memory: 64 rows of kLd
+// doubles (row-major, (row, k) at [row * kLd + k]). With kLd = 68 the
+// fragment loads of the FP64 tensor-core products (eight rows x four k per
+// warp instruction) fall in distinct bank pairs.
+constexpr int kLd = kTile + 4;
+constexpr int kTileBuf = kTile * kLd;  // doubles per operand tile
+
+// factor the diagonal tile k in shared memory (lower; T: a tile buffer, used
+// with leading dimension kTile + 1; buf: 3 kTile doubles) and form
+// W = L(k,k)^-1 into W (column-major, leading dimension ldw: shared or global
+// memory); 256 threads
+__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* buf, double* W, int ldw,
+                                                int* info) {
+  constexpr int ld = kTile + 1;
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
-    if (i >= j) cp_async8(&T[i][j], A + (base + j) * np + base + i);
+    if (i >= j) cp_async8(T + i * ld + j, A + (base + j) * np + base + i);
   }
   cp_async_wait_all();
   __syncthreads();
-  tile_potrf_inv<kTile, 16, 16, double>(&T[0][0], kTile + 1, buf, info, W, ldw);
+  tile_potrf_inv<kTile, 16, 16, double>(T, ld, buf, info, W, ldw);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
-    if (i >= j) A[(base + j) * np + base + i] = T[i][j];
+    if (i >= j) A[(base + j) * np + base + i] = T[i * ld + j];
   }
 }
 
 // W(k) of every diagonal tile, kTile x kTile column-major, at W + k kTile^2
 static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, int* info) {
-  __shared__ double T[kTile][kTile + 1];
-  __shared__ double buf[2 * kTile];
+  __shared__ double T[kTile * (kTile + 1)];
+  __shared__ double buf[3 * kTile];
   chol_potrf_tile(A, np, k, T, buf, W + (size_t)k * kTile * kTile, kTile, info);
 }
 
-constexpr int kTileSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
-// chol_factor_single: two operand tiles, W and the column buffer
-constexpr int kTileSmemSingle = 3 * kTile * (kTile + 1) * (int)sizeof(double) + 2 * kTile * (int)sizeof(double);
+constexpr int kTileSmem = 2 * kTileBuf * (int)sizeof(double);
+// chol_factor_single: two operand tiles, W and the factorization's vectors
+constexpr int kTileSmemSingle = 3 * kTileBuf * (int)sizeof(double) + 3 * kTile * (int)sizeof(double);
 
-// panel: L(i,k) = A(i,k) L(k,k)^-T = A(i,k) W^T for the tile i, with
-// Ws[c][r] = W(r, c) in shared memory; 4 x 4 outputs per thread (256 threads)
-__device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti, const double (*Ws)[kTile + 1],
-                                               double (*X)[kTile + 1]) {
-  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
+// P = X Y^T over k = 0..63 on the FP64 tensor cores (mma.sync m8n8k4, 256
+// threads): warp w owns rows 16 (w % 4) .. + 16 and columns 32 (w / 4) .. + 32
+// of P as 2 x 4 fragments of 8 x 8; lane (g, t) = (lane / 4, lane % 4) holds
+// P(i0 + 8u + g, j0 + 8v + 2t + e) in acc[u][v][e]. X is an operand tile
+// (row, k); Y is one too when KMAJOR is false, else Y(j, k) is at
+// Ys[k * kLd + j]. The k sums run in a fixed order: bit-reproducible.
+template <bool KMAJOR>
+__device__ __forceinline__ void chol_dmma_tile(const double* Xs, const double* Ys, double (&acc)[2][4][2]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v][0] = acc[u][v][1] = 0.0;
+#pragma unroll 4
+  for (int k0 = 0; k0 < kTile; k0 += 4) {
+    double fa[2], fb[4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) fa[u] = Xs[(i0 + 8 * u + g) * kLd + k0 + t];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      fb[v] = KMAJOR ? Ys[(k0 + t) * kLd + j0 + 8 * v + g] : Ys[(j0 + 8 * v + g) * kLd + k0 + t];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(acc[u][v][0]), "+d"(acc[u][v][1])
+                     : "d"(fa[u]), "d"(fb[v]));
+  }
+}
+
+// an operand tile (row, k) from the column-major tile of A at rows rb,
+// columns cb (k = column)
+__device__ __forceinline__ void chol_load_operand(const double* A, int np, size_t rb, size_t cb, double* Xs) {
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int r = e % kTile, c = e / kTile;
-    cp_async8(&X[r][c], A + (kb + c) * np + ib + r);
+    cp_async8(Xs + r * kLd + c, A + (cb + c) * np + rb + r);
   }
+}
+
+// panel: L(i,k) = A(i,k) L(k,k)^-T = A(i,k) W^T for the tile i, with
+// W(r, c) at Ws[c * kLd + r] in shared memory (256 threads)
+__device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti, const double* Ws, double* Xs) {
+  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
+  chol_load_operand(A, np, ib, kb, Xs);
   cp_async_wait_all();
   __syncthreads();
-  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
-  double acc[4][4];
+  double acc[2][4][2];
+  chol_dmma_tile<true>(Xs, Ws, acc);  // Y(j, t) = W(j, t) at Ws[t * kLd + j]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int u = 0; u < 2; ++u)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int t = 0; t < kTile; ++t) {
-    double x[4], w[4];
+    for (int v = 0; v < 4; ++v)
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      x[a] = X[tr + 16 * a][t];
-      w[a] = Ws[t][tc + 16 * a];  // W(c, t)
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * w[b];
-  }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) A[(kb + tc + 16 * b) * np + ib + tr + 16 * a] = acc[a][b];
+      for (int e = 0; e < 2; ++e)
+        A[(kb + j0 + 8 * v + 2 * t + e) * np + ib + i0 + 8 * u + g] = acc[u][v][e];
 }
 
 static __global__ void __launch_bounds__(256) chol_trsm(double* A, int np, int k, const int* tiles, const double* W) {
   extern __shared__ double sm_trsm[];
-  double (*Ws)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm);
-  double (*X)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_trsm + kTile * (kTile + 1));
+  double* Ws = sm_trsm;
+  double* Xs = sm_trsm + kTileBuf;
   const double* Wk = W + (size_t)k * kTile * kTile;
-  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Ws[e / kTile][e % kTile] = Wk[e];
-  chol_trsm_tile(A, np, k, tiles[blockIdx.x], Ws, X);
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Ws[(e / kTile) * kLd + e % kTile] = Wk[e];
+  chol_trsm_tile(A, np, k, tiles[blockIdx.x], Ws, Xs);
 }
 
-// trailing update: A(i,j) -= L(i,k) L(j,k)^T; 4x4 per thread (256 threads)
-__device__ __forceinline__ void chol_gemm_tile(double* A, int np, int k, int2 ij, double (*Li)[kTile + 1],
-                                               double (*Lj)[kTile + 1]) {
+// trailing update: A(i,j) -= L(i,k) L(j,k)^T (256 threads)
+__device__ __forceinline__ void chol_gemm_tile(double* A, int np, int k, int2 ij, double* Li, double* Lj) {
   const size_t kb = (size_t)k * kTile, ib = (size_t)ij.x * kTile, jb = (size_t)ij.y * kTile;
-  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-    const int r = e % kTile, c = e / kTile;
-    cp_async8(&Li[r][c], A + (kb + c) * np + ib + r);
-    cp_async8(&Lj[r][c], A + (kb + c) * np + jb + r);
-  }
+  chol_load_operand(A, np, ib, kb, Li);
+  chol_load_operand(A, np, jb, kb, Lj);
   cp_async_wait_all();
   __syncthreads();
-  const int tr = threadIdx.x % 16, tc = threadIdx.x / 16;
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int t = 0; t < kTile; ++t) {
-    double x[4], y[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      x[a] = Li[tr + 16 * a][t];
-      y[a] = Lj[tc + 16 * a][t];
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] += x[a] * y[b];
-  }
+  double acc[2][4][2];
+  chol_dmma_tile<false>(Li, Lj, acc);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
   const bool diag = ij.x == ij.y;
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int u = 0; u < 2; ++u)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int r = tr + 16 * a, c = tc + 16 * b;
-      if (diag && r < c) continue;
-      A[(jb + c) * np + ib + r] -= acc[a][b];
-    }
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = i0 + 8 * u + g, c = j0 + 8 * v + 2 * t + e;
+        if (diag && r < c) continue;
+        A[(jb + c) * np + ib + r] -= acc[u][v][e];
+      }
 }
 
 static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k, const int2* pairs) {
   extern __shared__ double sm_gemm[];
-  double (*Li)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm);
-  double (*Lj)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_gemm + kTile * (kTile + 1));
-  chol_gemm_tile(A, np, k, pairs[blockIdx.x], Li, Lj);
+  chol_gemm_tile(A, np, k, pairs[blockIdx.x], sm_gemm, sm_gemm + kTileBuf);
 }
 
 // The whole factorization in one CTA of 256 threads, for plans whose steps
@@ -328,14 +348,17 @@ static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k
 // buffer.
 static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int np, int nt, const int* pnl_ptr,
                                                                  const int* pnl, const int* upd_ptr,
-                                                                 const int2* upd, int* info) {
+                                                                 const int2* upd, double* W, int* info) {
   extern __shared__ double sm_single[];
-  double (*B0)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single);
-  double (*B1)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single + kTile * (kTile + 1));
-  double (*Ws)[kTile + 1] = reinterpret_cast<double (*)[kTile + 1]>(sm_single + 2 * kTile * (kTile + 1));
-  double* buf = sm_single + 3 * kTile * (kTile + 1);
+  double* B0 = sm_single;
+  double* B1 = sm_single + kTileBuf;
+  double* Ws = sm_single + 2 * kTileBuf;
+  double* buf = sm_single + 3 * kTileBuf;
   for (int k = 0; k < nt; ++k) {
-    chol_potrf_tile(A, np, k, B0, buf, &Ws[0][0], kTile + 1, info);
+    chol_potrf_tile(A, np, k, B0, buf, Ws, kLd, info);
+    // W(k) kept for the substitutions (chol_solve_single)
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x)
+      W[(size_t)k * kTile * kTile + e] = Ws[(e / kTile) * kLd + e % kTile];
     __syncthreads();
     for (int p = pnl_ptr[k]; p < pnl_ptr[k + 1]; ++p) {
       chol_trsm_tile(A, np, k, pnl[p], Ws, B1);
@@ -360,154 +383,125 @@ static __global__ void chol_store_x(const double* y, const int* perm, int bs, in
   if (t < n) x[t] = y[perm[t / bs] * bs + t % bs];
 }
 
-// L(k,k) y_k = y_k as y_k = W(k) y_k (thread per row)
-static __global__ void chol_fwd_diag(const double* W, int k, double* y) {
+// The substitutions take 64-long dot products with four threads per row
+// (16 terms each, all loads in flight, then a fixed xor tree over the four
+// lanes): 256 threads per 64 x 64 tile.
+__device__ __forceinline__ double chol_dot4(double s) {
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  return s;
+}
+
+// s = sum over this thread's 16 columns of M(row, c) v[c], M column-major
+// with leading dimension ld (M(row, c) at M[c * ld + row]), summed over the
+// row's four threads
+__device__ __forceinline__ double chol_rowdot(const double* M, size_t ld, const double* v) {
+  const int q = threadIdx.x & 3, row = threadIdx.x >> 2;
+  double t[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) t[c] = M[(size_t)(q * 16 + c) * ld + row];
+  double s = 0.0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) s += t[c] * v[q * 16 + c];
+  return chol_dot4(s);
+}
+
+// s = sum over this thread's 16 rows of M(r, col) v[r] (a column of M times
+// v), M column-major with leading dimension ld, col = the thread's row index
+__device__ __forceinline__ double chol_coldot(const double* M, size_t ld, const double* v) {
+  const int q = threadIdx.x & 3, col = threadIdx.x >> 2;
+  double t[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) t[r] = M[(size_t)col * ld + q * 16 + r];
+  double s = 0.0;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) s += t[r] * v[q * 16 + r];
+  return chol_dot4(s);
+}
+
+// L(k,k) y_k = y_k as y_k = W(k) y_k (256 threads)
+static __global__ void __launch_bounds__(256) chol_fwd_diag(const double* W, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
-  const double* Wk = W + kb * kTile;
-  const int r = threadIdx.x;
-  v[r] = y[kb + r];
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
   __syncthreads();
-  double s = 0.0;
-  for (int c = 0; c <= r; ++c) s += Wk[(size_t)c * kTile + r] * v[c];
-  y[kb + r] = s;
+  const double s = chol_rowdot(W + kb * kTile, kTile, v);
+  if ((threadIdx.x & 3) == 0) y[kb + (threadIdx.x >> 2)] = s;
 }
 
-// y_i -= L(i,k) y_k for the listed tiles i > k
-static __global__ void chol_fwd_update(const double* A, int np, int k, const int* tiles, double* y) {
-  const int ti = tiles[blockIdx.x];
-  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
-  __shared__ double yk[kTile];
-  if (threadIdx.x < kTile) yk[threadIdx.x] = y[kb + threadIdx.x];
+// y_i -= L(i,k) y_k for the listed tiles i > k (CTA per tile, 256 threads)
+static __global__ void __launch_bounds__(256) chol_fwd_update(const double* A, int np, int k, const int* tiles,
+                                                              double* y) {
+  __shared__ double v[kTile];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)tiles[blockIdx.x] * kTile;
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
   __syncthreads();
-  if (threadIdx.x < kTile) {
-    const int r = threadIdx.x;
-    double s = 0.0;
-    for (int t = 0; t < kTile; ++t) s += A[(kb + t) * np + ib + r] * yk[t];
-    y[ib + r] -= s;
-  }
+  const double s = chol_rowdot(A + kb * np + ib, np, v);
+  if ((threadIdx.x & 3) == 0) y[ib + (threadIdx.x >> 2)] -= s;
 }
 
-// L(k,k)^T x_k = y_k as y_k = W(k)^T y_k (thread per row)
-static __global__ void chol_bwd_diag(const double* W, int k, double* y) {
+// L(k,k)^T x_k = y_k as y_k = W(k)^T y_k (256 threads)
+static __global__ void __launch_bounds__(256) chol_bwd_diag(const double* W, int k, double* y) {
   __shared__ double v[kTile];
   const size_t kb = (size_t)k * kTile;
-  const double* Wk = W + kb * kTile;
-  const int r = threadIdx.x;
-  v[r] = y[kb + r];
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
   __syncthreads();
-  double s = 0.0;
-  for (int c = r; c < kTile; ++c) s += Wk[(size_t)r * kTile + c] * v[c];
-  y[kb + r] = s;
+  const double s = chol_coldot(W + kb * kTile, kTile, v);
+  if ((threadIdx.x & 3) == 0) y[kb + (threadIdx.x >> 2)] = s;
 }
 
-// y_i -= L(k,i)^T y_k for the listed tiles i < k
-static __global__ void chol_bwd_update(const double* A, int np, int k, const int* tiles, double* y) {
-  const int ti = tiles[blockIdx.x];
-  const size_t kb = (size_t)k * kTile, ib = (size_t)ti * kTile;
-  __shared__ double yk[kTile];
-  if (threadIdx.x < kTile) yk[threadIdx.x] = y[kb + threadIdx.x];
+// y_i -= L(k,i)^T y_k for the listed tiles i < k (CTA per tile, 256 threads)
+static __global__ void __launch_bounds__(256) chol_bwd_update(const double* A, int np, int k, const int* tiles,
+                                                              double* y) {
+  __shared__ double v[kTile];
+  const size_t kb = (size_t)k * kTile, ib = (size_t)tiles[blockIdx.x] * kTile;
+  if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
   __syncthreads();
-  if (threadIdx.x < kTile) {
-    const int c = threadIdx.x;
-    double s = 0.0;
-    for (int t = 0; t < kTile; ++t) s += A[(ib + c) * np + kb + t] * yk[t];
-    y[ib + c] -= s;
-  }
+  const double s = chol_coldot(A + ib * np + kb, np, v);
+  if ((threadIdx.x & 3) == 0) y[ib + (threadIdx.x >> 2)] -= s;
 }
 
 // Both substitutions of a single-CTA plan in one CTA of 256 threads: per
-// diagonal tile, warp 0 solves the 64 x 64 triangle from shared memory with
-// shuffles (lane l holds rows l and l + 32; a column's pivot division by its
-// owner, then the update of the rows below in column order, as
-// chol_fwd_diag), then the tiles the step updates take their products in
-// parallel (four tiles at a time, one thread per row or column).
-static __global__ void __launch_bounds__(256) chol_solve_single(const double* A, int np, int nt, const int* pnl_ptr,
-                                                                const int* pnl, const int* bwd_ptr, const int* bwd,
-                                                                double* y) {
-  __shared__ double L[kTile][kTile + 1];
-  __shared__ double v[kTile];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// diagonal tile the product with W(k) (kept by chol_factor_single), then
+// the products of the tiles the step updates, one tile at a time, with the
+// four-thread dot products above.
+static __global__ void __launch_bounds__(256) chol_solve_single(const double* A, const double* W, int np, int nt,
+                                                                const int* pnl_ptr, const int* pnl,
+                                                                const int* bwd_ptr, const int* bwd, double* y) {
+  __shared__ double v[kTile], x[kTile];
+  const bool lead = (threadIdx.x & 3) == 0;
+  const int row = threadIdx.x >> 2;
   for (int k = 0; k < nt; ++k) {
     const size_t kb = (size_t)k * kTile;
-    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-      const int r = e % kTile, c = e / kTile;
-      if (r >= c) cp_async8(&L[r][c], A + (kb + c) * np + kb + r);  // the substitutions read the lower triangle
-    }
     if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
-    cp_async_wait_all();
     __syncthreads();
-    if (warp == 0) {
-      double a0 = v[lane], a1 = v[lane + 32];
-      for (int t = 0; t < kTile; ++t) {
-        const bool lo = t < 32;
-        const int owner = t & 31;
-        double mine = lo ? a0 : a1;
-        if (lane == owner) mine = mine / L[t][t];
-        const double xt = __shfl_sync(0xffffffffu, mine, owner);
-        if (lane == owner) {
-          if (lo) a0 = xt;
-          else a1 = xt;
-        }
-        if (lane > t) a0 -= L[lane][t] * xt;
-        if (lane + 32 > t) a1 -= L[lane + 32][t] * xt;
-      }
-      v[lane] = a0;
-      v[lane + 32] = a1;
+    const double s = chol_rowdot(W + kb * kTile, kTile, v);
+    if (lead) {
+      x[row] = s;
+      y[kb + row] = s;
     }
     __syncthreads();
-    if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
-    const int np_k = pnl_ptr[k + 1] - pnl_ptr[k];
-    for (int q0 = 0; q0 < np_k; q0 += 4) {
-      const int q = q0 + (int)threadIdx.x / kTile, r = threadIdx.x % kTile;
-      if (q < np_k) {
-        const size_t ib = (size_t)pnl[pnl_ptr[k] + q] * kTile;
-        double s = 0.0;
-        for (int t = 0; t < kTile; ++t) s += A[(kb + t) * np + ib + r] * v[t];
-        y[ib + r] -= s;
-      }
+    for (int p = pnl_ptr[k]; p < pnl_ptr[k + 1]; ++p) {
+      const size_t ib = (size_t)pnl[p] * kTile;
+      const double t = chol_rowdot(A + kb * np + ib, np, x);
+      if (lead) y[ib + row] -= t;
     }
     __syncthreads();
   }
   for (int k = nt - 1; k >= 0; --k) {
     const size_t kb = (size_t)k * kTile;
-    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-      const int r = e % kTile, c = e / kTile;
-      if (r >= c) cp_async8(&L[r][c], A + (kb + c) * np + kb + r);  // the substitutions read the lower triangle
-    }
     if (threadIdx.x < kTile) v[threadIdx.x] = y[kb + threadIdx.x];
-    cp_async_wait_all();
     __syncthreads();
-    if (warp == 0) {
-      // L^T x = v: column t of L^T is row t of L, the rows above t in turn
-      double a0 = v[lane], a1 = v[lane + 32];
-      for (int t = kTile - 1; t >= 0; --t) {
-        const bool lo = t < 32;
-        const int owner = t & 31;
-        double mine = lo ? a0 : a1;
-        if (lane == owner) mine = mine / L[t][t];
-        const double xt = __shfl_sync(0xffffffffu, mine, owner);
-        if (lane == owner) {
-          if (lo) a0 = xt;
-          else a1 = xt;
-        }
-        if (lane < t) a0 -= L[t][lane] * xt;
-        if (lane + 32 < t) a1 -= L[t][lane + 32] * xt;
-      }
-      v[lane] = a0;
-      v[lane + 32] = a1;
+    const double s = chol_coldot(W + kb * kTile, kTile, v);
+    if (lead) {
+      x[row] = s;
+      y[kb + row] = s;
     }
     __syncthreads();
-    if (threadIdx.x < kTile) y[kb + threadIdx.x] = v[threadIdx.x];
-    const int nb_k = bwd_ptr[k + 1] - bwd_ptr[k];
-    for (int q0 = 0; q0 < nb_k; q0 += 4) {
-      const int q = q0 + (int)threadIdx.x / kTile, c = threadIdx.x % kTile;
-      if (q < nb_k) {
-        const size_t ib = (size_t)bwd[bwd_ptr[k] + q] * kTile;
-        double s = 0.0;
-        for (int t = 0; t < kTile; ++t) s += A[(ib + c) * np + kb + t] * v[t];
-        y[ib + c] -= s;
-      }
+    for (int p = bwd_ptr[k]; p < bwd_ptr[k + 1]; ++p) {
+      const size_t ib = (size_t)bwd[p] * kTile;
+      const double t = chol_coldot(A + ib * np + kb, np, x);
+      if (lead) y[ib + row] -= t;
     }
     __syncthreads();
   }
@@ -527,8 +521,8 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
   if (P.single) {
     G2OC_CUDA_TRY(
         cudaFuncSetAttribute(chol_factor_single, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemSingle));
-    chol_factor_single<<<1, 256, kTileSmemSingle, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p, P.d_upd.p,
-                                                  P.info.p);
+    chol_factor_single<<<1, 256, kTileSmemSingle, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p,
+                                                        P.d_upd.p, P.W.p, P.info.p);
     *nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
@@ -554,19 +548,20 @@ static int chol_resolve(CholPlan& P, cudaStream_t st, const double* rhs, double*
   const int np = P.np, nt = P.nt;
   chol_load_rhs<<<(np + 255) / 256, 256, 0, st>>>(rhs, P.d_perm.p, P.nb, P.bs, P.n, np, P.y.p);
   if (P.single) {
-    chol_solve_single<<<1, 256, 0, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_bwd_ptr.p, P.d_bwd.p, P.y.p);
+    chol_solve_single<<<1, 256, 0, st>>>(P.A.p, P.W.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_bwd_ptr.p, P.d_bwd.p,
+                                         P.y.p);
     nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
-    chol_fwd_diag<<<1, kTile, 0, st>>>(P.W.p, k, P.y.p);
+    chol_fwd_diag<<<1, 256, 0, st>>>(P.W.p, k, P.y.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
-    if (np_k > 0) chol_fwd_update<<<np_k, kTile, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
+    if (np_k > 0) chol_fwd_update<<<np_k, 256, 0, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.y.p);
     nl += 1 + (np_k > 0);
   }
   for (int k = (P.single ? -1 : nt - 1); k >= 0; --k) {
-    chol_bwd_diag<<<1, kTile, 0, st>>>(P.W.p, k, P.y.p);
+    chol_bwd_diag<<<1, 256, 0, st>>>(P.W.p, k, P.y.p);
     const int nbk = P.bwd_ptr[k + 1] - P.bwd_ptr[k];
-    if (nbk > 0) chol_bwd_update<<<nbk, kTile, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
+    if (nbk > 0) chol_bwd_update<<<nbk, 256, 0, st>>>(P.A.p, np, k, P.d_bwd.p + P.bwd_ptr[k], P.y.p);
     nl += 1 + (nbk > 0);
   }
   chol_store_x<<<(P.n + 255) / 256, 256, 0, st>>>(P.y.p, P.d_perm.p, P.bs, P.n, xout);

@@ -46,7 +46,7 @@ constexpr int kTcK = 64;           // K per staged chunk
 constexpr int kTcOpBytes = kTc * kTcK * 4;        // one operand tile (hi or lo): 32 KB
 constexpr int kTcSmem = 4 * kTcOpBytes + 1024;    // A hi/lo, B hi/lo, barrier and TMEM address
 constexpr long long kTcSpinLimit = 1ll << 26;     // bounded waits (tens of ms at worst)
-constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + 2 * kTc) * sizeof(double);
+constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + 3 * kTc) * sizeof(double);
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t tc_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -240,7 +240,7 @@ static __global__ void __launch_bounds__(512, 1) tc_potrf(float* A, int np, int 
   extern __shared__ double tcp_smem[];
   constexpr int LD = kTc + 1;
   double* T = tcp_smem;                 // 128 x 129, row-major: T[i * 129 + j]
-  double* buf = tcp_smem + kTc * LD;    // two column vectors
+  double* buf = tcp_smem + kTc * LD;    // two column vectors and the pivots' reciprocals
   const size_t kb = (size_t)k * kTc;
   for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
     const int i = e % kTc, j = e / kTc;
