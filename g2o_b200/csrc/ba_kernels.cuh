@@ -545,7 +545,8 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
                const int2* pairs, const int* block_order, const int* s_hpp, const Real* hpp, double lambda_all, const double* lambda_of, Real* S,
-               Real* tiles, const int* tile_off, DenseOut dn, const double* b_p, const double* b_l, double* bs) {
+               Real* tiles, const int* tile_off, DenseOut dn, const double* b_p, const double* b_l, double* bs,
+               int bds) {
   constexpr int TS = kTileBlocks * 6;  // scalar row stride of a tile
   static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "lanes per block: a power of two in [2, 32]");
   using R2 = typename Vec2<Real>::T;
@@ -570,6 +571,11 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
   // than shared memory holds, written to the camera-major scratch bdc and read
   // back in place); with B_a still in registers, its diagonal-block term
   // BD_a B_a^T (upper 21 entries) and its right-hand-side term BD_a b_l.
+  // staged BD blocks: bds entries apart, rows 0-2 at 0 and rows 3-5 at bds / 2
+  // (bds = 24 in FP32: each half starts on a 16-byte boundary, read with two
+  // 16-byte loads and one 4-byte load; else 18, packed)
+  if (!STAGE) bds = 18;
+  const int bhalf = bds / 2;
   Real* BDw = STAGE ? reinterpret_cast<Real*>(smem_raw) : const_cast<Real*>(bdc) + (size_t)a0 * 18;
   Real dacc[21];
   double racc[6] = {0, 0, 0, 0, 0, 0};
@@ -597,13 +603,13 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       b[2 * q + 1] = v.y;
       D[q] = Dl[q];
     }
-    Real* o = BDw + (size_t)t * 18;
+    Real* o = BDw + (size_t)t * bds;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         bd[i * 3 + c] = b[i * 3] * D[c] + b[i * 3 + 1] * D[3 + c] + b[i * 3 + 2] * D[6 + c];
-        o[i * 3 + c] = bd[i * 3 + c];
+        o[(i / 3) * bhalf + (i % 3) * 3 + c] = bd[i * 3 + c];
       }
     int u = 0;
 #pragma unroll
@@ -689,19 +695,45 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     // The pair list and S are touched once per pass: streamed (evict-first
     // loads and stores), so the L2 lines go to the Hpl blocks gathered again
     auto load_b = [&](int blk, Real (&b)[18]) {
-      const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
+      if constexpr (sizeof(Real) == 4) {
+        // a 72-byte FP32 block starts on a 16-byte boundary when its index is
+        // even (four 16-byte loads, then 8 bytes) and on an 8-byte one when odd
+        // (8 bytes, then four 16-byte loads): five loads instead of nine
+        const float* base = reinterpret_cast<const float*>(hpl) + (size_t)blk * 18;
+        const bool odd = blk & 1;
+        const int o4 = odd ? 2 : 0;
+        const float4 u0 = __ldg(reinterpret_cast<const float4*>(base + o4));
+        const float4 u1 = __ldg(reinterpret_cast<const float4*>(base + o4 + 4));
+        const float4 u2 = __ldg(reinterpret_cast<const float4*>(base + o4 + 8));
+        const float4 u3 = __ldg(reinterpret_cast<const float4*>(base + o4 + 12));
+        const float2 w = __ldg(reinterpret_cast<const float2*>(base + (odd ? 0 : 16)));
+        const float q[18] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w, u2.x,
+                             u2.y, u2.z, u2.w, u3.x, u3.y, u3.z, u3.w, w.x,  w.y};
 #pragma unroll
-      for (int t = 0; t < 9; ++t) {
-        const R2 v = __ldg(B2 + t);
-        b[2 * t] = v.x;
-        b[2 * t + 1] = v.y;
+        for (int t = 0; t < 18; ++t) b[t] = odd ? (t < 2 ? q[16 + t] : q[t - 2]) : q[t];
+      } else {
+        const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          const R2 v = __ldg(B2 + t);
+          b[2 * t] = v.x;
+          b[2 * t + 1] = v.y;
+        }
       }
     };
     auto accum = [&](int a, const Real (&b)[18]) {
-      const Real* D = BDa + (size_t)a * 18 + half * 9;
+      const Real* D = BDa + (size_t)a * bds + half * bhalf;
       Real d[9];
+      if (sizeof(Real) == 4 && bds == 24) {
+        const float4 d0 = *reinterpret_cast<const float4*>(D);
+        const float4 d1 = *reinterpret_cast<const float4*>(D + 4);
+        d[0] = d0.x; d[1] = d0.y; d[2] = d0.z; d[3] = d0.w;
+        d[4] = d1.x; d[5] = d1.y; d[6] = d1.z; d[7] = d1.w;
+        d[8] = D[8];
+      } else {
 #pragma unroll
-      for (int t = 0; t < 9; ++t) d[t] = D[t];
+        for (int t = 0; t < 9; ++t) d[t] = D[t];
+      }
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -751,10 +783,16 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
         // this lane's three scalar rows of the block: six contiguous entries each
         const int off = tile_off[k];
         Real* T = tiles + off + half * 3 * TS;
+        // (six entries of a row start on an 8-byte boundary in FP32: pairs)
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int c = 0; c < 6; ++c) __stcs(T + i * TS + c, v[i * 6 + c]);
+          for (int c = 0; c < 6; c += 2) {
+            R2 pr;
+            pr.x = v[i * 6 + c];
+            pr.y = v[i * 6 + c + 1];
+            __stcs(reinterpret_cast<R2*>(T + i * TS + c), pr);
+          }
         const int cc = rcol[k];
         if (r / kTileBlocks == cc / kTileBlocks) {
           Real* base = tiles + (size_t)(off / (TS * TS)) * (TS * TS);

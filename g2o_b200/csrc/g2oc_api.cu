@@ -678,6 +678,7 @@ struct Engine final : EngineBase {
   bool tiles_fresh = false;  // tiles hold the matrix of the current solve
   bool tiles_from_schur = false;  // the last Schur pass wrote the tiles, not the row-SoA values
   bool stage_in_smem = true;  // schur_rows: camera blocks staged in shared memory
+  int bd_stride = 18;         // schur_rows: entries between staged BD blocks
   size_t schur_smem = 0;
   DBuf<Real> hcontrib;
   DBuf<double> bcontrib;
@@ -746,7 +747,11 @@ struct Engine final : EngineBase {
           block_order.release();
         }
       }
-      schur_smem = (size_t)S.max_blocks_per_cam * 18 * sizeof(Real);
+      // FP32: BD blocks 24 floats apart when two CTAs of the row kernel still
+      // fit on an SM (their halves then start on 16-byte boundaries): 228 KB
+      // of shared memory per SM, 1 KB reserved and ~3 KB static per CTA
+      bd_stride = sizeof(Real) == 4 && (size_t)S.max_blocks_per_cam * 24 * 4 <= 110 * 1024 ? 24 : 18;
+      schur_smem = (size_t)S.max_blocks_per_cam * bd_stride * sizeof(Real);
       stage_in_smem = schur_smem <= 190 * 1024;
       if (!stage_in_smem) schur_smem = 0;
       if (!stage_in_smem) G2OC_TRY(bdc.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
@@ -941,12 +946,12 @@ struct Engine final : EngineBase {
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, block_order.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp,
-          bl, bs);
+          bl, bs, bd_stride);
     } else {
       G2OC_K(K_SCHUR_BLOCKS) schur_rows<Real, T, false, G><<<nrows, T, 0, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
           c->s_pair_ptr.p, c->s_pairs.p, block_order.p, c->s_hpp.p, hpp.p, lambda, lam_c, Sval.p, tl, toff, dn, bp,
-          bl, bs);
+          bl, bs, bd_stride);
     }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
