@@ -540,7 +540,7 @@ struct DenseOut {
 // dn.M != nullptr: into the windows' dense matrices (DenseOut) instead.
 // block_order (or nullptr: storage order): per row, the off-diagonal block j
 // that the q-th lane group of a round takes, block_order[rptr[r] + q].
-template <typename Real, int THREADS, bool STAGE, int G = 2>
+template <typename Real, int THREADS, bool STAGE, int G = 2, bool VEC = false>
 __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     schur_rows(const int* rows, const int* hc_ptr, const int* hc_blk, const int* hc_col, const Real* hpl,
                const Real* dinv, const Real* bdc, const int* rptr, const int* rcol, const int* pair_ptr,
@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     // The pair list and S are touched once per pass: streamed (evict-first
     // loads and stores), so the L2 lines go to the Hpl blocks gathered again
     auto load_b = [&](int blk, Real (&b)[18]) {
-      if constexpr (sizeof(Real) == 4) {
+      if constexpr (sizeof(Real) == 4 && VEC) {
         // a 72-byte FP32 block starts on a 16-byte boundary when its index is
         // even (four 16-byte loads, then 8 bytes) and on an 8-byte one when odd
         // (8 bytes, then four 16-byte loads): five loads instead of nine

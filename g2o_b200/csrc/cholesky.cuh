@@ -205,11 +205,9 @@ constexpr int kLd = kTile + 4;
 constexpr int kTileBuf = kTile * kLd;  // doubles per operand tile
 
 // factor the diagonal tile k in shared memory (lower; T: a tile buffer, used
-// with leading dimension kTile + 1; buf: 3 kTile doubles) and form
-// W = L(k,k)^-1 into W (column-major, leading dimension ldw: shared or global
-// memory); 256 threads
-__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* buf, double* W, int ldw,
-                                                int* info) {
+// with leading dimension kTile + 1) and form W = L(k,k)^-1 in Wsm (FP64
+// shared memory, column-major, leading dimension ldw); 256 threads
+__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* Wsm, int ldw, int* info) {
   constexpr int ld = kTile + 1;
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
@@ -218,7 +216,7 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
   }
   cp_async_wait_all();
   __syncthreads();
-  tile_potrf_inv<kTile, 16, 16, double>(T, ld, buf, info, W, ldw);
+  tile_potrf_inv_blk64(T, ld, Wsm, ldw, info);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
     if (i >= j) A[(base + j) * np + base + i] = T[i * ld + j];
@@ -226,15 +224,19 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
 }
 
 // W(k) of every diagonal tile, kTile x kTile column-major, at W + k kTile^2
+constexpr int kPotrfSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
 static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, int* info) {
-  __shared__ double T[kTile * (kTile + 1)];
-  __shared__ double buf[3 * kTile];
-  chol_potrf_tile(A, np, k, T, buf, W + (size_t)k * kTile * kTile, kTile, info);
+  extern __shared__ double sm_potrf[];
+  double* T = sm_potrf;
+  double* Wsm = sm_potrf + kTile * (kTile + 1);
+  chol_potrf_tile(A, np, k, T, Wsm, kTile + 1, info);
+  double* Wk = W + (size_t)k * kTile * kTile;
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Wk[e] = Wsm[(e / kTile) * (kTile + 1) + e % kTile];
 }
 
 constexpr int kTileSmem = 2 * kTileBuf * (int)sizeof(double);
-// chol_factor_single: two operand tiles, W and the factorization's vectors
-constexpr int kTileSmemSingle = 3 * kTileBuf * (int)sizeof(double) + 3 * kTile * (int)sizeof(double);
+// chol_factor_single: two operand tiles and W
+constexpr int kTileSmemSingle = 3 * kTileBuf * (int)sizeof(double);
 
 // P = X Y^T over k = 0..63 on the FP64 tensor cores (mma.sync m8n8k4, 256
 // threads): warp w owns rows 16 (w % 4) .. + 16 and columns 32 (w / 4) .. + 32
@@ -353,9 +355,8 @@ static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int 
   double* B0 = sm_single;
   double* B1 = sm_single + kTileBuf;
   double* Ws = sm_single + 2 * kTileBuf;
-  double* buf = sm_single + 3 * kTileBuf;
   for (int k = 0; k < nt; ++k) {
-    chol_potrf_tile(A, np, k, B0, buf, Ws, kLd, info);
+    chol_potrf_tile(A, np, k, B0, Ws, kLd, info);
     // W(k) kept for the substitutions (chol_solve_single)
     for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x)
       W[(size_t)k * kTile * kTile + e] = Ws[(e / kTile) * kLd + e % kTile];
@@ -512,6 +513,7 @@ template <typename Real>
 static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long long* nl) {
   const int nnzb = S.nnzb;
   const int np = P.np, nt = P.nt;
+  G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, kPotrfSmem));
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
   G2OC_CUDA_TRY(cudaFuncSetAttribute(chol_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
   G2OC_CUDA_TRY(cudaMemsetAsync(P.A.p, 0, P.A.bytes(), st));
@@ -526,7 +528,7 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
     *nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
-    chol_potrf<<<1, 256, 0, st>>>(P.A.p, np, k, P.W.p, P.info.p);
+    chol_potrf<<<1, 256, kPotrfSmem, st>>>(P.A.p, np, k, P.W.p, P.info.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.W.p);
     const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];

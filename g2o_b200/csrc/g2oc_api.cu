@@ -478,6 +478,28 @@ static int schur_row_order() {
   return v;
 }
 
+// entries between the staged BD blocks of a Schur row: 18 (packed, the
+// default) or 24 (G2OC_SCHUR_BD_STRIDE=24: 16-byte aligned halves; measured
+// slower, 417 vs 238 us per launch on the BA configuration, from 4-way bank
+// conflicts of the staging stores)
+static int schur_bd_stride() {
+  static const int v = [] {
+    const char* e = getenv("G2OC_SCHUR_BD_STRIDE");
+    return e ? atoi(e) : 18;
+  }();
+  return v;
+}
+
+// FP32 Schur rows: gather each Hpl block with five aligned vector loads
+// instead of nine 8-byte loads (G2OC_SCHUR_VEC=1)
+static bool schur_vec_loads() {
+  static const int v = [] {
+    const char* e = getenv("G2OC_SCHUR_VEC");
+    return e ? atoi(e) : 0;
+  }();
+  return v != 0;
+}
+
 // order of a Schur row's off-diagonal blocks over its lane groups: 1 by
 // pair count dealt in alternating rounds (the default), 0 storage order
 static int schur_block_order() {
@@ -750,7 +772,8 @@ struct Engine final : EngineBase {
       // FP32: BD blocks 24 floats apart when two CTAs of the row kernel still
       // fit on an SM (their halves then start on 16-byte boundaries): 228 KB
       // of shared memory per SM, 1 KB reserved and ~3 KB static per CTA
-      bd_stride = sizeof(Real) == 4 && (size_t)S.max_blocks_per_cam * 24 * 4 <= 110 * 1024 ? 24 : 18;
+      bd_stride = schur_bd_stride() == 24 && sizeof(Real) == 4 &&
+                          (size_t)S.max_blocks_per_cam * 24 * 4 <= 110 * 1024 ? 24 : 18;
       schur_smem = (size_t)S.max_blocks_per_cam * bd_stride * sizeof(Real);
       stage_in_smem = schur_smem <= 190 * 1024;
       if (!stage_in_smem) schur_smem = 0;
@@ -941,7 +964,7 @@ struct Engine final : EngineBase {
     const int* toff = to_tiles ? c->tile_off.p : nullptr;
     DenseOut dn{c->win_of_cam.p, c->win_cam.p, c->win_mat.p, to_windows ? c->win_scratch.p : nullptr};
     if (stage_in_smem) {
-      auto kern = schur_rows<Real, T, true, G>;
+      auto kern = schur_vec_loads() ? schur_rows<Real, T, true, G, true> : schur_rows<Real, T, true, G, false>;
       G2OC_TRY(raise_dyn_smem((const void*)kern, schur_smem));
       G2OC_K(K_SCHUR_BLOCKS) kern<<<nrows, T, schur_smem, st>>>(
           rows, c->hc_ptr.p, c->hc_blk.p, c->hc_col.p, hpl.p, dinv.p, bdc.p, c->sys_rptr.p, c->sys_rcol.p,
