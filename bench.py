@@ -826,7 +826,7 @@ def dense_cholesky_line(backend, fac, g, device, pcg_stats, iterations=3):
     pc.close()
     n = 6 * (g.num_poses - int(g.pose_fixed.sum()))
     nt = (n + 127) // 128
-    factorizations = d.get("tc_expand", (0, 0.0))[0]
+    factorizations = d.get("tc_potrf", (0, 0.0))[0] // max(nt, 1)
     tiles_per_factor = sum(m + m * (m + 1) // 2 for m in range(1, nt))
     mma_flops = factorizations * tiles_per_factor * 3 * 2 * 128 ** 3
     tiles_ms = d.get("tc_tiles", (0, 0.0))[1]

@@ -39,6 +39,7 @@ struct CholPlan {
   DBuf<int> d_pnl_ptr, d_upd_ptr, d_bwd_ptr;
   DBuf<double> A, y;
   DBuf<double> W;  // W(k) = L(k,k)^-1 per diagonal tile
+  DBuf<double> floor;  // pivot floor of the current factorization
   DBuf<int> info;
   // every step has at most kCholSingleWidth panel tiles plus trailing
   // updates: the whole plan runs in one CTA (chol_factor_single)
@@ -160,6 +161,7 @@ static int chol_plan_build(CholPlan& P, int nb, int bs, const std::vector<int32_
   G2OC_TRY(P.A.alloc((size_t)P.np * P.np));
   G2OC_TRY(P.y.alloc(P.np));
   G2OC_TRY(P.W.alloc((size_t)nt * kTile * kTile));
+  G2OC_TRY(P.floor.alloc(1));
   G2OC_TRY(P.info.alloc(1));
   return G2OC_OK;
 }
@@ -189,6 +191,24 @@ __global__ void chol_densify(SysDev<Real> S, int bs, const int* perm, int n, int
   }
 }
 
+// the pivot floor of a factorization: 4 n eps times the largest diagonal
+// entry of the (densified) matrix, one CTA of 1024 threads (fixed tree)
+template <typename Elem>
+static __global__ void __launch_bounds__(1024) chol_pivot_floor(const Elem* A, int np, int n, double* floor) {
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs((double)A[(size_t)i * np + i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, red[w]);
+    *floor = 4.0 * (double)n * 2.220446049250313e-16 * r;
+  }
+}
+
 // asynchronous 8-byte global -> shared copies (every load of a tile in
 // flight at once, instead of one round trip per loop step)
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
@@ -207,7 +227,8 @@ constexpr int kTileBuf = kTile * kLd;  // doubles per operand tile
 // factor the diagonal tile k in shared memory (lower; T: a tile buffer, used
 // with leading dimension kTile + 1) and form W = L(k,k)^-1 in Wsm (FP64
 // shared memory, column-major, leading dimension ldw); 256 threads
-__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* Wsm, int ldw, int* info) {
+__device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* Wsm, int ldw, int* info,
+                                                double floor) {
   constexpr int ld = kTile + 1;
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
@@ -216,7 +237,7 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
   }
   cp_async_wait_all();
   __syncthreads();
-  tile_potrf_inv_blk64(T, ld, Wsm, ldw, info);
+  tile_potrf_inv_blk64(T, ld, Wsm, ldw, info, floor);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
     if (i >= j) A[(base + j) * np + base + i] = T[i * ld + j];
@@ -225,11 +246,12 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
 
 // W(k) of every diagonal tile, kTile x kTile column-major, at W + k kTile^2
 constexpr int kPotrfSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
-static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, int* info) {
+static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, const double* floor,
+                                                         int* info) {
   extern __shared__ double sm_potrf[];
   double* T = sm_potrf;
   double* Wsm = sm_potrf + kTile * (kTile + 1);
-  chol_potrf_tile(A, np, k, T, Wsm, kTile + 1, info);
+  chol_potrf_tile(A, np, k, T, Wsm, kTile + 1, info, *floor);
   double* Wk = W + (size_t)k * kTile * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Wk[e] = Wsm[(e / kTile) * (kTile + 1) + e % kTile];
 }
@@ -237,39 +259,6 @@ static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int 
 constexpr int kTileSmem = 2 * kTileBuf * (int)sizeof(double);
 // chol_factor_single: two operand tiles and W
 constexpr int kTileSmemSingle = 3 * kTileBuf * (int)sizeof(double);
-
-// P = X Y^T over k = 0..63 on the FP64 tensor cores (mma.sync m8n8k4, 256
-// threads): warp w owns rows 16 (w % 4) .. + 16 and columns 32 (w / 4) .. + 32
-// of P as 2 x 4 fragments of 8 x 8; lane (g, t) = (lane / 4, lane % 4) holds
-// P(i0 + 8u + g, j0 + 8v + 2t + e) in acc[u][v][e]. X is an operand tile
-// (row, k); Y is one too when KMAJOR is false, else Y(j, k) is at
-// Ys[k * kLd + j]. The k sums run in a fixed order: bit-reproducible.
-template <bool KMAJOR>
-__device__ __forceinline__ void chol_dmma_tile(const double* Xs, const double* Ys, double (&acc)[2][4][2]) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
-#pragma unroll
-  for (int u = 0; u < 2; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v][0] = acc[u][v][1] = 0.0;
-#pragma unroll 4
-  for (int k0 = 0; k0 < kTile; k0 += 4) {
-    double fa[2], fb[4];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) fa[u] = Xs[(i0 + 8 * u + g) * kLd + k0 + t];
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      fb[v] = KMAJOR ? Ys[(k0 + t) * kLd + j0 + 8 * v + g] : Ys[(j0 + 8 * v + g) * kLd + k0 + t];
-#pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v)
-        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                     : "+d"(acc[u][v][0]), "+d"(acc[u][v][1])
-                     : "d"(fa[u]), "d"(fb[v]));
-  }
-}
 
 // an operand tile (row, k) from the column-major tile of A at rows rb,
 // columns cb (k = column)
@@ -288,7 +277,7 @@ __device__ __forceinline__ void chol_trsm_tile(double* A, int np, int k, int ti,
   cp_async_wait_all();
   __syncthreads();
   double acc[2][4][2];
-  chol_dmma_tile<true>(Xs, Ws, acc);  // Y(j, t) = W(j, t) at Ws[t * kLd + j]
+  tile_dmma64<false, true>(Xs, Ws, kLd, acc);  // Y(j, t) = W(j, t) at Ws[t * kLd + j]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
@@ -318,7 +307,7 @@ __device__ __forceinline__ void chol_gemm_tile(double* A, int np, int k, int2 ij
   cp_async_wait_all();
   __syncthreads();
   double acc[2][4][2];
-  chol_dmma_tile<false>(Li, Lj, acc);
+  tile_dmma64<false, false>(Li, Lj, kLd, acc);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int i0 = 16 * (w & 3), j0 = 32 * (w >> 2);
@@ -350,13 +339,15 @@ static __global__ void __launch_bounds__(256) chol_gemm(double* A, int np, int k
 // buffer.
 static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int np, int nt, const int* pnl_ptr,
                                                                  const int* pnl, const int* upd_ptr,
-                                                                 const int2* upd, double* W, int* info) {
+                                                                 const int2* upd, double* W, const double* floor,
+                                                                 int* info) {
   extern __shared__ double sm_single[];
   double* B0 = sm_single;
   double* B1 = sm_single + kTileBuf;
   double* Ws = sm_single + 2 * kTileBuf;
+  const double fl = *floor;
   for (int k = 0; k < nt; ++k) {
-    chol_potrf_tile(A, np, k, B0, Ws, kLd, info);
+    chol_potrf_tile(A, np, k, B0, Ws, kLd, info, fl);
     // W(k) kept for the substitutions (chol_solve_single)
     for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x)
       W[(size_t)k * kTile * kTile + e] = Ws[(e / kTile) * kLd + e % kTile];
@@ -520,15 +511,17 @@ static int chol_factor(CholPlan& P, cudaStream_t st, const SysDev<Real>& S, long
   G2OC_CUDA_TRY(cudaMemsetAsync(P.info.p, 0, sizeof(int), st));
   const long long work = (long long)nnzb * P.bs * P.bs + (np - P.n);
   chol_densify<Real><<<(int)((work + 255) / 256), 256, 0, st>>>(S, P.bs, P.d_perm.p, P.n, np, P.A.p);
+  chol_pivot_floor<double><<<1, 1024, 0, st>>>(P.A.p, np, P.n, P.floor.p);
+  *nl += 1;
   if (P.single) {
     G2OC_CUDA_TRY(
         cudaFuncSetAttribute(chol_factor_single, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemSingle));
     chol_factor_single<<<1, 256, kTileSmemSingle, st>>>(P.A.p, np, nt, P.d_pnl_ptr.p, P.d_pnl.p, P.d_upd_ptr.p,
-                                                        P.d_upd.p, P.W.p, P.info.p);
+                                                        P.d_upd.p, P.W.p, P.floor.p, P.info.p);
     *nl += 1;
   }
   for (int k = 0; k < (P.single ? 0 : nt); ++k) {
-    chol_potrf<<<1, 256, kPotrfSmem, st>>>(P.A.p, np, k, P.W.p, P.info.p);
+    chol_potrf<<<1, 256, kPotrfSmem, st>>>(P.A.p, np, k, P.W.p, P.floor.p, P.info.p);
     const int np_k = P.pnl_ptr[k + 1] - P.pnl_ptr[k];
     if (np_k > 0) chol_trsm<<<np_k, 256, kTileSmem, st>>>(P.A.p, np, k, P.d_pnl.p + P.pnl_ptr[k], P.W.p);
     const int nu = P.upd_ptr[k + 1] - P.upd_ptr[k];

@@ -491,21 +491,25 @@ static int schur_bd_stride() {
 }
 
 // FP32 Schur rows: gather each Hpl block with five aligned vector loads
-// instead of nine 8-byte loads (G2OC_SCHUR_VEC=1)
+// instead of nine 8-byte loads (the default: 229 vs 243 us per launch on the
+// BA configuration; G2OC_SCHUR_VEC=0 for the 8-byte loads)
 static bool schur_vec_loads() {
   static const int v = [] {
     const char* e = getenv("G2OC_SCHUR_VEC");
-    return e ? atoi(e) : 0;
+    return e ? atoi(e) : 1;
   }();
   return v != 0;
 }
 
-// order of a Schur row's off-diagonal blocks over its lane groups: 1 by
-// pair count dealt in alternating rounds (the default), 0 storage order
+// order of a Schur row's off-diagonal blocks over its lane groups: 0
+// storage order (the default), 1 by pair count dealt in alternating rounds
+// (measured slower: 249 vs 229 us per launch on the BA configuration, the
+// scattered block order costing more in the stores than it saves in lane
+// balance)
 static int schur_block_order() {
   static const int v = [] {
     const char* e = getenv("G2OC_SCHUR_BLOCK_ORDER");
-    return e ? atoi(e) : 1;
+    return e ? atoi(e) : 0;
   }();
   return v;
 }
@@ -1072,9 +1076,10 @@ struct Engine final : EngineBase {
       const long long total = (long long)P.np * P.np;
       G2OC_K(K_TC_EXPAND) tc_expand_tiles<<<cdiv(total, 256), 256, 0, st>>>(tiles.p, P.tile_index.p, P.nbt, P.n,
                                                                            P.np, P.A.p);
+      G2OC_K(K_TC_EXPAND) chol_pivot_floor<float><<<1, 1024, 0, st>>>(P.A.p, P.np, P.n, P.floor.p);
       for (int k = 0; k < P.nt; ++k) {
         float* Wk = P.W.p + (size_t)k * kTc * kTc;
-        G2OC_K(K_TC_POTRF) tc_potrf<<<1, 512, kTcPotrfSmem, st>>>(P.A.p, P.np, k, Wk, P.info.p);
+        G2OC_K(K_TC_POTRF) tc_potrf<<<1, 256, kTcPotrfSmem, st>>>(P.A.p, P.np, k, Wk, P.floor.p, P.info.p);
         const int p0 = P.list_ptr[2 * k], p1 = P.list_ptr[2 * k + 1], p2 = P.list_ptr[2 * k + 2];
         if (p1 > p0)
           G2OC_K(K_TC_TILES) tc_tiles<<<p1 - p0, 128, kTcSmem, st>>>(P.A.p, P.np, k, P.lists.p + p0, Wk, P.err.p);

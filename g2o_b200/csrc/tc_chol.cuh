@@ -46,7 +46,6 @@ constexpr int kTcK = 64;           // K per staged chunk
 constexpr int kTcOpBytes = kTc * kTcK * 4;        // one operand tile (hi or lo): 32 KB
 constexpr int kTcSmem = 4 * kTcOpBytes + 1024;    // A hi/lo, B hi/lo, barrier and TMEM address
 constexpr long long kTcSpinLimit = 1ll << 26;     // bounded waits (tens of ms at worst)
-constexpr size_t kTcPotrfSmem = (size_t)(kTc * (kTc + 1) + 3 * kTc) * sizeof(double);
 
 // ------------------------------------------------------------ PTX helpers
 __device__ __forceinline__ uint32_t tc_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -233,26 +232,98 @@ static __global__ void __launch_bounds__(128, 1)
 // ------------------------------------------------------------ diagonal tile
 // Factor the diagonal tile k in FP64 (lower), write L(k,k) back in FP32 and
 // W(k) = L(k,k)^-1 (FP32, column-major 128 x 128, zero above the diagonal)
-// to Wk. A non-positive pivot sets *info (the pivot is replaced by 1 so the
-// arithmetic stays finite). 512 threads as a 32 x 16 grid, each holding a
-// 4 x 8 interleaved sub-block of the tile in registers (tile_potrf_inv).
-static __global__ void __launch_bounds__(512, 1) tc_potrf(float* A, int np, int k, float* Wk, int* info) {
+// to Wk. The 128 x 128 tile is taken as 2 x 2 blocks of 64 (256 threads):
+//   L11 W11 = chol(A11)                    tile_potrf_inv_blk64
+//   L21 = A21 W11^T                        FP64 tensor-core product
+//   L22 W22 = chol(A22 - L21 L21^T)        product, then tile_potrf_inv_blk64
+//   W21 = -W22 (L21 W11)                   two products
+// A non-positive pivot sets *info (the pivot is replaced by 1 so the
+// arithmetic stays finite).
+constexpr int kTcLd = 68;                    // operand blocks, as tile_dmma64 reads them
+constexpr int kTcBlk = 64 * kTcLd;           // doubles per operand block
+constexpr int kTcTri = 64 * 65;              // doubles per diagonal block (leading dimension 65)
+constexpr size_t kTcPotrfSmem = (size_t)(2 * kTcTri + 3 * kTcBlk) * sizeof(double);
+
+static __global__ void __launch_bounds__(256, 1) tc_potrf(float* A, int np, int k, float* Wk, const double* floor,
+                                                           int* info) {
   extern __shared__ double tcp_smem[];
-  constexpr int LD = kTc + 1;
-  double* T = tcp_smem;                 // 128 x 129, row-major: T[i * 129 + j]
-  double* buf = tcp_smem + kTc * LD;    // two column vectors and the pivots' reciprocals
+  double* T1 = tcp_smem;                // A11 -> L11 (ld 65)
+  double* T2 = T1 + kTcTri;             // A22 -> L22
+  double* X = T2 + kTcTri;              // A21 -> L21 -> L21 W11 (ld kTcLd)
+  double* W1 = X + kTcBlk;              // W11 (column-major, ld kTcLd)
+  double* W2 = W1 + kTcBlk;             // W22
   const size_t kb = (size_t)k * kTc;
-  for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
-    const int i = e % kTc, j = e / kTc;
-    if (i >= j) T[i * LD + j] = (double)A[(kb + j) * np + kb + i];
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int i = e % 64, j = e / 64;
+    if (i >= j) {
+      T1[i * 65 + j] = (double)A[(kb + j) * np + kb + i];
+      T2[i * 65 + j] = (double)A[(kb + 64 + j) * np + kb + 64 + i];
+    }
+    X[i * kTcLd + j] = (double)A[(kb + j) * np + kb + 64 + i];
   }
   __syncthreads();
   int bad = 0;
-  tile_potrf_inv<kTc, 32, 16, float>(T, LD, buf, &bad, Wk, kTc);
+  const double fl = *floor;
+  tile_potrf_inv_blk64(T1, 65, W1, kTcLd, &bad, fl);
+  double acc[2][4][2];
+  // L21 = A21 W11^T (Y(j, t) = W11(j, t) at W1[t * ld + j])
+  tile_dmma64<false, true>(X, W1, kTcLd, acc);
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = tile_dmma64_row(u), c = tile_dmma64_col(v, e);
+        X[r * kTcLd + c] = acc[u][v][e];
+        A[(kb + c) * np + kb + 64 + r] = (float)acc[u][v][e];
+      }
+  __syncthreads();
+  // A22 -= L21 L21^T
+  tile_dmma64<false, false>(X, X, kTcLd, acc);
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = tile_dmma64_row(u), c = tile_dmma64_col(v, e);
+        if (r >= c) T2[r * 65 + c] -= acc[u][v][e];
+      }
+  __syncthreads();
+  tile_potrf_inv_blk64(T2, 65, W2, kTcLd, &bad, fl);
+  // M = L21 W11 (Y(c, t) = W11(t, c) at W1[c * ld + t]), into X
+  tile_dmma64<false, false>(X, W1, kTcLd, acc);
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) X[tile_dmma64_row(u) * kTcLd + tile_dmma64_col(v, e)] = acc[u][v][e];
+  __syncthreads();
+  // W21 = -W22 M (X(r, t) = W22(r, t) at W2[t * ld + r]; Y(c, t) = M(t, c) at X[t * ld + c])
+  tile_dmma64<true, true>(W2, X, kTcLd, acc);
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = tile_dmma64_row(u), c = tile_dmma64_col(v, e);
+        Wk[(size_t)c * kTc + 64 + r] = (float)(-acc[u][v][e]);
+      }
   if (threadIdx.x == 0 && bad) atomicExch(info, 1);
-  for (int e = threadIdx.x; e < kTc * kTc; e += blockDim.x) {
-    const int i = e % kTc, j = e / kTc;
-    if (i >= j) A[(kb + j) * np + kb + i] = (float)T[i * LD + j];
+  for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+    const int i = e % 64, j = e / 64;
+    if (i >= j) {
+      A[(kb + j) * np + kb + i] = (float)T1[i * 65 + j];
+      A[(kb + 64 + j) * np + kb + 64 + i] = (float)T2[i * 65 + j];
+    }
+    Wk[(size_t)j * kTc + i] = (float)W1[j * kTcLd + i];
+    Wk[(size_t)(64 + j) * kTc + 64 + i] = (float)W2[j * kTcLd + i];
+    Wk[(size_t)(64 + j) * kTc + i] = 0.0f;
   }
 }
 
@@ -337,6 +408,7 @@ struct TcChol {
   DBuf<float> A, W;
   DBuf<double> y;
   DBuf<int> info, err, tile_index;
+  DBuf<double> floor;  // pivot floor of the current factorization
   DBuf<int2> lists;                 // per step: panel tiles then update pairs
   std::vector<int> list_ptr;        // per step: [panel start, update start, end)
 };
@@ -366,6 +438,7 @@ static int tc_chol_plan(TcChol& P, int n, int nbt_tiles, const std::vector<int32
   G2OC_TRY(P.y.alloc(P.np));
   G2OC_TRY(P.info.alloc(1));
   G2OC_TRY(P.err.alloc(1));
+  G2OC_TRY(P.floor.alloc(1));
   return G2OC_OK;
 }
 
