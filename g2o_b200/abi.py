@@ -31,7 +31,8 @@ ERROR_NAMES = {
 
 POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
 EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_SE3_EXPMAP = 1, 2, 3, 4, 5
-BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
+EDGE_STEREO_SE3_PROJECT_XYZ = 6
+BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_STEREO_SE3_PROJECT_XYZ)
 ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG, ALGO_STRUCTURE_ONLY = 0, 1, 2, 3
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -39,8 +40,10 @@ RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2
 
 POSE_EST_DIM = {POSE_SE2: 3, POSE_SE3: 12, POSE_SE3EXPMAP: 7}
 POSE_DIM = {POSE_SE2: 3, POSE_SE3: 6, POSE_SE3EXPMAP: 6}
-EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 6}
-MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 7}
+EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 6,
+            EDGE_STEREO_SE3_PROJECT_XYZ: 3}
+MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 7,
+            EDGE_STEREO_SE3_PROJECT_XYZ: 3}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
@@ -65,6 +68,7 @@ class G2ocGraph(C.Structure):
         ("focal_length", C.c_double),
         ("principal_point", C.c_double * 2),
         ("focal_length_y", C.c_double),
+        ("stereo_bf", C.c_double),
     ]
 
 
@@ -188,7 +192,8 @@ class Graph:
     principal_point: tuple = (0.0, 0.0)
     name: str = ""
     extra: dict = field(default_factory=dict)
-    focal_length_y: Optional[float] = None  # EdgeSE3ProjectXYZ's fy (None: focal_length)
+    focal_length_y: Optional[float] = None  # fy of EdgeSE3ProjectXYZ / EdgeStereoSE3ProjectXYZ (None: focal_length)
+    stereo_bf: float = 0.0  # EdgeStereoSE3ProjectXYZ::bf (baseline times fx)
 
     def __post_init__(self):
         self.pose_estimate = np.ascontiguousarray(self.pose_estimate, dtype=np.float64)
@@ -228,7 +233,7 @@ class Graph:
                      c(self.measurement), c(self.information), c(self.pose_fixed),
                      c(self.point_estimate), c(self.point_fixed), c(self.robust_delta),
                      self.focal_length, tuple(self.principal_point), self.name, dict(self.extra),
-                     self.focal_length_y)
+                     self.focal_length_y, self.stereo_bf)
 
     def digest(self) -> str:
         """SHA-256 of the graph's types, arrays and intrinsics: equal digests
@@ -241,6 +246,8 @@ class Graph:
             h.update(b"-" if a is None else np.ascontiguousarray(a).tobytes())
         fy = self.focal_length if self.focal_length_y is None else self.focal_length_y
         h.update(np.array([self.focal_length, fy, *self.principal_point], np.float64).tobytes())
+        if self.edge_type == EDGE_STEREO_SE3_PROJECT_XYZ:
+            h.update(np.array([self.stereo_bf], np.float64).tobytes())
         return h.hexdigest()
 
     def to_c(self) -> G2ocGraph:
@@ -262,6 +269,7 @@ class Graph:
         g.principal_point[0] = float(self.principal_point[0])
         g.principal_point[1] = float(self.principal_point[1])
         g.focal_length_y = float(self.focal_length if self.focal_length_y is None else self.focal_length_y)
+        g.stereo_bf = float(self.stereo_bf)
         # keep the numpy arrays alive as long as the struct
         g._owner = self
         return g

@@ -24,7 +24,7 @@ from typing import List, Optional
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
+from .abi import (BA_EDGES, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, ERROR_NAMES, G2ocBackwardStats, G2ocGraph, G2ocHessianInfo,
                   G2ocIterationStats, G2ocKernelStat, G2ocParams, G2ocWindowStats, Graph, LINEAR_CHOLESKY, LINEAR_PCG,
                   POSE_DIM, POSE_EST_DIM)
 
@@ -225,7 +225,7 @@ class CudaProblem:
 
     @property
     def is_ba(self):
-        return self.graph.edge_type in (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
+        return self.graph.edge_type in BA_EDGES
 
     def set_params(self, params: G2ocParams):
         self.params = params

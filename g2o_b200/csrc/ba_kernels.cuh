@@ -34,6 +34,11 @@ struct BAEdges {
   const double2* z;       // measurement
   const double4* om;      // (Omega00, Omega01, Omega11, Huber delta; <= 0: none)
   const int* hpl;         // Hpl block per edge or -1
+  // stereo edges (stereo_kernels.cuh) instead of z / om: (u, v, u_right,
+  // Huber delta), (O00, O01, O02, O11), (O12, O22)
+  const double4* z3 = nullptr;
+  const double4* oa3 = nullptr;
+  const double2* ob3 = nullptr;
 };
 
 struct BACamEdges {       // camera-major copy of the edges of free cameras
@@ -41,6 +46,9 @@ struct BACamEdges {       // camera-major copy of the edges of free cameras
   const int2* v;
   const double2* z;
   const double4* om;
+  const double4* z3 = nullptr;  // stereo, as BAEdges
+  const double4* oa3 = nullptr;
+  const double2* ob3 = nullptr;
 };
 
 struct BAVertices {
@@ -49,6 +57,7 @@ struct BAVertices {
   const int* free_pose;   // Cf: pose index of Hessian row h
   const int* free_point;  // Pf: point index of landmark l
   double fx, fy, cx, cy;  // EdgeProjectXYZ2UV: fx = fy = focal_length
+  double bf = 0.0;        // EdgeStereoSE3ProjectXYZ::bf
 };
 
 // Per-edge residual, robust weight and weighted error in FP64.

@@ -26,6 +26,7 @@
 #include "pcg_persistent.cuh"
 #include "pcg_tiles.cuh"
 #include "tc_chol.cuh"
+#include "stereo_kernels.cuh"
 #include "pg_kernels.cuh"
 
 namespace g2oc {
@@ -167,7 +168,7 @@ struct g2oc_ctx {
   bool uploaded = false;
   bool last_upload_reused = false;  // the last g2oc_upload kept the structure (same topology)
   bool system_built = false;
-  double fx = 1, fy = 1, cx = 0, cy = 0;
+  double fx = 1, fy = 1, cx = 0, cy = 0, bf = 0;
   // vertex state
   g2oc::DBuf<double> pose, point, pose_bak, point_bak, pose_init, point_init;
   g2oc::DBuf<int> oplus_count, free_pose, free_point, pose_h, point_l;
@@ -175,6 +176,8 @@ struct g2oc_ctx {
   g2oc::DBuf<int2> e_v, c_v;
   g2oc::DBuf<double2> e_z, c_z;
   g2oc::DBuf<double4> e_om, c_om;
+  g2oc::DBuf<double4> e_z3, e_oa3, c_z3, c_oa3;  // stereo edges (stereo_kernels.cuh)
+  g2oc::DBuf<double2> e_ob3, c_ob3;
   g2oc::DBuf<int> e_hpl, e_lm, lm_chunk_ptr, l_ptr, c_ptr, hb_ptr, hpl_row, hpl_col, hc_ptr, hc_blk, hc_col, hc_index, s_pair_ptr, s_hpp;
   g2oc::DBuf<int2> s_pairs;
   // pose-graph edges
@@ -353,6 +356,7 @@ struct g2oc_ctx {
     V.fy = fy;
     V.cx = cx;
     V.cy = cy;
+    V.bf = bf;
     return V;
   }
   g2oc::BAEdges ba_edges() {
@@ -362,7 +366,17 @@ struct g2oc_ctx {
     E.z = e_z.p;
     E.om = e_om.p;
     E.hpl = e_hpl.p;
+    E.z3 = e_z3.p;
+    E.oa3 = e_oa3.p;
+    E.ob3 = e_ob3.p;
     return E;
+  }
+  g2oc::BACamEdges ba_cam_edges() {
+    g2oc::BACamEdges CE{c_ptr.p, c_v.p, c_z.p, c_om.p};
+    CE.z3 = c_z3.p;
+    CE.oa3 = c_oa3.p;
+    CE.ob3 = c_ob3.p;
+    return CE;
   }
   g2oc::PGEdges pg_edges() {
     g2oc::PGEdges E;
@@ -820,7 +834,18 @@ struct Engine final : EngineBase {
   int build_system() override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    if (S.ba) {
+    if (S.ba && S.D == 3) {
+      if (S.Pf > 0) {
+        G2OC_K(K_LANDMARK_PASS) st_landmark_pass<Real><<<cdiv(S.Pf, 128), 128, 0, st>>>(
+            c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, hll.p, hpl.p, c->b.p + (size_t)S.Cf * 6);
+        G2OC_LAUNCH_CHECK();
+      }
+      if (S.Cf > 0) {
+        G2OC_K(K_CAMERA_PASS) st_camera_pass<Real, 128><<<S.Cf, 128, 0, st>>>(c->ba_cam_edges(), c->ba_vertices(),
+                                                                              hpp.p, c->b.p);
+        G2OC_LAUNCH_CHECK();
+      }
+    } else if (S.ba) {
       if (S.Pf > 0 && S.lm_warp_ok) {
         const int nch = (int)S.lm_chunk_ptr.size() - 1;
         G2OC_K(K_LANDMARK_PASS) ba_landmark_warp<Real><<<cdiv(nch, 8), 256, 0, st>>>(
@@ -833,7 +858,7 @@ struct Engine final : EngineBase {
         G2OC_LAUNCH_CHECK();
       }
       if (S.Cf > 0) {
-        BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
+        BACamEdges CE = c->ba_cam_edges();
         G2OC_K(K_CAMERA_PASS) ba_camera_pass<Real, 128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), hpp.p, c->b.p);
         G2OC_LAUNCH_CHECK();
       }
@@ -1194,7 +1219,12 @@ struct Engine final : EngineBase {
         for (int k = 0; k <= c->prm.refine_max_iterations; ++k) {
           double* rp = c->resid.p;
           double* rl = c->resid.p + (size_t)S.Cf * 6;
-          if (S.Pf > 0 && S.lm_warp_ok) {
+          if (S.D == 3) {
+            if (S.Pf > 0)
+              G2OC_K(K_RESID_LM) st_resid64_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(
+                  c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, c->pose_h.p, lambda, bl, c->x.p,
+                  c->x.p + (size_t)S.Cf * 6, rl);
+          } else if (S.Pf > 0 && S.lm_warp_ok) {
             const int nch = (int)S.lm_chunk_ptr.size() - 1;
             G2OC_K(K_RESID_LM) ba_resid64_landmark_warp<<<cdiv(nch, 8), 256, 0, st>>>(
                 c->ba_edges(), c->ba_vertices(), c->lm_chunk_ptr.p, nch, c->e_lm.p, c->pose_h.p, lambda, bl, c->x.p,
@@ -1204,9 +1234,15 @@ struct Engine final : EngineBase {
                 c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, c->pose_h.p, lambda, bl, c->x.p,
                 c->x.p + (size_t)S.Cf * 6, rl);
           }
-          BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
-          G2OC_K(K_RESID_CAM) ba_resid64_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p, lambda,
-                                                                           bp, c->x.p, c->x.p + (size_t)S.Cf * 6, rp);
+          BACamEdges CE = c->ba_cam_edges();
+          if (S.D == 3)
+            G2OC_K(K_RESID_CAM) st_resid64_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p,
+                                                                             lambda, bp, c->x.p,
+                                                                             c->x.p + (size_t)S.Cf * 6, rp);
+          else
+            G2OC_K(K_RESID_CAM) ba_resid64_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p,
+                                                                             lambda, bp, c->x.p,
+                                                                             c->x.p + (size_t)S.Cf * 6, rp);
           G2OC_LAUNCH_CHECK();
           G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
           double check = 0.0, bound = 0.0;
@@ -1536,7 +1572,9 @@ struct Engine final : EngineBase {
 static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  if (S.ba && S.D == 3)
+    G2OC_K(K_CHI2) st_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  else if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE2><<<kRedBlocks, 256, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
@@ -1871,8 +1909,8 @@ static int dl_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
 
 static int structure_only(g2oc_ctx* c, int num_iters, int num_max_trials) {
   const Structure& S = c->S;
-  if (!S.ba) {
-    set_error("the structure-only solver optimizes the landmarks of a bundle adjustment");
+  if (!S.ba || S.D != 2) {
+    set_error("the structure-only solver optimizes the landmarks of a bundle adjustment with two-row projection edges");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   if (S.Pf == 0 || num_iters <= 0) return G2OC_OK;
@@ -2213,8 +2251,20 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
     G2OC_TRY(c->e_om.alloc(na));
     G2OC_TRY(c->c_z.alloc(nc));
     G2OC_TRY(c->c_om.alloc(nc));
-    G2OC_TRY(c->raw_meas.alloc((size_t)S.E * 2));
-    G2OC_TRY(c->raw_info.alloc((size_t)S.E * 4));
+    G2OC_TRY(c->raw_meas.alloc((size_t)S.E * S.md));
+    G2OC_TRY(c->raw_info.alloc((size_t)S.E * S.D * S.D));
+    if (S.D == 3) {
+      G2OC_TRY(c->e_z3.alloc(na));
+      G2OC_TRY(c->e_oa3.alloc(na));
+      G2OC_TRY(c->e_ob3.alloc(na));
+      G2OC_TRY(c->c_z3.alloc(nc));
+      G2OC_TRY(c->c_oa3.alloc(nc));
+      G2OC_TRY(c->c_ob3.alloc(nc));
+    } else {
+      for (auto* b : {&c->e_z3, &c->e_oa3, &c->c_z3, &c->c_oa3}) b->release();
+      c->e_ob3.release();
+      c->c_ob3.release();
+    }
     G2OC_TRY(c->raw_delta.alloc((size_t)S.E));
     G2OC_TRY(c->e_hpl.upload(S.e_hpl, st));
     G2OC_TRY(c->l_ptr.upload(S.l_ptr, st));
@@ -2312,7 +2362,10 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
   cudaStream_t st = c->stream;
   const int na = (int)S.act.size();
   c->fx = g->focal_length;
-  c->fy = g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? g->focal_length_y : g->focal_length;
+  c->fy = (g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ || g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
+              ? g->focal_length_y
+              : g->focal_length;
+  c->bf = g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ ? g->stereo_bf : 0.0;
   c->cx = g->principal_point[0];
   c->cy = g->principal_point[1];
   if (S.ba) {
@@ -2323,7 +2376,12 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
       if (g->robust_delta)
         G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_delta.p, g->robust_delta, c->raw_delta.bytes(), cudaMemcpyHostToDevice, st));
       const int nc = (int)S.c_edge.size();
-      if (na + nc > 0) {
+      if (na + nc > 0 && S.D == 3) {
+        G2OC_K(K_IO) st_gather_edges<<<cdiv((long long)na + nc, 256), 256, 0, st>>>(
+            na, nc, c->src_dev.p, c->src_cam.p, c->raw_meas.p, c->raw_info.p, g->robust_delta ? c->raw_delta.p : nullptr,
+            c->e_z3.p, c->e_oa3.p, c->e_ob3.p, c->c_z3.p, c->c_oa3.p, c->c_ob3.p);
+        G2OC_LAUNCH_CHECK();
+      } else if (na + nc > 0) {
         G2OC_K(K_IO) ba_gather_edges<<<cdiv((long long)na + nc, 256), 256, 0, st>>>(
             na, nc, c->src_dev.p, c->src_cam.p, c->raw_meas.p, c->raw_info.p, g->robust_delta ? c->raw_delta.p : nullptr,
             c->e_z.p, c->e_om.p, c->c_z.p, c->c_om.p);
@@ -2581,7 +2639,9 @@ int g2oc_errors(g2oc_ctx* c, double* out) {
   if (!out) return G2OC_ERR_INVALID_ARGUMENT;
   const Structure& S = c->S;
   const int na = (int)S.act.size();
-  if (S.ba) G2OC_K(K_ERRORS) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
+  if (S.ba && S.D == 3)
+    G2OC_K(K_ERRORS) st_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
+  else if (S.ba) G2OC_K(K_ERRORS) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
   else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
@@ -2606,7 +2666,9 @@ int g2oc_jacobians(g2oc_ctx* c, double* j0, double* j1) {
   DBuf<double> a, b;
   G2OC_TRY(a.alloc((size_t)na * D * d0));
   G2OC_TRY(b.alloc((size_t)na * D * d1));
-  if (S.ba) G2OC_K(K_JACOBIANS) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
+  if (S.ba && S.D == 3)
+    G2OC_K(K_JACOBIANS) st_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
+  else if (S.ba) G2OC_K(K_JACOBIANS) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_JACOBIANS) pg_jacobians_kernel<G2OC_POSE_SE2><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), a.p, b.p);
   else if (S.pose_type == G2OC_POSE_SE3EXPMAP)
@@ -2734,7 +2796,7 @@ static int adj_hessian_product(g2oc_ctx* c, const double* p, double* q) {
     G2OC_K(K_BACKWARD) ba_hvp_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->l_ptr.p,
                                                                         S.Pf, c->pose_h.p, S.Cf, p, q);
   }
-  BACamEdges CE{c->c_ptr.p, c->c_v.p, c->c_z.p, c->c_om.p};
+  BACamEdges CE = c->ba_cam_edges();
   G2OC_K(K_BACKWARD) ba_hvp_camera<128><<<S.Cf, 128, 0, st>>>(CE, c->ba_vertices(), c->point_l.p, S.Cf, p, q);
   G2OC_LAUNCH_CHECK();
   return G2OC_OK;
@@ -2763,8 +2825,8 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
     return G2OC_ERR_INVALID_ARGUMENT;
   }
   const Structure& S = c->S;
-  if (!S.ba || !S.schur || S.Cf == 0) {
-    set_error("g2oc_backward supports bundle adjustment (EdgeProjectXYZ2UV) with free cameras and landmarks");
+  if (!S.ba || !S.schur || S.Cf == 0 || S.D != 2) {
+    set_error("g2oc_backward supports bundle adjustment with two-row projection edges, free cameras and landmarks");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   cudaStream_t st = c->stream;

@@ -19,9 +19,16 @@ namespace g2oc {
 
 namespace {
 
-int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP) ? 6 : 2; }
+int edge_dim(int et) {
+  return (et == G2OC_EDGE_SE2 || et == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ) ? 3
+         : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP)          ? 6
+                                                                          : 2;
+}
 int meas_dim(int et) {
-  return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : et == G2OC_EDGE_SE3_EXPMAP ? 7 : 2;
+  return (et == G2OC_EDGE_SE2 || et == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ) ? 3
+         : et == G2OC_EDGE_SE3                                           ? 12
+         : et == G2OC_EDGE_SE3_EXPMAP                                    ? 7
+                                                                         : 2;
 }
 int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
 int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
@@ -261,7 +268,9 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
       for (int k = s.l_ptr[l] + 1; k < s.l_ptr[l + 1] && ok; ++k)
         if (s.e_hpl[k] >= 0 && s.e_hpl[k] == s.e_hpl[k - 1]) ok = false;
     }
-    s.lm_warp_ok = ok && s.Pf > 0;
+    // (the edge-parallel passes are written for the two-row projection
+    // edges; the stereo edge's landmarks take the thread-per-landmark ones)
+    s.lm_warp_ok = ok && s.Pf > 0 && s.D == 2;
     s.lm_chunk_ptr.clear();
     s.e_lm.clear();
     if (s.lm_warp_ok) {
@@ -546,8 +555,9 @@ int build_structure(const g2oc_graph* g, Structure& s) {
     set_error("graph is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
-  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 5 ||
+  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ||
+                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ;
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 6 ||
       (g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2) ||
       (g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3) ||
       (ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {

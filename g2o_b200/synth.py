@@ -23,7 +23,8 @@ import math
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_EXPMAP, EDGE_SE3_PROJECT_XYZ, EDGE_SE3, POSE_SE2, POSE_SE3,
+from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_EXPMAP, EDGE_SE3_PROJECT_XYZ, EDGE_SE3,
+                  EDGE_STEREO_SE3_PROJECT_XYZ, POSE_SE2, POSE_SE3,
                   POSE_SE3EXPMAP, Graph)
 
 SEED_BASE = 20261203
@@ -395,6 +396,32 @@ def bundle_adjustment(num_cameras=1000, num_points=200_000, ring_radius=30.0, he
     g.extra["truth_point"] = Xt
     g.extra["outliers"] = out
     return g
+
+
+def stereo_bundle_adjustment(num_cameras=100, num_points=20_000, baseline=0.12, focal=500.0, right_noise=0.5,
+                             seed=SEED_BASE + 5, **kw):
+    """EdgeStereoSE3ProjectXYZ (ORB-SLAM's stereo form): the ring bundle
+    adjustment with fx = fy = focal and a right-image coordinate per
+    observation, u_r = u - bf / z with bf = baseline * focal (z the true
+    depth), plus its own pixel noise; information I_3, Huber on every edge."""
+    g = bundle_adjustment(num_cameras=num_cameras, num_points=num_points, focal=focal, focal_y=focal, seed=seed, **kw)
+    rng = np.random.default_rng(seed + 7919)
+    tp, X = g.extra["truth_pose"], g.extra["truth_point"]
+    R = _quat_to_rot(tp[:, 3:7])
+    pts, cams = g.edge_vertex[:, 0], g.edge_vertex[:, 1]
+    z = ((R[cams, 2, 0] * X[pts, 0] + R[cams, 2, 1] * X[pts, 1]) + R[cams, 2, 2] * X[pts, 2]) + tp[cams, 2]
+    bf = baseline * focal
+    E = g.num_edges
+    meas = np.empty((E, 3))
+    meas[:, :2] = g.measurement
+    meas[:, 2] = g.measurement[:, 0] - bf / z + rng.normal(0.0, right_noise, E)
+    info = np.tile(np.eye(3).reshape(1, 9), (E, 1))
+    s = Graph(POSE_SE3EXPMAP, EDGE_STEREO_SE3_PROJECT_XYZ, g.pose_estimate, g.edge_vertex, meas, info,
+              pose_fixed=g.pose_fixed, point_estimate=g.point_estimate, point_fixed=g.point_fixed,
+              robust_delta=np.full(E, math.sqrt(7.815)), focal_length=focal, principal_point=g.principal_point,
+              name=f"stereo_bundle_adjustment_{num_cameras}x{g.num_points}", focal_length_y=focal, stereo_bf=bf)
+    s.extra = dict(g.extra)
+    return s
 
 
 def window_sizes(num_windows=512, cameras=(10, 60), points=(500, 8000), seed=SEED_BASE + 1000):

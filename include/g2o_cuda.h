@@ -97,6 +97,10 @@ extern "C" {
                                  SE3Quat (7, toVector: the edge's _measurement, not the file's inverse) */
 #define G2OC_EDGE_SE3_PROJECT_XYZ 4 /* EdgeSE3ProjectXYZ(VertexPointXYZ, VertexSE3Expmap), D=2, with
                                      fx = focal_length, fy = focal_length_y, (cx, cy) = principal_point */
+#define G2OC_EDGE_STEREO_SE3_PROJECT_XYZ 6 /* EdgeStereoSE3ProjectXYZ(VertexPointXYZ, VertexSE3Expmap), D=3,
+                                            measurement (u_left, v_left, u_right); fx, fy, (cx, cy) as
+                                            SE3_PROJECT_XYZ and bf = stereo_bf
+                                            (g2o/types/sba/edge_project_stereo_xyz.h:38-77) */
 
 /* algorithm / linear solver / precision */
 #define G2OC_ALGO_GAUSS_NEWTON 0
@@ -135,7 +139,8 @@ typedef struct g2oc_graph {
   const double* robust_delta;  /* num_edges Huber deltas; <= 0 or NULL: no kernel */
   double focal_length;         /* CameraParameters (PROJECT_XYZ2UV); fx of SE3_PROJECT_XYZ */
   double principal_point[2];
-  double focal_length_y;       /* fy of SE3_PROJECT_XYZ (EdgeSE3ProjectXYZ::fy); ignored otherwise */
+  double focal_length_y;       /* fy of SE3_PROJECT_XYZ and STEREO_SE3_PROJECT_XYZ; ignored otherwise */
+  double stereo_bf;            /* EdgeStereoSE3ProjectXYZ::bf (baseline times fx); ignored otherwise */
 } g2oc_graph;
 
 typedef struct g2oc_params {

@@ -401,12 +401,29 @@ bool inverse_small(const double* A, int n, double* out) {
 
 // ---------------------------------------------------------- edge functions
 
-int edge_dim(int et) { return et == G2OC_EDGE_SE2 ? 3 : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP) ? 6 : 2; }
+int edge_dim(int et) {
+  return (et == G2OC_EDGE_SE2 || et == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ) ? 3
+         : (et == G2OC_EDGE_SE3 || et == G2OC_EDGE_SE3_EXPMAP)          ? 6
+                                                                          : 2;
+}
 int meas_dim(int et) {
-  return et == G2OC_EDGE_SE2 ? 3 : et == G2OC_EDGE_SE3 ? 12 : et == G2OC_EDGE_SE3_EXPMAP ? 7 : 2;
+  return (et == G2OC_EDGE_SE2 || et == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ) ? 3
+         : et == G2OC_EDGE_SE3                                           ? 12
+         : et == G2OC_EDGE_SE3_EXPMAP                                    ? 7
+                                                                         : 2;
 }
 int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
 int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
+
+// EdgeStereoSE3ProjectXYZ (g2o/types/sba/edge_project_stereo_xyz.h:52-57,
+// edge_project_stereo_xyz.cpp:34-43 and 58-106), vertex0 = point, vertex1 =
+// camera. cam_project takes bf as a float reference, so the right image
+// coordinate uses bf rounded to single precision; invz = 1.0f / z is a double
+// division. The Jacobians keep bf in double precision.
+void stereo_error(const double* cam7, const double* X, const double* z, double fx, double fy, double cx, double cy,
+                  double bf, double e[3]);
+void stereo_jacobians(const double* cam7, const double* X, double fx, double fy, double bf, double Jp[9],
+                      double Jc[18]);
 
 struct SE2v {
   double x, y, th;
@@ -444,6 +461,55 @@ void ba_error(const double* cam7, const double* X, const double* z, double fx, d
   const double v = Xc[1] / Xc[2] * fy + cy;
   e[0] = z[0] - u;
   e[1] = z[1] - v;
+}
+
+void stereo_error(const double* cam7, const double* X, const double* z, double fx, double fy, double cx, double cy,
+                  double bf, double e[3]) {
+  SE3Q T = se3q_load(cam7);
+  double Xc[3];
+  quat_rotate(T.q, X, Xc);
+  Xc[0] += T.t[0]; Xc[1] += T.t[1]; Xc[2] += T.t[2];
+  const double invz = 1.0 / Xc[2];
+  const double u = Xc[0] * invz * fx + cx;
+  const double v = Xc[1] * invz * fy + cy;
+  const double ur = u - (double)(float)bf * invz;
+  e[0] = z[0] - u;
+  e[1] = z[1] - v;
+  e[2] = z[2] - ur;
+}
+
+void stereo_jacobians(const double* cam7, const double* X, double fx, double fy, double bf, double Jp[9],
+                      double Jc[18]) {
+  SE3Q T = se3q_load(cam7);
+  double Xc[3];
+  quat_rotate(T.q, X, Xc);
+  Xc[0] += T.t[0]; Xc[1] += T.t[1]; Xc[2] += T.t[2];
+  const double x = Xc[0], y = Xc[1], z = Xc[2], z2 = z * z;
+  double R[9];
+  quat_to_rot(T.q, R);
+  for (int c = 0; c < 3; ++c) {
+    Jp[c] = -fx * R[c] / z + fx * x * R[6 + c] / z2;
+    Jp[3 + c] = -fy * R[3 + c] / z + fy * y * R[6 + c] / z2;
+    Jp[6 + c] = Jp[c] - bf * R[6 + c] / z2;
+  }
+  Jc[0] = x * y / z2 * fx;
+  Jc[1] = -(1 + (x * x / z2)) * fx;
+  Jc[2] = y / z * fx;
+  Jc[3] = -1. / z * fx;
+  Jc[4] = 0;
+  Jc[5] = x / z2 * fx;
+  Jc[6] = (1 + y * y / z2) * fy;
+  Jc[7] = -x * y / z2 * fy;
+  Jc[8] = -x / z * fy;
+  Jc[9] = 0;
+  Jc[10] = -1. / z * fy;
+  Jc[11] = y / z2 * fy;
+  Jc[12] = Jc[0] - bf * y / z2;
+  Jc[13] = Jc[1] + bf * x / z2;
+  Jc[14] = Jc[2];
+  Jc[15] = Jc[3];
+  Jc[16] = 0;
+  Jc[17] = Jc[5] - bf / z2;
 }
 
 void ba_jacobians(const double* cam7, const double* X, double fx, double fy, double Jp[6], double Jc[12]) {
@@ -831,7 +897,7 @@ struct orc_problem {
   std::vector<uint8_t> pose_fixed, point_fixed;
   std::vector<int> ev;
   std::vector<double> meas, info, delta;
-  double fx = 1, fy = 1, cx = 0, cy = 0;
+  double fx = 1, fy = 1, cx = 0, cy = 0, bf = 0;
   bool ba = false;  // EdgeProjectXYZ2UV or EdgeSE3ProjectXYZ
   std::vector<int> oplus_count;  // VertexSE3 orthogonalization counter
   // active sets and index mapping (sparse_optimizer.cpp:175-287)
@@ -873,7 +939,9 @@ inline double* point_ptr(orc_problem* p, int i) { return p->point.data() + (size
 void compute_edge_error(orc_problem* p, int e, double* out) {
   const int v0 = p->ev[2 * e], v1 = p->ev[2 * e + 1];
   const double* m = p->meas.data() + (size_t)e * p->md;
-  if (p->ba)
+  if (p->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
+    stereo_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->fx, p->fy, p->cx, p->cy, p->bf, out);
+  else if (p->ba)
     ba_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->fx, p->fy, p->cx, p->cy, out);
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_error(pose_ptr(p, v0), pose_ptr(p, v1), m, out);
@@ -885,7 +953,9 @@ void compute_edge_error(orc_problem* p, int e, double* out) {
 void compute_edge_jac(orc_problem* p, int e, double* J0, double* J1) {
   const int v0 = p->ev[2 * e], v1 = p->ev[2 * e + 1];
   const double* m = p->meas.data() + (size_t)e * p->md;
-  if (p->ba)
+  if (p->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
+    stereo_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->fx, p->fy, p->bf, J0, J1);
+  else if (p->ba)
     ba_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->fx, p->fy, J0, J1);
   else if (p->edge_type == G2OC_EDGE_SE2)
     se2_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), m, J0, J1);
@@ -1703,8 +1773,9 @@ int orc_set_threads(int n) {
 int orc_create(const g2oc_graph* g, orc_problem** out) {
   if (!g || !out) return G2OC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 5) return G2OC_ERR_BAD_GRAPH;
+  const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ||
+                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ;
+  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 6) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2)) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3)) return G2OC_ERR_BAD_GRAPH;
   if ((ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) return G2OC_ERR_BAD_GRAPH;
@@ -1741,7 +1812,10 @@ int orc_create(const g2oc_graph* g, orc_problem** out) {
   if (g->robust_delta) p->delta.assign(g->robust_delta, g->robust_delta + p->E);
   p->ba = ba;
   p->fx = g->focal_length;
-  p->fy = g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ? g->focal_length_y : g->focal_length;
+  p->fy = (g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ || g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
+              ? g->focal_length_y
+              : g->focal_length;
+  p->bf = g->stereo_bf;
   p->cx = g->principal_point[0];
   p->cy = g->principal_point[1];
   p->oplus_count.assign(p->C, 0);

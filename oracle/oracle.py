@@ -12,7 +12,7 @@ import subprocess
 
 import numpy as np
 
-from g2o_b200.abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, G2ocHessianInfo, G2ocIterationStats, G2ocParams,
+from g2o_b200.abi import (BA_EDGES, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, G2ocHessianInfo, G2ocIterationStats, G2ocParams,
                           Graph, POSE_DIM, POSE_EST_DIM)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -111,7 +111,7 @@ class OracleProblem:
 
     @property
     def is_ba(self):
-        return self.graph.edge_type in (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ)
+        return self.graph.edge_type in BA_EDGES
 
     def estimates(self):
         g = self.graph

@@ -232,6 +232,28 @@ def test_projection_jacobians_match_numeric(oracle_lib, focal_y):
         np.testing.assert_allclose(a1[:, 1], b1[:, 1] * (455.0 / 500.0), rtol=1e-12)
 
 
+def test_stereo_projection_jacobians_match_numeric(oracle_lib):
+    """EdgeStereoSE3ProjectXYZ (g2o/types/sba/edge_project_stereo_xyz.cpp:58-106):
+    the analytic 3 x 3 and 3 x 6 Jacobians against central differences
+    (step 1e-9, BaseFixedSizedEdge's numeric form); the right row differs
+    from the left u row by the bf terms only."""
+    from g2o_b200 import synth
+    g = synth.stereo_bundle_adjustment(num_cameras=12, num_points=400, seed=17)
+    p = oracle_lib.OracleProblem(g)
+    a0, a1 = p.jacobians()
+    n0, n1 = p.jacobians(numeric=True)
+    assert a0.shape[1:] == (3, 3) and a1.shape[1:] == (3, 6)
+    for a, n in ((a0, n0), (a1, n1)):
+        assert np.abs(a - n).max() <= 1e-5 * max(1.0, np.abs(a).max())
+    g2 = g.copy()
+    g2.stereo_bf = 0.0
+    b0, b1 = oracle_lib.OracleProblem(g2).jacobians()
+    np.testing.assert_array_equal(b0[:, 2], b0[:, 0])
+    np.testing.assert_array_equal(b1[:, 2, [2, 3]], b1[:, 0, [2, 3]])
+    np.testing.assert_array_equal(a0[:, :2], b0[:, :2])
+    np.testing.assert_array_equal(a1[:, :2], b1[:, :2])
+
+
 def test_edge_se3_expmap_error_and_jacobians(oracle_lib):
     """EdgeSE3Expmap (g2o/types/sba/edge_se3_expmap.cpp:45-72): with T_i = I
     and C = I the error log(T_j^-1 C T_i) of T_j = exp(u)^-1 is u itself
