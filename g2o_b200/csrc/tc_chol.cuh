@@ -117,25 +117,29 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // stage a 128 (MN) x 64 (K) FP32 sub-tile of a column-major matrix (column
-// j of the sub-tile at G + j * ld, 16-byte aligned) as hi / lo TF32 parts in
-// the K-major layout above. Each thread reads four consecutive rows of one
-// column (a warp: four 64-byte runs of each of eight columns) and writes
-// them to the four rows' K slots.
+// j of the sub-tile at G + j * ld) as hi / lo TF32 parts in the K-major layout
+// above. One core matrix (8 rows x 4 K values, 32 consecutive words of shared
+// memory) per warp instruction: lane l takes row 8 mg + l / 4 and K value
+// 4 kg + l % 4, so each store covers the 32 banks once, and each load reads
+// four 32-byte column runs. Eight core matrices per loop step, their loads in
+// flight together.
 __device__ __forceinline__ void tc_stage(const float* G, size_t ld, unsigned char* hi, unsigned char* lo) {
-  for (int q = threadIdx.x; q < kTc * kTcK / 4; q += blockDim.x) {
-    const int lane = q & 31, w = q >> 5;
-    const int j = (w & 7) * 8 + (lane & 7);
-    const int g = (w >> 3) * 4 + (lane >> 3);
-    const float4 v = *reinterpret_cast<const float4*>(G + (size_t)j * ld + g * 4);
-    const float x[4] = {v.x, v.y, v.z, v.w};
-    const uint32_t kofs = (uint32_t)(j & 3) * 4 + (uint32_t)(j >> 2) * 2048;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int r = lane >> 2, kk = lane & 3;
+  for (int cm0 = warp * 8; cm0 < 256; cm0 += nw * 8) {
+    float x[8];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int i = g * 4 + c;
-      const uint32_t off = (uint32_t)(i & 7) * 16 + (uint32_t)(i >> 3) * 128 + kofs;
-      const float h = tc_tf32(x[c]);
+    for (int u = 0; u < 8; ++u) {
+      const int cm = cm0 + u, mg = cm & 15, kg = cm >> 4;
+      x[u] = G[(size_t)(4 * kg + kk) * ld + 8 * mg + r];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int cm = cm0 + u, mg = cm & 15, kg = cm >> 4;
+      const uint32_t off = (uint32_t)mg * 128 + (uint32_t)kg * 2048 + (uint32_t)lane * 4;
+      const float h = tc_tf32(x[u]);
       *reinterpret_cast<float*>(hi + off) = h;
-      *reinterpret_cast<float*>(lo + off) = tc_tf32(x[c] - h);
+      *reinterpret_cast<float*>(lo + off) = tc_tf32(x[u] - h);
     }
   }
 }
