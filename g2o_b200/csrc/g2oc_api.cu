@@ -445,10 +445,10 @@ static void coop_register(g2oc_ctx* c, int delta) {
   }
 }
 
-static int coop_launch(g2oc_ctx* c, const void* fn, int grid, int threads, void** args) {
+static int coop_launch(g2oc_ctx* c, const void* fn, int grid, int threads, void** args, size_t smem = 0) {
   cudaStream_t st = c->stream;
   if (c->device < 0 || c->device >= 64) {
-    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, smem, st));
     return G2OC_OK;
   }
   CoopChain& ch = g_coop[c->device];
@@ -456,12 +456,12 @@ static int coop_launch(g2oc_ctx* c, const void* fn, int grid, int threads, void*
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   G2OC_CUDA_TRY(cudaStreamIsCapturing(st, &cap));
   if (ch.live <= 1 || cap != cudaStreamCaptureStatusNone) {  // alone, or inside a graph capture
-    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+    G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, smem, st));
     return G2OC_OK;
   }
   if (!c->coop_done) G2OC_CUDA_TRY(cudaEventCreateWithFlags(&c->coop_done, cudaEventDisableTiming));
   if (ch.last && ch.owner != c) G2OC_CUDA_TRY(cudaStreamWaitEvent(st, ch.last, 0));
-  G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, st));
+  G2OC_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, smem, st));
   G2OC_CUDA_TRY(cudaEventRecord(c->coop_done, st));
   ch.owner = c;
   ch.last = c->coop_done;
@@ -511,6 +511,16 @@ static bool schur_vec_loads() {
   static const int v = [] {
     const char* e = getenv("G2OC_SCHUR_VEC");
     return e ? atoi(e) : 1;
+  }();
+  return v != 0;
+}
+
+// tensor-core Cholesky substitutions: one cooperative launch per direction
+// (the default) or two launches per tile step (G2OC_TC_SOLVE=launches)
+static bool tc_solve_coop_on() {
+  static const int v = [] {
+    const char* e = getenv("G2OC_TC_SOLVE");
+    return e && strcmp(e, "launches") == 0 ? 0 : 1;
   }();
   return v != 0;
 }
@@ -1130,6 +1140,36 @@ struct Engine final : EngineBase {
     TcChol& P = *tc;
     cudaStream_t st = c->stream;
     G2OC_K(K_TC_SOLVE) tc_load_rhs<<<cdiv(P.np, 256), 256, 0, st>>>(rhs, P.n, P.np, P.y.p);
+    if (tc_solve_coop_on()) {
+      // one cooperative launch per direction (a grid barrier per tile step)
+      int sms = 0;
+      G2OC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+      G2OC_TRY(raise_dyn_smem((const void*)tc_solve_coop, kTcSolveSmem));
+      int grid = std::min(sms, std::max(4 * (P.nt - 1), 1));
+      const float* A = P.A.p;
+      const float* W = P.W.p;
+      int np = P.np, nt = P.nt;
+      double* y = P.y.p;
+      PcgState* stp = P.sync.p;
+      unsigned extra = c->barrier_extra;
+      for (int dir = 0; dir < 2; ++dir) {
+        G2OC_CUDA_TRY(cudaMemsetAsync(P.sync.p, 0, sizeof(PcgState), st));
+        void* args[] = {&A, &W, &np, &nt, &y, &stp, &extra, &dir};
+        G2OC_K(K_TC_SOLVE) {
+          G2OC_TRY(coop_launch(c, (const void*)tc_solve_coop, grid, kTcSolveThreads, args, kTcSolveSmem));
+        }
+      }
+      G2OC_LAUNCH_CHECK();
+      int bad = 0;
+      G2OC_CUDA_TRY(cudaMemcpyAsync(&bad, &P.sync.p->sync_error, sizeof(int), cudaMemcpyDeviceToHost, st));
+      G2OC_CUDA_TRY(cudaStreamSynchronize(st));
+      if (bad) {
+        set_error("tensor-core Cholesky: a grid barrier of the substitutions gave up");
+        return G2OC_ERR_TIMEOUT;
+      }
+      G2OC_CUDA_TRY(cudaMemcpyAsync(xout, P.y.p, (size_t)P.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      return G2OC_OK;
+    }
     for (int k = 0; k < P.nt; ++k) {
       G2OC_K(K_TC_SOLVE) tc_apply_w<<<1, kTc, 0, st>>>(P.W.p + (size_t)k * kTc * kTc, P.y.p, k, false);
       if (k + 1 < P.nt) G2OC_K(K_TC_SOLVE) tc_fwd_update<<<P.nt - k - 1, kTc, 0, st>>>(P.A.p, P.np, k, P.y.p);

@@ -37,6 +37,7 @@
 #include <vector>
 
 #include "g2oc_internal.h"
+#include "pcg_persistent.cuh"
 #include "tile_potrf.cuh"
 
 namespace g2oc {
@@ -116,30 +117,41 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
   for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(r[t]);
 }
 
-// stage a 128 (MN) x 64 (K) FP32 sub-tile of a column-major matrix (column
-// j of the sub-tile at G + j * ld) as hi / lo TF32 parts in the K-major layout
-// above. One core matrix (8 rows x 4 K values, 32 consecutive words of shared
-// memory) per warp instruction: lane l takes row 8 mg + l / 4 and K value
-// 4 kg + l % 4, so each store covers the 32 banks once, and each load reads
-// four 32-byte column runs. Eight core matrices per loop step, their loads in
-// flight together.
-__device__ __forceinline__ void tc_stage(const float* G, size_t ld, unsigned char* hi, unsigned char* lo) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int r = lane >> 2, kk = lane & 3;
-  for (int cm0 = warp * 8; cm0 < 256; cm0 += nw * 8) {
-    float x[8];
+// stage the two 128 (MN) x 64 (K) FP32 operand sub-tiles of a tile product
+// (column j of a sub-tile at G + j * ld) as hi / lo TF32 parts in the K-major
+// layout above. One core matrix (8 rows x 4 K values, 32 consecutive words
+// of shared memory) per warp instruction: lane l takes row 8 mg + l / 4 and
+// K value 4 kg + l % 4, so each store covers the 32 banks once and each load
+// reads four 32-byte column runs. Each warp takes 64 core matrices of each
+// operand, 32 of each per round with all 64 loads in flight (the loads are
+// what the staging waits on).
+__device__ __forceinline__ void tc_stage_cm(const float* G, size_t ld, int cm, int lane, float& x) {
+  const int mg = cm & 15, kg = cm >> 4;
+  x = G[(size_t)(4 * kg + (lane & 3)) * ld + 8 * mg + (lane >> 2)];
+}
+__device__ __forceinline__ void tc_store_cm(unsigned char* hi, unsigned char* lo, int cm, int lane, float x) {
+  const int mg = cm & 15, kg = cm >> 4;
+  const uint32_t off = (uint32_t)mg * 128 + (uint32_t)kg * 2048 + (uint32_t)lane * 4;
+  const float h = tc_tf32(x);
+  *reinterpret_cast<float*>(hi + off) = h;
+  *reinterpret_cast<float*>(lo + off) = tc_tf32(x - h);
+}
+__device__ __forceinline__ void tc_stage2(const float* GA, size_t lda, const float* GB, size_t ldb, unsigned char* a_hi,
+                                          unsigned char* a_lo, unsigned char* b_hi, unsigned char* b_lo) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 4 warps
+#pragma unroll 1
+  for (int rnd = 0; rnd < 2; ++rnd) {
+    const int cm0 = warp * 64 + rnd * 32;
+    float xa[32], xb[32];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int cm = cm0 + u, mg = cm & 15, kg = cm >> 4;
-      x[u] = G[(size_t)(4 * kg + kk) * ld + 8 * mg + r];
+    for (int u = 0; u < 32; ++u) {
+      tc_stage_cm(GA, lda, cm0 + u, lane, xa[u]);
+      tc_stage_cm(GB, ldb, cm0 + u, lane, xb[u]);
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int cm = cm0 + u, mg = cm & 15, kg = cm >> 4;
-      const uint32_t off = (uint32_t)mg * 128 + (uint32_t)kg * 2048 + (uint32_t)lane * 4;
-      const float h = tc_tf32(x[u]);
-      *reinterpret_cast<float*>(hi + off) = h;
-      *reinterpret_cast<float*>(lo + off) = tc_tf32(x[u] - h);
+    for (int u = 0; u < 32; ++u) {
+      tc_store_cm(a_hi, a_lo, cm0 + u, lane, xa[u]);
+      tc_store_cm(b_hi, b_lo, cm0 + u, lane, xb[u]);
     }
   }
 }
@@ -184,8 +196,7 @@ static __global__ void __launch_bounds__(128, 1)
   const uint32_t mb = tc_smem_addr(mbar);
   bool ok = true;
   for (int ch = 0; ch < kTc / kTcK && ok; ++ch) {
-    tc_stage(X + (size_t)ch * kTcK * np, np, a_hi, a_lo);
-    tc_stage(Y + (size_t)ch * kTcK * ldy, ldy, b_hi, b_lo);
+    tc_stage2(X + (size_t)ch * kTcK * np, np, Y + (size_t)ch * kTcK * ldy, ldy, a_hi, a_lo, b_hi, b_lo);
     // the generic-proxy stores must be visible to the tensor core's reads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -211,17 +222,27 @@ static __global__ void __launch_bounds__(128, 1)
   if (!ok) {
     if (threadIdx.x == 0) atomicExch(err, 1);
   } else {
-    // epilogue: thread (warp w, lane t) holds row m = 32 w + t of P
+    // epilogue: thread (warp w, lane t) holds row m = 32 w + t of P; the
+    // trailing update's old values of the row are loaded 64 at a time, all
+    // in flight together
     const int m = threadIdx.x;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < kTc; c0 += 16) {
-      float v[16];
-      tc_ld16(lane_base + (uint32_t)c0, v);
+#pragma unroll 1
+    for (int h = 0; h < kTc; h += 64) {
+      float dold[64];
+      if (!panel) {
 #pragma unroll
-      for (int t = 0; t < 16; ++t) {
-        float* d = D + (size_t)(c0 + t) * np + m;
-        if (panel) *d = v[t];
-        else *d -= v[t];
+        for (int c = 0; c < 64; ++c) dold[c] = D[(size_t)(h + c) * np + m];
+      }
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 16) {
+        float v[16];
+        tc_ld16(lane_base + (uint32_t)(h + c0), v);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+          float* d = D + (size_t)(h + c0 + t) * np + m;
+          *d = panel ? v[t] : dold[c0 + t] - v[t];
+        }
       }
     }
   }
@@ -378,6 +399,90 @@ static __global__ void tc_bwd_update(const float* A, int np, int k, double* y) {
   }
 }
 
+// Both substitutions as one cooperative launch each (dir 0: y = L^-1 y,
+// dir 1: y = L^-T y), one grid barrier per tile step instead of two launches:
+// every CTA with work in step k stages W(k) in shared memory (FP32, columns
+// 129 floats apart: conflict-free in both orientations), forms
+// v = W(k) y_k (or W(k)^T y_k) in FP64 (thread per row, columns in order), CTA
+// 0 stores it as the new y_k after the step's barrier, and the CTAs take the
+// step's updates in units
+// of 32 rows of one tile: y_i -= L(i,k) v for the tiles i > k (dir 0), or
+// 32 columns of one tile: y_l -= L(k,l)^T v for l < k (dir 1), four threads
+// per 128-long dot product (32 terms each, a fixed xor tree). A barrier
+// that runs out of its spin limit sets the state's error flag and the
+// kernel returns (the host reports a timeout).
+constexpr int kTcSolveThreads = 128;
+constexpr size_t kTcSolveSmem = (size_t)kTc * (kTc + 1) * sizeof(float);
+
+static __global__ void __launch_bounds__(kTcSolveThreads) tc_solve_coop(const float* A, const float* W, int np, int nt,
+                                                                        double* y, PcgState* st, unsigned barrier_extra,
+                                                                        int dir) {
+  extern __shared__ float tcs_smem[];
+  float* Ws = tcs_smem;  // W(k)(r, c) at Ws[c * 129 + r]
+  __shared__ double vin[kTc], v[kTc];
+  unsigned gen = grid_gen_start(st);
+  const int tid = threadIdx.x;
+  for (int s = 0; s < nt; ++s) {
+    const int k = dir == 0 ? s : nt - 1 - s;
+    const size_t kb = (size_t)k * kTc;
+    const int nunits = 4 * (dir == 0 ? nt - 1 - k : k);
+    // the previous step's tile, stored only now: every CTA has read its old
+    // value (before the barrier), and no later step of this direction reads it
+    if (s > 0 && blockIdx.x == 0) y[(size_t)(dir == 0 ? k - 1 : k + 1) * kTc + tid] = v[tid];
+    if (blockIdx.x == 0 || (int)blockIdx.x < nunits) {
+      const float* Wk = W + kb * kTc;
+      for (int q = tid; q < kTc * kTc / 4; q += kTcSolveThreads) {
+        const int c = q >> 5, r4 = (q & 31) * 4;
+        const float4 w4 = *reinterpret_cast<const float4*>(Wk + (size_t)c * kTc + r4);
+        Ws[c * 129 + r4] = w4.x;
+        Ws[c * 129 + r4 + 1] = w4.y;
+        Ws[c * 129 + r4 + 2] = w4.z;
+        Ws[c * 129 + r4 + 3] = w4.w;
+      }
+      vin[tid] = y[kb + tid];
+      __syncthreads();
+      double acc = 0.0;
+      if (dir == 0) {
+        for (int c = 0; c <= tid; ++c) acc += (double)Ws[c * 129 + tid] * vin[c];
+      } else {
+        for (int c = tid; c < kTc; ++c) acc += (double)Ws[tid * 129 + c] * vin[c];
+      }
+      v[tid] = acc;
+      __syncthreads();
+      const int q4 = tid & 3, rr = tid >> 2;
+      for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int slab = u & 3, idx = u >> 2;
+        double t = 0.0;
+        if (dir == 0) {
+          const size_t ib = (size_t)(k + 1 + idx) * kTc + slab * 32 + rr;  // row of y and of L(i,k)
+          const float* L = A + kb * np + ib;                                 // L(i,k)(row, c) at L[c * np]
+          float x[32];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) x[c] = L[(size_t)(q4 * 32 + c) * np];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) t += (double)x[c] * v[q4 * 32 + c];
+          t += __shfl_xor_sync(0xffffffffu, t, 1);
+          t += __shfl_xor_sync(0xffffffffu, t, 2);
+          if (q4 == 0) y[ib] -= t;
+        } else {
+          const size_t lc = (size_t)idx * kTc + slab * 32 + rr;  // column of L(k,l), row of y
+          const float* L = A + lc * np + kb;                       // L(k,l)(t, col) at L[t]
+          float x[32];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) x[c] = L[q4 * 32 + c];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) t += (double)x[c] * v[q4 * 32 + c];
+          t += __shfl_xor_sync(0xffffffffu, t, 1);
+          t += __shfl_xor_sync(0xffffffffu, t, 2);
+          if (q4 == 0) y[lc] -= t;
+        }
+      }
+    }
+    if (!grid_barrier(st, gen, barrier_extra)) return;
+  }
+  if (blockIdx.x == 0) y[(size_t)(dir == 0 ? nt - 1 : 0) * kTc + tid] = v[tid];
+}
+
 // ------------------------------------------------------------ expansion
 // dense FP32 column-major lower triangle of the system held in the dense
 // 96 x 96 tiles of the tile PCG (kTileBlocks 6x6 blocks per tile edge; tile
@@ -413,6 +518,7 @@ struct TcChol {
   DBuf<double> y;
   DBuf<int> info, err, tile_index;
   DBuf<double> floor;  // pivot floor of the current factorization
+  DBuf<PcgState> sync;  // grid barrier of the cooperative substitutions
   DBuf<int2> lists;                 // per step: panel tiles then update pairs
   std::vector<int> list_ptr;        // per step: [panel start, update start, end)
 };
@@ -443,6 +549,7 @@ static int tc_chol_plan(TcChol& P, int n, int nbt_tiles, const std::vector<int32
   G2OC_TRY(P.info.alloc(1));
   G2OC_TRY(P.err.alloc(1));
   G2OC_TRY(P.floor.alloc(1));
+  G2OC_TRY(P.sync.alloc(1));
   return G2OC_OK;
 }
 
