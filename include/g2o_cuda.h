@@ -69,7 +69,7 @@
 extern "C" {
 #endif
 
-#define G2OC_ABI_VERSION 2
+#define G2OC_ABI_VERSION 3 /* 3: g2oc_graph.stereo_bf (EdgeStereoSE3ProjectXYZ); 2: focal_length_y */
 
 /* status codes */
 #define G2OC_OK 0
