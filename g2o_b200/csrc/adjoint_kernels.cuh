@@ -135,7 +135,7 @@ static __global__ void ba_hvp_landmark_warp(BAEdges E, BAVertices V, const int* 
     const int2 v = E.v[k];
     const int h = pose_h[v.y];
     double gc[6];
-    ba_edge_hvp(V, v, E.z[k], E.om[k], h >= 0 ? p + (size_t)h * 6 : nullptr, p + (size_t)Cf * 6 + (size_t)key * 3,
+    ba_edge_hvp(V, v, E.z[k], ba_om(E, k), h >= 0 ? p + (size_t)h * 6 : nullptr, p + (size_t)Cf * 6 + (size_t)key * 3,
                 acc, gc);
   }
 #pragma unroll
@@ -167,7 +167,7 @@ static __global__ void ba_hvp_landmark(BAEdges E, BAVertices V, const int* l_ptr
     const int2 v = E.v[k];
     const int h = pose_h[v.y];
     double gp[3], gc[6];
-    ba_edge_hvp(V, v, E.z[k], E.om[k], h >= 0 ? p + (size_t)h * 6 : nullptr, p + (size_t)Cf * 6 + (size_t)l * 3,
+    ba_edge_hvp(V, v, E.z[k], ba_om(E, k), h >= 0 ? p + (size_t)h * 6 : nullptr, p + (size_t)Cf * 6 + (size_t)l * 3,
                 gp, gc);
 #pragma unroll
     for (int i = 0; i < 3; ++i) acc[i] += gp[i];
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(THREADS) ba_hvp_camera(BACamEdges CE, BAVertic
     const int2 v = CE.v[j];
     const int l = point_l[v.x];
     double gp[3], gc[6];
-    ba_edge_hvp(V, v, CE.z[j], CE.om[j], p + (size_t)h * 6, l >= 0 ? p + (size_t)Cf * 6 + (size_t)l * 3 : nullptr,
+    ba_edge_hvp(V, v, CE.z[j], ba_om(CE, j), p + (size_t)h * 6, l >= 0 ? p + (size_t)Cf * 6 + (size_t)l * 3 : nullptr,
                 gp, gc);
 #pragma unroll
     for (int i = 0; i < 6; ++i) acc[i] += gc[i];
@@ -213,7 +213,7 @@ static __global__ void ba_backward_edges(BAEdges E, BAVertices V, const int* pos
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= E.n) return;
   const int2 vv = E.v[k];
-  const double4 om = E.om[k];
+  const double4 om = ba_om(E, k);
   double e[2], Xc[3], chi2, w;
   ba_edge_error(V, vv, E.z[k], om, e, Xc, chi2, w);
   double Jp[6], Jc[12];

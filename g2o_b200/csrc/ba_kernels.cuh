@@ -34,6 +34,9 @@ struct BAEdges {
   const double2* z;       // measurement
   const double4* om;      // (Omega00, Omega01, Omega11, Huber delta; <= 0: none)
   const int* hpl;         // Hpl block per edge or -1
+  // om == nullptr: every edge has the information and Huber delta om_const
+  // (a uniform graph reads no per-edge record)
+  double4 om_const = {0.0, 0.0, 0.0, 0.0};
   // stereo edges (stereo_kernels.cuh) instead of z / om: (u, v, u_right,
   // Huber delta), (O00, O01, O02, O11), (O12, O22)
   const double4* z3 = nullptr;
@@ -47,6 +50,7 @@ struct BACamEdges {       // camera-major copy of the edges of free cameras
   const double2* z;
   const double4* om;
   const double4* z3 = nullptr;  // stereo, as BAEdges
+  double4 om_const = {0.0, 0.0, 0.0, 0.0};  // om == nullptr: as BAEdges
   const double4* oa3 = nullptr;
   const double2* ob3 = nullptr;
 };
@@ -59,6 +63,10 @@ struct BAVertices {
   double fx, fy, cx, cy;  // EdgeProjectXYZ2UV: fx = fy = focal_length
   double bf = 0.0;        // EdgeStereoSE3ProjectXYZ::bf
 };
+
+// the information record of edge k (per edge, or the graph's uniform one)
+__device__ __forceinline__ double4 ba_om(const BAEdges& E, int k) { return E.om ? ba_om(E, k) : E.om_const; }
+__device__ __forceinline__ double4 ba_om(const BACamEdges& E, int k) { return E.om ? ba_om(E, k) : E.om_const; }
 
 // Per-edge residual, robust weight and weighted error in FP64.
 // robust weight = rho'(e^T Omega e) (BaseEdge::robustInformation keeps rho'
@@ -88,7 +96,7 @@ static __global__ void ba_chi2_kernel(BAEdges E, BAVertices V, double* partials)
   double c = 0.0, r = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n; k += gridDim.x * blockDim.x) {
     double e[2], Xc[3], chi2, w;
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, w);
     c += chi2;
     if (om.w > 0.0) {
@@ -113,7 +121,7 @@ __device__ __forceinline__ double so_robust_chi2(const BAEdges& E, const BAVerti
   double s = 0.0;
   for (int k = k0; k < k1; ++k) {
     double e[2], Xc[3], chi2, w;
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, w);
     if (om.w > 0.0) {
       double rho[3];
@@ -141,7 +149,7 @@ static __global__ void ba_structure_only(BAEdges E, BAVertices V, const int* l_p
     for (int k = k0; k < k1; ++k) {
       double e[2], Xc[3], c2, w;
       const int2 v = E.v[k];
-      const double4 om = E.om[k];
+      const double4 om = ba_om(E, k);
       ba_edge_error(V, v, E.z[k], om, e, Xc, c2, w);
       double Jp[6], Jc[12];
       ba_jacobians_from_xc(V.cam + (size_t)v.y * 8, Xc, V.fx, V.fy, Jp, Jc);
@@ -209,7 +217,7 @@ static __global__ void ba_errors_kernel(BAEdges E, BAVertices V, double* err) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= E.n) return;
   double e[2], Xc[3], chi2, w;
-  ba_edge_error(V, E.v[k], E.z[k], E.om[k], e, Xc, chi2, w);
+  ba_edge_error(V, E.v[k], E.z[k], ba_om(E, k), e, Xc, chi2, w);
   err[2 * k] = e[0];
   err[2 * k + 1] = e[1];
 }
@@ -246,7 +254,7 @@ __global__ void ba_landmark_pass(BAEdges E, BAVertices V, const int* l_ptr, int 
   const int k1 = l_ptr[l + 1];
   for (int k = l_ptr[l]; k < k1; ++k) {
     const int2 v = E.v[k];
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     const double* cam = V.cam + (size_t)v.y * 8;
@@ -332,7 +340,7 @@ __global__ void __launch_bounds__(256) ba_landmark_warp(BAEdges E, BAVertices V,
   if (act) {
     key = e_lm[k];
     const int2 v = E.v[k];
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jpd[6], Jcd[12];
@@ -429,7 +437,7 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
   if (j < j1) {
     vn = CE.v[j];
     zn = CE.z[j];
-    omn = CE.om[j];
+    omn = ba_om(CE, j);
   }
   for (; j < j1; j += THREADS) {
     const int2 v = vn;
@@ -438,7 +446,7 @@ __global__ void __launch_bounds__(THREADS) ba_camera_pass(BACamEdges CE, BAVerti
     if (j + THREADS < j1) {
       vn = CE.v[j + THREADS];
       zn = CE.z[j + THREADS];
-      omn = CE.om[j + THREADS];
+      omn = ba_om(CE, j + THREADS);
     }
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, z, om, e, Xc, chi2, w);
@@ -959,7 +967,7 @@ static __global__ void ba_resid64_landmark(BAEdges E, BAVertices V, const int* l
   const int k1 = l_ptr[l + 1];
   for (int k = l_ptr[l]; k < k1; ++k) {
     const int2 v = E.v[k];
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];
@@ -1000,7 +1008,7 @@ static __global__ void ba_resid64_landmark_warp(BAEdges E, BAVertices V, const i
     key = e_lm[k];
     const double* xl = x_l + (size_t)key * 3;
     const int2 v = E.v[k];
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, E.z[k], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];
@@ -1050,7 +1058,7 @@ __global__ void __launch_bounds__(THREADS) ba_resid64_camera(BACamEdges CE, BAVe
   const int j1 = CE.ptr[h + 1];
   for (int j = CE.ptr[h] + threadIdx.x; j < j1; j += THREADS) {
     const int2 v = CE.v[j];
-    const double4 om = CE.om[j];
+    const double4 om = ba_om(CE, j);
     double e[2], Xc[3], chi2, w;
     ba_edge_error(V, v, CE.z[j], om, e, Xc, chi2, w);
     double Jp[6], Jc[12];

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(THREADS) win_chi2_chunks(BAEdges E, BAVertices
   double r = 0.0;
   for (int k = chunk_e0[ch] + threadIdx.x; k < k1; k += THREADS) {
     double e[2], Xc[3], chi2, wt;
-    const double4 om = E.om[k];
+    const double4 om = ba_om(E, k);
     ba_edge_error(V, E.v[k], E.z[k], om, e, Xc, chi2, wt);
     if (om.w > 0.0) {
       double rho[3];

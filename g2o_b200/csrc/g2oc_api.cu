@@ -169,6 +169,10 @@ struct g2oc_ctx {
   bool last_upload_reused = false;  // the last g2oc_upload kept the structure (same topology)
   bool system_built = false;
   double fx = 1, fy = 1, cx = 0, cy = 0, bf = 0;
+  // every edge has the same information and Huber delta (two-row edges): the
+  // kernels take om_const and read no per-edge record
+  bool om_uniform = false;
+  double4 om_const = {0.0, 0.0, 0.0, 0.0};
   // vertex state
   g2oc::DBuf<double> pose, point, pose_bak, point_bak, pose_init, point_init;
   g2oc::DBuf<int> oplus_count, free_pose, free_point, pose_h, point_l;
@@ -364,7 +368,8 @@ struct g2oc_ctx {
     E.n = (int)S.act.size();
     E.v = e_v.p;
     E.z = e_z.p;
-    E.om = e_om.p;
+    E.om = om_uniform ? nullptr : e_om.p;
+    E.om_const = om_const;
     E.hpl = e_hpl.p;
     E.z3 = e_z3.p;
     E.oa3 = e_oa3.p;
@@ -372,7 +377,8 @@ struct g2oc_ctx {
     return E;
   }
   g2oc::BACamEdges ba_cam_edges() {
-    g2oc::BACamEdges CE{c_ptr.p, c_v.p, c_z.p, c_om.p};
+    g2oc::BACamEdges CE{c_ptr.p, c_v.p, c_z.p, om_uniform ? nullptr : c_om.p};
+    CE.om_const = om_const;
     CE.z3 = c_z3.p;
     CE.oa3 = c_oa3.p;
     CE.ob3 = c_ob3.p;
@@ -2422,6 +2428,18 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
             c->e_z3.p, c->e_oa3.p, c->e_ob3.p, c->c_z3.p, c->c_oa3.p, c->c_ob3.p);
         G2OC_LAUNCH_CHECK();
       } else if (na + nc > 0) {
+        // uniform information and Huber delta: one record for the graph
+        const double* I = g->information;
+        const double* dl = g->robust_delta;
+        const double d0 = dl ? dl[0] : 0.0;
+        bool uniform = true;
+#pragma omp parallel for schedule(static) reduction(&& : uniform) if (S.E > 65536)
+        for (int e = 0; e < S.E; ++e) {
+          const double* Ie = I + (size_t)e * 4;
+          uniform = uniform && Ie[0] == I[0] && Ie[1] == I[1] && Ie[3] == I[3] && (dl ? dl[e] : 0.0) == d0;
+        }
+        c->om_uniform = uniform;
+        c->om_const = make_double4(I[0], I[1], I[3], d0);
         G2OC_K(K_IO) ba_gather_edges<<<cdiv((long long)na + nc, 256), 256, 0, st>>>(
             na, nc, c->src_dev.p, c->src_cam.p, c->raw_meas.p, c->raw_info.p, g->robust_delta ? c->raw_delta.p : nullptr,
             c->e_z.p, c->e_om.p, c->c_z.p, c->c_om.p);
