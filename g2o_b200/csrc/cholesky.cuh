@@ -226,9 +226,10 @@ constexpr int kTileBuf = kTile * kLd;  // doubles per operand tile
 
 // factor the diagonal tile k in shared memory (lower; T: a tile buffer, used
 // with leading dimension kTile + 1) and form W = L(k,k)^-1 in Wsm (FP64
-// shared memory, column-major, leading dimension ldw); 256 threads
+// shared memory, column-major, leading dimension ldw; scratch: 768 doubles of
+// shared memory); 256 threads
 __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double* T, double* Wsm, int ldw, int* info,
-                                                double floor) {
+                                                double floor, double* scratch) {
   constexpr int ld = kTile + 1;
   const size_t base = (size_t)k * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
@@ -237,7 +238,7 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
   }
   cp_async_wait_all();
   __syncthreads();
-  tile_potrf_inv_blk64(T, ld, Wsm, ldw, info, floor);
+  tile_potrf_inv_blk64(T, ld, Wsm, ldw, info, floor, scratch);
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
     const int i = e % kTile, j = e / kTile;
     if (i >= j) A[(base + j) * np + base + i] = T[i * ld + j];
@@ -245,13 +246,13 @@ __device__ __forceinline__ void chol_potrf_tile(double* A, int np, int k, double
 }
 
 // W(k) of every diagonal tile, kTile x kTile column-major, at W + k kTile^2
-constexpr int kPotrfSmem = 2 * kTile * (kTile + 1) * (int)sizeof(double);
+constexpr int kPotrfSmem = (2 * kTile * (kTile + 1) + 768) * (int)sizeof(double);
 static __global__ void __launch_bounds__(256) chol_potrf(double* A, int np, int k, double* W, const double* floor,
                                                          int* info) {
   extern __shared__ double sm_potrf[];
   double* T = sm_potrf;
   double* Wsm = sm_potrf + kTile * (kTile + 1);
-  chol_potrf_tile(A, np, k, T, Wsm, kTile + 1, info, *floor);
+  chol_potrf_tile(A, np, k, T, Wsm, kTile + 1, info, *floor, sm_potrf + 2 * kTile * (kTile + 1));
   double* Wk = W + (size_t)k * kTile * kTile;
   for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) Wk[e] = Wsm[(e / kTile) * (kTile + 1) + e % kTile];
 }
@@ -347,7 +348,7 @@ static __global__ void __launch_bounds__(256) chol_factor_single(double* A, int 
   double* Ws = sm_single + 2 * kTileBuf;
   const double fl = *floor;
   for (int k = 0; k < nt; ++k) {
-    chol_potrf_tile(A, np, k, B0, Ws, kLd, info, fl);
+    chol_potrf_tile(A, np, k, B0, Ws, kLd, info, fl, B1);  // B1 is free until the panel
     // W(k) kept for the substitutions (chol_solve_single)
     for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x)
       W[(size_t)k * kTile * kTile + e] = Ws[(e / kTile) * kLd + e % kTile];

@@ -277,7 +277,7 @@ static __global__ void __launch_bounds__(128, 1)
 constexpr int kTcLd = 68;                    // operand blocks, as tile_dmma64 reads them
 constexpr int kTcBlk = 64 * kTcLd;           // doubles per operand block
 constexpr int kTcTri = 64 * 65;              // doubles per diagonal block (leading dimension 65)
-constexpr size_t kTcPotrfSmem = (size_t)(2 * kTcTri + 3 * kTcBlk) * sizeof(double);
+constexpr size_t kTcPotrfSmem = (size_t)(2 * kTcTri + 3 * kTcBlk + 768) * sizeof(double);
 
 static __global__ void __launch_bounds__(256, 1) tc_potrf(float* A, int np, int k, float* Wk, const double* floor,
                                                            int* info) {
@@ -287,6 +287,7 @@ static __global__ void __launch_bounds__(256, 1) tc_potrf(float* A, int np, int 
   double* X = T2 + kTcTri;              // A21 -> L21 -> L21 W11 (ld kTcLd)
   double* W1 = X + kTcBlk;              // W11 (column-major, ld kTcLd)
   double* W2 = W1 + kTcBlk;             // W22
+  double* scratch = W2 + kTcBlk;        // the blocked factorization's staging (768 doubles)
   const size_t kb = (size_t)k * kTc;
   for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
     const int i = e % 64, j = e / 64;
@@ -299,7 +300,7 @@ static __global__ void __launch_bounds__(256, 1) tc_potrf(float* A, int np, int 
   __syncthreads();
   int bad = 0;
   const double fl = *floor;
-  tile_potrf_inv_blk64(T1, 65, W1, kTcLd, &bad, fl);
+  tile_potrf_inv_blk64(T1, 65, W1, kTcLd, &bad, fl, scratch);
   double acc[2][4][2];
   // L21 = A21 W11^T (Y(j, t) = W11(j, t) at W1[t * ld + j])
   tile_dmma64<false, true>(X, W1, kTcLd, acc);
@@ -327,7 +328,7 @@ static __global__ void __launch_bounds__(256, 1) tc_potrf(float* A, int np, int 
         if (r >= c) T2[r * 65 + c] -= acc[u][v][e];
       }
   __syncthreads();
-  tile_potrf_inv_blk64(T2, 65, W2, kTcLd, &bad, fl);
+  tile_potrf_inv_blk64(T2, 65, W2, kTcLd, &bad, fl, scratch);
   // M = L21 W11 (Y(c, t) = W11(t, c) at W1[c * ld + t]), into X
   tile_dmma64<false, false>(X, W1, kTcLd, acc);
   __syncthreads();
