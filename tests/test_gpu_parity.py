@@ -370,6 +370,29 @@ def test_grid_barrier_wait_runs_out_and_reports_timeout(backend, monkeypatch, ca
     assert done == 2 and st[-1]["chi2"] < st[0]["chi2"] * 10
 
 
+def test_tensor_core_substitution_barrier_runs_out_and_reports_timeout(backend, monkeypatch):
+    """The tensor-core Cholesky's cooperative substitutions (one grid barrier
+    per tile step) wait a bounded time too: with one arrival too many
+    expected, every wait runs out, the kernel returns and the host reports
+    G2OC_ERR_TIMEOUT; another context then optimizes the same graph."""
+    from g2o_b200.abi import G2OC_ERR_TIMEOUT
+    g = small_ba(seed=23, cams=64, points=4000)
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    monkeypatch.setenv("G2OC_TEST_BARRIER_EXTRA", "1")
+    bad = backend.CudaProblem(g, fac.construct("lm_cuda_chol_mixed"))
+    monkeypatch.delenv("G2OC_TEST_BARRIER_EXTRA")
+    with pytest.raises(backend.G2ocError) as ei:
+        bad.optimize(1)
+    assert ei.value.status == G2OC_ERR_TIMEOUT
+    bad.close()
+    good = backend.CudaProblem(g, fac.construct("lm_cuda_chol_mixed"))
+    done, st = good.optimize(2)
+    _, ks = good.kernel_stats()
+    good.close()
+    assert done == 2 and st[-1]["chi2"] < st[0]["chi2"] * 10
+    assert ks["tc_solve"][0] > 0
+
+
 def test_not_positive_definite_is_reported(backend):
     offs = np.array([0, 3, 6], np.int32)
     rc = np.array([[0, 0], [0, 1], [1, 1]], np.int32)
