@@ -65,8 +65,8 @@ struct BAVertices {
 };
 
 // the information record of edge k (per edge, or the graph's uniform one)
-__device__ __forceinline__ double4 ba_om(const BAEdges& E, int k) { return E.om ? ba_om(E, k) : E.om_const; }
-__device__ __forceinline__ double4 ba_om(const BACamEdges& E, int k) { return E.om ? ba_om(E, k) : E.om_const; }
+__device__ __forceinline__ double4 ba_om(const BAEdges& E, int k) { return E.om ? E.om[k] : E.om_const; }
+__device__ __forceinline__ double4 ba_om(const BACamEdges& E, int k) { return E.om ? E.om[k] : E.om_const; }
 
 // Per-edge residual, robust weight and weighted error in FP64.
 // robust weight = rho'(e^T Omega e) (BaseEdge::robustInformation keeps rho'

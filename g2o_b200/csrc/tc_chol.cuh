@@ -45,9 +45,7 @@ namespace g2oc {
 constexpr int kTc = 128;           // tile edge
 constexpr int kTcK = 64;           // K per staged chunk
 constexpr int kTcOpBytes = kTc * kTcK * 4;        // one operand tile (hi or lo): 32 KB
-constexpr int kTcRawLd = kTc + 8;                 // raw FP32 staging: a column every 136 floats
-constexpr int kTcRawBytes = kTc * kTcRawLd * 4;   // the two raw operands of a chunk, or the output tile
-constexpr int kTcSmem = 4 * kTcOpBytes + kTcRawBytes + 1024;  // hi/lo operands, raw staging, barrier, TMEM address
+constexpr int kTcSmem = 4 * kTcOpBytes + 1024;    // A hi/lo, B hi/lo, barrier and TMEM address
 constexpr long long kTcSpinLimit = 1ll << 26;     // bounded waits (tens of ms at worst)
 
 // ------------------------------------------------------------ PTX helpers
@@ -119,37 +117,42 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
   for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(r[t]);
 }
 
-// Operand staging in two steps. (1) tc_issue_raw: a 128 (MN) x 64 (K) FP32
-// sub-tile of a column-major matrix (column j at G + j * ld, 16-byte aligned)
-// copied into shared memory with 16-byte asynchronous copies, column j at
-// raw + j * 136 (every copy of the CTA in flight together). (2) tc_convert:
-// the sub-tile split into hi / lo TF32 parts in the K-major layout above, one
-// core matrix (8 rows x 4 K values, 32 consecutive words) per warp
-// instruction: lane l takes row 8 mg + l / 4 and K value 4 kg + l % 4; with
-// the 136-float column stride the reads, and the stores, cover the 32 banks
-// once.
-__device__ __forceinline__ void tc_cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc_smem_addr(dst)), "l"(src) : "memory");
+// stage the two 128 (MN) x 64 (K) FP32 operand sub-tiles of a tile product
+// (column j of a sub-tile at G + j * ld) as hi / lo TF32 parts in the K-major
+// layout above. One core matrix (8 rows x 4 K values, 32 consecutive words
+// of shared memory) per warp instruction: lane l takes row 8 mg + l / 4 and
+// K value 4 kg + l % 4, so each store covers the 32 banks once and each load
+// reads four 32-byte column runs. Each warp takes 64 core matrices of each
+// operand, 32 of each per round with all 64 loads in flight (the loads are
+// what the staging waits on).
+__device__ __forceinline__ void tc_stage_cm(const float* G, size_t ld, int cm, int lane, float& x) {
+  const int mg = cm & 15, kg = cm >> 4;
+  x = G[(size_t)(4 * kg + (lane & 3)) * ld + 8 * mg + (lane >> 2)];
 }
-__device__ __forceinline__ void tc_cp_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-__device__ __forceinline__ void tc_issue_raw(const float* G, size_t ld, float* raw) {
-  for (int t = threadIdx.x; t < kTc * kTcK / 4; t += blockDim.x) {
-    const int j = t >> 5, q = t & 31;
-    tc_cp_async16(raw + j * kTcRawLd + 4 * q, G + (size_t)j * ld + 4 * q);
-  }
+__device__ __forceinline__ void tc_store_cm(unsigned char* hi, unsigned char* lo, int cm, int lane, float x) {
+  const int mg = cm & 15, kg = cm >> 4;
+  const uint32_t off = (uint32_t)mg * 128 + (uint32_t)kg * 2048 + (uint32_t)lane * 4;
+  const float h = tc_tf32(x);
+  *reinterpret_cast<float*>(hi + off) = h;
+  *reinterpret_cast<float*>(lo + off) = tc_tf32(x - h);
 }
-
-__device__ __forceinline__ void tc_convert(const float* raw, unsigned char* hi, unsigned char* lo) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll 8
-  for (int cm = warp; cm < 256; cm += nw) {
-    const int mg = cm & 15, kg = cm >> 4;
-    const float x = raw[(4 * kg + (lane & 3)) * kTcRawLd + 8 * mg + (lane >> 2)];
-    const uint32_t off = (uint32_t)mg * 128 + (uint32_t)kg * 2048 + (uint32_t)lane * 4;
-    const float h = tc_tf32(x);
-    *reinterpret_cast<float*>(hi + off) = h;
-    *reinterpret_cast<float*>(lo + off) = tc_tf32(x - h);
+__device__ __forceinline__ void tc_stage2(const float* GA, size_t lda, const float* GB, size_t ldb, unsigned char* a_hi,
+                                          unsigned char* a_lo, unsigned char* b_hi, unsigned char* b_lo) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;  // 4 warps
+#pragma unroll 1
+  for (int rnd = 0; rnd < 2; ++rnd) {
+    const int cm0 = warp * 64 + rnd * 32;
+    float xa[32], xb[32];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      tc_stage_cm(GA, lda, cm0 + u, lane, xa[u]);
+      tc_stage_cm(GB, ldb, cm0 + u, lane, xb[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      tc_store_cm(a_hi, a_lo, cm0 + u, lane, xa[u]);
+      tc_store_cm(b_hi, b_lo, cm0 + u, lane, xb[u]);
+    }
   }
 }
 
@@ -167,10 +170,8 @@ static __global__ void __launch_bounds__(128, 1)
   unsigned char* a_lo = tc_smem + kTcOpBytes;
   unsigned char* b_hi = tc_smem + 2 * kTcOpBytes;
   unsigned char* b_lo = tc_smem + 3 * kTcOpBytes;
-  float* rawA = reinterpret_cast<float*>(tc_smem + 4 * kTcOpBytes);  // columns 0..63 of the raw region
-  float* rawB = rawA + kTcK * kTcRawLd;                              // columns 64..127
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tc_smem + 4 * kTcOpBytes + kTcRawBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + 4 * kTcOpBytes + kTcRawBytes + 64);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tc_smem + 4 * kTcOpBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + 4 * kTcOpBytes + 64);
   const int2 ij = list[blockIdx.x];
   const bool panel = ij.y < 0;
   const size_t kb = (size_t)k * kTc;
@@ -179,9 +180,6 @@ static __global__ void __launch_bounds__(128, 1)
   const size_t ldy = panel ? (size_t)kTc : (size_t)np;
   float* D = A + (panel ? kb : (size_t)ij.y * kTc) * np + (size_t)ij.x * kTc;
   const int warp = threadIdx.x >> 5;
-  // chunk 0's operands start loading before the setup
-  tc_issue_raw(X, np, rawA);
-  tc_issue_raw(Y, ldy, rawB);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(tmem_slot)),
                  "r"(kTc));
@@ -191,7 +189,6 @@ static __global__ void __launch_bounds__(128, 1)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(mbar)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  tc_cp_async_wait();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -199,24 +196,10 @@ static __global__ void __launch_bounds__(128, 1)
   const uint32_t mb = tc_smem_addr(mbar);
   bool ok = true;
   for (int ch = 0; ch < kTc / kTcK && ok; ++ch) {
-    tc_convert(rawA, a_hi, a_lo);
-    tc_convert(rawB, b_hi, b_lo);
+    tc_stage2(X + (size_t)ch * kTcK * np, np, Y + (size_t)ch * kTcK * ldy, ldy, a_hi, a_lo, b_hi, b_lo);
     // the generic-proxy stores must be visible to the tensor core's reads
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    // the raw region is free again: the next chunk's operands, or (after
-    // the last chunk) the trailing update's old output tile, load while the
-    // products run
-    const bool last = ch == kTc / kTcK - 1;
-    if (!last) {
-      tc_issue_raw(X + (size_t)(ch + 1) * kTcK * np, np, rawA);
-      tc_issue_raw(Y + (size_t)(ch + 1) * kTcK * ldy, ldy, rawB);
-    } else if (!panel) {
-      for (int t = threadIdx.x; t < kTc * kTc / 4; t += blockDim.x) {
-        const int c = t >> 5, q = t & 31;
-        tc_cp_async16(rawA + c * kTcRawLd + 4 * q, D + (size_t)c * np + 4 * q);
-      }
-    }
     if (threadIdx.x == 0) {
       tc_fence_after();
       const uint32_t ah = tc_smem_addr(a_hi), al = tc_smem_addr(a_lo);
@@ -230,7 +213,6 @@ static __global__ void __launch_bounds__(128, 1)
       }
       tc_commit(mb);
     }
-    tc_cp_async_wait();
     // every thread waits for the products of this chunk before the operand
     // tiles are overwritten (or the accumulator is read); the outcome is
     // made uniform over the CTA so every thread takes the same path
@@ -241,18 +223,26 @@ static __global__ void __launch_bounds__(128, 1)
     if (threadIdx.x == 0) atomicExch(err, 1);
   } else {
     // epilogue: thread (warp w, lane t) holds row m = 32 w + t of P; the
-    // update's old values come from the staged tile (column c at
-    // rawA + c * 136)
+    // trailing update's old values of the row are loaded 64 at a time, all
+    // in flight together
     const int m = threadIdx.x;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
-    for (int c0 = 0; c0 < kTc; c0 += 16) {
-      float v[16];
-      tc_ld16(lane_base + (uint32_t)c0, v);
+    for (int h = 0; h < kTc; h += 64) {
+      float dold[64];
+      if (!panel) {
 #pragma unroll
-      for (int t = 0; t < 16; ++t) {
-        const int c = c0 + t;
-        D[(size_t)c * np + m] = panel ? v[t] : rawA[c * kTcRawLd + m] - v[t];
+        for (int c = 0; c < 64; ++c) dold[c] = D[(size_t)(h + c) * np + m];
+      }
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 16) {
+        float v[16];
+        tc_ld16(lane_base + (uint32_t)(h + c0), v);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+          float* d = D + (size_t)(h + c0 + t) * np + m;
+          *d = panel ? v[t] : dold[c0 + t] - v[t];
+        }
       }
     }
   }
