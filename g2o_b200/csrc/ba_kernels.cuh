@@ -524,6 +524,47 @@ __global__ void schur_landmark(const Real* hll, const Real* hpl, const int* hb_p
   }
 }
 
+// One 6 x 3 Hpl block (18 values, row-major) into registers. FP32 blocks are
+// 72 bytes at a 72-byte stride: a block starts on a 16-byte boundary when its
+// index is even (four 16-byte loads, then 8 bytes) and on an 8-byte one when
+// odd (8 bytes, then four 16-byte loads): five loads instead of nine. FP64
+// blocks (144 bytes) are nine 16-byte loads.
+template <bool VEC>
+__device__ __forceinline__ void ldg_block18(const float* hpl, int blk, float (&b)[18]) {
+  const float* base = hpl + (size_t)blk * 18;
+  if (VEC) {
+    const bool odd = blk & 1;
+    const int o4 = odd ? 2 : 0;
+    const float4 u0 = __ldg(reinterpret_cast<const float4*>(base + o4));
+    const float4 u1 = __ldg(reinterpret_cast<const float4*>(base + o4 + 4));
+    const float4 u2 = __ldg(reinterpret_cast<const float4*>(base + o4 + 8));
+    const float4 u3 = __ldg(reinterpret_cast<const float4*>(base + o4 + 12));
+    const float2 w = __ldg(reinterpret_cast<const float2*>(base + (odd ? 0 : 16)));
+    const float q[18] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w, u2.x,
+                         u2.y, u2.z, u2.w, u3.x, u3.y, u3.z, u3.w, w.x,  w.y};
+#pragma unroll
+    for (int t = 0; t < 18; ++t) b[t] = odd ? (t < 2 ? q[16 + t] : q[t - 2]) : q[t];
+  } else {
+    const float2* B2 = reinterpret_cast<const float2*>(base);
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const float2 v = __ldg(B2 + t);
+      b[2 * t] = v.x;
+      b[2 * t + 1] = v.y;
+    }
+  }
+}
+template <bool VEC>
+__device__ __forceinline__ void ldg_block18(const double* hpl, int blk, double (&b)[18]) {
+  const double2* B2 = reinterpret_cast<const double2*>(hpl + (size_t)blk * 18);
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    const double2 v = __ldg(B2 + t);
+    b[2 * t] = v.x;
+    b[2 * t + 1] = v.y;
+  }
+}
+
 // Dense output of the Schur rows for batched windows: each camera row belongs
 // to one window, whose reduced system is a dense FP64 matrix (n + 1 rows of
 // n, row-major, at M + mat[w]; the last row holds the right-hand side). Only
@@ -610,16 +651,11 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
       a_next = hc_blk[a0 + t + THREADS];
       l_next = hc_col[a0 + t + THREADS];
     }
-    const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)a * 18);
     const Real* Dl = dinv + (size_t)l * 9;
     Real b[18], D[9], bd[18];
+    ldg_block18<VEC>(hpl, a, b);
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      const R2 v = B2[q];
-      b[2 * q] = v.x;
-      b[2 * q + 1] = v.y;
-      D[q] = Dl[q];
-    }
+    for (int q = 0; q < 9; ++q) D[q] = Dl[q];
     Real* o = BDw + (size_t)t * bds;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
@@ -711,33 +747,7 @@ __global__ void __launch_bounds__(THREADS, sizeof(Real) == 4 ? 2 : 1)
     // gathers are in flight per thread; accumulation stays in pair order.
     // The pair list and S are touched once per pass: streamed (evict-first
     // loads and stores), so the L2 lines go to the Hpl blocks gathered again
-    auto load_b = [&](int blk, Real (&b)[18]) {
-      if constexpr (sizeof(Real) == 4 && VEC) {
-        // a 72-byte FP32 block starts on a 16-byte boundary when its index is
-        // even (four 16-byte loads, then 8 bytes) and on an 8-byte one when odd
-        // (8 bytes, then four 16-byte loads): five loads instead of nine
-        const float* base = reinterpret_cast<const float*>(hpl) + (size_t)blk * 18;
-        const bool odd = blk & 1;
-        const int o4 = odd ? 2 : 0;
-        const float4 u0 = __ldg(reinterpret_cast<const float4*>(base + o4));
-        const float4 u1 = __ldg(reinterpret_cast<const float4*>(base + o4 + 4));
-        const float4 u2 = __ldg(reinterpret_cast<const float4*>(base + o4 + 8));
-        const float4 u3 = __ldg(reinterpret_cast<const float4*>(base + o4 + 12));
-        const float2 w = __ldg(reinterpret_cast<const float2*>(base + (odd ? 0 : 16)));
-        const float q[18] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w, u2.x,
-                             u2.y, u2.z, u2.w, u3.x, u3.y, u3.z, u3.w, w.x,  w.y};
-#pragma unroll
-        for (int t = 0; t < 18; ++t) b[t] = odd ? (t < 2 ? q[16 + t] : q[t - 2]) : q[t];
-      } else {
-        const R2* B2 = reinterpret_cast<const R2*>(hpl + (size_t)blk * 18);
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-          const R2 v = __ldg(B2 + t);
-          b[2 * t] = v.x;
-          b[2 * t + 1] = v.y;
-        }
-      }
-    };
+    auto load_b = [&](int blk, Real (&b)[18]) { ldg_block18<VEC>(hpl, blk, b); };
     auto accum = [&](int a, const Real (&b)[18]) {
       const Real* D = BDa + (size_t)a * bds + half * bhalf;
       Real d[9];
