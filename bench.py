@@ -34,7 +34,8 @@ optimization per step).
 
 --config pg2d / pg3d: the pose graphs (latency-bound; roofline = launch
 latency floor). --config windows / adjoint: batched local BA windows and the
-implicit-function-theorem backward call.
+implicit-function-theorem backward call. --config bal: the BAL path
+(BlockSolver<9,3> + PCG, FP64) on a 356-camera / 226,730-point problem.
 
 Multi-GPU (torchrun): the default configuration becomes ba_sharded, the same
 bundle adjustment split by points over the ranks with one NCCL all-reduce of
@@ -68,13 +69,15 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-iterations", type=int, default=1)
-    ap.add_argument("--config", default=None, choices=["ba", "ba_sharded", "pg2d", "pg3d", "windows", "adjoint"],
+    ap.add_argument("--config", default=None,
+                    choices=["ba", "ba_sharded", "pg2d", "pg3d", "windows", "adjoint", "bal"],
                     help="ba: the 1000-camera bundle adjustment (the default on one GPU); ba_sharded: the same "
                          "bundle adjustment split by points over the GPUs (NCCL all-reduce of the reduced camera "
                          "system per LM trial; the default on more than one GPU); pg2d: the 3500-pose 2D pose graph, "
                          "Gauss-Newton + Cholesky, 10 iterations; pg3d: the 2500-pose 3D pose graph, LM + Cholesky, "
                          "20 iterations, FP64 and mixed precision; windows: 512 batched local BA windows; adjoint: "
-                         "implicit-function-theorem gradients through the converged 200-camera BA")
+                         "implicit-function-theorem gradients through the converged 200-camera BA; bal: the "
+                         "356-camera BAL problem (BlockSolver<9,3> + PCG, FP64, 10 LM iterations)")
     a = ap.parse_args()
     if a.config is None:
         a.config = "ba" if a.gpus <= 1 else "ba_sharded"
@@ -258,6 +261,8 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     if args.config in PG_CONFIGS:
         return run_reference_pg(args, threads)
+    if args.config == "bal":
+        return run_reference_bal(args, threads)
     g = build_graph()
     prob = oracle.OracleProblem(g, oracle.default_params(), threads=threads)
     pose0, point0 = prob.estimates()
@@ -797,6 +802,225 @@ def run_pg(args):
     }), flush=True)
 
 
+BAL_ITERS = 10
+BAL_SOLVER = "lm_cuda_pcg9_3"
+BAL_WORKLOAD = "bal_356cam_226730pt_1.27Mobs_lm10_pcg9_3"
+
+
+def bal_algorithmic_bytes(kernel, info, E, num_pairs, uniform_info=True):
+    """Bytes each array element read or written once, per launch, for the
+    BAL kernels (FP64 storage; cameras 72 bytes, points 32, edges: point and
+    camera index 8, measurement 16, information record 32 unless uniform,
+    Hpl block index 4)."""
+    C, P = info.num_free_poses, info.num_free_points
+    nH, nS = info.hpl_nnzb, info.schur_nnzb
+    n = C * 9
+    rec = 24 + (0 if uniform_info else 32)
+    if kernel == "ba_landmark_pass":  # edges, points, cameras -> Hpl, H_ll, b_l
+        return (rec + 4) * E + 32 * P + 72 * C + 216 * nH + 72 * P
+    if kernel == "ba_camera_pass":  # camera-major edge copy, points, cameras -> Hpp, b_p
+        return rec * E + 32 * P + 72 * C + 720 * C
+    if kernel == "schur_landmark":  # H_ll, Hpl -> Dinv, Y
+        return 48 * P + 216 * nH + 72 * P + 216 * nH
+    if kernel == "schur_blocks":  # Y and Hpl, Hpp, b, pair and block lists -> S (upper), b_s
+        return 432 * nH + 648 * C + 24 * P + 72 * C + 8 * num_pairs + 16 * nS + 648 * nS + 72 * C
+    if kernel == "pcg_iteration":  # S (upper) + column/perm index, T written and read, M^-1, x r s d, gathers of d
+        return (648 + 8) * nS + 2 * 72 * (nS - C) + 648 * C + 9 * 8 * n
+    if kernel == "ba_backsub":
+        return 216 * nH + 4 * nH + 72 * P + 24 * P + 72 * C + 24 * P
+    if kernel == "chi2":
+        return rec * E + 32 * P + 72 * C
+    return None
+
+
+def run_bal(args):
+    """BAL: BlockSolver<9,3> + LinearSolverPCG under Levenberg-Marquardt
+    (g2o/examples/bal/bal_example.cpp:227-250) on the seeded 356-camera /
+    226,730-point / ~1.27M-observation problem (synth.bal_problem: the shape of
+    the BAL collection's Dubrovnik-356, whose files are not shipped), FP64,
+    10 LM iterations per step from the initial estimates, graph resident in
+    HBM; value = LM iterations per second. The device time to the FP64 oracle's
+    10-iteration chi2 (+1e-6; tests/golden/oracle_targets.json), the end-to-end
+    form through the C-ABI with pinned host buffers, and the roofline of the
+    kernel with the largest device time. Multi-GPU: replicas."""
+    rank, world, local = dist_info()
+    import ctypes as C
+    import torch
+    from g2o_b200 import backend, synth
+
+    device = local
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    g = synth.bal_problem()
+    orc = oracle_target("bal", g)
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    prob = backend.CudaProblem(g, fac.construct(BAL_SOLVER), device=device)
+    stream = torch.cuda.ExternalStream(prob.stream(), device=device)
+    for _ in range(max(args.warmup, 1)):
+        prob.restore_initial_estimates()
+        prob.optimize(BAL_ITERS)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    l0, _ = prob.kernel_stats()
+    clocks = ClockSampler(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_it = 0
+    st = None
+    e0.record(stream)
+    for _ in range(args.steps):
+        prob.restore_initial_estimates()
+        _, st = prob.optimize(BAL_ITERS)
+        n_it += len(st)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    l1, _ = prob.kernel_stats()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_it / (ms * 1e-3)
+    target = orc["final_chi2"] if orc else st[-1]["chi2"]
+    # device time to the target
+    prob.restore_initial_estimates()
+    _, st2 = prob.optimize(2 * BAL_ITERS)
+    t_target, n_target, cum = None, None, 0.0
+    for x in st2:
+        cum += x["time_iteration"]
+        if x["chi2"] <= target * (1 + 1e-6):
+            t_target, n_target = cum, x["iteration"] + 1
+            break
+    # per-kernel device times over one optimization (CUDA events around each launch)
+    prob.restore_initial_estimates()
+    prob.set_kernel_timing(True)
+    _, st3 = prob.optimize(BAL_ITERS)
+    _, ks = prob.kernel_stats()
+    prob.set_kernel_timing(False)
+    info = prob.info
+    pcg_iters = sum(x["iterations_linear_solver"] for x in st3)
+    roof = None
+    peak, peak_kind = measured_peaks()
+    best = None
+    for k, (nl, tms) in ks.items():
+        if nl <= 0 or tms <= 0:
+            continue
+        if k == "pcg_solve":
+            b = bal_algorithmic_bytes("pcg_iteration", info, g.num_edges, info.schur_pairs)
+            units, per = max(pcg_iters, 1), "PCG iteration"
+        else:
+            b = bal_algorithmic_bytes(k, info, g.num_edges, info.schur_pairs)
+            units, per = nl, "launch"
+        if b is None:
+            continue
+        if best is None or tms > best[1]:
+            best = (k, tms, b, units, per, nl)
+    if best:
+        k, tms, b, units, per, nl = best
+        achieved = b * units / (tms * 1e-3) / 1e9
+        roof = {"kernel": k, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                f"algorithmic_bytes_per_{per.replace(' ', '_')}": b, "launches": nl,
+                "avg_ms_per_unit": tms / units}
+    kernels_ms = {k: round(v[1], 3) for k, v in sorted(ks.items(), key=lambda kv: -kv[1][1]) if v[0] > 0}
+    # end to end through the C-ABI with pinned host buffers
+    hg = pinned_copy(g)
+    cg = hg.to_c()
+    L = backend.library()
+    pose_out = pinned_empty(g.pose_estimate.shape)
+    point_out = pinned_empty(g.point_estimate.shape)
+    h2d = sum(a.nbytes for a in (hg.pose_estimate, hg.point_estimate, hg.measurement, hg.information)
+              if a is not None)
+    backend._check(L.g2oc_upload(prob.handle, C.byref(cg)))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_it = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        backend._check(L.g2oc_upload(prob.handle, C.byref(cg)))
+        _, s4 = prob.optimize(BAL_ITERS)
+        e_it += len(s4)
+        backend._check(L.g2oc_download(prob.handle, backend._p(pose_out), backend._p(point_out)))
+    e1.record(stream)
+    e1.synchronize()
+    ems = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ems], device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ems = float(t.item())
+    prob.close()
+    cpu = None
+    if rank == 0 and world == 1:
+        from g2o_b200.abi import ALGO_LEVENBERG, LINEAR_PCG
+        cpu = cpu_baselines(g, args.cpu_sample_iterations, algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_PCG)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": "BAL LM iter/s (BlockSolver<9,3> + PCG, FP64; time to the FP64 oracle's chi2+-1e-6)",
+        "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded bal_problem generator, the shape of Dubrovnik-356)",
+        "config": {"workload": BAL_WORKLOAD, "cameras": g.num_poses, "points": g.num_points, "edges": g.num_edges,
+                   "iterations_per_step": BAL_ITERS, "solver": BAL_SOLVER,
+                   "parallelism": "replicas" if world > 1 else "single-gpu",
+                   "l2": "working set ~0.5 GB, larger than L2: every LM iteration streams it"},
+        "target": {"chi2": target, "source": "fp64 oracle" if orc else "fp64 gpu run",
+                   "rule": "robust chi2 <= target * (1 + 1e-6)"},
+        "final_chi2": st[-1]["chi2"], "rel_to_target": st[-1]["chi2"] / target - 1,
+        "time_to_target_s": t_target, "iterations_to_target": n_target,
+        "pcg_iterations_per_lm_iteration": pcg_iters / max(len(st3), 1),
+        "kernels_ms_per_optimization": kernels_ms,
+        "roofline": roof,
+        "gpu_launches": int(l1 - l0),
+        "clocks": clk,
+        "e2e": {"value": world * e_it / (ems * 1e-3), "unit": "iter/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(pose_out.nbytes + point_out.nbytes),
+                "upload": "same topology each step: values copied"},
+        "cpu_baseline": cpu["all_cores"] if cpu else None,
+        "cpu_baseline_single_thread": cpu["single_thread"] if cpu else None,
+        "cpu_host": cpu["host"] if cpu else None,
+    }), flush=True)
+
+
+def run_reference_bal(args, threads):
+    """The reference arm on the BAL problem: the FP64 restatement (Schur +
+    block-Jacobi PCG, BlockSolver<9,3>) on all host cores, one LM iteration
+    from the initial estimates per step."""
+    from oracle import oracle
+    from g2o_b200 import synth
+    from g2o_b200.abi import ALGO_LEVENBERG, LINEAR_PCG
+    g = synth.bal_problem()
+    prob = oracle.OracleProblem(g, oracle.default_params(algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_PCG),
+                                threads=threads)
+    pose0, point0 = prob.estimates()
+    times = []
+    for s in range(args.warmup + args.steps):
+        prob.set_estimates(pose0, point0)
+        t0 = time.perf_counter()
+        prob.optimize(1)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    T = sum(times)
+    value = args.steps / T
+    sample = f"one LM iteration (BlockSolver<9,3>, Schur + block-Jacobi PCG, FP64) per step, {threads} threads"
+    print(json.dumps({
+        "impl": "reference", "metric": "BAL LM iter/s (BlockSolver<9,3> + PCG, FP64)", "value": value,
+        "unit": "iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * T / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded bal_problem generator)",
+        "config": {"workload": BAL_WORKLOAD, "iterations": 1, "cameras": g.num_poses, "points": g.num_points,
+                   "edges": g.num_edges, "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def tf32_peak():
     """Dense TF32 tensor rate: half of the measured bf16 GEMM rate (the
     nominal B200 ratio, 1.1 vs 2.25 PFLOP/s)."""
@@ -1078,5 +1302,7 @@ if __name__ == "__main__":
         run_ba_sharded(a)
     elif a.config in PG_CONFIGS:
         run_pg(a)
+    elif a.config == "bal":
+        run_bal(a)
     else:
         run_ours(a)

@@ -29,21 +29,23 @@ ERROR_NAMES = {
     6: "STATE", 7: "NO_DEVICE", 8: "UNKNOWN_SOLVER", 9: "TIMEOUT", 10: "NOT_SUPPORTED", 11: "NOT_CONVERGED",
 }
 
-POSE_SE2, POSE_SE3, POSE_SE3EXPMAP = 1, 2, 3
+POSE_SE2, POSE_SE3, POSE_SE3EXPMAP, POSE_BAL_CAMERA = 1, 2, 3, 4
 EDGE_SE2, EDGE_SE3, EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_SE3_EXPMAP = 1, 2, 3, 4, 5
 EDGE_STEREO_SE3_PROJECT_XYZ = 6
-BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_STEREO_SE3_PROJECT_XYZ)
+EDGE_BAL_OBSERVATION = 7
+# projection edges: vertex0 a point, vertex1 a camera
+BA_EDGES = (EDGE_PROJECT_XYZ2UV, EDGE_SE3_PROJECT_XYZ, EDGE_STEREO_SE3_PROJECT_XYZ, EDGE_BAL_OBSERVATION)
 ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, ALGO_DOGLEG, ALGO_STRUCTURE_ONLY = 0, 1, 2, 3
 LINEAR_PCG, LINEAR_CHOLESKY = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 RESULT_OK, RESULT_FAIL, RESULT_TERMINATE = 1, -1, 2
 
-POSE_EST_DIM = {POSE_SE2: 3, POSE_SE3: 12, POSE_SE3EXPMAP: 7}
-POSE_DIM = {POSE_SE2: 3, POSE_SE3: 6, POSE_SE3EXPMAP: 6}
+POSE_EST_DIM = {POSE_SE2: 3, POSE_SE3: 12, POSE_SE3EXPMAP: 7, POSE_BAL_CAMERA: 9}
+POSE_DIM = {POSE_SE2: 3, POSE_SE3: 6, POSE_SE3EXPMAP: 6, POSE_BAL_CAMERA: 9}
 EDGE_DIM = {EDGE_SE2: 3, EDGE_SE3: 6, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 6,
-            EDGE_STEREO_SE3_PROJECT_XYZ: 3}
+            EDGE_STEREO_SE3_PROJECT_XYZ: 3, EDGE_BAL_OBSERVATION: 2}
 MEAS_DIM = {EDGE_SE2: 3, EDGE_SE3: 12, EDGE_PROJECT_XYZ2UV: 2, EDGE_SE3_PROJECT_XYZ: 2, EDGE_SE3_EXPMAP: 7,
-            EDGE_STEREO_SE3_PROJECT_XYZ: 3}
+            EDGE_STEREO_SE3_PROJECT_XYZ: 3, EDGE_BAL_OBSERVATION: 2}
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)

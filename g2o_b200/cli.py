@@ -3,6 +3,7 @@
 
     python -m g2o_b200.cli --config ba --solver lm_cuda_pcg6_3 -i 20 [-stats]
     python -m g2o_b200.cli --config windows --windows 64 --solver lm_cuda_mixed_fast -i 10
+    python -m g2o_b200.cli --bal problem.txt --solver lm_cuda_pcg9_3 -i 5 -o out.txt
     python -m g2o_b200.cli --input graph.g2o -o graph_opt.g2o --solver lm_cuda -i 20
 
 (g2o_b200/g2o_cuda_cli is the native counterpart for .g2o files, with g2o_cli's
@@ -22,6 +23,8 @@ CONFIGS = {
     "ba_small": lambda: synth.bundle_adjustment(num_cameras=100, num_points=20000, seed=99),
     "pg2d": lambda: synth.pose_graph_2d(),
     "pg3d": lambda: synth.pose_graph_3d(),
+    "bal": lambda: synth.bal_problem(),
+    "bal_small": lambda: synth.bal_problem(num_cameras=60, num_points=8000, seed=98),
     "windows": None,  # batched local BA windows (synth.windows), see run_windows
 }
 
@@ -54,7 +57,9 @@ def main(argv=None):
     ap.add_argument("--listSolvers", action="store_true")
     ap.add_argument("--windows", type=int, default=512, help="windows: how many of the 512 local BA windows")
     ap.add_argument("--input", help="a .g2o file to optimize instead of a synthetic configuration")
-    ap.add_argument("-o", "--output", help="with --input: write the optimized graph here")
+    ap.add_argument("-o", "--output", help="with --input / --bal: write the optimized graph here")
+    ap.add_argument("--bal", help="a BAL problem file (the input of g2o's bal_example) to optimize, e.g. with "
+                                  "--solver lm_cuda_pcg9_3")
     a = ap.parse_args(argv)
     fac = backend.OptimizationAlgorithmFactory.instance()
     if a.listSolvers:
@@ -67,7 +72,10 @@ def main(argv=None):
     if a.config == "windows":
         return run_windows(a, params)
     gfile = None
-    if a.input:
+    if a.bal:
+        from .bal import read_bal
+        g = read_bal(a.bal)
+    elif a.input:
         from .g2ofile import G2oFile
         gfile = G2oFile.load(a.input)
         gid = gfile.fix_gauge()
@@ -91,6 +99,11 @@ def main(argv=None):
         print(f"# kernel launches: {total}")
         for k, (n, ms) in sorted(ks.items(), key=lambda kv: -kv[1][1]):
             print(f"#   {k:20s} {n:7d} {ms:10.3f} ms")
+    if a.bal and a.output:
+        from .bal import write_bal
+        out = g.copy()
+        out.pose_estimate, out.point_estimate = prob.estimates()
+        write_bal(out, a.output)
     if gfile is not None and a.output:
         pose, point = prob.estimates()
         gfile.set_estimates(pose, point)

@@ -17,6 +17,7 @@
 
 #include "adjoint_kernels.cuh"
 #include "ba_kernels.cuh"
+#include "bal_kernels.cuh"
 #include "batch_kernels.cuh"
 #include "cholesky.cuh"
 #include "g2oc_internal.h"
@@ -192,7 +193,7 @@ struct g2oc_ctx {
   // linear system lists
   g2oc::DBuf<int> sys_perm, sys_rptr, sys_rcol, sys_brow, sys_diag, sys_cptr, sys_cblk, sys_chunk_ptr, sys_chunk_row,
       tile_ij, tile_off;
-  int pcg_grid[4] = {0, 0, 0, 0};  // CTAs of the persistent PCG per (storage type, block size)
+  int pcg_grid[6] = {0, 0, 0, 0, 0, 0};  // CTAs of the persistent PCG per (storage type, block size 3 / 6 / 9)
   int tile_grid[2] = {0, 0};       // CTAs of the dense-tile PCG per storage type
   // FP64 vectors
   g2oc::DBuf<double> b, x, xs, rhs, resid, dx, partials, errbuf, db;
@@ -631,7 +632,7 @@ template <typename Real, int BS>
 static int run_pcg_persistent(g2oc_ctx* c, const SysDev<Real>& A, const double* minv, const double* rhs,
                               double* xout, double* r, double* s, double* d, double* tbuf, double* cpart,
                               bool fixed_d0) {
-  int& grid = c->pcg_grid[(sizeof(Real) == 4 ? 2 : 0) + (BS == 6 ? 1 : 0)];
+  int& grid = c->pcg_grid[(sizeof(Real) == 4 ? 3 : 0) + (BS == 9 ? 2 : BS == 6 ? 1 : 0)];
   if (grid == 0) {
     int per_sm = 0, sms = 0;
     G2OC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_solve_persistent<Real, BS>,
@@ -1614,11 +1615,211 @@ struct Engine final : EngineBase {
   }
 };
 
+// BlockSolver<9,3> of the BAL path (g2o/examples/bal/bal_example.cpp:227-250,
+// g2o/core/block_solver.hpp): landmark and camera passes of buildSystem, the
+// Schur complement of the 9 x 9 camera blocks, block-Jacobi PCG
+// (LinearSolverPCG) or the dense Cholesky on it, landmark back-substitution.
+// FP64.
+struct BalEngine final : EngineBase {
+  g2oc_ctx* c;
+  DBuf<double> hpp, hll, hpl, dinv, Y, Sval, minv, r, s, d, tbuf, cpart;
+  explicit BalEngine(g2oc_ctx* ctx) : c(ctx) {}
+
+  int alloc() override {
+    const Structure& S = c->S;
+    const size_t nh = S.hpl_rc.size() / 2;
+    G2OC_TRY(hpp.alloc((size_t)S.Cf * 81 + 1));
+    G2OC_TRY(hll.alloc((size_t)S.Pf * 6 + 1));
+    G2OC_TRY(hpl.alloc(nh * 27 + 1));
+    G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
+    G2OC_TRY(Y.alloc(nh * 27 + 1));
+    G2OC_TRY(Sval.alloc((size_t)S.sys_nnzb * 81 + 1));
+    const size_t n = (size_t)S.Cf * 9;
+    G2OC_TRY(minv.alloc((size_t)S.Cf * 81 + 1));
+    G2OC_TRY(r.alloc(n + 1));
+    G2OC_TRY(s.alloc(n + 1));
+    G2OC_TRY(d.alloc(n + 1));
+    G2OC_TRY(tbuf.alloc((size_t)S.sys_nnzb * 9 + 1));
+    G2OC_TRY(cpart.alloc(S.sys_chunk_row.size() * 9 + 1));
+    return G2OC_OK;
+  }
+
+  SysDev<double> sys(const double* val) {
+    SysDev<double> A;
+    A.nb = c->S.sys_nb;
+    A.nnzb = c->S.sys_nnzb;
+    A.rptr = c->sys_rptr.p;
+    A.rcol = c->sys_rcol.p;
+    A.brow = c->sys_brow.p;
+    A.diag = c->sys_diag.p;
+    A.cptr = c->sys_cptr.p;
+    A.cblk = c->sys_cblk.p;
+    A.perm = c->sys_perm.p;
+    A.val = val;
+    return A;
+  }
+
+  int build_system() override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.Pf > 0) {
+      G2OC_K(K_LANDMARK_PASS) bal_landmark_pass<<<cdiv(S.Pf, 128), 128, 0, st>>>(
+          c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, hll.p, hpl.p, c->b.p + (size_t)S.Cf * 9);
+      G2OC_LAUNCH_CHECK();
+    }
+    if (S.Cf > 0) {
+      G2OC_K(K_CAMERA_PASS) bal_camera_pass<128><<<S.Cf, 128, 0, st>>>(c->ba_cam_edges(), c->ba_vertices(), hpp.p,
+                                                                       c->b.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    return G2OC_OK;
+  }
+
+  int max_diag() override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    G2OC_K(K_MAX_DIAG) bal_max_diag<<<kRedBlocks, 256, 0, st>>>(hpp.p, S.Cf, hll.p, S.Pf, c->partials.p);
+    G2OC_LAUNCH_CHECK();
+    G2OC_K(K_REDUCE) finalize_max_kernel<<<1, 256, 0, st>>>(c->partials.p, kRedBlocks, &c->sc.p->max_diag);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int multiply_hessian(const double* src, double* dst) override {
+    const int n = c->vec_size();
+    if (n <= 0) return G2OC_OK;
+    G2OC_K(K_LM_CONTROL) bal_hpp_mult<<<cdiv(n, 256), 256, 0, c->stream>>>(c->S.Cf, hpp.p, src, dst, n);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  // Dinv, Y and S = Hpp + lambda - Hpl (H_ll + lambda)^-1 Hpl^T with the
+  // reduced right-hand side bs (optional)
+  int schur(double lambda, double* bs) {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    if (S.Pf > 0) {
+      G2OC_K(K_SCHUR_LANDMARK) bal_schur_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(
+          hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, Y.p, c->flag.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    if (S.Cf == 0) return G2OC_OK;
+    G2OC_K(K_SCHUR_BLOCKS) bal_schur_blocks<<<cdiv(S.sys_nnzb, kBalSchurWarps), kBalSchurWarps * 32, 0, st>>>(
+        S.sys_nnzb, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, c->s_pair_ptr.p, c->s_pairs.p, c->hc_ptr.p,
+        c->hc_blk.p, c->hpl_col.p, hpp.p, hpl.p, Y.p, lambda, c->b.p, c->b.p + (size_t)S.Cf * 9, Sval.p, bs);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int backsub(const double* rl, const double* xp, double* xl) {
+    const Structure& S = c->S;
+    if (S.Pf == 0) return G2OC_OK;
+    G2OC_K(K_BACKSUB) bal_backsub<<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(c->hb_ptr.p, c->hpl_row.p, S.Pf, hpl.p,
+                                                                          dinv.p, rl, xp, xl);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int solve(double lambda) override {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    int ok = 1;
+    const double* bl = c->b.p + (size_t)S.Cf * 9;
+    if (S.Cf == 0) {
+      // every camera fixed: x_l = (H_ll + lambda I)^-1 b_l
+      G2OC_CUDA_TRY(cudaMemsetAsync(c->x.p, 0, c->x.bytes(), st));
+      G2OC_TRY(schur(lambda, nullptr));
+      G2OC_TRY(backsub(bl, c->xs.p, c->x.p));
+    } else {
+      cudaEvent_t ts = c->cur_stats ? c->mark() : nullptr;
+      G2OC_TRY(schur(lambda, c->rhs.p));
+      if (ts) c->span(ts, &c->cur_stats->time_schur_complement, &c->cur_stats->time_linear_solver);
+      SysDev<double> A = sys(Sval.p);
+      if (c->prm.linear_solver == G2OC_LINEAR_CHOLESKY) {
+        if (!c->chol) {
+          std::unique_ptr<CholPlan> P(new CholPlan());
+          G2OC_TRY(chol_plan_build(*P, S.sys_nb, 9, S.schur ? S.schur_rc : S.hpp_rc, false, st));
+          c->chol = std::move(P);
+        }
+        G2OC_TRY(g2oc::chol_solve<double>(*c->chol, st, A, c->rhs.p, c->xs.p, &ok, &c->kcount[K_CHOLESKY]));
+      } else {
+        G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<double, 9><<<cdiv(A.nb, 128), 128, 0, st>>>(A, minv.p, c->flag.p);
+        G2OC_LAUNCH_CHECK();
+        const int rc = run_pcg_persistent<double, 9>(c, A, minv.p, c->rhs.p, c->xs.p, r.p, s.p, d.p, tbuf.p,
+                                                     cpart.p, false);
+        if (rc != G2OC_OK) return rc;
+      }
+      G2OC_CUDA_TRY(cudaMemcpyAsync(c->x.p, c->xs.p, (size_t)S.Cf * 9 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                    st));
+      G2OC_TRY(backsub(bl, c->xs.p, c->x.p + (size_t)S.Cf * 9));
+    }
+    G2OC_K(K_LM_CONTROL) set_solve_ok<<<1, 32, 0, st>>>(c->sc.p, ok);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
+  int get_hessian(double* hpp_out, double* hll_out, double* hpl_out) override {
+    const Structure& S = c->S;
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (hpp_out && S.Cf > 0)
+      G2OC_CUDA_TRY(cudaMemcpy(hpp_out, hpp.p, (size_t)S.Cf * 81 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (hll_out && S.Pf > 0) {
+      std::vector<double> h((size_t)S.Pf * 6);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), hll.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int l = 0; l < S.Pf; ++l) {
+        const double* a = h.data() + (size_t)l * 6;
+        double* o = hll_out + (size_t)l * 9;
+        o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
+        o[3] = a[1]; o[4] = a[3]; o[5] = a[4];
+        o[6] = a[2]; o[7] = a[4]; o[8] = a[5];
+      }
+    }
+    if (hpl_out && !S.hpl_rc.empty())
+      G2OC_CUDA_TRY(cudaMemcpy(hpl_out, hpl.p, S.hpl_rc.size() / 2 * 27 * sizeof(double), cudaMemcpyDeviceToHost));
+    return G2OC_OK;
+  }
+
+  int schur_export(double lambda, double* S_out, double* bs_out) override {
+    const Structure& S = c->S;
+    if (!S.schur) {
+      set_error("the graph has no Schur complement (no marginalized vertices)");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    G2OC_TRY(schur(lambda, c->rhs.p));
+    G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (S_out) {
+      std::vector<double> h((size_t)S.sys_nnzb * 81);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), Sval.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int k = 0; k < S.sys_nnzb; ++k) {
+        const int rr = S.sys_brow[k], rb = S.sys_rptr[rr], nblk = S.sys_rptr[rr + 1] - rb;
+        for (int e = 0; e < 81; ++e) S_out[(size_t)S.sys_perm[k] * 81 + e] = h[sys_offset<9>(rb, nblk, k - rb, e)];
+      }
+    }
+    if (bs_out) G2OC_CUDA_TRY(cudaMemcpy(bs_out, c->rhs.p, (size_t)S.Cf * 9 * sizeof(double), cudaMemcpyDeviceToHost));
+    return G2OC_OK;
+  }
+
+  int solve_rhs(const double*, double*, bool) override {
+    set_error("the adjoint solve is built for the SE3 bundle adjustment, not for BAL cameras");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  int batch_lambda_init(double, double) override {
+    set_error("batched windows take SE3 bundle adjustments");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+  int batch_solve(bool) override {
+    set_error("batched windows take SE3 bundle adjustments");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
+};
+
 // ------------------------------------------------------------ driver ops
 static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba && S.D == 3)
+  if (S.bal)
+    G2OC_K(K_CHI2) bal_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
+  else if (S.ba && S.D == 3)
     G2OC_K(K_CHI2) st_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.ba) G2OC_K(K_CHI2) ba_chi2_kernel<<<kChi2Blocks, 256, 0, st>>>(c->ba_edges(), c->ba_vertices(), c->partials.p);
   else if (S.pose_type == G2OC_POSE_SE2)
@@ -1635,7 +1836,10 @@ static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
 static int oplus(g2oc_ctx* c) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (S.ba) G2OC_K(K_OPLUS) ba_oplus<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
+  if (S.bal)
+    G2OC_K(K_OPLUS) bal_oplus<<<cdiv((long long)S.Cf * 9 + (long long)S.Pf * 3, 256), 256, 0, st>>>(
+        c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
+  else if (S.ba) G2OC_K(K_OPLUS) ba_oplus<<<cdiv(S.Cf + S.Pf, 256), 256, 0, st>>>(c->ba_vertices(), S.Cf, S.Pf, c->x.p, c->flag.p);
   else if (S.pose_type == G2OC_POSE_SE2)
     G2OC_K(K_OPLUS) pg_oplus<G2OC_POSE_SE2><<<cdiv(S.Cf, 128), 128, 0, st>>>(c->pose.p, c->free_pose.p, S.Cf, c->x.p,
                                                              c->oplus_count.p, c->flag.p);
@@ -1955,8 +2159,8 @@ static int dl_iteration(g2oc_ctx* c, int iteration, g2oc_iteration_stats* stv, i
 
 static int structure_only(g2oc_ctx* c, int num_iters, int num_max_trials) {
   const Structure& S = c->S;
-  if (!S.ba || S.D != 2) {
-    set_error("the structure-only solver optimizes the landmarks of a bundle adjustment with two-row projection edges");
+  if (!S.ba || S.D != 2 || S.bal) {
+    set_error("the structure-only solver optimizes the landmarks of an SE3 bundle adjustment with two-row projection edges");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   if (S.Pf == 0 || num_iters <= 0) return G2OC_OK;
@@ -2052,6 +2256,8 @@ static const char* kSolvers[][2] = {
     {"lm_cuda_pcg6_3", "Levenberg: B200 BlockSolver<6,3>, FP64, block-Jacobi PCG"},
     {"gn_cuda_pcg3_3", "Gauss-Newton: B200 BlockSolver<3,3>, FP64, block-Jacobi PCG"},
     {"lm_cuda_pcg3_3", "Levenberg: B200 BlockSolver<3,3>, FP64, block-Jacobi PCG"},
+    {"gn_cuda_pcg9_3", "Gauss-Newton: B200 BlockSolver<9,3> (BAL cameras), FP64, block-Jacobi PCG"},
+    {"lm_cuda_pcg9_3", "Levenberg: B200 BlockSolver<9,3> (BAL cameras), FP64, block-Jacobi PCG"},
     {"gn_cuda_chol", "Gauss-Newton: B200 block solver, FP64, dense Cholesky"},
     {"lm_cuda_chol", "Levenberg: B200 block solver, FP64, dense Cholesky"},
     {"gn_cuda_mixed", "Gauss-Newton: B200 block solver, FP32 Hessian/Schur/PCG with FP64 refinement"},
@@ -2175,7 +2381,13 @@ void g2oc_destroy(g2oc_ctx* c) {
 }
 
 static int make_engine(g2oc_ctx* c) {
-  if (c->prm.precision == G2OC_PREC_MIXED) c->eng.reset(new Engine<float>(c));
+  if (c->S.bal) {
+    if (c->prm.precision == G2OC_PREC_MIXED) {
+      set_error("the BAL block solver runs in FP64 (no mixed-precision form)");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
+    c->eng.reset(new BalEngine(c));
+  } else if (c->prm.precision == G2OC_PREC_MIXED) c->eng.reset(new Engine<float>(c));
   else c->eng.reset(new Engine<double>(c));
   G2OC_TRY(c->eng->alloc());
   c->system_built = false;
@@ -2258,11 +2470,12 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
   cudaStream_t st = c->stream;
   const int na = (int)S.act.size();
   if (S.ba) {
-    G2OC_TRY(c->pose.alloc((size_t)S.C * 8));
+    // SE3Quat cameras packed 8 doubles apart; BAL cameras as given (9)
+    G2OC_TRY(c->pose.alloc((size_t)S.C * (S.bal ? kBalCam : 8)));
     G2OC_TRY(c->point.alloc((size_t)S.P * 4));
     G2OC_TRY(c->point_bak.alloc(c->point.n));
     G2OC_TRY(c->point_init.alloc(c->point.n));
-    G2OC_TRY(c->raw_pose.alloc((size_t)S.C * 7));
+    G2OC_TRY(c->raw_pose.alloc(S.bal ? 1 : (size_t)S.C * 7));
     G2OC_TRY(c->raw_point.alloc((size_t)S.P * 3));
   } else {
     G2OC_TRY(c->pose.alloc((size_t)S.C * S.ped));
@@ -2388,7 +2601,9 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
 static int upload_ba_estimates(g2oc_ctx* c, const double* pose, const double* point) {
   const Structure& S = c->S;
   cudaStream_t st = c->stream;
-  if (pose && S.C > 0) {
+  if (pose && S.C > 0 && S.bal) {
+    G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, pose, c->pose.bytes(), cudaMemcpyHostToDevice, st));
+  } else if (pose && S.C > 0) {
     G2OC_CUDA_TRY(cudaMemcpyAsync(c->raw_pose.p, pose, c->raw_pose.bytes(), cudaMemcpyHostToDevice, st));
     G2OC_K(K_IO) ba_pack_poses<<<cdiv((long long)S.C * 8, 256), 256, 0, st>>>(S.C, c->raw_pose.p, c->pose.p);
     G2OC_LAUNCH_CHECK();
@@ -2550,7 +2765,9 @@ int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
   cudaStream_t st = c->stream;
   if (S.ba) {
     // reorder into the caller's layout on the device, then one copy each
-    if (pose && S.C > 0) {
+    if (pose && S.C > 0 && S.bal) {
+      G2OC_CUDA_TRY(cudaMemcpyAsync(pose, c->pose.p, c->pose.bytes(), cudaMemcpyDeviceToHost, st));
+    } else if (pose && S.C > 0) {
       G2OC_K(K_IO) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, st>>>(S.C, c->pose.p, c->raw_pose.p);
       G2OC_LAUNCH_CHECK();
       G2OC_CUDA_TRY(cudaMemcpyAsync(pose, c->raw_pose.p, c->raw_pose.bytes(), cudaMemcpyDeviceToHost, st));
@@ -2697,7 +2914,9 @@ int g2oc_errors(g2oc_ctx* c, double* out) {
   if (!out) return G2OC_ERR_INVALID_ARGUMENT;
   const Structure& S = c->S;
   const int na = (int)S.act.size();
-  if (S.ba && S.D == 3)
+  if (S.bal)
+    G2OC_K(K_ERRORS) bal_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
+  else if (S.ba && S.D == 3)
     G2OC_K(K_ERRORS) st_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
   else if (S.ba) G2OC_K(K_ERRORS) ba_errors_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), c->errbuf.p);
   else if (S.pose_type == G2OC_POSE_SE2)
@@ -2724,7 +2943,9 @@ int g2oc_jacobians(g2oc_ctx* c, double* j0, double* j1) {
   DBuf<double> a, b;
   G2OC_TRY(a.alloc((size_t)na * D * d0));
   G2OC_TRY(b.alloc((size_t)na * D * d1));
-  if (S.ba && S.D == 3)
+  if (S.bal)
+    G2OC_K(K_JACOBIANS) bal_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
+  else if (S.ba && S.D == 3)
     G2OC_K(K_JACOBIANS) st_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
   else if (S.ba) G2OC_K(K_JACOBIANS) ba_jacobians_kernel<<<cdiv(na, 128), 128, 0, c->stream>>>(c->ba_edges(), c->ba_vertices(), a.p, b.p);
   else if (S.pose_type == G2OC_POSE_SE2)
@@ -2883,8 +3104,8 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
     return G2OC_ERR_INVALID_ARGUMENT;
   }
   const Structure& S = c->S;
-  if (!S.ba || !S.schur || S.Cf == 0 || S.D != 2) {
-    set_error("g2oc_backward supports bundle adjustment with two-row projection edges, free cameras and landmarks");
+  if (!S.ba || !S.schur || S.Cf == 0 || S.D != 2 || S.bal) {
+    set_error("g2oc_backward supports SE3 bundle adjustment with two-row projection edges, free cameras and landmarks");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   cudaStream_t st = c->stream;
@@ -3113,8 +3334,8 @@ int g2oc_upload_windows(g2oc_ctx* c, int32_t num_windows, const g2oc_graph* w) {
   const bool same_windows = was_batch && c->last_upload_reused && old_nw == num_windows && old_pose == pose_off &&
                             old_point == point_off;
   const Structure& S = c->S;
-  if (!S.ba || !S.schur) {
-    set_error("batched windows need free landmarks (Schur complement)");
+  if (!S.ba || !S.schur || S.bal) {
+    set_error("batched windows need SE3 cameras and free landmarks (Schur complement)");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   // window ranges: free cameras and landmarks are numbered in vertex order, so

@@ -76,6 +76,7 @@ struct Structure {
   int C = 0, P = 0, E = 0;
   int pd = 0, ped = 0, D = 0, md = 0;
   bool ba = false, schur = false;
+  bool bal = false;  // EdgeObservationBAL + VertexCameraBAL (9-parameter cameras, bal_kernels.cuh)
   std::vector<int> act;                 // active edge ids, insertion order
   std::vector<int> pose_h, point_l;     // Hessian index of each pose / landmark index of each point, -1 = none
   std::vector<int> free_pose_of_h;      // pose index of Hessian row h

@@ -30,8 +30,10 @@ int meas_dim(int et) {
          : et == G2OC_EDGE_SE3_EXPMAP                                    ? 7
                                                                          : 2;
 }
-int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
-int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
+int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_BAL_CAMERA ? 9 : 6; }
+int pose_est_dim(int pt) {
+  return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : pt == G2OC_POSE_BAL_CAMERA ? 9 : 7;
+}
 
 // stable counting sort of items by key in [0, nkeys): returns the order and
 // the CSR pointer over keys
@@ -84,7 +86,7 @@ static void build_tiles(int nb, Structure& s) {
   s.tile_ij.clear();
   s.tile_off.clear();
   const int nnzb = s.sys_nnzb;
-  if (nb < 2 * kTileBlocks) return;
+  if (nb < 2 * kTileBlocks || s.pd != 6) return;  // the tiles hold 6 x 6 blocks
   const int nbt = (nb + kTileBlocks - 1) / kTileBlocks;
   std::vector<int> id((size_t)nbt * nbt, -1);
   for (int k = 0; k < nnzb; ++k) {
@@ -270,7 +272,7 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     }
     // (the edge-parallel passes are written for the two-row projection
     // edges; the stereo edge's landmarks take the thread-per-landmark ones)
-    s.lm_warp_ok = ok && s.Pf > 0 && s.D == 2;
+    s.lm_warp_ok = ok && s.Pf > 0 && s.D == 2 && !s.bal;
     s.lm_chunk_ptr.clear();
     s.e_lm.clear();
     if (s.lm_warp_ok) {
@@ -555,12 +557,14 @@ int build_structure(const g2oc_graph* g, Structure& s) {
     set_error("graph is NULL");
     return G2OC_ERR_INVALID_ARGUMENT;
   }
+  const bool bal = g->edge_type == G2OC_EDGE_BAL_OBSERVATION;
   const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ||
-                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 6 ||
+                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ || bal;
+  if (g->pose_type < 1 || g->pose_type > 4 || g->edge_type < 1 || g->edge_type > 7 ||
       (g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2) ||
       (g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3) ||
-      (ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {
+      bal != (g->pose_type == G2OC_POSE_BAL_CAMERA) ||
+      ((ba && !bal) || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) {
     set_error("unsupported vertex/edge type combination (pose %d, edge %d)", g->pose_type, g->edge_type);
     return G2OC_ERR_BAD_GRAPH;
   }
@@ -576,6 +580,7 @@ int build_structure(const g2oc_graph* g, Structure& s) {
   s.pose_type = g->pose_type;
   s.edge_type = g->edge_type;
   s.ba = ba;
+  s.bal = bal;
   s.C = g->num_poses;
   s.P = ba ? g->num_points : 0;
   s.E = g->num_edges;

@@ -13,6 +13,10 @@ benchmark configurations:
 * ``pose_graph_3d``  2,500 VertexSE3 on 10 rings x 250 on a 50 m sphere, EdgeSE3.
 * ``bundle_adjustment``  1,000 VertexSE3Expmap on a 30 m ring, 200,000
   VertexPointXYZ in a 20x20x5 m box, ~1.0M EdgeProjectXYZ2UV, Huber.
+* ``bal_problem``  the same scene seen by 356 BAL cameras (angle-axis pose,
+  focal length, two radial distortion terms), ~227k points, ~1.2M
+  EdgeObservationBAL (the shape of the Dubrovnik-356 problem of the BAL
+  collection, whose files are not shipped), no robust kernel, nothing fixed.
 
 Every generator takes a seed; the benchmark configurations use
 20261203 + configuration index.
@@ -23,8 +27,8 @@ import math
 
 import numpy as np
 
-from .abi import (EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_EXPMAP, EDGE_SE3_PROJECT_XYZ, EDGE_SE3,
-                  EDGE_STEREO_SE3_PROJECT_XYZ, POSE_SE2, POSE_SE3,
+from .abi import (EDGE_BAL_OBSERVATION, EDGE_PROJECT_XYZ2UV, EDGE_SE2, EDGE_SE3_EXPMAP, EDGE_SE3_PROJECT_XYZ,
+                  EDGE_SE3, EDGE_STEREO_SE3_PROJECT_XYZ, POSE_BAL_CAMERA, POSE_SE2, POSE_SE3,
                   POSE_SE3EXPMAP, Graph)
 
 SEED_BASE = 20261203
@@ -158,6 +162,63 @@ def _axis_angle(v):
         a = np.where(th > 1e-12, _sin(th) / th, 1.0)
         b = np.where(th > 1e-12, (1 - _cos(th)) / (th * th), 0.5)
     return np.eye(3) + a * K + b * _mm(K, K)
+
+
+_ATAN_C = [(-1.0) ** k / (2 * k + 1) for k in range(14)]
+
+
+def _atan(x):
+    """arctan of x >= 0 from +, -, *, / and sqrt only (each correctly
+    rounded, so the same bits on every CPU): x > 1 reflected to 1 / x, three
+    half-angle steps atan(y) = 2 atan(y / (1 + sqrt(1 + y^2))) bring the
+    argument below tan(pi / 32), then the Taylor series to y^27."""
+    x = np.asarray(x, dtype=np.float64)
+    inv = x > 1.0
+    with np.errstate(divide="ignore"):
+        y = np.where(inv, 1.0 / np.where(inv, x, 1.0), x)
+    for _ in range(3):
+        y = y / (1.0 + np.sqrt(1.0 + y * y))
+    y2 = y * y
+    s = np.full_like(y, _ATAN_C[-1])
+    for c in reversed(_ATAN_C[:-1]):
+        s = s * y2 + c
+    a = 8.0 * (s * y)
+    return np.where(inv, (_HALF_PI_HI - a) + _HALF_PI_LO, a)
+
+
+def _rot_to_angle_axis(R):
+    """Rotation matrices (..., 3, 3) -> angle-axis vectors (..., 3), angle in [0, pi]."""
+    q = _rot_to_quat(R)
+    v, w = q[..., :3], q[..., 3]
+    s = _norm(v)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        th = np.where(w > 0.0, 2.0 * _atan(s / np.where(w > 0.0, w, 1.0)), np.pi)
+        k = np.where(s > 0.0, th / np.where(s > 0.0, s, 1.0), 0.0)
+    return v * k[..., None]
+
+
+def bal_project(cam, X):
+    """EdgeObservationBAL's prediction (g2o/examples/bal/bal_example.cpp:160-200)
+    for cameras (..., 9) and points (..., 3): Rodrigues rotation, translation,
+    p = -P(0:2) / P(2), f (1 + k1 |p|^2 + k2 |p|^4) p."""
+    w = cam[..., 0:3]
+    th2 = (w[..., 0] * w[..., 0] + w[..., 1] * w[..., 1]) + w[..., 2] * w[..., 2]
+    th = np.sqrt(th2)
+    safe = np.where(th > 0.0, th, 1.0)
+    v = w / safe[..., None]
+    sth, cth = _sincos(th)
+    vxp = np.stack([v[..., 1] * X[..., 2] - v[..., 2] * X[..., 1], v[..., 2] * X[..., 0] - v[..., 0] * X[..., 2],
+                    v[..., 0] * X[..., 1] - v[..., 1] * X[..., 0]], -1)
+    vdp = (v[..., 0] * X[..., 0] + v[..., 1] * X[..., 1]) + v[..., 2] * X[..., 2]
+    P = (X * cth[..., None] + vxp * sth[..., None]) + (v * vdp[..., None]) * (1.0 - cth)[..., None]
+    wxp = np.stack([w[..., 1] * X[..., 2] - w[..., 2] * X[..., 1], w[..., 2] * X[..., 0] - w[..., 0] * X[..., 2],
+                    w[..., 0] * X[..., 1] - w[..., 1] * X[..., 0]], -1)
+    P = np.where((th2 > 0.0)[..., None], P, X + wxp) + cam[..., 3:6]
+    p0, p1 = -P[..., 0] / P[..., 2], -P[..., 1] / P[..., 2]
+    r2 = p0 * p0 + p1 * p1
+    rp = (1.0 + cam[..., 7] * r2) + (cam[..., 8] * r2) * r2
+    fr = cam[..., 6] * rp
+    return np.stack([fr * p0, fr * p1], -1)
 
 
 def _compact_quat_noise(rng, n, sigma):
@@ -424,6 +485,48 @@ def stereo_bundle_adjustment(num_cameras=100, num_points=20_000, baseline=0.12, 
     return s
 
 
+def bal_problem(num_cameras=356, num_points=226_730, mean_obs=5.5, focal=500.0, k1=(-0.05, 0.05),
+                k2=(-0.01, 0.01), pixel_noise=1.0, pose_noise=(0.05, 0.01), focal_noise=0.01, point_noise=0.1,
+                seed=SEED_BASE + 6, **kw):
+    """A BAL problem (g2o/examples/bal/bal_example.cpp: VertexCameraBAL,
+    VertexPointBAL, EdgeObservationBAL, identity information, no robust
+    kernel, no fixed vertex) on the ring scene of bundle_adjustment: the same
+    visibility, the cameras turned half a turn about their x axis (BAL
+    cameras look down -z, image y up), measurements from the BAL projection
+    with per-camera focal length and radial distortion plus pixel noise. The
+    initial guess perturbs the angle-axis, translation and focal length and
+    starts the distortion at zero."""
+    g = bundle_adjustment(num_cameras=num_cameras, num_points=num_points, mean_obs=mean_obs, focal=focal,
+                          pixel_noise=0.0, outlier_ratio=0.0, num_fixed=0, seed=seed, **kw)
+    rng = np.random.default_rng(seed + 104729)
+    tp, X = g.extra["truth_pose"], g.extra["truth_point"]
+    flip = np.diag([1.0, -1.0, -1.0])
+    Rb = _mm(np.broadcast_to(flip, (num_cameras, 3, 3)), _quat_to_rot(tp[:, 3:7]))
+    tb = tp[:, :3] * np.array([1.0, -1.0, -1.0])
+    cam = np.empty((num_cameras, 9))
+    cam[:, 0:3] = _rot_to_angle_axis(Rb)
+    cam[:, 3:6] = tb
+    cam[:, 6] = focal * (1.0 + rng.uniform(-0.02, 0.02, num_cameras))
+    cam[:, 7] = rng.uniform(k1[0], k1[1], num_cameras)
+    cam[:, 8] = rng.uniform(k2[0], k2[1], num_cameras)
+    pts, cams = g.edge_vertex[:, 0], g.edge_vertex[:, 1]
+    E = g.num_edges
+    meas = bal_project(cam[cams], X[pts]) + rng.normal(0.0, pixel_noise, size=(E, 2))
+    cam0 = cam.copy()
+    cam0[:, 0:3] += rng.normal(0.0, pose_noise[1], size=(num_cameras, 3))
+    cam0[:, 3:6] += rng.normal(0.0, pose_noise[0], size=(num_cameras, 3))
+    cam0[:, 6] *= 1.0 + rng.normal(0.0, focal_noise, num_cameras)
+    cam0[:, 7:9] = 0.0
+    X0 = X + rng.normal(0.0, point_noise, size=X.shape)
+    info = np.tile(np.eye(2).reshape(1, 4), (E, 1))
+    b = Graph(POSE_BAL_CAMERA, EDGE_BAL_OBSERVATION, cam0, g.edge_vertex, meas, info,
+              pose_fixed=np.zeros(num_cameras, np.uint8), point_estimate=X0,
+              point_fixed=np.zeros(len(X), np.uint8), name=f"bal_{num_cameras}x{len(X)}")
+    b.extra["truth_pose"] = cam
+    b.extra["truth_point"] = X
+    return b
+
+
 def window_sizes(num_windows=512, cameras=(10, 60), points=(500, 8000), seed=SEED_BASE + 1000):
     """(cameras, points) of each window: log-uniform in the given ranges."""
     rng = np.random.default_rng(seed)
@@ -480,4 +583,5 @@ CONFIGS = {
     "pg2d": lambda: pose_graph_2d(),
     "pg3d": lambda: pose_graph_3d(),
     "ba": lambda: bundle_adjustment(),
+    "bal": lambda: bal_problem(),
 }

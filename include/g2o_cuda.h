@@ -69,7 +69,8 @@
 extern "C" {
 #endif
 
-#define G2OC_ABI_VERSION 3 /* 3: g2oc_graph.stereo_bf (EdgeStereoSE3ProjectXYZ); 2: focal_length_y */
+#define G2OC_ABI_VERSION 4 /* 4: the BAL camera and observation types; 3: g2oc_graph.stereo_bf
+                             (EdgeStereoSE3ProjectXYZ); 2: focal_length_y */
 
 /* status codes */
 #define G2OC_OK 0
@@ -89,6 +90,8 @@ extern "C" {
 #define G2OC_POSE_SE2 1        /* VertexSE2: estimate (x, y, theta) */
 #define G2OC_POSE_SE3 2        /* VertexSE3: Isometry3, 12 doubles: R row-major (9) then t (3) */
 #define G2OC_POSE_SE3EXPMAP 3  /* VertexSE3Expmap: SE3Quat::toVector (tx,ty,tz,qx,qy,qz,qw) */
+#define G2OC_POSE_BAL_CAMERA 4 /* VertexCameraBAL (g2o/examples/bal/bal_example.cpp:67-93): 9 doubles
+                                  (rx, ry, rz angle-axis, tx, ty, tz, f, k1, k2), additive update */
 
 #define G2OC_EDGE_SE2 1            /* EdgeSE2(VertexSE2, VertexSE2), D=3, measurement (x,y,theta) */
 #define G2OC_EDGE_SE3 2            /* EdgeSE3(VertexSE3, VertexSE3), D=6, measurement Isometry3 (12) */
@@ -101,6 +104,13 @@ extern "C" {
                                             measurement (u_left, v_left, u_right); fx, fy, (cx, cy) as
                                             SE3_PROJECT_XYZ and bf = stereo_bf
                                             (g2o/types/sba/edge_project_stereo_xyz.h:38-77) */
+#define G2OC_EDGE_BAL_OBSERVATION 7 /* EdgeObservationBAL(VertexCameraBAL, VertexPointBAL), D=2
+                                       (g2o/examples/bal/bal_example.cpp:143-203): error = prediction -
+                                       measurement with the radial-distortion pinhole model. As for every
+                                       projection edge of this ABI, vertex0 is the point and vertex1 the
+                                       camera (the reverse of the class's vertex order), and the Jacobians
+                                       are j0 = d e / d point (2x3), j1 = d e / d camera (2x9). Points are
+                                       the num_points array (VertexPointBAL: 3 doubles, additive). */
 
 /* algorithm / linear solver / precision */
 #define G2OC_ALGO_GAUSS_NEWTON 0
@@ -123,7 +133,7 @@ extern "C" {
 typedef struct g2oc_graph {
   int32_t pose_type;           /* G2OC_POSE_* */
   int32_t num_poses;
-  const double* pose_estimate; /* num_poses * {3, 12, 7} */
+  const double* pose_estimate; /* num_poses * {3, 12, 7, 9} */
   const uint8_t* pose_fixed;   /* num_poses, may be NULL (none fixed) */
   int32_t num_points;          /* VertexPointXYZ count (0 for pose graphs) */
   const double* point_estimate;/* num_points * 3 */
@@ -131,7 +141,9 @@ typedef struct g2oc_graph {
   int32_t edge_type;           /* G2OC_EDGE_* */
   int32_t num_edges;
   const int32_t* edge_vertex;  /* num_edges * 2: (vertex0, vertex1). For
-                                  PROJECT_XYZ2UV vertex0 is a point index and
+                                  the projection edges (PROJECT_XYZ2UV,
+                                  SE3_PROJECT_XYZ, STEREO_SE3_PROJECT_XYZ,
+                                  BAL_OBSERVATION) vertex0 is a point index and
                                   vertex1 a pose index; otherwise both are pose
                                   indices. */
   const double* measurement;   /* num_edges * {3, 12, 2} */

@@ -373,7 +373,7 @@ bool inverse_small(const double* A, int n, double* out) {
     out[8] = (A[0] * A[4] - A[1] * A[3]) * id;
     return std::isfinite(id);
   }
-  double M[64], I[64];
+  double M[81], I[81];
   for (int i = 0; i < n * n; ++i) M[i] = A[i];
   for (int i = 0; i < n * n; ++i) I[i] = (i / n == i % n) ? 1.0 : 0.0;
   for (int c = 0; c < n; ++c) {
@@ -412,8 +412,125 @@ int meas_dim(int et) {
          : et == G2OC_EDGE_SE3_EXPMAP                                    ? 7
                                                                          : 2;
 }
-int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : 6; }
-int pose_est_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : 7; }
+int pose_dim(int pt) { return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_BAL_CAMERA ? 9 : 6; }
+int pose_est_dim(int pt) {
+  return pt == G2OC_POSE_SE2 ? 3 : pt == G2OC_POSE_SE3 ? 12 : pt == G2OC_POSE_BAL_CAMERA ? 9 : 7;
+}
+
+// Forward-mode automatic differentiation, the method of g2o's AutoDiff
+// (g2o/core/auto_differentiation.h:52-240 over the dual numbers of
+// g2o/autodiff/jet.h): every value carries its N partial derivatives, carried
+// through + - * / sqrt sin cos by the chain rule. Only what the BAL
+// observation uses is defined.
+template <int N>
+struct Jet {
+  double a = 0.0;
+  double v[N] = {};
+  Jet() = default;
+  explicit Jet(double x) : a(x) {}
+  Jet(double x, int k) : a(x) { v[k] = 1.0; }
+};
+template <int N> Jet<N> operator+(const Jet<N>& x, const Jet<N>& y) {
+  Jet<N> r(x.a + y.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.v[i] + y.v[i];
+  return r;
+}
+template <int N> Jet<N> operator-(const Jet<N>& x, const Jet<N>& y) {
+  Jet<N> r(x.a - y.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.v[i] - y.v[i];
+  return r;
+}
+template <int N> Jet<N> operator-(const Jet<N>& x) {
+  Jet<N> r(-x.a);
+  for (int i = 0; i < N; ++i) r.v[i] = -x.v[i];
+  return r;
+}
+template <int N> Jet<N> operator*(const Jet<N>& x, const Jet<N>& y) {
+  Jet<N> r(x.a * y.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.a * y.v[i] + x.v[i] * y.a;
+  return r;
+}
+template <int N> Jet<N> operator/(const Jet<N>& x, const Jet<N>& y) {
+  // (x / y)' = (x' - (x / y) y') / y
+  Jet<N> r(x.a / y.a);
+  const double inv = 1.0 / y.a;
+  for (int i = 0; i < N; ++i) r.v[i] = (x.v[i] - r.a * y.v[i]) * inv;
+  return r;
+}
+template <int N> Jet<N> jsqrt(const Jet<N>& x) {
+  Jet<N> r(std::sqrt(x.a));
+  const double h = 1.0 / (2.0 * r.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.v[i] * h;
+  return r;
+}
+template <int N> Jet<N> jcos(const Jet<N>& x) {
+  Jet<N> r(std::cos(x.a));
+  const double d = -std::sin(x.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.v[i] * d;
+  return r;
+}
+template <int N> Jet<N> jsin(const Jet<N>& x) {
+  Jet<N> r(std::sin(x.a));
+  const double d = std::cos(x.a);
+  for (int i = 0; i < N; ++i) r.v[i] = x.v[i] * d;
+  return r;
+}
+inline double jsqrt(double x) { return std::sqrt(x); }
+inline double jcos(double x) { return std::cos(x); }
+inline double jsin(double x) { return std::sin(x); }
+inline double jval(double x) { return x; }
+template <int N> double jval(const Jet<N>& x) { return x.a; }
+
+// EdgeObservationBAL::operator() (g2o/examples/bal/bal_example.cpp:160-200):
+// Rodrigues rotation of the point by the angle-axis camera(0:3) (first-order
+// form X + w x X when |w| == 0), translation camera(3:6), perspective
+// division p = -P(0:2) / P(2), radial distortion r(p) = 1 + k1 |p|^2 +
+// k2 |p|^4, prediction f r(p) p; error = prediction - measurement. The
+// operations and their order follow the reference's expression.
+template <typename T>
+void bal_error_t(const T* cam, const T* X, const double* z, T e[2]) {
+  const T theta2 = cam[0] * cam[0] + cam[1] * cam[1] + cam[2] * cam[2];
+  T P[3];
+  if (jval(theta2) > 0.0) {
+    const T theta = jsqrt(theta2);
+    const T v[3] = {cam[0] / theta, cam[1] / theta, cam[2] / theta};
+    const T cth = jcos(theta), sth = jsin(theta);
+    const T vXp[3] = {v[1] * X[2] - v[2] * X[1], v[2] * X[0] - v[0] * X[2], v[0] * X[1] - v[1] * X[0]};
+    const T vDotp = v[0] * X[0] + v[1] * X[1] + v[2] * X[2];
+    const T oneMinusCth = T(1.0) - cth;
+    for (int i = 0; i < 3; ++i) P[i] = X[i] * cth + vXp[i] * sth + v[i] * vDotp * oneMinusCth;
+  } else {
+    P[0] = X[0] + (cam[1] * X[2] - cam[2] * X[1]);
+    P[1] = X[1] + (cam[2] * X[0] - cam[0] * X[2]);
+    P[2] = X[2] + (cam[0] * X[1] - cam[1] * X[0]);
+  }
+  for (int i = 0; i < 3; ++i) P[i] = P[i] + cam[3 + i];
+  const T p0 = -P[0] / P[2], p1 = -P[1] / P[2];
+  const T r2 = p0 * p0 + p1 * p1;
+  const T rp = T(1.0) + cam[7] * r2 + cam[8] * r2 * r2;
+  const T fr = cam[6] * rp;
+  e[0] = fr * p0 - T(z[0]);
+  e[1] = fr * p1 - T(z[1]);
+}
+
+void bal_error(const double* cam9, const double* X, const double* z, double e[2]) {
+  bal_error_t<double>(cam9, X, z, e);
+}
+
+// the Jacobians by forward-mode differentiation of bal_error_t with respect
+// to the 9 camera and 3 point estimate entries (AutoDifferentiation::linearize:
+// additive vertices, so d e / d estimate): Jp 2x3, Jc 2x9, row-major
+void bal_jacobians(const double* cam9, const double* X, const double* z, double Jp[6], double Jc[18]) {
+  using J = Jet<12>;
+  J c[9], x[3], e[2];
+  for (int i = 0; i < 9; ++i) c[i] = J(cam9[i], i);
+  for (int i = 0; i < 3; ++i) x[i] = J(X[i], 9 + i);
+  bal_error_t<J>(c, x, z, e);
+  for (int r = 0; r < 2; ++r) {
+    for (int i = 0; i < 9; ++i) Jc[r * 9 + i] = e[r].v[i];
+    for (int i = 0; i < 3; ++i) Jp[r * 3 + i] = e[r].v[9 + i];
+  }
+}
 
 // EdgeStereoSE3ProjectXYZ (g2o/types/sba/edge_project_stereo_xyz.h:52-57,
 // edge_project_stereo_xyz.cpp:34-43 and 58-106), vertex0 = point, vertex1 =
@@ -941,6 +1058,8 @@ void compute_edge_error(orc_problem* p, int e, double* out) {
   const double* m = p->meas.data() + (size_t)e * p->md;
   if (p->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
     stereo_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->fx, p->fy, p->cx, p->cy, p->bf, out);
+  else if (p->edge_type == G2OC_EDGE_BAL_OBSERVATION)
+    bal_error(pose_ptr(p, v1), point_ptr(p, v0), m, out);
   else if (p->ba)
     ba_error(pose_ptr(p, v1), point_ptr(p, v0), m, p->fx, p->fy, p->cx, p->cy, out);
   else if (p->edge_type == G2OC_EDGE_SE2)
@@ -955,6 +1074,8 @@ void compute_edge_jac(orc_problem* p, int e, double* J0, double* J1) {
   const double* m = p->meas.data() + (size_t)e * p->md;
   if (p->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ)
     stereo_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->fx, p->fy, p->bf, J0, J1);
+  else if (p->edge_type == G2OC_EDGE_BAL_OBSERVATION)
+    bal_jacobians(pose_ptr(p, v1), point_ptr(p, v0), m, J0, J1);
   else if (p->ba)
     ba_jacobians(pose_ptr(p, v1), point_ptr(p, v0), p->fx, p->fy, J0, J1);
   else if (p->edge_type == G2OC_EDGE_SE2)
@@ -1306,7 +1427,7 @@ void schur_complement(orc_problem* p) {
     for (int a = p->hpl_col_ptr[l]; a < p->hpl_col_ptr[l + 1]; ++a) {
       const int i1 = p->hpl_rc[a].first;
       const double* Bi = p->hpl.data() + (size_t)a * pd * 3;
-      double BD[18];
+      double BD[27];
       for (int r = 0; r < pd; ++r)
         for (int c = 0; c < 3; ++c)
           BD[r * 3 + c] = Bi[r * 3] * Dinv[c] + Bi[r * 3 + 1] * Dinv[3 + c] + Bi[r * 3 + 2] * Dinv[6 + c];
@@ -1384,7 +1505,10 @@ bool block_solver_solve(orc_problem* p, double* t_schur, double* t_linear) {
 
 void vertex_oplus_pose(orc_problem* p, int i, const double* u) {
   double* est = pose_ptr(p, i);
-  if (p->pose_type == G2OC_POSE_SE3EXPMAP) {
+  if (p->pose_type == G2OC_POSE_BAL_CAMERA) {
+    // VertexCameraBAL::oplusImpl (g2o/examples/bal/bal_example.cpp:88-91)
+    for (int k = 0; k < 9; ++k) est[k] += u[k];
+  } else if (p->pose_type == G2OC_POSE_SE3EXPMAP) {
     // VertexSE3Expmap::oplusImpl (g2o/types/sba/vertex_se3_expmap.cpp:48-51)
     SE3Q T = se3q_load(est);
     se3q_store(se3q_mul(se3q_exp(u), T), est);
@@ -1663,7 +1787,7 @@ int so_calc(orc_problem* p, int num_iters, int num_max_trials) {
     for (int ig = 0; ig < num_iters; ++ig) {
       double H[9] = {0}, b[3] = {0};
       for (int e : tr) {
-        double er[2], Jp[6], Jc[12];
+        double er[2], Jp[6], Jc[18];
         compute_edge_error(p, e, er);
         compute_edge_jac(p, e, Jp, Jc);
         const double* Om = p->info.data() + (size_t)e * 4;
@@ -1773,12 +1897,15 @@ int orc_set_threads(int n) {
 int orc_create(const g2oc_graph* g, orc_problem** out) {
   if (!g || !out) return G2OC_ERR_INVALID_ARGUMENT;
   *out = nullptr;
+  const bool bal = g->edge_type == G2OC_EDGE_BAL_OBSERVATION;
   const bool ba = g->edge_type == G2OC_EDGE_PROJECT_XYZ2UV || g->edge_type == G2OC_EDGE_SE3_PROJECT_XYZ ||
-                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ;
-  if (g->pose_type < 1 || g->pose_type > 3 || g->edge_type < 1 || g->edge_type > 6) return G2OC_ERR_BAD_GRAPH;
+                  g->edge_type == G2OC_EDGE_STEREO_SE3_PROJECT_XYZ || bal;
+  if (g->pose_type < 1 || g->pose_type > 4 || g->edge_type < 1 || g->edge_type > 7) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE2) != (g->pose_type == G2OC_POSE_SE2)) return G2OC_ERR_BAD_GRAPH;
   if ((g->edge_type == G2OC_EDGE_SE3) != (g->pose_type == G2OC_POSE_SE3)) return G2OC_ERR_BAD_GRAPH;
-  if ((ba || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP)) return G2OC_ERR_BAD_GRAPH;
+  if (bal != (g->pose_type == G2OC_POSE_BAL_CAMERA)) return G2OC_ERR_BAD_GRAPH;
+  if (((ba && !bal) || g->edge_type == G2OC_EDGE_SE3_EXPMAP) != (g->pose_type == G2OC_POSE_SE3EXPMAP))
+    return G2OC_ERR_BAD_GRAPH;
   if (g->num_poses < 0 || g->num_points < 0 || g->num_edges <= 0) return G2OC_ERR_BAD_GRAPH;
   if (!g->pose_estimate || !g->edge_vertex || !g->measurement || !g->information) return G2OC_ERR_INVALID_ARGUMENT;
   if (ba && g->num_points > 0 && !g->point_estimate) return G2OC_ERR_INVALID_ARGUMENT;
@@ -1913,7 +2040,7 @@ int orc_numeric_jacobians(orc_problem* p, double* j0, double* j1) {
       const int pi = which == 0 ? v0 : v1;
       std::vector<double> bak(est, est + n);
       for (int d = 0; d < dim; ++d) {
-        double u[6] = {0, 0, 0, 0, 0, 0};
+        double u[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         double ep[6], em[6];
         const int cnt = (!ba || which == 1) ? p->oplus_count[pi] : 0;
         u[d] = delta;

@@ -13,9 +13,12 @@ Configurations (the generators' defaults in g2o_b200/synth.py):
         Huber, LM + Schur + block-Jacobi PCG, 20 iterations
   pg2d  3500 VertexSE2 / 5499 EdgeSE2, Gauss-Newton + Cholesky, 10 iterations
   pg3d  2500 VertexSE3 / 4759 EdgeSE3, LM + Cholesky, 20 iterations
+  bal   356 VertexCameraBAL / 226,730 VertexPointBAL / ~1.27M EdgeObservationBAL,
+        LM + Schur + block-Jacobi PCG (BlockSolver<9,3>), 10 iterations
 
-Run from the repository root (about a minute on 8 cores):
-    python tests/golden/make_oracle_targets.py
+Run from the repository root (a few minutes on 8 cores); names given on the
+command line recompute only those entries and keep the others:
+    python tests/golden/make_oracle_targets.py [ba pg2d pg3d bal]
 """
 import json
 import os
@@ -35,6 +38,7 @@ def configs():
         "ba": (synth.bundle_adjustment, dict(algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_PCG), 20),
         "pg2d": (synth.pose_graph_2d, dict(algorithm=ALGO_GAUSS_NEWTON, linear_solver=LINEAR_CHOLESKY), 10),
         "pg3d": (synth.pose_graph_3d, dict(algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_CHOLESKY), 20),
+        "bal": (synth.bal_problem, dict(algorithm=ALGO_LEVENBERG, linear_solver=LINEAR_PCG), 10),
     }
 
 
@@ -45,8 +49,11 @@ def load():
 def main():
     from oracle import oracle
     oracle.build()
-    out = {}
+    names = sys.argv[1:] or list(configs())
+    out = load() if sys.argv[1:] and os.path.exists(OUT) else {}
     for name, (make, prm, iters) in configs().items():
+        if name not in names:
+            continue
         g = make()
         t0 = time.perf_counter()
         o = oracle.OracleProblem(g, oracle.default_params(**prm), threads=os.cpu_count() or 1)
