@@ -8,8 +8,8 @@
 // The edge records are those of the other projection edges (BAEdges /
 // BACamEdges: point-major device order, camera-major copy, information and
 // Huber record); the cameras are 9 doubles each, the points 4 (x y z pad).
-// Hessian storage: H_ll 6 unique entries per landmark, Hpl 9 x 3 row-major
-// per (camera, landmark) block, Hpp 9 x 9 per camera, the Schur complement
+// Hessian storage: H_ll 6 unique entries per landmark, Hpl 9 x 3 per
+// (camera, landmark) block in the padded-triple layout (bal_bt), Hpp 9 x 9 per camera, the Schur complement
 // 9 x 9 blocks in the row-SoA layout of SysDev (sys_offset<9>).
 //
 // Every sum is in a fixed order (per-thread loops, fixed shuffle trees,
@@ -22,6 +22,14 @@
 namespace g2oc {
 
 constexpr int kBalCam = 9;
+
+// A 9 x 3 block (Hpl, Y = Hpl Dinv) is stored as three 3 x 3 row triples,
+// each padded to 10 doubles (kBalBlk = 30 per block, the pads zero): element
+// (r, c) at bal_bt(r, c). Every triple starts on a 16-byte boundary, so a
+// block is 15 aligned 16-byte pieces and a triple's 9 values are four
+// 16-byte loads and one 8-byte load.
+constexpr int kBalBlk = 30;
+__host__ __device__ constexpr int bal_bt(int r, int c) { return (r / 3) * 10 + (r % 3) * 3 + c; }
 
 // EdgeObservationBAL's prediction f r(p) p (bal_example.cpp:160-200) and,
 // with JAC, its derivatives: Jc = d pred / d camera (2 x 9, row-major), Jp =
@@ -194,6 +202,17 @@ static __global__ void bal_jacobians_kernel(BAEdges E, BAVertices V, double* jp,
   for (int i = 0; i < 18; ++i) jc[18 * k + i] = Jc[i];
 }
 
+// a row-major 9 x 3 block into the padded-triple layout
+__device__ __forceinline__ void bal_store_blk(double* o, const double (&B)[27]) {
+#pragma unroll
+  for (int r = 0; r < 9; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[bal_bt(r, c)] = B[r * 3 + c];
+  o[9] = 0.0;
+  o[19] = 0.0;
+  o[29] = 0.0;
+}
+
 // Landmark side of BlockSolver::buildSystem (g2o/core/block_solver.hpp:492-565):
 // one thread per free landmark over its (contiguous) edges: H_ll = sum Jp^T
 // Om' Jp, b_l = sum Jp^T we (we = -rho' Omega e), and each Hpl block Jc^T Om'
@@ -232,10 +251,7 @@ static __global__ void bal_landmark_pass(BAEdges E, BAVertices V, const int* l_p
     const int blk = E.hpl[k];
     if (blk >= 0) {
       if (blk != cur) {
-        if (cur >= 0) {
-#pragma unroll
-          for (int i = 0; i < 27; ++i) hpl[(size_t)cur * 27 + i] = B[i];
-        }
+        if (cur >= 0) bal_store_blk(hpl + (size_t)cur * kBalBlk, B);
 #pragma unroll
         for (int i = 0; i < 27; ++i) B[i] = 0.0;
         cur = blk;
@@ -246,14 +262,97 @@ static __global__ void bal_landmark_pass(BAEdges E, BAVertices V, const int* l_p
         for (int c = 0; c < 3; ++c) B[r * 3 + c] += Jc[r] * A0[c] + Jc[9 + r] * A1[c];
     }
   }
-  if (cur >= 0) {
-#pragma unroll
-    for (int i = 0; i < 27; ++i) hpl[(size_t)cur * 27 + i] = B[i];
-  }
+  if (cur >= 0) bal_store_blk(hpl + (size_t)cur * kBalBlk, B);
 #pragma unroll
   for (int i = 0; i < 6; ++i) hll[(size_t)l * 6 + i] = H[i];
 #pragma unroll
   for (int i = 0; i < 3; ++i) b_l[(size_t)l * 3 + i] = bl[i];
+}
+
+// Landmark pass, edge-parallel form (landmarks of at most 32 edges, unique
+// (camera, landmark) pairs; the chunks of whole landmarks packed on the host):
+// one warp per chunk, one lane per edge with coalesced edge loads. Each
+// lane's Hpl block goes to shared memory and the warp stores the chunk's
+// contiguous block range coalesced; H_ll and b_l are summed by a segmented
+// warp scan keyed by landmark (fixed shuffle order) and written by the
+// segment's last lane. Four warps per CTA (27 KB of staging).
+constexpr int kBalLmWarps = 4;
+
+__global__ void __launch_bounds__(kBalLmWarps * 32)
+    bal_landmark_warp(BAEdges E, BAVertices V, const int* chunk_ptr, int nchunks, const int* e_lm, double* hll,
+                      double* hpl, double* b_l) {
+  __shared__ double stage[kBalLmWarps][32 * kBalBlk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int ch = blockIdx.x * kBalLmWarps + wid;
+  if (ch >= nchunks) return;
+  const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
+  const int k = e0 + lane;
+  const bool act = k < e1;
+  double H[6] = {0, 0, 0, 0, 0, 0};
+  double bl[3] = {0, 0, 0};
+  int key = -1 - lane;  // distinct for idle lanes
+  const int blk = act ? E.hpl[k] : -1;
+  const unsigned has = __ballot_sync(0xffffffffu, blk >= 0);
+  const int blk0 = (int)__reduce_min_sync(0xffffffffu, blk >= 0 ? (unsigned)blk : 0x7fffffffu);
+  if (act) {
+    key = e_lm[k];
+    const int2 v = E.v[k];
+    const double4 om = ba_om(E, k);
+    double e[2], chi2, w, Jc[18], Jp[6];
+    bal_edge<true>(V, v, E.z[k], om, e, chi2, w, Jc, Jp);
+    const double we0 = -w * (om.x * e[0] + om.y * e[1]);
+    const double we1 = -w * (om.y * e[0] + om.z * e[1]);
+    const double o00 = w * om.x, o01 = w * om.y, o11 = w * om.z;
+    double A0[3], A1[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      A0[i] = Jp[i] * o00 + Jp[3 + i] * o01;
+      A1[i] = Jp[i] * o01 + Jp[3 + i] * o11;
+    }
+    H[0] = A0[0] * Jp[0] + A1[0] * Jp[3];
+    H[1] = A0[0] * Jp[1] + A1[0] * Jp[4];
+    H[2] = A0[0] * Jp[2] + A1[0] * Jp[5];
+    H[3] = A0[1] * Jp[1] + A1[1] * Jp[4];
+    H[4] = A0[1] * Jp[2] + A1[1] * Jp[5];
+    H[5] = A0[2] * Jp[2] + A1[2] * Jp[5];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bl[i] = Jp[i] * we0 + Jp[3 + i] * we1;
+    if (blk >= 0) {
+      double hb[27];
+#pragma unroll
+      for (int r = 0; r < 9; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hb[r * 3 + c] = Jc[r] * A0[c] + Jc[9 + r] * A1[c];
+      bal_store_blk(&stage[wid][(blk - blk0) * kBalBlk], hb);
+    }
+  }
+  // segmented inclusive scan by landmark
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ko = __shfl_up_sync(0xffffffffu, key, off);
+    double Ho[6], bo[3];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) Ho[i] = __shfl_up_sync(0xffffffffu, H[i], off);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) bo[i] = __shfl_up_sync(0xffffffffu, bl[i], off);
+    if (lane >= off && ko == key) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) H[i] += Ho[i];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) bl[i] += bo[i];
+    }
+  }
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  if (act && (lane == 31 || knext != key)) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) hll[(size_t)key * 6 + i] = H[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) b_l[(size_t)key * 3 + i] = bl[i];
+  }
+  __syncwarp();
+  const int n = __popc(has) * kBalBlk;
+  double* out = hpl + (size_t)blk0 * kBalBlk;
+  for (int i = lane; i < n; i += 32) out[i] = stage[wid][i];
 }
 
 // upper-triangle index of (i, j), i <= j, of a 9 x 9 block
@@ -326,6 +425,89 @@ __global__ void __launch_bounds__(THREADS) bal_camera_pass(BACamEdges CE, BAVert
   }
 }
 
+// Camera side in chunks: the camera-major edge list cut into chunks of at
+// most kBalCamChunk edges of one camera (host plan: camera, first edge, end),
+// a CTA per chunk summing its 45 + 9 values as bal_camera_pass does into
+// `cpart`; bal_camera_reduce adds each camera's chunk sums in chunk order and
+// writes the full 9 x 9 block and b_p. More CTAs than cameras keep the SMs
+// busy (a 356-camera problem has ~3,600 edges per camera).
+constexpr int kBalCamChunk = 512;
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+    bal_camera_chunks(BACamEdges CE, BAVertices V, const int4* cch, double* cpart) {
+  constexpr int WARPS = THREADS / 32;
+  __shared__ double red[WARPS][54];
+  const int4 cd = cch[blockIdx.x];
+  double H[45], bp[9];
+#pragma unroll
+  for (int i = 0; i < 45; ++i) H[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) bp[i] = 0.0;
+  for (int j = cd.y + threadIdx.x; j < cd.z; j += THREADS) {
+    const int2 v = CE.v[j];
+    const double4 om = ba_om(CE, j);
+    double e[2], chi2, w, Jc[18], Jp[6];
+    bal_edge<true>(V, v, CE.z[j], om, e, chi2, w, Jc, Jp);
+    const double we0 = -w * (om.x * e[0] + om.y * e[1]);
+    const double we1 = -w * (om.y * e[0] + om.z * e[1]);
+    const double o00 = w * om.x, o01 = w * om.y, o11 = w * om.z;
+    double A0[9], A1[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      A0[i] = Jc[i] * o00 + Jc[9 + i] * o01;
+      A1[i] = Jc[i] * o01 + Jc[9 + i] * o11;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+#pragma unroll
+      for (int k = i; k < 9; ++k) H[bal_ut(i, k)] += A0[i] * Jc[k] + A1[i] * Jc[9 + k];
+      bp[i] += Jc[i] * we0 + Jc[9 + i] * we1;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 45; ++i) {
+    const double s = warp_sum(H[i]);
+    if (lane == 0) red[wid][i] = s;
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const double s = warp_sum(bp[i]);
+    if (lane == 0) red[wid][45 + i] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 54) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < WARPS; ++q) s += red[q][threadIdx.x];
+    cpart[(size_t)blockIdx.x * 54 + threadIdx.x] = s;
+  }
+}
+
+// thread per (camera, value): the camera's chunk sums in order -> Hpp (both
+// triangles) and b_p
+static __global__ void bal_camera_reduce(int Cf, const int* cch_ptr, const double* cpart, double* hpp,
+                                         double* b_p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= Cf * 54) return;
+  const int h = t / 54, q = t % 54;
+  double s = 0.0;
+  for (int c = cch_ptr[h]; c < cch_ptr[h + 1]; ++c) s += cpart[(size_t)c * 54 + q];
+  if (q < 45) {
+    int i = 0, u = q;
+    while (u >= 9 - i) {
+      u -= 9 - i;
+      ++i;
+    }
+    const int k = i + u;
+    hpp[(size_t)h * 81 + i * 9 + k] = s;
+    hpp[(size_t)h * 81 + k * 9 + i] = s;
+  } else {
+    b_p[(size_t)h * 9 + q - 45] = s;
+  }
+}
+
 // max |diag H| over Hpp and H_ll (computeLambdaInit,
 // optimization_algorithm_levenberg.cpp:155-167): partial maxima per block
 static __global__ void bal_max_diag(const double* hpp, int Cf, const double* hll, int Pf, double* partials) {
@@ -344,11 +526,8 @@ static __global__ void bal_max_diag(const double* hpp, int Cf, const double* hll
   block_max(m, partials + blockIdx.x);
 }
 
-// Per landmark: Dinv = (H_ll + lambda I)^-1 and, for each of its Hpl blocks,
-// Y = Hpl Dinv (9 x 3), the factor every Schur product of the block uses
-// (block_solver.hpp:372-386)
-static __global__ void bal_schur_landmark(const double* hll, const double* hpl, const int* hb_ptr, int Pf,
-                                          double lambda, double* dinv, double* Y, int* nonfinite) {
+// Per landmark: Dinv = (H_ll + lambda I)^-1 (block_solver.hpp:372-386)
+static __global__ void bal_schur_landmark(const double* hll, int Pf, double lambda, double* dinv, int* nonfinite) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= Pf) return;
   const double* h = hll + (size_t)l * 6;
@@ -357,105 +536,310 @@ static __global__ void bal_schur_landmark(const double* hll, const double* hpl, 
   if (!inverse3(A, D)) *nonfinite = 1;
 #pragma unroll
   for (int i = 0; i < 9; ++i) dinv[(size_t)l * 9 + i] = D[i];
-  if (!Y) return;
-  const int b1 = hb_ptr[l + 1];
-  for (int a = hb_ptr[l]; a < b1; ++a) {
-    const double* B = hpl + (size_t)a * 27;
-    double* o = Y + (size_t)a * 27;
+}
+
+// Y_a = Hpl_a Dinv_l(a) for every Hpl block, the factor every Schur product
+// of the block uses: a CTA per kBalYBlocks consecutive blocks loads them into
+// shared memory coalesced, each thread forms its block's product in place,
+// and the CTA stores the range coalesced (the pads stay zero)
+constexpr int kBalYBlocks = 128;
+
+static __global__ void __launch_bounds__(kBalYBlocks)
+    bal_schur_y(int nh, const int* hpl_col, const double* hpl, const double* dinv, double* Y) {
+  __shared__ __align__(16) double sm[kBalYBlocks * kBalBlk];
+  const int a0 = blockIdx.x * kBalYBlocks;
+  const int n = min(kBalYBlocks, nh - a0);
+  // 16-byte pieces (a block is 15), all of a thread's loads issued before its stores
+  const double2* src = reinterpret_cast<const double2*>(hpl + (size_t)a0 * kBalBlk);
+  double2* sm2 = reinterpret_cast<double2*>(sm);
+  constexpr int kPer = kBalYBlocks * kBalBlk / 2 / kBalYBlocks;  // 15 pieces per thread
+  const int npc = n * kBalBlk / 2;
+  double2 v[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int t = u * kBalYBlocks + threadIdx.x;
+    if (t < npc) v[u] = __ldg(src + t);
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int t = u * kBalYBlocks + threadIdx.x;
+    if (t < npc) sm2[t] = v[u];
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < n) {
+    const double* D = dinv + (size_t)hpl_col[a0 + threadIdx.x] * 9;
+    double d[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) d[q] = D[q];
+    double* B = sm + threadIdx.x * kBalBlk;
 #pragma unroll
     for (int r = 0; r < 9; ++r) {
-      const double b0 = B[r * 3], b1v = B[r * 3 + 1], b2 = B[r * 3 + 2];
+      double* row = B + bal_bt(r, 0);
+      const double b0 = row[0], b1 = row[1], b2 = row[2];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) o[r * 3 + c] = b0 * D[c] + b1v * D[3 + c] + b2 * D[6 + c];
+      for (int c = 0; c < 3; ++c) row[c] = b0 * d[c] + b1 * d[3 + c] + b2 * d[6 + c];
     }
+  }
+  __syncthreads();
+  double2* dst = reinterpret_cast<double2*>(Y + (size_t)a0 * kBalBlk);
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int t = u * kBalYBlocks + threadIdx.x;
+    if (t < npc) dst[t] = sm2[t];
   }
 }
 
 // Schur complement S = Hpp + lambda I - sum Hpl (H_ll + lambda I)^-1 Hpl^T
-// (the Schur part of BlockSolver::solve, block_solver.hpp:346-433), one warp
-// per 9 x 9 block of S in the internal row-major order. A diagonal block
-// subtracts Y_a Hpl_a^T over its camera's Hpl blocks and also forms the
-// reduced right-hand side b_p - sum Y_a b_l(a); an off-diagonal block (r, c)
-// subtracts Y_a Hpl_b^T over its co-observation pairs (a of camera r, b of
-// camera c, same landmark) in landmark order. The products' operands are
-// staged four blocks at a time in shared memory (coalesced 216-byte rows);
-// lane t owns entries t, t + 32, t + 64 of the block.
-constexpr int kBalSchurWarps = 8;
-constexpr int kBalStage = 4;
+// (the Schur part of BlockSolver::solve, block_solver.hpp:346-433). The
+// products of a 9 x 9 block of S in the internal row-major order are its
+// items: a diagonal block (r, r) has one per Hpl block a of camera r
+// (Y_a Hpl_a^T), an off-diagonal block (r, c) one per co-observation pair (a
+// of camera r, b of camera c, same landmark; Y_a Hpl_b^T), in landmark order.
+// The items are cut into chunks of at most kBalChunk (host plan, fixed), one
+// warp per chunk. The operands of kBalStage items (Y_a and Hpl_b, 15 aligned
+// 16-byte pieces each) are copied into shared memory by asynchronous copies,
+// double-buffered: the next stage's copies are in flight while this stage is
+// multiplied, and the item indices are fetched one stage further ahead. The
+// warp's first 27 lanes form three groups of nine, group G taking the items
+// G, G + 3, ... of a stage and lane (bi, bj) of a group a 3 x 3 patch of the
+// block (row triple bi of Y_a against row triple bj of Hpl_b: ten shared
+// loads, 27 fused multiply-adds), two items at a time into two accumulator
+// sets; at the end the sets and then the three groups' sums are added in
+// order. A block of one chunk is written straight into S (diagonal:
+// Hpp + lambda I minus the sum); the chunks of a longer block leave their
+// sums in `part` and bal_schur_reduce adds them in chunk order, so every
+// block's sum has a fixed order whatever the launch shape. Items: a diagonal
+// block's are its camera's Hpl blocks (hc_blk), an off-diagonal block's its
+// pairs (a, b) of absolute Hpl block indices. An item occupies kBalItem
+// doubles of shared memory (Y at 0, Hpl_b at 30): 62 puts the two items a
+// quarter-warp of 16-byte loads can touch in distinct banks.
+constexpr int kBalChunk = 120;
+constexpr int kBalStage = 12;
+constexpr int kBalChunkWarps = 4;
+constexpr int kBalItem = 62;
+constexpr int kBalStageCopies = (kBalStage * 30 + 31) / 32;  // 16-byte copies per lane per stage
 
-__global__ void __launch_bounds__(kBalSchurWarps * 32)
-    bal_schur_blocks(int nnzb, const int* brow, const int* rptr, const int* rcol, const int* pair_ptr,
-                     const int2* pairs, const int* hc_ptr, const int* hc_blk, const int* hpl_col, const double* hpp,
-                     const double* hpl, const double* Y, double lambda, const double* b_p, const double* b_l,
-                     double* S, double* bs) {
-  __shared__ double stage[kBalSchurWarps][kBalStage][54];
+__device__ __forceinline__ void bal_cp16(double* dst, const double* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bal_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void bal_cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// the item indices of the stage starting at item p (lanes < np)
+__device__ __forceinline__ void bal_item(bool diag, const int* hc_blk, const int2* pairs, int p, int np, int lane,
+                                         int& a, int& b) {
+  a = 0;
+  b = 0;
+  if (lane < np) {
+    if (diag) {
+      a = __ldg(hc_blk + p + lane);
+      b = a;
+    } else {
+      const int2 pr = __ldg(pairs + p + lane);
+      a = pr.x;
+      b = pr.y;
+    }
+  }
+}
+
+// asynchronous copies of a stage's operands (every lane runs the same loop:
+// the shuffles see the whole warp); piece w < 15 of an item is Y_a's, the
+// rest Hpl_b's, both landing at 2 w in the item's slot
+__device__ __forceinline__ void bal_stage_copy(double* st, int np, int a, int b, const double* Y, const double* hpl,
+                                               int lane) {
+  const int tot = np * 30;
+#pragma unroll
+  for (int u = 0; u < kBalStageCopies; ++u) {
+    const int t = u * 32 + lane;
+    const int it = min(t / 30, max(np - 1, 0));
+    const int w = t - it * 30;
+    const int ai = __shfl_sync(0xffffffffu, a, it);
+    const int bi = __shfl_sync(0xffffffffu, b, it);
+    if (t < tot)
+      bal_cp16(st + it * kBalItem + 2 * w,
+               w < 15 ? Y + (size_t)ai * kBalBlk + 2 * w : hpl + (size_t)bi * kBalBlk + 2 * (w - 15));
+  }
+  bal_cp_commit();
+}
+
+// a row triple (9 doubles, 16-byte aligned) from shared memory
+__device__ __forceinline__ void bal_ld_triple(const double* p, double (&v)[9]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const double2 t = *reinterpret_cast<const double2*>(p + 2 * q);
+    v[2 * q] = t.x;
+    v[2 * q + 1] = t.y;
+  }
+  v[8] = p[8];
+}
+
+__global__ void __launch_bounds__(kBalChunkWarps * 32)
+    bal_schur_chunks(int nchunks, const int4* chunks, const int* brow, const int* rptr, const int* rcol,
+                     const int2* pairs, const int* hc_blk, const double* hpp, const double* hpl, const double* Y,
+                     double lambda, double* S, double* part) {
+  __shared__ __align__(16) double stage[kBalChunkWarps][2][kBalStage * kBalItem];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int k = blockIdx.x * kBalSchurWarps + wid;
-  if (k >= nnzb) return;
-  const int r = brow[k], rb = rptr[r], nblk = rptr[r + 1] - rb, j = k - rb;
+  const int ch = blockIdx.x * kBalChunkWarps + wid;
+  if (ch >= nchunks) return;
+  const int4 cd = chunks[ch];
+  const int k = cd.x, q0 = cd.y, q1 = cd.z, slot = cd.w;
+  const int r = brow[k];
   const bool diag = rcol[k] == r;
-  double (*st)[54] = stage[wid];
-  double acc[3] = {0.0, 0.0, 0.0};
-  int ei[3], ej[3];
+  const int grp = lane / 9, sub = lane % 9, bi = sub / 3, bj = sub % 3;
+  double acc[9], acc2[9];
 #pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const int e = lane + 32 * q;
-    ei[q] = e < 81 ? e / 9 : 0;
-    ej[q] = e < 81 ? e % 9 : 0;
+  for (int q = 0; q < 9; ++q) {
+    acc[q] = 0.0;
+    acc2[q] = 0.0;
   }
-  double rhs = 0.0;  // lanes < 9 of a diagonal block: the reduced right-hand side
-  int n0, n1;
-  if (diag) {
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int e = lane + 32 * q;
-      if (e < 81) acc[q] = hpp[(size_t)r * 81 + e] + (ei[q] == ej[q] ? lambda : 0.0);
-    }
-    if (lane < 9) rhs = b_p[(size_t)r * 9 + lane];
-    n0 = hc_ptr[r];
-    n1 = hc_ptr[r + 1];
-  } else {
-    n0 = pair_ptr[k];
-    n1 = pair_ptr[k + 1];
-  }
-  const int cam0 = hc_ptr[r];
-  for (int p0 = n0; p0 < n1; p0 += kBalStage) {
-    const int np = min(kBalStage, n1 - p0);
-    __syncwarp();
-    for (int t = lane; t < np * 54; t += 32) {
-      const int it = t / 54, w = t % 54;
-      int a, b;
-      if (diag) {
-        a = hc_blk[p0 + it];
-        b = a;
-      } else {
-        const int2 pr = pairs[p0 + it];
-        a = hc_blk[cam0 + pr.x];
-        b = pr.y;
-      }
-      st[it][w] = w < 27 ? __ldg(Y + (size_t)a * 27 + w) : __ldg(hpl + (size_t)b * 27 + (w - 27));
+  // stage s covers items q0 + s kBalStage ..; prologue: copies of stage 0,
+  // indices of stage 1
+  int a, b;
+  int np = min(kBalStage, q1 - q0);
+  bal_item(diag, hc_blk, pairs, q0, np, lane, a, b);
+  if (np > 0) bal_stage_copy(stage[wid][0], np, a, b, Y, hpl, lane);
+  int p1 = q0 + kBalStage;
+  int np1 = max(0, min(kBalStage, q1 - p1));
+  bal_item(diag, hc_blk, pairs, p1, np1, lane, a, b);
+  for (int s = 0; np > 0; ++s) {
+    if (np1 > 0) {
+      bal_stage_copy(stage[wid][(s + 1) & 1], np1, a, b, Y, hpl, lane);
+      const int p2 = p1 + kBalStage;
+      const int np2 = max(0, min(kBalStage, q1 - p2));
+      bal_item(diag, hc_blk, pairs, p2, np2, lane, a, b);
+      bal_cp_wait<1>();  // this stage's copies have landed; the next stage's may still be in flight
+      p1 = p2;
+      np1 = np2;
+    } else {
+      bal_cp_wait<0>();
     }
     __syncwarp();
-    for (int it = 0; it < np; ++it) {
-      const double* Ys = st[it];
-      const double* Hs = st[it] + 27;
+    const double* st = stage[wid][s & 1];
+    if (lane < 27) {
+      // two items at a time into two accumulator sets (independent chains)
+      int it = grp;
+      for (; it + 3 < np; it += 6) {
+        double y[9], h[9], y2[9], h2[9];
+        bal_ld_triple(st + it * kBalItem + bi * 10, y);  // Y rows 3bi .. 3bi + 2
+        bal_ld_triple(st + it * kBalItem + 30 + bj * 10, h);  // Hpl_b rows 3bj .. 3bj + 2
+        bal_ld_triple(st + (it + 3) * kBalItem + bi * 10, y2);
+        bal_ld_triple(st + (it + 3) * kBalItem + 30 + bj * 10, h2);
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int i = ei[q], jj = ej[q];
-        acc[q] -= Ys[i * 3] * Hs[jj * 3] + Ys[i * 3 + 1] * Hs[jj * 3 + 1] + Ys[i * 3 + 2] * Hs[jj * 3 + 2];
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+              acc[u * 3 + v] = fma(y[u * 3 + m], h[v * 3 + m], acc[u * 3 + v]);
+              acc2[u * 3 + v] = fma(y2[u * 3 + m], h2[v * 3 + m], acc2[u * 3 + v]);
+            }
       }
-      if (diag && lane < 9) {
-        const double* bl = b_l + (size_t)hpl_col[hc_blk[p0 + it]] * 3;
-        rhs -= Ys[lane * 3] * bl[0] + Ys[lane * 3 + 1] * bl[1] + Ys[lane * 3 + 2] * bl[2];
+      if (it < np) {
+        double y[9], h[9];
+        bal_ld_triple(st + it * kBalItem + bi * 10, y);
+        bal_ld_triple(st + it * kBalItem + 30 + bj * 10, h);
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int v = 0; v < 3; ++v) acc[u * 3 + v] = fma(y[u * 3 + m], h[v * 3 + m], acc[u * 3 + v]);
       }
     }
+    __syncwarp();  // the buffer is read before the copies of stage s + 2 overwrite it
+    np = min(kBalStage, q1 - (q0 + (s + 1) * kBalStage));
+  }
+  // the two sets, then the three groups' sums in group order, on lanes 0..8
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    acc[q] += acc2[q];
+    const double g1 = __shfl_sync(0xffffffffu, acc[q], lane + 9 < 32 ? lane + 9 : lane);
+    const double g2 = __shfl_sync(0xffffffffu, acc[q], lane + 18 < 32 ? lane + 18 : lane);
+    acc[q] = (acc[q] + g1) + g2;
+  }
+  if (lane >= 9) return;
+  if (slot >= 0) {
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+#pragma unroll
+      for (int v = 0; v < 3; ++v) part[(size_t)slot * 81 + (3 * bi + u) * 9 + 3 * bj + v] = acc[u * 3 + v];
+    return;
+  }
+  const int rb = rptr[r], nblk = rptr[r + 1] - rb, j = k - rb;
+#pragma unroll
+  for (int u = 0; u < 3; ++u)
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const int ii = 3 * bi + u, jj = 3 * bj + v, e = ii * 9 + jj;
+      const double base = diag ? hpp[(size_t)r * 81 + e] + (ii == jj ? lambda : 0.0) : 0.0;
+      S[sys_offset<9>(rb, nblk, j, e)] = base - acc[u * 3 + v];
+    }
+}
+
+// the blocks cut into several chunks: (block, first slot, slots), thread per entry
+static __global__ void bal_schur_reduce(int nred, const int4* red, const int* brow, const int* rptr,
+                                        const int* rcol, const double* hpp, double lambda, const double* part,
+                                        double* S) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nred * 81) return;
+  const int q = t / 81, e = t % 81;
+  const int4 rd = red[q];
+  double s = 0.0;
+  for (int n = 0; n < rd.z; ++n) s += part[(size_t)(rd.y + n) * 81 + e];
+  const int k = rd.x, r = brow[k];
+  const int i = e / 9, jj = e % 9;
+  const double base = rcol[k] == r ? hpp[(size_t)r * 81 + e] + (i == jj ? lambda : 0.0) : 0.0;
+  const int rb = rptr[r], nblk = rptr[r + 1] - rb;
+  S[sys_offset<9>(rb, nblk, k - rb, e)] = base - s;
+}
+
+// reduced right-hand side b_s = b_p - sum_a Y_a b_l(a) over each camera's Hpl
+// blocks. The camera's blocks are cut into chunks of at most kBalChunk (host
+// plan: camera, first block, end): one warp per chunk, lanes strided over the
+// blocks, a fixed shuffle tree, the chunk's 9 sums to `rpart`; then
+// bal_schur_rhs_reduce adds each camera's chunk sums in chunk order.
+static __global__ void bal_schur_rhs_chunks(int nrch, const int4* rch, const int* hc_blk, const int* hpl_col,
+                                            const double* Y, const double* b_l, double* rpart) {
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ch >= nrch) return;
+  const int4 cd = rch[ch];
+  double v[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) v[q] = 0.0;
+  for (int p = cd.y + lane; p < cd.z; p += 32) {
+    const int a = hc_blk[p];
+    const double* bl = b_l + (size_t)hpl_col[a] * 3;
+    const double l0 = bl[0], l1 = bl[1], l2 = bl[2];
+    const double* y = Y + (size_t)a * kBalBlk;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) v[q] += y[bal_bt(q, 0)] * l0 + y[bal_bt(q, 1)] * l1 + y[bal_bt(q, 2)] * l2;
   }
 #pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const int e = lane + 32 * q;
-    if (e < 81) S[sys_offset<9>(rb, nblk, j, e)] = acc[q];
+  for (int q = 0; q < 9; ++q) v[q] = warp_sum(v[q]);
+  if (lane < 9) {
+    double out = v[0];
+#pragma unroll
+    for (int q = 1; q < 9; ++q)
+      if (lane == q) out = v[q];
+    rpart[(size_t)ch * 9 + lane] = out;
   }
-  if (diag && lane < 9 && bs) bs[(size_t)r * 9 + lane] = rhs;
+}
+
+// thread per (camera, entry): b_s = b_p - the camera's chunk sums in order
+static __global__ void bal_schur_rhs_reduce(int Cf, const int* rch_ptr, const double* rpart, const double* b_p,
+                                            double* bs) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= Cf * 9) return;
+  const int r = t / 9, e = t % 9;
+  double s = 0.0;
+  for (int q = rch_ptr[r]; q < rch_ptr[r + 1]; ++q) s += rpart[(size_t)q * 9 + e];
+  bs[t] = b_p[t] - s;
 }
 
 // Landmark back-substitution (block_solver.hpp:449-474):
@@ -467,19 +851,70 @@ static __global__ void bal_backsub(const int* hb_ptr, const int* hpl_row, int Pf
   double cl[3] = {r_l[(size_t)l * 3], r_l[(size_t)l * 3 + 1], r_l[(size_t)l * 3 + 2]};
   const int b1 = hb_ptr[l + 1];
   for (int a = hb_ptr[l]; a < b1; ++a) {
-    const double* B = hpl + (size_t)a * 27;
+    const double* B = hpl + (size_t)a * kBalBlk;
     const double* xp = x_p + (size_t)hpl_row[a] * 9;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       double s = 0.0;
 #pragma unroll
-      for (int r = 0; r < 9; ++r) s += B[r * 3 + c] * xp[r];
+      for (int r = 0; r < 9; ++r) s += B[bal_bt(r, c)] * xp[r];
       cl[c] -= s;
     }
   }
   const double* D = dinv + (size_t)l * 9;
 #pragma unroll
   for (int i = 0; i < 3; ++i) x_l[(size_t)l * 3 + i] = D[i * 3] * cl[0] + D[i * 3 + 1] * cl[1] + D[i * 3 + 2] * cl[2];
+}
+
+// Back-substitution, one warp per chunk of whole landmarks (the chunks of
+// bal_landmark_warp), lane per edge: Hpl_a^T x_p(row a) per edge, summed per
+// landmark by a segmented warp scan (fixed shuffle order), x_l = Dinv (r_l -
+// sum) by the segment's last lane
+static __global__ void bal_backsub_warp(const int* e_hpl, const int* hpl_row, const int* chunk_ptr, int nchunks,
+                                        const int* e_lm, const double* hpl, const double* dinv, const double* r_l,
+                                        const double* x_p, double* x_l) {
+  const int lane = threadIdx.x & 31;
+  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (ch >= nchunks) return;
+  const int e0 = chunk_ptr[ch], e1 = chunk_ptr[ch + 1];
+  const int k = e0 + lane;
+  const bool act = k < e1;
+  double acc[3] = {0, 0, 0};
+  int key = -1 - lane;
+  if (act) {
+    key = e_lm[k];
+    const int blk = e_hpl[k];
+    if (blk >= 0) {
+      const double* B = hpl + (size_t)blk * kBalBlk;
+      const double* xp = x_p + (size_t)hpl_row[blk] * 9;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        double t = 0.0;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) t += B[bal_bt(r, c)] * xp[r];
+        acc[c] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int ko = __shfl_up_sync(0xffffffffu, key, off);
+    double ao[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ao[i] = __shfl_up_sync(0xffffffffu, acc[i], off);
+    if (lane >= off && ko == key) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) acc[i] += ao[i];
+    }
+  }
+  const int knext = __shfl_down_sync(0xffffffffu, key, 1);
+  if (act && (lane == 31 || knext != key)) {
+    const double cl[3] = {r_l[(size_t)key * 3] - acc[0], r_l[(size_t)key * 3 + 1] - acc[1],
+                          r_l[(size_t)key * 3 + 2] - acc[2]};
+    const double* D = dinv + (size_t)key * 9;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) x_l[(size_t)key * 3 + i] = D[i * 3] * cl[0] + D[i * 3 + 1] * cl[1] + D[i * 3 + 2] * cl[2];
+  }
 }
 
 // VertexCameraBAL::oplusImpl / VertexPointBAL::oplusImpl

@@ -1622,17 +1622,90 @@ struct Engine final : EngineBase {
 // FP64.
 struct BalEngine final : EngineBase {
   g2oc_ctx* c;
-  DBuf<double> hpp, hll, hpl, dinv, Y, Sval, minv, r, s, d, tbuf, cpart;
+  DBuf<double> hpp, hll, hpl, dinv, Y, Sval, minv, r, s, d, tbuf, cpart, part;
+  // the Schur complement's work plan: chunks (block, first item, end, slot or
+  // -1) and the blocks cut into several chunks (block, first slot, slots)
+  DBuf<int4> chunks, reds, rch, cch;
+  DBuf<int> cch_ptr;
+  DBuf<double> ccpart;
+  int ncch = 0;
+  DBuf<int2> pairs;  // co-observation pairs as absolute Hpl block indices (a of the row camera, b)
+  DBuf<int> rch_ptr;
+  DBuf<double> rpart;
+  int nchunks = 0, nreds = 0, nrch = 0;
   explicit BalEngine(g2oc_ctx* ctx) : c(ctx) {}
+
+  int plan_schur() {
+    const Structure& S = c->S;
+    std::vector<int4> ch, rd;
+    int nslots = 0;
+    for (int k = 0; k < S.sys_nnzb; ++k) {
+      const int r = S.sys_brow[k];
+      const bool diag = S.sys_rcol[k] == r;
+      const int q0 = diag ? S.hc_ptr[r] : S.s_pair_ptr[k];
+      const int q1 = diag ? S.hc_ptr[r + 1] : S.s_pair_ptr[k + 1];
+      const int n = std::max(1, (q1 - q0 + kBalChunk - 1) / kBalChunk);
+      if (n == 1) {
+        ch.push_back(make_int4(k, q0, q1, -1));
+        continue;
+      }
+      rd.push_back(make_int4(k, nslots, n, 0));
+      for (int t = 0; t < n; ++t)
+        ch.push_back(make_int4(k, q0 + t * kBalChunk, std::min(q1, q0 + (t + 1) * kBalChunk), nslots++));
+    }
+    nchunks = (int)ch.size();
+    nreds = (int)rd.size();
+    {
+      std::vector<int2> pa(S.s_pairs.size() / 2 + 1, make_int2(0, 0));
+      for (int k = 0; k < S.sys_nnzb; ++k) {
+        const int r = S.sys_brow[k];
+        if (S.sys_rcol[k] == r) continue;
+        for (int q = S.s_pair_ptr[k]; q < S.s_pair_ptr[k + 1]; ++q)
+          pa[q] = make_int2(S.hc_blk[S.hc_ptr[r] + S.s_pairs[2 * (size_t)q]], S.s_pairs[2 * (size_t)q + 1]);
+      }
+      G2OC_TRY(pairs.upload(pa, c->stream));
+    }
+    // the camera pass: each camera's edges in chunks
+    {
+      std::vector<int4> cc;
+      std::vector<int> cp(S.Cf + 1, 0);
+      for (int h = 0; h < S.Cf; ++h) {
+        const int j0 = S.c_ptr[h], j1 = S.c_ptr[h + 1];
+        if (j1 == j0) cc.push_back(make_int4(h, j0, j1, 0));
+        for (int j = j0; j < j1; j += kBalCamChunk) cc.push_back(make_int4(h, j, std::min(j1, j + kBalCamChunk), 0));
+        cp[h + 1] = (int)cc.size();
+      }
+      ncch = (int)cc.size();
+      G2OC_TRY(cch.upload(cc.empty() ? std::vector<int4>{make_int4(0, 0, 0, 0)} : cc, c->stream));
+      G2OC_TRY(cch_ptr.upload(cp, c->stream));
+      G2OC_TRY(ccpart.alloc((size_t)ncch * 54 + 1));
+    }
+    // the reduced right-hand side: each camera's Hpl blocks in chunks
+    std::vector<int4> rc;
+    std::vector<int> rp(S.Cf + 1, 0);
+    for (int r = 0; r < S.Cf; ++r) {
+      for (int q = S.hc_ptr[r]; q < S.hc_ptr[r + 1]; q += kBalChunk)
+        rc.push_back(make_int4(r, q, std::min(S.hc_ptr[r + 1], q + kBalChunk), 0));
+      rp[r + 1] = (int)rc.size();
+    }
+    nrch = (int)rc.size();
+    G2OC_TRY(rch.upload(rc.empty() ? std::vector<int4>{make_int4(0, 0, 0, 0)} : rc, c->stream));
+    G2OC_TRY(rch_ptr.upload(rp, c->stream));
+    G2OC_TRY(rpart.alloc((size_t)nrch * 9 + 1));
+    G2OC_TRY(chunks.upload(ch.empty() ? std::vector<int4>{make_int4(0, 0, 0, -1)} : ch, c->stream));
+    G2OC_TRY(reds.upload(rd.empty() ? std::vector<int4>{make_int4(0, 0, 0, 0)} : rd, c->stream));
+    G2OC_TRY(part.alloc((size_t)nslots * 81 + 1));
+    return G2OC_OK;
+  }
 
   int alloc() override {
     const Structure& S = c->S;
     const size_t nh = S.hpl_rc.size() / 2;
     G2OC_TRY(hpp.alloc((size_t)S.Cf * 81 + 1));
     G2OC_TRY(hll.alloc((size_t)S.Pf * 6 + 1));
-    G2OC_TRY(hpl.alloc(nh * 27 + 1));
+    G2OC_TRY(hpl.alloc(nh * kBalBlk + 1));
     G2OC_TRY(dinv.alloc((size_t)S.Pf * 9 + 1));
-    G2OC_TRY(Y.alloc(nh * 27 + 1));
+    G2OC_TRY(Y.alloc(nh * kBalBlk + 1));
     G2OC_TRY(Sval.alloc((size_t)S.sys_nnzb * 81 + 1));
     const size_t n = (size_t)S.Cf * 9;
     G2OC_TRY(minv.alloc((size_t)S.Cf * 81 + 1));
@@ -1641,7 +1714,7 @@ struct BalEngine final : EngineBase {
     G2OC_TRY(d.alloc(n + 1));
     G2OC_TRY(tbuf.alloc((size_t)S.sys_nnzb * 9 + 1));
     G2OC_TRY(cpart.alloc(S.sys_chunk_row.size() * 9 + 1));
-    return G2OC_OK;
+    return plan_schur();
   }
 
   SysDev<double> sys(const double* val) {
@@ -1662,14 +1735,22 @@ struct BalEngine final : EngineBase {
   int build_system() override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
-    if (S.Pf > 0) {
+    if (S.Pf > 0 && S.lm_warp_ok) {
+      const int nch = (int)S.lm_chunk_ptr.size() - 1;
+      G2OC_K(K_LANDMARK_PASS) bal_landmark_warp<<<cdiv(nch, kBalLmWarps), kBalLmWarps * 32, 0, st>>>(
+          c->ba_edges(), c->ba_vertices(), c->lm_chunk_ptr.p, nch, c->e_lm.p, hll.p, hpl.p,
+          c->b.p + (size_t)S.Cf * 9);
+      G2OC_LAUNCH_CHECK();
+    } else if (S.Pf > 0) {
       G2OC_K(K_LANDMARK_PASS) bal_landmark_pass<<<cdiv(S.Pf, 128), 128, 0, st>>>(
           c->ba_edges(), c->ba_vertices(), c->l_ptr.p, S.Pf, hll.p, hpl.p, c->b.p + (size_t)S.Cf * 9);
       G2OC_LAUNCH_CHECK();
     }
-    if (S.Cf > 0) {
-      G2OC_K(K_CAMERA_PASS) bal_camera_pass<128><<<S.Cf, 128, 0, st>>>(c->ba_cam_edges(), c->ba_vertices(), hpp.p,
-                                                                       c->b.p);
+    if (S.Cf > 0 && ncch > 0) {
+      G2OC_K(K_CAMERA_PASS) bal_camera_chunks<128><<<ncch, 128, 0, st>>>(c->ba_cam_edges(), c->ba_vertices(), cch.p,
+                                                                         ccpart.p);
+      G2OC_K(K_CAMERA_PASS) bal_camera_reduce<<<cdiv(S.Cf * 54, 256), 256, 0, st>>>(S.Cf, cch_ptr.p, ccpart.p, hpp.p,
+                                                                                    c->b.p);
       G2OC_LAUNCH_CHECK();
     }
     return G2OC_OK;
@@ -1699,23 +1780,48 @@ struct BalEngine final : EngineBase {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
     if (S.Pf > 0) {
-      G2OC_K(K_SCHUR_LANDMARK) bal_schur_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(
-          hll.p, hpl.p, c->hb_ptr.p, S.Pf, lambda, dinv.p, Y.p, c->flag.p);
+      G2OC_K(K_SCHUR_LANDMARK) bal_schur_landmark<<<cdiv(S.Pf, 128), 128, 0, st>>>(hll.p, S.Pf, lambda, dinv.p,
+                                                                                c->flag.p);
       G2OC_LAUNCH_CHECK();
+      const int nh = (int)(S.hpl_rc.size() / 2);
+      if (nh > 0) {
+        G2OC_K(K_SCHUR_LANDMARK) bal_schur_y<<<cdiv(nh, kBalYBlocks), kBalYBlocks, 0, st>>>(nh, c->hpl_col.p, hpl.p,
+                                                                                         dinv.p, Y.p);
+        G2OC_LAUNCH_CHECK();
+      }
     }
     if (S.Cf == 0) return G2OC_OK;
-    G2OC_K(K_SCHUR_BLOCKS) bal_schur_blocks<<<cdiv(S.sys_nnzb, kBalSchurWarps), kBalSchurWarps * 32, 0, st>>>(
-        S.sys_nnzb, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, c->s_pair_ptr.p, c->s_pairs.p, c->hc_ptr.p,
-        c->hc_blk.p, c->hpl_col.p, hpp.p, hpl.p, Y.p, lambda, c->b.p, c->b.p + (size_t)S.Cf * 9, Sval.p, bs);
+    G2OC_K(K_SCHUR_BLOCKS) bal_schur_chunks<<<cdiv(nchunks, kBalChunkWarps), kBalChunkWarps * 32, 0, st>>>(
+        nchunks, chunks.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, pairs.p, c->hc_blk.p, hpp.p, hpl.p, Y.p,
+        lambda, Sval.p, part.p);
     G2OC_LAUNCH_CHECK();
+    if (nreds > 0) {
+      G2OC_K(K_SCHUR_BLOCKS) bal_schur_reduce<<<cdiv((long long)nreds * 81, 256), 256, 0, st>>>(
+          nreds, reds.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, hpp.p, lambda, part.p, Sval.p);
+      G2OC_LAUNCH_CHECK();
+    }
+    if (bs) {
+      if (nrch > 0)
+        G2OC_K(K_SCHUR_RHS) bal_schur_rhs_chunks<<<cdiv(nrch, 8), 256, 0, st>>>(
+            nrch, rch.p, c->hc_blk.p, c->hpl_col.p, Y.p, c->b.p + (size_t)S.Cf * 9, rpart.p);
+      G2OC_K(K_SCHUR_RHS) bal_schur_rhs_reduce<<<cdiv(S.Cf * 9, 256), 256, 0, st>>>(S.Cf, rch_ptr.p, rpart.p, c->b.p,
+                                                                                    bs);
+      G2OC_LAUNCH_CHECK();
+    }
     return G2OC_OK;
   }
 
   int backsub(const double* rl, const double* xp, double* xl) {
     const Structure& S = c->S;
     if (S.Pf == 0) return G2OC_OK;
-    G2OC_K(K_BACKSUB) bal_backsub<<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(c->hb_ptr.p, c->hpl_row.p, S.Pf, hpl.p,
-                                                                          dinv.p, rl, xp, xl);
+    if (S.lm_warp_ok) {
+      const int nch = (int)S.lm_chunk_ptr.size() - 1;
+      G2OC_K(K_BACKSUB) bal_backsub_warp<<<cdiv(nch, 8), 256, 0, c->stream>>>(
+          c->e_hpl.p, c->hpl_row.p, c->lm_chunk_ptr.p, nch, c->e_lm.p, hpl.p, dinv.p, rl, xp, xl);
+    } else {
+      G2OC_K(K_BACKSUB) bal_backsub<<<cdiv(S.Pf, 128), 128, 0, c->stream>>>(c->hb_ptr.p, c->hpl_row.p, S.Pf, hpl.p,
+                                                                            dinv.p, rl, xp, xl);
+    }
     G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
@@ -1743,7 +1849,8 @@ struct BalEngine final : EngineBase {
         }
         G2OC_TRY(g2oc::chol_solve<double>(*c->chol, st, A, c->rhs.p, c->xs.p, &ok, &c->kcount[K_CHOLESKY]));
       } else {
-        G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv<double, 9><<<cdiv(A.nb, 128), 128, 0, st>>>(A, minv.p, c->flag.p);
+        G2OC_K(K_PCG_DIAG_INV) pcg_diag_inv_lanes<double, 9><<<cdiv(A.nb, 3 * 4), 128, 0, st>>>(A, minv.p,
+                                                                                             c->flag.p);
         G2OC_LAUNCH_CHECK();
         const int rc = run_pcg_persistent<double, 9>(c, A, minv.p, c->rhs.p, c->xs.p, r.p, s.p, d.p, tbuf.p,
                                                      cpart.p, false);
@@ -1774,8 +1881,14 @@ struct BalEngine final : EngineBase {
         o[6] = a[2]; o[7] = a[4]; o[8] = a[5];
       }
     }
-    if (hpl_out && !S.hpl_rc.empty())
-      G2OC_CUDA_TRY(cudaMemcpy(hpl_out, hpl.p, S.hpl_rc.size() / 2 * 27 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (hpl_out && !S.hpl_rc.empty()) {
+      const size_t nh = S.hpl_rc.size() / 2;
+      std::vector<double> h(nh * kBalBlk);
+      G2OC_CUDA_TRY(cudaMemcpy(h.data(), hpl.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      for (size_t a = 0; a < nh; ++a)
+        for (int r = 0; r < 9; ++r)
+          for (int cc = 0; cc < 3; ++cc) hpl_out[a * 27 + r * 3 + cc] = h[a * kBalBlk + bal_bt(r, cc)];
+    }
     return G2OC_OK;
   }
 

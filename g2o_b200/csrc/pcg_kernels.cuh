@@ -132,6 +132,35 @@ __device__ __forceinline__ bool inverse_gj_lanes(double (&m)[N], double (&inv)[N
   return ok;
 }
 
+// M^-1 of BS x BS diagonal blocks, 32 / BS blocks per warp (BS lanes each,
+// one row per lane; the lanes past the last group idle): the inverses of
+// pcg_diag_inv<Real, BS> without its per-thread local arrays. Launch with
+// ceil(nb / (32 / BS)) warps or more.
+template <typename Real, int BS>
+__global__ void pcg_diag_inv_lanes(SysDev<Real> A, double* minv, int* nonfinite) {
+  constexpr int G = 32 / BS;
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int grp = lane / BS, i = lane - BS * grp;
+  const int blk = gw * G + grp;
+  const bool act = grp < G && blk < A.nb;
+  double m[BS], inv[BS];
+  if (act) {
+    const int rb = A.rptr[blk], nblk = A.rptr[blk + 1] - rb, j = A.diag[blk] - rb;
+#pragma unroll
+    for (int c = 0; c < BS; ++c) m[c] = (double)A.val[sys_offset<BS>(rb, nblk, j, i * BS + c)];
+  } else {
+#pragma unroll
+    for (int c = 0; c < BS; ++c) m[c] = (c == i) ? 1.0 : 0.0;
+  }
+  const bool ok = inverse_gj_lanes<BS>(m, inv, i, lane - i);
+  if (act) {
+    if (!ok && i == 0) *nonfinite = 1;
+#pragma unroll
+    for (int c = 0; c < BS; ++c) minv[(size_t)blk * BS * BS + i * BS + c] = inv[c];
+  }
+}
+
 // M^-1 of 6x6 diagonal blocks, five blocks per warp (six lanes each, one
 // row per lane; lanes 30 and 31 idle): the inverses of pcg_diag_inv<Real, 6>
 // without its per-thread local arrays. Launch with nb * 32 / 5 threads or more.

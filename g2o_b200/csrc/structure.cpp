@@ -271,8 +271,9 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
         if (s.e_hpl[k] >= 0 && s.e_hpl[k] == s.e_hpl[k - 1]) ok = false;
     }
     // (the edge-parallel passes are written for the two-row projection
-    // edges; the stereo edge's landmarks take the thread-per-landmark ones)
-    s.lm_warp_ok = ok && s.Pf > 0 && s.D == 2 && !s.bal;
+    // edges, BAL's included; the stereo edge's landmarks take the
+    // thread-per-landmark ones)
+    s.lm_warp_ok = ok && s.Pf > 0 && s.D == 2;
     s.lm_chunk_ptr.clear();
     s.e_lm.clear();
     if (s.lm_warp_ok) {
