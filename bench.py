@@ -820,8 +820,8 @@ def bal_algorithmic_bytes(kernel, info, E, num_pairs, uniform_info=True):
         return (rec + 4) * E + 32 * P + 72 * C + 216 * nH + 72 * P
     if kernel == "ba_camera_pass":  # camera-major edge copy, points, cameras -> Hpp, b_p
         return rec * E + 32 * P + 72 * C + 720 * C
-    if kernel == "schur_landmark":  # H_ll, Hpl -> Dinv, Y
-        return 48 * P + 216 * nH + 72 * P + 216 * nH
+    if kernel == "schur_landmark":  # H_ll -> Dinv; Hpl, Dinv, b_l -> Y (with b_l)
+        return 48 * P + 72 * P + 216 * nH + 72 * P + 24 * P + 240 * nH
     if kernel == "schur_blocks":  # Y and Hpl, Hpp, b, pair and block lists -> S (upper), b_s
         return 432 * nH + 648 * C + 24 * P + 72 * C + 8 * num_pairs + 16 * nS + 648 * nS + 72 * C
     if kernel == "pcg_iteration":  # S (upper) + column/perm index, T written and read, M^-1, x r s d, gathers of d
@@ -902,15 +902,27 @@ def run_bal(args):
     prob.set_kernel_timing(False)
     info = prob.info
     pcg_iters = sum(x["iterations_linear_solver"] for x in st3)
+    trials = sum(x["levenberg_iterations"] for x in st3)
     roof = None
     peak, peak_kind = measured_peaks()
     best = None
+    # units each kernel id's algorithmic bytes are counted per (a kernel id can
+    # cover several launches: the Schur chunks and their reduction, the
+    # camera chunks and theirs, Dinv and Y)
+    per_trial = ("schur_blocks", "schur_landmark", "ba_backsub")
+    per_iteration = ("ba_landmark_pass", "ba_camera_pass")
     for k, (nl, tms) in ks.items():
         if nl <= 0 or tms <= 0:
             continue
         if k == "pcg_solve":
             b = bal_algorithmic_bytes("pcg_iteration", info, g.num_edges, info.schur_pairs)
             units, per = max(pcg_iters, 1), "PCG iteration"
+        elif k in per_trial:
+            b = bal_algorithmic_bytes(k, info, g.num_edges, info.schur_pairs)
+            units, per = max(trials, 1), "LM trial"
+        elif k in per_iteration:
+            b = bal_algorithmic_bytes(k, info, g.num_edges, info.schur_pairs)
+            units, per = max(len(st3), 1), "LM iteration"
         else:
             b = bal_algorithmic_bytes(k, info, g.num_edges, info.schur_pairs)
             units, per = nl, "launch"

@@ -541,11 +541,13 @@ static __global__ void bal_schur_landmark(const double* hll, int Pf, double lamb
 // Y_a = Hpl_a Dinv_l(a) for every Hpl block, the factor every Schur product
 // of the block uses: a CTA per kBalYBlocks consecutive blocks loads them into
 // shared memory coalesced, each thread forms its block's product in place,
-// and the CTA stores the range coalesced (the pads stay zero)
+// and the CTA stores the range coalesced. The three pads of a Y block carry
+// b_l(a), so the diagonal Schur chunks that stage Y_a also form the reduced
+// right-hand side's products Y_a b_l.
 constexpr int kBalYBlocks = 128;
 
 static __global__ void __launch_bounds__(kBalYBlocks)
-    bal_schur_y(int nh, const int* hpl_col, const double* hpl, const double* dinv, double* Y) {
+    bal_schur_y(int nh, const int* hpl_col, const double* hpl, const double* dinv, const double* b_l, double* Y) {
   __shared__ __align__(16) double sm[kBalYBlocks * kBalBlk];
   const int a0 = blockIdx.x * kBalYBlocks;
   const int n = min(kBalYBlocks, nh - a0);
@@ -567,7 +569,8 @@ static __global__ void __launch_bounds__(kBalYBlocks)
   }
   __syncthreads();
   if ((int)threadIdx.x < n) {
-    const double* D = dinv + (size_t)hpl_col[a0 + threadIdx.x] * 9;
+    const int l = hpl_col[a0 + threadIdx.x];
+    const double* D = dinv + (size_t)l * 9;
     double d[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) d[q] = D[q];
@@ -579,6 +582,9 @@ static __global__ void __launch_bounds__(kBalYBlocks)
 #pragma unroll
       for (int c = 0; c < 3; ++c) row[c] = b0 * d[c] + b1 * d[3 + c] + b2 * d[6 + c];
     }
+    B[9] = b_l[(size_t)l * 3];
+    B[19] = b_l[(size_t)l * 3 + 1];
+    B[29] = b_l[(size_t)l * 3 + 2];
   }
   __syncthreads();
   double2* dst = reinterpret_cast<double2*>(Y + (size_t)a0 * kBalBlk);
@@ -681,7 +687,7 @@ __device__ __forceinline__ void bal_ld_triple(const double* p, double (&v)[9]) {
 __global__ void __launch_bounds__(kBalChunkWarps * 32)
     bal_schur_chunks(int nchunks, const int4* chunks, const int* brow, const int* rptr, const int* rcol,
                      const int2* pairs, const int* hc_blk, const double* hpp, const double* hpl, const double* Y,
-                     double lambda, double* S, double* part) {
+                     double lambda, double* S, double* part, const double* b_p, double* bs, double* rpart) {
   __shared__ __align__(16) double stage[kBalChunkWarps][2][kBalStage * kBalItem];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int ch = blockIdx.x * kBalChunkWarps + wid;
@@ -697,6 +703,10 @@ __global__ void __launch_bounds__(kBalChunkWarps * 32)
     acc[q] = 0.0;
     acc2[q] = 0.0;
   }
+  // diagonal blocks: the lanes with bj == 0 also sum Y_a b_l(a) for their
+  // rows 3bi .. 3bi + 2 (b_l rides in Y_a's pads)
+  double rv[3] = {0.0, 0.0, 0.0};
+  const bool rhs = diag && bj == 0;
   // stage s covers items q0 + s kBalStage ..; prologue: copies of stage 0,
   // indices of stage 1
   int a, b;
@@ -738,6 +748,19 @@ __global__ void __launch_bounds__(kBalChunkWarps * 32)
               acc[u * 3 + v] = fma(y[u * 3 + m], h[v * 3 + m], acc[u * 3 + v]);
               acc2[u * 3 + v] = fma(y2[u * 3 + m], h2[v * 3 + m], acc2[u * 3 + v]);
             }
+        if (rhs) {
+          const double* p1 = st + it * kBalItem;
+          const double* p2 = st + (it + 3) * kBalItem;
+#pragma unroll
+          for (int u = 0; u < 3; ++u) {
+            rv[u] = fma(y[u * 3], p1[9], rv[u]);
+            rv[u] = fma(y[u * 3 + 1], p1[19], rv[u]);
+            rv[u] = fma(y[u * 3 + 2], p1[29], rv[u]);
+            rv[u] = fma(y2[u * 3], p2[9], rv[u]);
+            rv[u] = fma(y2[u * 3 + 1], p2[19], rv[u]);
+            rv[u] = fma(y2[u * 3 + 2], p2[29], rv[u]);
+          }
+        }
       }
       if (it < np) {
         double y[9], h[9];
@@ -749,6 +772,15 @@ __global__ void __launch_bounds__(kBalChunkWarps * 32)
           for (int u = 0; u < 3; ++u)
 #pragma unroll
             for (int v = 0; v < 3; ++v) acc[u * 3 + v] = fma(y[u * 3 + m], h[v * 3 + m], acc[u * 3 + v]);
+        if (rhs) {
+          const double* p1 = st + it * kBalItem;
+#pragma unroll
+          for (int u = 0; u < 3; ++u) {
+            rv[u] = fma(y[u * 3], p1[9], rv[u]);
+            rv[u] = fma(y[u * 3 + 1], p1[19], rv[u]);
+            rv[u] = fma(y[u * 3 + 2], p1[29], rv[u]);
+          }
+        }
       }
     }
     __syncwarp();  // the buffer is read before the copies of stage s + 2 overwrite it
@@ -762,13 +794,27 @@ __global__ void __launch_bounds__(kBalChunkWarps * 32)
     const double g2 = __shfl_sync(0xffffffffu, acc[q], lane + 18 < 32 ? lane + 18 : lane);
     acc[q] = (acc[q] + g1) + g2;
   }
+#pragma unroll
+  for (int u = 0; u < 3; ++u) {
+    const double g1 = __shfl_sync(0xffffffffu, rv[u], lane + 9 < 32 ? lane + 9 : lane);
+    const double g2 = __shfl_sync(0xffffffffu, rv[u], lane + 18 < 32 ? lane + 18 : lane);
+    rv[u] = (rv[u] + g1) + g2;
+  }
   if (lane >= 9) return;
   if (slot >= 0) {
 #pragma unroll
     for (int u = 0; u < 3; ++u)
 #pragma unroll
       for (int v = 0; v < 3; ++v) part[(size_t)slot * 81 + (3 * bi + u) * 9 + 3 * bj + v] = acc[u * 3 + v];
+    if (rhs) {
+#pragma unroll
+      for (int u = 0; u < 3; ++u) rpart[(size_t)slot * 9 + 3 * bi + u] = rv[u];
+    }
     return;
+  }
+  if (rhs && bs) {
+#pragma unroll
+    for (int u = 0; u < 3; ++u) bs[(size_t)r * 9 + 3 * bi + u] = b_p[(size_t)r * 9 + 3 * bi + u] - rv[u];
   }
   const int rb = rptr[r], nblk = rptr[r + 1] - rb, j = k - rb;
 #pragma unroll
@@ -784,7 +830,7 @@ __global__ void __launch_bounds__(kBalChunkWarps * 32)
 // the blocks cut into several chunks: (block, first slot, slots), thread per entry
 static __global__ void bal_schur_reduce(int nred, const int4* red, const int* brow, const int* rptr,
                                         const int* rcol, const double* hpp, double lambda, const double* part,
-                                        double* S) {
+                                        double* S, const double* rpart, const double* b_p, double* bs) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nred * 81) return;
   const int q = t / 81, e = t % 81;
@@ -792,54 +838,15 @@ static __global__ void bal_schur_reduce(int nred, const int4* red, const int* br
   double s = 0.0;
   for (int n = 0; n < rd.z; ++n) s += part[(size_t)(rd.y + n) * 81 + e];
   const int k = rd.x, r = brow[k];
+  if (e < 9 && bs && rcol[k] == r) {  // a diagonal block: the reduced right-hand side's entry e
+    double sr = 0.0;
+    for (int n = 0; n < rd.z; ++n) sr += rpart[(size_t)(rd.y + n) * 9 + e];
+    bs[(size_t)r * 9 + e] = b_p[(size_t)r * 9 + e] - sr;
+  }
   const int i = e / 9, jj = e % 9;
   const double base = rcol[k] == r ? hpp[(size_t)r * 81 + e] + (i == jj ? lambda : 0.0) : 0.0;
   const int rb = rptr[r], nblk = rptr[r + 1] - rb;
   S[sys_offset<9>(rb, nblk, k - rb, e)] = base - s;
-}
-
-// reduced right-hand side b_s = b_p - sum_a Y_a b_l(a) over each camera's Hpl
-// blocks. The camera's blocks are cut into chunks of at most kBalChunk (host
-// plan: camera, first block, end): one warp per chunk, lanes strided over the
-// blocks, a fixed shuffle tree, the chunk's 9 sums to `rpart`; then
-// bal_schur_rhs_reduce adds each camera's chunk sums in chunk order.
-static __global__ void bal_schur_rhs_chunks(int nrch, const int4* rch, const int* hc_blk, const int* hpl_col,
-                                            const double* Y, const double* b_l, double* rpart) {
-  const int lane = threadIdx.x & 31;
-  const int ch = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (ch >= nrch) return;
-  const int4 cd = rch[ch];
-  double v[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) v[q] = 0.0;
-  for (int p = cd.y + lane; p < cd.z; p += 32) {
-    const int a = hc_blk[p];
-    const double* bl = b_l + (size_t)hpl_col[a] * 3;
-    const double l0 = bl[0], l1 = bl[1], l2 = bl[2];
-    const double* y = Y + (size_t)a * kBalBlk;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) v[q] += y[bal_bt(q, 0)] * l0 + y[bal_bt(q, 1)] * l1 + y[bal_bt(q, 2)] * l2;
-  }
-#pragma unroll
-  for (int q = 0; q < 9; ++q) v[q] = warp_sum(v[q]);
-  if (lane < 9) {
-    double out = v[0];
-#pragma unroll
-    for (int q = 1; q < 9; ++q)
-      if (lane == q) out = v[q];
-    rpart[(size_t)ch * 9 + lane] = out;
-  }
-}
-
-// thread per (camera, entry): b_s = b_p - the camera's chunk sums in order
-static __global__ void bal_schur_rhs_reduce(int Cf, const int* rch_ptr, const double* rpart, const double* b_p,
-                                            double* bs) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= Cf * 9) return;
-  const int r = t / 9, e = t % 9;
-  double s = 0.0;
-  for (int q = rch_ptr[r]; q < rch_ptr[r + 1]; ++q) s += rpart[(size_t)q * 9 + e];
-  bs[t] = b_p[t] - s;
 }
 
 // Landmark back-substitution (block_solver.hpp:449-474):

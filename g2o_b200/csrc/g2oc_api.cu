@@ -1625,14 +1625,13 @@ struct BalEngine final : EngineBase {
   DBuf<double> hpp, hll, hpl, dinv, Y, Sval, minv, r, s, d, tbuf, cpart, part;
   // the Schur complement's work plan: chunks (block, first item, end, slot or
   // -1) and the blocks cut into several chunks (block, first slot, slots)
-  DBuf<int4> chunks, reds, rch, cch;
+  DBuf<int4> chunks, reds, cch;
   DBuf<int> cch_ptr;
   DBuf<double> ccpart;
   int ncch = 0;
   DBuf<int2> pairs;  // co-observation pairs as absolute Hpl block indices (a of the row camera, b)
-  DBuf<int> rch_ptr;
-  DBuf<double> rpart;
-  int nchunks = 0, nreds = 0, nrch = 0;
+  DBuf<double> rpart;  // the diagonal chunks' sums of Y_a b_l (reduced right-hand side), 9 per slot
+  int nchunks = 0, nreds = 0;
   explicit BalEngine(g2oc_ctx* ctx) : c(ctx) {}
 
   int plan_schur() {
@@ -1680,21 +1679,10 @@ struct BalEngine final : EngineBase {
       G2OC_TRY(cch_ptr.upload(cp, c->stream));
       G2OC_TRY(ccpart.alloc((size_t)ncch * 54 + 1));
     }
-    // the reduced right-hand side: each camera's Hpl blocks in chunks
-    std::vector<int4> rc;
-    std::vector<int> rp(S.Cf + 1, 0);
-    for (int r = 0; r < S.Cf; ++r) {
-      for (int q = S.hc_ptr[r]; q < S.hc_ptr[r + 1]; q += kBalChunk)
-        rc.push_back(make_int4(r, q, std::min(S.hc_ptr[r + 1], q + kBalChunk), 0));
-      rp[r + 1] = (int)rc.size();
-    }
-    nrch = (int)rc.size();
-    G2OC_TRY(rch.upload(rc.empty() ? std::vector<int4>{make_int4(0, 0, 0, 0)} : rc, c->stream));
-    G2OC_TRY(rch_ptr.upload(rp, c->stream));
-    G2OC_TRY(rpart.alloc((size_t)nrch * 9 + 1));
     G2OC_TRY(chunks.upload(ch.empty() ? std::vector<int4>{make_int4(0, 0, 0, -1)} : ch, c->stream));
     G2OC_TRY(reds.upload(rd.empty() ? std::vector<int4>{make_int4(0, 0, 0, 0)} : rd, c->stream));
     G2OC_TRY(part.alloc((size_t)nslots * 81 + 1));
+    G2OC_TRY(rpart.alloc((size_t)nslots * 9 + 1));
     return G2OC_OK;
   }
 
@@ -1785,27 +1773,20 @@ struct BalEngine final : EngineBase {
       G2OC_LAUNCH_CHECK();
       const int nh = (int)(S.hpl_rc.size() / 2);
       if (nh > 0) {
-        G2OC_K(K_SCHUR_LANDMARK) bal_schur_y<<<cdiv(nh, kBalYBlocks), kBalYBlocks, 0, st>>>(nh, c->hpl_col.p, hpl.p,
-                                                                                         dinv.p, Y.p);
+        G2OC_K(K_SCHUR_LANDMARK) bal_schur_y<<<cdiv(nh, kBalYBlocks), kBalYBlocks, 0, st>>>(
+            nh, c->hpl_col.p, hpl.p, dinv.p, c->b.p + (size_t)S.Cf * 9, Y.p);
         G2OC_LAUNCH_CHECK();
       }
     }
     if (S.Cf == 0) return G2OC_OK;
     G2OC_K(K_SCHUR_BLOCKS) bal_schur_chunks<<<cdiv(nchunks, kBalChunkWarps), kBalChunkWarps * 32, 0, st>>>(
         nchunks, chunks.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, pairs.p, c->hc_blk.p, hpp.p, hpl.p, Y.p,
-        lambda, Sval.p, part.p);
+        lambda, Sval.p, part.p, c->b.p, bs, rpart.p);
     G2OC_LAUNCH_CHECK();
     if (nreds > 0) {
-      G2OC_K(K_SCHUR_BLOCKS) bal_schur_reduce<<<cdiv((long long)nreds * 81, 256), 256, 0, st>>>(
-          nreds, reds.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, hpp.p, lambda, part.p, Sval.p);
-      G2OC_LAUNCH_CHECK();
-    }
-    if (bs) {
-      if (nrch > 0)
-        G2OC_K(K_SCHUR_RHS) bal_schur_rhs_chunks<<<cdiv(nrch, 8), 256, 0, st>>>(
-            nrch, rch.p, c->hc_blk.p, c->hpl_col.p, Y.p, c->b.p + (size_t)S.Cf * 9, rpart.p);
-      G2OC_K(K_SCHUR_RHS) bal_schur_rhs_reduce<<<cdiv(S.Cf * 9, 256), 256, 0, st>>>(S.Cf, rch_ptr.p, rpart.p, c->b.p,
-                                                                                    bs);
+      G2OC_K(K_SCHUR_RHS) bal_schur_reduce<<<cdiv((long long)nreds * 81, 256), 256, 0, st>>>(
+          nreds, reds.p, c->sys_brow.p, c->sys_rptr.p, c->sys_rcol.p, hpp.p, lambda, part.p, Sval.p, rpart.p, c->b.p,
+          bs);
       G2OC_LAUNCH_CHECK();
     }
     return G2OC_OK;
