@@ -71,6 +71,11 @@ class G2ocGraph(C.Structure):
         ("principal_point", C.c_double * 2),
         ("focal_length_y", C.c_double),
         ("stereo_bf", C.c_double),
+        ("num_pose_edges", C.c_int32),
+        ("pose_edge_vertex", _i32p),
+        ("pose_edge_measurement", _dp),
+        ("pose_edge_information", _dp),
+        ("pose_edge_robust_delta", _dp),
     ]
 
 
@@ -161,6 +166,7 @@ class G2ocHessianInfo(C.Structure):
         ("num_active_edges", C.c_int32),
         ("vector_size", C.c_int64),
         ("schur_pairs", C.c_int64),
+        ("num_active_pose_edges", C.c_int32),
     ]
 
 
@@ -196,6 +202,12 @@ class Graph:
     extra: dict = field(default_factory=dict)
     focal_length_y: Optional[float] = None  # fy of EdgeSE3ProjectXYZ / EdgeStereoSE3ProjectXYZ (None: focal_length)
     stereo_bf: float = 0.0  # EdgeStereoSE3ProjectXYZ::bf (baseline times fx)
+    # EdgeSE3Expmap edges between the cameras of a projection-edge graph
+    # (pose indices, SE3Quat::toVector measurement, 6x6 information, Huber deltas)
+    pose_edge_vertex: Optional[np.ndarray] = None
+    pose_edge_measurement: Optional[np.ndarray] = None
+    pose_edge_information: Optional[np.ndarray] = None
+    pose_edge_robust_delta: Optional[np.ndarray] = None
 
     def __post_init__(self):
         self.pose_estimate = np.ascontiguousarray(self.pose_estimate, dtype=np.float64)
@@ -210,6 +222,16 @@ class Graph:
             self.point_fixed = np.ascontiguousarray(self.point_fixed, dtype=np.uint8)
         if self.robust_delta is not None:
             self.robust_delta = np.ascontiguousarray(self.robust_delta, dtype=np.float64)
+        if self.pose_edge_vertex is not None:
+            self.pose_edge_vertex = np.ascontiguousarray(self.pose_edge_vertex, dtype=np.int32).reshape(-1, 2)
+            self.pose_edge_measurement = np.ascontiguousarray(self.pose_edge_measurement, dtype=np.float64)
+            self.pose_edge_information = np.ascontiguousarray(self.pose_edge_information, dtype=np.float64)
+        if self.pose_edge_robust_delta is not None:
+            self.pose_edge_robust_delta = np.ascontiguousarray(self.pose_edge_robust_delta, dtype=np.float64)
+
+    @property
+    def num_pose_edges(self) -> int:
+        return 0 if self.pose_edge_vertex is None else int(self.pose_edge_vertex.shape[0])
 
     @property
     def num_poses(self) -> int:
@@ -235,7 +257,8 @@ class Graph:
                      c(self.measurement), c(self.information), c(self.pose_fixed),
                      c(self.point_estimate), c(self.point_fixed), c(self.robust_delta),
                      self.focal_length, tuple(self.principal_point), self.name, dict(self.extra),
-                     self.focal_length_y, self.stereo_bf)
+                     self.focal_length_y, self.stereo_bf, c(self.pose_edge_vertex), c(self.pose_edge_measurement),
+                     c(self.pose_edge_information), c(self.pose_edge_robust_delta))
 
     def digest(self) -> str:
         """SHA-256 of the graph's types, arrays and intrinsics: equal digests
@@ -250,6 +273,10 @@ class Graph:
         h.update(np.array([self.focal_length, fy, *self.principal_point], np.float64).tobytes())
         if self.edge_type == EDGE_STEREO_SE3_PROJECT_XYZ:
             h.update(np.array([self.stereo_bf], np.float64).tobytes())
+        if self.num_pose_edges:
+            for a in (self.pose_edge_vertex, self.pose_edge_measurement, self.pose_edge_information,
+                      self.pose_edge_robust_delta):
+                h.update(b"-" if a is None else np.ascontiguousarray(a).tobytes())
         return h.hexdigest()
 
     def to_c(self) -> G2ocGraph:
@@ -272,6 +299,11 @@ class Graph:
         g.principal_point[1] = float(self.principal_point[1])
         g.focal_length_y = float(self.focal_length if self.focal_length_y is None else self.focal_length_y)
         g.stereo_bf = float(self.stereo_bf)
+        g.num_pose_edges = self.num_pose_edges
+        g.pose_edge_vertex = _ptr(self.pose_edge_vertex, C.c_int32)
+        g.pose_edge_measurement = _ptr(self.pose_edge_measurement, C.c_double)
+        g.pose_edge_information = _ptr(self.pose_edge_information, C.c_double)
+        g.pose_edge_robust_delta = _ptr(self.pose_edge_robust_delta, C.c_double)
         # keep the numpy arrays alive as long as the struct
         g._owner = self
         return g

@@ -259,6 +259,7 @@ struct g2oc_ctx {
     std::vector<int32_t> edge_vertex;
     std::vector<uint8_t> pose_fixed, point_fixed;
     bool has_pose_fixed = false, has_point_fixed = false;
+    std::vector<int32_t> pose_edge_vertex;  // the pose edge set's endpoints
   } topo;
   std::unique_ptr<g2oc::EngineBase> eng;
   std::unique_ptr<g2oc::CholPlan> chol;
@@ -384,6 +385,20 @@ struct g2oc_ctx {
     CE.oa3 = c_oa3.p;
     CE.ob3 = c_ob3.p;
     return CE;
+  }
+  // the pose edge set of a projection graph (EdgeSE3Expmap between cameras)
+  // on the pose-graph kernels: the active pose edges, the cameras in the
+  // SE3Quat::toVector layout those kernels read (pgpose, unpacked per use)
+  g2oc::DBuf<double> pgpose;
+  bool pose_edges() const { return !S.pact.empty(); }
+  g2oc::PGEdges ba_pose_edges() {
+    g2oc::PGEdges E;
+    E.n = (int)S.pact.size();
+    E.v = pe_v.p;
+    E.zinv = pe_zinv.p;
+    E.info = pe_info.p;
+    E.delta = pe_delta.p;
+    return E;
   }
   g2oc::PGEdges pg_edges() {
     g2oc::PGEdges E;
@@ -739,6 +754,8 @@ struct Engine final : EngineBase {
   size_t schur_smem = 0;
   DBuf<Real> hcontrib;
   DBuf<double> bcontrib;
+  DBuf<Real> phpp;  // the pose edge set's assembled blocks (storage order of hpp)
+  DBuf<double> pb;  // and its gradient
   std::unique_ptr<TcChol> tc;  // tensor-core Cholesky of the reduced camera system (mixed precision)
   explicit Engine(g2oc_ctx* ctx) : c(ctx) {}
 
@@ -814,6 +831,13 @@ struct Engine final : EngineBase {
       if (!stage_in_smem) schur_smem = 0;
       if (!stage_in_smem) G2OC_TRY(bdc.alloc((size_t)S.hpl_rc.size() / 2 * 18 + 1));
       G2OC_TRY(c->db.alloc((size_t)S.Pf * 3 + 1));
+      if (c->pose_edges()) {
+        const size_t npa = S.pact.size();
+        G2OC_TRY(hcontrib.alloc(npa * 3 * 36));
+        G2OC_TRY(bcontrib.alloc(npa * 2 * 6));
+        G2OC_TRY(phpp.alloc((size_t)(S.Cf + S.npp) * 36));
+        G2OC_TRY(pb.alloc((size_t)S.Cf * 6 + 1));
+      }
     } else {
       G2OC_TRY(hcontrib.alloc((size_t)S.act.size() * 3 * pd * pd));
       G2OC_TRY(bcontrib.alloc((size_t)S.act.size() * 2 * pd));
@@ -906,6 +930,32 @@ struct Engine final : EngineBase {
       }
       G2OC_LAUNCH_CHECK();
     }
+    if (S.ba && c->pose_edges()) G2OC_TRY(pose_edge_system());
+    return G2OC_OK;
+  }
+
+  // The pose edge set's part of buildSystem: the pose-graph kernels' edge
+  // contributions (pg_linearize on the cameras in SE3Quat::toVector layout),
+  // assembled per storage block and camera in edge order, then added to the
+  // camera pass's blocks and gradient (ba_add_pose_system)
+  int pose_edge_system() {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    const int npa = (int)S.pact.size();
+    G2OC_K(K_PG_LINEARIZE) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, st>>>(S.C, c->pose.p,
+                                                                                        c->pgpose.p);
+    G2OC_K(K_PG_LINEARIZE) pg_linearize<Real, G2OC_POSE_SE3EXPMAP><<<cdiv(npa, 64), 64, 0, st>>>(
+        c->pgpose.p, c->ba_pose_edges(), c->pe_trans.p, hcontrib.p, bcontrib.p);
+    G2OC_LAUNCH_CHECK();
+    const int nblk = S.Cf + S.npp;
+    G2OC_K(K_PG_ASSEMBLE_H) pg_assemble_h<Real, 6><<<cdiv((long long)nblk * 6, 128), 128, 0, st>>>(
+        nblk, c->hb_src_ptr.p, c->hb_src.p, hcontrib.p, phpp.p);
+    G2OC_K(K_PG_ASSEMBLE_B) pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(
+        S.Cf, c->bv_src_ptr.p, c->bv_src.p, bcontrib.p, pb.p);
+    const long long tot = (long long)nblk * 36 + (long long)S.Cf * 6;
+    G2OC_K(K_PG_ASSEMBLE_H) ba_add_pose_system<Real><<<cdiv(tot, 256), 256, 0, st>>>(S.Cf, S.npp, phpp.p, hpp.p,
+                                                                                      pb.p, c->b.p);
+    G2OC_LAUNCH_CHECK();
     return G2OC_OK;
   }
 
@@ -914,6 +964,10 @@ struct Engine final : EngineBase {
     cudaStream_t st = c->stream;
     const int n = c->vec_size();
     if (n <= 0) return G2OC_OK;
+    if (c->pose_edges()) {
+      set_error("the Hpp product (Dogleg, g2oc_multiply_hessian) takes no pose edge set");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
     if (S.Cf == 0) {
       G2OC_CUDA_TRY(cudaMemsetAsync(dst, 0, (size_t)n * sizeof(double), st));
       return G2OC_OK;
@@ -1428,7 +1482,12 @@ struct Engine final : EngineBase {
     if (hpp_out) {
       std::vector<Real> h(hpp.n);
       G2OC_CUDA_TRY(cudaMemcpy(h.data(), hpp.p, hpp.bytes(), cudaMemcpyDeviceToHost));
-      to_double(h, hpp_out);
+      if (S.ba && S.npp > 0) {  // storage (diagonal blocks, then pose-pose blocks) to hpp_rc order
+        for (size_t i = 0; i < S.hpp_store.size(); ++i)
+          for (int e = 0; e < 36; ++e) hpp_out[i * 36 + e] = (double)h[(size_t)S.hpp_store[i] * 36 + e];
+      } else {
+        to_double(h, hpp_out);
+      }
     }
     if (S.ba && hll_out && S.Pf > 0) {
       std::vector<Real> h((size_t)S.Pf * 6);
@@ -1922,7 +1981,16 @@ static int chi2_to(g2oc_ctx* c, double* out_plain, double* out_robust) {
     G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3EXPMAP><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   else G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3><<<kRedBlocks, 128, 0, st>>>(c->pose.p, c->pg_edges(), c->partials.p);
   G2OC_LAUNCH_CHECK();
-  G2OC_TRY(finalize_sum(c, S.ba ? kChi2Blocks : kRedBlocks, 2, out_plain, out_robust));
+  int nparts = S.ba ? kChi2Blocks : kRedBlocks;
+  if (S.ba && c->pose_edges()) {
+    // the pose edge set's chi2 in the partials after the projection edges'
+    G2OC_K(K_CHI2) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, st>>>(S.C, c->pose.p, c->pgpose.p);
+    G2OC_K(K_CHI2) pg_chi2_kernel<G2OC_POSE_SE3EXPMAP><<<kRedBlocks, 128, 0, st>>>(c->pgpose.p, c->ba_pose_edges(),
+                                                                                 c->partials.p + 2 * nparts);
+    G2OC_LAUNCH_CHECK();
+    nparts += kRedBlocks;
+  }
+  G2OC_TRY(finalize_sum(c, nparts, 2, out_plain, out_robust));
   G2OC_TRY(shard_reduce(c, out_plain, 1, G2OC_DT_F64, G2OC_RED_SUM));
   return shard_reduce(c, out_robust, 1, G2OC_DT_F64, G2OC_RED_SUM);
 }
@@ -2475,6 +2543,13 @@ void g2oc_destroy(g2oc_ctx* c) {
 }
 
 static int make_engine(g2oc_ctx* c) {
+  if (c->pose_edges() &&
+      (c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY ||
+       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0))) {
+    set_error("a graph with a pose edge set runs Gauss-Newton or Levenberg-Marquardt in FP64 or mixed precision "
+              "without FP64 refinement (*_mixed_fast)");
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
   if (c->S.bal) {
     if (c->prm.precision == G2OC_PREC_MIXED) {
       set_error("the BAL block solver runs in FP64 (no mixed-precision form)");
@@ -2515,6 +2590,11 @@ static bool same_topology(const g2oc_ctx::Topology& t, const g2oc_graph* g) {
       t.edge_type != g->edge_type || t.num_edges != g->num_edges || !g->edge_vertex)
     return false;
   if (t.has_pose_fixed != (g->pose_fixed != nullptr) || t.has_point_fixed != (g->point_fixed != nullptr)) return false;
+  if ((int32_t)(t.pose_edge_vertex.size() / 2) != g->num_pose_edges) return false;
+  if (g->num_pose_edges > 0 &&
+      (!g->pose_edge_vertex ||
+       memcmp(t.pose_edge_vertex.data(), g->pose_edge_vertex, t.pose_edge_vertex.size() * sizeof(int32_t))))
+    return false;
   if (!t.edge_vertex.empty()) {
     // compared in parallel chunks (tens of MB for large graphs)
     const size_t n = t.edge_vertex.size(), chunk = 1 << 20;
@@ -2541,6 +2621,10 @@ static void save_topology(g2oc_ctx::Topology& t, const g2oc_graph* g) {
   t.edge_type = g->edge_type;
   t.num_edges = g->num_edges;
   t.edge_vertex.assign(g->edge_vertex, g->edge_vertex + 2 * (size_t)g->num_edges);
+  if (g->num_pose_edges > 0)
+    t.pose_edge_vertex.assign(g->pose_edge_vertex, g->pose_edge_vertex + 2 * (size_t)g->num_pose_edges);
+  else
+    t.pose_edge_vertex.clear();
   t.has_pose_fixed = g->pose_fixed != nullptr;
   t.has_point_fixed = g->point_fixed != nullptr;
   t.pose_fixed.assign(g->pose_fixed ? g->pose_fixed : nullptr, g->pose_fixed ? g->pose_fixed + g->num_poses : nullptr);
@@ -2649,6 +2733,25 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
     for (size_t i = 0; i < ab.size(); ++i) ab[i] = make_int2(S.s_pairs[2 * i], S.s_pairs[2 * i + 1]);
     G2OC_TRY(c->s_pairs.upload(ab, st));
     G2OC_TRY(c->s_hpp.upload(S.s_hpp, st));
+    if (!S.pact.empty()) {
+      // the pose edge set, on the pose-graph kernels' arrays
+      const int npa = (int)S.pact.size();
+      std::vector<int2> pv(npa);
+      for (int k = 0; k < npa; ++k) {
+        const int e = S.pact[k];
+        pv[k] = make_int2(g->pose_edge_vertex[2 * e], g->pose_edge_vertex[2 * e + 1]);
+      }
+      G2OC_TRY(c->pe_v.upload(pv, st));
+      G2OC_TRY(c->pe_zinv.alloc((size_t)npa * 7));
+      G2OC_TRY(c->pe_info.alloc((size_t)npa * 36));
+      G2OC_TRY(c->pe_delta.alloc(npa));
+      G2OC_TRY(c->pe_trans.upload(S.pe_trans, st));
+      G2OC_TRY(c->hb_src_ptr.upload(S.hb_src_ptr, st));
+      G2OC_TRY(c->hb_src.upload(S.hb_src.empty() ? std::vector<int>{0} : S.hb_src, st));
+      G2OC_TRY(c->bv_src_ptr.upload(S.bv_src_ptr, st));
+      G2OC_TRY(c->bv_src.upload(S.bv_src.empty() ? std::vector<int>{0} : S.bv_src, st));
+      G2OC_TRY(c->pgpose.alloc((size_t)S.C * 7));
+    }
   } else {
     std::vector<int2> ev(na);
     for (int k = 0; k < na; ++k) {
@@ -2685,7 +2788,7 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
   G2OC_TRY(c->resid.alloc(n));
   G2OC_TRY(c->xs.alloc((size_t)S.Cf * S.pd));
   G2OC_TRY(c->rhs.alloc((size_t)S.Cf * S.pd));
-  G2OC_TRY(c->errbuf.alloc((size_t)na * 36));
+  G2OC_TRY(c->errbuf.alloc(std::max((size_t)na * 36, (size_t)na * S.D + S.pact.size() * 6)));
   G2OC_TRY(make_engine(c));
   save_topology(c->topo, g);
   return G2OC_OK;
@@ -2755,6 +2858,20 @@ static int upload_data(g2oc_ctx* c, const g2oc_graph* g) {
         G2OC_LAUNCH_CHECK();
       }
     }
+    if (!S.pact.empty()) {
+      // the pose edge set's values (EdgeSE3Expmap: the error uses the measurement C itself)
+      const int npa = (int)S.pact.size();
+      std::vector<double> zi((size_t)npa * 7), info((size_t)npa * 36), dl(npa);
+      for (int k = 0; k < npa; ++k) {
+        const int e = S.pact[k];
+        memcpy(zi.data() + (size_t)k * 7, g->pose_edge_measurement + (size_t)e * 7, 7 * sizeof(double));
+        memcpy(info.data() + (size_t)k * 36, g->pose_edge_information + (size_t)e * 36, 36 * sizeof(double));
+        dl[k] = g->pose_edge_robust_delta ? g->pose_edge_robust_delta[e] : 0.0;
+      }
+      G2OC_TRY(c->pe_zinv.upload(zi, st));
+      G2OC_TRY(c->pe_info.upload(info, st));
+      G2OC_TRY(c->pe_delta.upload(dl, st));
+    }
   } else {
     if (S.C > 0)
       G2OC_CUDA_TRY(cudaMemcpyAsync(c->pose.p, g->pose_estimate, c->pose.bytes(), cudaMemcpyHostToDevice, st));
@@ -2808,7 +2925,8 @@ int g2oc_upload(g2oc_ctx* c, const g2oc_graph* g) {
   c->last_upload_reused = false;
   if (reuse) {
     // the null checks build_structure makes for a new topology
-    if (!g->pose_estimate || !g->measurement || !g->information || (c->S.ba && g->num_points > 0 && !g->point_estimate)) {
+    if (!g->pose_estimate || !g->measurement || !g->information || (c->S.ba && g->num_points > 0 && !g->point_estimate) ||
+        (g->num_pose_edges > 0 && (!g->pose_edge_measurement || !g->pose_edge_information))) {
       set_error("graph array is NULL");
       return G2OC_ERR_INVALID_ARGUMENT;
     }
@@ -2836,6 +2954,7 @@ int g2oc_get_hessian_info(g2oc_ctx* c, g2oc_hessian_info* info) {
   info->num_active_edges = (int)S.act.size();
   info->vector_size = c->vec_size();
   info->schur_pairs = S.num_pairs;
+  info->num_active_pose_edges = (int32_t)S.pact.size();
   return G2OC_OK;
 }
 
@@ -2881,7 +3000,8 @@ int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
 static int check_sharding(g2oc_ctx* c) {
   if (c->shard_world <= 1) return G2OC_OK;
   const Structure& S = c->S;
-  if (!S.ba || !S.schur || !S.tile_ok || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY || pcg_mode() != PCG_AUTO ||
+  if (!S.ba || !S.schur || !S.tile_ok || c->pose_edges() || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY ||
+      pcg_mode() != PCG_AUTO ||
       c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY ||
       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0)) {
     set_error("sharded mode runs bundle adjustments with >= %d free cameras and landmarks, the PCG solver, FP64 or "
@@ -3020,11 +3140,21 @@ int g2oc_errors(g2oc_ctx* c, double* out) {
                                                                                                 c->errbuf.p);
   else G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE3><<<cdiv(na, 128), 128, 0, c->stream>>>(c->pose.p, c->pg_edges(), c->errbuf.p);
   G2OC_LAUNCH_CHECK();
-  std::vector<double> h((size_t)na * S.D);
+  const size_t npe = S.ba ? S.pact.size() : 0;
+  if (npe > 0) {
+    // the pose edge set's errors follow the projection edges'
+    G2OC_K(K_ERRORS) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, c->stream>>>(S.C, c->pose.p,
+                                                                                          c->pgpose.p);
+    G2OC_K(K_ERRORS) pg_errors_kernel<G2OC_POSE_SE3EXPMAP><<<cdiv((long long)npe, 128), 128, 0, c->stream>>>(
+        c->pgpose.p, c->ba_pose_edges(), c->errbuf.p + (size_t)na * S.D);
+    G2OC_LAUNCH_CHECK();
+  }
+  std::vector<double> h((size_t)na * S.D + npe * 6);
   G2OC_CUDA_TRY(cudaMemcpyAsync(h.data(), c->errbuf.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   G2OC_CUDA_TRY(cudaStreamSynchronize(c->stream));
   for (int a = 0; a < na; ++a)
     memcpy(out + (size_t)a * S.D, h.data() + (size_t)S.dev_of_act[a] * S.D, S.D * sizeof(double));
+  if (npe > 0) memcpy(out + (size_t)na * S.D, h.data() + (size_t)na * S.D, npe * 6 * sizeof(double));
   return G2OC_OK;
 }
 
@@ -3198,7 +3328,7 @@ int g2oc_backward(g2oc_ctx* c, const double* dL_dx, double* dL_dmeas, double* dL
     return G2OC_ERR_INVALID_ARGUMENT;
   }
   const Structure& S = c->S;
-  if (!S.ba || !S.schur || S.Cf == 0 || S.D != 2 || S.bal) {
+  if (!S.ba || !S.schur || S.Cf == 0 || S.D != 2 || S.bal || c->pose_edges()) {
     set_error("g2oc_backward supports SE3 bundle adjustment with two-row projection edges, free cameras and landmarks");
     return G2OC_ERR_NOT_SUPPORTED;
   }

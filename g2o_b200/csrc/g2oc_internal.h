@@ -77,6 +77,12 @@ struct Structure {
   int pd = 0, ped = 0, D = 0, md = 0;
   bool ba = false, schur = false;
   bool bal = false;  // EdgeObservationBAL + VertexCameraBAL (9-parameter cameras, bal_kernels.cuh)
+  // the pose edge set of a projection graph (EdgeSE3Expmap between cameras):
+  // active edges; the pose-pose Hpp blocks are stored after the Cf diagonal
+  // blocks (storage index Cf + p), hpp_store maps hpp_rc order to storage
+  std::vector<int> pact;
+  int npp = 0;
+  std::vector<int> hpp_store;
   std::vector<int> act;                 // active edge ids, insertion order
   std::vector<int> pose_h, point_l;     // Hessian index of each pose / landmark index of each point, -1 = none
   std::vector<int> free_pose_of_h;      // pose index of Hessian row h

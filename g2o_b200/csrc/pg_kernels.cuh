@@ -303,6 +303,19 @@ __global__ void pg_assemble_b(int Cf, const int* src_ptr, const int* src, const 
   b[(size_t)h * D + r] = acc;
 }
 
+// The pose edge set of a projection graph joins the camera system: its
+// assembled blocks (pg_assemble_h over the storage blocks: the Cf diagonal
+// blocks, then the pose-pose blocks) are added to the camera pass's diagonal
+// blocks and become the pose-pose blocks; its gradient is added to b_p
+template <typename Real>
+__global__ void ba_add_pose_system(int Cf, int npp, const Real* phpp, Real* hpp, const double* pb, double* b) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nd = (long long)Cf * 36, nh = (long long)(Cf + npp) * 36;
+  if (t < nd) hpp[t] = (Real)((double)hpp[t] + (double)phpp[t]);
+  else if (t < nh) hpp[t] = phpp[t];
+  else if (t < nh + (long long)Cf * 6) b[t - nh] += pb[t - nh];
+}
+
 // VertexSE2::oplusImpl (g2o/types/slam2d/vertex_se2.h:48-54) and
 // VertexSE3::oplusImpl with orthogonalization after 1000 updates
 // (g2o/types/slam3d/vertex_se3.h:99-108, isometry3d_mappings.h:81-85)

@@ -5,6 +5,7 @@
 // as device orderings, ranges and gather lists. Runs once per upload; all
 // sorts are stable counting / radix sorts, so every list is deterministic.
 #include <algorithm>
+#include <array>
 #include <cstdarg>
 #include <cstdio>
 #include <numeric>
@@ -178,6 +179,15 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     qa[v0] = 1;
     pa[v1] = 1;
   }
+  // the pose edge set (EdgeSE3Expmap between cameras): active unless both fixed
+  s.pact.clear();
+  for (int e = 0; e < g->num_pose_edges; ++e) {
+    const int v0 = g->pose_edge_vertex[2 * e], v1 = g->pose_edge_vertex[2 * e + 1];
+    if (pf && pf[v0] && pf[v1]) continue;
+    s.pact.push_back(e);
+    pa[v0] = 1;
+    pa[v1] = 1;
+  }
   if (s.act.empty()) {
     set_error("graph has no active edge");
     return G2OC_ERR_BAD_GRAPH;
@@ -313,13 +323,76 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     counting_sort(rk, s.Cf, ord, s.hc_ptr);
     s.hc_blk = ord;
   }
-  // Hpp: the diagonal blocks only (projection edges join a pose and a point)
-  s.hpp_rc.resize(2 * (size_t)s.Cf);
+  // Hpp: the diagonal blocks (projection edges join a pose and a point),
+  // stored at index h, and the pose edges' pose-pose blocks (row < column),
+  // stored after them at Cf + p in (row, column) order; hpp_rc lists all of
+  // them column-major (the order of SparseBlockMatrix::blockCols) and
+  // hpp_store maps that order to storage
+  std::vector<std::pair<int, int>> pp;  // (row, column) of the pose-pose blocks
+  for (int e : s.pact) {
+    int a = s.pose_h[g->pose_edge_vertex[2 * e]], b = s.pose_h[g->pose_edge_vertex[2 * e + 1]];
+    if (a < 0 || b < 0) continue;
+    if (a > b) std::swap(a, b);
+    pp.push_back({a, b});
+  }
+  std::sort(pp.begin(), pp.end());
+  pp.erase(std::unique(pp.begin(), pp.end()), pp.end());
+  s.npp = (int)pp.size();
   s.hpp_diag.resize(s.Cf);
-  for (int h = 0; h < s.Cf; ++h) {
-    s.hpp_rc[2 * h] = h;
-    s.hpp_rc[2 * h + 1] = h;
-    s.hpp_diag[h] = h;
+  for (int h = 0; h < s.Cf; ++h) s.hpp_diag[h] = h;
+  {
+    std::vector<std::array<int, 3>> cm;  // (column, row, storage)
+    cm.reserve(s.Cf + pp.size());
+    for (int h = 0; h < s.Cf; ++h) cm.push_back({h, h, h});
+    for (size_t q = 0; q < pp.size(); ++q) cm.push_back({pp[q].second, pp[q].first, s.Cf + (int)q});
+    std::sort(cm.begin(), cm.end());
+    s.hpp_rc.resize(2 * cm.size());
+    s.hpp_store.resize(cm.size());
+    for (size_t i = 0; i < cm.size(); ++i) {
+      s.hpp_rc[2 * i] = cm[i][1];
+      s.hpp_rc[2 * i + 1] = cm[i][0];
+      s.hpp_store[i] = cm[i][2];
+    }
+  }
+  auto pair_store = [&](int r, int c) -> int {  // storage index of pose-pose block (r < c), or -1
+    auto it = std::lower_bound(pp.begin(), pp.end(), std::make_pair(r, c));
+    return (it != pp.end() && *it == std::make_pair(r, c)) ? s.Cf + (int)(it - pp.begin()) : -1;
+  };
+  // the pose edges' contributions (pg_linearize slots: edge * 3 + {0: (v0,v0),
+  // 1: (v1,v1), 2: (v0,v1)}; gradient edge * 2 + {0, 1}) routed to the
+  // storage blocks and the cameras, in edge order
+  {
+    const int npa = (int)s.pact.size();
+    s.pe_trans.assign(npa, 0);
+    std::vector<int> src_key, src_val, bv_key, bv_val;
+    for (int k = 0; k < npa; ++k) {
+      const int e = s.pact[k];
+      const int a = s.pose_h[g->pose_edge_vertex[2 * e]], b = s.pose_h[g->pose_edge_vertex[2 * e + 1]];
+      if (a >= 0) {
+        src_key.push_back(a);
+        src_val.push_back(3 * k + 0);
+        bv_key.push_back(a);
+        bv_val.push_back(2 * k + 0);
+      }
+      if (b >= 0) {
+        src_key.push_back(b);
+        src_val.push_back(3 * k + 1);
+        bv_key.push_back(b);
+        bv_val.push_back(2 * k + 1);
+      }
+      if (a >= 0 && b >= 0) {
+        s.pe_trans[k] = a > b;
+        src_key.push_back(pair_store(std::min(a, b), std::max(a, b)));
+        src_val.push_back(3 * k + 2);
+      }
+    }
+    std::vector<int> ord;
+    counting_sort(src_key, s.Cf + s.npp, ord, s.hb_src_ptr);
+    s.hb_src.resize(ord.size());
+    for (size_t i = 0; i < ord.size(); ++i) s.hb_src[i] = src_val[ord[i]];
+    counting_sort(bv_key, s.Cf, ord, s.bv_src_ptr);
+    s.bv_src.resize(ord.size());
+    for (size_t i = 0; i < ord.size(); ++i) s.bv_src[i] = bv_val[ord[i]];
   }
   // position of each Hpl block in its camera's list
   s.hc_pos.assign(nhpl, 0);
@@ -417,6 +490,17 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
       }
     }
     s.s_pairs.swap(sp);
+    // the pose-pose blocks join the pattern (no co-observation pair of their own)
+    for (const auto& q : pp) {
+      std::vector<int32_t>& cols = row_cols[q.first];
+      std::vector<int32_t>& cc = row_cnt[q.first];
+      auto it = std::lower_bound(cols.begin(), cols.end(), q.second);
+      if (it == cols.end() || *it != q.second) {
+        const size_t at = (size_t)(it - cols.begin());
+        cols.insert(it, q.second);
+        cc.insert(cc.begin() + at, 0);
+      }
+    }
     // internal (row-major) blocks: per row the diagonal, then the columns
     std::vector<int32_t> rm;
     std::vector<int> ptr;
@@ -430,7 +514,7 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
       for (size_t i = 0; i < row_cols[r].size(); ++i) {
         rm.push_back(r);
         rm.push_back(row_cols[r][i]);
-        s.s_hpp.push_back(-1);
+        s.s_hpp.push_back(pp.empty() ? -1 : pair_store(r, row_cols[r][i]));
         acc += row_cnt[r][i];
         ptr.push_back((int)acc);
       }
@@ -449,6 +533,10 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
     }
     build_sym_lists(Cf, s.schur_rc, s);  // internal order = the row-major order above
   } else {
+    if (s.npp > 0) {
+      set_error("a pose edge set needs free landmarks (the Schur complement carries the pose-pose blocks)");
+      return G2OC_ERR_NOT_SUPPORTED;
+    }
     build_sym_lists(s.Cf, s.hpp_rc, s);
   }
   return G2OC_OK;
@@ -589,6 +677,27 @@ int build_structure(const g2oc_graph* g, Structure& s) {
   s.ped = pose_est_dim(s.pose_type);
   s.D = edge_dim(s.edge_type);
   s.md = meas_dim(s.edge_type);
+  if (g->num_pose_edges < 0) {
+    set_error("num_pose_edges is negative");
+    return G2OC_ERR_INVALID_ARGUMENT;
+  }
+  if (g->num_pose_edges > 0) {
+    if (!ba || bal || g->pose_type != G2OC_POSE_SE3EXPMAP) {
+      set_error("a pose edge set (EdgeSE3Expmap) joins the VertexSE3Expmap cameras of a projection-edge graph");
+      return G2OC_ERR_BAD_GRAPH;
+    }
+    if (!g->pose_edge_vertex || !g->pose_edge_measurement || !g->pose_edge_information) {
+      set_error("pose edge array is NULL");
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+    for (int e = 0; e < g->num_pose_edges; ++e) {
+      const int v0 = g->pose_edge_vertex[2 * e], v1 = g->pose_edge_vertex[2 * e + 1];
+      if (v0 < 0 || v0 >= s.C || v1 < 0 || v1 >= s.C || v0 == v1) {
+        set_error("pose edge %d has vertex indices (%d, %d) out of range", e, v0, v1);
+        return G2OC_ERR_BAD_GRAPH;
+      }
+    }
+  }
   const int n0 = ba ? s.P : s.C;
   for (int e = 0; e < s.E; ++e) {
     const int v0 = g->edge_vertex[2 * e], v1 = g->edge_vertex[2 * e + 1];

@@ -527,6 +527,38 @@ def bal_problem(num_cameras=356, num_points=226_730, mean_obs=5.5, focal=500.0, 
     return b
 
 
+def ba_with_odometry(num_cameras=40, num_points=3000, rot_sigma=0.01, trans_sigma=0.05, seed=SEED_BASE + 7, **kw):
+    """The ring bundle adjustment with a second edge set: EdgeSE3Expmap
+    odometry between consecutive cameras of the ring (and the last to the
+    first). The measurement is C_ij = T_j E T_i^-1 from the generating poses
+    with E = (R(w), u), w ~ N(0, rot_sigma^2), u ~ N(0, trans_sigma^2), so that
+    the edge error log(T_j^-1 C_ij T_i) = log(E) is that noise (to first
+    order), with information diag(1 / rot_sigma^2 x3, 1 / trans_sigma^2 x3) in
+    (omega, upsilon) order and no robust kernel: the graph of a visual SLAM
+    back end with odometry."""
+    g = bundle_adjustment(num_cameras=num_cameras, num_points=num_points, seed=seed, **kw)
+    rng = np.random.default_rng(seed + 15485863)
+    tp = g.extra["truth_pose"]
+    R = _quat_to_rot(tp[:, 3:7])
+    t = tp[:, :3]
+    i = np.arange(num_cameras)
+    j = (i + 1) % num_cameras
+    RE = _axis_angle(rng.normal(0.0, rot_sigma, size=(num_cameras, 3)))
+    tE = rng.normal(0.0, trans_sigma, size=(num_cameras, 3))
+    Rit = np.transpose(R[i], (0, 2, 1))
+    A = _mm(RE, Rit)  # E T_i^-1: rotation RE Ri^T, translation -RE Ri^T t_i + tE
+    a = -_mv(A, t[i]) + tE
+    Rc = _mm(R[j], A)
+    tc = _mv(R[j], a) + t[j]
+    info = np.diag([1.0 / rot_sigma ** 2] * 3 + [1.0 / trans_sigma ** 2] * 3).reshape(1, 36)
+    g.pose_edge_vertex = np.stack([i, j], 1).astype(np.int32)
+    g.pose_edge_measurement = np.concatenate([tc, _rot_to_quat(Rc)], axis=1)
+    g.pose_edge_information = np.tile(info, (num_cameras, 1))
+    g.pose_edge_robust_delta = None
+    g.name = g.name.replace("bundle_adjustment", "ba_odometry")
+    return g
+
+
 def window_sizes(num_windows=512, cameras=(10, 60), points=(500, 8000), seed=SEED_BASE + 1000):
     """(cameras, points) of each window: log-uniform in the given ranges."""
     rng = np.random.default_rng(seed)

@@ -69,8 +69,10 @@
 extern "C" {
 #endif
 
-#define G2OC_ABI_VERSION 4 /* 4: the BAL camera and observation types; 3: g2oc_graph.stereo_bf
-                             (EdgeStereoSE3ProjectXYZ); 2: focal_length_y */
+#define G2OC_ABI_VERSION 5 /* 5: g2oc_graph's pose edges (EdgeSE3Expmap beside projection edges),
+                             g2oc_hessian_info.num_active_pose_edges; 4: the BAL camera and
+                             observation types; 3: g2oc_graph.stereo_bf (EdgeStereoSE3ProjectXYZ);
+                             2: focal_length_y */
 
 /* status codes */
 #define G2OC_OK 0
@@ -153,6 +155,16 @@ typedef struct g2oc_graph {
   double principal_point[2];
   double focal_length_y;       /* fy of SE3_PROJECT_XYZ and STEREO_SE3_PROJECT_XYZ; ignored otherwise */
   double stereo_bf;            /* EdgeStereoSE3ProjectXYZ::bf (baseline times fx); ignored otherwise */
+  /* A second edge set, EdgeSE3Expmap between the VertexSE3Expmap cameras of
+     a projection-edge graph (PROJECT_XYZ2UV, SE3_PROJECT_XYZ,
+     STEREO_SE3_PROJECT_XYZ): BlockSolver assembles both kinds into one
+     system (g2o/core/block_solver.hpp:492-565), e.g. odometry or loop
+     constraints beside the observations of a visual SLAM back end. 0: none. */
+  int32_t num_pose_edges;
+  const int32_t* pose_edge_vertex;      /* num_pose_edges * 2 pose indices (vertex0, vertex1) */
+  const double* pose_edge_measurement;  /* num_pose_edges * 7: the edge's _measurement as SE3Quat::toVector */
+  const double* pose_edge_information;  /* num_pose_edges * 36, row-major, (omega, upsilon) order */
+  const double* pose_edge_robust_delta; /* num_pose_edges Huber deltas; <= 0 or NULL: no kernel */
 } g2oc_graph;
 
 typedef struct g2oc_params {
@@ -203,6 +215,7 @@ typedef struct g2oc_hessian_info {
   int32_t num_active_edges;
   int64_t vector_size;      /* Solver::vectorSize() */
   int64_t schur_pairs;      /* co-observing Hpl block pairs (a < b) summed into off-diagonal Schur blocks */
+  int32_t num_active_pose_edges; /* active edges of the pose edge set (g2oc_graph.num_pose_edges) */
 } g2oc_hessian_info;
 
 /* per-kernel launch count and (when timing is on) summed CUDA-event time */

@@ -1016,6 +1016,14 @@ struct orc_problem {
   std::vector<double> meas, info, delta;
   double fx = 1, fy = 1, cx = 0, cy = 0, bf = 0;
   bool ba = false;  // EdgeProjectXYZ2UV or EdgeSE3ProjectXYZ
+  // the pose edge set: EdgeSE3Expmap between the cameras of a projection-edge graph
+  int PE = 0;
+  std::vector<int> pev;                      // PE * 2 camera indices
+  std::vector<double> pmeas, pinfo, pdelta;  // 7, 36, 1 per edge
+  std::vector<int> pact;                     // active pose edges
+  std::vector<int> pe_diag0, pe_diag1, pe_off;
+  std::vector<char> pe_trans;
+  std::vector<double> perr;                  // per active pose edge, 6
   std::vector<int> oplus_count;  // VertexSE3 orthogonalization counter
   // active sets and index mapping (sparse_optimizer.cpp:175-287)
   std::vector<int> act;  // active edge ids
@@ -1098,11 +1106,28 @@ double edge_chi2(const orc_problem* p, int e, const double* er) {
   return s;
 }
 
+double pose_edge_chi2(const orc_problem* p, int e, const double* er) {
+  const double* Om = p->pinfo.data() + (size_t)e * 36;
+  double s = 0;
+  for (int i = 0; i < 6; ++i) {
+    double t = 0;
+    for (int j = 0; j < 6; ++j) t += Om[i * 6 + j] * er[j];
+    s += er[i] * t;
+  }
+  return s;
+}
+
 void compute_active_errors(orc_problem* p) {
   // SparseOptimizer::computeActiveErrors (sparse_optimizer.cpp:78-105)
   const int n = (int)p->act.size();
 #pragma omp parallel for schedule(static) num_threads(g_threads)
   for (int k = 0; k < n; ++k) compute_edge_error(p, p->act[k], p->err.data() + (size_t)k * p->D);
+  // EdgeSE3Expmap::computeError (g2o/types/sba/edge_se3_expmap.cpp:48-54)
+  for (size_t k = 0; k < p->pact.size(); ++k) {
+    const int e = p->pact[k];
+    se3exp_error(pose_ptr(p, p->pev[2 * e]), pose_ptr(p, p->pev[2 * e + 1]), p->pmeas.data() + (size_t)e * 7,
+                 p->perr.data() + k * 6);
+  }
 }
 
 void active_chi2(orc_problem* p, double* chi2, double* robust) {
@@ -1115,6 +1140,18 @@ void active_chi2(orc_problem* p, double* chi2, double* robust) {
     if (!p->delta.empty() && p->delta[e] > 0) {
       double rho[3];
       huber(v, p->delta[e], rho);
+      r += rho[0];
+    } else {
+      r += v;
+    }
+  }
+  for (size_t k = 0; k < p->pact.size(); ++k) {
+    const int e = p->pact[k];
+    const double v = pose_edge_chi2(p, e, p->perr.data() + k * 6);
+    c += v;
+    if (!p->pdelta.empty() && p->pdelta[e] > 0) {
+      double rho[3];
+      huber(v, p->pdelta[e], rho);
       r += rho[0];
     } else {
       r += v;
@@ -1145,6 +1182,14 @@ int build_structure(orc_problem* p) {
     if (ba) { qa[v0] = 1; pa[v1] = 1; }
     else { pa[v0] = 1; pa[v1] = 1; }
   }
+  p->pact.clear();
+  for (int e = 0; e < p->PE; ++e) {
+    const int v0 = p->pev[2 * e], v1 = p->pev[2 * e + 1];
+    if (p->pose_fixed[v0] && p->pose_fixed[v1]) continue;
+    p->pact.push_back(e);
+    pa[v0] = 1;
+    pa[v1] = 1;
+  }
   if (p->act.empty()) return G2OC_ERR_BAD_GRAPH;
   // buildIndexMapping (sparse_optimizer.cpp:175-200): free non-marginalized, then marginalized
   p->pose_h.assign(p->C, -1);
@@ -1172,6 +1217,13 @@ int build_structure(orc_problem* p) {
         if (a > c) std::swap(a, c);
         hpp_set.insert({c, a});
       }
+    }
+  }
+  for (int e : p->pact) {
+    int a = p->pose_h[p->pev[2 * e]], c = p->pose_h[p->pev[2 * e + 1]];
+    if (a >= 0 && c >= 0) {
+      if (a > c) std::swap(a, c);
+      hpp_set.insert({c, a});
     }
   }
   p->hpp_rc.clear();
@@ -1214,6 +1266,22 @@ int build_structure(orc_problem* p) {
       }
     }
   }
+  const int npa = (int)p->pact.size();
+  p->pe_diag0.assign(npa, -1);
+  p->pe_diag1.assign(npa, -1);
+  p->pe_off.assign(npa, -1);
+  p->pe_trans.assign(npa, 0);
+  for (int k = 0; k < npa; ++k) {
+    const int e = p->pact[k];
+    const int a = p->pose_h[p->pev[2 * e]], c = p->pose_h[p->pev[2 * e + 1]];
+    if (a >= 0) p->pe_diag0[k] = p->hpp_diag_idx[a];
+    if (c >= 0) p->pe_diag1[k] = p->hpp_diag_idx[c];
+    if (a >= 0 && c >= 0) {
+      p->pe_trans[k] = a > c;
+      p->pe_off[k] = hpp_idx[{std::min(a, c), std::max(a, c)}];
+    }
+  }
+  p->perr.assign((size_t)npa * 6, 0.0);
   // Schur pattern = Hpp pattern + co-observing pose pairs (block_solver.hpp:229-266)
   p->schur_rc.clear();
   p->schur_map.clear();
@@ -1349,6 +1417,39 @@ void build_system(orc_problem* p) {
     if (free1) {
       add_Atw(A1, d1, we, D, b1);
       add_AtOB(A1, d1, Om, A1, d1, D, H11, false);
+    }
+  }
+  // the pose edges (EdgeSE3Expmap::linearizeOplus, edge_se3_expmap.cpp:56-68),
+  // as the generic binary-edge branch above
+  for (size_t k = 0; k < p->pact.size(); ++k) {
+    const int e = p->pact[k];
+    const int v0 = p->pev[2 * e], v1 = p->pev[2 * e + 1];
+    double J0[36], J1[36];
+    se3exp_jacobians(pose_ptr(p, v0), pose_ptr(p, v1), p->pmeas.data() + (size_t)e * 7, J0, J1);
+    const double* er = p->perr.data() + k * 6;
+    const double* I = p->pinfo.data() + (size_t)e * 36;
+    double w = 1.0;
+    if (!p->pdelta.empty() && p->pdelta[e] > 0) {
+      double rho[3];
+      huber(pose_edge_chi2(p, e, er), p->pdelta[e], rho);
+      w = rho[1];
+    }
+    double Om[36], we[6];
+    for (int i = 0; i < 6; ++i) {
+      double t = 0;
+      for (int j = 0; j < 6; ++j) t += I[i * 6 + j] * er[j];
+      we[i] = -t * w;
+    }
+    for (int i = 0; i < 36; ++i) Om[i] = w * I[i];
+    const int a = p->pose_h[v0], c = p->pose_h[v1];
+    if (a >= 0) {
+      add_Atw(J0, 6, we, 6, p->b.data() + (size_t)a * 6);
+      add_AtOB(J0, 6, Om, J0, 6, 6, p->hpp.data() + (size_t)p->pe_diag0[k] * 36, false);
+      if (c >= 0) add_AtOB(J0, 6, Om, J1, 6, 6, p->hpp.data() + (size_t)p->pe_off[k] * 36, p->pe_trans[k]);
+    }
+    if (c >= 0) {
+      add_Atw(J1, 6, we, 6, p->b.data() + (size_t)c * 6);
+      add_AtOB(J1, 6, Om, J1, 6, 6, p->hpp.data() + (size_t)p->pe_diag1[k] * 36, false);
     }
   }
   p->system_built = true;
@@ -1934,6 +2035,26 @@ int orc_create(const g2oc_graph* g, orc_problem** out) {
       return G2OC_ERR_BAD_GRAPH;
     }
   }
+  if (g->num_pose_edges > 0) {
+    // the pose edge set: EdgeSE3Expmap between the cameras of an SE3 projection graph
+    if (!ba || bal || p->pose_type != G2OC_POSE_SE3EXPMAP || !g->pose_edge_vertex || !g->pose_edge_measurement ||
+        !g->pose_edge_information) {
+      delete p;
+      return G2OC_ERR_BAD_GRAPH;
+    }
+    p->PE = g->num_pose_edges;
+    p->pev.assign(g->pose_edge_vertex, g->pose_edge_vertex + 2 * (size_t)p->PE);
+    for (int e = 0; e < p->PE; ++e) {
+      const int v0 = p->pev[2 * e], v1 = p->pev[2 * e + 1];
+      if (v0 < 0 || v0 >= p->C || v1 < 0 || v1 >= p->C || v0 == v1) {
+        delete p;
+        return G2OC_ERR_BAD_GRAPH;
+      }
+    }
+    p->pmeas.assign(g->pose_edge_measurement, g->pose_edge_measurement + (size_t)p->PE * 7);
+    p->pinfo.assign(g->pose_edge_information, g->pose_edge_information + (size_t)p->PE * 36);
+    if (g->pose_edge_robust_delta) p->pdelta.assign(g->pose_edge_robust_delta, g->pose_edge_robust_delta + p->PE);
+  }
   p->meas.assign(g->measurement, g->measurement + (size_t)p->E * p->md);
   p->info.assign(g->information, g->information + (size_t)p->E * p->D * p->D);
   if (g->robust_delta) p->delta.assign(g->robust_delta, g->robust_delta + p->E);
@@ -1982,6 +2103,7 @@ int orc_get_hessian_info(orc_problem* p, g2oc_hessian_info* info) {
     np += m * (m - 1) / 2;
   }
   info->schur_pairs = np;
+  info->num_active_pose_edges = (int)p->pact.size();
   return G2OC_OK;
 }
 
@@ -2010,6 +2132,7 @@ int orc_errors(orc_problem* p, double* out) {
   if (!p || !out) return G2OC_ERR_INVALID_ARGUMENT;
   compute_active_errors(p);
   std::memcpy(out, p->err.data(), p->err.size() * sizeof(double));
+  if (!p->perr.empty()) std::memcpy(out + p->err.size(), p->perr.data(), p->perr.size() * sizeof(double));
   return G2OC_OK;
 }
 

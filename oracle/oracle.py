@@ -137,10 +137,14 @@ class OracleProblem:
         _check(lib().orc_chi2(self._h, C.byref(a), C.byref(b)), "chi2")
         return a.value, b.value
 
-    def errors(self):
-        e = np.empty((self.info.num_active_edges, self.graph.edge_dim))
-        _check(lib().orc_errors(self._h, _p(e)), "errors")
-        return e
+    def errors(self, with_pose_edges=False):
+        """Per active edge errors; with_pose_edges: also those of the pose
+        edge set (they follow the projection edges' in the output)."""
+        n, D, npe = self.info.num_active_edges, self.graph.edge_dim, self.info.num_active_pose_edges
+        buf = np.empty(n * D + npe * 6)
+        _check(lib().orc_errors(self._h, _p(buf)), "errors")
+        e = buf[: n * D].reshape(n, D)
+        return (e, buf[n * D:].reshape(npe, 6)) if with_pose_edges else e
 
     def _jac_shapes(self):
         D = self.graph.edge_dim

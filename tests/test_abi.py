@@ -64,7 +64,7 @@ def test_library_exports_every_declared_symbol(cuda_lib):
     assert len(names) >= 20
     for n in names:
         assert hasattr(cuda_lib, n), n
-    assert cuda_lib.g2oc_abi_version() == 4
+    assert cuda_lib.g2oc_abi_version() == 5
 
 
 def test_factory_lists_and_constructs():

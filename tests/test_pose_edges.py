@@ -1,0 +1,191 @@
+"""Graphs that mix edge types: projection edges (EdgeProjectXYZ2UV between
+VertexPointXYZ and VertexSE3Expmap) with a second edge set of EdgeSE3Expmap
+between the cameras (g2oc_graph.pose_edge_*), assembled into one
+BlockSolver system as g2o's BlockSolver::buildSystem does for any mix of
+binary edges (g2o/core/block_solver.hpp:492-565): the pose-pose blocks join
+Hpp and the Schur complement.
+
+CPU: the oracle's pose-edge errors are those of the same edges as a pure
+EdgeSE3Expmap pose graph (pinned by the pose-graph fixtures), and its Hessian
+of the mixed graph is the sum of the two edge sets' Hessians.
+
+GPU, through the C-ABI, against the oracle on a 40-camera / 3,000-point ring
+with odometry between consecutive cameras: errors of both edge sets 1e-12,
+chi2, Hessian blocks (the pose-pose blocks in the column-major pattern),
+gradient and Schur complement 1e-10; 10-iteration trajectories with LM + PCG,
+LM + Cholesky and Gauss-Newton (same trials, chi2 within 1e-6 while the PCG
+iteration counts agree; the Cholesky trajectory throughout); the
+mixed-precision form without refinement reaches the oracle's chi2; the
+combinations built for one edge set only are refused.
+"""
+import numpy as np
+import pytest
+
+from g2o_b200 import synth
+from g2o_b200.abi import (ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, EDGE_SE3_EXPMAP, LINEAR_CHOLESKY, LINEAR_PCG,
+                          POSE_SE3EXPMAP, PREC_MIXED, Graph)
+
+
+@pytest.fixture(scope="module")
+def graph():
+    g = synth.ba_with_odometry(num_cameras=40, num_points=3000)
+    assert g.num_pose_edges == 40
+    return g
+
+
+def pose_graph_of(g):
+    return Graph(POSE_SE3EXPMAP, EDGE_SE3_EXPMAP, g.pose_estimate, g.pose_edge_vertex, g.pose_edge_measurement,
+                 g.pose_edge_information, pose_fixed=g.pose_fixed)
+
+
+def projection_graph_of(g):
+    h = g.copy()
+    h.pose_edge_vertex = h.pose_edge_measurement = h.pose_edge_information = h.pose_edge_robust_delta = None
+    return h
+
+
+def test_oracle_pose_edge_errors_are_the_pose_graph_errors(oracle_lib, graph):
+    e, pe = oracle_lib.OracleProblem(graph).errors(with_pose_edges=True)
+    # edge (0, 1) joins two fixed cameras: not active
+    pg = oracle_lib.OracleProblem(pose_graph_of(graph)).errors()
+    np.testing.assert_array_equal(pe, pg)
+    np.testing.assert_array_equal(e, oracle_lib.OracleProblem(projection_graph_of(graph)).errors())
+
+
+def test_oracle_hessian_is_the_sum_of_the_edge_sets(oracle_lib, graph):
+    m = oracle_lib.OracleProblem(graph)
+    m.build_system()
+    hpp, hll, hpl, b = m.hessian()
+    rc = m.pattern()[0]
+    p = oracle_lib.OracleProblem(projection_graph_of(graph))
+    p.build_system()
+    hpp_p, hll_p, hpl_p, b_p = p.hessian()
+    q = oracle_lib.OracleProblem(pose_graph_of(graph))
+    q.build_system()
+    hpp_q, _, _, b_q = q.hessian()
+    rc_q = q.pattern()[0]
+    # the pose graph's pattern is the mixed graph's (every camera is free in both)
+    want = {tuple(x): v.copy() for x, v in zip(rc_q, hpp_q)}
+    for h in range(m.info.num_free_poses):
+        want[(h, h)] = want.get((h, h), 0) + hpp_p[h]
+    got = {tuple(x): v for x, v in zip(rc, hpp)}
+    assert set(got) == set(want)
+    for k in got:
+        np.testing.assert_allclose(got[k], want[k], rtol=1e-12, atol=1e-9 * np.abs(want[k]).max())
+    np.testing.assert_array_equal(hll, hll_p)
+    np.testing.assert_array_equal(hpl, hpl_p)
+    n = m.info.num_free_poses * 6
+    np.testing.assert_allclose(b[:n], b_p[:n] + b_q, rtol=1e-12, atol=1e-9 * np.abs(b_q).max())
+
+
+def test_oracle_lm_decreases_chi2(oracle_lib, graph):
+    o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(), threads=4)
+    _, st = o.optimize(10)
+    assert all(b["chi2"] <= a["chi2"] for a, b in zip(st, st[1:]))
+
+
+# ---------------------------------------------------------------- GPU
+@pytest.fixture(scope="module")
+def backend():
+    from g2o_b200 import backend as B
+    B.library()
+    return B
+
+
+def rel_block_err(a, b):
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return float((np.abs(a - b).max(axis=1) / scale).max())
+
+
+def relnorm(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.gpu
+def test_mixed_graph_errors_hessian_schur(backend, oracle_lib, graph):
+    o = oracle_lib.OracleProblem(graph, oracle_lib.default_params())
+    c = backend.CudaProblem(graph, backend.default_params())
+    assert c.info.num_active_pose_edges == o.info.num_active_pose_edges == 39
+    (ec, pc), (eo, po) = c.errors(with_pose_edges=True), o.errors(with_pose_edges=True)
+    assert relnorm(ec, eo) < 1e-12 and relnorm(pc, po) < 1e-12
+    (a, b), (x, y) = c.chi2(), o.chi2()
+    assert abs(a - x) <= 1e-12 * x and abs(b - y) <= 1e-12 * y
+    for u, v in zip(c.pattern(), o.pattern()):
+        np.testing.assert_array_equal(u, v)
+    o.build_system()
+    c.build_system()
+    hc, ho = c.hessian(), o.hessian()
+    for u, v in zip(hc[:3], ho[:3]):
+        assert rel_block_err(u, v) < 1e-10
+    n = o.info.num_free_poses * 6
+    assert rel_block_err(hc[3][:n].reshape(-1, 6), ho[3][:n].reshape(-1, 6)) < 1e-10
+    assert relnorm(hc[3][n:], ho[3][n:]) < 1e-10
+    for lam in (1e-3, 10.0):
+        Sc, bsc = c.schur(lam)
+        So, bso = o.schur(lam)
+        assert rel_block_err(Sc, So) < 1e-10 and relnorm(bsc, bso) < 1e-10
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algo,linear", [(ALGO_LEVENBERG, LINEAR_PCG), (ALGO_LEVENBERG, LINEAR_CHOLESKY),
+                                         (ALGO_GAUSS_NEWTON, LINEAR_PCG)])
+def test_mixed_graph_trajectory(backend, oracle_lib, graph, algo, linear):
+    prm = {"algorithm": algo, "linear_solver": linear}
+    o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(**prm), threads=4)
+    c = backend.CudaProblem(graph, backend.default_params(**prm))
+    do, so = o.optimize(10)
+    dc, sc = c.optimize(10)
+    c.close()
+    assert do == dc
+    # The stiff odometry blocks make the PCG's stopping iteration sensitive
+    # to rounding: the two trajectories agree (same trials, chi2 1e-6) while
+    # their PCG iteration counts do; once a count differs the steps differ at
+    # the tolerance's level and the trajectories stay within 1e-2, ending
+    # within 1e-3 of each other.
+    same = True
+    for a, b in zip(sc, so):
+        same = same and a["iterations_linear_solver"] == b["iterations_linear_solver"]
+        if same:
+            assert a["levenberg_iterations"] == b["levenberg_iterations"], (a["iteration"], a, b)
+            assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
+        else:
+            assert abs(a["chi2"] - b["chi2"]) <= 1e-2 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
+    if linear == LINEAR_CHOLESKY:
+        assert same
+    assert abs(sc[-1]["chi2"] - so[-1]["chi2"]) <= 1e-3 * so[-1]["chi2"], (sc[-1]["chi2"], so[-1]["chi2"])
+
+
+@pytest.mark.gpu
+def test_mixed_graph_fp32_steps_reach_oracle_chi2(backend, oracle_lib, graph):
+    o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(), threads=4)
+    _, so = o.optimize(20)
+    target = so[-1]["chi2"]
+    m = backend.CudaProblem(graph, backend.OptimizationAlgorithmFactory.instance().construct("lm_cuda_mixed_fast"))
+    _, sm = m.optimize(30)
+    m.close()
+    assert min(s["chi2"] for s in sm) <= target * (1 + 1e-6), (min(s["chi2"] for s in sm), target)
+
+
+@pytest.mark.gpu
+def test_mixed_graph_refusals(backend, graph):
+    fac = backend.OptimizationAlgorithmFactory.instance()
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(graph, fac.construct("lm_cuda_mixed"))  # FP64 refinement of every step
+    assert e.value.status == 10
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(graph, fac.construct("dl_cuda"))
+    assert e.value.status == 10
+    c = backend.CudaProblem(graph, backend.default_params())
+    with pytest.raises(backend.G2ocError) as e:
+        c.backward(np.zeros((graph.num_poses, 6)), np.zeros((graph.num_points, 3)))
+    assert e.value.status == 10
+    c.close()
+    # every landmark fixed: the pose-pose blocks have no Schur complement to join
+    g = graph.copy()
+    g.point_fixed = np.ones(g.num_points, np.uint8)
+    with pytest.raises(backend.G2ocError) as e:
+        backend.CudaProblem(g, backend.default_params())
+    assert e.value.status == 10
