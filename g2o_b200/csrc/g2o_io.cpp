@@ -220,6 +220,9 @@ struct g2oc_file {
   std::vector<double> pose_est, point_est, meas, infm, delta;
   std::vector<uint8_t> pose_fixed, point_fixed;
   std::vector<int32_t> ev;
+  // EDGE_SE3:EXPMAP edges beside projection edges: the graph's pose edge set
+  std::vector<int32_t> pev;
+  std::vector<double> pmeas, pinfm, pdelta;
   int32_t pose_type = 0, edge_type = 0;
   double focal = 1.0, pp[2] = {0.0, 0.0};
 
@@ -442,11 +445,16 @@ void g2oc_file::parse(const char* text, size_t size) {
 int g2oc_file::build_view() {
   if (view_valid) return G2OC_OK;
   int et = 0;
+  bool with_pose_edges = false;  // projection edges plus EDGE_SE3:EXPMAP: the latter are the pose edge set
   for (const Edg& e : edg) {
-    if (et == 0) et = e.kind;
-    else if (et != e.kind) {
-      set_error("the graph mixes %s and %s edges; the device path optimizes one edge type", kEdgeTag[et],
-                kEdgeTag[e.kind]);
+    if (et == 0 || et == e.kind) {
+      et = e.kind;
+    } else if ((et == eProj && e.kind == eSE3Exp) || (et == eSE3Exp && e.kind == eProj)) {
+      et = eProj;
+      with_pose_edges = true;
+    } else {
+      set_error("the graph mixes %s and %s edges; the device path takes projection edges with EDGE_SE3:EXPMAP "
+                "edges, or one edge type", kEdgeTag[et], kEdgeTag[e.kind]);
       return G2OC_ERR_NOT_SUPPORTED;
     }
   }
@@ -457,8 +465,11 @@ int g2oc_file::build_view() {
   const int pk = et == eSE2 ? kSE2 : et == eSE3 ? kSE3 : kExpmap;  // projection and SE3Expmap edges: VertexSE3Expmap
   focal = 1.0; pp[0] = pp[1] = 0.0;
   if (et == eProj) {
-    const Cam& c0 = params.at(edg[0].param);
+    int first = 0;
+    while (edg[first].kind != eProj) ++first;
+    const Cam& c0 = params.at(edg[first].param);
     for (const Edg& e : edg) {
+      if (e.kind != eProj) continue;
       const Cam& c = params.at(e.param);
       if (c.f != c0.f || c.cx != c0.cx || c.cy != c0.cy) {
         set_error("projection edges refer to CameraParameters %d and %d, which differ", edg[0].param, e.param);
@@ -495,21 +506,44 @@ int g2oc_file::build_view() {
     point_fixed[i] = v.fixed;
   }
   const int M = meas_dim(et), D = err_dim(et);
-  const size_t E = edg.size();
+  size_t E = 0, PE = 0;
+  bool robust = false, probust = false;
+  for (const Edg& e : edg) {
+    if (e.kind == et) {
+      ++E;
+      robust |= e.delta > 0;
+    } else {
+      ++PE;
+      probust |= e.delta > 0;
+    }
+  }
   ev.resize(2 * E);
   meas.resize(E * M);
   infm.resize(E * D * D);
-  bool robust = false;
-  for (const Edg& e : edg) robust |= e.delta > 0;
   delta.assign(robust ? E : 0, 0.0);
-  for (size_t k = 0; k < E; ++k) {
-    const Edg& e = edg[k];
-    ev[2 * k] = vtx[e.v0].view;
-    ev[2 * k + 1] = vtx[e.v1].view;
-    std::memcpy(&meas[k * M], &edata[e.off], sizeof(double) * M);
-    std::memcpy(&infm[k * D * D], &edata[e.off + M], sizeof(double) * D * D);
-    if (robust) delta[k] = e.delta;
+  pev.resize(2 * PE);
+  pmeas.resize(PE * 7);
+  pinfm.resize(PE * 36);
+  pdelta.assign(probust ? PE : 0, 0.0);
+  size_t k = 0, q = 0;
+  for (const Edg& e : edg) {
+    if (e.kind == et) {
+      ev[2 * k] = vtx[e.v0].view;
+      ev[2 * k + 1] = vtx[e.v1].view;
+      std::memcpy(&meas[k * M], &edata[e.off], sizeof(double) * M);
+      std::memcpy(&infm[k * D * D], &edata[e.off + M], sizeof(double) * D * D);
+      if (robust) delta[k] = e.delta;
+      ++k;
+    } else {
+      pev[2 * q] = vtx[e.v0].view;
+      pev[2 * q + 1] = vtx[e.v1].view;
+      std::memcpy(&pmeas[q * 7], &edata[e.off], sizeof(double) * 7);
+      std::memcpy(&pinfm[q * 36], &edata[e.off + 7], sizeof(double) * 36);
+      if (probust) pdelta[q] = e.delta;
+      ++q;
+    }
   }
+  (void)with_pose_edges;
   pose_type = pk == kSE2 ? G2OC_POSE_SE2 : pk == kSE3 ? G2OC_POSE_SE3 : G2OC_POSE_SE3EXPMAP;
   edge_type = et;
   view_valid = true;
@@ -743,6 +777,28 @@ int g2oc_file_from_graph(const g2oc_graph* g, const int32_t* pose_ids, const int
     f->edata.insert(f->edata.end(), g->information + (size_t)k * D * D, g->information + (size_t)(k + 1) * D * D);
     f->edg.push_back(e);
   }
+  if (g->num_pose_edges > 0 && ek == eProj) {  // the pose edge set as EDGE_SE3:EXPMAP records
+    if (!g->pose_edge_vertex || !g->pose_edge_measurement || !g->pose_edge_information) {
+      delete f;
+      set_error("g2oc_file_from_graph: pose edge array is NULL");
+      return G2OC_ERR_INVALID_ARGUMENT;
+    }
+    for (int32_t k = 0; k < g->num_pose_edges; ++k) {
+      const int32_t a = g->pose_edge_vertex[2 * k], b = g->pose_edge_vertex[2 * k + 1];
+      if (a < 0 || a >= g->num_poses || b < 0 || b >= g->num_poses || a == b) {
+        delete f;
+        set_error("g2oc_file_from_graph: pose edge %d has a vertex index out of range", k);
+        return G2OC_ERR_INVALID_ARGUMENT;
+      }
+      Edg e{(int8_t)eSE3Exp, prec[a], prec[b], -1, (int64_t)f->edata.size(),
+            g->pose_edge_robust_delta ? g->pose_edge_robust_delta[k] : 0.0};
+      f->edata.insert(f->edata.end(), g->pose_edge_measurement + (size_t)k * 7,
+                      g->pose_edge_measurement + (size_t)(k + 1) * 7);
+      f->edata.insert(f->edata.end(), g->pose_edge_information + (size_t)k * 36,
+                      g->pose_edge_information + (size_t)(k + 1) * 36);
+      f->edg.push_back(e);
+    }
+  }
   f->info.num_vertices = (int32_t)f->vtx.size();
   f->info.num_edges = (int32_t)f->edg.size();
   f->info.num_parameters = (int32_t)f->params.size();
@@ -781,8 +837,15 @@ int g2oc_file_graph(g2oc_file* f, g2oc_graph* out) {
   g.point_estimate = g.num_points ? f->point_est.data() : nullptr;
   g.point_fixed = g.num_points ? f->point_fixed.data() : nullptr;
   g.edge_type = f->edge_type;
-  g.num_edges = (int32_t)f->edg.size();
+  g.num_edges = (int32_t)(f->ev.size() / 2);
   g.edge_vertex = f->ev.data();
+  g.num_pose_edges = (int32_t)(f->pev.size() / 2);
+  if (g.num_pose_edges > 0) {
+    g.pose_edge_vertex = f->pev.data();
+    g.pose_edge_measurement = f->pmeas.data();
+    g.pose_edge_information = f->pinfm.data();
+    g.pose_edge_robust_delta = f->pdelta.empty() ? nullptr : f->pdelta.data();
+  }
   g.measurement = f->meas.data();
   g.information = f->infm.data();
   g.robust_delta = f->delta.empty() ? nullptr : f->delta.data();

@@ -98,6 +98,13 @@ class G2oFile:
         if N:
             kw = dict(point_estimate=arr(g.point_estimate, N * 3, (N, 3)),
                       point_fixed=arr(g.point_fixed, N, (N,), np.uint8))
+        Q = g.num_pose_edges
+        if Q:  # EDGE_SE3:EXPMAP edges beside projection edges: the pose edge set
+            kw.update(pose_edge_vertex=arr(g.pose_edge_vertex, 2 * Q, (Q, 2), np.int32),
+                      pose_edge_measurement=arr(g.pose_edge_measurement, Q * 7, (Q, 7)),
+                      pose_edge_information=arr(g.pose_edge_information, Q * 36, (Q, 36)),
+                      pose_edge_robust_delta=arr(g.pose_edge_robust_delta, Q, (Q,))
+                      if g.pose_edge_robust_delta else None)
         return Graph(g.pose_type, g.edge_type, arr(g.pose_estimate, P * pd, (P, pd)),
                      arr(g.edge_vertex, 2 * E, (E, 2), np.int32), arr(g.measurement, E * M, (E, M)),
                      arr(g.information, E * D * D, (E, D * D)), pose_fixed=arr(g.pose_fixed, P, (P,), np.uint8),

@@ -197,3 +197,21 @@ def test_mixed_graph_refusals(backend, graph):
     with pytest.raises(backend.G2ocError) as e:
         backend.CudaProblem(g, backend.default_params())
     assert e.value.status == 10
+
+
+def test_g2o_file_round_trip_keeps_the_pose_edge_set(tmp_path):
+    """EDGE_SE3:EXPMAP records beside EDGE_PROJECT_XYZ2UV:EXPMAP ones load as the
+    pose edge set (the saver writes the set as such records)."""
+    from g2o_b200.g2ofile import G2oFile
+    g = synth.ba_with_odometry(num_cameras=12, num_points=400)
+    p = str(tmp_path / "mixed.g2o")
+    G2oFile.from_graph(g).save(p)
+    text = open(p).read()
+    assert text.count("EDGE_SE3:EXPMAP") == g.num_pose_edges
+    h = G2oFile.load(p).graph()
+    assert (h.num_edges, h.num_pose_edges) == (g.num_edges, g.num_pose_edges)
+    np.testing.assert_array_equal(h.edge_vertex, g.edge_vertex)
+    np.testing.assert_array_equal(h.pose_edge_vertex, g.pose_edge_vertex)
+    # the text holds g2o's default stream precision (6 significant digits)
+    np.testing.assert_allclose(h.pose_edge_measurement, g.pose_edge_measurement, rtol=1e-5, atol=1e-4)
+    np.testing.assert_allclose(h.pose_edge_information, g.pose_edge_information, rtol=1e-5)
