@@ -430,11 +430,12 @@ __global__ void __launch_bounds__(THREADS) bal_camera_pass(BACamEdges CE, BAVert
 // a CTA per chunk summing its 45 + 9 values as bal_camera_pass does into
 // `cpart`; bal_camera_reduce adds each camera's chunk sums in chunk order and
 // writes the full 9 x 9 block and b_p. More CTAs than cameras keep the SMs
-// busy (a 356-camera problem has ~3,600 edges per camera).
+// busy (a 356-camera problem has ~3,600 edges per camera). Bounded to three
+// CTAs per SM (168 registers, a few spilled): 97 us against 113 us at two.
 constexpr int kBalCamChunk = 512;
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 3)
     bal_camera_chunks(BACamEdges CE, BAVertices V, const int4* cch, double* cpart) {
   constexpr int WARPS = THREADS / 32;
   __shared__ double red[WARPS][54];
