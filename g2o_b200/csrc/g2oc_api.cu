@@ -959,6 +959,24 @@ struct Engine final : EngineBase {
     return G2OC_OK;
   }
 
+  // the pose edge set's part of the FP64 residual of the refinement:
+  // r_p -= (J^T Om' J x)_p over the pose edges, matrix-free in FP64
+  // (pg_hx_contrib), summed per camera in edge order
+  int pose_edge_resid(double* rp) {
+    const Structure& S = c->S;
+    cudaStream_t st = c->stream;
+    const int npa = (int)S.pact.size();
+    G2OC_K(K_RESID_CAM) ba_unpack_poses<<<cdiv((long long)S.C * 7, 256), 256, 0, st>>>(S.C, c->pose.p,
+                                                                                     c->pgpose.p);
+    G2OC_K(K_RESID_CAM) pg_hx_contrib<G2OC_POSE_SE3EXPMAP><<<cdiv(npa, 64), 64, 0, st>>>(
+        c->pgpose.p, c->ba_pose_edges(), c->pose_h.p, c->x.p, bcontrib.p);
+    G2OC_K(K_RESID_CAM) pg_assemble_b<6><<<cdiv((long long)S.Cf * 6, 128), 128, 0, st>>>(
+        S.Cf, c->bv_src_ptr.p, c->bv_src.p, bcontrib.p, pb.p);
+    G2OC_K(K_RESID_CAM) axpy_kernel<<<cdiv((long long)S.Cf * 6, 256), 256, 0, st>>>(rp, pb.p, -1.0, S.Cf * 6);
+    G2OC_LAUNCH_CHECK();
+    return G2OC_OK;
+  }
+
   int multiply_hessian(const double* src, double* dst) override {
     const Structure& S = c->S;
     cudaStream_t st = c->stream;
@@ -1345,6 +1363,7 @@ struct Engine final : EngineBase {
                                                                              lambda, bp, c->x.p,
                                                                              c->x.p + (size_t)S.Cf * 6, rp);
           G2OC_LAUNCH_CHECK();
+          if (c->pose_edges()) G2OC_TRY(pose_edge_resid(rp));
           G2OC_TRY(schur_rhs_from(rp, rl, c->rhs.p));
           double check = 0.0, bound = 0.0;
           if (tc_chol) {
@@ -2543,11 +2562,8 @@ void g2oc_destroy(g2oc_ctx* c) {
 }
 
 static int make_engine(g2oc_ctx* c) {
-  if (c->pose_edges() &&
-      (c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY ||
-       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0))) {
-    set_error("a graph with a pose edge set runs Gauss-Newton or Levenberg-Marquardt in FP64 or mixed precision "
-              "without FP64 refinement (*_mixed_fast)");
+  if (c->pose_edges() && (c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY)) {
+    set_error("a graph with a pose edge set runs Gauss-Newton or Levenberg-Marquardt");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   if (c->S.bal) {

@@ -537,7 +537,16 @@ def ba_with_odometry(num_cameras=40, num_points=3000, rot_sigma=0.01, trans_sigm
     (omega, upsilon) order and no robust kernel: the graph of a visual SLAM
     back end with odometry."""
     g = bundle_adjustment(num_cameras=num_cameras, num_points=num_points, seed=seed, **kw)
-    rng = np.random.default_rng(seed + 15485863)
+    add_odometry(g, rot_sigma, trans_sigma, seed + 15485863)
+    g.name = g.name.replace("bundle_adjustment", "ba_odometry")
+    return g
+
+
+def add_odometry(g, rot_sigma=0.01, trans_sigma=0.05, seed=SEED_BASE + 7 + 15485863):
+    """Attach the ring odometry of ba_with_odometry to a projection-edge graph
+    whose extra["truth_pose"] holds its generating SE3Quat cameras."""
+    num_cameras = g.num_poses
+    rng = np.random.default_rng(seed)
     tp = g.extra["truth_pose"]
     R = _quat_to_rot(tp[:, 3:7])
     t = tp[:, :3]
@@ -555,7 +564,6 @@ def ba_with_odometry(num_cameras=40, num_points=3000, rot_sigma=0.01, trans_sigm
     g.pose_edge_measurement = np.concatenate([tc, _rot_to_quat(Rc)], axis=1)
     g.pose_edge_information = np.tile(info, (num_cameras, 1))
     g.pose_edge_robust_delta = None
-    g.name = g.name.replace("bundle_adjustment", "ba_odometry")
     return g
 
 

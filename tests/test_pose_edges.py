@@ -15,7 +15,9 @@ chi2, Hessian blocks (the pose-pose blocks in the column-major pattern),
 gradient and Schur complement 1e-10; 10-iteration trajectories with LM + PCG
 (converged solves) and LM + Cholesky (same trials, chi2 within 1e-6); LM +
 PCG at the default tolerance descends to the oracle's chi2 within 1e-2; the
-mixed-precision form without refinement reaches the oracle's chi2; the
+mixed-precision forms (with and without FP64 refinement, and the
+tensor-core Cholesky) reach the oracle's chi2; a stereo graph with pose
+edges follows the oracle's LM + Cholesky trajectory; the
 combinations built for one edge set only are refused.
 """
 import numpy as np
@@ -167,22 +169,40 @@ def test_mixed_graph_default_pcg_descends(backend, oracle_lib, graph):
 
 
 @pytest.mark.gpu
-def test_mixed_graph_fp32_steps_reach_oracle_chi2(backend, oracle_lib, graph):
+@pytest.mark.parametrize("solver", ["lm_cuda_mixed_fast", "lm_cuda_mixed", "lm_cuda_chol_mixed"])
+def test_mixed_graph_fp32_forms_reach_oracle_chi2(backend, oracle_lib, graph, solver):
+    """FP32 steps under FP64 LM control, with and without the FP64 refinement
+    (whose matrix-free residual carries the pose edges), and the tensor-core
+    Cholesky of the reduced system with the pose-pose blocks in its tiles."""
     o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(), threads=4)
     _, so = o.optimize(20)
     target = so[-1]["chi2"]
-    m = backend.CudaProblem(graph, backend.OptimizationAlgorithmFactory.instance().construct("lm_cuda_mixed_fast"))
+    m = backend.CudaProblem(graph, backend.OptimizationAlgorithmFactory.instance().construct(solver))
     _, sm = m.optimize(30)
     m.close()
-    assert min(s["chi2"] for s in sm) <= target * (1 + 1e-6), (min(s["chi2"] for s in sm), target)
+    assert min(s["chi2"] for s in sm) <= target * (1 + 1e-6), (solver, min(s["chi2"] for s in sm), target)
+
+
+@pytest.mark.gpu
+def test_stereo_graph_with_pose_edges(backend, oracle_lib):
+    """The pose edge set beside EdgeStereoSE3ProjectXYZ edges (their own
+    linearize passes, the shared Schur and solvers): LM + Cholesky against the
+    oracle, same trials, chi2 within 1e-6."""
+    g = synth.add_odometry(synth.stereo_bundle_adjustment(num_cameras=40, num_points=3000, seed=93))
+    prm = {"algorithm": ALGO_LEVENBERG, "linear_solver": LINEAR_CHOLESKY}
+    o = oracle_lib.OracleProblem(g, oracle_lib.default_params(**prm), threads=4)
+    c = backend.CudaProblem(g, backend.default_params(**prm))
+    _, so = o.optimize(10)
+    _, sc = c.optimize(10)
+    c.close()
+    for a, b in zip(sc, so):
+        assert a["levenberg_iterations"] == b["levenberg_iterations"], (a["iteration"], a, b)
+        assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (a["iteration"], a["chi2"], b["chi2"])
 
 
 @pytest.mark.gpu
 def test_mixed_graph_refusals(backend, graph):
     fac = backend.OptimizationAlgorithmFactory.instance()
-    with pytest.raises(backend.G2ocError) as e:
-        backend.CudaProblem(graph, fac.construct("lm_cuda_mixed"))  # FP64 refinement of every step
-    assert e.value.status == 10
     with pytest.raises(backend.G2ocError) as e:
         backend.CudaProblem(graph, fac.construct("dl_cuda"))
     assert e.value.status == 10
