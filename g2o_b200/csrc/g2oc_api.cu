@@ -390,6 +390,8 @@ struct g2oc_ctx {
   // on the pose-graph kernels: the active pose edges, the cameras in the
   // SE3Quat::toVector layout those kernels read (pgpose, unpacked per use)
   g2oc::DBuf<double> pgpose;
+  g2oc::DBuf<int> pp_ptr;    // per camera its pose-pose blocks (the Hpp product)
+  g2oc::DBuf<int4> pp_ent;
   bool pose_edges() const { return !S.pact.empty(); }
   g2oc::PGEdges ba_pose_edges() {
     g2oc::PGEdges E;
@@ -982,15 +984,17 @@ struct Engine final : EngineBase {
     cudaStream_t st = c->stream;
     const int n = c->vec_size();
     if (n <= 0) return G2OC_OK;
-    if (c->pose_edges()) {
-      set_error("the Hpp product (Dogleg, g2oc_multiply_hessian) takes no pose edge set");
-      return G2OC_ERR_NOT_SUPPORTED;
-    }
+
     if (S.Cf == 0) {
       G2OC_CUDA_TRY(cudaMemsetAsync(dst, 0, (size_t)n * sizeof(double), st));
       return G2OC_OK;
     }
-    if (S.ba) G2OC_K(K_LM_CONTROL) hpp_mult_diag6<Real><<<cdiv(n, 256), 256, 0, st>>>(S.Cf, hpp.p, src, dst, n);
+    if (S.ba) {
+      G2OC_K(K_LM_CONTROL) hpp_mult_diag6<Real><<<cdiv(n, 256), 256, 0, st>>>(S.Cf, hpp.p, src, dst, n);
+      if (c->pose_edges())
+        G2OC_K(K_LM_CONTROL) hpp_mult_pairs6<Real><<<cdiv(S.Cf * 6, 256), 256, 0, st>>>(
+            S.Cf, c->pp_ptr.p, c->pp_ent.p, hpp.p, src, dst);
+    }
     else if (S.pd == 3) G2OC_K(K_LM_CONTROL) hpp_mult_sym<Real, 3><<<cdiv(S.Cf, 128), 128, 0, st>>>(sys(nullptr), hpp.p, src, dst);
     else G2OC_K(K_LM_CONTROL) hpp_mult_sym<Real, 6><<<cdiv(S.Cf, 128), 128, 0, st>>>(sys(nullptr), hpp.p, src, dst);
     G2OC_LAUNCH_CHECK();
@@ -2562,8 +2566,8 @@ void g2oc_destroy(g2oc_ctx* c) {
 }
 
 static int make_engine(g2oc_ctx* c) {
-  if (c->pose_edges() && (c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY)) {
-    set_error("a graph with a pose edge set runs Gauss-Newton or Levenberg-Marquardt");
+  if (c->pose_edges() && c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY) {
+    set_error("a graph with a pose edge set runs Gauss-Newton, Levenberg-Marquardt or Dogleg");
     return G2OC_ERR_NOT_SUPPORTED;
   }
   if (c->S.bal) {
@@ -2767,6 +2771,11 @@ static int upload_topology(g2oc_ctx* c, const g2oc_graph* g) {
       G2OC_TRY(c->bv_src_ptr.upload(S.bv_src_ptr, st));
       G2OC_TRY(c->bv_src.upload(S.bv_src.empty() ? std::vector<int>{0} : S.bv_src, st));
       G2OC_TRY(c->pgpose.alloc((size_t)S.C * 7));
+      G2OC_TRY(c->pp_ptr.upload(S.pp_ptr, st));
+      std::vector<int4> pe4(S.pp_ent.size() / 4 + 1, make_int4(0, 0, 0, 0));
+      for (size_t q = 0; q < S.pp_ent.size() / 4; ++q)
+        pe4[q] = make_int4(S.pp_ent[4 * q], S.pp_ent[4 * q + 1], S.pp_ent[4 * q + 2], 0);
+      G2OC_TRY(c->pp_ent.upload(pe4, st));
     }
   } else {
     std::vector<int2> ev(na);

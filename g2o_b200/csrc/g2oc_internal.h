@@ -83,6 +83,8 @@ struct Structure {
   std::vector<int> pact;
   int npp = 0;
   std::vector<int> hpp_store;
+  std::vector<int> pp_ptr;    // Cf + 1: per camera its pose-pose blocks in pp_ent
+  std::vector<int> pp_ent;    // 4 per entry: storage block, other camera, transposed, 0
   std::vector<int> act;                 // active edge ids, insertion order
   std::vector<int> pose_h, point_l;     // Hessian index of each pose / landmark index of each point, -1 = none
   std::vector<int> free_pose_of_h;      // pose index of Hessian row h

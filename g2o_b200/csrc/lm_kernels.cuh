@@ -165,4 +165,24 @@ __global__ void hpp_mult_diag6(int nb, const Real* hv, const double* x, double* 
   y[t] = acc;
 }
 
+// y += the pose-pose blocks' part of Hpp x (a pose edge set): per camera row
+// h its pair blocks in order, pp_ptr / pp_ent (storage block, other camera,
+// transposed: the block is (other, h), read as its transpose)
+template <typename Real>
+__global__ void hpp_mult_pairs6(int Cf, const int* pp_ptr, const int4* pp_ent, const Real* hv, const double* x,
+                                double* y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= Cf * 6) return;
+  const int h = t / 6, i = t % 6;
+  double acc = 0.0;
+  for (int q = pp_ptr[h]; q < pp_ptr[h + 1]; ++q) {
+    const int4 en = pp_ent[q];
+    const Real* B = hv + (size_t)en.x * 36;
+    const double* xo = x + (size_t)en.y * 6;
+#pragma unroll
+    for (int b = 0; b < 6; ++b) acc += (double)(en.z ? B[b * 6 + i] : B[i * 6 + b]) * xo[b];
+  }
+  y[t] += acc;
+}
+
 }  // namespace g2oc

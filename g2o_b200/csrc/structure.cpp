@@ -354,6 +354,19 @@ static int build_ba(const g2oc_graph* g, Structure& s) {
       s.hpp_store[i] = cm[i][2];
     }
   }
+  {  // per camera its pose-pose blocks (the Hpp product of Dogleg / g2oc_multiply_hessian)
+    std::vector<std::vector<std::array<int, 3>>> per(s.Cf);
+    for (size_t q = 0; q < pp.size(); ++q) {
+      per[pp[q].first].push_back({s.Cf + (int)q, pp[q].second, 0});
+      per[pp[q].second].push_back({s.Cf + (int)q, pp[q].first, 1});
+    }
+    s.pp_ptr.assign(s.Cf + 1, 0);
+    s.pp_ent.clear();
+    for (int h = 0; h < s.Cf; ++h) {
+      for (const auto& en : per[h]) s.pp_ent.insert(s.pp_ent.end(), {en[0], en[1], en[2], 0});
+      s.pp_ptr[h + 1] = (int)(s.pp_ent.size() / 4);
+    }
+  }
   auto pair_store = [&](int r, int c) -> int {  // storage index of pose-pose block (r < c), or -1
     auto it = std::lower_bound(pp.begin(), pp.end(), std::make_pair(r, c));
     return (it != pp.end() && *it == std::make_pair(r, c)) ? s.Cf + (int)(it - pp.begin()) : -1;
