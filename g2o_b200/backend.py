@@ -521,8 +521,9 @@ def device_tensor(ptr: int, count: int, dtype: int, device: int = 0):
 
 def split_points(g: Graph, parts: int):
     """The shards of a bundle adjustment: every camera, and the points with
-    their edges cut into `parts` contiguous ranges of point index. Returns the
-    sub-graphs and, per part, the original indices of its points."""
+    their edges cut into `parts` contiguous ranges of point index; a pose edge
+    set goes to shard 0 alone. Returns the sub-graphs and, per part, the
+    original indices of its points."""
     bounds = [round(i * g.num_points / parts) for i in range(parts + 1)]
     out = []
     for r in range(parts):
@@ -539,7 +540,15 @@ def split_points(g: Graph, parts: int):
         sub = Graph(g.pose_type, g.edge_type, g.pose_estimate.copy(), ev, pick(g.measurement), pick(g.information),
                     None if g.pose_fixed is None else g.pose_fixed.copy(), g.point_estimate[p0:p1].copy(),
                     None if g.point_fixed is None else g.point_fixed[p0:p1].copy(), pick(g.robust_delta),
-                    g.focal_length, tuple(g.principal_point), f"{g.name}-shard{r}", {}, g.focal_length_y)
+                    g.focal_length, tuple(g.principal_point), f"{g.name}-shard{r}", {}, g.focal_length_y,
+                    stereo_bf=g.stereo_bf)
+        if r == 0 and g.num_pose_edges > 0:
+            # camera-side terms: added once, by rank 0, before the ranks sum
+            sub.pose_edge_vertex = g.pose_edge_vertex.copy()
+            sub.pose_edge_measurement = g.pose_edge_measurement.copy()
+            sub.pose_edge_information = g.pose_edge_information.copy()
+            if g.pose_edge_robust_delta is not None:
+                sub.pose_edge_robust_delta = g.pose_edge_robust_delta.copy()
         out.append((sub, np.arange(p0, p1)))
     return out
 

@@ -2570,6 +2570,13 @@ static int make_engine(g2oc_ctx* c) {
     set_error("a graph with a pose edge set runs Gauss-Newton, Levenberg-Marquardt or Dogleg");
     return G2OC_ERR_NOT_SUPPORTED;
   }
+  if (c->pose_edges() && c->shard_world > 1 && c->shard_rank != 0) {
+    // the ranks sum their parts of the reduced camera system, the gradient
+    // and chi2: the pose edges' terms are added once, by rank 0
+    set_error("sharded mode: the pose edge set belongs to rank 0's graph (rank %d has %d pose edges)", c->shard_rank,
+              (int)c->S.pact.size());
+    return G2OC_ERR_NOT_SUPPORTED;
+  }
   if (c->S.bal) {
     if (c->prm.precision == G2OC_PREC_MIXED) {
       set_error("the BAL block solver runs in FP64 (no mixed-precision form)");
@@ -3025,7 +3032,7 @@ int g2oc_download(g2oc_ctx* c, double* pose, double* point) {
 static int check_sharding(g2oc_ctx* c) {
   if (c->shard_world <= 1) return G2OC_OK;
   const Structure& S = c->S;
-  if (!S.ba || !S.schur || !S.tile_ok || c->pose_edges() || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY ||
+  if (!S.ba || !S.schur || !S.tile_ok || c->prm.linear_solver == G2OC_LINEAR_CHOLESKY ||
       pcg_mode() != PCG_AUTO ||
       c->prm.algorithm == G2OC_ALGO_DOGLEG || c->prm.algorithm == G2OC_ALGO_STRUCTURE_ONLY ||
       (c->prm.precision == G2OC_PREC_MIXED && c->prm.refine_max_iterations >= 0)) {

@@ -352,7 +352,10 @@ int g2oc_backward(g2oc_ctx* ctx, const double* dL_dx, double* dL_dmeas, double* 
  * the same points in the same order. Call before g2oc_upload; supported for
  * EdgeProjectXYZ2UV graphs with at least 32 free cameras, the PCG linear
  * solver, FP64 or mixed precision without FP64 refinement
- * (refine_max_iterations = -1). world = 1 switches it off. */
+ * (refine_max_iterations = -1). A pose edge set (g2oc_graph.num_pose_edges)
+ * belongs to rank 0's graph alone: its terms are added once, before the
+ * ranks sum; another rank's upload with pose edges returns
+ * G2OC_ERR_NOT_SUPPORTED. world = 1 switches it off. */
 #define G2OC_RED_SUM 0
 #define G2OC_RED_MAX 1
 #define G2OC_DT_F32 0

@@ -81,6 +81,19 @@ def test_oracle_hessian_is_the_sum_of_the_edge_sets(oracle_lib, graph):
     np.testing.assert_allclose(b[:n], b_p[:n] + b_q, rtol=1e-12, atol=1e-9 * np.abs(b_q).max())
 
 
+def test_split_points_gives_the_pose_edge_set_to_shard_0(graph):
+    # sharded mode: each rank adds its share of the projection edges' terms,
+    # rank 0 alone the pose edges' (backend.split_points)
+    from g2o_b200.backend import split_points
+    shards = split_points(graph, 3)
+    assert [s.num_pose_edges for s, _ in shards] == [graph.num_pose_edges, 0, 0]
+    s0 = shards[0][0]
+    assert np.array_equal(s0.pose_edge_vertex, graph.pose_edge_vertex)
+    assert np.array_equal(s0.pose_edge_measurement, graph.pose_edge_measurement)
+    assert np.array_equal(s0.pose_edge_information, graph.pose_edge_information)
+    assert sum(s.num_edges for s, _ in shards) == graph.num_edges
+
+
 def test_oracle_lm_decreases_chi2(oracle_lib, graph):
     o = oracle_lib.OracleProblem(graph, oracle_lib.default_params(), threads=4)
     _, st = o.optimize(10)

@@ -122,3 +122,31 @@ def test_sharding_rejects_unsupported_setups(backend):
         prob.optimize(1)
     with pytest.raises(Exception):
         backend.CudaProblem(g, fac.construct("lm_cuda"), shard=(2, 2, lambda *a: None))
+
+
+def test_shards_with_a_pose_edge_set(backend):
+    # the pose edges ride on shard 0 (split_points) and their terms are added
+    # once before the ranks sum; PCG solves converged (the stiff odometry
+    # blocks make the default stopping iteration depend on the last bits)
+    g = synth.ba_with_odometry(num_cameras=40, num_points=3000)
+    make = lambda: backend.default_params(pcg_tolerance=1e-14)  # noqa: E731
+    ref = backend.CudaProblem(g, make())
+    done_ref, st_ref = ref.optimize(ITER)
+    pose_ref, point_ref = ref.estimates()
+    ref.close()
+    out, shards, calls = run_sharded(backend, g, make, ITER, 2)
+    assert calls > 0
+    assert shards[0][0].num_pose_edges == g.num_pose_edges and shards[1][0].num_pose_edges == 0
+    for r, (done, st, pose, point) in enumerate(out):
+        assert done == done_ref
+        for a, b in zip(st, st_ref):
+            assert a["levenberg_iterations"] == b["levenberg_iterations"], (r, a, b)
+            assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (r, a["chi2"], b["chi2"])
+        assert np.abs(pose[:, :3] - pose_ref[:, :3]).max() < 1e-5
+        assert np.abs(point - point_ref[shards[r][1]]).max() < 1e-4
+
+
+def test_pose_edges_on_another_rank_are_refused(backend):
+    g = synth.ba_with_odometry(num_cameras=40, num_points=600)
+    with pytest.raises(Exception, match="rank 0"):
+        backend.CudaProblem(g, backend.default_params(), shard=(1, 2, lambda *a: None))
