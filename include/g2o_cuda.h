@@ -350,7 +350,8 @@ int g2oc_backward(g2oc_ctx* ctx, const double* dL_dx, double* dL_dmeas, double* 
  * on `stream` (the context's CUDA stream) and before the work enqueued on it
  * after the call returns; it returns 0 on success. Every rank calls it at
  * the same points in the same order. Call before g2oc_upload; supported for
- * EdgeProjectXYZ2UV graphs with at least 32 free cameras, the PCG linear
+ * the projection-edge graphs (EdgeProjectXYZ2UV, EdgeSE3ProjectXYZ,
+ * EdgeStereoSE3ProjectXYZ) with at least 32 free cameras, the PCG linear
  * solver, FP64 or mixed precision without FP64 refinement
  * (refine_max_iterations = -1). A pose edge set (g2oc_graph.num_pose_edges)
  * belongs to rank 0's graph alone: its terms are added once, before the

@@ -150,3 +150,22 @@ def test_pose_edges_on_another_rank_are_refused(backend):
     g = synth.ba_with_odometry(num_cameras=40, num_points=600)
     with pytest.raises(Exception, match="rank 0"):
         backend.CudaProblem(g, backend.default_params(), shard=(1, 2, lambda *a: None))
+
+
+def test_shards_of_a_stereo_graph(backend):
+    # EdgeStereoSE3ProjectXYZ (three-row edges): the shards keep bf
+    g = synth.stereo_bundle_adjustment(num_cameras=60, num_points=6000, seed=93)
+    make = lambda: backend.default_params()  # noqa: E731
+    ref = backend.CudaProblem(g, make())
+    done_ref, st_ref = ref.optimize(ITER)
+    pose_ref, point_ref = ref.estimates()
+    ref.close()
+    out, shards, calls = run_sharded(backend, g, make, ITER, 2)
+    assert calls > 0 and all(s.stereo_bf == g.stereo_bf for s, _ in shards)
+    for r, (done, st, pose, point) in enumerate(out):
+        assert done == done_ref
+        for a, b in zip(st, st_ref):
+            assert a["levenberg_iterations"] == b["levenberg_iterations"], (r, a, b)
+            assert abs(a["chi2"] - b["chi2"]) <= 1e-6 * b["chi2"], (r, a["chi2"], b["chi2"])
+        assert np.abs(pose[:, :3] - pose_ref[:, :3]).max() < 1e-6
+        assert np.abs(point - point_ref[shards[r][1]]).max() < 1e-5
