@@ -93,3 +93,15 @@ def test_split_points_partitions_the_bundle_adjustment():
             assert np.array_equal(s.edge_vertex[:, 1], g.edge_vertex[sel, 1])
             assert np.array_equal(s.measurement, g.measurement[sel])
             assert np.array_equal(s.information, g.information[sel])
+
+
+def test_split_points_keeps_the_edge_parameters():
+    """A stereo graph's shards keep bf (EdgeStereoSE3ProjectXYZ) and the
+    intrinsics; the measurement rows stay three wide."""
+    from g2o_b200 import backend, synth
+    g = synth.stereo_bundle_adjustment(num_cameras=12, num_points=600, seed=5)
+    for s, _ in backend.split_points(g, 2):
+        assert s.edge_type == g.edge_type and s.stereo_bf == g.stereo_bf and s.stereo_bf > 0
+        assert s.focal_length == g.focal_length and s.focal_length_y == g.focal_length_y
+        assert tuple(s.principal_point) == tuple(g.principal_point)
+        assert s.measurement.shape[1] == g.measurement.shape[1] == 3
